@@ -1,0 +1,330 @@
+#!/usr/bin/env python3
+"""Benchmark of the plain volume DMO on the Kuhn tet cube 48^3 (117,649 vertices, 663,552
+tetrahedra, 103,823 interior vertices, interior jitter +-0.3h, boundary fixed, mean ratio,
+8x8x8 grid, 3 levels, 20 iterations).
+
+One step = one complete 20-iteration optimisation of that mesh from its perturbed state
+(positions reset from a device copy at the start of the step; every colour launch of every
+iteration plus the per-iteration quality / monotonicity reduction). Metric: vertex updates
+per second = interior vertices x 20 x steps / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: every rank optimises its own copy of the mesh (replicas; the
+path has no exchange step), the time is the max over ranks and the value the sum of all
+ranks' vertex updates. ``--impl reference`` times the CPU restatement of the reference's
+own FP32 kernel (oracle/) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "vertex-updates/s (plain DMO, tet cube 48^3, 20 iterations)"
+UNIT = "vertex-updates/s"
+N_ITER = 20
+CUBE_N = 48
+
+
+def workload_config(extra=None):
+    cfg = {"workload": "tet cube 48^3 plain DMO (Kuhn, 117649 vertices / 663552 tets, jitter 0.3h, boundary fixed)",
+           "mesh_vertices": 117649, "mesh_tets": 663552, "inner_vertices": 103823,
+           "iterations_per_step": N_ITER, "grid": "8x8x8", "levels": 3, "quality": "mean ratio",
+           "parallelism": "replicas", "l2": "flushed between steps (256 MiB write)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def rank_info():
+    r = int(os.environ.get("RANK", "0"))
+    w = int(os.environ.get("WORLD_SIZE", "1"))
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    return r, w, lr
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline_sample(xyz, tets, max_seconds=20.0):
+    """Times the oracle's literal FP32 restatement of k_optimizeHierarchicalInnerTet on the
+    host cores over the first colour class(es) of the first iteration."""
+    from oracle import oracle as O
+    m = O.OracleMesh(O.TET, xyz, tets, color_seed=1)
+    x = m.xyz
+    cores = os.cpu_count() or 1
+    done = 0
+    t0 = time.perf_counter()
+    classes = 0
+    for (v0, v1) in m.color_ranges():
+        # bound the sample: at most ~max_seconds of CPU work
+        if time.perf_counter() - t0 > max_seconds:
+            break
+        x = m.dmo_color_ref32(x, v0, v1, 0.5, cores)
+        done += v1 - v0
+        classes += 1
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {classes} colour classes ({done} vertex updates) of iteration 1, "
+                      f"literal FP32 restatement of the reference kernel, OpenMP over {cores} threads, {dt:.1f} s"}
+
+
+def run_reference(args):
+    r, w, _ = rank_info()
+    if r != 0:
+        return 0
+    from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+    xyz, tets = G.config2()
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline_sample(xyz, tets, max_seconds=8.0 if args.steps > 3 else 15.0)
+        if i >= args.warmup:
+            vals.append(b["value"])
+            base = b
+    v = statistics.median(vals)
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 103823 * N_ITER / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Kuhn tet cube; the reference ships no meshes)",
+            "config": workload_config({"sample": "bounded CPU sample, see cpu_baseline"}),
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    r, world, lr = rank_info()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(lr)
+    dev = torch.device("cuda", lr)
+    from volumesurfacediscretemeshoptimization_b200 import build as B
+    if not os.path.exists(B.LIB_PATH):
+        raise SystemExit("libvsdmo.so missing: run __graft_entry__.build() first")
+    import volumesurfacediscretemeshoptimization_b200 as V
+    from volumesurfacediscretemeshoptimization_b200 import meshgen as G, _capi
+
+    lib = _capi.lib()
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+    xyz, tets = G.config2(seed=r)
+    # ---- device-resident workload -------------------------------------------------------------
+    mesh = V._Mesh.__new__(V.DMOMeshTet)
+    with torch.cuda.stream(stream):
+        d_xyz = torch.from_numpy(xyz).to(dev)
+        d_tets = torch.from_numpy(tets).to(dev)
+        stream.synchronize()
+        V.DMOMeshTet.__init__(mesh, None, None, 1, sp, (d_xyz.data_ptr(), d_tets.data_ptr(), len(xyz), len(tets)))
+    n_inner = mesh.info["nV"] - mesh.info["nSurf"]
+    opt = V.DMOTetClass(mesh, n_iter=10 ** 9)
+    launches_per_iter = opt.launches_per_iteration + 1
+    x0 = torch.empty(len(xyz) * 3, dtype=torch.float32, device=dev)
+    mesh.positions_to_device(x0.data_ptr(), original_order=False)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def reset():
+        _capi.check(lib.vsdmo_mesh_set_positions(mesh.h, C.c_void_p(x0.data_ptr()), 0, _capi.DEVICE))
+
+    def step():
+        reset()
+        opt.iterate(N_ITER)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    q_final = opt.getQuality()
+    # ---- timed region ----------------------------------------------------------------------------
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(lr) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+                ev[i][0].record(stream)
+                step()
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    total_updates = n_inner * N_ITER * args.steps * world
+    value = total_updates / (ms_max / 1e3)
+
+    # ---- roofline of the grid-search kernel (separate pass, same stream) -----------------------------
+    reset()
+    n_col = opt.launches_per_iteration
+    offs = mesh.array(V.A_COL_INNER)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for it in range(3):
+            for c in range(n_col):
+                _capi.check(lib.vsdmo_opt_run_color(opt.h, c))
+        e1.record(stream)
+    torch.cuda.synchronize()
+    dmo_ms = e0.elapsed_time(e1) / 3.0
+    bytes_per_update = 488  # 20 + 12k + 12|N| + 12 with k = 24 tets and |N| = 14 neighbours (interior Kuhn vertex)
+    bytes_iter = bytes_per_update * n_inner
+    achieved_gbs = bytes_iter / (dmo_ms / 1e3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "dmo_tet_config2_traffic.json")))
+        traffic = prof.get("dram_bytes_per_iteration")
+    except Exception:
+        pass
+    # FP32 work of the search as the reference formulates it: 3 levels x 512 candidates x 24
+    # tets x ~80 FP32 operations per mean-ratio evaluation (plus cbrt) per vertex update
+    ref_flop_per_update = 3 * 512 * 24 * 80
+    fp32_nominal_tflops = 148 * 128 * 2 * 1.965e9 / 1e12
+
+    # ---- end to end through the public API with host buffers ---------------------------------------------
+    pin_xyz = torch.from_numpy(xyz).pin_memory()
+    pin_tets = torch.from_numpy(tets).pin_memory()
+    out_host = torch.empty(len(xyz) * 3, dtype=torch.float32).pin_memory()
+    e2e_ms = []
+    for i in range(max(1, min(args.steps, 3)) + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            m2 = V._Mesh.__new__(V.DMOMeshTet)
+            h = C.c_void_p()
+            _capi.check(lib.vsdmo_mesh_create(_capi.TET, C.c_void_p(pin_xyz.data_ptr()), len(xyz),
+                                              C.c_void_p(pin_tets.data_ptr()), len(tets), _capi.HOST, 1,
+                                              C.c_void_p(sp), C.byref(h)))
+            m2.h = h
+            m2.info = {n: lib.vsdmo_mesh_info(h, j) for j, n in enumerate(V.INFO_NAMES)}
+            m2.nVertices = m2.info["nV"]
+            o2 = V.DMOTetClass(m2, n_iter=N_ITER)
+            o2.optimize()
+            _capi.check(lib.vsdmo_mesh_get_positions(h, C.c_void_p(out_host.data_ptr()), 1, _capi.HOST))
+            b.record(stream)
+        torch.cuda.synchronize()
+        o2.close()
+        m2.close()
+        if i > 0:  # first one is a warm-up
+            e2e_ms.append(a.elapsed_time(b))
+    e2e_ms_med = statistics.median(e2e_ms)
+    e2e_value = n_inner * N_ITER * world / (e2e_ms_med / 1e3)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Kuhn tet cube; the reference ships no meshes)",
+        "config": workload_config({"final_min_quality": q_final, "colours": n_col}),
+        "clocks": clk.summary(),
+        "gpu_launches": (launches_per_iter * N_ITER + 1) * args.steps,
+        "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": e2e_ms_med,
+                "h2d_bytes_per_step": int(xyz.nbytes + tets.nbytes), "d2h_bytes_per_step": int(xyz.nbytes),
+                "includes": "mesh build (connectivity + colouring) from pinned host arrays, 20 iterations, positions back to host"},
+        "roofline": {"bound": "hbm", "kernel": "k_dmo_tet", "achieved": achieved_gbs, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                     "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+                     "algorithmic_bytes_per_vertex_update": bytes_per_update,
+                     "kernel_ms_per_iteration": dmo_ms,
+                     "note": "compute-bound kernel: HBM fraction is reported as asked; see fp32"},
+        "fp32": {"reference_formulation_flop_per_vertex_update": ref_flop_per_update,
+                 "equivalent_tflops": ref_flop_per_update * n_inner / (dmo_ms / 1e3) / 1e12,
+                 "nominal_peak_tflops": fp32_nominal_tflops},
+    }
+    if r == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(xyz, tets)
+    if r == 0:
+        print(json.dumps(line), flush=True)
+    opt.close()
+    mesh.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,196 @@
+/*
+ * vsdmo.h -- C ABI of the B200 discrete mesh optimisation (DMO) engine.
+ *
+ * This is the drop-in boundary for the reference's C++ mesh/optimizer API
+ * (DanielZint/VolumeSurfaceDiscreteMeshOptimization). Every entry point below names the
+ * reference interface it replaces (path:line inside that project). The C++ classes with the
+ * reference's names live in include/vsdmo/DMO.hpp and call only these functions.
+ *
+ * Conventions
+ *   - Every call returns a vsdmo_status and never exits, throws or traps. A failed call
+ *     leaves a message for vsdmo_last_error() (thread-local).
+ *   - Handles are bound to the CUDA stream given at creation; calls on one handle are not
+ *     thread-safe. Distinct handles may be used from different host threads.
+ *   - The library owns everything it allocates. Caller pointers are borrowed for the
+ *     duration of the call. mem_space says whether a caller pointer is host or device memory.
+ *   - Vertex positions are float[3] per vertex (AoS, like the reference's Vec3f), element
+ *     indices int32 with 3 (tri), 4 (quad, tet) or 8 (hex) entries per element.
+ *   - The build reorders vertices exactly as the reference does (boundary / free / feature
+ *     partitions, each sorted by colour); vsdmo_mesh_permutation() returns new_of_old and
+ *     vsdmo_mesh_get_positions(..., original_order=1, ...) undoes it.
+ */
+#ifndef VSDMO_H
+#define VSDMO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define VSDMO_API __declspec(dllexport)
+#else
+#define VSDMO_API __attribute__((visibility("default")))
+#endif
+
+typedef enum vsdmo_status {
+    VSDMO_OK = 0,
+    VSDMO_E_ARG = 1,          /* invalid argument / size / null pointer                */
+    VSDMO_E_CUDA = 2,         /* CUDA runtime error                                    */
+    VSDMO_E_NONMANIFOLD = 3,  /* element list is not a manifold mesh                  */
+    VSDMO_E_VALENCE = 4,      /* a one-ring exceeds the kernels' shared-memory budget  */
+    VSDMO_E_MONOTONE = 5,     /* an element's quality fell below the last minimum      */
+    VSDMO_E_TIMEOUT = 6,      /* a bounded device-side wait gave up                    */
+    VSDMO_E_NAN = 7,          /* non-finite coordinates                                */
+    VSDMO_E_NOMEM = 8,        /* device allocation failed                              */
+    VSDMO_E_UNSUPPORTED = 9   /* combination of element type / options not supported   */
+} vsdmo_status;
+
+typedef enum vsdmo_elem_type {
+    VSDMO_TRI = 0,   /* triangle surface or flat 2D mesh  (DMOMeshTri,  mesh/DMOMeshTri.h:81-94)  */
+    VSDMO_QUAD = 1,  /* quad surface                      (DMOMeshQuad, mesh/DMOMeshQuad.h)      */
+    VSDMO_TET = 2,   /* tetrahedral volume                (DMOMeshTet,  mesh/DMOMeshTet.h:145-198) */
+    VSDMO_HEX = 3    /* hexahedral volume                 (DMOMeshHex,  mesh/DMOMeshHex.h)       */
+} vsdmo_elem_type;
+
+/* Same numbering as the reference's DMO::QualityCriterium (dmo/DMOQualityUtil.h:10-18). */
+typedef enum vsdmo_quality {
+    VSDMO_MEAN_RATIO = 0,
+    VSDMO_AREA = 1,
+    VSDMO_RIGHT_ANGLE = 2,
+    VSDMO_JACOBIAN = 3,
+    VSDMO_MIN_ANGLE = 4,
+    VSDMO_RADIUS_RATIO = 5,
+    VSDMO_MAX_ANGLE = 6
+} vsdmo_quality;
+
+typedef enum vsdmo_mem_space { VSDMO_HOST = 0, VSDMO_DEVICE = 1 } vsdmo_mem_space;
+
+/* ids for vsdmo_mesh_array / vsdmo_mesh_array_len (internal numbering, for golden tests) */
+typedef enum vsdmo_array_id {
+    VSDMO_A_XYZ = 0,             /* float [nV*3]      positions, internal order                */
+    VSDMO_A_NEW_OF_OLD = 1,      /* int32 [nV]        new index of every input vertex          */
+    VSDMO_A_ELEMS = 2,           /* int32 [nE*k]      elements, internal vertex numbering      */
+    VSDMO_A_SURF_TRIS = 3,       /* int32 [nTris*3]   surface triangles (tet: boundary faces)  */
+    VSDMO_A_HE_ROWPTR = 4,       /* int32 [nSurf+1]   halfedge CSR, CCW fan per vertex         */
+    VSDMO_A_HALFEDGES = 5,       /* int32 [nHE*4]     {target, opposite, face, next}           */
+    VSDMO_A_HF_ROWPTR = 6,       /* int32 [nV+1]      halfface CSR (tet)                       */
+    VSDMO_A_HALFFACES = 7,       /* int32 [4nT*3]     face opposite to the vertex, oriented    */
+    VSDMO_A_COL_FREE = 8,        /* int32 [nColorsFree+1]    colour offsets, free surface      */
+    VSDMO_A_COL_FEATURE = 9,     /* int32 [nColorsFeature+1] colour offsets, feature vertices  */
+    VSDMO_A_COL_INNER = 10,      /* int32 [nColorsInner+1]   colour offsets, volume interior   */
+    VSDMO_A_IS_BOUNDARY1D = 11,  /* uint8 [nSurf]                                              */
+    VSDMO_A_IS_FEATURE = 12,     /* uint8 [nSurf]                                              */
+    VSDMO_A_IS_BOUNDARY2D = 13,  /* uint8 [nV] (tet)                                           */
+    VSDMO_A_FACE_NORMALS = 14,   /* float [nTris*3]                                            */
+    VSDMO_A_VERTEX_NORMALS = 15  /* float [nSurf*3]                                            */
+} vsdmo_array_id;
+
+/* ids for vsdmo_mesh_info */
+typedef enum vsdmo_info_id {
+    VSDMO_I_NV = 0, VSDMO_I_NE, VSDMO_I_NSURF, VSDMO_I_NFEATURE, VSDMO_I_NTRIS, VSDMO_I_NHE,
+    VSDMO_I_NCOL_FREE, VSDMO_I_NCOL_FEATURE, VSDMO_I_NCOL_INNER, VSDMO_I_MAX_HE,
+    VSDMO_I_MAX_TETS, VSDMO_I_IS_FLAT, VSDMO_I_COUNT
+} vsdmo_info_id;
+
+typedef struct vsdmo_mesh_s* vsdmo_mesh_t;
+typedef struct vsdmo_opt_s* vsdmo_opt_t;
+
+/* Optimiser parameters. Defaults (vsdmo_params_default) follow the reference constructors:
+ * DMOTetClass(mesh, MEAN_RATIO, 0.5f, 30)  dmo/DMOTet.h:24,
+ * DMOTriFlatClass(mesh, MIN_ANGLE, 0.5f, 30) dmo/DMOTriFlat.h:25 (MEAN_RATIO is the only
+ * criterion implemented here so far, and the default), DMO_NQ = 8, DMO_DEPTH = 3
+ * (dmo/DMOConfig.h:4-6). */
+typedef struct vsdmo_params {
+    int   quality;        /* vsdmo_quality                                                  */
+    float grid_scale;     /* initial half-extent factor (0.5)                               */
+    int   n_iter;         /* iterations run by vsdmo_opt_optimize (30)                      */
+    int   grid_n;         /* candidates per axis; only 8 is implemented                     */
+    int   depth;          /* refinement levels; 1..4 (3)                                    */
+    int   fix_boundary;   /* 1: surface and feature passes are skipped (volume / flat runs  */
+                          /*    with the boundary held fixed); 0: reference behaviour       */
+    int   flat;           /* tri meshes: -1 = from the mesh (all z == 0), 0 = surface, 1 = 2D */
+    int   use_graph;      /* 1: each iteration is replayed from a captured CUDA graph       */
+    int   check_monotone; /* 1: per-element check against the last minimum (reference       */
+                          /*    k_updateCurrentQualities, dmo/DMOTet.cu:55-67)              */
+} vsdmo_params;
+
+/* ---- library --------------------------------------------------------------------------- */
+VSDMO_API const char* vsdmo_version(void);
+VSDMO_API const char* vsdmo_last_error(void);
+VSDMO_API const char* vsdmo_status_string(vsdmo_status s);
+VSDMO_API vsdmo_status vsdmo_params_default(int elem_type, vsdmo_params* out);
+
+/* ---- meshes ---------------------------------------------------------------------------- */
+/* Replaces DMOMeshTriFactory::create(int nVS, int nT, CudaArray<Vec3f>&, CudaArray<Triangle>&)
+ * (mesh/MeshFactory.cu:15-31), DMOMeshTetFactory::create (mesh/MeshFactory.cu:45-55, minus the
+ * file parsing) and the MeshTetGPU::init / MeshTriGPU::init builds they run
+ * (mesh/MeshTetGPU.cu:35-42, mesh/MeshTriGPU.cu:37-50). color_seed seeds the colouring
+ * priorities (the reference's live colouring is cusparseScsrcolor, VertexColoring.cu:128-153). */
+VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_vertices,
+                                         const int32_t* elems, int n_elems, int mem_space,
+                                         uint32_t color_seed, void* cuda_stream, vsdmo_mesh_t* out);
+/* Replaces the DMOMeshTri / DMOMeshTet destructors (mesh/DMOMeshBase.h:132-142). */
+VSDMO_API void vsdmo_mesh_destroy(vsdmo_mesh_t mesh);
+/* Counts the reference keeps as public members of DMOMeshBase / DMOMeshTet
+ * (mesh/DMOMeshBase.h:80-94, mesh/DMOMeshTet.h:145-151): nVertices, nVerticesSurf, ...   */
+VSDMO_API int vsdmo_mesh_info(vsdmo_mesh_t mesh, int which);
+VSDMO_API long vsdmo_mesh_array_len(vsdmo_mesh_t mesh, int array_id);
+/* Copies an internal array to host memory (the reference exposes them as device_ptr members
+ * of DMOMeshBase / DMOMeshTet, mesh/DMOMeshBase.h:97-105, mesh/DMOMeshTet.h:153-155). */
+VSDMO_API vsdmo_status vsdmo_mesh_array(vsdmo_mesh_t mesh, int array_id, void* host_out);
+/* new_of_old[nV]: the vertex permutation applied by the build (sortVerticesByBoundary2D,
+ * sortSurfVerticesByFeature, sort*RangeByColor: mesh/MeshTetGPU.cu:241-295,
+ * mesh/MeshTriGPU.cu:597-671). */
+VSDMO_API vsdmo_status vsdmo_mesh_permutation(vsdmo_mesh_t mesh, int32_t* host_new_of_old);
+/* Reads positions (DMOMeshBase::getVertexPoints, mesh/DMOMeshBase.h:146-148); with
+ * original_order = 1 they come back in the caller's input numbering. */
+VSDMO_API vsdmo_status vsdmo_mesh_get_positions(vsdmo_mesh_t mesh, float* xyz, int original_order,
+                                                int mem_space);
+/* Overwrites positions (internal or input numbering); used to restart an optimisation.
+ * With a device source the copy is queued on the handle's stream and the call returns
+ * without waiting; with a host source it returns after the copy. */
+VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* xyz, int original_order,
+                                                int mem_space);
+
+/* ---- optimiser ------------------------------------------------------------------------- */
+/* Replaces DMOTetClass / DMOTriFlatClass construction + init()
+ * (dmo/DMOTet.cu:82-125, dmo/DMOTriFlat.cu:84-126). */
+VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* params, vsdmo_opt_t* out);
+VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt);
+/* n_iter calls of doIteration() (dmo/DMOTet.cu:128-170, dmo/DMOTriFlat.cu:129-166). */
+VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t opt, int n_iter);
+/* DMOBaseClass::optimize() (dmo/DMOBase.h:44-52): iterate until isDone(). */
+VSDMO_API vsdmo_status vsdmo_opt_optimize(vsdmo_opt_t opt);
+/* DMOTetClass::isDone() (dmo/DMOTet.h:26). */
+VSDMO_API int vsdmo_opt_is_done(vsdmo_opt_t opt);
+VSDMO_API int vsdmo_opt_iterations_done(vsdmo_opt_t opt);
+/* DMOBaseClass::getQuality() (dmo/DMOBase.h:41): minimum quality after the last iteration. */
+VSDMO_API vsdmo_status vsdmo_opt_get_quality(vsdmo_opt_t opt, float* last_min_quality);
+/* DMOTetClass::findMinimumQuality() (dmo/DMOTet.cu:214-221), plus the mean quality. */
+VSDMO_API vsdmo_status vsdmo_opt_find_min_quality(vsdmo_opt_t opt, float* min_q, double* mean_q);
+/* DMOTetClass::getElementQualities(void*) (dmo/DMOTet.cu:235-240): one float per element in
+ * the internal element order. */
+VSDMO_API vsdmo_status vsdmo_opt_element_qualities(vsdmo_opt_t opt, float* out, int mem_space);
+/* DMOTetClass::getQualityHistogram (dmo/DMOTet.cu:202-212): n_cols bins of [0,1). */
+VSDMO_API vsdmo_status vsdmo_opt_quality_histogram(vsdmo_opt_t opt, int32_t* host_counts, int n_cols);
+/* DMOTetClass::displayQualityGPU (dmo/DMOTet.cu:188-200): prints the histogram table. */
+VSDMO_API vsdmo_status vsdmo_opt_display_quality(vsdmo_opt_t opt, int n_cols);
+/* Minimum and mean quality recorded after each completed iteration (the reference prints
+ * "it,q_min" lines, dmo/DMOTet.cu:167). Returns the count in *n (at most cap). */
+VSDMO_API vsdmo_status vsdmo_opt_history(vsdmo_opt_t opt, float* min_q, double* mean_q, int cap, int* n);
+/* One launch of the grid-search kernel over colour class `color` of the inner (tet) or free
+ * (flat tri) partition -- a single step of doIteration's colour loop, for parity tests and
+ * per-kernel timing. Asynchronous: it returns once the launch is queued on the stream. */
+VSDMO_API vsdmo_status vsdmo_opt_run_color(vsdmo_opt_t opt, int color);
+/* Number of grid-search kernel launches issued per iteration (for launch accounting). */
+VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t opt);
+
+/* Waits for all work queued on the handle's stream. */
+VSDMO_API vsdmo_status vsdmo_mesh_sync(vsdmo_mesh_t mesh);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VSDMO_H */

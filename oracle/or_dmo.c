@@ -1,0 +1,576 @@
+/*
+ * or_dmo.c -- CPU restatement of the reference DMO grid search and quality metrics
+ * (TEST INFRASTRUCTURE ONLY; see vsdmo_oracle.h).
+ *
+ * f64 functions restate the reference kernels literally, in double:
+ *   k_optimizeHierarchicalInnerTet   dmo/DMOTetImplCub.h:21-137
+ *   k_optimizeHierarchical2DFlat     dmo/DMOTriFlatImplCub.h:24-152
+ *   meanRatioMetricTet / ring        dmo/DMOQualityTet.h:119-162
+ *   meanRatioMetricTri2D / ring      dmo/DMOQualityTri.h:243-257, 297-311
+ *   DMO_NQ = 8, DMO_DEPTH = 3        dmo/DMOConfig.h:4-6
+ *   doIteration (fix-boundary mode)  dmo/DMOTet.cu:128-170, dmo/DMOTriFlat.cu:129-166
+ *
+ * f32 functions restate the same search with the product's float arithmetic, written
+ * independently of the product so that the CUDA result can be compared bit for bit:
+ *   - ring coordinates relative to the vertex, scaled by the power of two that brings the
+ *     largest per-axis extent into [0.5, 1) (exact, so it changes no rounding);
+ *   - per element: determinant affine in the candidate, det = d0 - n.p, and the sum of
+ *     squared edge lengths quadratic in it, L = C - 2 s.p + k|p|^2, evaluated with fmaf in
+ *     a fixed association (x, then y, then z);
+ *   - the ring minimum of the mean ratio compared through the monotone transform
+ *     det^2 / L^3 (tet) or A / L (triangle), kept as a fraction num/den and compared by
+ *     cross-multiplication; a ring with an inverted element is keyed by its most negative
+ *     determinant / area (the reference returns the negative volume / area there);
+ *   - per level the best candidate is the largest key with the lowest linear candidate
+ *     index (x fastest), moved to only if strictly better than the current position.
+ * Compile with -ffp-contract=off so that only the written fmaf calls fuse.
+ */
+#include "vsdmo_oracle.h"
+#include <math.h>
+#include <float.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+extern const int* or__hf_rowptr(const or_mesh* m);
+extern const int* or__hf(const or_mesh* m);
+extern const int* or__he_rowptr(const or_mesh* m);
+extern const int* or__he(const or_mesh* m);
+extern const int* or__elems(const or_mesh* m);
+extern const int* or__col(const or_mesh* m, int which);
+
+#define NQ 8
+#define DEPTH 3
+
+/* ======================================================================================= */
+/* reference metrics                                                                        */
+/* ======================================================================================= */
+
+double or_q_tet_mean_ratio_f64(const double* p0, const double* p1, const double* p2, const double* p3) {
+    double e[6][3];
+    for (int a = 0; a < 3; ++a) { e[0][a] = p1[a] - p0[a]; e[1][a] = p2[a] - p0[a]; e[2][a] = p3[a] - p0[a]; }
+    double cx = e[1][1] * e[2][2] - e[1][2] * e[2][1];
+    double cy = e[1][2] * e[2][0] - e[1][0] * e[2][2];
+    double cz = e[1][0] * e[2][1] - e[1][1] * e[2][0];
+    double volume = (1.0 / 6.0) * (e[0][0] * cx + e[0][1] * cy + e[0][2] * cz);
+    if (volume < 0.0) return volume;
+    double mu = cbrt(volume * volume);
+    for (int a = 0; a < 3; ++a) { e[3][a] = p2[a] - p1[a]; e[4][a] = p3[a] - p1[a]; e[5][a] = p3[a] - p2[a]; }
+    double l = 0.0;
+    for (int i = 0; i < 6; ++i) l += e[i][0] * e[i][0] + e[i][1] * e[i][1] + e[i][2] * e[i][2];
+    return 12.0 * cbrt(9.0) * mu / l;
+}
+
+float or_q_tet_mean_ratio_f32(const float* p0, const float* p1, const float* p2, const float* p3) {
+    float e[6][3];
+    for (int a = 0; a < 3; ++a) { e[0][a] = p1[a] - p0[a]; e[1][a] = p2[a] - p0[a]; e[2][a] = p3[a] - p0[a]; }
+    float cx = e[1][1] * e[2][2] - e[1][2] * e[2][1];
+    float cy = e[1][2] * e[2][0] - e[1][0] * e[2][2];
+    float cz = e[1][0] * e[2][1] - e[1][1] * e[2][0];
+    float volume = (1.f / 6.f) * ((e[0][0] * cx + e[0][1] * cy) + e[0][2] * cz);
+    if (volume < 0.f) return volume;
+    float mu = cbrtf(volume * volume);
+    for (int a = 0; a < 3; ++a) { e[3][a] = p2[a] - p1[a]; e[4][a] = p3[a] - p1[a]; e[5][a] = p3[a] - p2[a]; }
+    float l = 0.f;
+    for (int i = 0; i < 6; ++i) l += (e[i][0] * e[i][0] + e[i][1] * e[i][1]) + e[i][2] * e[i][2];
+    const float cbrtf9 = 2.0800838230519f;
+    return ((12.f * cbrtf9) * mu) / l;
+}
+
+double or_q_tri2d_mean_ratio_f64(const double* p0, const double* p1, const double* p2) {
+    const double* p[3] = { p0, p1, p2 };
+    double e[3][2], l = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        int j = (i + 1) % 3;
+        e[i][0] = p[j][0] - p[i][0]; e[i][1] = p[j][1] - p[i][1];
+        l += e[i][0] * e[i][0] + e[i][1] * e[i][1];
+    }
+    double area = e[0][0] * e[1][1] - e[0][1] * e[1][0];
+    if (area < 0.0) return area;
+    return 2.0 * sqrt(3.0) * area / l;
+}
+
+float or_q_tri2d_mean_ratio_f32(const float* p0, const float* p1, const float* p2) {
+    const float* p[3] = { p0, p1, p2 };
+    float e[3][2], el[3];
+    for (int i = 0; i < 3; ++i) {
+        int j = (i + 1) % 3;
+        e[i][0] = p[j][0] - p[i][0]; e[i][1] = p[j][1] - p[i][1];
+        el[i] = e[i][0] * e[i][0] + e[i][1] * e[i][1];
+    }
+    float l = (el[0] + el[1]) + el[2];
+    float area = e[0][0] * e[1][1] - e[0][1] * e[1][0];
+    if (area < 0.f) return area;
+    return ((2.f * sqrtf(3.f)) * area) / l;
+}
+
+void or_element_qualities_f64(const or_mesh* m, const double* xyz, double* q) {
+    int nE = or_mesh_info(m, OR_I_NE);
+    const int* el = or__elems(m);
+    if (or__hf_rowptr(m)) {
+        for (int t = 0; t < nE; ++t) {
+            const int* v = el + 4 * t;
+            q[t] = or_q_tet_mean_ratio_f64(xyz + 3 * v[0], xyz + 3 * v[1], xyz + 3 * v[2], xyz + 3 * v[3]);
+        }
+    } else {
+        for (int t = 0; t < nE; ++t) {
+            const int* v = el + 3 * t;
+            q[t] = or_q_tri2d_mean_ratio_f64(xyz + 3 * v[0], xyz + 3 * v[1], xyz + 3 * v[2]);
+        }
+    }
+}
+
+void or_element_qualities_f32(const or_mesh* m, const float* xyz, float* q) {
+    int nE = or_mesh_info(m, OR_I_NE);
+    const int* el = or__elems(m);
+    if (or__hf_rowptr(m)) {
+        for (int t = 0; t < nE; ++t) {
+            const int* v = el + 4 * t;
+            q[t] = or_q_tet_mean_ratio_f32(xyz + 3 * v[0], xyz + 3 * v[1], xyz + 3 * v[2], xyz + 3 * v[3]);
+        }
+    } else {
+        for (int t = 0; t < nE; ++t) {
+            const int* v = el + 3 * t;
+            q[t] = or_q_tri2d_mean_ratio_f32(xyz + 3 * v[0], xyz + 3 * v[1], xyz + 3 * v[2]);
+        }
+    }
+}
+
+/* ======================================================================================= */
+/* f64: literal restatement of the reference kernels                                        */
+/* ======================================================================================= */
+
+static double ring_q_tet_f64(int k, const double* ring, const double* p) {
+    double q = DBL_MAX;
+    for (int t = 0; t < k; ++t) {
+        double v = or_q_tet_mean_ratio_f64(p, ring + 9 * t, ring + 9 * t + 3, ring + 9 * t + 6);
+        q = fmin(q, v);
+    }
+    return q;
+}
+
+static void tet_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin) {
+    const int* rp = or__hf_rowptr(m);
+    const int* hf = or__hf(m);
+    int b = rp[v], k = rp[v + 1] - b;
+    if (k <= 0) return;
+    double* ring = (double*)malloc(sizeof(double) * 9 * (size_t)k);
+    double p0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
+    double md[3] = { -DBL_MAX, -DBL_MAX, -DBL_MAX };
+    for (int t = 0; t < k; ++t) for (int j = 0; j < 3; ++j) {
+        int u = hf[3 * (b + t) + j];
+        for (int a = 0; a < 3; ++a) {
+            ring[9 * t + 3 * j + a] = X[3 * u + a];
+            md[a] = fmax(md[a], fabs(X[3 * u + a] - p0[a]));
+        }
+    }
+    const double aff = 1.0 / (NQ - 1);
+    double ds = gs;
+    double cur[3] = { p0[0], p0[1], p0[2] };
+    double qMax[128], pMax[128][3];
+    for (int t = 0; t < 128; ++t) { qMax[t] = -DBL_MAX; pMax[t][0] = pMax[t][1] = pMax[t][2] = 0.0; }
+    int w = 0;
+    double mg = DBL_MAX;
+    for (int d = 0; d < DEPTH; ++d) {
+        double gmax[3], gmin[3];
+        for (int a = 0; a < 3; ++a) { gmax[a] = cur[a] + ds * md[a]; gmin[a] = cur[a] - ds * md[a]; }
+        double qLast = ring_q_tet_f64(k, ring, cur);
+        double best = -DBL_MAX, second = -DBL_MAX;
+        for (int t = 0; t < 128; ++t) {
+            for (int idx = 4 * t; idx < 4 * t + 4; ++idx) {
+                int i = idx % NQ, j = (idx / NQ) % NQ, kk = idx / (NQ * NQ);
+                double p[3];
+                p[0] = aff * (i * gmin[0] + (NQ - 1 - i) * gmax[0]);
+                p[1] = aff * (j * gmin[1] + (NQ - 1 - j) * gmax[1]);
+                p[2] = aff * (kk * gmin[2] + (NQ - 1 - kk) * gmax[2]);
+                double q = ring_q_tet_f64(k, ring, p);
+                if (q > best) { second = best; best = q; } else if (q > second) second = q;
+                if (q > qMax[t]) { qMax[t] = q; pMax[t][0] = p[0]; pMax[t][1] = p[1]; pMax[t][2] = p[2]; }
+            }
+        }
+        w = 0;
+        for (int t = 1; t < 128; ++t) if (qMax[t] > qMax[w]) w = t;
+        /* decision margins of this level: best vs runner-up, best vs current position */
+        mg = fmin(mg, best - second);
+        mg = fmin(mg, fabs(best - qLast));
+        if (qLast < qMax[w]) { cur[0] = pMax[w][0]; cur[1] = pMax[w][1]; cur[2] = pMax[w][2]; }
+        ds = ds * (2.0 / (NQ - 1));
+    }
+    double qOld = ring_q_tet_f64(k, ring, p0);
+    mg = fmin(mg, fabs(qMax[w] - qOld));
+    if (qOld < qMax[w]) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; X[3 * v + 2] = cur[2]; }
+    if (margin) *margin = mg;
+    free(ring);
+}
+
+static double ring_q_tri2d_f64(int n1, const double* ring, const double* p) {
+    double q = DBL_MAX;
+    for (int i = 0; i < n1 - 1; ++i) q = fmin(q, or_q_tri2d_mean_ratio_f64(p, ring + 3 * i, ring + 3 * (i + 1)));
+    return q;
+}
+
+static void tri2d_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin) {
+    const int* rp = or__he_rowptr(m);
+    const int* he = or__he(m);
+    int b = rp[v], k = rp[v + 1] - b;
+    if (k <= 0) return;
+    double* ring = (double*)malloc(sizeof(double) * 3 * ((size_t)k + 1));
+    double p0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
+    double md[3] = { -DBL_MAX, -DBL_MAX, -DBL_MAX };
+    for (int i = 0; i < k; ++i) {
+        int u = he[4 * (b + i)];
+        for (int a = 0; a < 3; ++a) { ring[3 * i + a] = X[3 * u + a]; md[a] = fmax(md[a], fabs(X[3 * u + a] - p0[a])); }
+    }
+    for (int a = 0; a < 3; ++a) ring[3 * k + a] = ring[a];
+    int n1 = k + 1;
+    const double aff = 1.0 / (NQ - 1);
+    double ds = gs;
+    double cur[3] = { p0[0], p0[1], p0[2] };
+    double lastMax = -DBL_MAX, mg = DBL_MAX;
+    for (int d = 0; d < DEPTH; ++d) {
+        double gmax[2], gmin[2];
+        for (int a = 0; a < 2; ++a) { gmax[a] = cur[a] + ds * md[a]; gmin[a] = cur[a] - ds * md[a]; }
+        double qLast = ring_q_tri2d_f64(n1, ring, cur);
+        double val[32], pp[32][2];
+        double best = -DBL_MAX, second = -DBL_MAX;
+        for (int t = 0; t < 32; ++t) {
+            int i1 = t / NQ, j1 = t % NQ, i2 = i1 + 4;
+            double p1[3] = { aff * (i1 * gmin[0] + (NQ - 1 - i1) * gmax[0]), aff * (j1 * gmin[1] + (NQ - 1 - j1) * gmax[1]), cur[2] };
+            double p2[3] = { aff * (i2 * gmin[0] + (NQ - 1 - i2) * gmax[0]), aff * (j1 * gmin[1] + (NQ - 1 - j1) * gmax[1]), cur[2] };
+            double q1 = ring_q_tri2d_f64(n1, ring, p1), q2 = ring_q_tri2d_f64(n1, ring, p2);
+            val[t] = q1; if (q2 > q1) val[t] = q2;
+            if (q1 > q2) { pp[t][0] = p1[0]; pp[t][1] = p1[1]; } else { pp[t][0] = p2[0]; pp[t][1] = p2[1]; }
+            double qs[2] = { q1, q2 };
+            for (int s = 0; s < 2; ++s) { if (qs[s] > best) { second = best; best = qs[s]; } else if (qs[s] > second) second = qs[s]; }
+        }
+        int w = 0;
+        for (int t = 1; t < 32; ++t) if (val[t] > val[w]) w = t;
+        mg = fmin(mg, best - second);
+        mg = fmin(mg, fabs(best - qLast));
+        if (qLast < val[w]) { cur[0] = pp[w][0]; cur[1] = pp[w][1]; }
+        lastMax = val[w];
+        ds = ds * (2.0 / (NQ - 1));
+    }
+    double qOld = ring_q_tri2d_f64(n1, ring, p0);
+    mg = fmin(mg, fabs(lastMax - qOld));
+    if (qOld < lastMax) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; }
+    if (margin) *margin = mg;
+    free(ring);
+}
+
+void or_dmo_tet_f64(const or_mesh* m, double* xyz, int v0, int v1, double gs, double* margin, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int v = v0; v < v1; ++v) tet_vertex_f64(m, xyz, v, gs, margin ? margin + (v - v0) : NULL);
+}
+
+void or_dmo_tri2d_f64(const or_mesh* m, double* xyz, int v0, int v1, double gs, double* margin, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int v = v0; v < v1; ++v) tri2d_vertex_f64(m, xyz, v, gs, margin ? margin + (v - v0) : NULL);
+}
+
+/* literal float restatement of k_optimizeHierarchicalInnerTet (the reference's own FP32
+ * arithmetic with cbrtf per element): the CPU baseline that bench.py times.                  */
+static float ring_q_tet_ref32(int k, const float* ring, const float* p) {
+    float q = FLT_MAX;
+    for (int t = 0; t < k; ++t) q = fminf(q, or_q_tet_mean_ratio_f32(p, ring + 9 * t, ring + 9 * t + 3, ring + 9 * t + 6));
+    return q;
+}
+
+static void tet_vertex_ref32(const or_mesh* m, float* X, int v, float gs) {
+    const int* rp = or__hf_rowptr(m);
+    const int* hf = or__hf(m);
+    int b = rp[v], k = rp[v + 1] - b;
+    if (k <= 0) return;
+    float* ring = (float*)malloc(sizeof(float) * 9 * (size_t)k);
+    float p0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
+    float md[3] = { -FLT_MAX, -FLT_MAX, -FLT_MAX };
+    for (int t = 0; t < k; ++t) for (int j = 0; j < 3; ++j) {
+        int u = hf[3 * (b + t) + j];
+        for (int a = 0; a < 3; ++a) { ring[9 * t + 3 * j + a] = X[3 * u + a]; md[a] = fmaxf(md[a], fabsf(X[3 * u + a] - p0[a])); }
+    }
+    const float aff = 1.f / (float)(NQ - 1);
+    float ds = gs, cur[3] = { p0[0], p0[1], p0[2] };
+    float qMax[128], pMax[128][3];
+    for (int t = 0; t < 128; ++t) { qMax[t] = -FLT_MAX; pMax[t][0] = pMax[t][1] = pMax[t][2] = 0.f; }
+    int w = 0;
+    for (int d = 0; d < DEPTH; ++d) {
+        float gmax[3], gmin[3];
+        for (int a = 0; a < 3; ++a) { gmax[a] = cur[a] + ds * md[a]; gmin[a] = cur[a] - ds * md[a]; }
+        float qLast = ring_q_tet_ref32(k, ring, cur);
+        for (int t = 0; t < 128; ++t)
+            for (int idx = 4 * t; idx < 4 * t + 4; ++idx) {
+                int i = idx % NQ, j = (idx / NQ) % NQ, kk = idx / (NQ * NQ);
+                float p[3] = { aff * (i * gmin[0] + (NQ - 1 - i) * gmax[0]), aff * (j * gmin[1] + (NQ - 1 - j) * gmax[1]),
+                               aff * (kk * gmin[2] + (NQ - 1 - kk) * gmax[2]) };
+                float q = ring_q_tet_ref32(k, ring, p);
+                if (q > qMax[t]) { qMax[t] = q; pMax[t][0] = p[0]; pMax[t][1] = p[1]; pMax[t][2] = p[2]; }
+            }
+        w = 0;
+        for (int t = 1; t < 128; ++t) if (qMax[t] > qMax[w]) w = t;
+        if (qLast < qMax[w]) { cur[0] = pMax[w][0]; cur[1] = pMax[w][1]; cur[2] = pMax[w][2]; }
+        ds = ds * (2.f / (NQ - 1));
+    }
+    float qOld = ring_q_tet_ref32(k, ring, p0);
+    if (qOld < qMax[w]) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; X[3 * v + 2] = cur[2]; }
+    free(ring);
+}
+
+void or_dmo_tet_ref32(const or_mesh* m, float* xyz, int v0, int v1, float gs, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+    for (int v = v0; v < v1; ++v) tet_vertex_ref32(m, xyz, v, gs);
+}
+
+/* ======================================================================================= */
+/* f32: the product's arithmetic                                                            */
+/* ======================================================================================= */
+
+static inline float grid_offset(int i) { return (float)(NQ - 1 - 2 * i) / (float)(NQ - 1); }
+
+/* per tet: (nn.x, nn.y, nn.z, d0) and (m.x, m.y, m.z, C) from scaled a, b, c */
+static void tet_coeffs(const float* a, const float* b, const float* c, float* K) {
+    float ux = b[0] - a[0], uy = b[1] - a[1], uz = b[2] - a[2];
+    float wx = c[0] - a[0], wy = c[1] - a[1], wz = c[2] - a[2];
+    float vx = c[0] - b[0], vy = c[1] - b[1], vz = c[2] - b[2];
+    float nx = uy * wz - uz * wy;
+    float ny = uz * wx - ux * wz;
+    float nz = ux * wy - uy * wx;
+    float d0 = (a[0] * nx + a[1] * ny) + a[2] * nz;
+    float sx = (a[0] + b[0]) + c[0], sy = (a[1] + b[1]) + c[1], sz = (a[2] + b[2]) + c[2];
+    float a2 = (a[0] * a[0] + a[1] * a[1]) + a[2] * a[2];
+    float b2 = (b[0] * b[0] + b[1] * b[1]) + b[2] * b[2];
+    float c2 = (c[0] * c[0] + c[1] * c[1]) + c[2] * c[2];
+    float u2 = (ux * ux + uy * uy) + uz * uz;
+    float w2 = (wx * wx + wy * wy) + wz * wz;
+    float v2 = (vx * vx + vy * vy) + vz * vz;
+    K[0] = -nx; K[1] = -ny; K[2] = -nz; K[3] = d0;
+    K[4] = -2.0f * sx; K[5] = -2.0f * sy; K[6] = -2.0f * sz;
+    K[7] = ((((a2 + b2) + c2) + u2) + w2) + v2;
+}
+
+static float tet_key(int k, const float* K, float x, float y, float z) {
+    float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    float N = 0.f, D = 1.f, dmin = 0.f;
+    for (int t = 0; t < k; ++t) {
+        const float* c = K + 8 * t;
+        float detA = fmaf(c[0], x, c[3]);
+        float LA = c[7] + fmaf(c[4], x, tx);
+        float detB = fmaf(c[1], y, detA);
+        float LB = LA + fmaf(c[5], y, ty);
+        float det = fmaf(c[2], z, detB);
+        float L = LB + fmaf(c[6], z, tz);
+        float num = det * det;
+        float den = (L * L) * L;
+        if (t == 0) { N = num; D = den; dmin = det; continue; }
+        if (num * D < N * den) { N = num; D = den; }
+        dmin = fminf(dmin, det);
+    }
+    return dmin < 0.f ? dmin : N / D;
+}
+
+static void tet_vertex_f32(const or_mesh* m, float* X, int v, float gs) {
+    const int* rp = or__hf_rowptr(m);
+    const int* hf = or__hf(m);
+    int b = rp[v], k = rp[v + 1] - b;
+    if (k <= 0) return;
+    float c0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
+    float* r = (float*)malloc(sizeof(float) * 9 * (size_t)k);
+    float* K = (float*)malloc(sizeof(float) * 8 * (size_t)k);
+    float md[3] = { 0.f, 0.f, 0.f };
+    for (int t = 0; t < k; ++t) for (int j = 0; j < 3; ++j) {
+        int u = hf[3 * (b + t) + j];
+        for (int a = 0; a < 3; ++a) {
+            float d = X[3 * u + a] - c0[a];
+            r[9 * t + 3 * j + a] = d;
+            md[a] = fmaxf(md[a], fabsf(d));
+        }
+    }
+    float mm = fmaxf(md[0], fmaxf(md[1], md[2]));
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) { free(r); free(K); return; }
+    int ex; (void)frexpf(mm, &ex);
+    for (int i = 0; i < 9 * k; ++i) r[i] = ldexpf(r[i], -ex);
+    for (int a = 0; a < 3; ++a) md[a] = ldexpf(md[a], -ex);
+    for (int t = 0; t < k; ++t) tet_coeffs(r + 9 * t, r + 9 * t + 3, r + 9 * t + 6, K + 8 * t);
+    float dlt[3] = { 0.f, 0.f, 0.f };
+    float qLast = tet_key(k, K, 0.f, 0.f, 0.f);
+    int moved = 0;
+    float ds = gs;
+    for (int d = 0; d < DEPTH; ++d) {
+        float xs[NQ], ys[NQ], zs[NQ];
+        float Sx = ds * md[0], Sy = ds * md[1], Sz = ds * md[2];
+        for (int i = 0; i < NQ; ++i) {
+            float o = grid_offset(i);
+            xs[i] = fmaf(o, Sx, dlt[0]); ys[i] = fmaf(o, Sy, dlt[1]); zs[i] = fmaf(o, Sz, dlt[2]);
+        }
+        float best = -FLT_MAX; int bi = -1;
+        for (int idx = 0; idx < NQ * NQ * NQ; ++idx) {
+            int i = idx % NQ, j = (idx / NQ) % NQ, kk = idx / (NQ * NQ);
+            float q = tet_key(k, K, xs[i], ys[j], zs[kk]);
+            if (q > best) { best = q; bi = idx; }
+        }
+        if (bi >= 0 && qLast < best) {
+            dlt[0] = xs[bi % NQ]; dlt[1] = ys[(bi / NQ) % NQ]; dlt[2] = zs[bi / (NQ * NQ)];
+            qLast = best; moved = 1;
+        }
+        ds = ds * (2.0f / (float)(NQ - 1));
+    }
+    if (moved) {
+        X[3 * v] = c0[0] + ldexpf(dlt[0], ex);
+        X[3 * v + 1] = c0[1] + ldexpf(dlt[1], ex);
+        X[3 * v + 2] = c0[2] + ldexpf(dlt[2], ex);
+    }
+    free(r); free(K);
+}
+
+/* per triangle (p, a, b): (nA.x, nA.y, A0, m.x, m.y, C) */
+static void tri_coeffs(const float* a, const float* b, float* K) {
+    float ux = b[0] - a[0], uy = b[1] - a[1];
+    K[0] = -uy; K[1] = ux;
+    K[2] = a[0] * uy - a[1] * ux;
+    K[3] = -2.0f * (a[0] + b[0]); K[4] = -2.0f * (a[1] + b[1]);
+    K[5] = ((a[0] * a[0] + a[1] * a[1]) + (b[0] * b[0] + b[1] * b[1])) + (ux * ux + uy * uy);
+}
+
+static float tri_key(int k, const float* K, float x, float y) {
+    float tx = (2.0f * x) * x, ty = (2.0f * y) * y;
+    float N = 0.f, D = 1.f, amin = 0.f;
+    for (int t = 0; t < k; ++t) {
+        const float* c = K + 6 * t;
+        float A = fmaf(c[1], y, fmaf(c[0], x, c[2]));
+        float L = (c[5] + fmaf(c[3], x, tx)) + fmaf(c[4], y, ty);
+        if (t == 0) { N = A; D = L; amin = A; continue; }
+        if (A * D < N * L) { N = A; D = L; }
+        amin = fminf(amin, A);
+    }
+    return amin < 0.f ? amin : N / D;
+}
+
+static void tri2d_vertex_f32(const or_mesh* m, float* X, int v, float gs) {
+    const int* rp = or__he_rowptr(m);
+    const int* he = or__he(m);
+    int b = rp[v], k = rp[v + 1] - b;
+    if (k <= 0) return;
+    float c0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
+    float* r = (float*)malloc(sizeof(float) * 2 * ((size_t)k + 1));
+    float* K = (float*)malloc(sizeof(float) * 6 * (size_t)k);
+    float md[2] = { 0.f, 0.f };
+    for (int i = 0; i < k; ++i) {
+        int u = he[4 * (b + i)];
+        for (int a = 0; a < 2; ++a) { float d = X[3 * u + a] - c0[a]; r[2 * i + a] = d; md[a] = fmaxf(md[a], fabsf(d)); }
+    }
+    float mm = fmaxf(md[0], md[1]);
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) { free(r); free(K); return; }
+    int ex; (void)frexpf(mm, &ex);
+    for (int i = 0; i < 2 * k; ++i) r[i] = ldexpf(r[i], -ex);
+    r[2 * k] = r[0]; r[2 * k + 1] = r[1];
+    md[0] = ldexpf(md[0], -ex); md[1] = ldexpf(md[1], -ex);
+    for (int t = 0; t < k; ++t) tri_coeffs(r + 2 * t, r + 2 * t + 2, K + 6 * t);
+    float dlt[2] = { 0.f, 0.f };
+    float qOld = tri_key(k, K, 0.f, 0.f);
+    float qLast = qOld, lastMax = -FLT_MAX;
+    float ds = gs;
+    for (int d = 0; d < DEPTH; ++d) {
+        float xs[NQ], ys[NQ];
+        float Sx = ds * md[0], Sy = ds * md[1];
+        for (int i = 0; i < NQ; ++i) { float o = grid_offset(i); xs[i] = fmaf(o, Sx, dlt[0]); ys[i] = fmaf(o, Sy, dlt[1]); }
+        float bv = 0.f; int bt = -1; float bx = 0.f, by = 0.f;
+        for (int t = 0; t < 32; ++t) {
+            int i1 = t / NQ, j1 = t % NQ, i2 = i1 + 4;
+            float q1 = tri_key(k, K, xs[i1], ys[j1]);
+            float q2 = tri_key(k, K, xs[i2], ys[j1]);
+            float val = q1; if (q2 > q1) val = q2;
+            if (bt < 0 || val > bv) {
+                bv = val; bt = t;
+                if (q1 > q2) { bx = xs[i1]; by = ys[j1]; } else { bx = xs[i2]; by = ys[j1]; }
+            }
+        }
+        if (qLast < bv) { dlt[0] = bx; dlt[1] = by; qLast = bv; }
+        lastMax = bv;
+        ds = ds * (2.0f / (float)(NQ - 1));
+    }
+    if (qOld < lastMax) {
+        X[3 * v] = c0[0] + ldexpf(dlt[0], ex);
+        X[3 * v + 1] = c0[1] + ldexpf(dlt[1], ex);
+    }
+    free(r); free(K);
+}
+
+void or_dmo_tet_f32(const or_mesh* m, float* xyz, int v0, int v1, float gs, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int v = v0; v < v1; ++v) tet_vertex_f32(m, xyz, v, gs);
+}
+
+void or_dmo_tri2d_f32(const or_mesh* m, float* xyz, int v0, int v1, float gs, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int v = v0; v < v1; ++v) tri2d_vertex_f32(m, xyz, v, gs);
+}
+
+/* ======================================================================================= */
+/* optimisation loops (fix-boundary mode)                                                   */
+/* ======================================================================================= */
+
+static void stats_f64(const double* q, int n, double* mn, double* mean) {
+    double a = DBL_MAX, s = 0.0;
+    for (int i = 0; i < n; ++i) { a = fmin(a, q[i]); s += q[i]; }
+    *mn = a; *mean = s / n;
+}
+
+void or_optimize_f32(const or_mesh* m, float* xyz, int n_iter, float gs, int nthreads, double* min_hist, double* mean_hist) {
+    int isTet = or__hf_rowptr(m) != NULL;
+    int nE = or_mesh_info(m, OR_I_NE);
+    int nc = isTet ? or_mesh_info(m, OR_I_NCOL_INNER) : or_mesh_info(m, OR_I_NCOL_FREE);
+    const int* off = isTet ? or__col(m, 2) : or__col(m, 0);
+    float* q = (float*)malloc(sizeof(float) * (size_t)nE);
+    double* qd = (double*)malloc(sizeof(double) * (size_t)nE);
+    for (int it = 0; it < n_iter; ++it) {
+        for (int c = 0; c < nc; ++c) {
+            if (isTet) or_dmo_tet_f32(m, xyz, off[c], off[c + 1], gs, nthreads);
+            else or_dmo_tri2d_f32(m, xyz, off[c], off[c + 1], gs, nthreads);
+        }
+        if (min_hist || mean_hist) {
+            or_element_qualities_f32(m, xyz, q);
+            for (int i = 0; i < nE; ++i) qd[i] = q[i];
+            double mn, mean; stats_f64(qd, nE, &mn, &mean);
+            if (min_hist) min_hist[it] = mn;
+            if (mean_hist) mean_hist[it] = mean;
+        }
+    }
+    free(q); free(qd);
+}
+
+void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double gs, int nthreads, double* min_hist, double* mean_hist) {
+    int isTet = or__hf_rowptr(m) != NULL;
+    int nE = or_mesh_info(m, OR_I_NE);
+    int nc = isTet ? or_mesh_info(m, OR_I_NCOL_INNER) : or_mesh_info(m, OR_I_NCOL_FREE);
+    const int* off = isTet ? or__col(m, 2) : or__col(m, 0);
+    double* q = (double*)malloc(sizeof(double) * (size_t)nE);
+    for (int it = 0; it < n_iter; ++it) {
+        for (int c = 0; c < nc; ++c) {
+            if (isTet) or_dmo_tet_f64(m, xyz, off[c], off[c + 1], gs, NULL, nthreads);
+            else or_dmo_tri2d_f64(m, xyz, off[c], off[c + 1], gs, NULL, nthreads);
+        }
+        if (min_hist || mean_hist) {
+            or_element_qualities_f64(m, xyz, q);
+            double mn, mean; stats_f64(q, nE, &mn, &mean);
+            if (min_hist) min_hist[it] = mn;
+            if (mean_hist) mean_hist[it] = mean;
+        }
+    }
+    free(q);
+}

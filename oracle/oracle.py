@@ -1,0 +1,186 @@
+"""ctypes wrapper of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loaded by tests/, ``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py``;
+the product never imports this module. See ``vsdmo_oracle.h`` for what is restated and
+from which reference lines.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+TRI, QUAD, TET, HEX = 0, 1, 2, 3
+
+A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
+    A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
+    A_FACE_NORMALS, A_VERTEX_NORMALS = range(16)
+ARRAY_DTYPES = {A_XYZ: np.float32, A_FACE_NORMALS: np.float32, A_VERTEX_NORMALS: np.float32,
+                A_IS_BOUNDARY1D: np.uint8, A_IS_FEATURE: np.uint8, A_IS_BOUNDARY2D: np.uint8}
+ARRAY_NAMES = {A_XYZ: "xyz", A_NEW_OF_OLD: "new_of_old", A_ELEMS: "elems", A_SURF_TRIS: "surf_tris",
+               A_HE_ROWPTR: "he_rowptr", A_HALFEDGES: "halfedges", A_HF_ROWPTR: "hf_rowptr",
+               A_HALFFACES: "halffaces", A_COL_FREE: "col_free", A_COL_FEATURE: "col_feature",
+               A_COL_INNER: "col_inner", A_IS_BOUNDARY1D: "is_boundary1d", A_IS_FEATURE: "is_feature",
+               A_IS_BOUNDARY2D: "is_boundary2d", A_FACE_NORMALS: "face_normals",
+               A_VERTEX_NORMALS: "vertex_normals"}
+I_NAMES = ["nV", "nE", "nSurf", "nFeature", "nTris", "nHE", "nColorsFree", "nColorsFeature",
+           "nColorsInner", "maxNumHalfedges", "maxNumTetrahedra", "isFlat"]
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P, I, F, D, U = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_uint32
+        L.or_mesh_build.restype = P
+        L.or_mesh_build.argtypes = [I, I, P, I, P, U, C.c_char_p, I]
+        L.or_mesh_free.argtypes = [P]
+        L.or_mesh_info.argtypes = [P, I]
+        L.or_mesh_array_len.restype = C.c_long
+        L.or_mesh_array_len.argtypes = [P, I]
+        L.or_mesh_array.argtypes = [P, I, P]
+        L.or_color_jpl.argtypes = [I, P, P, U, P]
+        L.or_priority.restype = U
+        L.or_priority.argtypes = [U, U]
+        for n in ("or_dmo_tet_f32", "or_dmo_tri2d_f32", "or_dmo_tet_ref32"):
+            getattr(L, n).argtypes = [P, P, I, I, F, I]
+        for n in ("or_dmo_tet_f64", "or_dmo_tri2d_f64"):
+            getattr(L, n).argtypes = [P, P, I, I, D, P, I]
+        L.or_element_qualities_f64.argtypes = [P, P, P]
+        L.or_element_qualities_f32.argtypes = [P, P, P]
+        L.or_optimize_f32.argtypes = [P, P, I, F, I, P, P]
+        L.or_optimize_f64.argtypes = [P, P, I, D, I, P, P]
+        L.or_q_tet_mean_ratio_f64.restype = D
+        L.or_q_tet_mean_ratio_f64.argtypes = [P, P, P, P]
+        L.or_q_tet_mean_ratio_f32.restype = F
+        L.or_q_tet_mean_ratio_f32.argtypes = [P, P, P, P]
+        L.or_q_tri2d_mean_ratio_f64.restype = D
+        L.or_q_tri2d_mean_ratio_f64.argtypes = [P, P, P]
+        L.or_q_tri2d_mean_ratio_f32.restype = F
+        L.or_q_tri2d_mean_ratio_f32.argtypes = [P, P, P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class OracleMesh:
+    """Connectivity, colouring and DMO of the reference, on the CPU."""
+
+    def __init__(self, elem_type, xyz, elems, color_seed=1):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+        elems = np.ascontiguousarray(elems, dtype=np.int32)
+        err = C.create_string_buffer(512)
+        self.h = lib().or_mesh_build(elem_type, len(xyz), _p(xyz), len(elems), _p(elems),
+                                     color_seed, err, 512)
+        if not self.h:
+            raise ValueError("oracle mesh build failed: " + err.value.decode())
+        self.elem_type = elem_type
+        self.info = {n: lib().or_mesh_info(self.h, i) for i, n in enumerate(I_NAMES)}
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_mesh_free(self.h)
+            self.h = None
+
+    def array(self, aid):
+        n = lib().or_mesh_array_len(self.h, aid)
+        out = np.zeros(max(n, 0), dtype=ARRAY_DTYPES.get(aid, np.int32))
+        if n > 0:
+            lib().or_mesh_array(self.h, aid, _p(out))
+        return out
+
+    def arrays(self):
+        return {ARRAY_NAMES[a]: self.array(a) for a in ARRAY_NAMES}
+
+    @property
+    def xyz(self):
+        return self.array(A_XYZ).reshape(-1, 3)
+
+    def color_ranges(self):
+        """(pass, start, end) of every colour class in doIteration order."""
+        if self.elem_type == TET:
+            off = self.array(A_COL_INNER)
+        else:
+            off = self.array(A_COL_FREE)
+        return [(int(off[c]), int(off[c + 1])) for c in range(len(off) - 1)]
+
+    # ---- DMO steps ----------------------------------------------------------------------
+    def dmo_color_f32(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        fn = lib().or_dmo_tet_f32 if self.elem_type == TET else lib().or_dmo_tri2d_f32
+        fn(self.h, _p(xyz), v0, v1, grid_scale, nthreads)
+        return xyz
+
+    def dmo_color_ref32(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
+        """The reference kernel's own float arithmetic (tet interior only)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        lib().or_dmo_tet_ref32(self.h, _p(xyz), v0, v1, grid_scale, nthreads)
+        return xyz
+
+    def dmo_color_f64(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        margin = np.zeros(max(v1 - v0, 1), dtype=np.float64)
+        fn = lib().or_dmo_tet_f64 if self.elem_type == TET else lib().or_dmo_tri2d_f64
+        fn(self.h, _p(xyz), v0, v1, grid_scale, _p(margin), nthreads)
+        return xyz, margin[: v1 - v0]
+
+    def optimize_f32(self, xyz, n_iter, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        mn = np.zeros(n_iter); mean = np.zeros(n_iter)
+        lib().or_optimize_f32(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
+        return xyz, mn, mean
+
+    def optimize_f64(self, xyz, n_iter, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        mn = np.zeros(n_iter); mean = np.zeros(n_iter)
+        lib().or_optimize_f64(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
+        return xyz, mn, mean
+
+    def element_qualities_f64(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        q = np.zeros(self.info["nE"], dtype=np.float64)
+        lib().or_element_qualities_f64(self.h, _p(xyz), _p(q))
+        return q
+
+    def element_qualities_f32(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+        q = np.zeros(self.info["nE"], dtype=np.float32)
+        lib().or_element_qualities_f32(self.h, _p(xyz), _p(q))
+        return q
+
+
+def color_jpl(rowptr, col, seed=1):
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    n = len(rowptr) - 1
+    colors = np.zeros(n, dtype=np.int32)
+    nc = lib().or_color_jpl(n, _p(rowptr), _p(col), seed, _p(colors))
+    return colors, nc
+
+
+def q_tet(p, dtype=np.float64):
+    p = [np.ascontiguousarray(x, dtype=dtype) for x in p]
+    f = lib().or_q_tet_mean_ratio_f64 if dtype == np.float64 else lib().or_q_tet_mean_ratio_f32
+    return f(*[_p(x) for x in p])
+
+
+def q_tri2d(p, dtype=np.float64):
+    p = [np.ascontiguousarray(x, dtype=dtype) for x in p]
+    f = lib().or_q_tri2d_mean_ratio_f64 if dtype == np.float64 else lib().or_q_tri2d_mean_ratio_f32
+    return f(*[_p(x) for x in p])

@@ -1,0 +1,106 @@
+/*
+ * vsdmo_oracle.h -- CPU restatement of the reference DMO path (TEST INFRASTRUCTURE ONLY).
+ *
+ * This library is the checker for the CUDA product in
+ * volumesurfacediscretemeshoptimization_b200/. Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py may load it. Nothing in the product links
+ * or calls it.
+ *
+ * Parity status: PARTIAL PIN. The reference repository ships no tests, no golden vectors and
+ * no sample meshes, and its live colouring is the closed cusparseScsrcolor. The restatement
+ * is pinned by (a) known-answer cases the reference's formulas fix exactly (regular
+ * simplices / unit cube = quality 1, flipped elements return their signed volume/area,
+ * unperturbed structured meshes are fixed points) and (b) golden fixtures produced by this
+ * restatement and committed under tests/golden/. See the file header of each .c file for
+ * the reference lines each function follows.
+ *
+ * Two arithmetic modes of the DMO grid search are provided:
+ *   *_f64 : the reference kernels' algorithm and formulas (mean ratio with cbrt, candidate
+ *           grid in absolute coordinates, per-thread carried maxima) evaluated in double;
+ *   *_f32 : the product's float arithmetic (local, power-of-two scaled coordinates, affine
+ *           per-element determinant and quadratic edge-length sums, ring minimum kept as a
+ *           fraction), written independently here so the GPU result can be checked bitwise.
+ */
+#ifndef VSDMO_ORACLE_H
+#define VSDMO_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OR_TRI = 0, OR_QUAD = 1, OR_TET = 2, OR_HEX = 3 };
+
+/* array ids for or_mesh_array / or_mesh_array_len (same ids as the product's C ABI) */
+enum {
+    OR_A_XYZ = 0,          /* float [nV*3] permuted positions                       */
+    OR_A_NEW_OF_OLD = 1,   /* int   [nV]                                            */
+    OR_A_ELEMS = 2,        /* int   [nE*k] remapped elements                        */
+    OR_A_SURF_TRIS = 3,    /* int   [nTris*3] surface triangles (tet: boundary)      */
+    OR_A_HE_ROWPTR = 4,    /* int   [nSurf+1]                                       */
+    OR_A_HALFEDGES = 5,    /* int   [nHE*4] target, opposite, face, next            */
+    OR_A_HF_ROWPTR = 6,    /* int   [nV+1]  (tet)                                   */
+    OR_A_HALFFACES = 7,    /* int   [4nT*3] (tet)                                   */
+    OR_A_COL_FREE = 8,     /* int   [nColorsFree+1]                                 */
+    OR_A_COL_FEATURE = 9,  /* int   [nColorsFeature+1]                              */
+    OR_A_COL_INNER = 10,   /* int   [nColorsInner+1]                                */
+    OR_A_IS_BOUNDARY1D = 11, /* uint8 [nSurf]                                       */
+    OR_A_IS_FEATURE = 12,  /* uint8 [nSurf]                                         */
+    OR_A_IS_BOUNDARY2D = 13, /* uint8 [nV] (tet)                                    */
+    OR_A_FACE_NORMALS = 14,  /* float [nTris*3]                                     */
+    OR_A_VERTEX_NORMALS = 15,/* float [nSurf*3]                                     */
+    OR_A_COUNT
+};
+
+typedef struct or_mesh or_mesh;
+
+/* counts: nV, nE, nSurf, nFeature, nTris, nHE, nColorsFree, nColorsFeature, nColorsInner,
+ *         maxNumHalfedges, maxNumTetrahedra, isFlat */
+enum { OR_I_NV = 0, OR_I_NE, OR_I_NSURF, OR_I_NFEATURE, OR_I_NTRIS, OR_I_NHE,
+       OR_I_NCOL_FREE, OR_I_NCOL_FEATURE, OR_I_NCOL_INNER, OR_I_MAX_HE, OR_I_MAX_TETS,
+       OR_I_IS_FLAT, OR_I_COUNT };
+
+/* Build connectivity + colouring for a tri (elem_type OR_TRI) or tet (OR_TET) mesh.
+ * Returns NULL on invalid input (err set to a message). */
+or_mesh* or_mesh_build(int elem_type, int nV, const float* xyz, int nE, const int32_t* elems,
+                       uint32_t color_seed, char* err, int err_len);
+void     or_mesh_free(or_mesh* m);
+int      or_mesh_info(const or_mesh* m, int which);
+long     or_mesh_array_len(const or_mesh* m, int id);          /* elements of the array   */
+int      or_mesh_array(const or_mesh* m, int id, void* out);    /* copies; 0 on success    */
+
+/* JPL colouring of a CSR graph with the seeded priorities; returns number of colours. */
+int      or_color_jpl(int n, const int32_t* rowptr, const int32_t* col, uint32_t seed, int32_t* colors);
+uint32_t or_priority(uint32_t i, uint32_t seed);
+
+/* ---- DMO grid search (one colour class = vertex range [v0, v1)) ---------------------- */
+/* tet inner vertices: reference k_optimizeHierarchicalInnerTet                           */
+void or_dmo_tet_f32(const or_mesh* m, float* xyz, int v0, int v1, float grid_scale, int nthreads);
+void or_dmo_tet_f64(const or_mesh* m, double* xyz, int v0, int v1, double grid_scale,
+                    double* margin, int nthreads);
+/* the reference kernel's own float arithmetic (cbrtf per element): CPU baseline            */
+void or_dmo_tet_ref32(const or_mesh* m, float* xyz, int v0, int v1, float grid_scale, int nthreads);
+/* flat triangle free vertices: reference k_optimizeHierarchical2DFlat                     */
+void or_dmo_tri2d_f32(const or_mesh* m, float* xyz, int v0, int v1, float grid_scale, int nthreads);
+void or_dmo_tri2d_f64(const or_mesh* m, double* xyz, int v0, int v1, double grid_scale,
+                      double* margin, int nthreads);
+
+/* ---- element quality (reference formulas) ------------------------------------------- */
+double or_q_tet_mean_ratio_f64(const double* p0, const double* p1, const double* p2, const double* p3);
+float  or_q_tet_mean_ratio_f32(const float* p0, const float* p1, const float* p2, const float* p3);
+double or_q_tri2d_mean_ratio_f64(const double* p0, const double* p1, const double* p2);
+float  or_q_tri2d_mean_ratio_f32(const float* p0, const float* p1, const float* p2);
+/* per-element quality of the whole mesh (elements in the mesh's internal numbering)      */
+void   or_element_qualities_f64(const or_mesh* m, const double* xyz, double* q);
+void   or_element_qualities_f32(const or_mesh* m, const float* xyz, float* q);
+
+/* Full optimisation loop (reference doIteration, fix-boundary mode): n_iter iterations,
+ * colours in order; writes min quality after each iteration to min_hist (may be NULL).  */
+void or_optimize_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale, int nthreads,
+                     double* min_hist, double* mean_hist);
+void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
+                     double* min_hist, double* mean_hist);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

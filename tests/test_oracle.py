@@ -1,0 +1,228 @@
+"""CPU tests of the oracle: known answers of the reference formulas, structural invariants
+of the connectivity / colouring it restates, golden fixtures, and agreement of its two
+arithmetic modes (literal FP64 restatement vs the product's FP32 arithmetic)."""
+import os
+
+import numpy as np
+import pytest
+
+from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+# ---- known answers (the reference formulas fix these exactly) -------------------------------
+def test_equilateral_triangle_is_one(oracle_mod):
+    s = np.sqrt(3.0)
+    p = [[0, 0, 0], [1, 0, 0], [0.5, s / 2, 0]]
+    assert oracle_mod.q_tri2d(p) == pytest.approx(1.0, abs=1e-12)
+    assert oracle_mod.q_tri2d(p, np.float32) == pytest.approx(1.0, abs=1e-6)
+
+
+def test_regular_tet_is_one_and_flip_returns_volume(oracle_mod):
+    reg = np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], float)
+    # TetGen order: (v1-v0).((v2-v0)x(v3-v0)) > 0
+    pos = reg[[0, 2, 1, 3]]
+    assert oracle_mod.q_tet(pos) == pytest.approx(1.0, abs=1e-12)
+    assert oracle_mod.q_tet(pos, np.float32) == pytest.approx(1.0, abs=1e-6)
+    flipped = reg
+    vol = np.dot(flipped[1] - flipped[0], np.cross(flipped[2] - flipped[0], flipped[3] - flipped[0])) / 6
+    assert vol < 0
+    assert oracle_mod.q_tet(flipped) == pytest.approx(vol, rel=1e-12)
+
+
+def test_flipped_triangle_returns_signed_area(oracle_mod):
+    p = [[0, 0, 0], [0, 1, 0], [1, 0, 0]]
+    assert oracle_mod.q_tri2d(p) == pytest.approx(-1.0)
+
+
+def test_unperturbed_grids_are_fixed_points(oracle_mod):
+    xyz, tris = G.tri_grid(8, seed=None)
+    m = oracle_mod.OracleMesh(oracle_mod.TRI, xyz, tris)
+    x = m.xyz
+    x64, _, _ = m.optimize_f64(x, 2)
+    x32, _, _ = m.optimize_f32(x, 2)
+    assert np.array_equal(x64.astype(np.float32), x)
+    assert np.array_equal(x32, x)
+    xyz, tets = G.tet_cube(3, seed=None)
+    m = oracle_mod.OracleMesh(oracle_mod.TET, xyz, tets)
+    x = m.xyz
+    x32, _, _ = m.optimize_f32(x, 1)
+    x64, _, _ = m.optimize_f64(x, 1)
+    assert np.array_equal(x32, x)
+    assert np.allclose(x64, x, atol=1e-12)
+
+
+# ---- structural invariants ----------------------------------------------------------------------
+def _check_coloring(rowptr_pairs, colors):
+    for a, b in rowptr_pairs:
+        assert colors[a] != colors[b]
+
+
+def _color_of(offsets, n):
+    col = np.full(n, -1)
+    for c in range(len(offsets) - 1):
+        col[offsets[c]:offsets[c + 1]] = c
+    return col
+
+
+@pytest.mark.parametrize("n", [3, 6])
+def test_tet_structure(oracle_mod, n):
+    xyz, tets = G.tet_cube(n, seed=1)
+    m = oracle_mod.OracleMesh(oracle_mod.TET, xyz, tets)
+    A = m.arrays()
+    nV = (n + 1) ** 3
+    nS = nV - (n - 1) ** 3
+    assert m.info["nSurf"] == nS
+    assert m.info["nTris"] == 12 * n * n
+    assert m.info["nFeature"] == 12 * (n - 1) + 8
+    # permutation consistency
+    noo = A["new_of_old"]
+    assert sorted(noo) == list(range(nV))
+    assert np.array_equal(A["xyz"].reshape(-1, 3)[noo], xyz)
+    el = A["elems"].reshape(-1, 4)
+    assert np.array_equal(np.sort(el, 1), np.sort(noo[tets], 1))
+    # every halfface is a positively oriented tet with its vertex
+    rp, hf = A["hf_rowptr"], A["halffaces"].reshape(-1, 3)
+    lattice, _ = G.tet_cube(n, seed=None)       # orientation is checked on the unperturbed lattice
+    x = np.zeros((nV, 3))
+    x[noo] = lattice
+    for v in range(nV):
+        for r in range(rp[v], rp[v + 1]):
+            a, b, c = hf[r]
+            d = np.dot(x[a] - x[v], np.cross(x[b] - x[v], x[c] - x[v]))
+            assert d > 0
+    # inner colouring valid (no tet edge inside one colour class)
+    col = np.full(nV, -1)
+    off = A["col_inner"]
+    for c in range(len(off) - 1):
+        col[off[c]:off[c + 1]] = c
+    for t in el:
+        for i in range(4):
+            for j in range(i + 1, 4):
+                if col[t[i]] >= 0 and col[t[j]] >= 0:
+                    assert col[t[i]] != col[t[j]]
+    assert off[0] == nS and off[-1] == nV
+
+
+def test_tri_structure(oracle_mod):
+    xyz, tris = G.tri_grid(10, seed=2)
+    m = oracle_mod.OracleMesh(oracle_mod.TRI, xyz, tris)
+    A = m.arrays()
+    nV = 100
+    assert m.info["isFlat"] == 1
+    assert m.info["nFeature"] == 36  # boundary vertices of a 10x10 grid
+    rp, he = A["he_rowptr"], A["halfedges"].reshape(-1, 4)
+    el = A["elems"].reshape(-1, 3)
+    x = A["xyz"].reshape(-1, 3)
+    for v in range(nV):
+        row = he[rp[v]:rp[v + 1]]
+        for i, h in enumerate(row):
+            tgt, opp, face, nxt = h
+            # opposite points back
+            assert he[opp][0] == v
+            if face >= 0:
+                assert v in el[face] and tgt in el[face]
+                # CCW fan: consecutive targets span a positive triangle with v
+        for i in range(len(row) - 1):
+            if row[i][2] < 0:
+                continue
+            a, b = x[row[i][0]], x[row[i + 1][0]]
+            cr = (a[0] - x[v][0]) * (b[1] - x[v][1]) - (a[1] - x[v][1]) * (b[0] - x[v][0])
+            assert cr > 0
+    # free colouring valid
+    col = _color_of(A["col_free"], nV)
+    for t in el:
+        for i in range(3):
+            a, b = t[i], t[(i + 1) % 3]
+            if col[a] >= 0 and col[b] >= 0:
+                assert col[a] != col[b]
+
+
+def test_jpl_is_order_independent_and_valid(oracle_mod):
+    rng = np.random.default_rng(0)
+    n = 300
+    pairs = set()
+    for _ in range(900):
+        a, b = rng.integers(0, n, 2)
+        if a != b:
+            pairs.add((a, b)); pairs.add((b, a))
+    pairs = sorted(pairs)
+    rowptr = np.zeros(n + 1, np.int32)
+    for a, _ in pairs:
+        rowptr[a + 1] += 1
+    rowptr = np.cumsum(rowptr).astype(np.int32)
+    col = np.array([b for _, b in pairs], np.int32)
+    c, nc = oracle_mod.color_jpl(rowptr, col, seed=7)
+    assert c.min() == 0 and c.max() == nc - 1
+    for a, b in pairs:
+        assert c[a] != c[b]
+    # JPL round rule: v was passed over in every round k < colour(v) because a neighbour
+    # still competing in that round (colour >= k) had a higher priority
+    pr = np.array([oracle_mod.lib().or_priority(i, 7) for i in range(n)], dtype=np.uint64)
+    for v in range(n):
+        nb = col[rowptr[v]:rowptr[v + 1]]
+        for k in range(c[v]):
+            assert any(c[u] >= k and pr[u] > pr[v] for u in nb)
+        # and in its own round it beat every competitor
+        assert all(pr[v] > pr[u] for u in nb if c[u] >= c[v])
+
+
+# ---- golden fixtures ------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["tri_grid8", "tet_cube4"])
+def test_golden(oracle_mod, name):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mg", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    ref = np.load(os.path.join(GOLDEN, name + ".npz"))
+    now = mg.make(name)
+    for k in ref.files:
+        a, b = ref[k], now[k]
+        if k in ("dmo_f64_xyz", "dmo_f64_min", "dmo_f64_mean", "dmo_f32_mean", "dmo_f32_min"):
+            np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12, err_msg=k)
+        else:
+            assert np.array_equal(a, b), k
+
+
+# ---- FP32 product arithmetic vs literal FP64 restatement ----------------------------------------------
+def test_f32_vs_f64_quality_tri(oracle_mod):
+    xyz, tris = G.config1()
+    m = oracle_mod.OracleMesh(oracle_mod.TRI, xyz, tris)
+    x = m.xyz
+    _, mn32, me32 = m.optimize_f32(x, 10)
+    _, mn64, me64 = m.optimize_f64(x, 10)
+    assert abs(mn32[-1] - mn64[-1]) < 1e-4
+    assert abs(me32[-1] - me64[-1]) < 1e-4
+    assert np.all(np.diff(mn64) >= -1e-12)
+
+
+def test_f32_vs_f64_quality_tet(oracle_mod):
+    xyz, tets = G.tet_cube(8, seed=4)
+    m = oracle_mod.OracleMesh(oracle_mod.TET, xyz, tets)
+    x = m.xyz
+    _, mn32, me32 = m.optimize_f32(x, 4)
+    _, mn64, me64 = m.optimize_f64(x, 4)
+    assert abs(mn32[-1] - mn64[-1]) < 1e-4
+    assert abs(me32[-1] - me64[-1]) < 1e-4
+    assert np.all(np.diff(mn64) >= -1e-12)
+
+
+def test_one_color_step_matches_within_margin(oracle_mod):
+    """From identical state, one colour launch of the f32 arithmetic lands within 1e-5*h of
+    the f64 restatement wherever the f64 decision margins are clear."""
+    n = 8
+    h = 1.0 / n
+    xyz, tets = G.tet_cube(n, seed=9)
+    m = oracle_mod.OracleMesh(oracle_mod.TET, xyz, tets)
+    x = m.xyz
+    checked = 0
+    for (v0, v1) in m.color_ranges()[:4]:
+        x32 = m.dmo_color_f32(x, v0, v1)
+        x64, margin = m.dmo_color_f64(x.astype(np.float64), v0, v1)
+        clear = margin > 1e-5
+        d = np.abs(x32[v0:v1] - x64[v0:v1]).max(1)
+        assert np.all(d[clear] < 1e-5 * h), d[clear].max()
+        checked += int(clear.sum())
+        x = x32
+    assert checked > 0

@@ -1,0 +1,274 @@
+"""B200-native discrete mesh optimisation (DMO) with the reference's mesh / optimizer API.
+
+Python mirror of the reference's C++ interface (DanielZint/VolumeSurfaceDiscreteMeshOptimization):
+
+* ``DMOMeshTriFactory.create(points, tris)`` / ``DMOMeshTetFactory.create(points, tets)``
+  -- ``mesh/MeshFactory.h:17-40`` (device-array overloads; file parsing is separate);
+* ``DMOTetClass(mesh, QualityCriterium.MEAN_RATIO, gridScale=0.5, n_iter=30)`` and
+  ``DMOTriFlatClass(...)`` -- ``dmo/DMOTet.h:21-62``, ``dmo/DMOTriFlat.h:19-51`` with
+  ``optimize()``, ``doIteration()``, ``isDone()``, ``getQuality()``, ``findMinimumQuality()``,
+  ``getElementQualities()``, ``getQualityHistogram()``, ``displayQualityGPU()``
+  (``dmo/DMOBase.h:23-88``).
+
+Everything runs in ``lib/libvsdmo.so`` through the C ABI of ``include/vsdmo.h``; this module
+only marshals arguments. Differences from the reference: meshes are built from arrays you
+pass (host numpy or device pointers), vertex numbering is reported through
+``permutation()`` / ``positions(original_order=True)``, errors raise ``VSDMOError`` instead of
+exiting, and ``fix_boundary`` selects the boundary-fixed runs of the benchmark configs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+import numpy as np
+
+from . import _capi
+from ._capi import VSDMOError, Params, check
+
+__all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshTet", "DMOMeshTriFactory", "DMOMeshTetFactory",
+           "DMOTetClass", "DMOTriFlatClass", "DMOTriClass", "VSDMOError", "Params", "default_params",
+           "version"]
+
+A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
+    A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
+    A_FACE_NORMALS, A_VERTEX_NORMALS = range(16)
+ARRAY_NAMES = {A_XYZ: "xyz", A_NEW_OF_OLD: "new_of_old", A_ELEMS: "elems", A_SURF_TRIS: "surf_tris",
+               A_HE_ROWPTR: "he_rowptr", A_HALFEDGES: "halfedges", A_HF_ROWPTR: "hf_rowptr",
+               A_HALFFACES: "halffaces", A_COL_FREE: "col_free", A_COL_FEATURE: "col_feature",
+               A_COL_INNER: "col_inner", A_IS_BOUNDARY1D: "is_boundary1d", A_IS_FEATURE: "is_feature",
+               A_IS_BOUNDARY2D: "is_boundary2d", A_FACE_NORMALS: "face_normals",
+               A_VERTEX_NORMALS: "vertex_normals"}
+_F32 = {A_XYZ, A_FACE_NORMALS, A_VERTEX_NORMALS}
+_U8 = {A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D}
+INFO_NAMES = ["nV", "nE", "nSurf", "nFeature", "nTris", "nHE", "nColorsFree", "nColorsFeature",
+              "nColorsInner", "maxNumHalfedges", "maxNumTetrahedra", "isFlat"]
+
+
+class QualityCriterium(enum.IntEnum):
+    """``DMO::QualityCriterium`` (``dmo/DMOQualityUtil.h:10-18``)."""
+    MEAN_RATIO = 0
+    AREA = 1
+    RIGHT_ANGLE = 2
+    JACOBIAN = 3
+    MIN_ANGLE = 4
+    RADIUS_RATIO = 5
+    MAX_ANGLE = 6
+
+
+def version() -> str:
+    return _capi.lib().vsdmo_version().decode()
+
+
+def default_params(elem_type: int) -> Params:
+    p = Params()
+    check(_capi.lib().vsdmo_params_default(elem_type, C.byref(p)))
+    return p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class _Mesh:
+    elem_type = -1
+    k = 0
+
+    def __init__(self, points, elems, color_seed: int = 1, stream=None, device_ptrs=None):
+        L = _capi.lib()
+        h = C.c_void_p()
+        if device_ptrs is not None:
+            xyz_ptr, el_ptr, nV, nE = device_ptrs
+            check(L.vsdmo_mesh_create(self.elem_type, C.c_void_p(xyz_ptr), nV, C.c_void_p(el_ptr), nE,
+                                      _capi.DEVICE, color_seed, C.c_void_p(stream or 0), C.byref(h)))
+        else:
+            xyz = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+            el = np.ascontiguousarray(elems, dtype=np.int32).reshape(-1, self.k)
+            check(L.vsdmo_mesh_create(self.elem_type, _ptr(xyz), len(xyz), _ptr(el), len(el), _capi.HOST,
+                                      color_seed, C.c_void_p(stream or 0), C.byref(h)))
+        self.h = h
+        self.info = {n: L.vsdmo_mesh_info(h, i) for i, n in enumerate(INFO_NAMES)}
+        self.nVertices = self.info["nV"]
+        self.nVerticesSurf = self.info["nSurf"]
+        self.nVerticesFeature = self.info["nFeature"]
+
+    def close(self):
+        if getattr(self, "h", None):
+            _capi.lib().vsdmo_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def array(self, aid: int) -> np.ndarray:
+        L = _capi.lib()
+        n = L.vsdmo_mesh_array_len(self.h, aid)
+        dt = np.float32 if aid in _F32 else (np.uint8 if aid in _U8 else np.int32)
+        out = np.zeros(max(n, 0), dtype=dt)
+        if n > 0:
+            check(L.vsdmo_mesh_array(self.h, aid, _ptr(out)))
+        return out
+
+    def arrays(self) -> dict:
+        return {ARRAY_NAMES[a]: self.array(a) for a in ARRAY_NAMES}
+
+    def permutation(self) -> np.ndarray:
+        return self.array(A_NEW_OF_OLD)
+
+    def positions(self, original_order: bool = False) -> np.ndarray:
+        out = np.zeros((self.nVertices, 3), dtype=np.float32)
+        check(_capi.lib().vsdmo_mesh_get_positions(self.h, _ptr(out), int(original_order), _capi.HOST))
+        return out
+
+    def set_positions(self, xyz, original_order: bool = False):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        if len(xyz) != self.nVertices:
+            raise ValueError("wrong number of vertices")
+        check(_capi.lib().vsdmo_mesh_set_positions(self.h, _ptr(xyz), int(original_order), _capi.HOST))
+
+    def positions_to_device(self, dev_ptr: int, original_order: bool = True):
+        check(_capi.lib().vsdmo_mesh_get_positions(self.h, C.c_void_p(dev_ptr), int(original_order), _capi.DEVICE))
+
+
+class DMOMeshTri(_Mesh):
+    """``DMOMeshTri`` (``mesh/DMOMeshTri.h:81-94``)."""
+    elem_type = _capi.TRI
+    k = 3
+
+
+class DMOMeshTet(_Mesh):
+    """``DMOMeshTet`` (``mesh/DMOMeshTet.h:145-198``)."""
+    elem_type = _capi.TET
+    k = 4
+
+
+class DMOMeshTriFactory:
+    """``DMOMeshTriFactory::create`` (``mesh/MeshFactory.cu:15-31``)."""
+
+    @staticmethod
+    def create(points, tris, color_seed: int = 1) -> DMOMeshTri:
+        return DMOMeshTri(points, tris, color_seed)
+
+
+class DMOMeshTetFactory:
+    """``DMOMeshTetFactory::create`` (``mesh/MeshFactory.cu:45-55``) from arrays."""
+
+    @staticmethod
+    def create(points, tets, color_seed: int = 1) -> DMOMeshTet:
+        return DMOMeshTet(points, tets, color_seed)
+
+
+class _DMOBase:
+    """``DMO::DMOBaseClass`` (``dmo/DMOBase.h:23-88``)."""
+    _flat = -1
+
+    def __init__(self, dmo_mesh, qualityCriterium=QualityCriterium.MEAN_RATIO, gridScale: float = 0.5,
+                 n_iter: int = 30, fix_boundary: bool = True, use_graph: bool = True, depth: int = 3,
+                 check_monotone: bool = True):
+        self.mesh = dmo_mesh
+        p = default_params(dmo_mesh.elem_type)
+        p.quality = int(qualityCriterium)
+        p.grid_scale = float(gridScale)
+        p.n_iter = int(n_iter)
+        p.fix_boundary = int(fix_boundary)
+        p.use_graph = int(use_graph)
+        p.depth = int(depth)
+        p.check_monotone = int(check_monotone)
+        p.flat = self._flat
+        self.params = p
+        h = C.c_void_p()
+        check(_capi.lib().vsdmo_opt_create(dmo_mesh.h, C.byref(p), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _capi.lib().vsdmo_opt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def doIteration(self):
+        check(_capi.lib().vsdmo_opt_iterate(self.h, 1))
+
+    def iterate(self, n: int):
+        check(_capi.lib().vsdmo_opt_iterate(self.h, int(n)))
+
+    def optimize(self):
+        check(_capi.lib().vsdmo_opt_optimize(self.h))
+
+    def isDone(self) -> bool:
+        return bool(_capi.lib().vsdmo_opt_is_done(self.h))
+
+    @property
+    def curr_it(self) -> int:
+        return _capi.lib().vsdmo_opt_iterations_done(self.h)
+
+    def getQuality(self) -> float:
+        q = C.c_float()
+        check(_capi.lib().vsdmo_opt_get_quality(self.h, C.byref(q)))
+        return q.value
+
+    def findMinimumQuality(self) -> float:
+        q = C.c_float()
+        check(_capi.lib().vsdmo_opt_find_min_quality(self.h, C.byref(q), None))
+        return q.value
+
+    def quality_stats(self):
+        q = C.c_float()
+        m = C.c_double()
+        check(_capi.lib().vsdmo_opt_find_min_quality(self.h, C.byref(q), C.byref(m)))
+        return q.value, m.value
+
+    def getElementQualities(self, out=None):
+        """Host numpy array of per-element qualities, or write into a device pointer ``out``."""
+        if out is not None:
+            check(_capi.lib().vsdmo_opt_element_qualities(self.h, C.c_void_p(out), _capi.DEVICE))
+            return None
+        q = np.zeros(self.mesh.info["nE"], dtype=np.float32)
+        check(_capi.lib().vsdmo_opt_element_qualities(self.h, _ptr(q), _capi.HOST))
+        return q
+
+    def getQualityHistogram(self, n_cols: int = 10):
+        c = np.zeros(n_cols, dtype=np.int32)
+        check(_capi.lib().vsdmo_opt_quality_histogram(self.h, _ptr(c), n_cols))
+        return c
+
+    def displayQualityGPU(self, n_cols: int = 10):
+        check(_capi.lib().vsdmo_opt_display_quality(self.h, n_cols))
+
+    def history(self):
+        n_cap = self.curr_it + 1
+        mn = np.zeros(n_cap, dtype=np.float32)
+        mean = np.zeros(n_cap, dtype=np.float64)
+        n = C.c_int()
+        check(_capi.lib().vsdmo_opt_history(self.h, _ptr(mn), _ptr(mean), n_cap, C.byref(n)))
+        return mn[: n.value], mean[: n.value]
+
+    def run_color(self, color: int):
+        check(_capi.lib().vsdmo_opt_run_color(self.h, int(color)))
+
+    @property
+    def launches_per_iteration(self) -> int:
+        return _capi.lib().vsdmo_opt_launches_per_iteration(self.h)
+
+
+class DMOTetClass(_DMOBase):
+    """``DMO::DMOTetClass`` (``dmo/DMOTet.h:21-62``)."""
+
+
+class DMOTriFlatClass(_DMOBase):
+    """``DMO::DMOTriFlatClass`` (``dmo/DMOTriFlat.h:19-51``); MEAN_RATIO is the implemented
+    criterion (the reference's default argument is MIN_ANGLE)."""
+    _flat = 1
+
+
+class DMOTriClass(_DMOBase):
+    """``DMO::DMOTriClass`` (``dmo/DMOTri.h``): surface triangle DMO."""
+    _flat = 0

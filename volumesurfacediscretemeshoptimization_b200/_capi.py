@@ -1,0 +1,112 @@
+"""ctypes binding of ``lib/libvsdmo.so`` (the C ABI declared in ``include/vsdmo.h``).
+
+The library is the only compute path: importing this module fails loudly when the shared
+object is missing, and every call raises ``VSDMOError`` on a non-zero status. There is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("VSDMO_LIB", os.path.join(HERE, "lib", "libvsdmo.so"))
+
+OK, E_ARG, E_CUDA, E_NONMANIFOLD, E_VALENCE, E_MONOTONE, E_TIMEOUT, E_NAN, E_NOMEM, E_UNSUPPORTED = range(10)
+TRI, QUAD, TET, HEX = 0, 1, 2, 3
+HOST, DEVICE = 0, 1
+
+# every entry point include/vsdmo.h declares (checked by the CPU symbol test)
+EXPORTED = [
+    "vsdmo_version", "vsdmo_last_error", "vsdmo_status_string", "vsdmo_params_default",
+    "vsdmo_mesh_create", "vsdmo_mesh_destroy", "vsdmo_mesh_info", "vsdmo_mesh_array_len",
+    "vsdmo_mesh_array", "vsdmo_mesh_permutation", "vsdmo_mesh_get_positions",
+    "vsdmo_mesh_set_positions", "vsdmo_mesh_sync", "vsdmo_opt_create", "vsdmo_opt_destroy",
+    "vsdmo_opt_iterate", "vsdmo_opt_optimize", "vsdmo_opt_is_done", "vsdmo_opt_iterations_done",
+    "vsdmo_opt_get_quality", "vsdmo_opt_find_min_quality", "vsdmo_opt_element_qualities",
+    "vsdmo_opt_quality_histogram", "vsdmo_opt_display_quality", "vsdmo_opt_history",
+    "vsdmo_opt_run_color", "vsdmo_opt_launches_per_iteration",
+]
+
+
+class VSDMOError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"vsdmo status {status}: {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [("quality", C.c_int), ("grid_scale", C.c_float), ("n_iter", C.c_int),
+                ("grid_n", C.c_int), ("depth", C.c_int), ("fix_boundary", C.c_int),
+                ("flat", C.c_int), ("use_graph", C.c_int), ("check_monotone", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"CUDA library {LIB_PATH} is missing; build it with "
+                          "`python volumesurfacediscretemeshoptimization_b200/build.py`")
+    L = C.CDLL(LIB_PATH)
+    P, I, U, F = C.c_void_p, C.c_int, C.c_uint32, C.c_float
+    S = C.c_int  # vsdmo_status
+    L.vsdmo_version.restype = C.c_char_p
+    L.vsdmo_last_error.restype = C.c_char_p
+    L.vsdmo_status_string.restype = C.c_char_p
+    L.vsdmo_status_string.argtypes = [I]
+    L.vsdmo_params_default.restype = S
+    L.vsdmo_params_default.argtypes = [I, C.POINTER(Params)]
+    L.vsdmo_mesh_create.restype = S
+    L.vsdmo_mesh_create.argtypes = [I, P, I, P, I, I, U, P, C.POINTER(P)]
+    L.vsdmo_mesh_destroy.argtypes = [P]
+    L.vsdmo_mesh_destroy.restype = None
+    L.vsdmo_mesh_info.argtypes = [P, I]
+    L.vsdmo_mesh_array_len.restype = C.c_long
+    L.vsdmo_mesh_array_len.argtypes = [P, I]
+    L.vsdmo_mesh_array.restype = S
+    L.vsdmo_mesh_array.argtypes = [P, I, P]
+    L.vsdmo_mesh_permutation.restype = S
+    L.vsdmo_mesh_permutation.argtypes = [P, P]
+    L.vsdmo_mesh_get_positions.restype = S
+    L.vsdmo_mesh_get_positions.argtypes = [P, P, I, I]
+    L.vsdmo_mesh_set_positions.restype = S
+    L.vsdmo_mesh_set_positions.argtypes = [P, P, I, I]
+    L.vsdmo_mesh_sync.restype = S
+    L.vsdmo_mesh_sync.argtypes = [P]
+    L.vsdmo_opt_create.restype = S
+    L.vsdmo_opt_create.argtypes = [P, C.POINTER(Params), C.POINTER(P)]
+    L.vsdmo_opt_destroy.argtypes = [P]
+    L.vsdmo_opt_destroy.restype = None
+    L.vsdmo_opt_iterate.restype = S
+    L.vsdmo_opt_iterate.argtypes = [P, I]
+    L.vsdmo_opt_optimize.restype = S
+    L.vsdmo_opt_optimize.argtypes = [P]
+    L.vsdmo_opt_is_done.argtypes = [P]
+    L.vsdmo_opt_iterations_done.argtypes = [P]
+    L.vsdmo_opt_launches_per_iteration.argtypes = [P]
+    L.vsdmo_opt_get_quality.restype = S
+    L.vsdmo_opt_get_quality.argtypes = [P, C.POINTER(F)]
+    L.vsdmo_opt_find_min_quality.restype = S
+    L.vsdmo_opt_find_min_quality.argtypes = [P, C.POINTER(F), C.POINTER(C.c_double)]
+    L.vsdmo_opt_element_qualities.restype = S
+    L.vsdmo_opt_element_qualities.argtypes = [P, P, I]
+    L.vsdmo_opt_quality_histogram.restype = S
+    L.vsdmo_opt_quality_histogram.argtypes = [P, P, I]
+    L.vsdmo_opt_display_quality.restype = S
+    L.vsdmo_opt_display_quality.argtypes = [P, I]
+    L.vsdmo_opt_history.restype = S
+    L.vsdmo_opt_history.argtypes = [P, P, P, I, C.POINTER(I)]
+    L.vsdmo_opt_run_color.restype = S
+    L.vsdmo_opt_run_color.argtypes = [P, I]
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != OK:
+        msg = lib().vsdmo_last_error().decode(errors="replace")
+        raise VSDMOError(status, msg or lib().vsdmo_status_string(status).decode())

@@ -1,0 +1,577 @@
+// capi.cu -- the extern "C" boundary declared in include/vsdmo.h.
+//
+// Mesh handles own the device mesh (Mesh, mesh_build.cu); optimiser handles own the
+// per-iteration statistics and a CUDA graph of one doIteration(): every colour launch of the
+// grid search followed by the fused quality / monotonicity kernel (dmo/DMOTet.cu:128-170,
+// dmo/DMOTriFlat.cu:129-166 issue the same steps with a cudaDeviceSynchronize after each).
+#include "vsdmo_internal.cuh"
+#include <cstring>
+#include <cmath>
+#include <algorithm>
+#include <memory>
+#include <iostream>
+#include <sstream>
+
+using namespace vsdmo;
+
+struct vsdmo_mesh_s {
+    Mesh m;
+};
+
+struct vsdmo_opt_s {
+    vsdmo_mesh_s* mesh = nullptr;
+    vsdmo_params p{};
+    int iters_done = 0;
+    int capacity = 0;
+    bool tet = false;
+    std::vector<std::pair<int, int>> ranges;  // colour classes in launch order
+    DBuf<IterStats> stats;
+    DBuf<int> d_iter;
+    DBuf<float> pmin;
+    DBuf<double> psum;
+    DBuf<int> pfail;
+    DBuf<unsigned> done;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float last_min = 0.f;
+    ~vsdmo_opt_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+vsdmo_status fail(vsdmo_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+template <class F>
+vsdmo_status guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return VSDMO_OK;
+    } catch (const Error& e) {
+        return fail(e.status, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(VSDMO_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(VSDMO_E_CUDA, e.what());
+    }
+}
+
+__global__ void k_pack_xyz(const float4* pos, int n, const int* new_of_old, float* out) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const float4 p = pos[new_of_old ? new_of_old[i] : i];
+        out[3 * i] = p.x; out[3 * i + 1] = p.y; out[3 * i + 2] = p.z;
+    }
+}
+
+__global__ void k_unpack_xyz(float4* pos, int n, const int* new_of_old, const float* in) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int d = new_of_old ? new_of_old[i] : (int)i;
+        float4 p = pos[d];
+        p.x = in[3 * i]; p.y = in[3 * i + 1]; p.z = in[3 * i + 2];
+        pos[d] = p;
+    }
+}
+
+__global__ void k_pack_hf(const int4* hf, long n, int* out) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int4 h = hf[i];
+        out[3 * i] = h.x; out[3 * i + 1] = h.y; out[3 * i + 2] = h.z;
+    }
+}
+
+void copy_in(void* dst, const void* src, size_t bytes, int mem_space, cudaStream_t s) {
+    VSDMO_CUDA(cudaMemcpyAsync(dst, src, bytes, mem_space == VSDMO_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+}
+
+void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
+    const Mesh& m = o->mesh->m;
+    for (auto& r : o->ranges) {
+        DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
+        if (o->tet) launch_dmo_tet(m, L, s); else launch_dmo_tri2d(m, L, s);
+    }
+    launch_quality_stats(m, o->p.quality, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p,
+                         o->p.check_monotone ? 1 : 0, s);
+}
+
+void ensure_capacity(vsdmo_opt_s* o, int need) {
+    if (need + 1 <= o->capacity) return;
+    cudaStream_t s = o->mesh->m.stream;
+    int cap = std::max(need + 1, std::max(2 * o->capacity, 256));
+    DBuf<IterStats> ns(cap, s);
+    ns.zero();
+    if (o->stats.p)
+        VSDMO_CUDA(cudaMemcpyAsync(ns.p, o->stats.p, sizeof(IterStats) * o->capacity, cudaMemcpyDeviceToDevice, s));
+    o->stats = std::move(ns);
+    o->capacity = cap;
+    if (o->exec) { cudaGraphExecDestroy(o->exec); o->exec = nullptr; }
+    if (o->graph) { cudaGraphDestroy(o->graph); o->graph = nullptr; }
+}
+
+void ensure_graph(vsdmo_opt_s* o) {
+    if (o->exec || !o->p.use_graph) return;
+    cudaStream_t s = o->mesh->m.stream;
+    VSDMO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+        run_iteration_body(o, s);
+    } catch (...) {
+        cudaGraph_t g;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    VSDMO_CUDA(cudaStreamEndCapture(s, &o->graph));
+    VSDMO_CUDA(cudaGraphInstantiate(&o->exec, o->graph, 0));
+}
+
+std::vector<IterStats> read_stats(vsdmo_opt_s* o, int from, int count) {
+    std::vector<IterStats> h(count);
+    if (count > 0) {
+        VSDMO_CUDA(cudaMemcpyAsync(h.data(), o->stats.p + from, sizeof(IterStats) * count, cudaMemcpyDeviceToHost, o->mesh->m.stream));
+        VSDMO_CUDA(cudaStreamSynchronize(o->mesh->m.stream));
+    }
+    return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+VSDMO_API const char* vsdmo_version(void) { return "vsdmo-b200 0.1.0 (sm_100a)"; }
+
+VSDMO_API const char* vsdmo_last_error(void) { return g_last_error.c_str(); }
+
+VSDMO_API const char* vsdmo_status_string(vsdmo_status s) {
+    switch (s) {
+    case VSDMO_OK: return "ok";
+    case VSDMO_E_ARG: return "invalid argument";
+    case VSDMO_E_CUDA: return "CUDA error";
+    case VSDMO_E_NONMANIFOLD: return "non-manifold mesh";
+    case VSDMO_E_VALENCE: return "one-ring too large";
+    case VSDMO_E_MONOTONE: return "quality decreased";
+    case VSDMO_E_TIMEOUT: return "device wait timed out";
+    case VSDMO_E_NAN: return "non-finite coordinates";
+    case VSDMO_E_NOMEM: return "out of memory";
+    case VSDMO_E_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+VSDMO_API vsdmo_status vsdmo_params_default(int elem_type, vsdmo_params* out) {
+    if (!out) return fail(VSDMO_E_ARG, "null params");
+    if (elem_type < VSDMO_TRI || elem_type > VSDMO_HEX) return fail(VSDMO_E_ARG, "bad element type");
+    out->quality = VSDMO_MEAN_RATIO;
+    out->grid_scale = 0.5f;
+    out->n_iter = 30;
+    out->grid_n = 8;
+    out->depth = 3;
+    out->fix_boundary = 1;
+    out->flat = -1;
+    out->use_graph = 1;
+    out->check_monotone = 1;
+    return VSDMO_OK;
+}
+
+VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_vertices, const int32_t* elems,
+                                         int n_elems, int mem_space, uint32_t color_seed, void* cuda_stream,
+                                         vsdmo_mesh_t* out) {
+    if (!out) return fail(VSDMO_E_ARG, "null output handle");
+    *out = nullptr;
+    if (elem_type != VSDMO_TRI && elem_type != VSDMO_TET && elem_type != VSDMO_QUAD && elem_type != VSDMO_HEX)
+        return fail(VSDMO_E_ARG, "bad element type");
+    if (elem_type == VSDMO_QUAD || elem_type == VSDMO_HEX)
+        return fail(VSDMO_E_UNSUPPORTED, "quad and hex meshes are not supported yet");
+    if (!xyz || !elems || n_vertices <= 0 || n_elems <= 0) return fail(VSDMO_E_ARG, "empty mesh or null arrays");
+    if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
+    const int k = elem_type == VSDMO_TET ? 4 : 3;
+    if ((long)n_elems * k > (long)INT32_MAX / 2 || (long)n_vertices * 4 > (long)INT32_MAX)
+        return fail(VSDMO_E_ARG, "mesh too large for 32-bit indices");
+    std::unique_ptr<vsdmo_mesh_s> h(new vsdmo_mesh_s);
+    vsdmo_status st = guarded([&] {
+        Mesh& m = h->m;
+        m.type = elem_type;
+        m.k = k;
+        m.nV = n_vertices;
+        m.nE = n_elems;
+        m.seed = color_seed;
+        if (cuda_stream) {
+            m.stream = (cudaStream_t)cuda_stream;
+        } else {
+            VSDMO_CUDA(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+            m.own_stream = true;
+        }
+        DBuf<float> dx(3L * n_vertices, m.stream);
+        DBuf<int> de((long)n_elems * k, m.stream);
+        copy_in(dx.p, xyz, sizeof(float) * 3L * n_vertices, mem_space, m.stream);
+        copy_in(de.p, elems, sizeof(int) * (long)n_elems * k, mem_space, m.stream);
+        build_mesh(m, dx.p, de.p);
+        m.sync();
+    });
+    if (st != VSDMO_OK) {
+        if (h->m.own_stream && h->m.stream) {
+            cudaStream_t s = h->m.stream;
+            h.reset();
+            cudaStreamDestroy(s);
+        }
+        return st;
+    }
+    *out = h.release();
+    return VSDMO_OK;
+}
+
+VSDMO_API void vsdmo_mesh_destroy(vsdmo_mesh_t mesh) {
+    if (!mesh) return;
+    cudaStream_t s = mesh->m.stream;
+    bool own = mesh->m.own_stream;
+    cudaStreamSynchronize(s);
+    delete mesh;
+    if (own) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+}
+
+VSDMO_API vsdmo_status vsdmo_mesh_sync(vsdmo_mesh_t mesh) {
+    if (!mesh) return fail(VSDMO_E_ARG, "null mesh");
+    return guarded([&] { mesh->m.sync(); });
+}
+
+VSDMO_API int vsdmo_mesh_info(vsdmo_mesh_t mesh, int which) {
+    if (!mesh) return -1;
+    const Mesh& m = mesh->m;
+    switch (which) {
+    case VSDMO_I_NV: return m.nV;
+    case VSDMO_I_NE: return m.nE;
+    case VSDMO_I_NSURF: return m.nSurf;
+    case VSDMO_I_NFEATURE: return m.nFeature;
+    case VSDMO_I_NTRIS: return m.nTris;
+    case VSDMO_I_NHE: return m.nHE;
+    case VSDMO_I_NCOL_FREE: return m.nColFree;
+    case VSDMO_I_NCOL_FEATURE: return m.nColFeature;
+    case VSDMO_I_NCOL_INNER: return m.nColInner;
+    case VSDMO_I_MAX_HE: return m.maxHE;
+    case VSDMO_I_MAX_TETS: return m.maxTets;
+    case VSDMO_I_IS_FLAT: return m.isFlat;
+    default: return -1;
+    }
+}
+
+VSDMO_API long vsdmo_mesh_array_len(vsdmo_mesh_t mesh, int id) {
+    if (!mesh) return -1;
+    const Mesh& m = mesh->m;
+    switch (id) {
+    case VSDMO_A_XYZ: return 3L * m.nV;
+    case VSDMO_A_NEW_OF_OLD: return m.nV;
+    case VSDMO_A_ELEMS: return (long)m.nE * m.k;
+    case VSDMO_A_SURF_TRIS: return 3L * m.nTris;
+    case VSDMO_A_HE_ROWPTR: return m.he_rowptr.p ? m.nSurf + 1L : 0;
+    case VSDMO_A_HALFEDGES: return 4L * m.nHE;
+    case VSDMO_A_HF_ROWPTR: return m.hf_rowptr.p ? m.nV + 1L : 0;
+    case VSDMO_A_HALFFACES: return m.hf.p ? 12L * m.nE : 0;
+    case VSDMO_A_COL_FREE: return (long)m.col_free.size();
+    case VSDMO_A_COL_FEATURE: return (long)m.col_feature.size();
+    case VSDMO_A_COL_INNER: return (long)m.col_inner.size();
+    case VSDMO_A_IS_BOUNDARY1D: return m.isB1.p ? m.nSurf : 0;
+    case VSDMO_A_IS_FEATURE: return m.isFeat.p ? m.nSurf : 0;
+    case VSDMO_A_IS_BOUNDARY2D: return m.isB2.p ? m.nV : 0;
+    case VSDMO_A_FACE_NORMALS: return m.fn.p ? 3L * m.nTris : 0;
+    case VSDMO_A_VERTEX_NORMALS: return m.vn.p ? 3L * m.nSurf : 0;
+    default: return -1;
+    }
+}
+
+VSDMO_API vsdmo_status vsdmo_mesh_array(vsdmo_mesh_t mesh, int id, void* host_out) {
+    if (!mesh || !host_out) return fail(VSDMO_E_ARG, "null argument");
+    long n = vsdmo_mesh_array_len(mesh, id);
+    if (n < 0) return fail(VSDMO_E_ARG, "bad array id");
+    if (n == 0) return VSDMO_OK;
+    return guarded([&] {
+        Mesh& m = mesh->m;
+        cudaStream_t s = m.stream;
+        auto d2h = [&](const void* src, size_t bytes) {
+            VSDMO_CUDA(cudaMemcpyAsync(host_out, src, bytes, cudaMemcpyDeviceToHost, s));
+            VSDMO_CUDA(cudaStreamSynchronize(s));
+        };
+        switch (id) {
+        case VSDMO_A_XYZ: {
+            DBuf<float> t(3L * m.nV, s);
+            k_pack_xyz<<<grid_for(m.nV, 256), 256, 0, s>>>(m.pos.p, m.nV, nullptr, t.p);
+            VSDMO_CHECK_LAUNCH();
+            d2h(t.p, sizeof(float) * 3L * m.nV);
+            break;
+        }
+        case VSDMO_A_NEW_OF_OLD: d2h(m.new_of_old.p, sizeof(int) * n); break;
+        case VSDMO_A_ELEMS: d2h(m.elems.p, sizeof(int) * n); break;
+        case VSDMO_A_SURF_TRIS: d2h(m.tris.p, sizeof(int) * n); break;
+        case VSDMO_A_HE_ROWPTR: d2h(m.he_rowptr.p, sizeof(int) * n); break;
+        case VSDMO_A_HALFEDGES: d2h(m.he.p, sizeof(int) * n); break;
+        case VSDMO_A_HF_ROWPTR: d2h(m.hf_rowptr.p, sizeof(int) * n); break;
+        case VSDMO_A_HALFFACES: {
+            DBuf<int> t(n, s);
+            k_pack_hf<<<grid_for(n / 3, 256), 256, 0, s>>>(m.hf.p, n / 3, t.p);
+            VSDMO_CHECK_LAUNCH();
+            d2h(t.p, sizeof(int) * n);
+            break;
+        }
+        case VSDMO_A_COL_FREE: std::memcpy(host_out, m.col_free.data(), sizeof(int) * n); break;
+        case VSDMO_A_COL_FEATURE: std::memcpy(host_out, m.col_feature.data(), sizeof(int) * n); break;
+        case VSDMO_A_COL_INNER: std::memcpy(host_out, m.col_inner.data(), sizeof(int) * n); break;
+        case VSDMO_A_IS_BOUNDARY1D: d2h(m.isB1.p, n); break;
+        case VSDMO_A_IS_FEATURE: d2h(m.isFeat.p, n); break;
+        case VSDMO_A_IS_BOUNDARY2D: d2h(m.isB2.p, n); break;
+        case VSDMO_A_FACE_NORMALS: d2h(m.fn.p, sizeof(float) * n); break;
+        case VSDMO_A_VERTEX_NORMALS: d2h(m.vn.p, sizeof(float) * n); break;
+        }
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_mesh_permutation(vsdmo_mesh_t mesh, int32_t* host_new_of_old) {
+    return vsdmo_mesh_array(mesh, VSDMO_A_NEW_OF_OLD, host_new_of_old);
+}
+
+VSDMO_API vsdmo_status vsdmo_mesh_get_positions(vsdmo_mesh_t mesh, float* xyz, int original_order, int mem_space) {
+    if (!mesh || !xyz) return fail(VSDMO_E_ARG, "null argument");
+    if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
+    return guarded([&] {
+        Mesh& m = mesh->m;
+        cudaStream_t s = m.stream;
+        const int* map = original_order ? m.new_of_old.p : nullptr;
+        if (mem_space == VSDMO_DEVICE) {
+            k_pack_xyz<<<grid_for(m.nV, 256), 256, 0, s>>>(m.pos.p, m.nV, map, xyz);
+            VSDMO_CHECK_LAUNCH();
+            m.sync();
+        } else {
+            DBuf<float> t(3L * m.nV, s);
+            k_pack_xyz<<<grid_for(m.nV, 256), 256, 0, s>>>(m.pos.p, m.nV, map, t.p);
+            VSDMO_CHECK_LAUNCH();
+            VSDMO_CUDA(cudaMemcpyAsync(xyz, t.p, sizeof(float) * 3L * m.nV, cudaMemcpyDeviceToHost, s));
+            m.sync();
+        }
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* xyz, int original_order, int mem_space) {
+    if (!mesh || !xyz) return fail(VSDMO_E_ARG, "null argument");
+    if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
+    return guarded([&] {
+        Mesh& m = mesh->m;
+        cudaStream_t s = m.stream;
+        const int* map = original_order ? m.new_of_old.p : nullptr;
+        DBuf<float> t;
+        const float* src = xyz;
+        if (mem_space == VSDMO_HOST) {
+            t.alloc(3L * m.nV, s);
+            VSDMO_CUDA(cudaMemcpyAsync(t.p, xyz, sizeof(float) * 3L * m.nV, cudaMemcpyHostToDevice, s));
+            src = t.p;
+        }
+        k_unpack_xyz<<<grid_for(m.nV, 256), 256, 0, s>>>(m.pos.p, m.nV, map, src);
+        VSDMO_CHECK_LAUNCH();
+        if (mem_space == VSDMO_HOST) m.sync();  // the caller's host buffer may be reused on return
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* params, vsdmo_opt_t* out) {
+    if (!out) return fail(VSDMO_E_ARG, "null output handle");
+    *out = nullptr;
+    if (!mesh) return fail(VSDMO_E_ARG, "null mesh");
+    vsdmo_params p;
+    if (params) p = *params; else vsdmo_params_default(mesh->m.type, &p);
+    const Mesh& m = mesh->m;
+    if (p.quality != VSDMO_MEAN_RATIO) return fail(VSDMO_E_UNSUPPORTED, "only MEAN_RATIO is implemented");
+    if (p.grid_n != 8) return fail(VSDMO_E_UNSUPPORTED, "only an 8-point grid per axis is implemented");
+    if (p.depth < 1 || p.depth > 8) return fail(VSDMO_E_ARG, "depth must be in 1..8");
+    if (!(p.grid_scale > 0.f) || !std::isfinite(p.grid_scale)) return fail(VSDMO_E_ARG, "grid_scale must be positive");
+    if (p.n_iter < 0) return fail(VSDMO_E_ARG, "n_iter must be >= 0");
+    std::unique_ptr<vsdmo_opt_s> o(new vsdmo_opt_s);
+    o->mesh = mesh;
+    o->p = p;
+    if (m.type == VSDMO_TET) {
+        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "surface passes of volume meshes are not implemented yet; set fix_boundary=1");
+        if (m.maxTets > dmo_tet_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more tetrahedra than the kernel's ring budget");
+        o->tet = true;
+        for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
+    } else if (m.type == VSDMO_TRI) {
+        int flat = p.flat < 0 ? m.isFlat : p.flat;
+        if (!flat) return fail(VSDMO_E_UNSUPPORTED, "surface triangle DMO is not implemented yet");
+        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "sliding boundary vertices are not implemented yet; set fix_boundary=1");
+        if (m.maxHE > dmo_tri2d_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
+        o->tet = false;
+        for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+    } else {
+        return fail(VSDMO_E_UNSUPPORTED, "element type not supported");
+    }
+    vsdmo_status st = guarded([&] {
+        cudaStream_t s = m.stream;
+        o->d_iter.alloc(1, s); o->d_iter.zero();
+        o->pmin.alloc(quality_stats_blocks(), s);
+        o->psum.alloc(quality_stats_blocks(), s);
+        o->pfail.alloc(quality_stats_blocks(), s);
+        o->done.alloc(1, s); o->done.zero();
+        ensure_capacity(o.get(), std::max(p.n_iter, 1));
+        launch_quality_stats(m, p.quality, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1, s);
+        auto h = read_stats(o.get(), 0, 1);
+        o->last_min = h[0].min_q;
+    });
+    if (st != VSDMO_OK) return st;
+    *out = o.release();
+    return VSDMO_OK;
+}
+
+VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt) {
+    if (!opt) return;
+    cudaStreamSynchronize(opt->mesh->m.stream);
+    delete opt;
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t o, int n_iter) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    if (n_iter < 0) return fail(VSDMO_E_ARG, "n_iter < 0");
+    if (n_iter == 0) return VSDMO_OK;
+    int failures = 0;
+    vsdmo_status st = guarded([&] {
+        cudaStream_t s = o->mesh->m.stream;
+        ensure_capacity(o, o->iters_done + n_iter);
+        ensure_graph(o);
+        for (int i = 0; i < n_iter; ++i) {
+            if (o->exec) VSDMO_CUDA(cudaGraphLaunch(o->exec, s));
+            else run_iteration_body(o, s);
+        }
+        auto h = read_stats(o, o->iters_done + 1, n_iter);
+        for (auto& x : h) failures += x.fail_count;
+        o->iters_done += n_iter;
+        o->last_min = h.back().min_q;
+    });
+    if (st != VSDMO_OK) return st;
+    if (failures) return fail(VSDMO_E_MONOTONE, "minimum quality decreased during the iteration");
+    return VSDMO_OK;
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_optimize(vsdmo_opt_t o) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    int left = o->p.n_iter - o->iters_done;
+    if (left <= 0) return VSDMO_OK;
+    return vsdmo_opt_iterate(o, left);
+}
+
+VSDMO_API int vsdmo_opt_is_done(vsdmo_opt_t o) { return o ? (o->iters_done >= o->p.n_iter) : 1; }
+
+VSDMO_API int vsdmo_opt_iterations_done(vsdmo_opt_t o) { return o ? o->iters_done : -1; }
+
+VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t o) { return o ? (int)o->ranges.size() : -1; }
+
+VSDMO_API vsdmo_status vsdmo_opt_get_quality(vsdmo_opt_t o, float* q) {
+    if (!o || !q) return fail(VSDMO_E_ARG, "null argument");
+    *q = o->last_min;
+    return VSDMO_OK;
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_element_qualities(vsdmo_opt_t o, float* out, int mem_space) {
+    if (!o || !out) return fail(VSDMO_E_ARG, "null argument");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        cudaStream_t s = m.stream;
+        if (mem_space == VSDMO_DEVICE) {
+            launch_element_qualities(m, o->p.quality, out, s);
+            m.sync();
+        } else {
+            DBuf<float> t(m.nE, s);
+            launch_element_qualities(m, o->p.quality, t.p, s);
+            VSDMO_CUDA(cudaMemcpyAsync(out, t.p, sizeof(float) * m.nE, cudaMemcpyDeviceToHost, s));
+            m.sync();
+        }
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_find_min_quality(vsdmo_opt_t o, float* min_q, double* mean_q) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    std::vector<float> q;
+    vsdmo_status st = guarded([&] {
+        const Mesh& m = o->mesh->m;
+        DBuf<float> t(m.nE, m.stream);
+        launch_element_qualities(m, o->p.quality, t.p, m.stream);
+        q = t.to_host();
+    });
+    if (st != VSDMO_OK) return st;
+    float mn = INFINITY;
+    double sm = 0.0;
+    for (float x : q) { mn = std::min(mn, x); sm += x; }
+    if (min_q) *min_q = mn;
+    if (mean_q) *mean_q = q.empty() ? 0.0 : sm / (double)q.size();
+    return VSDMO_OK;
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_quality_histogram(vsdmo_opt_t o, int32_t* host_counts, int n_cols) {
+    if (!o || !host_counts || n_cols <= 0) return fail(VSDMO_E_ARG, "bad argument");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        DBuf<int> c(n_cols, m.stream);
+        c.zero();
+        launch_quality_histogram(m, o->p.quality, c.p, n_cols, m.stream);
+        auto h = c.to_host();
+        std::memcpy(host_counts, h.data(), sizeof(int) * n_cols);
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_display_quality(vsdmo_opt_t o, int n_cols) {
+    if (n_cols <= 0) n_cols = 10;
+    std::vector<int32_t> c(n_cols);
+    vsdmo_status st = vsdmo_opt_quality_histogram(o, c.data(), n_cols);
+    if (st != VSDMO_OK) return st;
+    float mn;
+    st = vsdmo_opt_find_min_quality(o, &mn, nullptr);
+    if (st != VSDMO_OK) return st;
+    // table layout of DMOBaseClass::printFormattedQuality (dmo/DMOBase.h:61-87)
+    int maxnum = *std::max_element(c.begin(), c.end());
+    int maxlen = std::max((int)std::log10(std::max(maxnum, 1)) + 1, 5);
+    std::ostringstream os;
+    os << "interval ";
+    for (int i = 0; i < n_cols; ++i) {
+        std::string si = std::to_string((float)i / (float)n_cols).substr(0, 4);
+        os << si;
+        for (int j = 0; j < maxlen - (int)si.size(); ++j) os << " |";
+    }
+    os << "\namount   ";
+    for (int i = 0; i < n_cols; ++i) {
+        std::string sn = std::to_string(c[i]);
+        os << sn;
+        for (int j = 0; j < maxlen - (int)sn.size(); ++j) os << " ";
+        os << "|";
+    }
+    os << "\nq_min = " << mn << "\n";
+    std::cout << os.str() << std::flush;
+    return VSDMO_OK;
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_history(vsdmo_opt_t o, float* min_q, double* mean_q, int cap, int* n) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    std::vector<IterStats> h;
+    vsdmo_status st = guarded([&] { h = read_stats(o, 0, o->iters_done + 1); });
+    if (st != VSDMO_OK) return st;
+    const int cnt = std::min(cap, (int)h.size());
+    const double nE = (double)o->mesh->m.nE;
+    for (int i = 0; i < cnt; ++i) {
+        if (min_q) min_q[i] = h[i].min_q;
+        if (mean_q) mean_q[i] = h[i].sum_q / nE;
+    }
+    if (n) *n = cnt;
+    return VSDMO_OK;
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_run_color(vsdmo_opt_t o, int color) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    if (color < 0 || color >= (int)o->ranges.size()) return fail(VSDMO_E_ARG, "colour out of range");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        DmoLaunch L{o->ranges[color].first, o->ranges[color].second, o->p.grid_scale, o->p.depth};
+        if (o->tet) launch_dmo_tet(m, L, m.stream); else launch_dmo_tri2d(m, L, m.stream);
+    });
+}
+
+}  // extern "C"

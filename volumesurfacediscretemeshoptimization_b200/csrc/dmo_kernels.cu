@@ -1,0 +1,474 @@
+// dmo_kernels.cu -- the DMO grid search and the quality reductions.
+//
+// Grid search (one colour class per launch, one warp per free vertex). Replaces
+//   k_optimizeHierarchicalInnerTet<128>  dmo/DMOTetImplCub.h:21-137  (tet interior)
+//   k_optimizeHierarchical2DFlat<32>     dmo/DMOTriFlatImplCub.h:24-152 (flat triangles)
+// Same search as the reference: N x N (x N) candidates per level centred on the current
+// position, half-extent grid_scale * (per-axis max ring distance) shrinking by 2/(N-1) per
+// level, the vertex moved to the best candidate (largest ring minimum of the mean ratio,
+// lowest linear index x-fastest on ties) when it strictly beats the current position, and
+// written back only on improvement. What differs is the arithmetic:
+//   * the ring is staged as per-element coefficients in shared memory: relative to the
+//     vertex and scaled by an exact power of two, the tet determinant is affine in the
+//     candidate p (det = d0 - n.p) and the sum of the six squared edge lengths is
+//     quadratic (L = C - 2 s.p + 3|p|^2); the flat-triangle area and edge sum likewise;
+//   * each lane owns 16 (tet) or 2 (2D) candidates of a separable grid, so one element
+//     costs 3 FMAs + a compare per candidate instead of a full metric evaluation;
+//   * the ring minimum is compared through the monotone transform det^2/L^3 (A/L in 2D),
+//     kept as a fraction and compared by cross-multiplication (no cbrt or divide per
+//     element); inverted elements key the ring by their most negative det / area, the
+//     analogue of the reference returning the negative volume / area;
+//   * the block-wide cub::ArgMax becomes a warp butterfly on (key, candidate index).
+// The library is compiled with --fmad=false: the only fused multiply-adds are the written
+// fmaf() calls, so the CPU restatement in oracle/or_dmo.c reproduces every bit.
+//
+// Quality reductions: k_quality_stats replaces k_updateCurrentQualities + k_findMinimumQuality
+// (dmo/DMOTet.cu:45-67) in one deterministic launch; k_quality_histogram and
+// k_element_qualities replace k_qualityHistogram / k_getElementQualities (dmo/DMOTet.cu:31-43,69-75).
+#include "vsdmo_internal.cuh"
+#include <cfloat>
+
+namespace vsdmo {
+namespace {
+
+constexpr int NQ = 8;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int TET_WARPS = 4;
+constexpr int TRI_WARPS = 4;
+constexpr int TET_MAX_RING = 512;
+constexpr int TRI_MAX_RING = 256;
+
+// candidate offsets (N-1-2i)/(N-1): i = 0 is +extent, i = N-1 is -extent (DMOTetImplCub.h:101-103)
+__device__ __forceinline__ float grid_offset(int i) {
+    switch (i) {
+    case 0: return 7.0f / 7.0f;
+    case 1: return 5.0f / 7.0f;
+    case 2: return 3.0f / 7.0f;
+    case 3: return 1.0f / 7.0f;
+    case 4: return -1.0f / 7.0f;
+    case 5: return -3.0f / 7.0f;
+    case 6: return -5.0f / 7.0f;
+    default: return -7.0f / 7.0f;
+    }
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+// (key, index): larger key wins, equal keys -> lower index (cub::ArgMax semantics)
+__device__ __forceinline__ void warp_argmax(float& k, int& i) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        float ok = __shfl_xor_sync(FULL, k, o);
+        int oi = __shfl_xor_sync(FULL, i, o);
+        if (ok > k || (ok == k && oi < i)) { k = ok; i = oi; }
+    }
+}
+
+// ---- tetrahedra ------------------------------------------------------------------------------
+// coefficients of tet (p, a, b, c) in scaled local coordinates
+__device__ __forceinline__ void tet_coeffs(float ax, float ay, float az, float bx, float by, float bz,
+                                           float cx, float cy, float cz, float4& K0, float4& K1) {
+    float ux = bx - ax, uy = by - ay, uz = bz - az;
+    float wx = cx - ax, wy = cy - ay, wz = cz - az;
+    float vx = cx - bx, vy = cy - by, vz = cz - bz;
+    float nx = uy * wz - uz * wy;
+    float ny = uz * wx - ux * wz;
+    float nz = ux * wy - uy * wx;
+    float d0 = (ax * nx + ay * ny) + az * nz;
+    float sx = (ax + bx) + cx, sy = (ay + by) + cy, sz = (az + bz) + cz;
+    float a2 = (ax * ax + ay * ay) + az * az;
+    float b2 = (bx * bx + by * by) + bz * bz;
+    float c2 = (cx * cx + cy * cy) + cz * cz;
+    float u2 = (ux * ux + uy * uy) + uz * uz;
+    float w2 = (wx * wx + wy * wy) + wz * wz;
+    float v2 = (vx * vx + vy * vy) + vz * vz;
+    K0 = make_float4(-nx, -ny, -nz, d0);
+    K1 = make_float4(-2.0f * sx, -2.0f * sy, -2.0f * sz, ((((a2 + b2) + c2) + u2) + w2) + v2);
+}
+
+// key of one candidate (used for the current position)
+__device__ float tet_key1(const float4* co, int k, float x, float y, float z) {
+    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    float N = 0.f, D = 1.f, dm = 0.f;
+    for (int t = 0; t < k; ++t) {
+        const float4 c0 = co[2 * t], c1 = co[2 * t + 1];
+        float detA = fmaf(c0.x, x, c0.w);
+        float LA = c1.w + fmaf(c1.x, x, tx);
+        float detB = fmaf(c0.y, y, detA);
+        float LB = LA + fmaf(c1.y, y, ty);
+        float det = fmaf(c0.z, z, detB);
+        float L = LB + fmaf(c1.z, z, tz);
+        float num = det * det;
+        float den = (L * L) * L;
+        if (t == 0) { N = num; D = den; dm = det; continue; }
+        if (num * D < N * den) { N = num; D = den; }
+        dm = fminf(dm, det);
+    }
+    return dm < 0.f ? dm : N / D;
+}
+
+__global__ void __launch_bounds__(TET_WARPS * 32)
+k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
+          int v0, int v1, float grid_scale, int depth, int maxk) {
+    extern __shared__ float4 smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int v = v0 + blockIdx.x * TET_WARPS + w;
+    if (v >= v1) return;
+    float4* co = smem + (size_t)w * maxk * 2;
+    const int b = rowptr[v], k = rowptr[v + 1] - b;
+    if (k <= 0 || k > maxk) return;
+    const float4 c0 = pos[v];
+    // pass 1: per-axis extent of the ring (DMOTetImplCub.h:54-64)
+    float mdx = 0.f, mdy = 0.f, mdz = 0.f;
+    for (int t = lane; t < k; t += 32) {
+        const int4 h = hf[b + t];
+        const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
+        mdx = fmaxf(mdx, fabsf(pa.x - c0.x)); mdy = fmaxf(mdy, fabsf(pa.y - c0.y)); mdz = fmaxf(mdz, fabsf(pa.z - c0.z));
+        mdx = fmaxf(mdx, fabsf(pb.x - c0.x)); mdy = fmaxf(mdy, fabsf(pb.y - c0.y)); mdz = fmaxf(mdz, fabsf(pb.z - c0.z));
+        mdx = fmaxf(mdx, fabsf(pc.x - c0.x)); mdy = fmaxf(mdy, fabsf(pc.y - c0.y)); mdz = fmaxf(mdz, fabsf(pc.z - c0.z));
+    }
+    mdx = warp_max(mdx); mdy = warp_max(mdy); mdz = warp_max(mdz);
+    const float mm = fmaxf(mdx, fmaxf(mdy, mdz));
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) return;
+    int ex;
+    (void)frexpf(mm, &ex);
+    // pass 2: element coefficients
+    for (int t = lane; t < k; t += 32) {
+        const int4 h = hf[b + t];
+        const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
+        float4 K0, K1;
+        tet_coeffs(ldexpf(pa.x - c0.x, -ex), ldexpf(pa.y - c0.y, -ex), ldexpf(pa.z - c0.z, -ex),
+                   ldexpf(pb.x - c0.x, -ex), ldexpf(pb.y - c0.y, -ex), ldexpf(pb.z - c0.z, -ex),
+                   ldexpf(pc.x - c0.x, -ex), ldexpf(pc.y - c0.y, -ex), ldexpf(pc.z - c0.z, -ex), K0, K1);
+        co[2 * t] = K0;
+        co[2 * t + 1] = K1;
+    }
+    __syncwarp();
+    const float sx = ldexpf(mdx, -ex), sy = ldexpf(mdy, -ex), sz = ldexpf(mdz, -ex);
+    const int ci = lane & 7, cj = lane >> 3;
+    const float oi = grid_offset(ci), oj0 = grid_offset(cj), oj1 = grid_offset(cj + 4);
+    float dx = 0.f, dy = 0.f, dz = 0.f;
+    float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
+    bool moved = false;
+    float ds = grid_scale;
+    for (int level = 0; level < depth; ++level) {
+        const float Sx = ds * sx, Sy = ds * sy, Sz = ds * sz;
+        const float x = fmaf(oi, Sx, dx);
+        const float y0 = fmaf(oj0, Sy, dy), y1 = fmaf(oj1, Sy, dy);
+        const float tx = (3.0f * x) * x, ty0 = (3.0f * y0) * y0, ty1 = (3.0f * y1) * y1;
+        float z[NQ], tz[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) { z[q] = fmaf(grid_offset(q), Sz, dz); tz[q] = (3.0f * z[q]) * z[q]; }
+        float N[2][NQ], D[2][NQ], dm[2][NQ];
+        {
+            const float4 K0 = co[0], K1 = co[1];
+            const float detA = fmaf(K0.x, x, K0.w);
+            const float LA = K1.w + fmaf(K1.x, x, tx);
+            const float detB0 = fmaf(K0.y, y0, detA), detB1 = fmaf(K0.y, y1, detA);
+            const float LB0 = LA + fmaf(K1.y, y0, ty0), LB1 = LA + fmaf(K1.y, y1, ty1);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const float lz = fmaf(K1.z, z[q], tz[q]);
+                float det = fmaf(K0.z, z[q], detB0), L = LB0 + lz;
+                N[0][q] = det * det; D[0][q] = (L * L) * L; dm[0][q] = det;
+                det = fmaf(K0.z, z[q], detB1); L = LB1 + lz;
+                N[1][q] = det * det; D[1][q] = (L * L) * L; dm[1][q] = det;
+            }
+        }
+        for (int t = 1; t < k; ++t) {
+            const float4 K0 = co[2 * t], K1 = co[2 * t + 1];
+            const float detA = fmaf(K0.x, x, K0.w);
+            const float LA = K1.w + fmaf(K1.x, x, tx);
+            const float detB0 = fmaf(K0.y, y0, detA), detB1 = fmaf(K0.y, y1, detA);
+            const float LB0 = LA + fmaf(K1.y, y0, ty0), LB1 = LA + fmaf(K1.y, y1, ty1);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const float lz = fmaf(K1.z, z[q], tz[q]);
+                {
+                    const float det = fmaf(K0.z, z[q], detB0), L = LB0 + lz;
+                    const float num = det * det, den = (L * L) * L;
+                    if (num * D[0][q] < N[0][q] * den) { N[0][q] = num; D[0][q] = den; }
+                    dm[0][q] = fminf(dm[0][q], det);
+                }
+                {
+                    const float det = fmaf(K0.z, z[q], detB1), L = LB1 + lz;
+                    const float num = det * det, den = (L * L) * L;
+                    if (num * D[1][q] < N[1][q] * den) { N[1][q] = num; D[1][q] = den; }
+                    dm[1][q] = fminf(dm[1][q], det);
+                }
+            }
+        }
+        // lane best in increasing linear index (i + 8 j + 64 k), strict >
+        float bk = -FLT_MAX;
+        int bi = 1 << 30;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj) {
+                const float key = dm[jj][q] < 0.f ? dm[jj][q] : N[jj][q] / D[jj][q];
+                if (key > bk) { bk = key; bi = ci + 8 * (cj + 4 * jj) + 64 * q; }
+            }
+        }
+        warp_argmax(bk, bi);
+        if (bi < NQ * NQ * NQ && qLast < bk) {
+            const float nx = fmaf(grid_offset(bi & 7), Sx, dx);
+            const float ny = fmaf(grid_offset((bi >> 3) & 7), Sy, dy);
+            const float nz = fmaf(grid_offset(bi >> 6), Sz, dz);
+            dx = nx; dy = ny; dz = nz;
+            qLast = bk;
+            moved = true;
+        }
+        ds = ds * (2.0f / 7.0f);
+    }
+    if (moved && lane == 0)
+        pos[v] = make_float4(c0.x + ldexpf(dx, ex), c0.y + ldexpf(dy, ex), c0.z + ldexpf(dz, ex), c0.w);
+}
+
+// ---- flat triangles ---------------------------------------------------------------------------
+__device__ __forceinline__ float tri_key(const float4* co, int k, float x, float y) {
+    const float tx = (2.0f * x) * x, ty = (2.0f * y) * y;
+    float N = 0.f, D = 1.f, am = 0.f;
+    for (int t = 0; t < k; ++t) {
+        const float4 c0 = co[2 * t], c1 = co[2 * t + 1];
+        const float A = fmaf(c0.y, y, fmaf(c0.x, x, c0.z));
+        const float L = (c0.w + fmaf(c1.x, x, tx)) + fmaf(c1.y, y, ty);
+        if (t == 0) { N = A; D = L; am = A; continue; }
+        if (A * D < N * L) { N = A; D = L; }
+        am = fminf(am, A);
+    }
+    return am < 0.f ? am : N / D;
+}
+
+__global__ void __launch_bounds__(TRI_WARPS * 32)
+k_dmo_tri2d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
+            int v0, int v1, float grid_scale, int depth, int maxk) {
+    extern __shared__ float4 smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int v = v0 + blockIdx.x * TRI_WARPS + w;
+    if (v >= v1) return;
+    float4* co = smem + (size_t)w * maxk * 2;
+    const int b = rowptr[v], k = rowptr[v + 1] - b;
+    if (k <= 0 || k > maxk) return;
+    const float4 c0 = pos[v];
+    float mdx = 0.f, mdy = 0.f;
+    for (int t = lane; t < k; t += 32) {
+        const float4 p = pos[he[b + t].x];
+        mdx = fmaxf(mdx, fabsf(p.x - c0.x));
+        mdy = fmaxf(mdy, fabsf(p.y - c0.y));
+    }
+    mdx = warp_max(mdx); mdy = warp_max(mdy);
+    const float mm = fmaxf(mdx, mdy);
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) return;
+    int ex;
+    (void)frexpf(mm, &ex);
+    for (int t = lane; t < k; t += 32) {
+        const float4 pa = pos[he[b + t].x];
+        const float4 pb = pos[he[b + (t + 1 == k ? 0 : t + 1)].x];
+        const float ax = ldexpf(pa.x - c0.x, -ex), ay = ldexpf(pa.y - c0.y, -ex);
+        const float bx = ldexpf(pb.x - c0.x, -ex), by = ldexpf(pb.y - c0.y, -ex);
+        const float ux = bx - ax, uy = by - ay;
+        const float C = ((ax * ax + ay * ay) + (bx * bx + by * by)) + (ux * ux + uy * uy);
+        co[2 * t] = make_float4(-uy, ux, ax * uy - ay * ux, C);
+        co[2 * t + 1] = make_float4(-2.0f * (ax + bx), -2.0f * (ay + by), 0.f, 0.f);
+    }
+    __syncwarp();
+    const float sx = ldexpf(mdx, -ex), sy = ldexpf(mdy, -ex);
+    const int i1 = lane >> 3, j1 = lane & 7;
+    const float o1 = grid_offset(i1), o2 = grid_offset(i1 + 4), oj = grid_offset(j1);
+    float dx = 0.f, dy = 0.f;
+    const float qOld = tri_key(co, k, 0.f, 0.f);
+    float qLast = qOld, lastMax = -FLT_MAX;
+    float ds = grid_scale;
+    for (int level = 0; level < depth; ++level) {
+        const float Sx = ds * sx, Sy = ds * sy;
+        const float x1 = fmaf(o1, Sx, dx), x2 = fmaf(o2, Sx, dx), y = fmaf(oj, Sy, dy);
+        const float q1 = tri_key(co, k, x1, y);
+        const float q2 = tri_key(co, k, x2, y);
+        float val = q1;
+        if (q2 > q1) val = q2;
+        const float selx = (q1 > q2) ? x1 : x2;
+        float bv = val;
+        int bl = lane;
+        warp_argmax(bv, bl);
+        if (qLast < bv) {
+            dx = __shfl_sync(FULL, selx, bl);
+            dy = __shfl_sync(FULL, y, bl);
+            qLast = bv;
+        }
+        lastMax = bv;
+        ds = ds * (2.0f / 7.0f);
+    }
+    if (qOld < lastMax && lane == 0)
+        pos[v] = make_float4(c0.x + ldexpf(dx, ex), c0.y + ldexpf(dy, ex), c0.z, c0.w);
+}
+
+// ---- reference element metrics ---------------------------------------------------------------
+// meanRatioMetricTet (dmo/DMOQualityTet.h:119-143)
+__device__ __forceinline__ float q_tet(float4 p0, float4 p1, float4 p2, float4 p3) {
+    const float e0x = p1.x - p0.x, e0y = p1.y - p0.y, e0z = p1.z - p0.z;
+    const float e1x = p2.x - p0.x, e1y = p2.y - p0.y, e1z = p2.z - p0.z;
+    const float e2x = p3.x - p0.x, e2y = p3.y - p0.y, e2z = p3.z - p0.z;
+    const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+    const float volume = (1.f / 6.f) * ((e0x * cx + e0y * cy) + e0z * cz);
+    if (volume < 0.f) return volume;
+    const float mu = cbrtf(volume * volume);
+    const float e3x = p2.x - p1.x, e3y = p2.y - p1.y, e3z = p2.z - p1.z;
+    const float e4x = p3.x - p1.x, e4y = p3.y - p1.y, e4z = p3.z - p1.z;
+    const float e5x = p3.x - p2.x, e5y = p3.y - p2.y, e5z = p3.z - p2.z;
+    float l = 0.f;
+    l += (e0x * e0x + e0y * e0y) + e0z * e0z;
+    l += (e1x * e1x + e1y * e1y) + e1z * e1z;
+    l += (e2x * e2x + e2y * e2y) + e2z * e2z;
+    l += (e3x * e3x + e3y * e3y) + e3z * e3z;
+    l += (e4x * e4x + e4y * e4y) + e4z * e4z;
+    l += (e5x * e5x + e5y * e5y) + e5z * e5z;
+    const float cbrtf9 = 2.0800838230519f;
+    return ((12.f * cbrtf9) * mu) / l;
+}
+
+// meanRatioMetricTri2D (dmo/DMOQualityTri.h:243-257)
+__device__ __forceinline__ float q_tri2d(float4 p0, float4 p1, float4 p2) {
+    const float e0x = p1.x - p0.x, e0y = p1.y - p0.y;
+    const float e1x = p2.x - p1.x, e1y = p2.y - p1.y;
+    const float e2x = p0.x - p2.x, e2y = p0.y - p2.y;
+    const float l = ((e0x * e0x + e0y * e0y) + (e1x * e1x + e1y * e1y)) + (e2x * e2x + e2y * e2y);
+    const float area = e0x * e1y - e0y * e1x;
+    if (area < 0.f) return area;
+    return ((2.f * sqrtf(3.f)) * area) / l;
+}
+
+__device__ __forceinline__ float element_quality(const int* __restrict__ el, int k, const float4* __restrict__ pos, long e) {
+    if (k == 4) {
+        const int4 t = reinterpret_cast<const int4*>(el)[e];
+        return q_tet(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
+    }
+    const int* t = el + 3 * e;
+    return q_tri2d(pos[t[0]], pos[t[1]], pos[t[2]]);
+}
+
+constexpr int QS_BLOCKS = 296;
+constexpr int QS_THREADS = 256;
+
+__global__ void __launch_bounds__(QS_THREADS)
+k_quality_stats(const int* __restrict__ el, int k, long nE, const float4* __restrict__ pos, IterStats* stats,
+                int* iter, float* pmin, double* psum, int* pfail, unsigned* done, int check, int init) {
+    __shared__ float smin[QS_THREADS / 32];
+    __shared__ double ssum[QS_THREADS / 32];
+    __shared__ int sfail[QS_THREADS / 32];
+    __shared__ bool last;
+    const int it = *iter;
+    const float lastMin = init ? -FLT_MAX : stats[it].min_q;
+    const float tol = 1e-6f * fmaxf(fabsf(lastMin), 1e-30f);
+    float mn = FLT_MAX;
+    double sm = 0.0;
+    int fl = 0;
+    for (long e = (long)blockIdx.x * QS_THREADS + threadIdx.x; e < nE; e += (long)QS_BLOCKS * QS_THREADS) {
+        const float q = element_quality(el, k, pos, e);
+        mn = fminf(mn, q);
+        sm += (double)q;
+        if (check && q < lastMin - tol) ++fl;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(FULL, mn, o));
+        sm += __shfl_xor_sync(FULL, sm, o);
+        fl += __shfl_xor_sync(FULL, fl, o);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) { smin[w] = mn; ssum[w] = sm; sfail[w] = fl; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float a = smin[0]; double s = ssum[0]; int f = sfail[0];
+        for (int i = 1; i < QS_THREADS / 32; ++i) { a = fminf(a, smin[i]); s += ssum[i]; f += sfail[i]; }
+        pmin[blockIdx.x] = a; psum[blockIdx.x] = s; pfail[blockIdx.x] = f;
+        __threadfence();
+        last = atomicAdd(done, 1u) == QS_BLOCKS - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        float a = FLT_MAX; double s = 0.0; int f = 0;
+        for (int i = 0; i < QS_BLOCKS; ++i) { a = fminf(a, ((volatile float*)pmin)[i]); s += ((volatile double*)psum)[i]; f += ((volatile int*)pfail)[i]; }
+        const int slot = init ? 0 : it + 1;
+        stats[slot].min_q = a;
+        stats[slot].sum_q = s;
+        stats[slot].fail_count = f;
+        if (!init) *iter = it + 1;
+        *done = 0u;
+    }
+}
+
+__global__ void k_element_qualities(const int* __restrict__ el, int k, long nE, const float4* __restrict__ pos, float* out) {
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nE; e += (long)gridDim.x * blockDim.x)
+        out[e] = element_quality(el, k, pos, e);
+}
+
+__global__ void k_quality_histogram(const int* __restrict__ el, int k, long nE, const float4* __restrict__ pos,
+                                    int* counts, int n_cols) {
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nE; e += (long)gridDim.x * blockDim.x) {
+        float q = fminf(0.9999f, element_quality(el, k, pos, e));
+        int idx = q > 0.f ? (int)(q * n_cols) : 0;  // a negative quality lands in bin 0
+        atomicAdd(&counts[idx], 1);
+    }
+}
+
+}  // namespace
+
+int dmo_tet_max_ring() { return TET_MAX_RING; }
+int dmo_tri2d_max_ring() { return TRI_MAX_RING; }
+int quality_stats_blocks() { return QS_BLOCKS; }
+
+void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxk = m.maxTets;
+    const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
+    static bool attr_set = false;
+    if (!attr_set) {
+        VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
+        attr_set = true;
+    }
+    k_dmo_tet<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
+        m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_dmo_tri2d(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxk = m.maxHE;
+    const size_t smem = (size_t)TRI_WARPS * maxk * 2 * sizeof(float4);
+    k_dmo_tri2d<<<(n + TRI_WARPS - 1) / TRI_WARPS, TRI_WARPS * 32, smem, s>>>(
+        m.pos.p, m.he_rowptr.p, m.he.p, L.v0, L.v1, L.grid_scale, L.depth, maxk);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_quality_stats(const Mesh& m, int quality, IterStats* d_stats, int* d_iter, float* d_partial_min,
+                          double* d_partial_sum, int* d_partial_fail, unsigned* d_done, int check_monotone,
+                          cudaStream_t s) {
+    (void)quality;
+    // check_monotone < 0 marks the initial evaluation (slot 0, no check, no increment)
+    const int init = check_monotone < 0 ? 1 : 0;
+    k_quality_stats<<<QS_BLOCKS, QS_THREADS, 0, s>>>(m.elems.p, m.k, m.nE, m.pos.p, d_stats, d_iter, d_partial_min,
+                                                     d_partial_sum, d_partial_fail, d_done, init ? 0 : check_monotone, init);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_element_qualities(const Mesh& m, int quality, float* d_out, cudaStream_t s) {
+    (void)quality;
+    k_element_qualities<<<grid_for(m.nE, 256), 256, 0, s>>>(m.elems.p, m.k, m.nE, m.pos.p, d_out);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_quality_histogram(const Mesh& m, int quality, int* d_counts, int n_cols, cudaStream_t s) {
+    (void)quality;
+    k_quality_histogram<<<grid_for(m.nE, 256), 256, 0, s>>>(m.elems.p, m.k, m.nE, m.pos.p, d_counts, n_cols);
+    VSDMO_CHECK_LAUNCH();
+}
+
+}  // namespace vsdmo

@@ -1,0 +1,200 @@
+// prim.cu -- device-wide primitives used by the connectivity build: exclusive scan, stable
+// LSD radix sort of (key, value) pairs, stable compaction and CSR offsets. These replace the
+// thrust::sort_by_key / remove_if / inclusive_scan calls of the reference's mesh build
+// (e.g. mesh/MeshTriGPU.cu:142,162-170, mesh/MeshTetGPU.cu:125) and k_find_first_n
+// (mesh/SortUtil.cu:3-35). The build runs once per mesh; these kernels are HBM-bound.
+#include "vsdmo_internal.cuh"
+
+namespace vsdmo {
+
+namespace {
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr unsigned FULL = 0xffffffffu;
+
+__global__ void k_scan_tiles(const int* in, int* out, long n, int* block_sums) {
+    __shared__ int warp_sum[SCAN_THREADS / 32];
+    const long base = (long)blockIdx.x * SCAN_TILE + (long)threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        v[i] = (base + i < n) ? in[base + i] : 0;
+        s += v[i];
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = lane < SCAN_THREADS / 32 ? warp_sum[lane] : 0;
+        int u = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(FULL, u, o);
+            if (lane >= o) u += y;
+        }
+        if (lane < SCAN_THREADS / 32) warp_sum[lane] = u - t;  // exclusive
+        if (lane == SCAN_THREADS / 32 - 1) block_sums[blockIdx.x] = u;
+    }
+    __syncthreads();
+    int run = warp_sum[w] + (x - s);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        if (base + i < n) out[base + i] = run;
+        run += v[i];
+    }
+}
+
+__global__ void k_scan_add(int* out, long n, const int* block_offs) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[i] += block_offs[i / SCAN_TILE];
+}
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ROUNDS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;
+constexpr int RS_WARPS = RS_THREADS / 32;
+
+__global__ void k_radix_hist(const uint32_t* keys, long n, int shift, int* counts, int nTiles) {
+    __shared__ int h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const long base = (long)blockIdx.x * RS_TILE;
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+        long idx = base + (long)r * RS_THREADS + threadIdx.x;
+        if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255u], 1);
+    }
+    __syncthreads();
+    counts[(long)threadIdx.x * nTiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void k_radix_scatter(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout,
+                                long n, int shift, const int* offs, int nTiles) {
+    __shared__ int base[256];
+    __shared__ int wcnt[RS_WARPS][257];
+    base[threadIdx.x] = offs[(long)threadIdx.x * nTiles + blockIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const long tile = (long)blockIdx.x * RS_TILE;
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+        for (int j = threadIdx.x; j < RS_WARPS * 257; j += RS_THREADS) (&wcnt[0][0])[j] = 0;
+        __syncthreads();
+        const long idx = tile + (long)r * RS_THREADS + threadIdx.x;
+        const bool valid = idx < n;
+        uint32_t k = valid ? kin[idx] : 0u;
+        int d = valid ? (int)((k >> shift) & 255u) : 256;
+        unsigned peers = __match_any_sync(FULL, d);
+        int rank = __popc(peers & lt);
+        if (lane == __ffs(peers) - 1) wcnt[w][d] = __popc(peers);
+        __syncthreads();
+        {
+            int s = base[threadIdx.x];
+#pragma unroll
+            for (int ww = 0; ww < RS_WARPS; ++ww) {
+                int t = wcnt[ww][threadIdx.x];
+                wcnt[ww][threadIdx.x] = s;
+                s += t;
+            }
+            base[threadIdx.x] = s;
+        }
+        __syncthreads();
+        if (valid) {
+            int pos = wcnt[w][d] + rank;
+            kout[pos] = k;
+            vout[pos] = vin[idx];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_flags_to_int(const uint8_t* f, int* o, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        o[i] = f[i] ? 1 : 0;
+}
+
+__global__ void k_compact_scatter(const uint8_t* f, const int* pos, long n, int* out) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        if (f[i]) out[pos[i]] = (int)i;
+}
+
+__global__ void k_count_keys(const uint32_t* keys, long n, int* counts) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        atomicAdd(&counts[keys[i]], 1);
+}
+}  // namespace
+
+int bits_for(uint32_t maxval) {
+    int b = 1;
+    while (b < 32 && (maxval >> b) != 0u) ++b;
+    return b;
+}
+
+void exclusive_scan(const int* d_in, int* d_out, long n, int* d_total, cudaStream_t s) {
+    if (n <= 0) {
+        if (d_total) VSDMO_CUDA(cudaMemsetAsync(d_total, 0, sizeof(int), s));
+        return;
+    }
+    long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    DBuf<int> sums(nb, s);
+    k_scan_tiles<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(d_in, d_out, n, sums.p);
+    VSDMO_CHECK_LAUNCH();
+    if (nb > 1) {
+        exclusive_scan(sums.p, sums.p, nb, d_total, s);
+        k_scan_add<<<grid_for(n, 256), 256, 0, s>>>(d_out, n, sums.p);
+        VSDMO_CHECK_LAUNCH();
+    } else if (d_total) {
+        VSDMO_CUDA(cudaMemcpyAsync(d_total, sums.p, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    }
+}
+
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, long n, int bits, cudaStream_t s) {
+    if (n <= 1 || bits <= 0) return;
+    const int nTiles = (int)((n + RS_TILE - 1) / RS_TILE);
+    DBuf<uint32_t> k2(n, s), v2(n, s);
+    DBuf<int> counts((long)256 * nTiles, s);
+    uint32_t *ka = keys, *va = vals, *kb = k2.p, *vb = v2.p;
+    int passes = 0;
+    for (int shift = 0; shift < bits; shift += 8, ++passes) {
+        k_radix_hist<<<nTiles, RS_THREADS, 0, s>>>(ka, n, shift, counts.p, nTiles);
+        VSDMO_CHECK_LAUNCH();
+        exclusive_scan(counts.p, counts.p, (long)256 * nTiles, nullptr, s);
+        k_radix_scatter<<<nTiles, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, counts.p, nTiles);
+        VSDMO_CHECK_LAUNCH();
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    if (ka != keys) {
+        VSDMO_CUDA(cudaMemcpyAsync(keys, ka, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        VSDMO_CUDA(cudaMemcpyAsync(vals, va, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    }
+}
+
+int compact_flags(const uint8_t* d_flags, long n, int* d_out_index, cudaStream_t s) {
+    if (n <= 0) return 0;
+    DBuf<int> pos(n, s), tot(1, s);
+    k_flags_to_int<<<grid_for(n, 256), 256, 0, s>>>(d_flags, pos.p, n);
+    VSDMO_CHECK_LAUNCH();
+    exclusive_scan(pos.p, pos.p, n, tot.p, s);
+    k_compact_scatter<<<grid_for(n, 256), 256, 0, s>>>(d_flags, pos.p, n, d_out_index);
+    VSDMO_CHECK_LAUNCH();
+    return read_scalar(tot.p, s);
+}
+
+void rowptr_from_sorted(const uint32_t* d_sorted_keys, long n, int K, int* d_rowptr, cudaStream_t s) {
+    DBuf<int> counts((long)K + 1, s);
+    counts.zero();
+    if (n > 0) {
+        k_count_keys<<<grid_for(n, 256), 256, 0, s>>>(d_sorted_keys, n, counts.p);
+        VSDMO_CHECK_LAUNCH();
+    }
+    exclusive_scan(counts.p, d_rowptr, (long)K + 1, nullptr, s);
+}
+
+}  // namespace vsdmo

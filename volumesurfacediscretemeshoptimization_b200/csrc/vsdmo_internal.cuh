@@ -1,0 +1,162 @@
+// vsdmo_internal.cuh -- shared declarations of the CUDA implementation behind include/vsdmo.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <stdexcept>
+#include <utility>
+
+#include "../../include/vsdmo.h"
+
+namespace vsdmo {
+
+// Internal error: carries a status code to the C ABI boundary (capi.cu), where it is
+// turned into a return value; nothing escapes the library as an exception.
+struct Error : std::runtime_error {
+    vsdmo_status status;
+    Error(vsdmo_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define VSDMO_CUDA(call)                                                                   \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            throw ::vsdmo::Error(e_ == cudaErrorMemoryAllocation ? VSDMO_E_NOMEM           \
+                                                                 : VSDMO_E_CUDA,           \
+                                 std::string(#call) + ": " + cudaGetErrorString(e_));      \
+        }                                                                                  \
+    } while (0)
+
+#define VSDMO_CHECK_LAUNCH() VSDMO_CUDA(cudaGetLastError())
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on the owning stream).
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    DBuf() = default;
+    DBuf(size_t count, cudaStream_t st) { alloc(count, st); }
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DBuf() { release(); }
+    void alloc(size_t count, cudaStream_t st) {
+        release();
+        s = st;
+        n = count;
+        if (count) VSDMO_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    void zero() { if (n) VSDMO_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void fill_bytes(int v) { if (n) VSDMO_CUDA(cudaMemsetAsync(p, v, n * sizeof(T), s)); }
+    std::vector<T> to_host() const {
+        std::vector<T> h(n);
+        if (n) {
+            VSDMO_CUDA(cudaMemcpyAsync(h.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+            VSDMO_CUDA(cudaStreamSynchronize(s));
+        }
+        return h;
+    }
+    T* get() const { return p; }
+};
+
+template <class T>
+inline T read_scalar(const T* dptr, cudaStream_t s) {
+    T v;
+    VSDMO_CUDA(cudaMemcpyAsync(&v, dptr, sizeof(T), cudaMemcpyDeviceToHost, s));
+    VSDMO_CUDA(cudaStreamSynchronize(s));
+    return v;
+}
+
+inline int grid_for(long n, int block, int cap = 148 * 32) {
+    long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+// ---- primitives (prim.cu) --------------------------------------------------------------
+// exclusive prefix sum of n ints (in may alias out); returns nothing, total written to
+// *d_total if non-null.
+void exclusive_scan(const int* d_in, int* d_out, long n, int* d_total, cudaStream_t s);
+// Stable LSD radix sort of (key, value) pairs on the low `bits` bits of the keys.
+void radix_sort_pairs(uint32_t* keys, uint32_t* vals, long n, int bits, cudaStream_t s);
+// Stable compaction: out[j] = i for the flagged positions i, in increasing order; returns count.
+int compact_flags(const uint8_t* d_flags, long n, int* d_out_index, cudaStream_t s);
+// CSR offsets [K+1] from n keys already sorted ascending (keys < K).
+void rowptr_from_sorted(const uint32_t* d_sorted_keys, long n, int K, int* d_rowptr, cudaStream_t s);
+int bits_for(uint32_t maxval);
+
+// ---- mesh (mesh_build.cu) ----------------------------------------------------------------
+struct Mesh {
+    int type = VSDMO_TRI;   // vsdmo_elem_type
+    int k = 3;              // vertices per element
+    int nV = 0, nE = 0;
+    int nSurf = 0, nFeature = 0, nTris = 0, nHE = 0;
+    int nColFree = 0, nColFeature = 0, nColInner = 0;
+    int maxHE = 0, maxTets = 0, isFlat = 0;
+    uint32_t seed = 1;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    DBuf<float4> pos;         // [nV] xyz + pad, internal numbering (the optimiser's state)
+    DBuf<int> new_of_old;     // [nV]
+    DBuf<int> elems;          // [nE*k]
+    DBuf<int> tris;           // [nTris*3]
+    DBuf<int> he_rowptr;      // [nSurf+1]
+    DBuf<int4> he;            // [nHE] target, opposite, face, next
+    DBuf<int> hf_rowptr;      // [nV+1]
+    DBuf<int4> hf;            // [4nT] v0, v1, v2, tet
+    DBuf<uint8_t> isB1, isFeat, isB2;
+    DBuf<float> fn, vn;       // [nTris*3], [nSurf*3]
+    std::vector<int> col_free, col_feature, col_inner;  // host copies of colour offsets
+    DBuf<int> d_col_free, d_col_feature, d_col_inner;
+
+    void sync() const { VSDMO_CUDA(cudaStreamSynchronize(stream)); }
+};
+
+// Builds connectivity + colouring from device arrays xyz [nV*3] and elems [nE*k].
+void build_mesh(Mesh& m, const float* d_xyz, const int* d_elems);
+
+// Normals of the surface (reference k_calcFaceNormals / k_calcVertexNormals).
+void update_normals(Mesh& m);
+
+// ---- DMO kernels (dmo_kernels.cu) ---------------------------------------------------------
+struct DmoLaunch {
+    int v0, v1;          // vertex range of one colour class
+    float grid_scale;
+    int depth;
+};
+void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
+void launch_dmo_tri2d(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
+int dmo_tet_max_ring();      // largest halfface row the tet kernel accepts
+int dmo_tri2d_max_ring();    // largest halfedge row the 2D kernel accepts
+
+// Per-iteration statistics written by the quality kernel.
+struct IterStats {
+    float min_q;
+    int fail_count;
+    double sum_q;
+};
+// Element qualities (reference formulas) -> min / sum into stats[*d_iter], monotonicity check
+// against min of the previous slot (or init_min for slot 0), then ++*d_iter.
+void launch_quality_stats(const Mesh& m, int quality, IterStats* d_stats, int* d_iter, float* d_partial_min,
+                          double* d_partial_sum, int* d_partial_fail, unsigned* d_done, int check_monotone,
+                          cudaStream_t s);
+void launch_element_qualities(const Mesh& m, int quality, float* d_out, cudaStream_t s);
+void launch_quality_histogram(const Mesh& m, int quality, int* d_counts, int n_cols, cudaStream_t s);
+int quality_stats_blocks();
+
+}  // namespace vsdmo
