@@ -414,7 +414,8 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->psum.alloc(quality_stats_blocks(), s);
         o->pfail.alloc(quality_stats_blocks(), s);
         o->done.alloc(1, s); o->done.zero();
-        ensure_capacity(o.get(), std::max(p.n_iter, 1));
+        prepare_dmo_kernels();
+        ensure_capacity(o.get(), std::min(std::max(p.n_iter, 1), 4096));
         launch_quality_stats(m, p.quality, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1, s);
         auto h = read_stats(o.get(), 0, 1);
         o->last_min = h[0].min_q;

@@ -419,6 +419,15 @@ __global__ void k_quality_histogram(const int* __restrict__ el, int k, long nE, 
 }  // namespace
 
 int dmo_tet_max_ring() { return TET_MAX_RING; }
+
+// Raises the dynamic shared-memory limit of the grid-search kernels (called once per
+// optimiser, outside any stream capture, on the current device).
+void prepare_dmo_kernels() {
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tri2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TRI_WARPS * TRI_MAX_RING * 2 * (int)sizeof(float4)));
+}
 int dmo_tri2d_max_ring() { return TRI_MAX_RING; }
 int quality_stats_blocks() { return QS_BLOCKS; }
 
@@ -427,12 +436,6 @@ void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
     if (n <= 0) return;
     const int maxk = m.maxTets;
     const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
-    static bool attr_set = false;
-    if (!attr_set) {
-        VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
-        attr_set = true;
-    }
     k_dmo_tet<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
         m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk);
     VSDMO_CHECK_LAUNCH();

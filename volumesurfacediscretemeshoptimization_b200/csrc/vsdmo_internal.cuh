@@ -142,6 +142,7 @@ struct DmoLaunch {
 void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
 void launch_dmo_tri2d(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
 int dmo_tet_max_ring();      // largest halfface row the tet kernel accepts
+void prepare_dmo_kernels();
 int dmo_tri2d_max_ring();    // largest halfedge row the 2D kernel accepts
 
 // Per-iteration statistics written by the quality kernel.
