@@ -161,6 +161,10 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
 VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt);
 /* n_iter calls of doIteration() (dmo/DMOTet.cu:128-170, dmo/DMOTriFlat.cu:129-166). */
 VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t opt, int n_iter);
+/* Restarts the optimiser from the mesh's current positions: iteration count back to 0 and
+ * the initial minimum quality re-evaluated (the reference constructs a new DMO object for
+ * that, dmo/DMOTet.cu:82-125). Use after vsdmo_mesh_set_positions. */
+VSDMO_API vsdmo_status vsdmo_opt_restart(vsdmo_opt_t opt);
 /* DMOBaseClass::optimize() (dmo/DMOBase.h:44-52): iterate until isDone(). */
 VSDMO_API vsdmo_status vsdmo_opt_optimize(vsdmo_opt_t opt);
 /* DMOTetClass::isDone() (dmo/DMOTet.h:26). */

@@ -49,6 +49,7 @@ struct or_mesh {
     int nSurf, nFeature, nTris, nHE;
     int nColFree, nColFeature, nColInner;
     int maxHE, maxTets, isFlat;
+    int fk;           /* vertices per surface face: 3 (tri / tet boundary) or 4 (quad) */
     float* xyz;
     int* new_of_old;
     int* elems;
@@ -229,11 +230,20 @@ static int third_vertex_tri(const int* t, int src, int dst) {
     return t[2];
 }
 
-static void calc_face_normals(int nTris, const int* tris, const float* xyz, float* fn, int* bad) {
+/* getThirdVertex for quads (mesh/MeshGPUCommon.cu:149-162): the corner two after dst */
+static int third_vertex_quad(const int* q, int src, int dst) {
+    (void)src;
+    if (dst == q[1]) return q[3];
+    if (dst == q[2]) return q[0];
+    if (dst == q[3]) return q[1];
+    return q[2];
+}
+
+static void calc_face_normals(int nTris, int fk, const int* tris, const float* xyz, float* fn, int* bad) {
     for (int t = 0; t < nTris; ++t) {
-        const float* p0 = xyz + 3 * (size_t)tris[3 * t];
-        const float* p1 = xyz + 3 * (size_t)tris[3 * t + 1];
-        const float* p2 = xyz + 3 * (size_t)tris[3 * t + 2];
+        const float* p0 = xyz + 3 * (size_t)tris[fk * t];
+        const float* p1 = xyz + 3 * (size_t)tris[fk * t + 1];
+        const float* p2 = xyz + 3 * (size_t)tris[fk * t + (fk == 4 ? 3 : 2)];
         float e0[3] = { p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2] };
         float e1[3] = { p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2] };
         float l0 = sqrtf(e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2]);
@@ -246,17 +256,17 @@ static void calc_face_normals(int nTris, const int* tris, const float* xyz, floa
 }
 
 /* first-pass halfedges (no dummies): rows by src in triangle order; he4[i] = {target,opp,face,next} */
-static void first_halfedges(int nS, int nTris, const int* tris, int** rowptr_out, int** he_out) {
-    int nHE = 3 * nTris;
+static void first_halfedges(int nS, int nTris, int fk, const int* tris, int** rowptr_out, int** he_out) {
+    int nHE = fk * nTris;
     int* keys = (int*)xc((size_t)nHE, sizeof(int));
-    for (int t = 0; t < nTris; ++t) for (int j = 0; j < 3; ++j) keys[3 * t + j] = tris[3 * t + j];
+    for (int t = 0; t < nTris; ++t) for (int j = 0; j < fk; ++j) keys[fk * t + j] = tris[fk * t + j];
     int* order = (int*)xc((size_t)nHE, sizeof(int));
     int* rowptr = (int*)xc((size_t)nS + 1, sizeof(int));
     counting_sort(nHE, keys, nS, order, rowptr);
     int* he = (int*)xc((size_t)nHE * 4, sizeof(int));
     for (int i = 0; i < nHE; ++i) {
-        int e = order[i], t = e / 3, j = e % 3;
-        he[4 * i] = tris[3 * t + (j + 1) % 3];
+        int e = order[i], t = e / fk, j = e % fk;
+        he[4 * i] = tris[fk * t + (j + 1) % fk];
         he[4 * i + 1] = -1; he[4 * i + 2] = t; he[4 * i + 3] = 0;
     }
     /* opposite: last entry of target's row pointing back to src */
@@ -272,8 +282,8 @@ static void first_halfedges(int nS, int nTris, const int* tris, int** rowptr_out
 
 static int final_halfedges(or_mesh* m, int nS, char* err, int err_len) {
     int* r1; int* h1;
-    first_halfedges(nS, m->nTris, m->tris, &r1, &h1);
-    int nHE1 = 3 * m->nTris;
+    first_halfedges(nS, m->nTris, m->fk, m->tris, &r1, &h1);
+    int nHE1 = m->fk * m->nTris;
     /* dummies: for every halfedge without opposite, a reversed one with face -1, keyed by its
      * target, appended after all real ones in sorted order (stable sort keeps that order) */
     int nD = 0;
@@ -326,7 +336,8 @@ static int final_halfedges(or_mesh* m, int nS, char* err, int err_len) {
         do {
             int currDst = h[0], currTri = h[2];
             if (currTri == -1) ERR("fan walk reached a boundary at vertex %d", src);
-            int nextVert = third_vertex_tri(m->tris + 3 * (size_t)currTri, src, currDst);
+            int nextVert = m->fk == 4 ? third_vertex_quad(m->tris + 4 * (size_t)currTri, src, currDst)
+                                      : third_vertex_tri(m->tris + 3 * (size_t)currTri, src, currDst);
             found = 0;
             for (int j = 0; j < n; ++j) if (in[4 * (start + j)] == nextVert) {
                 if (outPos >= n) ERR("non-manifold fan at vertex %d", src);
@@ -373,10 +384,10 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
     int nS = m->nSurf;
     int bad = 0;
     m->fn = (float*)xc((size_t)m->nTris * 3, sizeof(float));
-    calc_face_normals(m->nTris, m->tris, m->xyz, m->fn, &bad);
+    calc_face_normals(m->nTris, m->fk, m->tris, m->xyz, m->fn, &bad);
     if (bad) { if (err) snprintf(err, err_len, "degenerate triangle (edge shorter than 1e-6)"); return -1; }
     int* r1; int* h1;
-    first_halfedges(nS, m->nTris, m->tris, &r1, &h1);
+    first_halfedges(nS, m->nTris, m->fk, m->tris, &r1, &h1);
     m->isB1 = (uint8_t*)xc((size_t)nS, 1);
     m->isFeat = (uint8_t*)xc((size_t)nS, 1);
     for (int v = 0; v < nS; ++v)
@@ -403,7 +414,7 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
     int nTot = m->nV;
     int* inv = (int*)xc((size_t)nTot, sizeof(int));
     permute_range(0, nS, order, m->xyz, old_of_cur, m->isB1, m->isFeat, NULL, inv, nTot);
-    remap(m->nTris * 3, m->tris, inv, nS);
+    remap(m->nTris * m->fk, m->tris, inv, nS);
     if (m->type == OR_TET) remap(m->nE * 4, m->elems, inv, nS);
     free(order); free(inv);
     int nFree = 0;
@@ -419,7 +430,7 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
             else { m->col_feature = offs; m->nColFeature = 0; }
             continue;
         }
-        int cap = m->type == OR_TET ? 12 * m->nE : 6 * m->nTris;
+        int cap = m->type == OR_TET ? 12 * m->nE : (m->fk == 4 ? 12 : 6) * m->nTris;
         int* ps = (int*)xc((size_t)cap, sizeof(int));
         int* pd = (int*)xc((size_t)cap, sizeof(int));
         int np = 0;
@@ -427,6 +438,13 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
             static const int E[6][2] = { {0,1},{0,2},{0,3},{1,2},{1,3},{2,3} };
             for (int t = 0; t < m->nE; ++t) for (int e = 0; e < 6; ++e) {
                 int a = m->elems[4 * t + E[e][0]] - lo, b = m->elems[4 * t + E[e][1]] - lo;
+                if (a >= 0 && a < num && b >= 0 && b < num) { ps[np] = a; pd[np++] = b; ps[np] = b; pd[np++] = a; }
+            }
+        } else if (m->fk == 4) {
+            /* quad edges and both diagonals (mesh/MeshGPUCommon.cu:1067-1097) */
+            static const int E[6][2] = { {0,1},{1,2},{2,3},{3,0},{0,2},{1,3} };
+            for (int t = 0; t < m->nTris; ++t) for (int e = 0; e < 6; ++e) {
+                int a = m->tris[4 * t + E[e][0]] - lo, b = m->tris[4 * t + E[e][1]] - lo;
                 if (a >= 0 && a < num && b >= 0 && b < num) { ps[np] = a; pd[np++] = b; ps[np] = b; pd[np++] = a; }
             }
         } else {
@@ -438,7 +456,7 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
         }
         int* offs;
         int nc = color_and_sort_range(lo, num, np, ps, pd, seed, m->xyz, old_of_cur, m->isB1, m->isFeat, NULL,
-                                      nTot, m->tris, m->nTris * 3, m->type == OR_TET ? m->elems : NULL,
+                                      nTot, m->tris, m->nTris * m->fk, m->type == OR_TET ? m->elems : NULL,
                                       m->type == OR_TET ? m->nE * 4 : 0, &offs);
         if (part == 0) { m->col_free = offs; m->nColFree = nc; }
         else { m->col_feature = offs; m->nColFeature = nc; }
@@ -470,9 +488,9 @@ static int cmp_tri(const void* A, const void* B) {
 or_mesh* or_mesh_build(int elem_type, int nV, const float* xyz, int nE, const int32_t* elems,
                        uint32_t seed, char* err, int err_len) {
     if (err && err_len > 0) err[0] = 0;
-    if (elem_type != OR_TRI && elem_type != OR_TET) { if (err) snprintf(err, err_len, "element type not supported by the oracle"); return NULL; }
+    if (elem_type != OR_TRI && elem_type != OR_TET && elem_type != OR_QUAD) { if (err) snprintf(err, err_len, "element type not supported by the oracle"); return NULL; }
     if (nV <= 0 || nE <= 0 || !xyz || !elems) { if (err) snprintf(err, err_len, "empty mesh"); return NULL; }
-    int k = elem_type == OR_TET ? 4 : 3;
+    int k = elem_type == OR_TRI ? 3 : 4;
     for (long i = 0; i < (long)nE * k; ++i) if (elems[i] < 0 || elems[i] >= nV) { if (err) snprintf(err, err_len, "element index out of range"); return NULL; }
     or_mesh* m = (or_mesh*)xc(1, sizeof(or_mesh));
     m->type = elem_type; m->nV = nV; m->nE = nE; m->k = k;
@@ -482,16 +500,18 @@ or_mesh* or_mesh_build(int elem_type, int nV, const float* xyz, int nE, const in
     memcpy(m->elems, elems, sizeof(int) * (size_t)nE * k);
     int* old_of_cur = (int*)xc((size_t)nV, sizeof(int));
     for (int i = 0; i < nV; ++i) old_of_cur[i] = i;
-    if (elem_type == OR_TRI) {
+    if (elem_type == OR_TRI || elem_type == OR_QUAD) {
+        m->fk = k;
         m->isFlat = 1;
         for (int i = 0; i < nV; ++i) if (xyz[3 * i + 2] != 0.f) { m->isFlat = 0; break; }
         m->nSurf = nV; m->nTris = nE;
-        m->tris = (int*)xc((size_t)nE * 3, sizeof(int));
-        memcpy(m->tris, m->elems, sizeof(int) * 3 * (size_t)nE);
+        m->tris = (int*)xc((size_t)nE * k, sizeof(int));
+        memcpy(m->tris, m->elems, sizeof(int) * k * (size_t)nE);
         m->col_inner = (int*)xc(1, sizeof(int)); m->col_inner[0] = nV;
         if (surface_init(m, old_of_cur, seed, err, err_len)) goto fail;
-        memcpy(m->elems, m->tris, sizeof(int) * 3 * (size_t)nE);
+        memcpy(m->elems, m->tris, sizeof(int) * k * (size_t)nE);
     } else {
+        m->fk = 3;
         int nF = 4 * nE;
         tri3* f = (tri3*)xc((size_t)nF, sizeof(tri3));
         for (int t = 0; t < nE; ++t) {
@@ -612,7 +632,7 @@ long or_mesh_array_len(const or_mesh* m, int id) {
     case OR_A_XYZ: return 3L * m->nV;
     case OR_A_NEW_OF_OLD: return m->nV;
     case OR_A_ELEMS: return (long)m->nE * m->k;
-    case OR_A_SURF_TRIS: return 3L * m->nTris;
+    case OR_A_SURF_TRIS: return (long)m->fk * m->nTris;
     case OR_A_HE_ROWPTR: return m->he_rowptr ? m->nSurf + 1L : 0;
     case OR_A_HALFEDGES: return 4L * m->nHE;
     case OR_A_HF_ROWPTR: return m->hf_rowptr ? m->nV + 1L : 0;
@@ -662,3 +682,9 @@ const int* or__he_rowptr(const or_mesh* m) { return m->he_rowptr; }
 const int* or__he(const or_mesh* m) { return m->he; }
 const int* or__elems(const or_mesh* m) { return m->elems; }
 const int* or__col(const or_mesh* m, int which) { return which == 0 ? m->col_free : which == 1 ? m->col_feature : m->col_inner; }
+const int* or__faces(const or_mesh* m) { return m->tris; }
+int or__fk(const or_mesh* m) { return m->fk; }
+const float* or__vn(const or_mesh* m) { return m->vn; }
+const float* or__fn(const or_mesh* m) { return m->fn; }
+const uint8_t* or__isFeat(const or_mesh* m) { return m->isFeat; }
+int or__type(const or_mesh* m) { return m->type; }

@@ -203,6 +203,10 @@ class _DMOBase:
     def optimize(self):
         check(_capi.lib().vsdmo_opt_optimize(self.h))
 
+    def restart(self):
+        """Start over from the mesh's current positions (iteration count 0)."""
+        check(_capi.lib().vsdmo_opt_restart(self.h))
+
     def isDone(self) -> bool:
         return bool(_capi.lib().vsdmo_opt_is_done(self.h))
 

@@ -22,7 +22,7 @@ EXPORTED = [
     "vsdmo_mesh_create", "vsdmo_mesh_destroy", "vsdmo_mesh_info", "vsdmo_mesh_array_len",
     "vsdmo_mesh_array", "vsdmo_mesh_permutation", "vsdmo_mesh_get_positions",
     "vsdmo_mesh_set_positions", "vsdmo_mesh_sync", "vsdmo_opt_create", "vsdmo_opt_destroy",
-    "vsdmo_opt_iterate", "vsdmo_opt_optimize", "vsdmo_opt_is_done", "vsdmo_opt_iterations_done",
+    "vsdmo_opt_iterate", "vsdmo_opt_restart", "vsdmo_opt_optimize", "vsdmo_opt_is_done", "vsdmo_opt_iterations_done",
     "vsdmo_opt_get_quality", "vsdmo_opt_find_min_quality", "vsdmo_opt_element_qualities",
     "vsdmo_opt_quality_histogram", "vsdmo_opt_display_quality", "vsdmo_opt_history",
     "vsdmo_opt_run_color", "vsdmo_opt_launches_per_iteration",
@@ -83,6 +83,8 @@ def lib():
     L.vsdmo_opt_destroy.restype = None
     L.vsdmo_opt_iterate.restype = S
     L.vsdmo_opt_iterate.argtypes = [P, I]
+    L.vsdmo_opt_restart.restype = S
+    L.vsdmo_opt_restart.argtypes = [P]
     L.vsdmo_opt_optimize.restype = S
     L.vsdmo_opt_optimize.argtypes = [P]
     L.vsdmo_opt_is_done.argtypes = [P]

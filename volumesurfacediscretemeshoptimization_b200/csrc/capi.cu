@@ -454,6 +454,19 @@ VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t o, int n_iter) {
     return VSDMO_OK;
 }
 
+VSDMO_API vsdmo_status vsdmo_opt_restart(vsdmo_opt_t o) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        o->iters_done = 0;
+        o->d_iter.zero();
+        launch_quality_stats(m, o->p.quality, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1,
+                             m.stream);
+        auto h = read_stats(o, 0, 1);
+        o->last_min = h[0].min_q;
+    });
+}
+
 VSDMO_API vsdmo_status vsdmo_opt_optimize(vsdmo_opt_t o) {
     if (!o) return fail(VSDMO_E_ARG, "null optimiser");
     int left = o->p.n_iter - o->iters_done;
