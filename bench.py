@@ -245,7 +245,8 @@ def run_ours(args):
     traffic = None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "dmo_tet_config2_traffic.json")))
-        traffic = prof.get("dram_bytes_per_iteration")
+        # ncu DRAM bytes per vertex update, scaled to one iteration (the unit `achieved` uses)
+        traffic = prof["dram_bytes_per_vertex_update"] * n_inner
     except Exception:
         pass
     # FP32 work of the search as the reference formulates it: 3 levels x 512 candidates x 24
@@ -298,6 +299,7 @@ def run_ours(args):
                      "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
                      "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
                      "algorithmic_bytes_per_vertex_update": bytes_per_update,
+                     "per": "one iteration (all colour launches); achieved = algorithmic bytes / kernel time",
                      "kernel_ms_per_iteration": dmo_ms,
                      "note": "compute-bound kernel: HBM fraction is reported as asked; see fp32"},
         "fp32": {"reference_formulation_flop_per_vertex_update": ref_flop_per_update,

@@ -63,6 +63,17 @@ def lib():
         L.or_element_qualities_f32.argtypes = [P, P, P]
         L.or_optimize_f32.argtypes = [P, P, I, F, I, P, P]
         L.or_optimize_f64.argtypes = [P, P, I, D, I, P, P]
+        L.or_surface_normals_f32.argtypes = [P, P, P, P]
+        L.or_surface_fit_f32.argtypes = [P, P, P, P]
+        L.or_surface_fit_f64.argtypes = [P, P, P, P]
+        L.or_update_nn_f32.argtypes = [P, P, P, P]
+        L.or_update_nn_f64.argtypes = [P, P, P, P]
+        L.or_dmo_surf_f32.argtypes = [P, P, P, P, P, P, I, I, F, I]
+        L.or_dmo_surf_f64.argtypes = [P, P, P, P, P, P, I, I, D, P, I]
+        L.or_surface_qualities_f32.argtypes = [P, P, P]
+        L.or_surface_qualities_f64.argtypes = [P, P, P]
+        L.or_optimize_surf_f32.argtypes = [P, P, I, F, I, P, P]
+        L.or_optimize_surf_f64.argtypes = [P, P, I, D, I, P, P]
         L.or_q_tet_mean_ratio_f64.restype = D
         L.or_q_tet_mean_ratio_f64.argtypes = [P, P, P, P]
         L.or_q_tet_mean_ratio_f32.restype = F
@@ -140,28 +151,70 @@ class OracleMesh:
         fn(self.h, _p(xyz), v0, v1, grid_scale, _p(margin), nthreads)
         return xyz, margin[: v1 - v0]
 
+    @property
+    def is_surface(self):
+        """tri mesh that is not flat, or a quad mesh: optimised by the surface kernels"""
+        return self.elem_type == QUAD or (self.elem_type == TRI and not self.info["isFlat"])
+
     def optimize_f32(self, xyz, n_iter, grid_scale=0.5, nthreads=0):
         xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
         mn = np.zeros(n_iter); mean = np.zeros(n_iter)
-        lib().or_optimize_f32(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
+        fn = lib().or_optimize_surf_f32 if self.is_surface else lib().or_optimize_f32
+        fn(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
         return xyz, mn, mean
 
     def optimize_f64(self, xyz, n_iter, grid_scale=0.5, nthreads=0):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
         mn = np.zeros(n_iter); mean = np.zeros(n_iter)
-        lib().or_optimize_f64(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
+        fn = lib().or_optimize_surf_f64 if self.is_surface else lib().or_optimize_f64
+        fn(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
         return xyz, mn, mean
+
+    # ---- surface state (quadric fit, nearest initial vertex, normals) --------------------
+    def surface_state_f32(self, xyz):
+        """(xyz_init, local_surfaces[nSurf,16], nearest[nSurf], face_normals, vertex_normals)"""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+        nS, nF = self.info["nSurf"], self.info["nTris"]
+        fn = np.zeros((nF, 3), np.float32); vn = np.zeros((nS, 3), np.float32)
+        lib().or_surface_normals_f32(self.h, _p(xyz), _p(fn), _p(vn))
+        ls = np.zeros((nS, 16), np.float32)
+        lib().or_surface_fit_f32(self.h, _p(xyz), _p(vn), _p(ls))
+        return xyz.copy(), ls, np.arange(nS, dtype=np.int32), fn, vn
+
+    def surface_state_f64(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        nS = self.info["nSurf"]
+        vn = self.array(A_VERTEX_NORMALS).reshape(-1, 3).astype(np.float64)
+        ls = np.zeros((nS, 16), np.float64)
+        lib().or_surface_fit_f64(self.h, _p(xyz), _p(vn), _p(ls))
+        return xyz.copy(), ls, np.arange(nS, dtype=np.int32), vn
+
+    def dmo_surf_color_f32(self, xyz, state, v0, v1, grid_scale=0.5, nthreads=0):
+        x0, ls, nn, _, vn = state
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        lib().or_dmo_surf_f32(self.h, _p(xyz), _p(x0), _p(ls), _p(nn), _p(vn), v0, v1, grid_scale, nthreads)
+        return xyz
+
+    def dmo_surf_color_f64(self, xyz, x0, ls, nn, vn, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        margin = np.zeros(max(v1 - v0, 1))
+        lib().or_dmo_surf_f64(self.h, _p(xyz), _p(np.ascontiguousarray(x0, np.float64)),
+                              _p(np.ascontiguousarray(ls, np.float64)), _p(np.ascontiguousarray(nn, np.int32)),
+                              _p(np.ascontiguousarray(vn, np.float64)), v0, v1, grid_scale, _p(margin), nthreads)
+        return xyz, margin[: v1 - v0]
 
     def element_qualities_f64(self, xyz):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         q = np.zeros(self.info["nE"], dtype=np.float64)
-        lib().or_element_qualities_f64(self.h, _p(xyz), _p(q))
+        fn = lib().or_surface_qualities_f64 if self.is_surface else lib().or_element_qualities_f64
+        fn(self.h, _p(xyz), _p(q))
         return q
 
     def element_qualities_f32(self, xyz):
         xyz = np.ascontiguousarray(xyz, dtype=np.float32)
         q = np.zeros(self.info["nE"], dtype=np.float32)
-        lib().or_element_qualities_f32(self.h, _p(xyz), _p(q))
+        fn = lib().or_surface_qualities_f32 if self.is_surface else lib().or_element_qualities_f32
+        fn(self.h, _p(xyz), _p(q))
         return q
 
 

@@ -100,6 +100,29 @@ void or_optimize_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale,
 void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
                      double* min_hist, double* mean_hist);
 
+/* ---- surfaces (tri / quad meshes without feature vertices) ----------------------------- */
+/* local surfaces: 16 values per surface vertex: p0[3] a, e0[3] b, e1[3] c, e2[3] numPoints  */
+void or_surface_normals_f32(const or_mesh* m, const float* xyz, float* face_normals, float* vertex_normals);
+int  or_surface_fit_f32(const or_mesh* m, const float* xyz, const float* vertex_normals, float* local_surfaces);
+int  or_surface_fit_f64(const or_mesh* m, const double* xyz, const double* vertex_normals, double* local_surfaces);
+void or_update_nn_f32(const or_mesh* m, const float* xyz, const float* xyz_init, int32_t* nearest);
+void or_update_nn_f64(const or_mesh* m, const double* xyz, const double* xyz_init, int32_t* nearest);
+void or_dmo_surf_f32(const or_mesh* m, float* xyz, const float* xyz_init, const float* local_surfaces,
+                     const int32_t* nearest, const float* vertex_normals, int v0, int v1, float grid_scale, int nthreads);
+void or_dmo_surf_f64(const or_mesh* m, double* xyz, const double* xyz_init, const double* local_surfaces,
+                     const int32_t* nearest, const double* vertex_normals, int v0, int v1, double grid_scale,
+                     double* margin, int nthreads);
+void or_surface_qualities_f32(const or_mesh* m, const float* xyz, float* q);
+void or_surface_qualities_f64(const or_mesh* m, const double* xyz, double* q);
+void or_optimize_surf_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale, int nthreads,
+                          double* min_hist, double* mean_hist);
+void or_optimize_surf_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
+                          double* min_hist, double* mean_hist);
+float  or_q_tri3d_f32(const float* p0, const float* p1, const float* p2);
+double or_q_tri3d_f64(const double* p0, const double* p1, const double* p2);
+float  or_q_quad_f32(const float* p0, const float* p1, const float* p2, const float* p3, const float* n);
+double or_q_quad_f64(const double* p0, const double* p1, const double* p2, const double* p3, const double* n);
+
 #ifdef __cplusplus
 }
 #endif

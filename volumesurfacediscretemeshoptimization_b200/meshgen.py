@@ -172,7 +172,10 @@ def torus_quads(nu: int = 512, nv: int = 256, R: float = 1.0, r: float = 0.35):
 
 def perturb_surface(xyz, elems, seed: int = 0, tangential: float = 0.35, normal_sigma: float = 1e-3):
     """Tangential noise ``U(-t*l, t*l)`` (``l`` = mean incident edge length) in the tangent
-    plane of the area-weighted vertex normal, plus ``N(0, normal_sigma)`` along it."""
+    plane of the area-weighted vertex normal, plus ``N(0, normal_sigma * l)`` along it. The
+    normal noise is relative to the edge length: an absolute sigma of 1e-3 on edges of ~0.01
+    tilts neighbouring faces by more than 20 degrees and turns most vertices into feature
+    vertices under the reference's dihedral rule (mesh/MeshTriGPU.cu:506)."""
     xyz = xyz.astype(np.float64)
     k = elems.shape[1]
     nV = len(xyz)
@@ -194,7 +197,7 @@ def perturb_surface(xyz, elems, seed: int = 0, tangential: float = 0.35, normal_
     g = _rng(seed)
     a = g.uniform(-tangential, tangential, size=(nV, 2)) * lmean[:, None]
     nn = g.normal(0.0, normal_sigma, size=nV)
-    out = xyz + a[:, :1] * t1 + a[:, 1:] * t2 + nn[:, None] * vn
+    out = xyz + a[:, :1] * t1 + a[:, 1:] * t2 + (nn * lmean)[:, None] * vn
     return out.astype(np.float32)
 
 
