@@ -194,6 +194,30 @@ VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t opt);
 /* Waits for all work queued on the handle's stream. */
 VSDMO_API vsdmo_status vsdmo_mesh_sync(vsdmo_mesh_t mesh);
 
+/* ---- allocation-free quality reduction ------------------------------------------------- */
+/* No counterpart in the reference: an addition for callers that cannot allocate device
+ * memory -- an engine that hands this library a fixed arena and forbids further cudaMalloc,
+ * or code running where cudaMalloc / cudaFree are not allowed or would stall the device.
+ * Computes, over the n_elems elements of a mesh the caller holds on the device
+ * (d_xyz: float[3] per vertex, d_elems: 4 (VSDMO_TET) or 3 (VSDMO_TRI with flat = 1) int32 per
+ * element), the minimum element quality (mean ratio, the formula of vsdmo_opt_find_min_quality),
+ * the double-precision sum of the qualities and the number of elements whose quality is below
+ * `threshold`, written to the caller's device pointers d_min / d_sum / d_below.
+ *   - Allocates nothing: the per-block partial results live in a fixed 16,640-byte
+ *     __device__ array inside the library that every GPU loading the library holds until the
+ *     process exits. At most 8,388,608 elements per call; larger meshes are rejected with
+ *     VSDMO_E_ARG.
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ *     with that device current; make that first call before any stream capture.
+ *   - Asynchronous on cuda_stream (NULL = legacy default stream); results are valid after the
+ *     stream is synchronised.
+ *   - Every call shares the array: calls that overlap on the GPU (other streams, other host
+ *     threads) race and must be serialised by the caller. Each call clears the part that must
+ *     start at zero. */
+VSDMO_API vsdmo_status vsdmo_quality_reduce_noalloc(int elem_type, int flat, const float* d_xyz, int n_vertices,
+                                                    const int32_t* d_elems, int n_elems, float threshold,
+                                                    float* d_min, double* d_sum, int32_t* d_below, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

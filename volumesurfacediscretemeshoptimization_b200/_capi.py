@@ -25,7 +25,7 @@ EXPORTED = [
     "vsdmo_opt_iterate", "vsdmo_opt_restart", "vsdmo_opt_optimize", "vsdmo_opt_is_done", "vsdmo_opt_iterations_done",
     "vsdmo_opt_get_quality", "vsdmo_opt_find_min_quality", "vsdmo_opt_element_qualities",
     "vsdmo_opt_quality_histogram", "vsdmo_opt_display_quality", "vsdmo_opt_history",
-    "vsdmo_opt_run_color", "vsdmo_opt_launches_per_iteration",
+    "vsdmo_opt_run_color", "vsdmo_opt_launches_per_iteration", "vsdmo_quality_reduce_noalloc",
 ]
 
 
@@ -104,6 +104,8 @@ def lib():
     L.vsdmo_opt_history.argtypes = [P, P, P, I, C.POINTER(I)]
     L.vsdmo_opt_run_color.restype = S
     L.vsdmo_opt_run_color.argtypes = [P, I]
+    L.vsdmo_quality_reduce_noalloc.restype = S
+    L.vsdmo_quality_reduce_noalloc.argtypes = [I, I, P, I, P, I, F, P, P, P, P]
     _lib = L
     return L
 

@@ -588,4 +588,20 @@ VSDMO_API vsdmo_status vsdmo_opt_run_color(vsdmo_opt_t o, int color) {
     });
 }
 
+VSDMO_API vsdmo_status vsdmo_quality_reduce_noalloc(int elem_type, int flat, const float* d_xyz, int n_vertices,
+                                                    const int32_t* d_elems, int n_elems, float threshold, float* d_min,
+                                                    double* d_sum, int32_t* d_below, void* cuda_stream) {
+    if (elem_type != VSDMO_TET && !(elem_type == VSDMO_TRI && flat))
+        return fail(VSDMO_E_UNSUPPORTED, "the no-alloc reduction covers tetrahedra and flat triangles");
+    if (!d_xyz || !d_elems || !d_min || !d_sum || !d_below) return fail(VSDMO_E_ARG, "null pointer");
+    if (n_vertices <= 0 || n_elems <= 0) return fail(VSDMO_E_ARG, "empty mesh");
+    if ((long)n_elems > noalloc_max_elements())
+        return fail(VSDMO_E_ARG, "n_elems " + std::to_string(n_elems) + " exceeds the no-alloc limit of " +
+                                     std::to_string(noalloc_max_elements()) + " elements per call");
+    return guarded([&] {
+        quality_reduce_noalloc(elem_type == VSDMO_TET ? 4 : 3, d_xyz, d_elems, n_elems, threshold, d_min, d_sum, d_below,
+                               (cudaStream_t)cuda_stream);
+    });
+}
+
 }  // extern "C"

@@ -160,4 +160,9 @@ void launch_element_qualities(const Mesh& m, int quality, float* d_out, cudaStre
 void launch_quality_histogram(const Mesh& m, int quality, int* d_counts, int n_cols, cudaStream_t s);
 int quality_stats_blocks();
 
+// ---- allocation-free quality reduction (noalloc.cu) -----------------------------------------
+long noalloc_max_elements();
+void quality_reduce_noalloc(int k, const float* d_xyz, const int* d_elems, long n_elems, float threshold,
+                            float* d_min, double* d_sum, int* d_below, cudaStream_t s);
+
 }  // namespace vsdmo
