@@ -33,7 +33,17 @@ namespace {
 
 constexpr int NQ = 8;
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int TET_WARPS = 4;
+// launch shape of the tet kernel (tuned on B200, see profiles/)
+#ifndef TET_WARPS_CFG
+#define TET_WARPS_CFG 4
+#endif
+#ifndef TET_MIN_BLOCKS
+#define TET_MIN_BLOCKS 0
+#endif
+#ifndef TET_SPLIT_Y
+#define TET_SPLIT_Y 0
+#endif
+constexpr int TET_WARPS = TET_WARPS_CFG;
 constexpr int TRI_WARPS = 4;
 constexpr int TET_MAX_RING = 512;
 constexpr int TRI_MAX_RING = 256;
@@ -111,7 +121,62 @@ __device__ float tet_key1(const float4* co, int k, float x, float y, float z) {
     return dm < 0.f ? dm : N / D;
 }
 
-__global__ void __launch_bounds__(TET_WARPS * 32)
+// Ring minimum of the lane's candidates (fixed x, NJ y values, all NQ z values) over the k
+// tets of the ring; returns the lane's best (key, linear index), strict > in index order.
+template <int NJ>
+__device__ __forceinline__ void tet_lane_best(const float4* __restrict__ co, int k, float x, const float* y,
+                                              const float* z, const float* tz, int ci, int cj, int jbase,
+                                              float& bk, int& bi) {
+    const float tx = (3.0f * x) * x;
+    float ty[NJ];
+#pragma unroll
+    for (int jj = 0; jj < NJ; ++jj) ty[jj] = (3.0f * y[jj]) * y[jj];
+    float N[NJ][NQ], D[NJ][NQ], dm[NJ][NQ];
+    {
+        const float4 K0 = co[0], K1 = co[1];
+        const float detA = fmaf(K0.x, x, K0.w);
+        const float LA = K1.w + fmaf(K1.x, x, tx);
+#pragma unroll
+        for (int jj = 0; jj < NJ; ++jj) {
+            const float detB = fmaf(K0.y, y[jj], detA), LB = LA + fmaf(K1.y, y[jj], ty[jj]);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const float det = fmaf(K0.z, z[q], detB), L = LB + fmaf(K1.z, z[q], tz[q]);
+                N[jj][q] = det * det; D[jj][q] = (L * L) * L; dm[jj][q] = det;
+            }
+        }
+    }
+    for (int t = 1; t < k; ++t) {
+        const float4 K0 = co[2 * t], K1 = co[2 * t + 1];
+        const float detA = fmaf(K0.x, x, K0.w);
+        const float LA = K1.w + fmaf(K1.x, x, tx);
+        float detB[NJ], LB[NJ];
+#pragma unroll
+        for (int jj = 0; jj < NJ; ++jj) { detB[jj] = fmaf(K0.y, y[jj], detA); LB[jj] = LA + fmaf(K1.y, y[jj], ty[jj]); }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const float lz = fmaf(K1.z, z[q], tz[q]);
+#pragma unroll
+            for (int jj = 0; jj < NJ; ++jj) {
+                const float det = fmaf(K0.z, z[q], detB[jj]), L = LB[jj] + lz;
+                const float num = det * det, den = (L * L) * L;
+                if (num * D[jj][q] < N[jj][q] * den) { N[jj][q] = num; D[jj][q] = den; }
+                dm[jj][q] = fminf(dm[jj][q], det);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+#pragma unroll
+        for (int jj = 0; jj < NJ; ++jj) {
+            const float key = dm[jj][q] < 0.f ? dm[jj][q] : N[jj][q] / D[jj][q];
+            const int idx = ci + 8 * (cj + 4 * (jbase + jj)) + 64 * q;
+            if (key > bk || (key == bk && idx < bi)) { bk = key; bi = idx; }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
 k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
           int v0, int v1, float grid_scale, int depth, int maxk) {
     extern __shared__ float4 smem[];
@@ -158,61 +223,18 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
     for (int level = 0; level < depth; ++level) {
         const float Sx = ds * sx, Sy = ds * sy, Sz = ds * sz;
         const float x = fmaf(oi, Sx, dx);
-        const float y0 = fmaf(oj0, Sy, dy), y1 = fmaf(oj1, Sy, dy);
-        const float tx = (3.0f * x) * x, ty0 = (3.0f * y0) * y0, ty1 = (3.0f * y1) * y1;
+        const float y[2] = { fmaf(oj0, Sy, dy), fmaf(oj1, Sy, dy) };
         float z[NQ], tz[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; ++q) { z[q] = fmaf(grid_offset(q), Sz, dz); tz[q] = (3.0f * z[q]) * z[q]; }
-        float N[2][NQ], D[2][NQ], dm[2][NQ];
-        {
-            const float4 K0 = co[0], K1 = co[1];
-            const float detA = fmaf(K0.x, x, K0.w);
-            const float LA = K1.w + fmaf(K1.x, x, tx);
-            const float detB0 = fmaf(K0.y, y0, detA), detB1 = fmaf(K0.y, y1, detA);
-            const float LB0 = LA + fmaf(K1.y, y0, ty0), LB1 = LA + fmaf(K1.y, y1, ty1);
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                const float lz = fmaf(K1.z, z[q], tz[q]);
-                float det = fmaf(K0.z, z[q], detB0), L = LB0 + lz;
-                N[0][q] = det * det; D[0][q] = (L * L) * L; dm[0][q] = det;
-                det = fmaf(K0.z, z[q], detB1); L = LB1 + lz;
-                N[1][q] = det * det; D[1][q] = (L * L) * L; dm[1][q] = det;
-            }
-        }
-        for (int t = 1; t < k; ++t) {
-            const float4 K0 = co[2 * t], K1 = co[2 * t + 1];
-            const float detA = fmaf(K0.x, x, K0.w);
-            const float LA = K1.w + fmaf(K1.x, x, tx);
-            const float detB0 = fmaf(K0.y, y0, detA), detB1 = fmaf(K0.y, y1, detA);
-            const float LB0 = LA + fmaf(K1.y, y0, ty0), LB1 = LA + fmaf(K1.y, y1, ty1);
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                const float lz = fmaf(K1.z, z[q], tz[q]);
-                {
-                    const float det = fmaf(K0.z, z[q], detB0), L = LB0 + lz;
-                    const float num = det * det, den = (L * L) * L;
-                    if (num * D[0][q] < N[0][q] * den) { N[0][q] = num; D[0][q] = den; }
-                    dm[0][q] = fminf(dm[0][q], det);
-                }
-                {
-                    const float det = fmaf(K0.z, z[q], detB1), L = LB1 + lz;
-                    const float num = det * det, den = (L * L) * L;
-                    if (num * D[1][q] < N[1][q] * den) { N[1][q] = num; D[1][q] = den; }
-                    dm[1][q] = fminf(dm[1][q], det);
-                }
-            }
-        }
-        // lane best in increasing linear index (i + 8 j + 64 k), strict >
         float bk = -FLT_MAX;
         int bi = 1 << 30;
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-#pragma unroll
-            for (int jj = 0; jj < 2; ++jj) {
-                const float key = dm[jj][q] < 0.f ? dm[jj][q] : N[jj][q] / D[jj][q];
-                if (key > bk) { bk = key; bi = ci + 8 * (cj + 4 * jj) + 64 * q; }
-            }
-        }
+#if TET_SPLIT_Y
+        tet_lane_best<1>(co, k, x, &y[0], z, tz, ci, cj, 0, bk, bi);
+        tet_lane_best<1>(co, k, x, &y[1], z, tz, ci, cj, 1, bk, bi);
+#else
+        tet_lane_best<2>(co, k, x, y, z, tz, ci, cj, 0, bk, bi);
+#endif
         warp_argmax(bk, bi);
         if (bi < NQ * NQ * NQ && qLast < bk) {
             const float nx = fmaf(grid_offset(bi & 7), Sx, dx);
