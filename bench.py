@@ -179,7 +179,7 @@ def run_ours(args):
         V.DMOMeshTet.__init__(mesh, None, None, 1, sp, (d_xyz.data_ptr(), d_tets.data_ptr(), len(xyz), len(tets)))
     n_inner = mesh.info["nV"] - mesh.info["nSurf"]
     opt = V.DMOTetClass(mesh, n_iter=10 ** 9)
-    launches_per_iter = opt.launches_per_iteration + 1
+    launches_per_iter = opt.launches_per_iteration   # colour launches + the quality kernel
     x0 = torch.empty(len(xyz) * 3, dtype=torch.float32, device=dev)
     mesh.positions_to_device(x0.data_ptr(), original_order=False)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -222,8 +222,7 @@ def run_ours(args):
     # ---- roofline of the grid-search kernel (separate pass, same stream) -----------------------------
     reset()
     opt.restart()
-    n_col = opt.launches_per_iteration
-    offs = mesh.array(V.A_COL_INNER)
+    n_col = mesh.info["nColorsInner"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)

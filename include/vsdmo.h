@@ -72,7 +72,7 @@ typedef enum vsdmo_array_id {
     VSDMO_A_XYZ = 0,             /* float [nV*3]      positions, internal order                */
     VSDMO_A_NEW_OF_OLD = 1,      /* int32 [nV]        new index of every input vertex          */
     VSDMO_A_ELEMS = 2,           /* int32 [nE*k]      elements, internal vertex numbering      */
-    VSDMO_A_SURF_TRIS = 3,       /* int32 [nTris*3]   surface triangles (tet: boundary faces)  */
+    VSDMO_A_SURF_TRIS = 3,       /* int32 [nTris*fk]  surface faces, fk = 4 for quad meshes else 3 */
     VSDMO_A_HE_ROWPTR = 4,       /* int32 [nSurf+1]   halfedge CSR, CCW fan per vertex         */
     VSDMO_A_HALFEDGES = 5,       /* int32 [nHE*4]     {target, opposite, face, next}           */
     VSDMO_A_HF_ROWPTR = 6,       /* int32 [nV+1]      halfface CSR (tet)                       */
@@ -155,11 +155,14 @@ VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* 
                                                 int mem_space);
 
 /* ---- optimiser ------------------------------------------------------------------------- */
-/* Replaces DMOTetClass / DMOTriFlatClass construction + init()
- * (dmo/DMOTet.cu:82-125, dmo/DMOTriFlat.cu:84-126). */
+/* Replaces DMOTetClass / DMOTriFlatClass / DMOTriClass / DMOQuadClass construction + init()
+ * (dmo/DMOTet.cu:82-125, dmo/DMOTriFlat.cu:84-126, dmo/DMOTri.cu:80-126, dmo/DMOQuad.cu:78-123).
+ * Tri meshes that are not flat (or flat = 0) and quad meshes get the surface optimiser; it
+ * needs a mesh without feature vertices (VSDMO_E_UNSUPPORTED otherwise). */
 VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* params, vsdmo_opt_t* out);
 VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt);
-/* n_iter calls of doIteration() (dmo/DMOTet.cu:128-170, dmo/DMOTriFlat.cu:129-166). */
+/* n_iter calls of doIteration() (dmo/DMOTet.cu:128-170, dmo/DMOTriFlat.cu:129-166,
+ * dmo/DMOTri.cu:129-165, dmo/DMOQuad.cu:125-162). */
 VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t opt, int n_iter);
 /* Restarts the optimiser from the mesh's current positions: iteration count back to 0 and
  * the initial minimum quality re-evaluated (the reference constructs a new DMO object for
@@ -185,11 +188,19 @@ VSDMO_API vsdmo_status vsdmo_opt_display_quality(vsdmo_opt_t opt, int n_cols);
  * "it,q_min" lines, dmo/DMOTet.cu:167). Returns the count in *n (at most cap). */
 VSDMO_API vsdmo_status vsdmo_opt_history(vsdmo_opt_t opt, float* min_q, double* mean_q, int cap, int* n);
 /* One launch of the grid-search kernel over colour class `color` of the inner (tet) or free
- * (flat tri) partition -- a single step of doIteration's colour loop, for parity tests and
+ * (tri / quad) partition -- a single step of doIteration's colour loop, for parity tests and
  * per-kernel timing. Asynchronous: it returns once the launch is queued on the stream. */
 VSDMO_API vsdmo_status vsdmo_opt_run_color(vsdmo_opt_t opt, int color);
-/* Number of grid-search kernel launches issued per iteration (for launch accounting). */
+/* Number of kernel launches one iteration issues: the colour launches, the quality kernel
+ * and, for surface optimisers, the nearest-neighbour walk and the two normal kernels. */
 VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t opt);
+/* Surface optimisers (tri / quad surface meshes): copies to host memory, in the internal
+ * vertex numbering, the state the reference keeps as DMOTriClass / DMOQuadClass members
+ * (dmo/DMOTri.cu:95-112): vertexPointsInit as xyz_init [nSurf*3], localSurfacesInit as
+ * local_surfaces [nSurf*16] (p0[3] a, t1[3] b, t2[3] c, n[3] numPoints) and nearestNeighbors
+ * as nearest [nSurf]. Any output may be NULL. VSDMO_E_ARG for other optimisers. */
+VSDMO_API vsdmo_status vsdmo_opt_surface_state(vsdmo_opt_t opt, float* xyz_init, float* local_surfaces,
+                                               int32_t* nearest);
 
 /* Waits for all work queued on the handle's stream. */
 VSDMO_API vsdmo_status vsdmo_mesh_sync(vsdmo_mesh_t mesh);

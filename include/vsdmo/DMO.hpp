@@ -1,11 +1,13 @@
 // DMO.hpp -- C++ host API with the reference's class names, over the C ABI of vsdmo.h.
 //
 // Mirrors the interface a user of DanielZint/VolumeSurfaceDiscreteMeshOptimization calls:
-//   DMOMeshTriFactory / DMOMeshTetFactory::create   mesh/MeshFactory.h:17-40
-//   DMOMeshTri / DMOMeshTet                         mesh/DMOMeshTri.h:81-94, mesh/DMOMeshTet.h:145-198
+//   DMOMeshTri/Quad/TetFactory::create              mesh/MeshFactory.h:17-40
+//   DMOMeshTri / DMOMeshQuad / DMOMeshTet           mesh/DMOMeshTri.h:81-94, mesh/DMOMeshQuad.h,
+//                                                   mesh/DMOMeshTet.h:145-198
 //   DMO::QualityCriterium                           dmo/DMOQualityUtil.h:10-18
 //   DMO::DMOBaseClass, DMOTetClass, DMOTriFlatClass dmo/DMOBase.h:23-88, dmo/DMOTet.h:21-62,
 //                                                   dmo/DMOTriFlat.h:19-51
+//   DMO::DMOTriClass, DMOQuadClass (surfaces)       dmo/DMOTri.h, dmo/DMOQuad.h
 // Header-only; link against libvsdmo.so. Errors surface as DMO::Error exceptions carrying the
 // vsdmo_status (the reference exits through gpuErrchk or throws 1 instead).
 #pragma once
@@ -78,6 +80,12 @@ public:
         : DMOMesh(VSDMO_TRI, points, nVS, tris, nT, memSpace) {}
 };
 
+class DMOMeshQuad : public DMOMesh {
+public:
+    DMOMeshQuad(int nVS, int nQ, const float* points, const int32_t* quads, int memSpace = VSDMO_HOST)
+        : DMOMesh(VSDMO_QUAD, points, nVS, quads, nQ, memSpace) {}
+};
+
 class DMOMeshTet : public DMOMesh {
 public:
     DMOMeshTet(int nV, int nT, const float* points, const int32_t* tets, int memSpace = VSDMO_HOST)
@@ -88,6 +96,13 @@ struct DMOMeshTriFactory {
     static std::shared_ptr<DMOMeshTri> create(int nVS, int nT, const float* points, const int32_t* tris,
                                               int memSpace = VSDMO_HOST) {
         return std::make_shared<DMOMeshTri>(nVS, nT, points, tris, memSpace);
+    }
+};
+
+struct DMOMeshQuadFactory {
+    static std::shared_ptr<DMOMeshQuad> create(int nVS, int nQ, const float* points, const int32_t* quads,
+                                               int memSpace = VSDMO_HOST) {
+        return std::make_shared<DMOMeshQuad>(nVS, nQ, points, quads, memSpace);
     }
 };
 
@@ -154,6 +169,22 @@ public:
     DMOTriFlatClass(DMOMeshTri& mesh, QualityCriterium q = QualityCriterium::MEAN_RATIO, float gridScale = 0.5f,
                     int n_iter = 30, bool fixBoundary = true)
         : DMOBaseClass(mesh, q, gridScale, n_iter, 1, fixBoundary) {}
+};
+
+// surface triangle DMO (meshes without feature vertices)
+class DMOTriClass : public DMOBaseClass {
+public:
+    DMOTriClass(DMOMeshTri& mesh, QualityCriterium q = QualityCriterium::MEAN_RATIO, float gridScale = 0.5f,
+                int n_iter = 30)
+        : DMOBaseClass(mesh, q, gridScale, n_iter, 0, true) {}
+};
+
+// surface quad DMO (meshes without feature vertices)
+class DMOQuadClass : public DMOBaseClass {
+public:
+    DMOQuadClass(DMOMeshQuad& mesh, QualityCriterium q = QualityCriterium::MEAN_RATIO, float gridScale = 0.5f,
+                 int n_iter = 30)
+        : DMOBaseClass(mesh, q, gridScale, n_iter, 0, true) {}
 };
 
 }  // namespace DMO

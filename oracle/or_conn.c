@@ -687,4 +687,5 @@ int or__fk(const or_mesh* m) { return m->fk; }
 const float* or__vn(const or_mesh* m) { return m->vn; }
 const float* or__fn(const or_mesh* m) { return m->fn; }
 const uint8_t* or__isFeat(const or_mesh* m) { return m->isFeat; }
+const uint8_t* or__isB1(const or_mesh* m) { return m->isB1; }
 int or__type(const or_mesh* m) { return m->type; }

@@ -214,6 +214,159 @@ int or_surface_fit_f64(const or_mesh* m, const double* X, const double* vn, doub
 }
 
 /* ======================================================================================== */
+/* per-sector surfaces of feature vertices (SurfaceFeature.h:79-106, SurfaceFeature.cu:12-221)*/
+/* ======================================================================================== */
+#define TABLE_SIZE 20
+#define MAX_NEIGHBORS 40
+
+/* sector neighbour lists of every feature vertex: nb[s*MAX_NEIGHBORS + i], nnb[s];
+ * returns the number of sectors or -1 (valence beyond the reference's table / list sizes) */
+static int feature_sectors(const or_mesh* m, int32_t* rowptr, int32_t* table, int* nb, int* nnb, int cap) {
+    const int nS = or_mesh_info(m, OR_I_NSURF), nFeat = or_mesh_info(m, OR_I_NFEATURE), nFree = nS - nFeat;
+    const int* rp = or__he_rowptr(m);
+    const int* he = or__he(m);
+    extern const uint8_t* or__isFeat(const or_mesh* m);
+    extern const uint8_t* or__isB1(const or_mesh* m);
+    const uint8_t* isB1 = or__isB1(m);
+    rowptr[0] = 0;
+    for (int idx = 0; idx < nFeat; ++idx) {
+        int vid = nFree + idx, b = rp[vid], e = rp[vid + 1];
+        if (e - b > TABLE_SIZE) return -1;
+        int sid = 0;
+        for (int i = b + 1; i < e; ++i) if (he[4 * i] >= nFree) ++sid;
+        if (!isB1[vid]) ++sid;
+        rowptr[idx + 1] = rowptr[idx] + sid;
+    }
+    if (rowptr[nFeat] > cap) return -1;
+    for (int i = 0; i < nFeat * TABLE_SIZE; ++i) table[i] = -1;
+    for (int idx = 0; idx < nFeat; ++idx) {
+        int vid = nFree + idx, b = rp[vid], e = rp[vid + 1];
+        int sid = 0, nn = 0, last = 1, lastHE = b, vindex = 1;
+        int* T = table + TABLE_SIZE * idx;
+        T[0] = 0;
+        for (int i = b + 1; i < e; ++i) {
+            int vdst = he[4 * i];
+            int* L = nb + MAX_NEIGHBORS * (size_t)(rowptr[idx] + sid);
+            if (last) { nn = 0; L[nn++] = vid; L[nn++] = he[4 * lastHE]; }
+            if (vdst >= nFree) {
+                T[vindex] = sid; L[nn++] = vdst; nnb[rowptr[idx] + sid] = nn; ++sid; nn = 0; last = 1;
+            } else {
+                if (nn >= MAX_NEIGHBORS) return -1;
+                T[vindex] = sid; L[nn++] = vdst; last = 0;
+            }
+            ++lastHE; ++vindex;
+        }
+        if (!isB1[vid]) {
+            int* L = nb + MAX_NEIGHBORS * (size_t)(rowptr[idx] + sid);
+            if (last) { nn = 0; L[nn++] = vid; L[nn++] = he[4 * lastHE]; }
+            L[nn++] = he[4 * b];
+            nnb[rowptr[idx] + sid] = nn;
+        }
+    }
+    return rowptr[nFeat];
+}
+
+/* face normal of the halfedge vid -> target (last match, SurfaceFeature.cu:36-40) */
+static int face_of(const or_mesh* m, int vid, int target) {
+    const int* rp = or__he_rowptr(m);
+    const int* he = or__he(m);
+    int f = -1;
+    for (int i = rp[vid]; i < rp[vid + 1]; ++i) if (he[4 * i] == target) f = he[4 * i + 2];
+    return f;
+}
+
+int or_feature_surfaces_f32(const or_mesh* m, const float* X, const float* fn, int32_t* rowptr, int32_t* table,
+                            float* LS, int cap) {
+    int* nb = (int*)calloc((size_t)(cap > 0 ? cap : 1) * MAX_NEIGHBORS, sizeof(int));
+    int* nnb = (int*)calloc((size_t)(cap > 0 ? cap : 1), sizeof(int));
+    int ns = feature_sectors(m, rowptr, table, nb, nnb, cap);
+    for (int s_ = 0; s_ < ns; ++s_) {
+        const int* L = nb + MAX_NEIGHBORS * (size_t)s_;
+        int np = nnb[s_];
+        const int vid = L[0];
+        const float* c = X + 3 * (size_t)vid;
+        float P[MAX_NEIGHBORS + 1][3];
+        for (int i = 0; i < np; ++i) for (int a = 0; a < 3; ++a) P[i][a] = X[3 * (size_t)L[i] + a];
+        if (np == 5) { for (int a = 0; a < 3; ++a) P[np][a] = 0.5f * (P[2][a] + P[3][a]); np++; }
+        int f = face_of(m, vid, L[1]);
+        float n[3] = { fn[3 * f], fn[3 * f + 1], fn[3 * f + 2] };
+        const float* q0 = X + 3 * (size_t)L[1];
+        float rv[3] = { q0[0] - c[0], q0[1] - c[1], q0[2] - c[2] };
+        float cr[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+        if (sqrtf(dot3f(cr, cr)) < 10.f * EPS) { rv[0] = n[0]; rv[1] = n[2]; rv[2] = -n[1]; }
+        float t1[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+        float t2[3] = { n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0] };
+        float ln = sqrtf(dot3f(n, n)), l1 = sqrtf(dot3f(t1, t1)), l2 = sqrtf(dot3f(t2, t2));
+        for (int a = 0; a < 3; ++a) { n[a] = n[a] / ln; t1[a] = t1[a] / l1; t2[a] = t2[a] / l2; }
+        float M00 = 0.f, M01 = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, r0 = 0.f, r1 = 0.f, r2 = 0.f;
+        for (int i = 0; i < np; ++i) {
+            float p[3] = { P[i][0] - c[0], P[i][1] - c[1], P[i][2] - c[2] };
+            float u = dot3f(t1, p), vv = dot3f(t2, p), w = dot3f(n, p);
+            float uu = u * u, uv = u * vv, v2 = vv * vv;
+            r0 = r0 + uu * w; r1 = r1 + uv * w; r2 = r2 + v2 * w;
+            M00 = M00 + uu * uu; M01 = M01 + uu * uv; M11 = M11 + uu * v2; M12 = M12 + uv * v2; M22 = M22 + v2 * v2;
+        }
+        float A[3][3] = { { M00, M01, M11 }, { M01, M11, M12 }, { M11, M12, M22 } };
+        float sv[3] = { r0, r1, r2 };
+        solve3_f32(A, sv);
+        if (np <= 4) { sv[0] = sv[1] = sv[2] = 0.f; }
+        for (int a = 0; a < 3; ++a) if (sv[a] != sv[a]) sv[a] = 0.f;
+        float* o = LS + LSF * (size_t)s_;
+        o[0] = c[0]; o[1] = c[1]; o[2] = c[2]; o[3] = sv[0];
+        o[4] = t1[0]; o[5] = t1[1]; o[6] = t1[2]; o[7] = sv[1];
+        o[8] = t2[0]; o[9] = t2[1]; o[10] = t2[2]; o[11] = sv[2];
+        o[12] = n[0]; o[13] = n[1]; o[14] = n[2]; o[15] = (float)np;
+    }
+    free(nb); free(nnb);
+    return ns;
+}
+
+int or_feature_surfaces_f64(const or_mesh* m, const double* X, const double* fn, int32_t* rowptr, int32_t* table,
+                            double* LS, int cap) {
+    int* nb = (int*)calloc((size_t)(cap > 0 ? cap : 1) * MAX_NEIGHBORS, sizeof(int));
+    int* nnb = (int*)calloc((size_t)(cap > 0 ? cap : 1), sizeof(int));
+    int ns = feature_sectors(m, rowptr, table, nb, nnb, cap);
+    for (int s_ = 0; s_ < ns; ++s_) {
+        const int* L = nb + MAX_NEIGHBORS * (size_t)s_;
+        int np = nnb[s_];
+        const int vid = L[0];
+        const double* c = X + 3 * (size_t)vid;
+        double P[MAX_NEIGHBORS + 1][3];
+        for (int i = 0; i < np; ++i) for (int a = 0; a < 3; ++a) P[i][a] = X[3 * (size_t)L[i] + a];
+        if (np == 5) { for (int a = 0; a < 3; ++a) P[np][a] = 0.5 * (P[2][a] + P[3][a]); np++; }
+        int f = face_of(m, vid, L[1]);
+        double n[3] = { fn[3 * f], fn[3 * f + 1], fn[3 * f + 2] };
+        const double* q0 = X + 3 * (size_t)L[1];
+        double rv[3] = { q0[0] - c[0], q0[1] - c[1], q0[2] - c[2] };
+        double cr[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+        if (sqrt(dot3d(cr, cr)) < 10.0 * EPS) { rv[0] = n[0]; rv[1] = n[2]; rv[2] = -n[1]; }
+        double t1[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+        double t2[3] = { n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0] };
+        double ln = sqrt(dot3d(n, n)), l1 = sqrt(dot3d(t1, t1)), l2 = sqrt(dot3d(t2, t2));
+        for (int a = 0; a < 3; ++a) { n[a] /= ln; t1[a] /= l1; t2[a] /= l2; }
+        double M[9] = { 0 }, r[3] = { 0 };
+        for (int i = 0; i < np; ++i) {
+            double p[3] = { P[i][0] - c[0], P[i][1] - c[1], P[i][2] - c[2] };
+            double u = dot3d(t1, p), vv = dot3d(t2, p), w = dot3d(n, p);
+            r[0] += u * u * w; r[1] += u * vv * w; r[2] += vv * vv * w;
+            M[0] += u * u * u * u; M[1] += u * u * u * vv; M[4] += u * u * vv * vv; M[2] += u * u * vv * vv;
+            M[5] += u * vv * vv * vv; M[8] += vv * vv * vv * vv;
+        }
+        double A[3][3] = { { M[0], M[1], M[2] }, { M[1], M[4], M[5] }, { M[2], M[5], M[8] } };
+        solve3_f64(A, r);
+        if (np <= 4) { r[0] = r[1] = r[2] = 0.0; }
+        for (int a = 0; a < 3; ++a) if (r[a] != r[a]) r[a] = 0.0;
+        double* o = LS + LSF * (size_t)s_;
+        o[0] = c[0]; o[1] = c[1]; o[2] = c[2]; o[3] = r[0];
+        o[4] = t1[0]; o[5] = t1[1]; o[6] = t1[2]; o[7] = r[1];
+        o[8] = t2[0]; o[9] = t2[1]; o[10] = t2[2]; o[11] = r[2];
+        o[12] = n[0]; o[13] = n[1]; o[14] = n[2]; o[15] = (double)np;
+    }
+    free(nb); free(nnb);
+    return ns;
+}
+
+/* ======================================================================================== */
 /* nearest initial vertex (k_updateNearestNeighbor)                                          */
 /* ======================================================================================== */
 void or_update_nn_f32(const or_mesh* m, const float* X, const float* X0, int32_t* nn) {

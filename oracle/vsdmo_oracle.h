@@ -105,6 +105,13 @@ void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scal
 void or_surface_normals_f32(const or_mesh* m, const float* xyz, float* face_normals, float* vertex_normals);
 int  or_surface_fit_f32(const or_mesh* m, const float* xyz, const float* vertex_normals, float* local_surfaces);
 int  or_surface_fit_f64(const or_mesh* m, const double* xyz, const double* vertex_normals, double* local_surfaces);
+/* per-sector surfaces of feature vertices: rowptr [nFeature+1], table [nFeature*20] (sector of
+ * each halfedge of a feature vertex, -1 unused), local_surfaces [cap*16]; returns the sector
+ * count, -1 when a feature vertex exceeds 20 halfedges / 40 sector points or cap is too small */
+int  or_feature_surfaces_f32(const or_mesh* m, const float* xyz, const float* face_normals, int32_t* rowptr,
+                             int32_t* table, float* local_surfaces, int cap);
+int  or_feature_surfaces_f64(const or_mesh* m, const double* xyz, const double* face_normals, int32_t* rowptr,
+                             int32_t* table, double* local_surfaces, int cap);
 void or_update_nn_f32(const or_mesh* m, const float* xyz, const float* xyz_init, int32_t* nearest);
 void or_update_nn_f64(const or_mesh* m, const double* xyz, const double* xyz_init, int32_t* nearest);
 void or_dmo_surf_f32(const or_mesh* m, float* xyz, const float* xyz_init, const float* local_surfaces,

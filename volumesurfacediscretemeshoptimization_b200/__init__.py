@@ -139,6 +139,12 @@ class DMOMeshTri(_Mesh):
     k = 3
 
 
+class DMOMeshQuad(_Mesh):
+    """``DMOMeshQuad`` (``mesh/DMOMeshQuad.h``): quad surface mesh."""
+    elem_type = _capi.QUAD
+    k = 4
+
+
 class DMOMeshTet(_Mesh):
     """``DMOMeshTet`` (``mesh/DMOMeshTet.h:145-198``)."""
     elem_type = _capi.TET
@@ -151,6 +157,14 @@ class DMOMeshTriFactory:
     @staticmethod
     def create(points, tris, color_seed: int = 1) -> DMOMeshTri:
         return DMOMeshTri(points, tris, color_seed)
+
+
+class DMOMeshQuadFactory:
+    """``DMOMeshQuadFactory::create`` (``mesh/MeshFactory.cu``) from arrays."""
+
+    @staticmethod
+    def create(points, quads, color_seed: int = 1) -> DMOMeshQuad:
+        return DMOMeshQuad(points, quads, color_seed)
 
 
 class DMOMeshTetFactory:
@@ -262,6 +276,16 @@ class _DMOBase:
     def launches_per_iteration(self) -> int:
         return _capi.lib().vsdmo_opt_launches_per_iteration(self.h)
 
+    def surface_state(self):
+        """(xyz_init [nSurf,3], local_surfaces [nSurf,16], nearest [nSurf]) of a surface
+        optimiser, internal vertex numbering."""
+        nS = self.mesh.info["nSurf"]
+        x0 = np.zeros((nS, 3), np.float32)
+        ls = np.zeros((nS, 16), np.float32)
+        nn = np.zeros(nS, np.int32)
+        check(_capi.lib().vsdmo_opt_surface_state(self.h, _ptr(x0), _ptr(ls), _ptr(nn)))
+        return x0, ls, nn
+
 
 class DMOTetClass(_DMOBase):
     """``DMO::DMOTetClass`` (``dmo/DMOTet.h:21-62``)."""
@@ -274,5 +298,12 @@ class DMOTriFlatClass(_DMOBase):
 
 
 class DMOTriClass(_DMOBase):
-    """``DMO::DMOTriClass`` (``dmo/DMOTri.h``): surface triangle DMO."""
+    """``DMO::DMOTriClass`` (``dmo/DMOTri.h``): surface triangle DMO (meshes without feature
+    vertices)."""
+    _flat = 0
+
+
+class DMOQuadClass(_DMOBase):
+    """``DMO::DMOQuadClass`` (``dmo/DMOQuad.h``): surface quad DMO (meshes without feature
+    vertices)."""
     _flat = 0

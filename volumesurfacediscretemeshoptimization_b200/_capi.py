@@ -25,7 +25,8 @@ EXPORTED = [
     "vsdmo_opt_iterate", "vsdmo_opt_restart", "vsdmo_opt_optimize", "vsdmo_opt_is_done", "vsdmo_opt_iterations_done",
     "vsdmo_opt_get_quality", "vsdmo_opt_find_min_quality", "vsdmo_opt_element_qualities",
     "vsdmo_opt_quality_histogram", "vsdmo_opt_display_quality", "vsdmo_opt_history",
-    "vsdmo_opt_run_color", "vsdmo_opt_launches_per_iteration", "vsdmo_quality_reduce_noalloc",
+    "vsdmo_opt_run_color", "vsdmo_opt_launches_per_iteration", "vsdmo_opt_surface_state",
+    "vsdmo_quality_reduce_noalloc",
 ]
 
 
@@ -90,6 +91,7 @@ def lib():
     L.vsdmo_opt_is_done.argtypes = [P]
     L.vsdmo_opt_iterations_done.argtypes = [P]
     L.vsdmo_opt_launches_per_iteration.argtypes = [P]
+    L.vsdmo_opt_surface_state.argtypes = [P, P, P, P]
     L.vsdmo_opt_get_quality.restype = S
     L.vsdmo_opt_get_quality.argtypes = [P, C.POINTER(F)]
     L.vsdmo_opt_find_min_quality.restype = S

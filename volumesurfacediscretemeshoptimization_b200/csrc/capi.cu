@@ -4,6 +4,9 @@
 // per-iteration statistics and a CUDA graph of one doIteration(): every colour launch of the
 // grid search followed by the fused quality / monotonicity kernel (dmo/DMOTet.cu:128-170,
 // dmo/DMOTriFlat.cu:129-166 issue the same steps with a cudaDeviceSynchronize after each).
+// Surface optimisers (dmo/DMOTri.cu:129-165, dmo/DMOQuad.cu:125-162) also own the initial
+// positions, the local surfaces and the nearest-neighbour map, and their iteration adds the
+// nearest-neighbour walk and the normal update after the colour launches.
 #include "vsdmo_internal.cuh"
 #include <cstring>
 #include <cmath>
@@ -18,13 +21,19 @@ struct vsdmo_mesh_s {
     Mesh m;
 };
 
+enum OptMode { MODE_TET = 0, MODE_TRI2D = 1, MODE_SURF = 2 };
+
 struct vsdmo_opt_s {
     vsdmo_mesh_s* mesh = nullptr;
     vsdmo_params p{};
     int iters_done = 0;
     int capacity = 0;
-    bool tet = false;
+    int mode = MODE_TET;
+    int kind = MK_TET;                         // element metric of the quality kernels
     std::vector<std::pair<int, int>> ranges;  // colour classes in launch order
+    DBuf<float4> X0;                           // surface mode: initial surface positions [nSurf]
+    DBuf<float4> LS;                           // local surfaces [4 nSurf]
+    DBuf<int> nn;                              // nearest initial vertex [nSurf]
     DBuf<IterStats> stats;
     DBuf<int> d_iter;
     DBuf<float> pmin;
@@ -91,14 +100,46 @@ void copy_in(void* dst, const void* src, size_t bytes, int mem_space, cudaStream
     VSDMO_CUDA(cudaMemcpyAsync(dst, src, bytes, mem_space == VSDMO_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
 }
 
+void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
+    const Mesh& m = o->mesh->m;
+    DmoLaunch L{o->ranges[c].first, o->ranges[c].second, o->p.grid_scale, o->p.depth};
+    if (o->mode == MODE_TET) launch_dmo_tet(m, L, s);
+    else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
+    else launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, s);
+}
+
 void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
     const Mesh& m = o->mesh->m;
-    for (auto& r : o->ranges) {
-        DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
-        if (o->tet) launch_dmo_tet(m, L, s); else launch_dmo_tri2d(m, L, s);
+    for (int c = 0; c < (int)o->ranges.size(); ++c) launch_color(o, c, s);
+    if (o->mode == MODE_SURF) {
+        launch_update_nn(m, o->X0.p, o->nn.p, s);
+        update_normals(m, s);
     }
-    launch_quality_stats(m, o->p.quality, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p,
+    launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p,
                          o->p.check_monotone ? 1 : 0, s);
+}
+
+__global__ void k_surface_state(const float4* pos, int nS, float4* X0, int* nn) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nS; i += gridDim.x * blockDim.x) {
+        X0[i] = pos[i];
+        nn[i] = i;
+    }
+}
+
+// initial positions, normals, local surfaces and nn = identity from the current positions
+// (the constructor of DMOTriClass / DMOQuadClass, dmo/DMOTri.cu:80-126)
+void init_surface_state(vsdmo_opt_s* o) {
+    const Mesh& m = o->mesh->m;
+    cudaStream_t s = m.stream;
+    if (!o->X0.p) {
+        o->X0.alloc(m.nSurf, s);
+        o->LS.alloc(4L * m.nSurf, s);
+        o->nn.alloc(m.nSurf, s);
+    }
+    k_surface_state<<<grid_for(m.nSurf, 256), 256, 0, s>>>(m.pos.p, m.nSurf, o->X0.p, o->nn.p);
+    VSDMO_CHECK_LAUNCH();
+    update_normals(m, s);
+    launch_surface_fit(m, o->X0.p, o->LS.p, s);
 }
 
 void ensure_capacity(vsdmo_opt_s* o, int need) {
@@ -186,11 +227,10 @@ VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_
     *out = nullptr;
     if (elem_type != VSDMO_TRI && elem_type != VSDMO_TET && elem_type != VSDMO_QUAD && elem_type != VSDMO_HEX)
         return fail(VSDMO_E_ARG, "bad element type");
-    if (elem_type == VSDMO_QUAD || elem_type == VSDMO_HEX)
-        return fail(VSDMO_E_UNSUPPORTED, "quad and hex meshes are not supported yet");
+    if (elem_type == VSDMO_HEX) return fail(VSDMO_E_UNSUPPORTED, "hex meshes are not supported yet");
     if (!xyz || !elems || n_vertices <= 0 || n_elems <= 0) return fail(VSDMO_E_ARG, "empty mesh or null arrays");
     if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
-    const int k = elem_type == VSDMO_TET ? 4 : 3;
+    const int k = elem_type == VSDMO_TRI ? 3 : 4;
     if ((long)n_elems * k > (long)INT32_MAX / 2 || (long)n_vertices * 4 > (long)INT32_MAX)
         return fail(VSDMO_E_ARG, "mesh too large for 32-bit indices");
     std::unique_ptr<vsdmo_mesh_s> h(new vsdmo_mesh_s);
@@ -270,7 +310,7 @@ VSDMO_API long vsdmo_mesh_array_len(vsdmo_mesh_t mesh, int id) {
     case VSDMO_A_XYZ: return 3L * m.nV;
     case VSDMO_A_NEW_OF_OLD: return m.nV;
     case VSDMO_A_ELEMS: return (long)m.nE * m.k;
-    case VSDMO_A_SURF_TRIS: return 3L * m.nTris;
+    case VSDMO_A_SURF_TRIS: return (long)m.fk * m.nTris;
     case VSDMO_A_HE_ROWPTR: return m.he_rowptr.p ? m.nSurf + 1L : 0;
     case VSDMO_A_HALFEDGES: return 4L * m.nHE;
     case VSDMO_A_HF_ROWPTR: return m.hf_rowptr.p ? m.nV + 1L : 0;
@@ -395,14 +435,22 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     if (m.type == VSDMO_TET) {
         if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "surface passes of volume meshes are not implemented yet; set fix_boundary=1");
         if (m.maxTets > dmo_tet_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more tetrahedra than the kernel's ring budget");
-        o->tet = true;
+        o->mode = MODE_TET;
+        o->kind = MK_TET;
         for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
-    } else if (m.type == VSDMO_TRI) {
-        int flat = p.flat < 0 ? m.isFlat : p.flat;
-        if (!flat) return fail(VSDMO_E_UNSUPPORTED, "surface triangle DMO is not implemented yet");
+    } else if (m.type == VSDMO_TRI && (p.flat < 0 ? m.isFlat : p.flat)) {
         if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "sliding boundary vertices are not implemented yet; set fix_boundary=1");
         if (m.maxHE > dmo_tri2d_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
-        o->tet = false;
+        o->mode = MODE_TRI2D;
+        o->kind = MK_TRI2D;
+        for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+    } else if (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) {
+        if (m.nFeature > 0)
+            return fail(VSDMO_E_UNSUPPORTED, "surface meshes with feature or boundary vertices need the feature passes, "
+                                             "which are not implemented yet");
+        if (m.maxHE > dmo_surf_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
+        o->mode = MODE_SURF;
+        o->kind = m.type == VSDMO_QUAD ? MK_QUAD : MK_TRI3D;
         for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
     } else {
         return fail(VSDMO_E_UNSUPPORTED, "element type not supported");
@@ -415,8 +463,9 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->pfail.alloc(quality_stats_blocks(), s);
         o->done.alloc(1, s); o->done.zero();
         prepare_dmo_kernels();
+        if (o->mode == MODE_SURF) init_surface_state(o.get());
         ensure_capacity(o.get(), std::min(std::max(p.n_iter, 1), 4096));
-        launch_quality_stats(m, p.quality, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1, s);
+        launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1, s);
         auto h = read_stats(o.get(), 0, 1);
         o->last_min = h[0].min_q;
     });
@@ -460,7 +509,8 @@ VSDMO_API vsdmo_status vsdmo_opt_restart(vsdmo_opt_t o) {
         const Mesh& m = o->mesh->m;
         o->iters_done = 0;
         o->d_iter.zero();
-        launch_quality_stats(m, o->p.quality, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1,
+        if (o->mode == MODE_SURF) init_surface_state(o);
+        launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1,
                              m.stream);
         auto h = read_stats(o, 0, 1);
         o->last_min = h[0].min_q;
@@ -478,7 +528,33 @@ VSDMO_API int vsdmo_opt_is_done(vsdmo_opt_t o) { return o ? (o->iters_done >= o-
 
 VSDMO_API int vsdmo_opt_iterations_done(vsdmo_opt_t o) { return o ? o->iters_done : -1; }
 
-VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t o) { return o ? (int)o->ranges.size() : -1; }
+VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t o) {
+    if (!o) return -1;
+    // colour launches + quality kernel (+ nearest-neighbour walk and two normal kernels)
+    return (int)o->ranges.size() + 1 + (o->mode == MODE_SURF ? 3 : 0);
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_surface_state(vsdmo_opt_t o, float* xyz_init, float* local_surfaces,
+                                               int32_t* nearest) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    if (o->mode != MODE_SURF) return fail(VSDMO_E_ARG, "not a surface optimiser");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        cudaStream_t s = m.stream;
+        const int nS = m.nSurf;
+        if (xyz_init) {
+            DBuf<float> t(3L * nS, s);
+            k_pack_xyz<<<grid_for(nS, 256), 256, 0, s>>>(o->X0.p, nS, nullptr, t.p);
+            VSDMO_CHECK_LAUNCH();
+            VSDMO_CUDA(cudaMemcpyAsync(xyz_init, t.p, sizeof(float) * 3L * nS, cudaMemcpyDeviceToHost, s));
+            m.sync();
+        }
+        if (local_surfaces)
+            VSDMO_CUDA(cudaMemcpyAsync(local_surfaces, o->LS.p, sizeof(float4) * 4L * nS, cudaMemcpyDeviceToHost, s));
+        if (nearest) VSDMO_CUDA(cudaMemcpyAsync(nearest, o->nn.p, sizeof(int) * nS, cudaMemcpyDeviceToHost, s));
+        m.sync();
+    });
+}
 
 VSDMO_API vsdmo_status vsdmo_opt_get_quality(vsdmo_opt_t o, float* q) {
     if (!o || !q) return fail(VSDMO_E_ARG, "null argument");
@@ -492,11 +568,11 @@ VSDMO_API vsdmo_status vsdmo_opt_element_qualities(vsdmo_opt_t o, float* out, in
         const Mesh& m = o->mesh->m;
         cudaStream_t s = m.stream;
         if (mem_space == VSDMO_DEVICE) {
-            launch_element_qualities(m, o->p.quality, out, s);
+            launch_element_qualities(m, o->kind, out, s);
             m.sync();
         } else {
             DBuf<float> t(m.nE, s);
-            launch_element_qualities(m, o->p.quality, t.p, s);
+            launch_element_qualities(m, o->kind, t.p, s);
             VSDMO_CUDA(cudaMemcpyAsync(out, t.p, sizeof(float) * m.nE, cudaMemcpyDeviceToHost, s));
             m.sync();
         }
@@ -509,7 +585,7 @@ VSDMO_API vsdmo_status vsdmo_opt_find_min_quality(vsdmo_opt_t o, float* min_q, d
     vsdmo_status st = guarded([&] {
         const Mesh& m = o->mesh->m;
         DBuf<float> t(m.nE, m.stream);
-        launch_element_qualities(m, o->p.quality, t.p, m.stream);
+        launch_element_qualities(m, o->kind, t.p, m.stream);
         q = t.to_host();
     });
     if (st != VSDMO_OK) return st;
@@ -527,7 +603,7 @@ VSDMO_API vsdmo_status vsdmo_opt_quality_histogram(vsdmo_opt_t o, int32_t* host_
         const Mesh& m = o->mesh->m;
         DBuf<int> c(n_cols, m.stream);
         c.zero();
-        launch_quality_histogram(m, o->p.quality, c.p, n_cols, m.stream);
+        launch_quality_histogram(m, o->kind, c.p, n_cols, m.stream);
         auto h = c.to_host();
         std::memcpy(host_counts, h.data(), sizeof(int) * n_cols);
     });
@@ -581,11 +657,7 @@ VSDMO_API vsdmo_status vsdmo_opt_history(vsdmo_opt_t o, float* min_q, double* me
 VSDMO_API vsdmo_status vsdmo_opt_run_color(vsdmo_opt_t o, int color) {
     if (!o) return fail(VSDMO_E_ARG, "null optimiser");
     if (color < 0 || color >= (int)o->ranges.size()) return fail(VSDMO_E_ARG, "colour out of range");
-    return guarded([&] {
-        const Mesh& m = o->mesh->m;
-        DmoLaunch L{o->ranges[color].first, o->ranges[color].second, o->p.grid_scale, o->p.depth};
-        if (o->tet) launch_dmo_tet(m, L, m.stream); else launch_dmo_tri2d(m, L, m.stream);
-    });
+    return guarded([&] { launch_color(o, color, o->mesh->m.stream); });
 }
 
 VSDMO_API vsdmo_status vsdmo_quality_reduce_noalloc(int elem_type, int flat, const float* d_xyz, int n_vertices,

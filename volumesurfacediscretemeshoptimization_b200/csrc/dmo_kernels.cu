@@ -363,12 +363,44 @@ __device__ __forceinline__ float q_tri2d(float4 p0, float4 p1, float4 p2) {
     return ((2.f * sqrtf(3.f)) * area) / l;
 }
 
-__device__ __forceinline__ float element_quality(const int* __restrict__ el, int k, const float4* __restrict__ pos, long e) {
-    if (k == 4) {
+// meanRatioMetricTri(p) (dmo/DMOQualityTri.h:260-272), unsigned
+__device__ __forceinline__ float q_tri3d(float4 p0, float4 p1, float4 p2) {
+    const float e0x = p1.x - p0.x, e0y = p1.y - p0.y, e0z = p1.z - p0.z;
+    const float e1x = p2.x - p0.x, e1y = p2.y - p0.y, e1z = p2.z - p0.z;
+    const float e2x = p2.x - p1.x, e2y = p2.y - p1.y, e2z = p2.z - p1.z;
+    const float l = (((e0x * e0x + e0y * e0y) + e0z * e0z) + ((e1x * e1x + e1y * e1y) + e1z * e1z)) +
+                    ((e2x * e2x + e2y * e2y) + e2z * e2z);
+    const float cx = e0y * e1z - e0z * e1y, cy = e0z * e1x - e0x * e1z, cz = e0x * e1y - e0y * e1x;
+    return ((2.f * sqrtf(3.f)) * sqrtf((cx * cx + cy * cy) + cz * cz)) / l;
+}
+
+// meanRatioMetricQuad(p) (dmo/DMOQualityQuad.h:13-28): 2 (A1 + A2) / sum |e|^2
+__device__ __forceinline__ float q_quad(float4 p0, float4 p1, float4 p2, float4 p3) {
+    const float e0x = p1.x - p0.x, e0y = p1.y - p0.y, e0z = p1.z - p0.z;
+    const float e1x = p2.x - p1.x, e1y = p2.y - p1.y, e1z = p2.z - p1.z;
+    const float e2x = p3.x - p2.x, e2y = p3.y - p2.y, e2z = p3.z - p2.z;
+    const float e3x = p0.x - p3.x, e3y = p0.y - p3.y, e3z = p0.z - p3.z;
+    const float l = ((((e0x * e0x + e0y * e0y) + e0z * e0z) + ((e1x * e1x + e1y * e1y) + e1z * e1z)) +
+                     ((e2x * e2x + e2y * e2y) + e2z * e2z)) + ((e3x * e3x + e3y * e3y) + e3z * e3z);
+    const float m0x = -e0x, m0y = -e0y, m0z = -e0z, m2x = -e2x, m2y = -e2y, m2z = -e2z;
+    const float c1x = e1y * m0z - e1z * m0y, c1y = e1z * m0x - e1x * m0z, c1z = e1x * m0y - e1y * m0x;
+    const float c2x = e3y * m2z - e3z * m2y, c2y = e3z * m2x - e3x * m2z, c2z = e3x * m2y - e3y * m2x;
+    const float a1 = sqrtf((c1x * c1x + c1y * c1y) + c1z * c1z);
+    const float a2 = sqrtf((c2x * c2x + c2y * c2y) + c2z * c2z);
+    return (2.f * (a1 + a2)) / l;
+}
+
+__device__ __forceinline__ float element_quality(const int* __restrict__ el, int kind, const float4* __restrict__ pos, long e) {
+    if (kind == MK_TET) {
         const int4 t = reinterpret_cast<const int4*>(el)[e];
         return q_tet(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
     }
+    if (kind == MK_QUAD) {
+        const int4 t = reinterpret_cast<const int4*>(el)[e];
+        return q_quad(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
+    }
     const int* t = el + 3 * e;
+    if (kind == MK_TRI3D) return q_tri3d(pos[t[0]], pos[t[1]], pos[t[2]]);
     return q_tri2d(pos[t[0]], pos[t[1]], pos[t[2]]);
 }
 
@@ -376,7 +408,7 @@ constexpr int QS_BLOCKS = 296;
 constexpr int QS_THREADS = 256;
 
 __global__ void __launch_bounds__(QS_THREADS)
-k_quality_stats(const int* __restrict__ el, int k, long nE, const float4* __restrict__ pos, IterStats* stats,
+k_quality_stats(const int* __restrict__ el, int kind, long nE, const float4* __restrict__ pos, IterStats* stats,
                 int* iter, float* pmin, double* psum, int* pfail, unsigned* done, int check, int init) {
     __shared__ float smin[QS_THREADS / 32];
     __shared__ double ssum[QS_THREADS / 32];
@@ -389,7 +421,7 @@ k_quality_stats(const int* __restrict__ el, int k, long nE, const float4* __rest
     double sm = 0.0;
     int fl = 0;
     for (long e = (long)blockIdx.x * QS_THREADS + threadIdx.x; e < nE; e += (long)QS_BLOCKS * QS_THREADS) {
-        const float q = element_quality(el, k, pos, e);
+        const float q = element_quality(el, kind, pos, e);
         mn = fminf(mn, q);
         sm += (double)q;
         if (check && q < lastMin - tol) ++fl;
@@ -424,15 +456,15 @@ k_quality_stats(const int* __restrict__ el, int k, long nE, const float4* __rest
     }
 }
 
-__global__ void k_element_qualities(const int* __restrict__ el, int k, long nE, const float4* __restrict__ pos, float* out) {
+__global__ void k_element_qualities(const int* __restrict__ el, int kind, long nE, const float4* __restrict__ pos, float* out) {
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nE; e += (long)gridDim.x * blockDim.x)
-        out[e] = element_quality(el, k, pos, e);
+        out[e] = element_quality(el, kind, pos, e);
 }
 
-__global__ void k_quality_histogram(const int* __restrict__ el, int k, long nE, const float4* __restrict__ pos,
+__global__ void k_quality_histogram(const int* __restrict__ el, int kind, long nE, const float4* __restrict__ pos,
                                     int* counts, int n_cols) {
     for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nE; e += (long)gridDim.x * blockDim.x) {
-        float q = fminf(0.9999f, element_quality(el, k, pos, e));
+        float q = fminf(0.9999f, element_quality(el, kind, pos, e));
         int idx = q > 0.f ? (int)(q * n_cols) : 0;  // a negative quality lands in bin 0
         atomicAdd(&counts[idx], 1);
     }
@@ -473,26 +505,23 @@ void launch_dmo_tri2d(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
     VSDMO_CHECK_LAUNCH();
 }
 
-void launch_quality_stats(const Mesh& m, int quality, IterStats* d_stats, int* d_iter, float* d_partial_min,
+void launch_quality_stats(const Mesh& m, int kind, IterStats* d_stats, int* d_iter, float* d_partial_min,
                           double* d_partial_sum, int* d_partial_fail, unsigned* d_done, int check_monotone,
                           cudaStream_t s) {
-    (void)quality;
     // check_monotone < 0 marks the initial evaluation (slot 0, no check, no increment)
     const int init = check_monotone < 0 ? 1 : 0;
-    k_quality_stats<<<QS_BLOCKS, QS_THREADS, 0, s>>>(m.elems.p, m.k, m.nE, m.pos.p, d_stats, d_iter, d_partial_min,
+    k_quality_stats<<<QS_BLOCKS, QS_THREADS, 0, s>>>(m.elems.p, kind, m.nE, m.pos.p, d_stats, d_iter, d_partial_min,
                                                      d_partial_sum, d_partial_fail, d_done, init ? 0 : check_monotone, init);
     VSDMO_CHECK_LAUNCH();
 }
 
-void launch_element_qualities(const Mesh& m, int quality, float* d_out, cudaStream_t s) {
-    (void)quality;
-    k_element_qualities<<<grid_for(m.nE, 256), 256, 0, s>>>(m.elems.p, m.k, m.nE, m.pos.p, d_out);
+void launch_element_qualities(const Mesh& m, int kind, float* d_out, cudaStream_t s) {
+    k_element_qualities<<<grid_for(m.nE, 256), 256, 0, s>>>(m.elems.p, kind, m.nE, m.pos.p, d_out);
     VSDMO_CHECK_LAUNCH();
 }
 
-void launch_quality_histogram(const Mesh& m, int quality, int* d_counts, int n_cols, cudaStream_t s) {
-    (void)quality;
-    k_quality_histogram<<<grid_for(m.nE, 256), 256, 0, s>>>(m.elems.p, m.k, m.nE, m.pos.p, d_counts, n_cols);
+void launch_quality_histogram(const Mesh& m, int kind, int* d_counts, int n_cols, cudaStream_t s) {
+    k_quality_histogram<<<grid_for(m.nE, 256), 256, 0, s>>>(m.elems.p, kind, m.nE, m.pos.p, d_counts, n_cols);
     VSDMO_CHECK_LAUNCH();
 }
 

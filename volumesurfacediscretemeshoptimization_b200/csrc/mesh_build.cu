@@ -1,4 +1,4 @@
-// mesh_build.cu -- connectivity and colouring of tri / tet meshes on the GPU.
+// mesh_build.cu -- connectivity and colouring of tri / quad / tet meshes on the GPU.
 //
 // Produces, bit for bit, the layout the reference's MeshTetGPU::init / MeshTriGPU::init build
 // (mesh/MeshTetGPU.cu:35-42, mesh/MeshTriGPU.cu:37-50):
@@ -9,7 +9,10 @@
 //     through stable partitions and stable colour sorts (mesh/MeshTetGPU.cu:241-295,
 //     mesh/MeshTriGPU.cu:597-671), elements remapped after each step;
 //   * halfedge CSR with boundary dummies, CCW fan order, opposite and next
-//     (mesh/MeshTriGPU.cu:128-214, mesh/MeshGPUCommon.cu:96-135,211-285,565-620);
+//     (mesh/MeshTriGPU.cu:128-214, mesh/MeshGPUCommon.cu:96-135,211-285,565-620); quad meshes
+//     the same with faces of four corners (mesh/MeshQuadGPU.cu), the fan walk stepping to the
+//     corner two after the target (getThirdVertex, mesh/MeshGPUCommon.cu:149-162) and the
+//     colouring adjacency holding both diagonals (:1067-1097);
 //   * halfface CSR, rows in tetrahedron order (mesh/MeshTetGPU.cu:113-142);
 //   * boundary / feature flags (dihedral > 20 deg, mesh/MeshGPUCommon.cu:466-495) and face /
 //     vertex normals (:363-434).
@@ -173,6 +176,22 @@ __global__ void k_tri_edge_pairs(const int* tris, int nTris, int lo, int num, ui
     }
 }
 
+// quad edges and both diagonals
+__global__ void k_quad_edge_pairs(const int* quads, int nQ, int lo, int num, uint32_t* ks, uint32_t* vs, int* counter) {
+    const int E[6][2] = { {0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 2}, {1, 3} };
+    GRID_STRIDE(t, nQ) {
+        const int* v = quads + 4 * t;
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+            int a = v[E[e][0]] - lo, b = v[E[e][1]] - lo;
+            if (a >= 0 && a < num && b >= 0 && b < num) {
+                int p = atomicAdd(counter, 2);
+                ks[p] = a; vs[p] = b; ks[p + 1] = b; vs[p + 1] = a;
+            }
+        }
+    }
+}
+
 __global__ void k_unique_flags(const uint32_t* ks, const uint32_t* vs, long n, uint8_t* f) {
     GRID_STRIDE(i, n) f[i] = (i == 0 || ks[i] != ks[i - 1] || vs[i] != vs[i - 1]) ? 1 : 0;
 }
@@ -202,9 +221,11 @@ __global__ void k_jpl_round(int n, const int* rowptr, const int* col, uint32_t s
 __global__ void k_add_const(int* a, long n, int v) { GRID_STRIDE(i, n) a[i] += v; }
 
 // ---- surface ------------------------------------------------------------------------------------
-__global__ void k_face_normals(const int* tris, int nTris, const float4* pos, float* fn, int* err) {
+// face normal from corners 0, 1 and 2 (triangles) or 0, 1 and 3 (quads)
+__global__ void k_face_normals(const int* tris, int fk, int nTris, const float4* pos, float* fn, int* err) {
     GRID_STRIDE(t, nTris) {
-        float4 p0 = pos[tris[3 * t]], p1 = pos[tris[3 * t + 1]], p2 = pos[tris[3 * t + 2]];
+        const int* f = tris + (long)fk * t;
+        float4 p0 = pos[f[0]], p1 = pos[f[1]], p2 = pos[f[fk == 4 ? 3 : 2]];
         float e0x = p1.x - p0.x, e0y = p1.y - p0.y, e0z = p1.z - p0.z;
         float e1x = p2.x - p0.x, e1y = p2.y - p0.y, e1z = p2.z - p0.z;
         if (err) {
@@ -218,11 +239,11 @@ __global__ void k_face_normals(const int* tris, int nTris, const float4* pos, fl
     }
 }
 
-// first-pass halfedges from the sorted (src, 3t+j) pairs
-__global__ void k_he_records(const uint32_t* order, long nHE, const int* tris, int4* he) {
+// first-pass halfedges from the sorted (src, fk*t+j) pairs
+__global__ void k_he_records(const uint32_t* order, long nHE, const int* tris, int fk, int4* he) {
     GRID_STRIDE(i, nHE) {
-        int e = (int)order[i], t = e / 3, j = e % 3;
-        he[i] = make_int4(tris[3 * t + (j + 1) % 3], -1, t, 0);
+        int e = (int)order[i], t = e / fk, j = e % fk;
+        he[i] = make_int4(tris[(long)fk * t + (j + 1) % fk], -1, t, 0);
     }
 }
 
@@ -276,8 +297,16 @@ __device__ __forceinline__ int third_vertex(const int* t, int src, int dst) {
     return t[2];
 }
 
+// the corner two after dst (getThirdVertex for quads)
+__device__ __forceinline__ int third_vertex_quad(const int* q, int dst) {
+    if (dst == q[1]) return q[3];
+    if (dst == q[2]) return q[0];
+    if (dst == q[3]) return q[1];
+    return q[2];
+}
+
 __global__ void k_ccw(int nS, const int* rowptr, const int4* in, int4* out, const uint8_t* isB1, const uint8_t* isFeat,
-                      const int* tris, int* err) {
+                      const int* tris, int fk, int* err) {
     GRID_STRIDE(src, nS) {
         const int start = rowptr[src], n = rowptr[src + 1] - start;
         if (n == 0) { atomicMax(err, BE_FAN); continue; }
@@ -308,7 +337,8 @@ __global__ void k_ccw(int nS, const int* rowptr, const int4* in, int4* out, cons
         do {
             int currDst = h.x, currTri = h.z;
             if (currTri == -1) { bad = true; break; }
-            int nextVert = third_vertex(tris + 3 * (long)currTri, (int)src, currDst);
+            int nextVert = fk == 4 ? third_vertex_quad(tris + 4 * (long)currTri, currDst)
+                                   : third_vertex(tris + 3 * (long)currTri, (int)src, currDst);
             found = false;
             for (int j = 0; j < n; ++j) {
                 int4 t = in[start + j];
@@ -493,10 +523,10 @@ struct Builder {
 
     void surface_init() {
         const int nS = m.nSurf;
-        const long nHE1 = 3L * m.nTris;
+        const long nHE1 = (long)m.fk * m.nTris;
         m.fn.alloc(3L * m.nTris, s);
         err.zero();
-        k_face_normals<<<G(m.nTris), 256, 0, s>>>(m.tris.p, m.nTris, m.pos.p, m.fn.p, err.p);
+        k_face_normals<<<G(m.nTris), 256, 0, s>>>(m.tris.p, m.fk, m.nTris, m.pos.p, m.fn.p, err.p);
         VSDMO_CHECK_LAUNCH();
         check_err(err, s, "surface");
         // first-pass halfedges
@@ -509,7 +539,7 @@ struct Builder {
             DBuf<int> rowptr(nS + 1, s);
             rowptr_from_sorted(keys.p, nHE1, nS, rowptr.p, s);
             DBuf<int4> he(nHE1, s);
-            k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, he.p);
+            k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, m.fk, he.p);
             VSDMO_CHECK_LAUNCH();
             k_opposite<<<G(nHE1), 256, 0, s>>>(keys.p, he.p, nHE1, rowptr.p);
             VSDMO_CHECK_LAUNCH();
@@ -526,7 +556,7 @@ struct Builder {
         {
             DBuf<int> order;
             int nFree = stable_partition(m.isFeat.p, nS, 0, order);
-            std::vector<std::pair<int*, long>> el = { {m.tris.p, 3L * m.nTris} };
+            std::vector<std::pair<int*, long>> el = { {m.tris.p, (long)m.fk * m.nTris} };
             if (m.type == VSDMO_TET) el.push_back({m.elems.p, 4L * m.nE});
             permute_range(order.p, 0, nS, {&m.isB1, &m.isFeat}, el, nS);
             m.nFeature = nS - nFree;
@@ -544,17 +574,19 @@ struct Builder {
                 nc = 0;
                 continue;
             }
-            long cap = m.type == VSDMO_TET ? 12L * m.nE : 6L * m.nTris;
+            long cap = m.type == VSDMO_TET ? 12L * m.nE : (m.fk == 4 ? 12L : 6L) * m.nTris;
             DBuf<uint32_t> ks(cap, s), vs(cap, s);
             DBuf<int> cnt(1, s);
             cnt.zero();
             if (m.type == VSDMO_TET)
                 k_tet_edge_pairs<<<G(m.nE), 256, 0, s>>>(m.elems.p, m.nE, lo, num, ks.p, vs.p, cnt.p);
+            else if (m.fk == 4)
+                k_quad_edge_pairs<<<G(m.nTris), 256, 0, s>>>(m.tris.p, m.nTris, lo, num, ks.p, vs.p, cnt.p);
             else
                 k_tri_edge_pairs<<<G(m.nTris), 256, 0, s>>>(m.tris.p, m.nTris, lo, num, ks.p, vs.p, cnt.p);
             VSDMO_CHECK_LAUNCH();
             int np = read_scalar(cnt.p, s);
-            std::vector<std::pair<int*, long>> el = { {m.tris.p, 3L * m.nTris} };
+            std::vector<std::pair<int*, long>> el = { {m.tris.p, (long)m.fk * m.nTris} };
             if (m.type == VSDMO_TET) el.push_back({m.elems.p, 4L * m.nE});
             nc = color_range(lo, num, ks, vs, np, oh, od, {&m.isB1, &m.isFeat}, el);
         }
@@ -566,7 +598,7 @@ struct Builder {
 
     void final_halfedges() {
         const int nS = m.nSurf;
-        const long nHE1 = 3L * m.nTris;
+        const long nHE1 = (long)m.fk * m.nTris;
         DBuf<uint32_t> keys(nHE1, s), order(nHE1, s);
         VSDMO_CUDA(cudaMemcpyAsync(keys.p, m.tris.p, sizeof(int) * nHE1, cudaMemcpyDeviceToDevice, s));
         k_iota<<<G(nHE1), 256, 0, s>>>(order.p, nHE1);
@@ -576,7 +608,7 @@ struct Builder {
         DBuf<int> rowptr1(nS + 1, s);
         rowptr_from_sorted(keys.p, nHE1, nS, rowptr1.p, s);
         DBuf<int4> he1(nHE1, s);
-        k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, he1.p);
+        k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, m.fk, he1.p);
         VSDMO_CHECK_LAUNCH();
         k_opposite<<<G(nHE1), 256, 0, s>>>(keys.p, he1.p, nHE1, rowptr1.p);
         VSDMO_CHECK_LAUNCH();
@@ -602,7 +634,7 @@ struct Builder {
         VSDMO_CHECK_LAUNCH();
         m.he.alloc(nHE, s);
         err.zero();
-        k_ccw<<<G(nS), 256, 0, s>>>(nS, m.he_rowptr.p, in.p, m.he.p, m.isB1.p, m.isFeat.p, m.tris.p, err.p);
+        k_ccw<<<G(nS), 256, 0, s>>>(nS, m.he_rowptr.p, in.p, m.he.p, m.isB1.p, m.isFeat.p, m.tris.p, m.fk, err.p);
         VSDMO_CHECK_LAUNCH();
         check_err(err, s, "halfedges");
         k_opp_next<<<G(nS), 256, 0, s>>>(nS, m.he_rowptr.p, m.he.p);
@@ -687,18 +719,20 @@ struct Builder {
         orig_of_cur.alloc(m.nV, s);
         k_iota<<<G(m.nV), 256, 0, s>>>((uint32_t*)orig_of_cur.p, m.nV);
         VSDMO_CHECK_LAUNCH();
-        if (m.type == VSDMO_TRI) {
+        if (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) {
+            m.fk = m.k;
             m.isFlat = read_scalar(nz.p, s) ? 0 : 1;
             m.nSurf = m.nV;
             m.nTris = m.nE;
-            m.tris.alloc(3L * m.nE, s);
-            VSDMO_CUDA(cudaMemcpyAsync(m.tris.p, m.elems.p, sizeof(int) * 3L * m.nE, cudaMemcpyDeviceToDevice, s));
+            m.tris.alloc(nIdx, s);
+            VSDMO_CUDA(cudaMemcpyAsync(m.tris.p, m.elems.p, sizeof(int) * nIdx, cudaMemcpyDeviceToDevice, s));
             m.col_inner.assign(1, m.nV);
             m.d_col_inner.alloc(1, s);
             VSDMO_CUDA(cudaMemcpyAsync(m.d_col_inner.p, m.col_inner.data(), sizeof(int), cudaMemcpyHostToDevice, s));
             surface_init();
-            VSDMO_CUDA(cudaMemcpyAsync(m.elems.p, m.tris.p, sizeof(int) * 3L * m.nE, cudaMemcpyDeviceToDevice, s));
+            VSDMO_CUDA(cudaMemcpyAsync(m.elems.p, m.tris.p, sizeof(int) * nIdx, cudaMemcpyDeviceToDevice, s));
         } else if (m.type == VSDMO_TET) {
+            m.fk = 3;
             m.isFlat = 0;
             tet_boundary();
             {
@@ -726,7 +760,7 @@ struct Builder {
             if (m.nSurf > 0) surface_init();
             tet_halffaces();
         } else {
-            throw Error(VSDMO_E_UNSUPPORTED, "quad and hex meshes are not supported yet");
+            throw Error(VSDMO_E_UNSUPPORTED, "hex meshes are not supported yet");
         }
         m.new_of_old.alloc(m.nV, s);
         k_final_perm<<<G(m.nV), 256, 0, s>>>(orig_of_cur.p, m.nV, m.new_of_old.p);
@@ -742,11 +776,11 @@ void build_mesh(Mesh& m, const float* d_xyz, const int* d_elems) {
     b.run(d_xyz, d_elems);
 }
 
-void update_normals(Mesh& m) {
+void update_normals(const Mesh& m, cudaStream_t s) {
     if (m.nTris <= 0 || m.nSurf <= 0) return;
-    k_face_normals<<<G(m.nTris), 256, 0, m.stream>>>(m.tris.p, m.nTris, m.pos.p, m.fn.p, nullptr);
+    k_face_normals<<<G(m.nTris), 256, 0, s>>>(m.tris.p, m.fk, m.nTris, m.pos.p, m.fn.p, nullptr);
     VSDMO_CHECK_LAUNCH();
-    k_vertex_normals<<<G(m.nSurf), 256, 0, m.stream>>>(m.nSurf, m.he_rowptr.p, m.he.p, m.fn.p, m.vn.p);
+    k_vertex_normals<<<G(m.nSurf), 256, 0, s>>>(m.nSurf, m.he_rowptr.p, m.he.p, m.fn.p, m.vn.p);
     VSDMO_CHECK_LAUNCH();
 }
 

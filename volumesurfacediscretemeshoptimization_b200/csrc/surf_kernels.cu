@@ -1,0 +1,386 @@
+// surf_kernels.cu -- surface DMO of triangle and quad meshes (free surface vertices).
+//
+// Per optimiser the state of the reference's DMOTriClass / DMOQuadClass (dmo/DMOTri.cu:80-126,
+// dmo/DMOQuad.cu:78-123): the initial positions X0, one local quadric surface per surface
+// vertex fitted to them, and for every vertex the nearest initial vertex nn[v] whose surface
+// is used for it. Kernels:
+//
+//   k_surface_fit   computeLocalCoordinates + computeLocalSurface1/2 (dmo/surfaceP/Surface.h:66-93,
+//                   Surface.cu:11-104): frame t1 = n x (q0 - p), t2 = n x t1, least squares
+//                   quadric w = a u^2 + b uv + c v^2 over the centre and its 1-ring (plus the
+//                   midpoint of neighbours 1 and 2 for valence 4); the 3x3 normal equations are
+//                   solved by LU with partial pivoting in registers (the reference calls the
+//                   batched cuBLAS getrf/getrs; the published algorithm is restated here).
+//   k_update_nn     k_updateNearestNeighbor (dmo/DMOCommon.cu:11-42): greedy walk over the
+//                   initial positions to the initial vertex nearest to the current position.
+//   k_dmo_surf<FK>  k_optimizeHierarchical2D (dmo/DMOTriImplCub.h:26-201 for FK = 3,
+//                   dmo/DMOQuadImplCub.h:24-209 for FK = 4): 8 x 8 grid in the (u, v) frame of
+//                   the surface of nn[v], each candidate projected by the inverse-distance blend
+//                   over the 1-ring surfaces (localSurfaceEstimationWithFeature,
+//                   dmo/SurfaceEstimation.h:122-197), three levels, the normal-signed mean ratio
+//                   of the ring (meanRatioMetricTri(p, n), dmo/DMOQualityTri.h:276-293;
+//                   meanRatioMetricQuad(p, n), dmo/DMOQualityQuad.h:30-50).
+//
+// Layout: one warp per vertex. The lanes stage the ring positions, the neighbours' surfaces
+// (64 B each) and their nearest initial positions in shared memory; lane t evaluates the
+// candidates (i, j) = (t >> 3, t & 7) and (i + 4, j) of the reference's 32-thread block and
+// keeps the better one. The winning lane is the first maximum in lane order (a scan of the 32
+// values, which is what the reference's cub::BlockReduce ArgMax gives).
+//
+// Arithmetic: the triangle ring minimum is compared as the fraction sign |n_t|^2 / L^2
+// (monotone in the reference's 2 sqrt3 sign |n_t| / L), without its square root and division
+// per element; the quad metric is the reference formula. Projections and blends use a fixed
+// operation order, reproduced by the oracle's f32 mirror bit for bit (built with
+// --fmad=false here and without contraction there).
+#include "vsdmo_internal.cuh"
+#include <cfloat>
+
+namespace vsdmo {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int SURF_WARPS = 4;
+constexpr int SURF_MAX_RING = 64;
+constexpr float SURF_EPS = 1.19209e-07f;   // EPSILON of the reference's surface code
+
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return (ax * bx + ay * by) + az * bz;
+}
+
+// ---- quadric fit ----------------------------------------------------------------------------
+// LU with partial pivoting of a 3 x 3 system (row-major A), solution returned in b
+__device__ void solve3(float A[3][3], float b[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int p = k;
+#pragma unroll
+        for (int i = k + 1; i < 3; ++i) if (fabsf(A[i][k]) > fabsf(A[p][k])) p = i;
+        if (p != k) {
+#pragma unroll
+            for (int j = 0; j < 3; ++j) { float t = A[k][j]; A[k][j] = A[p][j]; A[p][j] = t; }
+            float t = b[k]; b[k] = b[p]; b[p] = t;
+        }
+#pragma unroll
+        for (int i = k + 1; i < 3; ++i) {
+            const float f = A[i][k] / A[k][k];
+#pragma unroll
+            for (int j = k + 1; j < 3; ++j) A[i][j] = A[i][j] - f * A[k][j];
+            b[i] = b[i] - f * b[k];
+        }
+    }
+    b[2] = b[2] / A[2][2];
+    b[1] = (b[1] - A[1][2] * b[2]) / A[1][1];
+    b[0] = ((b[0] - A[0][1] * b[1]) - A[0][2] * b[2]) / A[0][0];
+}
+
+// LS[4v + 0..3] = (p0, a), (t1, b), (t2, c), (n, numPoints)
+__global__ void k_surface_fit(int nS, const int* __restrict__ rowptr, const int4* __restrict__ he,
+                              const float4* __restrict__ pos, const float* __restrict__ vn, float4* __restrict__ LS) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nS; v += gridDim.x * blockDim.x) {
+        const float4 c = pos[v];
+        const int b = rowptr[v], k = rowptr[v + 1] - b;
+        const int nb = k < 62 ? k : 62;            // the reference keeps at most 63 points
+        const int np = 1 + nb + (1 + nb == 5 ? 1 : 0);
+        float n[3] = { vn[3 * v], vn[3 * v + 1], vn[3 * v + 2] };
+        const float4 q0 = pos[he[b].x];
+        float rv[3] = { q0.x - c.x, q0.y - c.y, q0.z - c.z };
+        float cr[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+        if (sqrtf(dot3(cr[0], cr[1], cr[2], cr[0], cr[1], cr[2])) < 10.f * SURF_EPS) {
+            rv[0] = n[0]; rv[1] = n[2]; rv[2] = -n[1];
+        }
+        float t1[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+        float t2[3] = { n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0] };
+        const float ln = sqrtf(dot3(n[0], n[1], n[2], n[0], n[1], n[2]));
+        const float l1 = sqrtf(dot3(t1[0], t1[1], t1[2], t1[0], t1[1], t1[2]));
+        const float l2 = sqrtf(dot3(t2[0], t2[1], t2[2], t2[0], t2[1], t2[2]));
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { n[a] = n[a] / ln; t1[a] = t1[a] / l1; t2[a] = t2[a] / l2; }
+        float M00 = 0.f, M01 = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, r0 = 0.f, r1 = 0.f, r2 = 0.f;
+        for (int i = 0; i < np; ++i) {
+            float px, py, pz;
+            if (i == 0) {
+                px = c.x; py = c.y; pz = c.z;
+            } else if (i <= nb) {
+                const float4 q = pos[he[b + i - 1].x];
+                px = q.x; py = q.y; pz = q.z;
+            } else {  // valence 4: midpoint of points 2 and 3 (neighbours 1 and 2)
+                const float4 qa = pos[he[b + 1].x], qb = pos[he[b + 2].x];
+                px = 0.5f * (qa.x + qb.x); py = 0.5f * (qa.y + qb.y); pz = 0.5f * (qa.z + qb.z);
+            }
+            const float dx = px - c.x, dy = py - c.y, dz = pz - c.z;
+            const float u = dot3(t1[0], t1[1], t1[2], dx, dy, dz);
+            const float w2 = dot3(t2[0], t2[1], t2[2], dx, dy, dz);
+            const float w = dot3(n[0], n[1], n[2], dx, dy, dz);
+            const float uu = u * u, uv = u * w2, v2 = w2 * w2;
+            r0 = r0 + uu * w; r1 = r1 + uv * w; r2 = r2 + v2 * w;
+            M00 = M00 + uu * uu; M01 = M01 + uu * uv; M11 = M11 + uu * v2; M12 = M12 + uv * v2; M22 = M22 + v2 * v2;
+        }
+        float A[3][3] = { { M00, M01, M11 }, { M01, M11, M12 }, { M11, M12, M22 } };
+        float s[3] = { r0, r1, r2 };
+        solve3(A, s);
+        if (np <= 4) { s[0] = 0.f; s[1] = 0.f; s[2] = 0.f; }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) if (s[a] != s[a]) s[a] = 0.f;
+        LS[4L * v + 0] = make_float4(c.x, c.y, c.z, s[0]);
+        LS[4L * v + 1] = make_float4(t1[0], t1[1], t1[2], s[1]);
+        LS[4L * v + 2] = make_float4(t2[0], t2[1], t2[2], s[2]);
+        LS[4L * v + 3] = make_float4(n[0], n[1], n[2], (float)np);
+    }
+}
+
+// ---- nearest initial vertex -------------------------------------------------------------------
+__global__ void k_update_nn(int nS, int nFree, const int* __restrict__ rowptr, const int4* __restrict__ he,
+                            const float4* __restrict__ pos, const float4* __restrict__ X0, int* __restrict__ nn) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nS; v += gridDim.x * blockDim.x) {
+        const float4 p = pos[v];
+        int vh = nn[v];
+        const float4 pi = X0[vh];
+        float sd = dot3(p.x - pi.x, p.y - pi.y, p.z - pi.z, p.x - pi.x, p.y - pi.y, p.z - pi.z);
+        const bool fv = v >= nFree;
+        int vnew;
+        // every step strictly lowers the distance, so the walk visits at most nS vertices
+        int steps = 0;
+        do {
+            vnew = vh;
+            for (int i = rowptr[vnew]; i < rowptr[vnew + 1]; ++i) {
+                const int d = he[i].x;
+                if (fv != (d >= nFree)) continue;
+                const float4 q = X0[d];
+                const float ex = p.x - q.x, ey = p.y - q.y, ez = p.z - q.z;
+                const float s2 = dot3(ex, ey, ez, ex, ey, ez);
+                if (s2 < sd) { sd = s2; vh = d; }
+            }
+        } while (vnew != vh && ++steps <= nS);
+        nn[v] = vnew;
+    }
+}
+
+// ---- grid search --------------------------------------------------------------------------------
+struct Surf {
+    float4 l0, l1, l2, l3;   // (p0, a), (t1, b), (t2, c), (n, numPoints)
+};
+
+__device__ __forceinline__ float poly(const float4& l0, const float4& l1, const float4& l2, float u, float v) {
+    return (((l0.w * u) * u) + ((l1.w * u) * v)) + ((l2.w * v) * v);
+}
+
+// blended projection of (u, v) of the vertex's own surface onto the ring's surfaces
+__device__ __forceinline__ float3 estimate(const Surf& L, const float4 x0, const float4* __restrict__ nbL,
+                                           const float4* __restrict__ nbX, int k, float u, float v) {
+    const float w = poly(L.l0, L.l1, L.l2, u, v);
+    const float pwx = ((L.l0.x + u * L.l1.x) + v * L.l2.x) + w * L.l3.x;
+    const float pwy = ((L.l0.y + u * L.l1.y) + v * L.l2.y) + w * L.l3.y;
+    const float pwz = ((L.l0.z + u * L.l1.z) + v * L.l2.z) + w * L.l3.z;
+    const float dx = x0.x - pwx, dy = x0.y - pwy, dz = x0.z - pwz;
+    const float id = 1.0f / (dot3(dx, dy, dz, dx, dy, dz) + SURF_EPS);
+    float isum = id;
+    float ax = pwx * id, ay = pwy * id, az = pwz * id;
+    for (int i = 0; i < k; ++i) {
+        const float4 xn = nbX[i];
+        const float ex = xn.x - pwx, ey = xn.y - pwy, ez = xn.z - pwz;
+        const float idn = 1.0f / (dot3(ex, ey, ez, ex, ey, ez) + SURF_EPS);
+        isum = isum + idn;
+        const float4 m0 = nbL[4 * i], m1 = nbL[4 * i + 1], m2 = nbL[4 * i + 2], m3 = nbL[4 * i + 3];
+        const float qx = pwx - m0.x, qy = pwy - m0.y, qz = pwz - m0.z;
+        const float lu = dot3(qx, qy, qz, m1.x, m1.y, m1.z);
+        const float lv = dot3(qx, qy, qz, m2.x, m2.y, m2.z);
+        const float lw = poly(m0, m1, m2, lu, lv);
+        const float p2x = ((m0.x + lu * m1.x) + lv * m2.x) + lw * m3.x;
+        const float p2y = ((m0.y + lu * m1.y) + lv * m2.y) + lw * m3.y;
+        const float p2z = ((m0.z + lu * m1.z) + lv * m2.z) + lw * m3.z;
+        ax = ax + p2x * idn; ay = ay + p2y * idn; az = az + p2z * idn;
+    }
+    const float inv = 1.0f / isum;
+    return make_float3(ax * inv, ay * inv, az * inv);
+}
+
+// ring key of a triangle fan: min over the fan of sign(n_t . n) |n_t|^2 / L^2 (unsigned without n)
+template <bool SIGNED>
+__device__ __forceinline__ float ring_key_tri(const float4* __restrict__ ring, int k, float px, float py, float pz,
+                                              float3 n) {
+    float N = 0.f, D = 1.f;
+    for (int i = 0; i < k; ++i) {
+        const float4 a = ring[i], b = ring[i + 1];
+        const float e0x = a.x - px, e0y = a.y - py, e0z = a.z - pz;
+        const float e1x = b.x - px, e1y = b.y - py, e1z = b.z - pz;
+        const float e2x = b.x - a.x, e2y = b.y - a.y, e2z = b.z - a.z;
+        const float l = (dot3(e0x, e0y, e0z, e0x, e0y, e0z) + dot3(e1x, e1y, e1z, e1x, e1y, e1z)) +
+                        dot3(e2x, e2y, e2z, e2x, e2y, e2z);
+        const float nx = e0y * e1z - e0z * e1y, ny = e0z * e1x - e0x * e1z, nz = e0x * e1y - e0y * e1x;
+        const float a2 = dot3(nx, ny, nz, nx, ny, nz);
+        float num = a2;
+        if (SIGNED) {
+            const float dn = dot3(nx, ny, nz, n.x, n.y, n.z);
+            num = dn > 0.f ? a2 : (dn < 0.f ? -a2 : 0.f);
+        }
+        const float den = l * l;
+        if (i == 0) { N = num; D = den; continue; }
+        if (num * D < N * den) { N = num; D = den; }
+    }
+    return N / D;
+}
+
+// meanRatioMetricQuad(p, n) / (p): 2 (A1 + A2) / sum |e|^2, -1 when a corner normal leaves n
+template <bool SIGNED>
+__device__ __forceinline__ float quad_metric(float p0x, float p0y, float p0z, float4 p1, float4 p2, float4 p3, float3 n) {
+    const float e0x = p1.x - p0x, e0y = p1.y - p0y, e0z = p1.z - p0z;
+    const float e1x = p2.x - p1.x, e1y = p2.y - p1.y, e1z = p2.z - p1.z;
+    const float e2x = p3.x - p2.x, e2y = p3.y - p2.y, e2z = p3.z - p2.z;
+    const float e3x = p0x - p3.x, e3y = p0y - p3.y, e3z = p0z - p3.z;
+    const float l = ((dot3(e0x, e0y, e0z, e0x, e0y, e0z) + dot3(e1x, e1y, e1z, e1x, e1y, e1z)) +
+                     dot3(e2x, e2y, e2z, e2x, e2y, e2z)) + dot3(e3x, e3y, e3z, e3x, e3y, e3z);
+    const float m0x = -e0x, m0y = -e0y, m0z = -e0z, m2x = -e2x, m2y = -e2y, m2z = -e2z;
+    const float c1x = e1y * m0z - e1z * m0y, c1y = e1z * m0x - e1x * m0z, c1z = e1x * m0y - e1y * m0x;
+    const float c2x = e3y * m2z - e3z * m2y, c2y = e3z * m2x - e3x * m2z, c2z = e3x * m2y - e3y * m2x;
+    const float a1 = sqrtf(dot3(c1x, c1y, c1z, c1x, c1y, c1z));
+    const float a2 = sqrtf(dot3(c2x, c2y, c2z, c2x, c2y, c2z));
+    if (SIGNED) {
+        const float d1 = dot3(c1x, c1y, c1z, n.x, n.y, n.z) / a1;
+        const float d2 = dot3(c2x, c2y, c2z, n.x, n.y, n.z) / a2;
+        if (d1 < 0.7f || d2 < 0.7f) return -1.f;
+    }
+    return (2.f * (a1 + a2)) / l;
+}
+
+template <bool SIGNED>
+__device__ __forceinline__ float ring_key_quad(const float4* __restrict__ ring, int k, float px, float py, float pz,
+                                               float3 n) {
+    float q = 0.f;
+    for (int i = 0; i < k; ++i) {
+        const float v = quad_metric<SIGNED>(px, py, pz, ring[2 * i], ring[2 * i + 1], ring[2 * i + 2], n);
+        q = i == 0 ? v : fminf(q, v);
+    }
+    return q;
+}
+
+template <int FK, bool SIGNED>
+__device__ __forceinline__ float ring_key(const float4* ring, int k, float px, float py, float pz, float3 n) {
+    if (FK == 3) return ring_key_tri<SIGNED>(ring, k, px, py, pz, n);
+    return ring_key_quad<SIGNED>(ring, k, px, py, pz, n);
+}
+
+// shared memory per warp, in float4: ring [2 maxk + 1], neighbour surfaces [4 maxk], X0 [maxk]
+__host__ __device__ constexpr int surf_warp_f4(int maxk) { return 7 * maxk + 1; }
+
+template <int FK>
+__global__ void __launch_bounds__(SURF_WARPS * 32)
+k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
+           const float4* __restrict__ X0, const float4* __restrict__ LS, const int* __restrict__ nn,
+           const float* __restrict__ vn, int v0, int v1, float grid_scale, int depth, int maxk) {
+    extern __shared__ float4 smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int v = v0 + blockIdx.x * SURF_WARPS + warp;
+    if (v >= v1) return;
+    const int b = rowptr[v], k = rowptr[v + 1] - b;
+    if (k <= 0 || k > maxk) return;   // maxk is the mesh's largest row, checked on the host
+    float4* ring = smem + (size_t)warp * surf_warp_f4(maxk);
+    float4* nbL = ring + 2 * maxk + 1;
+    float4* nbX = nbL + 4 * maxk;
+    const float4 c0 = pos[v];
+    float md = 0.f;
+    for (int i = lane; i < k; i += 32) {
+        const int4 h = he[b + i];
+        const float4 t = pos[h.x];
+        float dx = t.x - c0.x, dy = t.y - c0.y, dz = t.z - c0.z;
+        md = fmaxf(md, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+        if (FK == 3) {
+            ring[i] = t;
+        } else {
+            const float4 t2 = pos[he[h.w].x];
+            ring[2 * i] = t;
+            ring[2 * i + 1] = t2;
+            dx = t2.x - c0.x; dy = t2.y - c0.y; dz = t2.z - c0.z;
+            md = fmaxf(md, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+        }
+        const int nnN = nn[h.x];
+        nbL[4 * i] = LS[4L * nnN];
+        nbL[4 * i + 1] = LS[4L * nnN + 1];
+        nbL[4 * i + 2] = LS[4L * nnN + 2];
+        nbL[4 * i + 3] = LS[4L * nnN + 3];
+        nbX[i] = X0[nnN];
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) md = fmaxf(md, __shfl_xor_sync(FULL, md, o));
+    __syncwarp();
+    if (lane == 0) ring[FK == 3 ? k : 2 * k] = ring[0];
+    __syncwarp();
+
+    const int nnv = nn[v];
+    Surf L;
+    L.l0 = LS[4L * nnv]; L.l1 = LS[4L * nnv + 1]; L.l2 = LS[4L * nnv + 2]; L.l3 = LS[4L * nnv + 3];
+    const float4 x0 = X0[nnv];
+    const float3 n = make_float3(vn[3L * nnv], vn[3L * nnv + 1], vn[3L * nnv + 2]);
+    float cu, cv;
+    {
+        const float dx = c0.x - L.l0.x, dy = c0.y - L.l0.y, dz = c0.z - L.l0.z;
+        cu = dot3(dx, dy, dz, L.l1.x, L.l1.y, L.l1.z);
+        cv = dot3(dx, dy, dz, L.l2.x, L.l2.y, L.l2.z);
+    }
+    float qLast = ring_key<FK, true>(ring, k, c0.x, c0.y, c0.z, n);
+    const float qOld = ring_key<FK, false>(ring, k, c0.x, c0.y, c0.z, n);
+
+    const int i1 = lane >> 3, j1 = lane & 7, i2 = i1 + 4;
+    const float o1 = (float)(7 - 2 * i1) / 7.f, oj = (float)(7 - 2 * j1) / 7.f, o2 = (float)(7 - 2 * i2) / 7.f;
+    float cx = c0.x, cy = c0.y, cz = c0.z;
+    float ds = grid_scale, lastMax = -FLT_MAX;
+    for (int d = 0; d < depth; ++d) {
+        const float S = ds * md;
+        const float u1 = fmaf(o1, S, cu), vv = fmaf(oj, S, cv), u2 = fmaf(o2, S, cu);
+        const float3 p1 = estimate(L, x0, nbL, nbX, k, u1, vv);
+        const float3 p2 = estimate(L, x0, nbL, nbX, k, u2, vv);
+        const float q1 = ring_key<FK, true>(ring, k, p1.x, p1.y, p1.z, n);
+        const float q2 = ring_key<FK, true>(ring, k, p2.x, p2.y, p2.z, n);
+        const bool second = q2 > q1;
+        const float val = second ? q2 : q1;
+        float bv = __shfl_sync(FULL, val, 0);
+        int bt = 0;
+        for (int t = 1; t < 32; ++t) {
+            const float vt = __shfl_sync(FULL, val, t);
+            if (vt > bv) { bv = vt; bt = t; }
+        }
+        const float bu = __shfl_sync(FULL, second ? u2 : u1, bt);
+        const float bw = __shfl_sync(FULL, vv, bt);
+        const float bx = __shfl_sync(FULL, second ? p2.x : p1.x, bt);
+        const float by = __shfl_sync(FULL, second ? p2.y : p1.y, bt);
+        const float bz = __shfl_sync(FULL, second ? p2.z : p1.z, bt);
+        if (qLast < bv) { cx = bx; cy = by; cz = bz; cu = bu; cv = bw; qLast = bv; }
+        lastMax = bv;
+        ds = ds * (2.0f / 7.0f);
+    }
+    if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
+}
+
+}  // namespace
+
+int dmo_surf_max_ring() { return SURF_MAX_RING; }
+
+void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, cudaStream_t s) {
+    if (m.nSurf <= 0) return;
+    k_surface_fit<<<grid_for(m.nSurf, 128), 128, 0, s>>>(m.nSurf, m.he_rowptr.p, m.he.p, pos, m.vn.p, LS);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_update_nn(const Mesh& m, const float4* X0, int* nn, cudaStream_t s) {
+    if (m.nSurf <= 0) return;
+    k_update_nn<<<grid_for(m.nSurf, 256), 256, 0, s>>>(m.nSurf, m.nSurf - m.nFeature, m.he_rowptr.p, m.he.p, m.pos.p,
+                                                      X0, nn);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
+                     cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxk = m.maxHE;
+    const size_t smem = (size_t)SURF_WARPS * surf_warp_f4(maxk) * sizeof(float4);
+    const int blocks = (n + SURF_WARPS - 1) / SURF_WARPS;
+    if (m.fk == 4)
+        k_dmo_surf<4><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0,
+                                                            L.v1, L.grid_scale, L.depth, maxk);
+    else
+        k_dmo_surf<3><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0,
+                                                            L.v1, L.grid_scale, L.depth, maxk);
+    VSDMO_CHECK_LAUNCH();
+}
+
+}  // namespace vsdmo

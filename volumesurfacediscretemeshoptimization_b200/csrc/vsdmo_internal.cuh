@@ -103,6 +103,7 @@ int bits_for(uint32_t maxval);
 struct Mesh {
     int type = VSDMO_TRI;   // vsdmo_elem_type
     int k = 3;              // vertices per element
+    int fk = 3;             // vertices per surface face: 3 (triangles, tet boundary) or 4 (quads)
     int nV = 0, nE = 0;
     int nSurf = 0, nFeature = 0, nTris = 0, nHE = 0;
     int nColFree = 0, nColFeature = 0, nColInner = 0;
@@ -114,13 +115,13 @@ struct Mesh {
     DBuf<float4> pos;         // [nV] xyz + pad, internal numbering (the optimiser's state)
     DBuf<int> new_of_old;     // [nV]
     DBuf<int> elems;          // [nE*k]
-    DBuf<int> tris;           // [nTris*3]
+    DBuf<int> tris;           // [nTris*fk] surface faces
     DBuf<int> he_rowptr;      // [nSurf+1]
     DBuf<int4> he;            // [nHE] target, opposite, face, next
     DBuf<int> hf_rowptr;      // [nV+1]
     DBuf<int4> hf;            // [4nT] v0, v1, v2, tet
     DBuf<uint8_t> isB1, isFeat, isB2;
-    DBuf<float> fn, vn;       // [nTris*3], [nSurf*3]
+    DBuf<float> fn, vn;       // [nTris*3], [nSurf*3]; quad normals from corners 0, 1, 3
     std::vector<int> col_free, col_feature, col_inner;  // host copies of colour offsets
     DBuf<int> d_col_free, d_col_feature, d_col_inner;
 
@@ -131,7 +132,7 @@ struct Mesh {
 void build_mesh(Mesh& m, const float* d_xyz, const int* d_elems);
 
 // Normals of the surface (reference k_calcFaceNormals / k_calcVertexNormals).
-void update_normals(Mesh& m);
+void update_normals(const Mesh& m, cudaStream_t s);
 
 // ---- DMO kernels (dmo_kernels.cu) ---------------------------------------------------------
 struct DmoLaunch {
@@ -145,6 +146,19 @@ int dmo_tet_max_ring();      // largest halfface row the tet kernel accepts
 void prepare_dmo_kernels();
 int dmo_tri2d_max_ring();    // largest halfedge row the 2D kernel accepts
 
+// ---- surface DMO (surf_kernels.cu) ----------------------------------------------------------
+// Local quadric surfaces LS [4 nSurf] float4 fitted to pos with the mesh's vertex normals.
+void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, cudaStream_t s);
+// nn [nSurf]: nearest initial vertex of every surface vertex, walked from its previous value.
+void launch_update_nn(const Mesh& m, const float4* X0, int* nn, cudaStream_t s);
+// One colour class of free surface vertices (triangles when m.fk == 3, quads when 4).
+void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
+                     cudaStream_t s);
+int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
+
+// Element metric used by the quality kernels.
+enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3 };
+
 // Per-iteration statistics written by the quality kernel.
 struct IterStats {
     float min_q;
@@ -153,11 +167,11 @@ struct IterStats {
 };
 // Element qualities (reference formulas) -> min / sum into stats[*d_iter], monotonicity check
 // against min of the previous slot (or init_min for slot 0), then ++*d_iter.
-void launch_quality_stats(const Mesh& m, int quality, IterStats* d_stats, int* d_iter, float* d_partial_min,
+void launch_quality_stats(const Mesh& m, int kind, IterStats* d_stats, int* d_iter, float* d_partial_min,
                           double* d_partial_sum, int* d_partial_fail, unsigned* d_done, int check_monotone,
                           cudaStream_t s);
-void launch_element_qualities(const Mesh& m, int quality, float* d_out, cudaStream_t s);
-void launch_quality_histogram(const Mesh& m, int quality, int* d_counts, int n_cols, cudaStream_t s);
+void launch_element_qualities(const Mesh& m, int kind, float* d_out, cudaStream_t s);
+void launch_quality_histogram(const Mesh& m, int kind, int* d_counts, int n_cols, cudaStream_t s);
 int quality_stats_blocks();
 
 // ---- allocation-free quality reduction (noalloc.cu) -----------------------------------------
