@@ -96,6 +96,7 @@ typedef enum vsdmo_info_id {
 
 typedef struct vsdmo_mesh_s* vsdmo_mesh_t;
 typedef struct vsdmo_opt_s* vsdmo_opt_t;
+typedef struct vsdmo_model_s* vsdmo_model_t;
 
 /* Optimiser parameters. Defaults (vsdmo_params_default) follow the reference constructors:
  * DMOTetClass(mesh, MEAN_RATIO, 0.5f, 30)  dmo/DMOTet.h:24,
@@ -228,6 +229,52 @@ VSDMO_API vsdmo_status vsdmo_mesh_sync(vsdmo_mesh_t mesh);
 VSDMO_API vsdmo_status vsdmo_quality_reduce_noalloc(int elem_type, int flat, const float* d_xyz, int n_vertices,
                                                     const int32_t* d_elems, int n_elems, float threshold,
                                                     float* d_min, double* d_sum, int32_t* d_below, void* cuda_stream);
+
+/* ---- learned proposal (tet meshes) ----------------------------------------------------- */
+/* No counterpart in the reference. A small network (96 -> 128 -> 128 -> 128 -> 3, ReLU, BF16
+ * weights and activations, FP32 accumulation, run and trained by the library's own tcgen05
+ * tensor-core kernels) maps the one-ring of an inner vertex -- up to 32 distinct ring
+ * vertices in first-occurrence order of its halfface row, relative to the vertex and divided
+ * by the ring's largest per-axis extent -- to the displacement plain DMO picks for it, in the
+ * same units. In learned mode an optimiser searches a reduced grid around that proposal and
+ * runs the full plain search whenever the reduced one does not raise the vertex's ring
+ * minimum, so every move is one the plain search would accept and the minimum quality stays
+ * monotone. Parameters: one flat FP32 array of vsdmo_model_num_params() values
+ * (W1 [128x96] b1 W2 [128x128] b2 W3 [128x128] b3 W4 [16x128] b4 [16]; rows 3..15 of W4 and
+ * b4 are padding and stay zero). */
+VSDMO_API int vsdmo_model_num_params(void);
+/* He-uniform weights from seed, zero biases; runs on cuda_stream (NULL: a stream of its own). */
+VSDMO_API vsdmo_status vsdmo_model_create(uint64_t seed, void* cuda_stream, vsdmo_model_t* out);
+VSDMO_API void vsdmo_model_destroy(vsdmo_model_t model);
+VSDMO_API vsdmo_status vsdmo_model_get_params(vsdmo_model_t model, float* host_params);
+VSDMO_API vsdmo_status vsdmo_model_set_params(vsdmo_model_t model, const float* host_params);
+/* out [n x 3] = network(feats [n x 96]); host or device arrays. */
+VSDMO_API vsdmo_status vsdmo_model_forward(vsdmo_model_t model, const float* feats, long n, float* out, int mem_space);
+/* Mean squared error of one batch (n a multiple of 128, host arrays) and its gradient with
+ * respect to every parameter (grads: host, vsdmo_model_num_params() values). */
+VSDMO_API vsdmo_status vsdmo_model_gradients(vsdmo_model_t model, const float* feats, const float* targets, int n,
+                                             float* loss, float* grads);
+/* Adam (lr, betas 0.9 / 0.999) on `steps` batches of `batch` rows (a multiple of 128) drawn
+ * with replacement from the n_rows pairs (feats [n_rows x 96], targets [n_rows x 3], host or
+ * device); loss_history (host, may be NULL) receives each step's mean squared error. */
+VSDMO_API vsdmo_status vsdmo_model_train(vsdmo_model_t model, const float* feats, const float* targets, long n_rows,
+                                         int mem_space, int steps, int batch, float lr, uint64_t seed,
+                                         float* loss_history);
+/* Runs n_iter plain iterations of a tet optimiser (outside its iteration history: call
+ * vsdmo_opt_restart afterwards) and writes one training pair per vertex update into the
+ * DEVICE arrays feats [capacity x 96] and targets [capacity x 3]; *n_out = pairs written. */
+VSDMO_API vsdmo_status vsdmo_opt_collect_pairs(vsdmo_opt_t opt, int n_iter, float* feats, float* targets,
+                                               long capacity, long* n_out);
+/* Learned mode for a tet optimiser (model = NULL switches it off): reduced grid of
+ * reduced_n^3 candidates per level (2..8), reduced_depth levels (1..4). The model must stay
+ * alive while the optimiser uses it. */
+VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t opt, vsdmo_model_t model, int reduced_n, int reduced_depth);
+/* Learned-mode counters since vsdmo_opt_set_model: [0] vertex updates accepted from the
+ * reduced search, [1] fallbacks to the plain search, [2] fallbacks that moved the vertex. */
+VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t opt, unsigned long long* counters3);
+/* Test entry point of the tensor-core GEMM: D [M x N] = bf16(A) [M x K] . bf16(B) [N x K]^T
+ * in FP32, host arrays; N in {16, 32, 64, 96, 128}, K a multiple of 32. */
+VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int M, int N, int K, float* D);
 
 #ifdef __cplusplus
 }

@@ -4,8 +4,9 @@ Python mirror of the reference's C++ interface (DanielZint/VolumeSurfaceDiscrete
 
 * ``DMOMeshTriFactory.create(points, tris)`` / ``DMOMeshTetFactory.create(points, tets)``
   -- ``mesh/MeshFactory.h:17-40`` (device-array overloads; file parsing is separate);
-* ``DMOTetClass(mesh, QualityCriterium.MEAN_RATIO, gridScale=0.5, n_iter=30)`` and
-  ``DMOTriFlatClass(...)`` -- ``dmo/DMOTet.h:21-62``, ``dmo/DMOTriFlat.h:19-51`` with
+* ``DMOTetClass(mesh, QualityCriterium.MEAN_RATIO, gridScale=0.5, n_iter=30)``,
+  ``DMOTriFlatClass(...)``, ``DMOTriClass(...)`` and ``DMOQuadClass(...)`` --
+  ``dmo/DMOTet.h:21-62``, ``dmo/DMOTriFlat.h:19-51``, ``dmo/DMOTri.h``, ``dmo/DMOQuad.h`` with
   ``optimize()``, ``doIteration()``, ``isDone()``, ``getQuality()``, ``findMinimumQuality()``,
   ``getElementQualities()``, ``getQualityHistogram()``, ``displayQualityGPU()``
   (``dmo/DMOBase.h:23-88``).
@@ -15,20 +16,24 @@ only marshals arguments. Differences from the reference: meshes are built from a
 pass (host numpy or device pointers), vertex numbering is reported through
 ``permutation()`` / ``positions(original_order=True)``, errors raise ``VSDMOError`` instead of
 exiting, and ``fix_boundary`` selects the boundary-fixed runs of the benchmark configs.
+
+``ProposalModel`` and ``DMOTetClass.set_model`` add the learned proposal, which has no
+counterpart in the reference.
 """
 from __future__ import annotations
 
 import ctypes as C
 import enum
+import sys
 
 import numpy as np
 
 from . import _capi
 from ._capi import VSDMOError, Params, check
 
-__all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshTet", "DMOMeshTriFactory", "DMOMeshTetFactory",
-           "DMOTetClass", "DMOTriFlatClass", "DMOTriClass", "VSDMOError", "Params", "default_params",
-           "version"]
+__all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshQuad", "DMOMeshTet", "DMOMeshTriFactory",
+           "DMOMeshQuadFactory", "DMOMeshTetFactory", "DMOTetClass", "DMOTriFlatClass", "DMOTriClass",
+           "DMOQuadClass", "ProposalModel", "VSDMOError", "Params", "default_params", "version"]
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -98,6 +103,9 @@ class _Mesh:
             self.h = None
 
     def __del__(self):
+        # no library calls while the interpreter shuts down: the CUDA runtime may be gone
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:
@@ -203,6 +211,9 @@ class _DMOBase:
             self.h = None
 
     def __del__(self):
+        # no library calls while the interpreter shuts down: the CUDA runtime may be gone
+        if sys.is_finalizing():
+            return
         try:
             self.close()
         except Exception:
@@ -289,6 +300,95 @@ class _DMOBase:
 
 class DMOTetClass(_DMOBase):
     """``DMO::DMOTetClass`` (``dmo/DMOTet.h:21-62``)."""
+
+    def collect_pairs(self, n_iter: int, feats_dev_ptr: int, targets_dev_ptr: int, capacity: int) -> int:
+        """Runs n_iter plain iterations, writing one (ring features, DMO displacement) pair per
+        vertex update into caller-owned device arrays; returns the number of pairs."""
+        n = C.c_long(0)
+        check(_capi.lib().vsdmo_opt_collect_pairs(self.h, n_iter, C.c_void_p(feats_dev_ptr), C.c_void_p(targets_dev_ptr),
+                                                  capacity, C.byref(n)))
+        return n.value
+
+    def set_model(self, model, reduced_n: int = 4, reduced_depth: int = 2):
+        """Learned mode: reduced grid around the model's proposal, plain search as fallback."""
+        check(_capi.lib().vsdmo_opt_set_model(self.h, model.h if model is not None else None, reduced_n, reduced_depth))
+        self._model = model
+
+    def learned_counters(self):
+        """(reduced accepted, fallbacks, fallbacks that moved) since set_model."""
+        c = (C.c_ulonglong * 3)()
+        check(_capi.lib().vsdmo_opt_learned_counters(self.h, c))
+        return tuple(int(x) for x in c)
+
+
+class ProposalModel:
+    """The learned proposal network (no reference counterpart): 96 -> 128 -> 128 -> 128 -> 3."""
+
+    def __init__(self, seed: int = 0, stream=None):
+        self.h = C.c_void_p()
+        check(_capi.lib().vsdmo_model_create(seed, C.c_void_p(stream), C.byref(self.h)))
+        self.n_params = _capi.lib().vsdmo_model_num_params()
+
+    def close(self):
+        if getattr(self, "h", None):
+            _capi.lib().vsdmo_model_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        # no library calls while the interpreter shuts down: the CUDA runtime may be gone
+        if sys.is_finalizing():
+            return
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, np.float32)
+        check(_capi.lib().vsdmo_model_get_params(self.h, _ptr(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        check(_capi.lib().vsdmo_model_set_params(self.h, _ptr(p)))
+
+    def forward(self, feats) -> np.ndarray:
+        feats = np.ascontiguousarray(feats, np.float32)
+        out = np.zeros((len(feats), 3), np.float32)
+        check(_capi.lib().vsdmo_model_forward(self.h, _ptr(feats), len(feats), _ptr(out), _capi.HOST))
+        return out
+
+    def gradients(self, feats, targets):
+        feats = np.ascontiguousarray(feats, np.float32)
+        targets = np.ascontiguousarray(targets, np.float32)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_float(0)
+        check(_capi.lib().vsdmo_model_gradients(self.h, _ptr(feats), _ptr(targets), len(feats), C.byref(loss), _ptr(g)))
+        return float(loss.value), g
+
+    def train(self, feats, targets, steps: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0,
+              device_ptrs=None, n_rows: int = 0):
+        """Adam on minibatches drawn from (feats, targets); host arrays, or device pointers
+        (device_ptrs = (feats_ptr, targets_ptr), n_rows). Returns the per-step loss."""
+        hist = np.zeros(max(steps, 1), np.float32)
+        if device_ptrs is not None:
+            check(_capi.lib().vsdmo_model_train(self.h, C.c_void_p(device_ptrs[0]), C.c_void_p(device_ptrs[1]), n_rows,
+                                                _capi.DEVICE, steps, batch, lr, seed, _ptr(hist)))
+        else:
+            feats = np.ascontiguousarray(feats, np.float32)
+            targets = np.ascontiguousarray(targets, np.float32)
+            check(_capi.lib().vsdmo_model_train(self.h, _ptr(feats), _ptr(targets), len(feats), _capi.HOST, steps, batch,
+                                                lr, seed, _ptr(hist)))
+        return hist[:steps]
+
+
+def debug_gemm_bf16(A, B) -> np.ndarray:
+    """D = bf16(A) . bf16(B)^T through the library's tensor-core GEMM (test entry point)."""
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    D = np.zeros((A.shape[0], B.shape[0]), np.float32)
+    check(_capi.lib().vsdmo_debug_gemm_bf16(_ptr(A), _ptr(B), A.shape[0], B.shape[0], A.shape[1], _ptr(D)))
+    return D
 
 
 class DMOTriFlatClass(_DMOBase):

@@ -26,7 +26,10 @@ EXPORTED = [
     "vsdmo_opt_get_quality", "vsdmo_opt_find_min_quality", "vsdmo_opt_element_qualities",
     "vsdmo_opt_quality_histogram", "vsdmo_opt_display_quality", "vsdmo_opt_history",
     "vsdmo_opt_run_color", "vsdmo_opt_launches_per_iteration", "vsdmo_opt_surface_state",
-    "vsdmo_quality_reduce_noalloc",
+    "vsdmo_quality_reduce_noalloc", "vsdmo_model_num_params", "vsdmo_model_create", "vsdmo_model_destroy",
+    "vsdmo_model_get_params", "vsdmo_model_set_params", "vsdmo_model_forward", "vsdmo_model_gradients",
+    "vsdmo_model_train", "vsdmo_opt_collect_pairs", "vsdmo_opt_set_model", "vsdmo_opt_learned_counters",
+    "vsdmo_debug_gemm_bf16",
 ]
 
 
@@ -108,6 +111,30 @@ def lib():
     L.vsdmo_opt_run_color.argtypes = [P, I]
     L.vsdmo_quality_reduce_noalloc.restype = S
     L.vsdmo_quality_reduce_noalloc.argtypes = [I, I, P, I, P, I, F, P, P, P, P]
+    Lg, U64 = C.c_long, C.c_uint64
+    L.vsdmo_model_num_params.argtypes = []
+    L.vsdmo_model_create.restype = S
+    L.vsdmo_model_create.argtypes = [U64, P, C.POINTER(P)]
+    L.vsdmo_model_destroy.restype = None
+    L.vsdmo_model_destroy.argtypes = [P]
+    L.vsdmo_model_get_params.restype = S
+    L.vsdmo_model_get_params.argtypes = [P, P]
+    L.vsdmo_model_set_params.restype = S
+    L.vsdmo_model_set_params.argtypes = [P, P]
+    L.vsdmo_model_forward.restype = S
+    L.vsdmo_model_forward.argtypes = [P, P, Lg, P, I]
+    L.vsdmo_model_gradients.restype = S
+    L.vsdmo_model_gradients.argtypes = [P, P, P, I, C.POINTER(F), P]
+    L.vsdmo_model_train.restype = S
+    L.vsdmo_model_train.argtypes = [P, P, P, Lg, I, I, I, F, U64, P]
+    L.vsdmo_opt_collect_pairs.restype = S
+    L.vsdmo_opt_collect_pairs.argtypes = [P, I, P, P, Lg, C.POINTER(Lg)]
+    L.vsdmo_opt_set_model.restype = S
+    L.vsdmo_opt_set_model.argtypes = [P, P, I, I]
+    L.vsdmo_opt_learned_counters.restype = S
+    L.vsdmo_opt_learned_counters.argtypes = [P, P]
+    L.vsdmo_debug_gemm_bf16.restype = S
+    L.vsdmo_debug_gemm_bf16.argtypes = [P, P, I, I, I, P]
     _lib = L
     return L
 

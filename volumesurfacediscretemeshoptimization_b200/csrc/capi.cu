@@ -7,7 +7,7 @@
 // Surface optimisers (dmo/DMOTri.cu:129-165, dmo/DMOQuad.cu:125-162) also own the initial
 // positions, the local surfaces and the nearest-neighbour map, and their iteration adds the
 // nearest-neighbour walk and the normal update after the colour launches.
-#include "vsdmo_internal.cuh"
+#include "capi_internal.cuh"
 #include <cstring>
 #include <cmath>
 #include <algorithm>
@@ -15,63 +15,7 @@
 #include <iostream>
 #include <sstream>
 
-using namespace vsdmo;
-
-struct vsdmo_mesh_s {
-    Mesh m;
-};
-
-enum OptMode { MODE_TET = 0, MODE_TRI2D = 1, MODE_SURF = 2 };
-
-struct vsdmo_opt_s {
-    vsdmo_mesh_s* mesh = nullptr;
-    vsdmo_params p{};
-    int iters_done = 0;
-    int capacity = 0;
-    int mode = MODE_TET;
-    int kind = MK_TET;                         // element metric of the quality kernels
-    std::vector<std::pair<int, int>> ranges;  // colour classes in launch order
-    DBuf<float4> X0;                           // surface mode: initial surface positions [nSurf]
-    DBuf<float4> LS;                           // local surfaces [4 nSurf]
-    DBuf<int> nn;                              // nearest initial vertex [nSurf]
-    DBuf<IterStats> stats;
-    DBuf<int> d_iter;
-    DBuf<float> pmin;
-    DBuf<double> psum;
-    DBuf<int> pfail;
-    DBuf<unsigned> done;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    float last_min = 0.f;
-    ~vsdmo_opt_s() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-    }
-};
-
 namespace {
-
-thread_local std::string g_last_error;
-
-vsdmo_status fail(vsdmo_status s, const std::string& msg) {
-    g_last_error = msg;
-    return s;
-}
-
-template <class F>
-vsdmo_status guarded(F&& f) {
-    try {
-        f();
-        g_last_error.clear();
-        return VSDMO_OK;
-    } catch (const Error& e) {
-        return fail(e.status, e.what());
-    } catch (const std::bad_alloc&) {
-        return fail(VSDMO_E_NOMEM, "host allocation failed");
-    } catch (const std::exception& e) {
-        return fail(VSDMO_E_CUDA, e.what());
-    }
-}
 
 __global__ void k_pack_xyz(const float4* pos, int n, const int* new_of_old, float* out) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -103,7 +47,13 @@ void copy_in(void* dst, const void* src, size_t bytes, int mem_space, cudaStream
 void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
     const Mesh& m = o->mesh->m;
     DmoLaunch L{o->ranges[c].first, o->ranges[c].second, o->p.grid_scale, o->p.depth};
-    if (o->mode == MODE_TET) launch_dmo_tet(m, L, s);
+    if (o->mode == MODE_TET && o->model) {
+        // learned proposal: ring features -> network -> reduced grid around the proposal
+        const int n = L.v1 - L.v0;
+        launch_tet_features(m, L.v0, L.v1, nullptr, o->ws.X.p, nullptr, nullptr, s);
+        o->model->m.forward(o->ws, n, false, s);
+        launch_dmo_tet_learned(m, L, o->ws.Y.p, mlp::OUTP, o->reduced_n, o->reduced_depth, o->counters.p, s);
+    } else if (o->mode == MODE_TET) launch_dmo_tet(m, L, s);
     else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
     else launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, s);
 }
@@ -494,6 +444,7 @@ VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t o, int n_iter) {
             else run_iteration_body(o, s);
         }
         auto h = read_stats(o, o->iters_done + 1, n_iter);
+        if (o->model) o->model->m.check(s);
         for (auto& x : h) failures += x.fail_count;
         o->iters_done += n_iter;
         o->last_min = h.back().min_q;

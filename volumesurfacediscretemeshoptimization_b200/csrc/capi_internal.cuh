@@ -1,0 +1,76 @@
+// capi_internal.cuh -- handle structures and error plumbing shared by the C-ABI files.
+#pragma once
+#include "vsdmo_internal.cuh"
+#include "mlp.cuh"
+#include <memory>
+#include <string>
+
+using namespace vsdmo;
+
+struct vsdmo_mesh_s {
+    Mesh m;
+};
+
+enum OptMode { MODE_TET = 0, MODE_TRI2D = 1, MODE_SURF = 2 };
+
+struct vsdmo_opt_s {
+    vsdmo_mesh_s* mesh = nullptr;
+    vsdmo_params p{};
+    int iters_done = 0;
+    int capacity = 0;
+    int mode = MODE_TET;
+    int kind = MK_TET;                         // element metric of the quality kernels
+    std::vector<std::pair<int, int>> ranges;  // colour classes in launch order
+    DBuf<float4> X0;                           // surface mode: initial surface positions [nSurf]
+    DBuf<float4> LS;                           // local surfaces [4 nSurf]
+    DBuf<int> nn;                              // nearest initial vertex [nSurf]
+    DBuf<IterStats> stats;
+    DBuf<int> d_iter;
+    DBuf<float> pmin;
+    DBuf<double> psum;
+    DBuf<int> pfail;
+    DBuf<unsigned> done;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float last_min = 0.f;
+    // learned proposal (tet): model, feature rows of one colour class, proposals, counters
+    struct vsdmo_model_s* model = nullptr;
+    int reduced_n = 4, reduced_depth = 2;
+    mlp::Workspace ws;
+    DBuf<float> feats, scale, prop;
+    DBuf<unsigned long long> counters;    // [0] reduced accepted, [1] fallback, [2] fallback moved
+    bool collect = false;
+    ~vsdmo_opt_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+inline thread_local std::string g_last_error;
+
+inline vsdmo_status fail(vsdmo_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+template <class F>
+inline vsdmo_status guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return VSDMO_OK;
+    } catch (const Error& e) {
+        return fail(e.status, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(VSDMO_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(VSDMO_E_CUDA, e.what());
+    }
+}
+
+struct vsdmo_model_s {
+    mlp::Model m;
+    mlp::Workspace ws;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+};

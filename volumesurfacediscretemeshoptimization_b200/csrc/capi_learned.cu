@@ -1,0 +1,241 @@
+// capi_learned.cu -- C ABI of the learned proposal: the network handle (create, parameters,
+// forward, gradients, training), training-pair collection from plain DMO, and the switch that
+// puts a tet optimiser into learned mode. None of this has a counterpart in the reference.
+#include "capi_internal.cuh"
+#include <algorithm>
+#include <cstring>
+#include <random>
+#include <vector>
+
+namespace {
+
+void copy_in_rows(DBuf<float>& dst, const float* src, size_t count, int mem_space, cudaStream_t s) {
+    dst.alloc(count, s);
+    VSDMO_CUDA(cudaMemcpyAsync(dst.p, src, sizeof(float) * count,
+                               mem_space == VSDMO_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+}
+
+}  // namespace
+
+extern "C" {
+
+VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int M, int N, int K, float* D) {
+    if (!A || !B || !D || M <= 0 || K <= 0 || K % 32) return fail(VSDMO_E_ARG, "need M > 0, K a multiple of 32");
+    return guarded([&] {
+        cudaStream_t s;
+        VSDMO_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        try {
+            mlp::prepare(s);
+            mlp::debug_gemm(A, B, M, N, K, D, s);
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        VSDMO_CUDA(cudaStreamSynchronize(s));
+        cudaStreamDestroy(s);
+    });
+}
+
+VSDMO_API int vsdmo_model_num_params(void) { return mlp::N_PARAMS; }
+
+VSDMO_API vsdmo_status vsdmo_model_create(uint64_t seed, void* cuda_stream, vsdmo_model_t* out) {
+    if (!out) return fail(VSDMO_E_ARG, "null output handle");
+    *out = nullptr;
+    std::unique_ptr<vsdmo_model_s> h(new vsdmo_model_s);
+    vsdmo_status st = guarded([&] {
+        if (cuda_stream) {
+            h->stream = (cudaStream_t)cuda_stream;
+        } else {
+            VSDMO_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+            h->own_stream = true;
+        }
+        mlp::prepare(h->stream);
+        h->m.init(seed, h->stream);
+    });
+    if (st != VSDMO_OK) {
+        if (h->own_stream && h->stream) {
+            cudaStream_t s = h->stream;
+            h.reset();
+            cudaStreamDestroy(s);
+        }
+        return st;
+    }
+    *out = h.release();
+    return VSDMO_OK;
+}
+
+VSDMO_API void vsdmo_model_destroy(vsdmo_model_t m) {
+    if (!m) return;
+    cudaStream_t s = m->stream;
+    const bool own = m->own_stream;
+    cudaStreamSynchronize(s);
+    delete m;
+    if (own) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+}
+
+VSDMO_API vsdmo_status vsdmo_model_get_params(vsdmo_model_t m, float* host) {
+    if (!m || !host) return fail(VSDMO_E_ARG, "null argument");
+    return guarded([&] { m->m.get_params(host); });
+}
+
+VSDMO_API vsdmo_status vsdmo_model_set_params(vsdmo_model_t m, const float* host) {
+    if (!m || !host) return fail(VSDMO_E_ARG, "null argument");
+    return guarded([&] { m->m.set_params(host); });
+}
+
+VSDMO_API vsdmo_status vsdmo_model_forward(vsdmo_model_t m, const float* feats, long n, float* out, int mem_space) {
+    if (!m || !feats || !out || n <= 0) return fail(VSDMO_E_ARG, "bad argument");
+    if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
+    return guarded([&] {
+        cudaStream_t s = m->stream;
+        DBuf<float> f;
+        copy_in_rows(f, feats, (size_t)n * mlp::IN, mem_space, s);
+        m->ws.ensure(n, false, s);
+        m->m.gather(m->ws, f.p, nullptr, nullptr, (int)n, (int)n, false, s);
+        m->m.forward(m->ws, (int)n, false, s);
+        m->m.check(s);
+        std::vector<float> y = m->ws.Y.to_host();
+        std::vector<float> o((size_t)n * mlp::OUT);
+        for (long r = 0; r < n; ++r)
+            for (int j = 0; j < mlp::OUT; ++j) o[(size_t)r * mlp::OUT + j] = y[(size_t)r * mlp::OUTP + j];
+        if (mem_space == VSDMO_DEVICE)
+            VSDMO_CUDA(cudaMemcpyAsync(out, o.data(), sizeof(float) * o.size(), cudaMemcpyHostToDevice, s));
+        else
+            std::memcpy(out, o.data(), sizeof(float) * o.size());
+        VSDMO_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_model_gradients(vsdmo_model_t m, const float* feats, const float* targets, int n,
+                                             float* loss, float* grads) {
+    if (!m || !feats || !targets || n <= 0 || n % 128) return fail(VSDMO_E_ARG, "n must be a positive multiple of 128");
+    return guarded([&] {
+        cudaStream_t s = m->stream;
+        DBuf<float> f, t;
+        copy_in_rows(f, feats, (size_t)n * mlp::IN, VSDMO_HOST, s);
+        copy_in_rows(t, targets, (size_t)n * mlp::OUT, VSDMO_HOST, s);
+        m->ws.ensure(n, true, s);
+        m->m.gather(m->ws, f.p, t.p, nullptr, n, n, true, s);
+        m->m.forward(m->ws, n, true, s);
+        m->m.backward(m->ws, n, s);
+        m->m.check(s);
+        if (loss) *loss = read_scalar(m->ws.loss.p, s) / (3.f * (float)n);
+        if (grads) {
+            VSDMO_CUDA(cudaMemcpyAsync(grads, m->m.grads.p, sizeof(float) * mlp::N_PARAMS, cudaMemcpyDeviceToHost, s));
+            VSDMO_CUDA(cudaStreamSynchronize(s));
+        }
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_model_train(vsdmo_model_t m, const float* feats, const float* targets, long n_rows,
+                                         int mem_space, int steps, int batch, float lr, uint64_t seed,
+                                         float* loss_history) {
+    if (!m || !feats || !targets || n_rows <= 0 || steps < 0) return fail(VSDMO_E_ARG, "bad argument");
+    if (batch <= 0 || batch % 128) return fail(VSDMO_E_ARG, "batch must be a positive multiple of 128");
+    if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
+    return guarded([&] {
+        cudaStream_t s = m->stream;
+        DBuf<float> fh, th;
+        const float* df = feats;
+        const float* dt = targets;
+        if (mem_space == VSDMO_HOST) {
+            copy_in_rows(fh, feats, (size_t)n_rows * mlp::IN, VSDMO_HOST, s);
+            copy_in_rows(th, targets, (size_t)n_rows * mlp::OUT, VSDMO_HOST, s);
+            df = fh.p;
+            dt = th.p;
+        }
+        m->ws.ensure(batch, true, s);
+        DBuf<float> hist(std::max(steps, 1), s);
+        std::mt19937_64 g(seed);
+        std::uniform_int_distribution<long> pick(0, n_rows - 1);
+        std::vector<int> idx(batch);
+        DBuf<int> didx[2] = { DBuf<int>(batch, s), DBuf<int>(batch, s) };
+        for (int it = 0; it < steps; ++it) {
+            for (int i = 0; i < batch; ++i) idx[i] = (int)pick(g);
+            DBuf<int>& d = didx[it & 1];
+            VSDMO_CUDA(cudaMemcpyAsync(d.p, idx.data(), sizeof(int) * batch, cudaMemcpyHostToDevice, s));
+            m->m.gather(m->ws, df, dt, d.p, batch, batch, true, s);
+            m->m.forward(m->ws, batch, true, s);
+            m->m.backward(m->ws, batch, s);
+            m->m.adam(lr, s);
+            VSDMO_CUDA(cudaMemcpyAsync(hist.p + it, m->ws.loss.p, sizeof(float), cudaMemcpyDeviceToDevice, s));
+        }
+        m->m.check(s);
+        if (loss_history && steps > 0) {
+            std::vector<float> h = hist.to_host();
+            for (int i = 0; i < steps; ++i) loss_history[i] = h[i] / (3.f * (float)batch);
+        }
+        VSDMO_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t o, vsdmo_model_t model, int reduced_n, int reduced_depth) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    if (model && o->mode != MODE_TET) return fail(VSDMO_E_UNSUPPORTED, "the learned proposal is implemented for tet meshes");
+    if (model && (reduced_n < 2 || reduced_n > 8 || reduced_depth < 1 || reduced_depth > 4))
+        return fail(VSDMO_E_ARG, "reduced grid: 2..8 points per axis, 1..4 levels");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        cudaStream_t s = m.stream;
+        o->model = model;
+        o->reduced_n = reduced_n;
+        o->reduced_depth = reduced_depth;
+        if (model) {
+            int maxn = 1;
+            for (auto& r : o->ranges) maxn = std::max(maxn, r.second - r.first);
+            o->ws.ensure(maxn, false, s);
+            if (!o->counters.p) o->counters.alloc(3, s);
+            o->counters.zero();
+        }
+        // the captured iteration changes
+        if (o->exec) { cudaGraphExecDestroy(o->exec); o->exec = nullptr; }
+        if (o->graph) { cudaGraphDestroy(o->graph); o->graph = nullptr; }
+        m.sync();
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t o, unsigned long long* out3) {
+    if (!o || !out3) return fail(VSDMO_E_ARG, "null argument");
+    if (!o->counters.p) {
+        out3[0] = out3[1] = out3[2] = 0;
+        return VSDMO_OK;
+    }
+    return guarded([&] {
+        std::vector<unsigned long long> h = o->counters.to_host();
+        for (int i = 0; i < 3; ++i) out3[i] = h[i];
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_collect_pairs(vsdmo_opt_t o, int n_iter, float* feats, float* targets, long capacity,
+                                               long* n_out) {
+    if (!o || !feats || !targets || capacity <= 0 || n_iter < 0) return fail(VSDMO_E_ARG, "bad argument");
+    if (o->mode != MODE_TET) return fail(VSDMO_E_UNSUPPORTED, "training pairs are collected from tet meshes");
+    long rows = 0;
+    vsdmo_status st = guarded([&] {
+        const Mesh& m = o->mesh->m;
+        cudaStream_t s = m.stream;
+        int maxn = 1;
+        for (auto& r : o->ranges) maxn = std::max(maxn, r.second - r.first);
+        DBuf<float> scale(maxn, s);
+        DBuf<float4> old(maxn, s);
+        for (int it = 0; it < n_iter && rows < capacity; ++it) {
+            for (auto& r : o->ranges) {
+                const int n = (int)std::min<long>(r.second - r.first, capacity - rows);
+                if (n <= 0) break;
+                launch_tet_features(m, r.first, r.first + n, feats + rows * mlp::IN, nullptr, scale.p, old.p, s);
+                DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
+                launch_dmo_tet(m, L, s);
+                launch_tet_targets(m, r.first, r.first + n, scale.p, old.p, targets + rows * mlp::OUT, s);
+                rows += n;
+            }
+        }
+        m.sync();
+    });
+    if (n_out) *n_out = rows;
+    return st;
+}
+
+}  // extern "C"

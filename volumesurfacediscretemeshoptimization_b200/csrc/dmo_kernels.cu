@@ -26,13 +26,18 @@
 // (dmo/DMOTet.cu:45-67) in one deterministic launch; k_quality_histogram and
 // k_element_qualities replace k_qualityHistogram / k_getElementQualities (dmo/DMOTet.cu:31-43,69-75).
 #include "vsdmo_internal.cuh"
+#include "tc_gemm.cuh"
 #include <cfloat>
+#include <cuda_bf16.h>
 
 namespace vsdmo {
 namespace {
 
 constexpr int NQ = 8;
 constexpr unsigned FULL = 0xffffffffu;
+
+// packed position of feature (row, col) in the network's 96-column input operand
+__device__ __forceinline__ size_t learned_pk_off(long row, int col) { return tc::pk_off(row, col, 96); }
 // launch shape of the tet kernel (tuned on B200, see profiles/)
 #ifndef TET_WARPS_CFG
 #define TET_WARPS_CFG 4
@@ -176,18 +181,11 @@ __device__ __forceinline__ void tet_lane_best(const float4* __restrict__ co, int
     }
 }
 
-__global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
-k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
-          int v0, int v1, float grid_scale, int depth, int maxk) {
-    extern __shared__ float4 smem[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int v = v0 + blockIdx.x * TET_WARPS + w;
-    if (v >= v1) return;
-    float4* co = smem + (size_t)w * maxk * 2;
-    const int b = rowptr[v], k = rowptr[v + 1] - b;
-    if (k <= 0 || k > maxk) return;
-    const float4 c0 = pos[v];
-    // pass 1: per-axis extent of the ring (DMOTetImplCub.h:54-64)
+// Setup of one tet vertex shared by the plain and the learned search: per-axis extent of the
+// ring (DMOTetImplCub.h:54-64), the exact power-of-two scale 2^ex and the element coefficients
+// in shared memory. Returns false when the ring is degenerate (the vertex is left alone).
+__device__ __forceinline__ bool tet_setup(const float4* __restrict__ pos, const int4* __restrict__ hf, int b, int k,
+                                          float4 c0, int lane, float4* co, float& sx, float& sy, float& sz, int& ex) {
     float mdx = 0.f, mdy = 0.f, mdz = 0.f;
     for (int t = lane; t < k; t += 32) {
         const int4 h = hf[b + t];
@@ -198,10 +196,8 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
     }
     mdx = warp_max(mdx); mdy = warp_max(mdy); mdz = warp_max(mdz);
     const float mm = fmaxf(mdx, fmaxf(mdy, mdz));
-    if (!(mm > 0.f) || !(mm < FLT_MAX)) return;
-    int ex;
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) return false;
     (void)frexpf(mm, &ex);
-    // pass 2: element coefficients
     for (int t = lane; t < k; t += 32) {
         const int4 h = hf[b + t];
         const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
@@ -213,11 +209,19 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
         co[2 * t + 1] = K1;
     }
     __syncwarp();
-    const float sx = ldexpf(mdx, -ex), sy = ldexpf(mdy, -ex), sz = ldexpf(mdz, -ex);
+    sx = ldexpf(mdx, -ex); sy = ldexpf(mdy, -ex); sz = ldexpf(mdz, -ex);
+    return true;
+}
+
+// The plain hierarchical search (DMOTetImplCub.h:66-136) from the local origin: depth levels
+// of 8 x 8 x 8 candidates, moving on strict improvement of the ring key qLast. Returns whether
+// the vertex moved; (dx, dy, dz) is the new position in scaled local coordinates.
+__device__ __forceinline__ bool tet_plain_search(const float4* __restrict__ co, int k, float sx, float sy, float sz,
+                                                 float grid_scale, int depth, int lane, float qLast, float& dx,
+                                                 float& dy, float& dz) {
     const int ci = lane & 7, cj = lane >> 3;
     const float oi = grid_offset(ci), oj0 = grid_offset(cj), oj1 = grid_offset(cj + 4);
-    float dx = 0.f, dy = 0.f, dz = 0.f;
-    float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
+    dx = 0.f; dy = 0.f; dz = 0.f;
     bool moved = false;
     float ds = grid_scale;
     for (int level = 0; level < depth; ++level) {
@@ -246,8 +250,171 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
         }
         ds = ds * (2.0f / 7.0f);
     }
+    return moved;
+}
+
+__global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
+k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
+          int v0, int v1, float grid_scale, int depth, int maxk) {
+    extern __shared__ float4 smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int v = v0 + blockIdx.x * TET_WARPS + w;
+    if (v >= v1) return;
+    float4* co = smem + (size_t)w * maxk * 2;
+    const int b = rowptr[v], k = rowptr[v + 1] - b;
+    if (k <= 0 || k > maxk) return;
+    const float4 c0 = pos[v];
+    float sx, sy, sz;
+    int ex;
+    if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
+    const float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
+    float dx, dy, dz;
+    const bool moved = tet_plain_search(co, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
     if (moved && lane == 0)
         pos[v] = make_float4(c0.x + ldexpf(dx, ex), c0.y + ldexpf(dy, ex), c0.z + ldexpf(dz, ex), c0.w);
+}
+
+// ---- learned proposal (tet) -------------------------------------------------------------------
+// Features of the vertices [v0, v1): the distinct ring vertices in first-occurrence order of
+// the halfface row (up to 32), relative to the vertex and divided by the ring's largest
+// per-axis extent mm, zero padded to 96 values; FP32 rows and / or BF16 packed rows of the
+// network's input operand. scale[i] = mm, old[i] = the vertex position.
+__global__ void k_tet_features(const float4* __restrict__ pos, const int* __restrict__ rowptr,
+                               const int4* __restrict__ hf, int v0, int v1, float* __restrict__ feats,
+                               uint8_t* __restrict__ packed, float* __restrict__ scale, float4* __restrict__ old) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v1 - v0; i += gridDim.x * blockDim.x) {
+        const int v = v0 + i;
+        const float4 c0 = pos[v];
+        const int b = rowptr[v], k = rowptr[v + 1] - b;
+        int nb[32];
+        int n = 0;
+        float mm = 0.f;
+        for (int t = 0; t < k; ++t) {
+            const int4 h = hf[b + t];
+            const int u3[3] = { h.x, h.y, h.z };
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int u = u3[j];
+                const float4 q = pos[u];
+                mm = fmaxf(mm, fmaxf(fabsf(q.x - c0.x), fmaxf(fabsf(q.y - c0.y), fabsf(q.z - c0.z))));
+                bool seen = false;
+                for (int a = 0; a < n; ++a) seen |= nb[a] == u;
+                if (!seen && n < 32) nb[n++] = u;
+            }
+        }
+        const float inv = mm > 0.f ? 1.f / mm : 0.f;
+        if (scale) scale[i] = mm;
+        if (old) old[i] = c0;
+        for (int a = 0; a < 32; ++a) {
+            float f[3] = { 0.f, 0.f, 0.f };
+            if (a < n) {
+                const float4 q = pos[nb[a]];
+                f[0] = (q.x - c0.x) * inv; f[1] = (q.y - c0.y) * inv; f[2] = (q.z - c0.z) * inv;
+            }
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                if (feats) feats[(size_t)i * 96 + 3 * a + j] = f[j];
+                if (packed)
+                    *reinterpret_cast<__nv_bfloat16*>(packed + learned_pk_off(i, 3 * a + j)) = __float2bfloat16_rn(f[j]);
+            }
+        }
+    }
+}
+
+// training targets of the vertices [v0, v1) after a plain colour launch: the displacement the
+// search chose, in units of the ring extent
+__global__ void k_tet_targets(const float4* __restrict__ pos, int v0, int v1, const float* __restrict__ scale,
+                              const float4* __restrict__ old, float* __restrict__ targets) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v1 - v0; i += gridDim.x * blockDim.x) {
+        const float4 p = pos[v0 + i], o = old[i];
+        const float inv = scale[i] > 0.f ? 1.f / scale[i] : 0.f;
+        targets[(size_t)i * 3 + 0] = (p.x - o.x) * inv;
+        targets[(size_t)i * 3 + 1] = (p.y - o.y) * inv;
+        targets[(size_t)i * 3 + 2] = (p.z - o.z) * inv;
+    }
+}
+
+// offsets of the reduced grid with n points per axis: (n - 1 - 2i) / (n - 1)
+__device__ __forceinline__ float reduced_offset(int i, int n) { return (float)(n - 1 - 2 * i) / (float)(n - 1); }
+
+// Learned search: the network's displacement y (units of mm) centres a reduced grid of
+// rn^3 candidates per level, rdepth levels, half-extent starting at the plain search's second
+// level (grid_scale * 2/7 of the ring extent) and shrinking by 2/(rn-1); the proposal itself is
+// a candidate too. The vertex moves when the best of them strictly raises its ring minimum;
+// otherwise the full plain search runs (fallback), so every move is one plain DMO could
+// accept and the minimum quality never decreases. counters: [0] reduced accepted,
+// [1] fallbacks, [2] fallbacks that moved.
+__global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
+k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf, int v0,
+                  int v1, float grid_scale, int depth, int maxk, const float* __restrict__ Y, int ldy, int rn, int rdepth,
+                  unsigned long long* __restrict__ counters) {
+    extern __shared__ float4 smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int v = v0 + blockIdx.x * TET_WARPS + w;
+    if (v >= v1) return;
+    float4* co = smem + (size_t)w * maxk * 2;
+    const int b = rowptr[v], k = rowptr[v + 1] - b;
+    if (k <= 0 || k > maxk) return;
+    const float4 c0 = pos[v];
+    float sx, sy, sz;
+    int ex;
+    if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
+    const float q0 = tet_key1(co, k, 0.f, 0.f, 0.f);
+    // proposal in scaled local coordinates (the features were divided by mm = max(sx, sy, sz) 2^ex)
+    const float mms = fmaxf(sx, fmaxf(sy, sz));
+    const float* y = Y + (size_t)(v - v0) * ldy;
+    float px = y[0] * mms, py = y[1] * mms, pz = y[2] * mms;
+    const float bx = grid_scale * sx, by = grid_scale * sy, bz = grid_scale * sz;
+    bool have = isfinite(px) && isfinite(py) && isfinite(pz);
+    if (have) {
+        px = fminf(fmaxf(px, -bx), bx); py = fminf(fmaxf(py, -by), by); pz = fminf(fmaxf(pz, -bz), bz);
+    }
+    float best = -FLT_MAX, cx = 0.f, cy = 0.f, cz = 0.f;
+    if (have) {
+        best = tet_key1(co, k, px, py, pz);
+        cx = px; cy = py; cz = pz;
+        float rx = grid_scale * (2.0f / 7.0f) * sx, ry = grid_scale * (2.0f / 7.0f) * sy, rz = grid_scale * (2.0f / 7.0f) * sz;
+        const int nc = rn * rn * rn;
+        for (int level = 0; level < rdepth; ++level) {
+            float bk = -FLT_MAX;
+            int bi = 1 << 30;
+            for (int c = lane; c < nc; c += 32) {
+                const int ix = c % rn, iy = (c / rn) % rn, iz = c / (rn * rn);
+                const float x = fmaf(reduced_offset(ix, rn), rx, cx);
+                const float yy = fmaf(reduced_offset(iy, rn), ry, cy);
+                const float z = fmaf(reduced_offset(iz, rn), rz, cz);
+                const float key = tet_key1(co, k, x, yy, z);
+                if (key > bk || (key == bk && c < bi)) { bk = key; bi = c; }
+            }
+            warp_argmax(bk, bi);
+            if (bi < nc && bk > best) {
+                const int ix = bi % rn, iy = (bi / rn) % rn, iz = bi / (rn * rn);
+                const float nx = fmaf(reduced_offset(ix, rn), rx, cx);
+                const float ny = fmaf(reduced_offset(iy, rn), ry, cy);
+                const float nz = fmaf(reduced_offset(iz, rn), rz, cz);
+                cx = nx; cy = ny; cz = nz;
+                best = bk;
+            }
+            const float sh = 2.0f / (float)(rn - 1);
+            rx *= sh; ry *= sh; rz *= sh;
+        }
+    }
+    if (have && best > q0) {
+        if (lane == 0) {
+            pos[v] = make_float4(c0.x + ldexpf(cx, ex), c0.y + ldexpf(cy, ex), c0.z + ldexpf(cz, ex), c0.w);
+            atomicAdd(&counters[0], 1ull);
+        }
+        return;
+    }
+    float dx, dy, dz;
+    const bool moved = tet_plain_search(co, k, sx, sy, sz, grid_scale, depth, lane, q0, dx, dy, dz);
+    if (lane == 0) {
+        atomicAdd(&counters[1], 1ull);
+        if (moved) {
+            pos[v] = make_float4(c0.x + ldexpf(dx, ex), c0.y + ldexpf(dy, ex), c0.z + ldexpf(dz, ex), c0.w);
+            atomicAdd(&counters[2], 1ull);
+        }
+    }
 }
 
 // ---- flat triangles ---------------------------------------------------------------------------
@@ -481,6 +648,8 @@ void prepare_dmo_kernels() {
                                     TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tri2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TRI_WARPS * TRI_MAX_RING * 2 * (int)sizeof(float4)));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet_learned, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
 }
 int dmo_tri2d_max_ring() { return TRI_MAX_RING; }
 int quality_stats_blocks() { return QS_BLOCKS; }
@@ -492,6 +661,31 @@ void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
     const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
     k_dmo_tet<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
         m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_tet_features(const Mesh& m, int v0, int v1, float* feats, uint8_t* packed, float* scale, float4* old,
+                         cudaStream_t s) {
+    if (v1 <= v0) return;
+    k_tet_features<<<grid_for(v1 - v0, 128), 128, 0, s>>>(m.pos.p, m.hf_rowptr.p, m.hf.p, v0, v1, feats, packed, scale, old);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_tet_targets(const Mesh& m, int v0, int v1, const float* scale, const float4* old, float* targets,
+                        cudaStream_t s) {
+    if (v1 <= v0) return;
+    k_tet_targets<<<grid_for(v1 - v0, 256), 256, 0, s>>>(m.pos.p, v0, v1, scale, old, targets);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, int ldy, int rn, int rdepth,
+                            unsigned long long* counters, cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxk = m.maxTets;
+    const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
+    k_dmo_tet_learned<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
+        m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk, Y, ldy, rn, rdepth, counters);
     VSDMO_CHECK_LAUNCH();
 }
 

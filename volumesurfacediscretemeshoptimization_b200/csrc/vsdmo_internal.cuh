@@ -146,6 +146,18 @@ int dmo_tet_max_ring();      // largest halfface row the tet kernel accepts
 void prepare_dmo_kernels();
 int dmo_tri2d_max_ring();    // largest halfedge row the 2D kernel accepts
 
+// ---- learned proposal (tet; dmo_kernels.cu) ----------------------------------------------------
+// network inputs of vertices [v0, v1): FP32 rows [n x 96] and / or BF16 packed operand rows,
+// ring extent and old position per vertex (any output may be null)
+void launch_tet_features(const Mesh& m, int v0, int v1, float* feats, uint8_t* packed, float* scale, float4* old,
+                         cudaStream_t s);
+// displacement of [v0, v1) since launch_tet_features, in units of the ring extent
+void launch_tet_targets(const Mesh& m, int v0, int v1, const float* scale, const float4* old, float* targets,
+                        cudaStream_t s);
+// reduced grid around the network's proposal (Y [n x ldy], first 3 columns), plain fallback
+void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, int ldy, int rn, int rdepth,
+                            unsigned long long* counters, cudaStream_t s);
+
 // ---- surface DMO (surf_kernels.cu) ----------------------------------------------------------
 // Local quadric surfaces LS [4 nSurf] float4 fitted to pos with the mesh's vertex normals.
 void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, cudaStream_t s);
