@@ -115,6 +115,9 @@ typedef struct vsdmo_params {
     int   use_graph;      /* 1: each iteration is replayed from a captured CUDA graph       */
     int   check_monotone; /* 1: per-element check against the last minimum (reference       */
                           /*    k_updateCurrentQualities, dmo/DMOTet.cu:55-67)              */
+    int   active_set;     /* tet: 1 = skip a vertex whose last search found no improvement   */
+                          /*    while none of its ring vertices moved since (the result is   */
+                          /*    the same with or without skipping); 0 = search every vertex  */
 } vsdmo_params;
 
 /* ---- library --------------------------------------------------------------------------- */
@@ -266,12 +269,16 @@ VSDMO_API vsdmo_status vsdmo_model_train(vsdmo_model_t model, const float* feats
 VSDMO_API vsdmo_status vsdmo_opt_collect_pairs(vsdmo_opt_t opt, int n_iter, float* feats, float* targets,
                                                long capacity, long* n_out);
 /* Learned mode for a tet optimiser (model = NULL switches it off): reduced grid of
- * reduced_n^3 candidates per level (2..8), reduced_depth levels (1..4). The model must stay
- * alive while the optimiser uses it. */
-VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t opt, vsdmo_model_t model, int reduced_n, int reduced_depth);
-/* Learned-mode counters since vsdmo_opt_set_model: [0] vertex updates accepted from the
- * reduced search, [1] fallbacks to the plain search, [2] fallbacks that moved the vertex. */
-VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t opt, unsigned long long* counters3);
+ * reduced_n^3 candidates per level (2..8), reduced_depth levels (1..4), first half-extent
+ * reduced_scale x grid_scale x the ring's per-axis extent (0 < reduced_scale <= 1; each
+ * further level shrinks it by 2 / (reduced_n - 1)). The model must stay alive while the
+ * optimiser uses it. */
+VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t opt, vsdmo_model_t model, int reduced_n, int reduced_depth,
+                                           float reduced_scale);
+/* Counters since vsdmo_opt_set_model / vsdmo_opt_restart: [0] vertex updates accepted from the
+ * reduced search, [1] fallbacks to the plain search, [2] fallbacks that moved the vertex,
+ * [3] vertices skipped by the active set (plain and learned mode). */
+VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t opt, unsigned long long* counters4);
 /* Test entry point of the tensor-core GEMM: D [M x N] = bf16(A) [M x K] . bf16(B) [N x K]^T
  * in FP32, host arrays; N in {16, 32, 64, 96, 128}, K a multiple of 32. */
 VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int M, int N, int K, float* D);

@@ -152,7 +152,7 @@ def test_learned_mode_monotone_and_gain(vsdmo):
         mn, mean = opt.history()
         assert np.all(np.diff(mn) >= -1e-6)          # the fallback keeps the minimum monotone
         assert mn[-1] > q0 and mean[-1] > mean[0]
-        acc, fb, fb_moved = opt.learned_counters()
+        acc, fb, fb_moved, skipped = opt.learned_counters()
         assert acc + fb == 6 * (mesh.info["nV"] - mesh.info["nSurf"])
         res[name] = (acc, fb, mean[-1])
     # what training gains: more updates accepted from the cheap reduced search

@@ -26,6 +26,7 @@ import ctypes as C
 import enum
 import sys
 
+
 import numpy as np
 
 from . import _capi
@@ -102,9 +103,10 @@ class _Mesh:
             _capi.lib().vsdmo_mesh_destroy(self.h)
             self.h = None
 
-    def __del__(self):
+    def __del__(self, _finalizing=sys.is_finalizing):
         # no library calls while the interpreter shuts down: the CUDA runtime may be gone
-        if sys.is_finalizing():
+        # (bound as a default: module globals are cleared during shutdown)
+        if _finalizing():
             return
         try:
             self.close()
@@ -189,7 +191,7 @@ class _DMOBase:
 
     def __init__(self, dmo_mesh, qualityCriterium=QualityCriterium.MEAN_RATIO, gridScale: float = 0.5,
                  n_iter: int = 30, fix_boundary: bool = True, use_graph: bool = True, depth: int = 3,
-                 check_monotone: bool = True):
+                 check_monotone: bool = True, active_set: bool = False):
         self.mesh = dmo_mesh
         p = default_params(dmo_mesh.elem_type)
         p.quality = int(qualityCriterium)
@@ -199,6 +201,7 @@ class _DMOBase:
         p.use_graph = int(use_graph)
         p.depth = int(depth)
         p.check_monotone = int(check_monotone)
+        p.active_set = int(active_set)
         p.flat = self._flat
         self.params = p
         h = C.c_void_p()
@@ -210,9 +213,10 @@ class _DMOBase:
             _capi.lib().vsdmo_opt_destroy(self.h)
             self.h = None
 
-    def __del__(self):
+    def __del__(self, _finalizing=sys.is_finalizing):
         # no library calls while the interpreter shuts down: the CUDA runtime may be gone
-        if sys.is_finalizing():
+        # (bound as a default: module globals are cleared during shutdown)
+        if _finalizing():
             return
         try:
             self.close()
@@ -309,14 +313,15 @@ class DMOTetClass(_DMOBase):
                                                   capacity, C.byref(n)))
         return n.value
 
-    def set_model(self, model, reduced_n: int = 4, reduced_depth: int = 2):
+    def set_model(self, model, reduced_n: int = 4, reduced_depth: int = 2, reduced_scale: float = 2.0 / 7.0):
         """Learned mode: reduced grid around the model's proposal, plain search as fallback."""
-        check(_capi.lib().vsdmo_opt_set_model(self.h, model.h if model is not None else None, reduced_n, reduced_depth))
+        check(_capi.lib().vsdmo_opt_set_model(self.h, model.h if model is not None else None, reduced_n, reduced_depth,
+                                              reduced_scale))
         self._model = model
 
     def learned_counters(self):
-        """(reduced accepted, fallbacks, fallbacks that moved) since set_model."""
-        c = (C.c_ulonglong * 3)()
+        """(reduced accepted, fallbacks, fallbacks that moved, skipped by the active set)."""
+        c = (C.c_ulonglong * 4)()
         check(_capi.lib().vsdmo_opt_learned_counters(self.h, c))
         return tuple(int(x) for x in c)
 
@@ -334,9 +339,10 @@ class ProposalModel:
             _capi.lib().vsdmo_model_destroy(self.h)
             self.h = None
 
-    def __del__(self):
+    def __del__(self, _finalizing=sys.is_finalizing):
         # no library calls while the interpreter shuts down: the CUDA runtime may be gone
-        if sys.is_finalizing():
+        # (bound as a default: module globals are cleared during shutdown)
+        if _finalizing():
             return
         try:
             self.close()

@@ -42,7 +42,8 @@ class VSDMOError(RuntimeError):
 class Params(C.Structure):
     _fields_ = [("quality", C.c_int), ("grid_scale", C.c_float), ("n_iter", C.c_int),
                 ("grid_n", C.c_int), ("depth", C.c_int), ("fix_boundary", C.c_int),
-                ("flat", C.c_int), ("use_graph", C.c_int), ("check_monotone", C.c_int)]
+                ("flat", C.c_int), ("use_graph", C.c_int), ("check_monotone", C.c_int),
+                ("active_set", C.c_int)]
 
 
 _lib = None
@@ -130,7 +131,7 @@ def lib():
     L.vsdmo_opt_collect_pairs.restype = S
     L.vsdmo_opt_collect_pairs.argtypes = [P, I, P, P, Lg, C.POINTER(Lg)]
     L.vsdmo_opt_set_model.restype = S
-    L.vsdmo_opt_set_model.argtypes = [P, P, I, I]
+    L.vsdmo_opt_set_model.argtypes = [P, P, I, I, F]
     L.vsdmo_opt_learned_counters.restype = S
     L.vsdmo_opt_learned_counters.argtypes = [P, P]
     L.vsdmo_debug_gemm_bf16.restype = S

@@ -50,13 +50,31 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
     if (o->mode == MODE_TET && o->model) {
         // learned proposal: ring features -> network -> reduced grid around the proposal
         const int n = L.v1 - L.v0;
-        launch_tet_features(m, L.v0, L.v1, nullptr, o->ws.X.p, nullptr, nullptr, s);
+        launch_tet_features(m, L.v0, L.v1, o->nb.p, o->nbn.p, o->nb_base, nullptr, o->ws.X.p, nullptr, nullptr, s);
         o->model->m.forward(o->ws, n, false, s);
-        launch_dmo_tet_learned(m, L, o->ws.Y.p, mlp::OUTP, o->reduced_n, o->reduced_depth, o->counters.p, s);
-    } else if (o->mode == MODE_TET) launch_dmo_tet(m, L, s);
+        launch_dmo_tet_learned(m, L, o->ws.Y.p, mlp::OUTP, o->reduced_n, o->reduced_depth, o->reduced_scale,
+                               o->counters.p, o->dirty.p, o->fb_list.p, o->fb_count.p, s);
+    } else if (o->mode == MODE_TET) {
+        launch_dmo_tet(m, L, s, o->dirty.p, o->dirty.p ? o->counters.p + 3 : nullptr);
+    }
     else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
     else launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, s);
 }
+
+}  // namespace
+
+// ring-vertex table of the inner (tet) range, built once: the topology never changes
+void vsdmo_opt_s::ensure_neighbours() {
+    if (nb.p) return;
+    const Mesh& m = mesh->m;
+    const int n = m.nV - m.nSurf;
+    nb_base = m.nSurf;
+    nb.alloc((size_t)std::max(n, 1) * 32, m.stream);
+    nbn.alloc(std::max(n, 1), m.stream);
+    launch_tet_neighbours(m, m.nSurf, m.nV, nb.p, nbn.p, m.stream);
+}
+
+namespace {
 
 void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
     const Mesh& m = o->mesh->m;
@@ -167,6 +185,7 @@ VSDMO_API vsdmo_status vsdmo_params_default(int elem_type, vsdmo_params* out) {
     out->flat = -1;
     out->use_graph = 1;
     out->check_monotone = 1;
+    out->active_set = 0;
     return VSDMO_OK;
 }
 
@@ -414,6 +433,12 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->done.alloc(1, s); o->done.zero();
         prepare_dmo_kernels();
         if (o->mode == MODE_SURF) init_surface_state(o.get());
+        o->counters.alloc(4, s);
+        o->counters.zero();
+        if (o->mode == MODE_TET && p.active_set) {
+            o->dirty.alloc(m.nV, s);
+            o->dirty.fill_bytes(1);
+        }
         ensure_capacity(o.get(), std::min(std::max(p.n_iter, 1), 4096));
         launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1, s);
         auto h = read_stats(o.get(), 0, 1);
@@ -461,6 +486,8 @@ VSDMO_API vsdmo_status vsdmo_opt_restart(vsdmo_opt_t o) {
         o->iters_done = 0;
         o->d_iter.zero();
         if (o->mode == MODE_SURF) init_surface_state(o);
+        o->counters.zero();
+        if (o->dirty.p) o->dirty.fill_bytes(1);
         launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1,
                              m.stream);
         auto h = read_stats(o, 0, 1);

@@ -36,9 +36,14 @@ struct vsdmo_opt_s {
     // learned proposal (tet): model, feature rows of one colour class, proposals, counters
     struct vsdmo_model_s* model = nullptr;
     int reduced_n = 4, reduced_depth = 2;
+    float reduced_scale = 2.0f / 7.0f;
     mlp::Workspace ws;
-    DBuf<float> feats, scale, prop;
-    DBuf<unsigned long long> counters;    // [0] reduced accepted, [1] fallback, [2] fallback moved
+    DBuf<unsigned long long> counters;    // [0] reduced accepted, [1] fallback, [2] fallback moved, [3] skipped
+    DBuf<uint8_t> dirty;                  // active-set flags [nV] (params.active_set)
+    DBuf<int> nb, nbn;                    // ring vertices of the inner range [32 per vertex], counts
+    DBuf<int> fb_list, fb_count;          // fallback queue of one colour class
+    int nb_base = 0;
+    void ensure_neighbours();
     bool collect = false;
     ~vsdmo_opt_s() {
         if (exec) cudaGraphExecDestroy(exec);

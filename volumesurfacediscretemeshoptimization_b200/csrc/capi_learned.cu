@@ -172,24 +172,29 @@ VSDMO_API vsdmo_status vsdmo_model_train(vsdmo_model_t m, const float* feats, co
     });
 }
 
-VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t o, vsdmo_model_t model, int reduced_n, int reduced_depth) {
+VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t o, vsdmo_model_t model, int reduced_n, int reduced_depth,
+                                           float reduced_scale) {
     if (!o) return fail(VSDMO_E_ARG, "null optimiser");
     if (model && o->mode != MODE_TET) return fail(VSDMO_E_UNSUPPORTED, "the learned proposal is implemented for tet meshes");
     if (model && (reduced_n < 2 || reduced_n > 8 || reduced_depth < 1 || reduced_depth > 4))
         return fail(VSDMO_E_ARG, "reduced grid: 2..8 points per axis, 1..4 levels");
+    if (model && !(reduced_scale > 0.f && reduced_scale <= 1.f)) return fail(VSDMO_E_ARG, "reduced_scale must be in (0, 1]");
     return guarded([&] {
         const Mesh& m = o->mesh->m;
         cudaStream_t s = m.stream;
         o->model = model;
         o->reduced_n = reduced_n;
         o->reduced_depth = reduced_depth;
+        o->reduced_scale = reduced_scale;
         if (model) {
             int maxn = 1;
             for (auto& r : o->ranges) maxn = std::max(maxn, r.second - r.first);
             o->ws.ensure(maxn, false, s);
-            if (!o->counters.p) o->counters.alloc(3, s);
-            o->counters.zero();
+            o->ensure_neighbours();
+            if (!o->fb_list.p || (int)o->fb_list.n < maxn) o->fb_list.alloc(maxn, s);
+            if (!o->fb_count.p) o->fb_count.alloc(1, s);
         }
+        o->counters.zero();
         // the captured iteration changes
         if (o->exec) { cudaGraphExecDestroy(o->exec); o->exec = nullptr; }
         if (o->graph) { cudaGraphDestroy(o->graph); o->graph = nullptr; }
@@ -197,15 +202,11 @@ VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t o, vsdmo_model_t model, i
     });
 }
 
-VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t o, unsigned long long* out3) {
-    if (!o || !out3) return fail(VSDMO_E_ARG, "null argument");
-    if (!o->counters.p) {
-        out3[0] = out3[1] = out3[2] = 0;
-        return VSDMO_OK;
-    }
+VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t o, unsigned long long* out4) {
+    if (!o || !out4) return fail(VSDMO_E_ARG, "null argument");
     return guarded([&] {
         std::vector<unsigned long long> h = o->counters.to_host();
-        for (int i = 0; i < 3; ++i) out3[i] = h[i];
+        for (int i = 0; i < 4; ++i) out4[i] = h[i];
     });
 }
 
@@ -221,11 +222,13 @@ VSDMO_API vsdmo_status vsdmo_opt_collect_pairs(vsdmo_opt_t o, int n_iter, float*
         for (auto& r : o->ranges) maxn = std::max(maxn, r.second - r.first);
         DBuf<float> scale(maxn, s);
         DBuf<float4> old(maxn, s);
+        o->ensure_neighbours();
         for (int it = 0; it < n_iter && rows < capacity; ++it) {
             for (auto& r : o->ranges) {
                 const int n = (int)std::min<long>(r.second - r.first, capacity - rows);
                 if (n <= 0) break;
-                launch_tet_features(m, r.first, r.first + n, feats + rows * mlp::IN, nullptr, scale.p, old.p, s);
+                launch_tet_features(m, r.first, r.first + n, o->nb.p, o->nbn.p, o->nb_base, feats + rows * mlp::IN,
+                                    nullptr, scale.p, old.p, s);
                 DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
                 launch_dmo_tet(m, L, s);
                 launch_tet_targets(m, r.first, r.first + n, scale.p, old.p, targets + rows * mlp::OUT, s);

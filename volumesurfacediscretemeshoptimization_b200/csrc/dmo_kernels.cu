@@ -29,6 +29,7 @@
 #include "tc_gemm.cuh"
 #include <cfloat>
 #include <cuda_bf16.h>
+#include <algorithm>
 
 namespace vsdmo {
 namespace {
@@ -66,6 +67,11 @@ __device__ __forceinline__ float grid_offset(int i) {
     default: return -7.0f / 7.0f;
     }
 }
+
+// 2^e as a float when it is a normal number, else 0. Multiplying by it is exactly ldexpf(x, e)
+// (both are the correctly rounded value of x 2^e), at the cost of one multiply.
+__device__ __forceinline__ float exp2_exact(int e) { return (e >= -126 && e <= 127) ? __int_as_float((e + 127) << 23) : 0.f; }
+__device__ __forceinline__ float scale2(float x, float p, int e) { return p != 0.f ? x * p : ldexpf(x, e); }
 
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
@@ -122,6 +128,36 @@ __device__ float tet_key1(const float4* co, int k, float x, float y, float z) {
         if (t == 0) { N = num; D = den; dm = det; continue; }
         if (num * D < N * den) { N = num; D = den; }
         dm = fminf(dm, det);
+    }
+    return dm < 0.f ? dm : N / D;
+}
+
+// tet_key1 with the k tets spread over the lanes and combined in tet order by shuffles: the
+// same operations in the same order, so the same bits, for about a third of the instructions
+__device__ float tet_key_lanes(const float4* co, int k, float x, float y, float z, int lane) {
+    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    float N = 0.f, D = 1.f, dm = 0.f;
+    for (int base = 0; base < k; base += 32) {
+        const int t = base + lane;
+        float num = 0.f, den = 1.f, det = 0.f;
+        if (t < k) {
+            const float4 c0 = co[2 * t], c1 = co[2 * t + 1];
+            const float detA = fmaf(c0.x, x, c0.w);
+            const float LA = c1.w + fmaf(c1.x, x, tx);
+            const float detB = fmaf(c0.y, y, detA);
+            const float LB = LA + fmaf(c1.y, y, ty);
+            det = fmaf(c0.z, z, detB);
+            const float L = LB + fmaf(c1.z, z, tz);
+            num = det * det;
+            den = (L * L) * L;
+        }
+        const int cnt = min(32, k - base);
+        for (int j = 0; j < cnt; ++j) {
+            const float nj = __shfl_sync(FULL, num, j), dj = __shfl_sync(FULL, den, j), mj = __shfl_sync(FULL, det, j);
+            if (base + j == 0) { N = nj; D = dj; dm = mj; continue; }
+            if (nj * D < N * dj) { N = nj; D = dj; }
+            dm = fminf(dm, mj);
+        }
     }
     return dm < 0.f ? dm : N / D;
 }
@@ -198,19 +234,26 @@ __device__ __forceinline__ bool tet_setup(const float4* __restrict__ pos, const 
     const float mm = fmaxf(mdx, fmaxf(mdy, mdz));
     if (!(mm > 0.f) || !(mm < FLT_MAX)) return false;
     (void)frexpf(mm, &ex);
+    const float p = exp2_exact(-ex);
     for (int t = lane; t < k; t += 32) {
         const int4 h = hf[b + t];
         const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
         float4 K0, K1;
-        tet_coeffs(ldexpf(pa.x - c0.x, -ex), ldexpf(pa.y - c0.y, -ex), ldexpf(pa.z - c0.z, -ex),
-                   ldexpf(pb.x - c0.x, -ex), ldexpf(pb.y - c0.y, -ex), ldexpf(pb.z - c0.z, -ex),
-                   ldexpf(pc.x - c0.x, -ex), ldexpf(pc.y - c0.y, -ex), ldexpf(pc.z - c0.z, -ex), K0, K1);
+        tet_coeffs(scale2(pa.x - c0.x, p, -ex), scale2(pa.y - c0.y, p, -ex), scale2(pa.z - c0.z, p, -ex),
+                   scale2(pb.x - c0.x, p, -ex), scale2(pb.y - c0.y, p, -ex), scale2(pb.z - c0.z, p, -ex),
+                   scale2(pc.x - c0.x, p, -ex), scale2(pc.y - c0.y, p, -ex), scale2(pc.z - c0.z, p, -ex), K0, K1);
         co[2 * t] = K0;
         co[2 * t + 1] = K1;
     }
     __syncwarp();
-    sx = ldexpf(mdx, -ex); sy = ldexpf(mdy, -ex); sz = ldexpf(mdz, -ex);
+    sx = scale2(mdx, p, -ex); sy = scale2(mdy, p, -ex); sz = scale2(mdz, p, -ex);
     return true;
+}
+
+// position c0 + (dx, dy, dz) 2^ex of a move found in scaled local coordinates
+__device__ __forceinline__ float4 tet_unscale(float4 c0, float dx, float dy, float dz, int ex) {
+    const float p = exp2_exact(ex);
+    return make_float4(c0.x + scale2(dx, p, ex), c0.y + scale2(dy, p, ex), c0.z + scale2(dz, p, ex), c0.w);
 }
 
 // The plain hierarchical search (DMOTetImplCub.h:66-136) from the local origin: depth levels
@@ -253,13 +296,31 @@ __device__ __forceinline__ bool tet_plain_search(const float4* __restrict__ co, 
     return moved;
 }
 
+// Active set (optional, dirty != null): a vertex whose last search found no improvement and
+// none of whose ring vertices moved since is skipped -- the search would see the same ring and
+// return the same "no move", so skipping changes no result. A search that finds nothing clears
+// the vertex's flag; a move sets the flags of its ring vertices (adjacent vertices are never in
+// the same colour class, so no flag a launch reads is written by that launch).
+__device__ __forceinline__ void tet_mark_ring(const int4* __restrict__ hf, int b, int k, int lane,
+                                              uint8_t* __restrict__ dirty) {
+    for (int t = lane; t < k; t += 32) {
+        const int4 h = hf[b + t];
+        dirty[h.x] = 1; dirty[h.y] = 1; dirty[h.z] = 1;
+    }
+}
+
 __global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
 k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
-          int v0, int v1, float grid_scale, int depth, int maxk) {
+          int v0, int v1, float grid_scale, int depth, int maxk, uint8_t* __restrict__ dirty,
+          unsigned long long* __restrict__ skipped) {
     extern __shared__ float4 smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int v = v0 + blockIdx.x * TET_WARPS + w;
     if (v >= v1) return;
+    if (dirty && !dirty[v]) {
+        if (lane == 0 && skipped) atomicAdd(skipped, 1ull);
+        return;
+    }
     float4* co = smem + (size_t)w * maxk * 2;
     const int b = rowptr[v], k = rowptr[v + 1] - b;
     if (k <= 0 || k > maxk) return;
@@ -270,52 +331,114 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
     const float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
     float dx, dy, dz;
     const bool moved = tet_plain_search(co, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
-    if (moved && lane == 0)
-        pos[v] = make_float4(c0.x + ldexpf(dx, ex), c0.y + ldexpf(dy, ex), c0.z + ldexpf(dz, ex), c0.w);
+    if (moved && lane == 0) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
+    if (dirty) {
+        if (moved) tet_mark_ring(hf, b, k, lane, dirty);
+        else if (lane == 0) dirty[v] = 0;
+    }
+}
+
+// The plain search over a list of vertices of one colour class (the learned mode's fallback):
+// warps stride over list[0 .. *count).
+__global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
+k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
+               const int* __restrict__ list, const int* __restrict__ count, float grid_scale, int depth, int maxk,
+               uint8_t* __restrict__ dirty, unsigned long long* __restrict__ moved_count) {
+    extern __shared__ float4 smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float4* co = smem + (size_t)w * maxk * 2;
+    const int n = *count;
+    for (int idx = blockIdx.x * TET_WARPS + w; idx < n; idx += gridDim.x * TET_WARPS) {
+        const int v = list[idx];
+        const int b = rowptr[v], k = rowptr[v + 1] - b;
+        if (k <= 0 || k > maxk) continue;
+        const float4 c0 = pos[v];
+        float sx, sy, sz;
+        int ex;
+        if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) continue;
+        const float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
+        float dx, dy, dz;
+        const bool moved = tet_plain_search(co, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
+        if (moved && lane == 0) {
+            pos[v] = tet_unscale(c0, dx, dy, dz, ex);
+            atomicAdd(moved_count, 1ull);
+        }
+        if (dirty) {
+            if (moved) tet_mark_ring(hf, b, k, lane, dirty);
+            else if (lane == 0) dirty[v] = 0;
+        }
+        __syncwarp();
+    }
 }
 
 // ---- learned proposal (tet) -------------------------------------------------------------------
-// Features of the vertices [v0, v1): the distinct ring vertices in first-occurrence order of
-// the halfface row (up to 32), relative to the vertex and divided by the ring's largest
-// per-axis extent mm, zero padded to 96 values; FP32 rows and / or BF16 packed rows of the
-// network's input operand. scale[i] = mm, old[i] = the vertex position.
-__global__ void k_tet_features(const float4* __restrict__ pos, const int* __restrict__ rowptr,
-                               const int4* __restrict__ hf, int v0, int v1, float* __restrict__ feats,
-                               uint8_t* __restrict__ packed, float* __restrict__ scale, float4* __restrict__ old) {
+// Distinct ring vertices of every vertex in [v0, v1), in first-occurrence order of its
+// halfface row, at most 32 (the topology is fixed, so this runs once per optimiser):
+// nb [(v - v0) * 32 + a], nbn [v - v0].
+__global__ void k_tet_neighbours(const int* __restrict__ rowptr, const int4* __restrict__ hf, int v0, int v1,
+                                 int* __restrict__ nb, int* __restrict__ nbn) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v1 - v0; i += gridDim.x * blockDim.x) {
         const int v = v0 + i;
-        const float4 c0 = pos[v];
         const int b = rowptr[v], k = rowptr[v + 1] - b;
-        int nb[32];
+        int* out = nb + (size_t)i * 32;
         int n = 0;
-        float mm = 0.f;
         for (int t = 0; t < k; ++t) {
             const int4 h = hf[b + t];
             const int u3[3] = { h.x, h.y, h.z };
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                const int u = u3[j];
-                const float4 q = pos[u];
-                mm = fmaxf(mm, fmaxf(fabsf(q.x - c0.x), fmaxf(fabsf(q.y - c0.y), fabsf(q.z - c0.z))));
                 bool seen = false;
-                for (int a = 0; a < n; ++a) seen |= nb[a] == u;
-                if (!seen && n < 32) nb[n++] = u;
+                for (int a = 0; a < n; ++a) seen |= out[a] == u3[j];
+                if (!seen && n < 32) out[n++] = u3[j];
             }
+        }
+        nbn[i] = n;
+    }
+}
+
+// Features of the vertices [v0, v1): the ring vertices nb (in first-occurrence order of the
+// halfface row, at most 32) relative to the vertex and divided by the ring's largest
+// per-axis extent mm, zero padded to 96 values; FP32 rows and / or BF16 packed rows of the
+// network's input operand. scale[i] = mm, old[i] = the vertex position. nb / nbn index the
+// range relative to nb_base (the first vertex of the table).
+__global__ void k_tet_features(const float4* __restrict__ pos, int v0, int v1, const int* __restrict__ nb,
+                               const int* __restrict__ nbn, int nb_base, float* __restrict__ feats,
+                               uint8_t* __restrict__ packed, float* __restrict__ scale, float4* __restrict__ old) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < v1 - v0; i += gridDim.x * blockDim.x) {
+        const int v = v0 + i;
+        const float4 c0 = pos[v];
+        const int* list = nb + (size_t)(v - nb_base) * 32;
+        const int n = nbn[v - nb_base];
+        float mm = 0.f;
+        for (int a = 0; a < n; ++a) {
+            const float4 q = pos[list[a]];
+            mm = fmaxf(mm, fmaxf(fabsf(q.x - c0.x), fmaxf(fabsf(q.y - c0.y), fabsf(q.z - c0.z))));
         }
         const float inv = mm > 0.f ? 1.f / mm : 0.f;
         if (scale) scale[i] = mm;
         if (old) old[i] = c0;
-        for (int a = 0; a < 32; ++a) {
-            float f[3] = { 0.f, 0.f, 0.f };
-            if (a < n) {
-                const float4 q = pos[nb[a]];
-                f[0] = (q.x - c0.x) * inv; f[1] = (q.y - c0.y) * inv; f[2] = (q.z - c0.z) * inv;
-            }
+        // 12 groups of 8 features (one 16-byte packed store each)
+        for (int g = 0; g < 12; ++g) {
+            float f[8];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                if (feats) feats[(size_t)i * 96 + 3 * a + j] = f[j];
-                if (packed)
-                    *reinterpret_cast<__nv_bfloat16*>(packed + learned_pk_off(i, 3 * a + j)) = __float2bfloat16_rn(f[j]);
+            for (int e = 0; e < 8; ++e) {
+                const int c = 8 * g + e, a = c / 3, j = c % 3;
+                float val = 0.f;
+                if (a < n) {
+                    const float4 q = pos[list[a]];
+                    val = (j == 0 ? q.x - c0.x : (j == 1 ? q.y - c0.y : q.z - c0.z)) * inv;
+                }
+                f[e] = val;
+            }
+            if (feats) {
+#pragma unroll
+                for (int e = 0; e < 8; ++e) feats[(size_t)i * 96 + 8 * g + e] = f[e];
+            }
+            if (packed) {
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) h[e] = __float2bfloat16_rn(f[e]);
+                *reinterpret_cast<uint4*>(packed + learned_pk_off(i, 8 * g)) = *reinterpret_cast<const uint4*>(h);
             }
         }
     }
@@ -343,15 +466,21 @@ __device__ __forceinline__ float reduced_offset(int i, int n) { return (float)(n
 // a candidate too. The vertex moves when the best of them strictly raises its ring minimum;
 // otherwise the full plain search runs (fallback), so every move is one plain DMO could
 // accept and the minimum quality never decreases. counters: [0] reduced accepted,
-// [1] fallbacks, [2] fallbacks that moved.
-__global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
+// [1] fallbacks, [2] fallbacks that moved, [3] skipped by the active set. rscale: first
+// reduced half-extent in units of grid_scale x the per-axis ring extent.
+__global__ void __launch_bounds__(TET_WARPS * 32)
 k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf, int v0,
-                  int v1, float grid_scale, int depth, int maxk, const float* __restrict__ Y, int ldy, int rn, int rdepth,
-                  unsigned long long* __restrict__ counters) {
+                  int v1, float grid_scale, int maxk, const float* __restrict__ Y, int ldy, int rn, int rdepth,
+                  float rscale, unsigned long long* __restrict__ counters, uint8_t* __restrict__ dirty,
+                  int* __restrict__ fb_list, int* __restrict__ fb_count) {
     extern __shared__ float4 smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int v = v0 + blockIdx.x * TET_WARPS + w;
     if (v >= v1) return;
+    if (dirty && !dirty[v]) {
+        if (lane == 0) atomicAdd(&counters[3], 1ull);
+        return;
+    }
     float4* co = smem + (size_t)w * maxk * 2;
     const int b = rowptr[v], k = rowptr[v + 1] - b;
     if (k <= 0 || k > maxk) return;
@@ -359,32 +488,58 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
     float sx, sy, sz;
     int ex;
     if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
-    const float q0 = tet_key1(co, k, 0.f, 0.f, 0.f);
+    const float q0 = tet_key_lanes(co, k, 0.f, 0.f, 0.f, lane);
     // proposal in scaled local coordinates (the features were divided by mm = max(sx, sy, sz) 2^ex)
     const float mms = fmaxf(sx, fmaxf(sy, sz));
     const float* y = Y + (size_t)(v - v0) * ldy;
     float px = y[0] * mms, py = y[1] * mms, pz = y[2] * mms;
     const float bx = grid_scale * sx, by = grid_scale * sy, bz = grid_scale * sz;
-    bool have = isfinite(px) && isfinite(py) && isfinite(pz);
-    if (have) {
-        px = fminf(fmaxf(px, -bx), bx); py = fminf(fmaxf(py, -by), by); pz = fminf(fmaxf(pz, -bz), bz);
-    }
+    const bool have = isfinite(px) && isfinite(py) && isfinite(pz);
     float best = -FLT_MAX, cx = 0.f, cy = 0.f, cz = 0.f;
     if (have) {
-        best = tet_key1(co, k, px, py, pz);
+        px = fminf(fmaxf(px, -bx), bx); py = fminf(fmaxf(py, -by), by); pz = fminf(fmaxf(pz, -bz), bz);
+        best = tet_key_lanes(co, k, px, py, pz, lane);
         cx = px; cy = py; cz = pz;
-        float rx = grid_scale * (2.0f / 7.0f) * sx, ry = grid_scale * (2.0f / 7.0f) * sy, rz = grid_scale * (2.0f / 7.0f) * sz;
+        float rx = grid_scale * rscale * sx, ry = grid_scale * rscale * sy, rz = grid_scale * rscale * sz;
         const int nc = rn * rn * rn;
         for (int level = 0; level < rdepth; ++level) {
             float bk = -FLT_MAX;
             int bi = 1 << 30;
-            for (int c = lane; c < nc; c += 32) {
-                const int ix = c % rn, iy = (c / rn) % rn, iz = c / (rn * rn);
-                const float x = fmaf(reduced_offset(ix, rn), rx, cx);
-                const float yy = fmaf(reduced_offset(iy, rn), ry, cy);
-                const float z = fmaf(reduced_offset(iz, rn), rz, cz);
-                const float key = tet_key1(co, k, x, yy, z);
-                if (key > bk || (key == bk && c < bi)) { bk = key; bi = c; }
+            if (rn == 4) {
+                // 64 candidates, index ix + 4 iy + 16 iz: lane (ix, iy, iz0) also takes iz0 + 2,
+                // sharing the x and y parts of every tet; offsets (3 - 2i) / 3
+                const int ix = lane & 3, iy = (lane >> 2) & 3, iz0 = lane >> 4;
+                const float o4[4] = { 1.0f, 1.0f / 3.0f, -1.0f / 3.0f, -1.0f };
+                const float x = fmaf(o4[ix], rx, cx);
+                const float yy = fmaf(o4[iy], ry, cy);
+                const float z0 = fmaf(o4[iz0], rz, cz), z1 = fmaf(o4[iz0 + 2], rz, cz);
+                const float tx = (3.0f * x) * x, ty = (3.0f * yy) * yy;
+                const float tz0 = (3.0f * z0) * z0, tz1 = (3.0f * z1) * z1;
+                float N0 = 0.f, D0 = 1.f, m0 = 0.f, N1 = 0.f, D1 = 1.f, m1 = 0.f;
+                for (int t = 0; t < k; ++t) {
+                    const float4 K0 = co[2 * t], K1 = co[2 * t + 1];
+                    const float detB = fmaf(K0.y, yy, fmaf(K0.x, x, K0.w));
+                    const float LB = (K1.w + fmaf(K1.x, x, tx)) + fmaf(K1.y, yy, ty);
+                    const float d0 = fmaf(K0.z, z0, detB), L0 = LB + fmaf(K1.z, z0, tz0);
+                    const float d1 = fmaf(K0.z, z1, detB), L1 = LB + fmaf(K1.z, z1, tz1);
+                    const float n0 = d0 * d0, e0 = (L0 * L0) * L0, n1 = d1 * d1, e1 = (L1 * L1) * L1;
+                    if (t == 0) { N0 = n0; D0 = e0; m0 = d0; N1 = n1; D1 = e1; m1 = d1; continue; }
+                    if (n0 * D0 < N0 * e0) { N0 = n0; D0 = e0; }
+                    if (n1 * D1 < N1 * e1) { N1 = n1; D1 = e1; }
+                    m0 = fminf(m0, d0); m1 = fminf(m1, d1);
+                }
+                const float k0 = m0 < 0.f ? m0 : N0 / D0, k1 = m1 < 0.f ? m1 : N1 / D1;
+                bk = k0; bi = lane;
+                if (k1 > bk) { bk = k1; bi = lane + 32; }
+            } else {
+                for (int c = lane; c < nc; c += 32) {
+                    const int ix = c % rn, iy = (c / rn) % rn, iz = c / (rn * rn);
+                    const float x = fmaf(reduced_offset(ix, rn), rx, cx);
+                    const float yy = fmaf(reduced_offset(iy, rn), ry, cy);
+                    const float z = fmaf(reduced_offset(iz, rn), rz, cz);
+                    const float key = tet_key1(co, k, x, yy, z);
+                    if (key > bk || (key == bk && c < bi)) { bk = key; bi = c; }
+                }
             }
             warp_argmax(bk, bi);
             if (bi < nc && bk > best) {
@@ -401,19 +556,16 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
     }
     if (have && best > q0) {
         if (lane == 0) {
-            pos[v] = make_float4(c0.x + ldexpf(cx, ex), c0.y + ldexpf(cy, ex), c0.z + ldexpf(cz, ex), c0.w);
+            pos[v] = tet_unscale(c0, cx, cy, cz, ex);
             atomicAdd(&counters[0], 1ull);
         }
+        if (dirty) tet_mark_ring(hf, b, k, lane, dirty);
         return;
     }
-    float dx, dy, dz;
-    const bool moved = tet_plain_search(co, k, sx, sy, sz, grid_scale, depth, lane, q0, dx, dy, dz);
+    // the proposal did not raise the ring minimum: queue the vertex for the plain search
     if (lane == 0) {
+        fb_list[atomicAdd(fb_count, 1)] = v;
         atomicAdd(&counters[1], 1ull);
-        if (moved) {
-            pos[v] = make_float4(c0.x + ldexpf(dx, ex), c0.y + ldexpf(dy, ex), c0.z + ldexpf(dz, ex), c0.w);
-            atomicAdd(&counters[2], 1ull);
-        }
     }
 }
 
@@ -454,18 +606,19 @@ k_dmo_tri2d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4
     if (!(mm > 0.f) || !(mm < FLT_MAX)) return;
     int ex;
     (void)frexpf(mm, &ex);
+    const float p = exp2_exact(-ex);
     for (int t = lane; t < k; t += 32) {
         const float4 pa = pos[he[b + t].x];
         const float4 pb = pos[he[b + (t + 1 == k ? 0 : t + 1)].x];
-        const float ax = ldexpf(pa.x - c0.x, -ex), ay = ldexpf(pa.y - c0.y, -ex);
-        const float bx = ldexpf(pb.x - c0.x, -ex), by = ldexpf(pb.y - c0.y, -ex);
+        const float ax = scale2(pa.x - c0.x, p, -ex), ay = scale2(pa.y - c0.y, p, -ex);
+        const float bx = scale2(pb.x - c0.x, p, -ex), by = scale2(pb.y - c0.y, p, -ex);
         const float ux = bx - ax, uy = by - ay;
         const float C = ((ax * ax + ay * ay) + (bx * bx + by * by)) + (ux * ux + uy * uy);
         co[2 * t] = make_float4(-uy, ux, ax * uy - ay * ux, C);
         co[2 * t + 1] = make_float4(-2.0f * (ax + bx), -2.0f * (ay + by), 0.f, 0.f);
     }
     __syncwarp();
-    const float sx = ldexpf(mdx, -ex), sy = ldexpf(mdy, -ex);
+    const float sx = scale2(mdx, p, -ex), sy = scale2(mdy, p, -ex);
     const int i1 = lane >> 3, j1 = lane & 7;
     const float o1 = grid_offset(i1), o2 = grid_offset(i1 + 4), oj = grid_offset(j1);
     float dx = 0.f, dy = 0.f;
@@ -492,7 +645,7 @@ k_dmo_tri2d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4
         ds = ds * (2.0f / 7.0f);
     }
     if (qOld < lastMax && lane == 0)
-        pos[v] = make_float4(c0.x + ldexpf(dx, ex), c0.y + ldexpf(dy, ex), c0.z, c0.w);
+        pos[v] = make_float4(c0.x + scale2(dx, exp2_exact(ex), ex), c0.y + scale2(dy, exp2_exact(ex), ex), c0.z, c0.w);
 }
 
 // ---- reference element metrics ---------------------------------------------------------------
@@ -650,24 +803,33 @@ void prepare_dmo_kernels() {
                                     TRI_WARPS * TRI_MAX_RING * 2 * (int)sizeof(float4)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet_learned, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet_list, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
 }
 int dmo_tri2d_max_ring() { return TRI_MAX_RING; }
 int quality_stats_blocks() { return QS_BLOCKS; }
 
-void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
+void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s, uint8_t* dirty,
+                    unsigned long long* skipped) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
     const int maxk = m.maxTets;
     const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
     k_dmo_tet<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
-        m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk);
+        m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk, dirty, skipped);
     VSDMO_CHECK_LAUNCH();
 }
 
-void launch_tet_features(const Mesh& m, int v0, int v1, float* feats, uint8_t* packed, float* scale, float4* old,
-                         cudaStream_t s) {
+void launch_tet_neighbours(const Mesh& m, int v0, int v1, int* nb, int* nbn, cudaStream_t s) {
     if (v1 <= v0) return;
-    k_tet_features<<<grid_for(v1 - v0, 128), 128, 0, s>>>(m.pos.p, m.hf_rowptr.p, m.hf.p, v0, v1, feats, packed, scale, old);
+    k_tet_neighbours<<<grid_for(v1 - v0, 128), 128, 0, s>>>(m.hf_rowptr.p, m.hf.p, v0, v1, nb, nbn);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_tet_features(const Mesh& m, int v0, int v1, const int* nb, const int* nbn, int nb_base, float* feats,
+                         uint8_t* packed, float* scale, float4* old, cudaStream_t s) {
+    if (v1 <= v0) return;
+    k_tet_features<<<grid_for(v1 - v0, 128), 128, 0, s>>>(m.pos.p, v0, v1, nb, nbn, nb_base, feats, packed, scale, old);
     VSDMO_CHECK_LAUNCH();
 }
 
@@ -679,13 +841,21 @@ void launch_tet_targets(const Mesh& m, int v0, int v1, const float* scale, const
 }
 
 void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, int ldy, int rn, int rdepth,
-                            unsigned long long* counters, cudaStream_t s) {
+                            float rscale, unsigned long long* counters, uint8_t* dirty, int* fb_list, int* fb_count,
+                            cudaStream_t s) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
     const int maxk = m.maxTets;
     const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
+    VSDMO_CUDA(cudaMemsetAsync(fb_count, 0, sizeof(int), s));
     k_dmo_tet_learned<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
-        m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk, Y, ldy, rn, rdepth, counters);
+        m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, maxk, Y, ldy, rn, rdepth, rscale, counters, dirty,
+        fb_list, fb_count);
+    VSDMO_CHECK_LAUNCH();
+    // fallback: the plain search over the queued vertices, a fixed grid striding over the list
+    const int blocks = std::min((n + TET_WARPS - 1) / TET_WARPS, 148 * 4);
+    k_dmo_tet_list<<<blocks, TET_WARPS * 32, smem, s>>>(m.pos.p, m.hf_rowptr.p, m.hf.p, fb_list, fb_count, L.grid_scale,
+                                                       L.depth, maxk, dirty, counters + 2);
     VSDMO_CHECK_LAUNCH();
 }
 

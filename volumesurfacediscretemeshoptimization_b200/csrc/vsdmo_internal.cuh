@@ -140,23 +140,32 @@ struct DmoLaunch {
     float grid_scale;
     int depth;
 };
-void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
+// dirty (optional): active-set flags [nV], see k_dmo_tet; skipped (optional): skip counter
+void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s, uint8_t* dirty = nullptr,
+                    unsigned long long* skipped = nullptr);
 void launch_dmo_tri2d(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
 int dmo_tet_max_ring();      // largest halfface row the tet kernel accepts
 void prepare_dmo_kernels();
 int dmo_tri2d_max_ring();    // largest halfedge row the 2D kernel accepts
 
 // ---- learned proposal (tet; dmo_kernels.cu) ----------------------------------------------------
-// network inputs of vertices [v0, v1): FP32 rows [n x 96] and / or BF16 packed operand rows,
-// ring extent and old position per vertex (any output may be null)
-void launch_tet_features(const Mesh& m, int v0, int v1, float* feats, uint8_t* packed, float* scale, float4* old,
-                         cudaStream_t s);
+// distinct ring vertices of [v0, v1) (first occurrence in the halfface row, at most 32):
+// nb [(v - v0) * 32 + a], nbn [v - v0]
+void launch_tet_neighbours(const Mesh& m, int v0, int v1, int* nb, int* nbn, cudaStream_t s);
+// network inputs of vertices [v0, v1) from the neighbour table (whose first vertex is nb_base):
+// FP32 rows [n x 96] and / or BF16 packed operand rows, ring extent and old position per
+// vertex (any output may be null)
+void launch_tet_features(const Mesh& m, int v0, int v1, const int* nb, const int* nbn, int nb_base, float* feats,
+                         uint8_t* packed, float* scale, float4* old, cudaStream_t s);
 // displacement of [v0, v1) since launch_tet_features, in units of the ring extent
 void launch_tet_targets(const Mesh& m, int v0, int v1, const float* scale, const float4* old, float* targets,
                         cudaStream_t s);
-// reduced grid around the network's proposal (Y [n x ldy], first 3 columns), plain fallback
+// reduced grid around the network's proposal (Y [n x ldy], first 3 columns), plain fallback;
+// counters [4], dirty: optional active-set flags
+// fb_list [colour size] / fb_count: scratch of the fallback queue
 void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, int ldy, int rn, int rdepth,
-                            unsigned long long* counters, cudaStream_t s);
+                            float rscale, unsigned long long* counters, uint8_t* dirty, int* fb_list, int* fb_count,
+                            cudaStream_t s);
 
 // ---- surface DMO (surf_kernels.cu) ----------------------------------------------------------
 // Local quadric surfaces LS [4 nSurf] float4 fitted to pos with the mesh's vertex normals.
