@@ -14,6 +14,14 @@ N > 1 runs under torchrun: every rank optimises its own copy of the mesh (replic
 path has no exchange step), the time is the max over ranks and the value the sum of all
 ranks' vertex updates. ``--impl reference`` times the CPU restatement of the reference's
 own FP32 kernel (oracle/) on the host cores instead.
+
+The second half of the metric, time-to-plain-DMO min-quality learned vs plain, is the
+``learned`` object (rank 0 at N = 1; ``--no-learned`` skips it): the proposal network is
+trained from scratch on the GPU on the (ring, DMO displacement) pairs of 20 plain iterations
+of a separate seeded 48^3 tet cube; then on the 100^3 tet cube (1,030,301 vertices,
+6,000,000 tetrahedra, jitter 0.3h) plain DMO runs 20 iterations, and the learned mode runs
+from the same start until its minimum element quality reaches plain's final minimum - 1e-4.
+Both times are the sums of per-iteration CUDA-event times.
 """
 from __future__ import annotations
 
@@ -305,15 +313,105 @@ def run_ours(args):
                  "equivalent_tflops": ref_flop_per_update * n_inner / (dmo_ms / 1e3) / 1e12,
                  "nominal_peak_tflops": fp32_nominal_tflops},
     }
+    opt.close()
+    mesh.close()
+    if r == 0 and world == 1 and not args.no_learned:
+        line["learned"] = learned_time_to_quality(dev, stream)
     if r == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(xyz, tets)
     if r == 0:
         print(json.dumps(line), flush=True)
-    opt.close()
-    mesh.close()
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+LEARNED_CFG = {"reduced_n": 4, "reduced_depth": 2, "reduced_scale": 0.012,
+               "train_steps": (6000, 2000), "train_lr": (1e-3, 2e-4), "batch": 4096}
+
+
+def learned_time_to_quality(dev, stream):
+    """Trains the proposal network on plain-DMO pairs, then times plain vs learned DMO on the
+    100^3 tet cube to plain's final (20-iteration) minimum quality."""
+    import torch
+    import volumesurfacediscretemeshoptimization_b200 as V
+    from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+    sp = stream.cuda_stream
+    t0 = time.perf_counter()
+    # training pairs from plain DMO on a separate seeded 48^3 cube
+    xyz, tets = G.config2(seed=1000)
+    tm = V.DMOMeshTet(xyz, tets, stream=sp)
+    topt = V.DMOTetClass(tm, n_iter=N_ITER)
+    cap = (tm.info["nV"] - tm.info["nSurf"]) * N_ITER
+    feats = torch.empty(cap * 96, dtype=torch.float32, device=dev)
+    targ = torch.empty(cap * 3, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    n_pairs = topt.collect_pairs(N_ITER, feats.data_ptr(), targ.data_ptr(), cap)
+    t_collect = time.perf_counter() - t0
+    model = V.ProposalModel(seed=0, stream=sp)
+    t1 = time.perf_counter()
+    losses = []
+    for k, (steps, lr) in enumerate(zip(LEARNED_CFG["train_steps"], LEARNED_CFG["train_lr"])):
+        h = model.train(None, None, steps=steps, batch=LEARNED_CFG["batch"], lr=lr, seed=k,
+                        device_ptrs=(feats.data_ptr(), targ.data_ptr()), n_rows=n_pairs)
+        losses.append(float(h[-50:].mean()))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    tvar = float(targ.view(-1, 3)[:n_pairs].var(0).mean().item())
+    topt.close(); tm.close()
+    del feats, targ
+    # evaluation mesh
+    xyz5, tets5 = G.config5()
+    m5 = V.DMOMeshTet(xyz5, tets5, stream=sp)
+    n5 = m5.info["nV"] - m5.info["nSurf"]
+    x0 = m5.positions()
+    o5 = V.DMOTetClass(m5, n_iter=10 ** 9)
+
+    def run(stop_q, max_it):
+        ts, qs = [], []
+        for _ in range(max_it):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                a.record(stream)
+                o5.iterate(1)
+                b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+            qs.append(o5.getQuality())
+            if stop_q is not None and qs[-1] >= stop_q:
+                break
+        return ts, qs
+
+    run(None, 3)                                   # warm-up (graph capture, clocks)
+    m5.set_positions(x0); o5.restart()
+    tp, qp = run(None, N_ITER)
+    target = qp[-1] - 1e-4
+    m5.set_positions(x0); o5.restart()
+    o5.set_model(model, LEARNED_CFG["reduced_n"], LEARNED_CFG["reduced_depth"], LEARNED_CFG["reduced_scale"])
+    run(None, 2)                                   # warm-up of the learned graph
+    m5.set_positions(x0); o5.restart()
+    tl, ql = run(target, 4 * N_ITER)
+    acc, fb, fb_moved, _ = o5.learned_counters()
+    reached = ql[-1] >= target
+    o5.close(); m5.close(); model.close()
+    return {
+        "workload": "tet cube 100^3 (1030301 vertices / 6000000 tets, jitter 0.3h, boundary fixed), seed 0",
+        "plain_ms": sum(tp), "plain_iterations": len(tp), "plain_final_min_quality": qp[-1],
+        "target_min_quality": target,
+        "learned_ms": sum(tl) if reached else None, "learned_iterations": len(tl), "learned_reached": bool(reached),
+        "learned_final_min_quality": ql[-1],
+        "time_ratio_learned_over_plain": (sum(tl) / sum(tp)) if reached else None,
+        "plain_vertex_updates_per_s": n5 * len(tp) / (sum(tp) / 1e3),
+        "reduced_accepted": acc, "fallbacks": fb, "fallbacks_moved": fb_moved,
+        "reduced_accept_fraction": acc / max(1, acc + fb),
+        "search": {k: LEARNED_CFG[k] for k in ("reduced_n", "reduced_depth", "reduced_scale")},
+        "training": {"pairs": n_pairs, "source": "20 plain iterations, tet cube 48^3 seed 1000",
+                     "steps": list(LEARNED_CFG["train_steps"]), "lr": list(LEARNED_CFG["train_lr"]),
+                     "batch": LEARNED_CFG["batch"], "final_mse": losses[-1], "target_variance": tvar,
+                     "collect_s": t_collect, "train_s": t_train},
+        "plain_ms_per_iteration": tp, "learned_ms_per_iteration": tl,
+        "timing": "sum of per-iteration CUDA-event times on the library stream",
+    }
 
 
 def main():
@@ -323,6 +421,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -275,6 +275,9 @@ VSDMO_API vsdmo_status vsdmo_opt_collect_pairs(vsdmo_opt_t opt, int n_iter, floa
  * optimiser uses it. */
 VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t opt, vsdmo_model_t model, int reduced_n, int reduced_depth,
                                            float reduced_scale);
+/* Network proposals [n x 3] (host) of colour class `color` at the current positions, computed
+ * by the fused inference kernel the learned search uses (for tests and inspection). */
+VSDMO_API vsdmo_status vsdmo_opt_proposals(vsdmo_opt_t opt, int color, float* out);
 /* Counters since vsdmo_opt_set_model / vsdmo_opt_restart: [0] vertex updates accepted from the
  * reduced search, [1] fallbacks to the plain search, [2] fallbacks that moved the vertex,
  * [3] vertices skipped by the active set (plain and learned mode). */

@@ -122,6 +122,38 @@ def test_collect_pairs_first_colour_exact(vsdmo):
     assert moved > 0
 
 
+def test_fused_inference_matches_gemm_path(vsdmo):
+    """The fused features + network kernel of the learned search against the per-layer GEMM
+    path fed with the collected FP32 features of the same vertices."""
+    import torch
+    xyz, tets = G.tet_cube(12, seed=2)
+    mesh = vsdmo.DMOMeshTet(xyz, tets)
+    opt = vsdmo.DMOTetClass(mesh, n_iter=1)
+    model = vsdmo.ProposalModel(seed=4)
+    r = np.random.default_rng(0)
+    p = model.get_params()
+    p[mlp_bias_slice()] = r.uniform(-0.05, 0.05, size=p[mlp_bias_slice()].shape)
+    model.set_params(p)
+    opt.set_model(model, 4, 2, 0.05)
+    y_fused = opt.proposals(0)
+    cap = 4096
+    f = torch.zeros(cap * 96, dtype=torch.float32, device="cuda")
+    t = torch.zeros(cap * 3, dtype=torch.float32, device="cuda")
+    opt.set_model(None)
+    opt.collect_pairs(1, f.data_ptr(), t.data_ptr(), cap)
+    n = len(y_fused)
+    feats = f.cpu().numpy().reshape(cap, 96)[:n]
+    y_gemm = model.forward(feats)
+    # same BF16 inputs and weights; accumulation order inside the tensor cores may differ
+    assert np.abs(y_fused - y_gemm).max() <= 1e-3 * max(1.0, np.abs(y_gemm).max())
+
+
+def mlp_bias_slice():
+    from oracle import mlp_oracle as mo
+    o = mo.IN * mo.HID
+    return slice(o, o + mo.HID)
+
+
 def _train_on_plain_pairs(vsdmo, seed, n_cells=14, iters=8, steps=400):
     import torch
     xyz, tets = G.tet_cube(n_cells, seed=seed)

@@ -313,11 +313,18 @@ class DMOTetClass(_DMOBase):
                                                   capacity, C.byref(n)))
         return n.value
 
-    def set_model(self, model, reduced_n: int = 4, reduced_depth: int = 2, reduced_scale: float = 2.0 / 7.0):
+    def set_model(self, model, reduced_n: int = 4, reduced_depth: int = 2, reduced_scale: float = 0.012):
         """Learned mode: reduced grid around the model's proposal, plain search as fallback."""
         check(_capi.lib().vsdmo_opt_set_model(self.h, model.h if model is not None else None, reduced_n, reduced_depth,
                                               reduced_scale))
         self._model = model
+
+    def proposals(self, color: int) -> np.ndarray:
+        """Network proposals [n x 3] of one colour class (fused inference kernel)."""
+        r = self.mesh.array(A_COL_INNER)
+        out = np.zeros((int(r[color + 1] - r[color]), 3), np.float32)
+        check(_capi.lib().vsdmo_opt_proposals(self.h, color, _ptr(out)))
+        return out
 
     def learned_counters(self):
         """(reduced accepted, fallbacks, fallbacks that moved, skipped by the active set)."""

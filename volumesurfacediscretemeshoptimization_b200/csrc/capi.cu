@@ -48,10 +48,10 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
     const Mesh& m = o->mesh->m;
     DmoLaunch L{o->ranges[c].first, o->ranges[c].second, o->p.grid_scale, o->p.depth};
     if (o->mode == MODE_TET && o->model) {
-        // learned proposal: ring features -> network -> reduced grid around the proposal
+        // learned proposal: ring features + network (one fused tensor-core kernel) -> reduced
+        // grid around the proposal -> plain search for the vertices it did not improve
         const int n = L.v1 - L.v0;
-        launch_tet_features(m, L.v0, L.v1, o->nb.p, o->nbn.p, o->nb_base, nullptr, o->ws.X.p, nullptr, nullptr, s);
-        o->model->m.forward(o->ws, n, false, s);
+        o->model->m.infer_tet(m.pos.p, o->nb.p, o->nbn.p, o->nb_base, L.v0, n, o->ws.Y.p, mlp::OUTP, s);
         launch_dmo_tet_learned(m, L, o->ws.Y.p, mlp::OUTP, o->reduced_n, o->reduced_depth, o->reduced_scale,
                                o->counters.p, o->dirty.p, o->fb_list.p, o->fb_count.p, s);
     } else if (o->mode == MODE_TET) {

@@ -202,6 +202,24 @@ VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t o, vsdmo_model_t model, i
     });
 }
 
+VSDMO_API vsdmo_status vsdmo_opt_proposals(vsdmo_opt_t o, int color, float* out) {
+    if (!o || !out) return fail(VSDMO_E_ARG, "null argument");
+    if (!o->model) return fail(VSDMO_E_ARG, "no model set");
+    if (color < 0 || color >= (int)o->ranges.size()) return fail(VSDMO_E_ARG, "colour out of range");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        cudaStream_t s = m.stream;
+        const int v0 = o->ranges[color].first, n = o->ranges[color].second - v0;
+        o->model->m.infer_tet(m.pos.p, o->nb.p, o->nbn.p, o->nb_base, v0, n, o->ws.Y.p, mlp::OUTP, s);
+        o->model->m.check(s);
+        std::vector<float> y((size_t)n * mlp::OUTP);
+        VSDMO_CUDA(cudaMemcpyAsync(y.data(), o->ws.Y.p, sizeof(float) * y.size(), cudaMemcpyDeviceToHost, s));
+        VSDMO_CUDA(cudaStreamSynchronize(s));
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < 3; ++j) out[(size_t)i * 3 + j] = y[(size_t)i * mlp::OUTP + j];
+    });
+}
+
 VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t o, unsigned long long* out4) {
     if (!o || !out4) return fail(VSDMO_E_ARG, "null argument");
     return guarded([&] {

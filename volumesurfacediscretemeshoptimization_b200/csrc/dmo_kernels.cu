@@ -409,35 +409,35 @@ __global__ void k_tet_features(const float4* __restrict__ pos, int v0, int v1, c
         const float4 c0 = pos[v];
         const int* list = nb + (size_t)(v - nb_base) * 32;
         const int n = nbn[v - nb_base];
+        // each ring vertex loaded once; the 96 inputs stay in registers (fully unrolled)
+        float f[96];
         float mm = 0.f;
-        for (int a = 0; a < n; ++a) {
-            const float4 q = pos[list[a]];
-            mm = fmaxf(mm, fmaxf(fabsf(q.x - c0.x), fmaxf(fabsf(q.y - c0.y), fabsf(q.z - c0.z))));
+#pragma unroll
+        for (int a = 0; a < 32; ++a) {
+            float dx = 0.f, dy = 0.f, dz = 0.f;
+            if (a < n) {
+                const float4 q = pos[list[a]];
+                dx = q.x - c0.x; dy = q.y - c0.y; dz = q.z - c0.z;
+                mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
+            }
+            f[3 * a] = dx; f[3 * a + 1] = dy; f[3 * a + 2] = dz;
         }
         const float inv = mm > 0.f ? 1.f / mm : 0.f;
+#pragma unroll
+        for (int c = 0; c < 96; ++c) f[c] = f[c] * inv;
         if (scale) scale[i] = mm;
         if (old) old[i] = c0;
-        // 12 groups of 8 features (one 16-byte packed store each)
-        for (int g = 0; g < 12; ++g) {
-            float f[8];
+        if (feats) {
+            float4* o = reinterpret_cast<float4*>(feats + (size_t)i * 96);
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                const int c = 8 * g + e, a = c / 3, j = c % 3;
-                float val = 0.f;
-                if (a < n) {
-                    const float4 q = pos[list[a]];
-                    val = (j == 0 ? q.x - c0.x : (j == 1 ? q.y - c0.y : q.z - c0.z)) * inv;
-                }
-                f[e] = val;
-            }
-            if (feats) {
+            for (int g = 0; g < 24; ++g) o[g] = make_float4(f[4 * g], f[4 * g + 1], f[4 * g + 2], f[4 * g + 3]);
+        }
+        if (packed) {
 #pragma unroll
-                for (int e = 0; e < 8; ++e) feats[(size_t)i * 96 + 8 * g + e] = f[e];
-            }
-            if (packed) {
+            for (int g = 0; g < 12; ++g) {
                 __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
-                for (int e = 0; e < 8; ++e) h[e] = __float2bfloat16_rn(f[e]);
+                for (int e = 0; e < 8; ++e) h[e] = __float2bfloat16_rn(f[8 * g + e]);
                 *reinterpret_cast<uint4*>(packed + learned_pk_off(i, 8 * g)) = *reinterpret_cast<const uint4*>(h);
             }
         }

@@ -264,6 +264,166 @@ __global__ void k_sum(const float* a, int n, float* out) {
     if (threadIdx.x == 0) *out = sh[0];
 }
 
+// ---- fused inference for the learned tet search --------------------------------------------------
+// One persistent CTA per SM keeps the packed BF16 weights in shared memory (loaded once by bulk
+// copies) and loops over tiles of 128 vertices: each thread builds its vertex's 96 inputs from
+// the ring-vertex table straight into the packed A operand in shared memory, then the four
+// layers run back to back on the tensor cores (one 128-column TMEM accumulator, reused), the
+// hidden activations ping-ponging between two shared-memory buffers.
+constexpr int FI_THREADS = 128;
+constexpr uint32_t FI_W1 = 0, FI_W2 = FI_W1 + 3 * 8192, FI_W3 = FI_W2 + 4 * 8192, FI_W4 = FI_W3 + 4 * 8192;
+constexpr uint32_t FI_X = FI_W4 + 4 * 1024, FI_HA = FI_X + 3 * 8192, FI_HB = FI_HA + 4 * 8192;
+constexpr uint32_t FI_SMEM = FI_HB + 4 * 8192;                      // 184,320 bytes
+constexpr uint32_t FI_WBYTES = FI_X;                                // weights: 94,208 bytes
+
+// packed offset of (row, col) inside one 128-row tile held in shared memory
+__device__ __forceinline__ uint32_t tile_off(int r, int c) {
+    return (uint32_t)(c >> 5) * 8192u + (uint32_t)(r >> 3) * 512u + (uint32_t)((c & 31) >> 3) * 128u +
+           (uint32_t)(r & 7) * 16u + (uint32_t)(c & 7) * 2u;
+}
+
+__device__ __forceinline__ void fi_store8(uint8_t* base, uint32_t off, const float* v) {
+    __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16_rn(v[i]);
+    *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(h);
+}
+
+// issue one layer: D[128 x N] = A (K columns, tile in smem) . B^T; b_chunk: bytes between the
+// 32-column chunks of B (8192, or 1024 for the compact 16-row W4)
+__device__ __forceinline__ void fi_layer_issue(uint32_t tmem, uint32_t a, uint32_t b, int K, uint32_t b_chunk,
+                                               uint32_t idesc, uint32_t bar) {
+    for (int j = 0; j < K / 16; ++j) {
+        const uint32_t ao = a + (uint32_t)(j >> 1) * 8192u + (uint32_t)(j & 1) * 256u;
+        const uint32_t bo = b + (uint32_t)(j >> 1) * b_chunk + (uint32_t)(j & 1) * 256u;
+        tc::mma_bf16(tmem, tc::smem_desc(ao), tc::smem_desc(bo), idesc, j > 0 ? 1u : 0u);
+    }
+    tc::mma_commit(bar);
+}
+
+__global__ void __launch_bounds__(FI_THREADS, 1)
+k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, const int* __restrict__ nbn, int nb_base,
+                int v0, int n, const uint8_t* __restrict__ W1p, const uint8_t* __restrict__ W2p,
+                const uint8_t* __restrict__ W3p, const uint8_t* __restrict__ W4p, const float* __restrict__ params,
+                float* __restrict__ Y, int ldy, int* err) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ int fail;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = threadIdx.x;
+    const uint32_t sb = tc::smem_u32(sm);
+    const uint32_t bar_w = tc::smem_u32(&bars[0]), bar_m = tc::smem_u32(&bars[1]);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(bar_w, 1);
+        tc::mbar_init(bar_m, 1);
+        tc::mbar_init_fence();
+        fail = 0;
+    }
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    if (threadIdx.x == 0) {
+        tc::mbar_expect_tx(bar_w, FI_WBYTES);
+        tc::bulk_g2s(sb + FI_W1, W1p, 3 * 8192, bar_w);
+        tc::bulk_g2s(sb + FI_W2, W2p, 4 * 8192, bar_w);
+        tc::bulk_g2s(sb + FI_W3, W3p, 4 * 8192, bar_w);
+        for (int c = 0; c < 4; ++c) tc::bulk_g2s(sb + FI_W4 + 1024u * c, W4p + (size_t)c * 8192, 1024, bar_w);
+    }
+    if (!tc::mbar_wait(bar_w, 0)) {
+        if (lane == 0) { atomicExch(err, tc::TC_TIMEOUT_LOAD); fail = 1; }
+    }
+    __syncthreads();
+    const uint32_t id128 = tc::idesc_bf16(HID), id16 = tc::idesc_bf16(OUTP);
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    uint32_t phase = 0;
+    const int ntiles = (n + 127) / 128;
+    for (int tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x) {
+        // ---- inputs of this thread's vertex -> packed rows of X
+        const int i = tile * 128 + r;
+        {
+            float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f);
+            const int* list = nullptr;
+            int cnt = 0;
+            if (i < n) {
+                c0 = pos[v0 + i];
+                list = nb + (size_t)(v0 + i - nb_base) * MAX_NB;
+                cnt = nbn[v0 + i - nb_base];
+            }
+            // each ring vertex loaded once; the 96 inputs stay in registers (fully unrolled)
+            float f[IN];
+            float mm = 0.f;
+#pragma unroll
+            for (int a = 0; a < MAX_NB; ++a) {
+                float dx = 0.f, dy = 0.f, dz = 0.f;
+                if (a < cnt) {
+                    const float4 q = pos[list[a]];
+                    dx = q.x - c0.x; dy = q.y - c0.y; dz = q.z - c0.z;
+                    mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
+                }
+                f[3 * a] = dx; f[3 * a + 1] = dy; f[3 * a + 2] = dz;
+            }
+            const float inv = mm > 0.f ? 1.f / mm : 0.f;
+#pragma unroll
+            for (int c = 0; c < IN; ++c) f[c] = f[c] * inv;
+#pragma unroll
+            for (int g = 0; g < IN / 8; ++g) fi_store8(sm + FI_X, tile_off(r, 8 * g), f + 8 * g);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc::tc_fence_before();
+        __syncthreads();
+        // ---- layers 1..3: H = relu(A W^T + b) -> bf16, packed in shared memory
+        const uint32_t srcA[3] = { FI_X, FI_HA, FI_HB }, dstH[3] = { FI_HA, FI_HB, FI_HA };
+        const uint32_t srcW[3] = { FI_W1, FI_W2, FI_W3 };
+        const int Ks[3] = { IN, HID, HID };
+        const int boff[3] = { OFF_B1, OFF_B2, OFF_B3 };
+        for (int l = 0; l < 4 && !fail; ++l) {
+            if (threadIdx.x == 0) {
+                tc::tc_fence_after();
+                if (l < 3) fi_layer_issue(tmem, sb + srcA[l], sb + srcW[l], Ks[l], 8192u, id128, bar_m);
+                else fi_layer_issue(tmem, sb + FI_HA, sb + FI_W4, HID, 1024u, id16, bar_m);
+            }
+            __syncwarp();
+            if (!tc::mbar_wait(bar_m, phase)) {
+                if (lane == 0) { atomicExch(err, tc::TC_TIMEOUT_MMA); fail = 1; }
+            }
+            phase ^= 1u;
+            tc::tc_fence_after();
+            if (l < 3) {
+                const float* bias = params + boff[l];
+#pragma unroll 1
+                for (int c = 0; c < HID; c += 16) {
+                    float v[16];
+                    tc::tmem_ld16(lane_addr + (uint32_t)c, v);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) v[e] = i < n ? fmaxf(v[e] + bias[c + e], 0.f) : 0.f;
+                    fi_store8(sm + dstH[l], tile_off(r, c), v);
+                    fi_store8(sm + dstH[l], tile_off(r, c + 8), v + 8);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            } else {
+                float v[16];
+                tc::tmem_ld16(lane_addr, v);
+                if (i < n) {
+                    const float* b4 = params + OFF_B4;
+                    float* y = Y + (size_t)i * ldy;
+                    y[0] = v[0] + b4[0];
+                    y[1] = v[1] + b4[1];
+                    y[2] = v[2] + b4[2];
+                }
+            }
+            tc::tc_fence_before();
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 128);
+    }
+}
+
 }  // namespace
 
 // ---- Model ------------------------------------------------------------------------------------------
@@ -475,6 +635,18 @@ void Model::gather(Workspace& w, const float* feats, const float* targets, const
     VSDMO_CHECK_LAUNCH();
 }
 
+void Model::infer_tet(const float4* pos, const int* nb, const int* nbn, int nb_base, int v0, int n, float* Y,
+                      int ldy, cudaStream_t s) {
+    if (n <= 0) return;
+    const int tiles = (n + 127) / 128;
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_mlp_tet_infer<<<std::min(tiles, sms), FI_THREADS, FI_SMEM, s>>>(pos, nb, nbn, nb_base, v0, n, W1p.p, W2p.p, W3p.p,
+                                                                     W4p.p, params.p, Y, ldy, err.p);
+    VSDMO_CHECK_LAUNCH();
+}
+
 void Model::check(cudaStream_t s) {
     const int e = read_scalar(err.p, s);
     if (e) throw Error(VSDMO_E_TIMEOUT, "tensor-core GEMM wait expired (code " + std::to_string(e) + ")");
@@ -494,6 +666,7 @@ void prepare(cudaStream_t s) {
     cfg((const void*)k_gemm<IN, EPI_RAW>, tc::gemm_smem_bytes<IN>());
     cfg((const void*)k_gemm<32, EPI_RAW>, tc::gemm_smem_bytes<32>());
     cfg((const void*)k_gemm<64, EPI_RAW>, tc::gemm_smem_bytes<64>());
+    cfg((const void*)k_mlp_tet_infer, FI_SMEM);
 }
 
 // D [M x N] = A [M x K] . B [N x K]^T for the GEMM test entry point (FP32 in, BF16 operands)

@@ -57,6 +57,10 @@ struct Model {
     void gather(Workspace& w, const float* feats, const float* targets, const int* idx, int B, int n_valid,
                 bool training, cudaStream_t s);
     void check(cudaStream_t s);
+    // fused inference for tet vertices [v0, v0 + n): ring features from the neighbour table
+    // (nb / nbn index vertices from nb_base) -> network -> Y [n x ldy] (first 3 columns)
+    void infer_tet(const float4* pos, const int* nb, const int* nbn, int nb_base, int v0, int n, float* Y, int ldy,
+                   cudaStream_t s);
 };
 
 void prepare(cudaStream_t s);
