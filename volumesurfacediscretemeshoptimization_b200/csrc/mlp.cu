@@ -266,15 +266,18 @@ __global__ void k_sum(const float* a, int n, float* out) {
 
 // ---- fused inference for the learned tet search --------------------------------------------------
 // One persistent CTA per SM keeps the packed BF16 weights in shared memory (loaded once by bulk
-// copies) and loops over tiles of 128 vertices: each thread builds its vertex's 96 inputs from
-// the ring-vertex table straight into the packed A operand in shared memory, then the four
-// layers run back to back on the tensor cores (one 128-column TMEM accumulator, reused), the
-// hidden activations ping-ponging between two shared-memory buffers.
-constexpr int FI_THREADS = 128;
+// copies) and runs FI_GROUPS independent groups of four warps. A group owns one 128-column
+// TMEM accumulator and one 32 KB activation buffer and loops over tiles of 128 vertices: each
+// thread builds its vertex's 96 inputs from the ring-vertex table straight into the packed A
+// operand, then the four layers run back to back on the tensor cores, every layer's
+// epilogue overwriting the buffer its own MMAs have finished reading. Groups synchronise on
+// their own named barrier, so one group's tensor-core phase overlaps another's feature gather.
+constexpr int FI_GROUPS = 4;
+constexpr int FI_THREADS = 128 * FI_GROUPS;
 constexpr uint32_t FI_W1 = 0, FI_W2 = FI_W1 + 3 * 8192, FI_W3 = FI_W2 + 4 * 8192, FI_W4 = FI_W3 + 4 * 8192;
-constexpr uint32_t FI_X = FI_W4 + 4 * 1024, FI_HA = FI_X + 3 * 8192, FI_HB = FI_HA + 4 * 8192;
-constexpr uint32_t FI_SMEM = FI_HB + 4 * 8192;                      // 184,320 bytes
-constexpr uint32_t FI_WBYTES = FI_X;                                // weights: 94,208 bytes
+constexpr uint32_t FI_WBYTES = FI_W4 + 4 * 1024;                    // weights: 94,208 bytes
+constexpr uint32_t FI_BUF = FI_WBYTES;                              // + 32 KB per group
+constexpr uint32_t FI_SMEM = FI_BUF + FI_GROUPS * 4 * 8192;         // 225,280 bytes
 
 // packed offset of (row, col) inside one 128-row tile held in shared memory
 __device__ __forceinline__ uint32_t tile_off(int r, int c) {
@@ -287,6 +290,10 @@ __device__ __forceinline__ void fi_store8(uint8_t* base, uint32_t off, const flo
 #pragma unroll
     for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16_rn(v[i]);
     *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(h);
+}
+
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(128) : "memory");
 }
 
 // issue one layer: D[128 x N] = A (K columns, tile in smem) . B^T; b_chunk: bytes between the
@@ -307,23 +314,23 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
                 const uint8_t* __restrict__ W3p, const uint8_t* __restrict__ W4p, const float* __restrict__ params,
                 float* __restrict__ Y, int ldy, int* err) {
     extern __shared__ __align__(1024) uint8_t sm[];
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[1 + FI_GROUPS];
     __shared__ uint32_t tmem_slot;
-    __shared__ int fail;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = threadIdx.x;
+    __shared__ int fail[FI_GROUPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = threadIdx.x >> 7, r = threadIdx.x & 127;       // group, row of the tile
     const uint32_t sb = tc::smem_u32(sm);
-    const uint32_t bar_w = tc::smem_u32(&bars[0]), bar_m = tc::smem_u32(&bars[1]);
+    const uint32_t bar_w = tc::smem_u32(&bars[0]), bar_m = tc::smem_u32(&bars[1 + g]);
     if (threadIdx.x == 0) {
-        tc::mbar_init(bar_w, 1);
-        tc::mbar_init(bar_m, 1);
+        for (int i = 0; i < 1 + FI_GROUPS; ++i) tc::mbar_init(tc::smem_u32(&bars[i]), 1);
         tc::mbar_init_fence();
-        fail = 0;
+        for (int i = 0; i < FI_GROUPS; ++i) fail[i] = 0;
     }
-    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128);
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128 * FI_GROUPS);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
-    const uint32_t tmem = tmem_slot;
+    const uint32_t tmem = tmem_slot + 128u * g;
     if (threadIdx.x == 0) {
         tc::mbar_expect_tx(bar_w, FI_WBYTES);
         tc::bulk_g2s(sb + FI_W1, W1p, 3 * 8192, bar_w);
@@ -331,16 +338,21 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
         tc::bulk_g2s(sb + FI_W3, W3p, 4 * 8192, bar_w);
         for (int c = 0; c < 4; ++c) tc::bulk_g2s(sb + FI_W4 + 1024u * c, W4p + (size_t)c * 8192, 1024, bar_w);
     }
-    if (!tc::mbar_wait(bar_w, 0)) {
-        if (lane == 0) { atomicExch(err, tc::TC_TIMEOUT_LOAD); fail = 1; }
+    if (!tc::mbar_wait(bar_w, 0) && lane == 0) {
+        atomicExch(err, tc::TC_TIMEOUT_LOAD);
+        fail[g] = 1;
     }
     __syncthreads();
+    uint8_t* buf = sm + FI_BUF + (uint32_t)g * 4 * 8192;
+    const uint32_t sbuf = sb + FI_BUF + (uint32_t)g * 4 * 8192;
     const uint32_t id128 = tc::idesc_bf16(HID), id16 = tc::idesc_bf16(OUTP);
-    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const bool issuer = r == 0;
     uint32_t phase = 0;
     const int ntiles = (n + 127) / 128;
-    for (int tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x) {
-        // ---- inputs of this thread's vertex -> packed rows of X
+    // group-major tile order: every CTA's first group gets a tile before any second group does
+    for (int tile = g * gridDim.x + blockIdx.x; tile < ntiles && !fail[g]; tile += gridDim.x * FI_GROUPS) {
+        // ---- inputs of this thread's vertex -> packed rows of X (in the group's buffer)
         const int i = tile * 128 + r;
         {
             float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -368,29 +380,29 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
 #pragma unroll
             for (int c = 0; c < IN; ++c) f[c] = f[c] * inv;
 #pragma unroll
-            for (int g = 0; g < IN / 8; ++g) fi_store8(sm + FI_X, tile_off(r, 8 * g), f + 8 * g);
+            for (int q = 0; q < IN / 8; ++q) fi_store8(buf, tile_off(r, 8 * q), f + 8 * q);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc::tc_fence_before();
-        __syncthreads();
-        // ---- layers 1..3: H = relu(A W^T + b) -> bf16, packed in shared memory
-        const uint32_t srcA[3] = { FI_X, FI_HA, FI_HB }, dstH[3] = { FI_HA, FI_HB, FI_HA };
+        group_sync(g);
         const uint32_t srcW[3] = { FI_W1, FI_W2, FI_W3 };
         const int Ks[3] = { IN, HID, HID };
         const int boff[3] = { OFF_B1, OFF_B2, OFF_B3 };
-        for (int l = 0; l < 4 && !fail; ++l) {
-            if (threadIdx.x == 0) {
+        for (int l = 0; l < 4; ++l) {
+            if (issuer) {
                 tc::tc_fence_after();
-                if (l < 3) fi_layer_issue(tmem, sb + srcA[l], sb + srcW[l], Ks[l], 8192u, id128, bar_m);
-                else fi_layer_issue(tmem, sb + FI_HA, sb + FI_W4, HID, 1024u, id16, bar_m);
+                if (l < 3) fi_layer_issue(tmem, sbuf, sb + srcW[l], Ks[l], 8192u, id128, bar_m);
+                else fi_layer_issue(tmem, sbuf, sb + FI_W4, HID, 1024u, id16, bar_m);
             }
             __syncwarp();
-            if (!tc::mbar_wait(bar_m, phase)) {
-                if (lane == 0) { atomicExch(err, tc::TC_TIMEOUT_MMA); fail = 1; }
+            if (!tc::mbar_wait(bar_m, phase) && lane == 0) {
+                atomicExch(err, tc::TC_TIMEOUT_MMA);
+                fail[g] = 1;
             }
             phase ^= 1u;
             tc::tc_fence_after();
             if (l < 3) {
+                // the MMAs are done with the buffer: the activations overwrite it
                 const float* bias = params + boff[l];
 #pragma unroll 1
                 for (int c = 0; c < HID; c += 16) {
@@ -398,8 +410,8 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
                     tc::tmem_ld16(lane_addr + (uint32_t)c, v);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) v[e] = i < n ? fmaxf(v[e] + bias[c + e], 0.f) : 0.f;
-                    fi_store8(sm + dstH[l], tile_off(r, c), v);
-                    fi_store8(sm + dstH[l], tile_off(r, c + 8), v + 8);
+                    fi_store8(buf, tile_off(r, c), v);
+                    fi_store8(buf, tile_off(r, c + 8), v + 8);
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             } else {
@@ -414,13 +426,14 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
                 }
             }
             tc::tc_fence_before();
-            __syncthreads();
+            group_sync(g);
+            if (fail[g]) break;
         }
     }
     __syncthreads();
     if (warp == 0) {
         tc::tc_fence_after();
-        tc::tmem_dealloc(tmem, 128);
+        tc::tmem_dealloc(tmem_slot, 128 * FI_GROUPS);
     }
 }
 
