@@ -76,7 +76,8 @@ typedef enum vsdmo_array_id {
     VSDMO_A_HE_ROWPTR = 4,       /* int32 [nSurf+1]   halfedge CSR, CCW fan per vertex         */
     VSDMO_A_HALFEDGES = 5,       /* int32 [nHE*4]     {target, opposite, face, next}           */
     VSDMO_A_HF_ROWPTR = 6,       /* int32 [nV+1]      halfface CSR (tet)                       */
-    VSDMO_A_HALFFACES = 7,       /* int32 [4nT*3]     face opposite to the vertex, oriented    */
+    VSDMO_A_HALFFACES = 7,       /* int32 [4nT*3]     face opposite to the vertex, oriented;   */
+                                 /*       hex: [8nH*7] the other corners of each halfhex      */
     VSDMO_A_COL_FREE = 8,        /* int32 [nColorsFree+1]    colour offsets, free surface      */
     VSDMO_A_COL_FEATURE = 9,     /* int32 [nColorsFeature+1] colour offsets, feature vertices  */
     VSDMO_A_COL_INNER = 10,      /* int32 [nColorsInner+1]   colour offsets, volume interior   */
@@ -135,7 +136,9 @@ VSDMO_API vsdmo_status vsdmo_params_default(int elem_type, vsdmo_params* out);
 VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_vertices,
                                          const int32_t* elems, int n_elems, int mem_space,
                                          uint32_t color_seed, void* cuda_stream, vsdmo_mesh_t* out);
-/* Replaces the DMOMeshTri / DMOMeshTet destructors (mesh/DMOMeshBase.h:132-142). */
+/* Replaces the DMOMeshTri / DMOMeshTet destructors (mesh/DMOMeshBase.h:132-142). While
+ * optimisers created on the mesh are alive the release is deferred to the destruction of the
+ * last of them (the reference's DMO classes hold a reference to their mesh). */
 VSDMO_API void vsdmo_mesh_destroy(vsdmo_mesh_t mesh);
 /* Counts the reference keeps as public members of DMOMeshBase / DMOMeshTet
  * (mesh/DMOMeshBase.h:80-94, mesh/DMOMeshTet.h:145-151): nVertices, nVerticesSurf, ...   */
@@ -162,7 +165,8 @@ VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* 
 /* Replaces DMOTetClass / DMOTriFlatClass / DMOTriClass / DMOQuadClass construction + init()
  * (dmo/DMOTet.cu:82-125, dmo/DMOTriFlat.cu:84-126, dmo/DMOTri.cu:80-126, dmo/DMOQuad.cu:78-123).
  * Tri meshes that are not flat (or flat = 0) and quad meshes get the surface optimiser; it
- * needs a mesh without feature vertices (VSDMO_E_UNSUPPORTED otherwise). */
+ * needs a mesh without feature vertices (VSDMO_E_UNSUPPORTED otherwise). Hex meshes get the
+ * interior search of DMOHexClass (dmo/DMOHex.cu, k_optimizeHierarchicalInnerHex). */
 VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* params, vsdmo_opt_t* out);
 VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt);
 /* n_iter calls of doIteration() (dmo/DMOTet.cu:128-170, dmo/DMOTriFlat.cu:129-166,

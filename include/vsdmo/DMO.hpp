@@ -8,6 +8,7 @@
 //   DMO::DMOBaseClass, DMOTetClass, DMOTriFlatClass dmo/DMOBase.h:23-88, dmo/DMOTet.h:21-62,
 //                                                   dmo/DMOTriFlat.h:19-51
 //   DMO::DMOTriClass, DMOQuadClass (surfaces)       dmo/DMOTri.h, dmo/DMOQuad.h
+//   DMOMeshHex, DMO::DMOHexClass                    mesh/DMOMeshHex.h, dmo/DMOHex.h
 // Header-only; link against libvsdmo.so. Errors surface as DMO::Error exceptions carrying the
 // vsdmo_status (the reference exits through gpuErrchk or throws 1 instead).
 #pragma once
@@ -92,6 +93,12 @@ public:
         : DMOMesh(VSDMO_TET, points, nV, tets, nT, memSpace) {}
 };
 
+class DMOMeshHex : public DMOMesh {
+public:
+    DMOMeshHex(int nV, int nH, const float* points, const int32_t* hexes, int memSpace = VSDMO_HOST)
+        : DMOMesh(VSDMO_HEX, points, nV, hexes, nH, memSpace) {}
+};
+
 struct DMOMeshTriFactory {
     static std::shared_ptr<DMOMeshTri> create(int nVS, int nT, const float* points, const int32_t* tris,
                                               int memSpace = VSDMO_HOST) {
@@ -103,6 +110,13 @@ struct DMOMeshQuadFactory {
     static std::shared_ptr<DMOMeshQuad> create(int nVS, int nQ, const float* points, const int32_t* quads,
                                                int memSpace = VSDMO_HOST) {
         return std::make_shared<DMOMeshQuad>(nVS, nQ, points, quads, memSpace);
+    }
+};
+
+struct DMOMeshHexFactory {
+    static std::shared_ptr<DMOMeshHex> create(int nV, int nH, const float* points, const int32_t* hexes,
+                                              int memSpace = VSDMO_HOST) {
+        return std::make_shared<DMOMeshHex>(nV, nH, points, hexes, memSpace);
     }
 };
 
@@ -169,6 +183,14 @@ public:
     DMOTriFlatClass(DMOMeshTri& mesh, QualityCriterium q = QualityCriterium::MEAN_RATIO, float gridScale = 0.5f,
                     int n_iter = 30, bool fixBoundary = true)
         : DMOBaseClass(mesh, q, gridScale, n_iter, 1, fixBoundary) {}
+};
+
+// interior hex DMO (dmo/DMOHex.h), boundary fixed
+class DMOHexClass : public DMOBaseClass {
+public:
+    DMOHexClass(DMOMeshHex& mesh, QualityCriterium q = QualityCriterium::MEAN_RATIO, float gridScale = 0.5f,
+                int n_iter = 30, bool fixBoundary = true)
+        : DMOBaseClass(mesh, q, gridScale, n_iter, -1, fixBoundary) {}
 };
 
 // surface triangle DMO (meshes without feature vertices)

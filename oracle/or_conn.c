@@ -415,7 +415,7 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
     int* inv = (int*)xc((size_t)nTot, sizeof(int));
     permute_range(0, nS, order, m->xyz, old_of_cur, m->isB1, m->isFeat, NULL, inv, nTot);
     remap(m->nTris * m->fk, m->tris, inv, nS);
-    if (m->type == OR_TET) remap(m->nE * 4, m->elems, inv, nS);
+    if (m->type == OR_TET || m->type == OR_HEX) remap(m->nE * m->k, m->elems, inv, nS);
     free(order); free(inv);
     int nFree = 0;
     for (int v = 0; v < nS; ++v) if (!m->isFeat[v]) nFree++;
@@ -430,11 +430,19 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
             else { m->col_feature = offs; m->nColFeature = 0; }
             continue;
         }
-        int cap = m->type == OR_TET ? 12 * m->nE : (m->fk == 4 ? 12 : 6) * m->nTris;
+        int cap = m->type == OR_TET ? 12 * m->nE : m->type == OR_HEX ? 56 * m->nE : (m->fk == 4 ? 12 : 6) * m->nTris;
         int* ps = (int*)xc((size_t)cap, sizeof(int));
         int* pd = (int*)xc((size_t)cap, sizeof(int));
         int np = 0;
-        if (m->type == OR_TET) {
+        if (m->type == OR_HEX) {
+            /* every vertex pair of a hexahedron (mesh/MeshGPUCommon.cu:982-1037) */
+            for (int t = 0; t < m->nE; ++t)
+                for (int i = 0; i < 7; ++i)
+                    for (int j = i + 1; j < 8; ++j) {
+                        int a = m->elems[8 * t + i] - lo, b = m->elems[8 * t + j] - lo;
+                        if (a >= 0 && a < num && b >= 0 && b < num) { ps[np] = a; pd[np++] = b; ps[np] = b; pd[np++] = a; }
+                    }
+        } else if (m->type == OR_TET) {
             static const int E[6][2] = { {0,1},{0,2},{0,3},{1,2},{1,3},{2,3} };
             for (int t = 0; t < m->nE; ++t) for (int e = 0; e < 6; ++e) {
                 int a = m->elems[4 * t + E[e][0]] - lo, b = m->elems[4 * t + E[e][1]] - lo;
@@ -456,8 +464,9 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
         }
         int* offs;
         int nc = color_and_sort_range(lo, num, np, ps, pd, seed, m->xyz, old_of_cur, m->isB1, m->isFeat, NULL,
-                                      nTot, m->tris, m->nTris * m->fk, m->type == OR_TET ? m->elems : NULL,
-                                      m->type == OR_TET ? m->nE * 4 : 0, &offs);
+                                      nTot, m->tris, m->nTris * m->fk,
+                                      (m->type == OR_TET || m->type == OR_HEX) ? m->elems : NULL,
+                                      (m->type == OR_TET || m->type == OR_HEX) ? m->nE * m->k : 0, &offs);
         if (part == 0) { m->col_free = offs; m->nColFree = nc; }
         else { m->col_feature = offs; m->nColFeature = nc; }
         free(ps); free(pd);
@@ -479,6 +488,116 @@ static tri3 smallest_first(int a, int b, int c) {
     return t;
 }
 
+typedef struct { int v[4]; } quad4;
+
+/* getQuadSmallestFirst / k_reorderVertices for quads (mesh/MeshGPUCommon.cu:37-54) */
+static quad4 quad_smallest_first(int a, int b, int c, int d) {
+    quad4 q;
+    if (b < a && b < c && b < d) { q.v[0] = b; q.v[1] = c; q.v[2] = d; q.v[3] = a; }
+    else if (c < a && c < b && c < d) { q.v[0] = c; q.v[1] = d; q.v[2] = a; q.v[3] = b; }
+    else if (d < a && d < b && d < c) { q.v[0] = d; q.v[1] = a; q.v[2] = b; q.v[3] = c; }
+    else { q.v[0] = a; q.v[1] = b; q.v[2] = c; q.v[3] = d; }
+    return q;
+}
+
+static int cmp_quad(const void* A, const void* B) {
+    const quad4* a = (const quad4*)A; const quad4* b = (const quad4*)B;
+    for (int i = 0; i < 4; ++i) { if (a->v[i] < b->v[i]) return -1; if (a->v[i] > b->v[i]) return 1; }
+    return 0;
+}
+
+/* halfhex of corner j: the other seven corners (k_constructHalfhexesNew,
+ * mesh/MeshGPUCommon.cu:1334-1368) */
+static const int HALFHEX[8][7] = {
+    { 1, 2, 3, 4, 5, 6, 7 }, { 5, 6, 2, 0, 4, 7, 3 }, { 6, 7, 3, 1, 5, 4, 0 }, { 7, 4, 0, 2, 6, 5, 1 },
+    { 0, 3, 7, 5, 1, 2, 6 }, { 4, 7, 6, 1, 0, 3, 2 }, { 5, 4, 7, 2, 1, 0, 3 }, { 6, 5, 4, 3, 2, 1, 0 } };
+
+/* MeshHexGPU::init (mesh/MeshHexGPU.cu:35-43): boundary quads, boundary-first order, interior
+ * colouring, the quad surface, halfhexes */
+static int build_hex(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, int err_len) {
+    const int nV = m->nV, nE = m->nE;
+    m->fk = 4;
+    int nF = 6 * nE;
+    quad4* f = (quad4*)xc((size_t)nF, sizeof(quad4));
+    for (int t = 0; t < nE; ++t) {
+        const int* v = m->elems + 8 * t;
+        f[6 * t + 0] = quad_smallest_first(v[0], v[1], v[2], v[3]);
+        f[6 * t + 1] = quad_smallest_first(v[1], v[5], v[6], v[2]);
+        f[6 * t + 2] = quad_smallest_first(v[3], v[2], v[6], v[7]);
+        f[6 * t + 3] = quad_smallest_first(v[4], v[0], v[3], v[7]);
+        f[6 * t + 4] = quad_smallest_first(v[1], v[0], v[4], v[5]);
+        f[6 * t + 5] = quad_smallest_first(v[5], v[4], v[7], v[6]);
+    }
+    qsort(f, (size_t)nF, sizeof(quad4), cmp_quad);
+    /* k_markDuplicateQuads in index order */
+    for (int idx = 0; idx < nF; ++idx) {
+        quad4* q = &f[idx];
+        if (q->v[1] < q->v[3]) {
+            for (int i = idx + 1; i < nF; ++i) {
+                quad4* it = &f[i];
+                if (it->v[0] > q->v[0]) break;
+                if (q->v[0] == it->v[0] && q->v[1] == it->v[3] && q->v[2] == it->v[2] && q->v[3] == it->v[1]) {
+                    q->v[0] = -1; it->v[0] = -1; break;
+                }
+            }
+        }
+    }
+    int nB = 0;
+    for (int i = 0; i < nF; ++i) if (f[i].v[0] != -1) nB++;
+    m->nTris = nB;
+    m->tris = (int*)xc((size_t)nB * 4, sizeof(int));
+    for (int i = 0, w = 0; i < nF; ++i) if (f[i].v[0] != -1) { memcpy(m->tris + 4 * w, f[i].v, 4 * sizeof(int)); w++; }
+    free(f);
+    m->isB2 = (uint8_t*)xc((size_t)nV, 1);
+    for (int i = 0; i < 4 * nB; ++i) m->isB2[m->tris[i]] = 1;
+    int* order = (int*)xc((size_t)nV, sizeof(int));
+    stable_partition(nV, m->isB2, 1, order);
+    int* inv = (int*)xc((size_t)nV, sizeof(int));
+    permute_range(0, nV, order, m->xyz, old_of_cur, m->isB2, NULL, NULL, inv, nV);
+    remap(4 * nB, m->tris, inv, nV);
+    remap(8 * nE, m->elems, inv, nV);
+    free(order); free(inv);
+    int nS = 0;
+    for (int i = 0; i < nV; ++i) if (m->isB2[i]) nS++;
+    m->nSurf = nS;
+    const int nI = nV - nS;
+    if (nI > 0) {
+        int* ps = (int*)xc((size_t)56 * nE, sizeof(int));
+        int* pd = (int*)xc((size_t)56 * nE, sizeof(int));
+        int np = 0;
+        for (int t = 0; t < nE; ++t)
+            for (int i = 0; i < 7; ++i)
+                for (int j = i + 1; j < 8; ++j) {
+                    int a = m->elems[8 * t + i], b = m->elems[8 * t + j];
+                    if (!m->isB2[a] && !m->isB2[b]) { ps[np] = a - nS; pd[np++] = b - nS; ps[np] = b - nS; pd[np++] = a - nS; }
+                }
+        m->nColInner = color_and_sort_range(nS, nI, np, ps, pd, seed, m->xyz, old_of_cur, m->isB2, NULL, NULL,
+                                            nV, m->tris, 4 * nB, m->elems, 8 * nE, &m->col_inner);
+        free(ps); free(pd);
+    } else {
+        m->col_inner = (int*)xc(1, sizeof(int)); m->col_inner[0] = nS; m->nColInner = 0;
+    }
+    if (nS > 0 && surface_init(m, old_of_cur, seed, err, err_len)) return -1;
+    /* halfhexes: stable by vertex => rows in hexahedron order */
+    const int nH = 8 * nE;
+    int* keys = (int*)xc((size_t)nH, sizeof(int));
+    for (int i = 0; i < nH; ++i) keys[i] = m->elems[i];
+    int* ord = (int*)xc((size_t)nH, sizeof(int));
+    m->hf_rowptr = (int*)xc((size_t)nV + 1, sizeof(int));
+    counting_sort(nH, keys, nV, ord, m->hf_rowptr);
+    m->hf = (int*)xc((size_t)nH * 7, sizeof(int));
+    for (int i = 0; i < nH; ++i) {
+        const int t = ord[i] / 8, j = ord[i] % 8;
+        const int* v = m->elems + 8 * t;
+        for (int a = 0; a < 7; ++a) m->hf[7 * i + a] = v[HALFHEX[j][a]];
+    }
+    int mx = 0;
+    for (int v = 0; v < nV; ++v) if (m->hf_rowptr[v + 1] - m->hf_rowptr[v] > mx) mx = m->hf_rowptr[v + 1] - m->hf_rowptr[v];
+    m->maxTets = mx;
+    free(keys); free(ord);
+    return 0;
+}
+
 static int cmp_tri(const void* A, const void* B) {
     const tri3* a = (const tri3*)A; const tri3* b = (const tri3*)B;
     for (int i = 0; i < 3; ++i) { if (a->v[i] < b->v[i]) return -1; if (a->v[i] > b->v[i]) return 1; }
@@ -488,9 +607,9 @@ static int cmp_tri(const void* A, const void* B) {
 or_mesh* or_mesh_build(int elem_type, int nV, const float* xyz, int nE, const int32_t* elems,
                        uint32_t seed, char* err, int err_len) {
     if (err && err_len > 0) err[0] = 0;
-    if (elem_type != OR_TRI && elem_type != OR_TET && elem_type != OR_QUAD) { if (err) snprintf(err, err_len, "element type not supported by the oracle"); return NULL; }
+    if (elem_type != OR_TRI && elem_type != OR_TET && elem_type != OR_QUAD && elem_type != OR_HEX) { if (err) snprintf(err, err_len, "element type not supported by the oracle"); return NULL; }
     if (nV <= 0 || nE <= 0 || !xyz || !elems) { if (err) snprintf(err, err_len, "empty mesh"); return NULL; }
-    int k = elem_type == OR_TRI ? 3 : 4;
+    int k = elem_type == OR_TRI ? 3 : elem_type == OR_HEX ? 8 : 4;
     for (long i = 0; i < (long)nE * k; ++i) if (elems[i] < 0 || elems[i] >= nV) { if (err) snprintf(err, err_len, "element index out of range"); return NULL; }
     or_mesh* m = (or_mesh*)xc(1, sizeof(or_mesh));
     m->type = elem_type; m->nV = nV; m->nE = nE; m->k = k;
@@ -510,6 +629,8 @@ or_mesh* or_mesh_build(int elem_type, int nV, const float* xyz, int nE, const in
         m->col_inner = (int*)xc(1, sizeof(int)); m->col_inner[0] = nV;
         if (surface_init(m, old_of_cur, seed, err, err_len)) goto fail;
         memcpy(m->elems, m->tris, sizeof(int) * k * (size_t)nE);
+    } else if (elem_type == OR_HEX) {
+        if (build_hex(m, old_of_cur, seed, err, err_len)) goto fail;
     } else {
         m->fk = 3;
         int nF = 4 * nE;
@@ -636,7 +757,7 @@ long or_mesh_array_len(const or_mesh* m, int id) {
     case OR_A_HE_ROWPTR: return m->he_rowptr ? m->nSurf + 1L : 0;
     case OR_A_HALFEDGES: return 4L * m->nHE;
     case OR_A_HF_ROWPTR: return m->hf_rowptr ? m->nV + 1L : 0;
-    case OR_A_HALFFACES: return m->hf ? 12L * m->nE : 0;
+    case OR_A_HALFFACES: return m->hf ? (m->type == OR_HEX ? 56L : 12L) * m->nE : 0;
     case OR_A_COL_FREE: return m->col_free ? m->nColFree + 1L : 0;
     case OR_A_COL_FEATURE: return m->col_feature ? m->nColFeature + 1L : 0;
     case OR_A_COL_INNER: return m->col_inner ? m->nColInner + 1L : 0;

@@ -74,6 +74,12 @@ def lib():
         L.or_surface_qualities_f64.argtypes = [P, P, P]
         L.or_optimize_surf_f32.argtypes = [P, P, I, F, I, P, P]
         L.or_optimize_surf_f64.argtypes = [P, P, I, D, I, P, P]
+        L.or_dmo_hex_f32.argtypes = [P, P, I, I, F, I]
+        L.or_dmo_hex_f64.argtypes = [P, P, I, I, D, P, I]
+        L.or_hex_qualities_f32.argtypes = [P, P, P]
+        L.or_hex_qualities_f64.argtypes = [P, P, P]
+        L.or_optimize_hex_f32.argtypes = [P, P, I, F, I, P, P]
+        L.or_optimize_hex_f64.argtypes = [P, P, I, D, I, P, P]
         L.or_q_tet_mean_ratio_f64.restype = D
         L.or_q_tet_mean_ratio_f64.argtypes = [P, P, P, P]
         L.or_q_tet_mean_ratio_f32.restype = F
@@ -125,7 +131,7 @@ class OracleMesh:
 
     def color_ranges(self):
         """(pass, start, end) of every colour class in doIteration order."""
-        if self.elem_type == TET:
+        if self.elem_type in (TET, HEX):
             off = self.array(A_COL_INNER)
         else:
             off = self.array(A_COL_FREE)
@@ -134,7 +140,7 @@ class OracleMesh:
     # ---- DMO steps ----------------------------------------------------------------------
     def dmo_color_f32(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
         xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
-        fn = lib().or_dmo_tet_f32 if self.elem_type == TET else lib().or_dmo_tri2d_f32
+        fn = {TET: lib().or_dmo_tet_f32, HEX: lib().or_dmo_hex_f32}.get(self.elem_type, lib().or_dmo_tri2d_f32)
         fn(self.h, _p(xyz), v0, v1, grid_scale, nthreads)
         return xyz
 
@@ -147,7 +153,7 @@ class OracleMesh:
     def dmo_color_f64(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
         margin = np.zeros(max(v1 - v0, 1), dtype=np.float64)
-        fn = lib().or_dmo_tet_f64 if self.elem_type == TET else lib().or_dmo_tri2d_f64
+        fn = {TET: lib().or_dmo_tet_f64, HEX: lib().or_dmo_hex_f64}.get(self.elem_type, lib().or_dmo_tri2d_f64)
         fn(self.h, _p(xyz), v0, v1, grid_scale, _p(margin), nthreads)
         return xyz, margin[: v1 - v0]
 
@@ -160,6 +166,8 @@ class OracleMesh:
         xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
         mn = np.zeros(n_iter); mean = np.zeros(n_iter)
         fn = lib().or_optimize_surf_f32 if self.is_surface else lib().or_optimize_f32
+        if self.elem_type == HEX:
+            fn = lib().or_optimize_hex_f32
         fn(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
         return xyz, mn, mean
 
@@ -167,6 +175,8 @@ class OracleMesh:
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
         mn = np.zeros(n_iter); mean = np.zeros(n_iter)
         fn = lib().or_optimize_surf_f64 if self.is_surface else lib().or_optimize_f64
+        if self.elem_type == HEX:
+            fn = lib().or_optimize_hex_f64
         fn(self.h, _p(xyz), n_iter, grid_scale, nthreads, _p(mn), _p(mean))
         return xyz, mn, mean
 
@@ -207,6 +217,8 @@ class OracleMesh:
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         q = np.zeros(self.info["nE"], dtype=np.float64)
         fn = lib().or_surface_qualities_f64 if self.is_surface else lib().or_element_qualities_f64
+        if self.elem_type == HEX:
+            fn = lib().or_hex_qualities_f64
         fn(self.h, _p(xyz), _p(q))
         return q
 
@@ -214,6 +226,8 @@ class OracleMesh:
         xyz = np.ascontiguousarray(xyz, dtype=np.float32)
         q = np.zeros(self.info["nE"], dtype=np.float32)
         fn = lib().or_surface_qualities_f32 if self.is_surface else lib().or_element_qualities_f32
+        if self.elem_type == HEX:
+            fn = lib().or_hex_qualities_f32
         fn(self.h, _p(xyz), _p(q))
         return q
 

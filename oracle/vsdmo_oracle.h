@@ -59,7 +59,8 @@ enum { OR_I_NV = 0, OR_I_NE, OR_I_NSURF, OR_I_NFEATURE, OR_I_NTRIS, OR_I_NHE,
        OR_I_NCOL_FREE, OR_I_NCOL_FEATURE, OR_I_NCOL_INNER, OR_I_MAX_HE, OR_I_MAX_TETS,
        OR_I_IS_FLAT, OR_I_COUNT };
 
-/* Build connectivity + colouring for a tri (elem_type OR_TRI) or tet (OR_TET) mesh.
+/* Build connectivity + colouring for a tri (OR_TRI), quad (OR_QUAD), tet (OR_TET) or hex
+ * (OR_HEX) mesh; for hex meshes the halfface arrays hold halfhexes (7 ints each).
  * Returns NULL on invalid input (err set to a message). */
 or_mesh* or_mesh_build(int elem_type, int nV, const float* xyz, int nE, const int32_t* elems,
                        uint32_t color_seed, char* err, int err_len);
@@ -99,6 +100,23 @@ void or_optimize_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale,
                      double* min_hist, double* mean_hist);
 void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
                      double* min_hist, double* mean_hist);
+
+/* ---- hexahedra (or_hex.c) ------------------------------------------------------------- */
+/* shapeMetricHex of corners v[0..7] (literal f64 / reference-order f32 with cbrtf) */
+double or_q_hex_f64(const double v[8][3]);
+float  or_q_hex_f32(const float v[8][3]);
+/* one colour class of interior hex vertices: f64 = the reference kernel literally (margin per
+ * vertex: smallest gap between competing keys), f32 = the product's arithmetic */
+void or_dmo_hex_f64(const or_mesh* m, double* xyz, int v0, int v1, double grid_scale, double* margin, int nthreads);
+void or_dmo_hex_f32(const or_mesh* m, float* xyz, int v0, int v1, float grid_scale, int nthreads);
+void or_hex_qualities_f64(const or_mesh* m, const double* xyz, double* q);
+void or_hex_qualities_f32(const or_mesh* m, const float* xyz, float* q);
+void or_optimize_hex_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale, int nthreads,
+                         double* min_hist, double* mean_hist);
+void or_optimize_hex_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
+                         double* min_hist, double* mean_hist);
+/* per-halfhex coefficients of the product arithmetic (43 floats, see or_hex.c) */
+void or_hex_coeffs_f32(const float r[7][3], float eps_s, float eps_a, float* out);
 
 /* ---- surfaces (tri / quad meshes without feature vertices) ----------------------------- */
 /* local surfaces: 16 values per surface vertex: p0[3] a, e0[3] b, e1[3] c, e2[3] numPoints  */

@@ -51,7 +51,9 @@ def test_host_only_calls(vsdmo):
     # argument errors are reported before any CUDA call
     assert lib.vsdmo_mesh_create(_capi.TET, None, 0, None, 0, 0, 1, None, C.byref(h)) == _capi.E_ARG
     assert b"empty" in lib.vsdmo_last_error()
-    assert lib.vsdmo_mesh_create(_capi.HEX, C.c_void_p(1), 1, C.c_void_p(1), 1, 0, 1, None, C.byref(h)) == _capi.E_UNSUPPORTED
+    assert lib.vsdmo_mesh_create(7, C.c_void_p(1), 1, C.c_void_p(1), 1, 0, 1, None, C.byref(h)) == _capi.E_ARG
+    assert b"element type" in lib.vsdmo_last_error()
+    assert lib.vsdmo_mesh_create(_capi.HEX, C.c_void_p(1), 1, C.c_void_p(1), 1, 5, 1, None, C.byref(h)) == _capi.E_ARG
     assert lib.vsdmo_opt_iterate(None, 1) == _capi.E_ARG
 
 

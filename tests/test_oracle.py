@@ -226,3 +226,38 @@ def test_one_color_step_matches_within_margin(oracle_mod):
         checked += int(clear.sum())
         x = x32
     assert checked > 0
+
+
+def test_hex_shape_metric_known_answers(oracle_mod):
+    """shapeMetricHex: 1 for the unit cube in the reference's corner order, 0 when a corner
+    is pushed through its opposite face, invariant under uniform scaling."""
+    import ctypes as C
+    import numpy as np
+    from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+    L = oracle_mod.lib()
+    L.or_q_hex_f64.restype = C.c_double
+    xyz, hx = G.hex_cube(1, seed=None)
+    v = np.ascontiguousarray(xyz[hx[0]], dtype=np.float64)
+    q = L.or_q_hex_f64(v.ctypes.data_as(C.c_void_p))
+    assert abs(q - 1.0) < 1e-12
+    w = v * 3.7
+    assert abs(L.or_q_hex_f64(np.ascontiguousarray(w).ctypes.data_as(C.c_void_p)) - 1.0) < 1e-12
+    bad = v.copy()
+    bad[0] = bad[4] + (bad[4] - bad[0]) * 0.5      # corner 0 pushed below the opposite face
+    assert L.or_q_hex_f64(bad.ctypes.data_as(C.c_void_p)) == 0.0
+
+
+def test_hex_oracle_fixed_point_and_progress(oracle_mod):
+    import numpy as np
+    from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+    xyz, hx = G.hex_cube(4, seed=None)
+    m = oracle_mod.OracleMesh(3, xyz, hx)
+    x, mn, _ = m.optimize_f32(m.xyz, 1)
+    assert np.array_equal(x, m.xyz) and abs(mn[0] - 1.0) < 1e-6
+    xyz, hx = G.hex_cube(4, seed=5)
+    m = oracle_mod.OracleMesh(3, xyz, hx)
+    q0 = m.element_qualities_f64(m.xyz.astype(np.float64))
+    x32, mn32, me32 = m.optimize_f32(m.xyz, 3)
+    x64, mn64, me64 = m.optimize_f64(m.xyz.astype(np.float64), 3)
+    assert me32[-1] > q0.mean() and mn32[-1] >= q0.min()
+    assert abs(mn32[-1] - mn64[-1]) < 1e-4 and abs(me32[-1] - me64[-1]) < 1e-4

@@ -32,9 +32,10 @@ import numpy as np
 from . import _capi
 from ._capi import VSDMOError, Params, check
 
-__all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshQuad", "DMOMeshTet", "DMOMeshTriFactory",
-           "DMOMeshQuadFactory", "DMOMeshTetFactory", "DMOTetClass", "DMOTriFlatClass", "DMOTriClass",
-           "DMOQuadClass", "ProposalModel", "VSDMOError", "Params", "default_params", "version"]
+__all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshQuad", "DMOMeshTet", "DMOMeshHex", "DMOMeshTriFactory",
+           "DMOMeshQuadFactory", "DMOMeshTetFactory", "DMOMeshHexFactory", "DMOTetClass", "DMOHexClass",
+           "DMOTriFlatClass", "DMOTriClass", "DMOQuadClass", "ProposalModel", "VSDMOError", "Params",
+           "default_params", "version"]
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -161,6 +162,13 @@ class DMOMeshTet(_Mesh):
     k = 4
 
 
+class DMOMeshHex(_Mesh):
+    """``DMOMeshHex`` (``mesh/DMOMeshHex.h``): hexahedral volume mesh (corner order of
+    ``meshgen.hex_cube``: 0-3 one face, 4-7 the opposite face, 4 below 0)."""
+    elem_type = _capi.HEX
+    k = 8
+
+
 class DMOMeshTriFactory:
     """``DMOMeshTriFactory::create`` (``mesh/MeshFactory.cu:15-31``)."""
 
@@ -175,6 +183,14 @@ class DMOMeshQuadFactory:
     @staticmethod
     def create(points, quads, color_seed: int = 1) -> DMOMeshQuad:
         return DMOMeshQuad(points, quads, color_seed)
+
+
+class DMOMeshHexFactory:
+    """``DMOMeshHexFactory::create`` (``mesh/MeshFactory.cu``) from arrays."""
+
+    @staticmethod
+    def create(points, hexes, color_seed: int = 1) -> DMOMeshHex:
+        return DMOMeshHex(points, hexes, color_seed)
 
 
 class DMOMeshTetFactory:
@@ -402,6 +418,10 @@ def debug_gemm_bf16(A, B) -> np.ndarray:
     D = np.zeros((A.shape[0], B.shape[0]), np.float32)
     check(_capi.lib().vsdmo_debug_gemm_bf16(_ptr(A), _ptr(B), A.shape[0], B.shape[0], A.shape[1], _ptr(D)))
     return D
+
+
+class DMOHexClass(_DMOBase):
+    """``DMO::DMOHexClass`` (``dmo/DMOHex.h``): interior hex DMO with ``shapeMetricHex``."""
 
 
 class DMOTriFlatClass(_DMOBase):

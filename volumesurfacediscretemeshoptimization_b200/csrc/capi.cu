@@ -40,6 +40,14 @@ __global__ void k_pack_hf(const int4* hf, long n, int* out) {
     }
 }
 
+__global__ void k_pack_hh(const int4* hh, long n, int* out) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int4 a = hh[2 * i], b = hh[2 * i + 1];
+        int* o = out + 7 * i;
+        o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z;
+    }
+}
+
 void copy_in(void* dst, const void* src, size_t bytes, int mem_space, cudaStream_t s) {
     VSDMO_CUDA(cudaMemcpyAsync(dst, src, bytes, mem_space == VSDMO_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
 }
@@ -56,6 +64,8 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
                                o->counters.p, o->dirty.p, o->fb_list.p, o->fb_count.p, s);
     } else if (o->mode == MODE_TET) {
         launch_dmo_tet(m, L, s, o->dirty.p, o->dirty.p ? o->counters.p + 3 : nullptr);
+    } else if (o->mode == MODE_HEX) {
+        launch_dmo_hex(m, L, s);
     }
     else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
     else launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, s);
@@ -196,10 +206,9 @@ VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_
     *out = nullptr;
     if (elem_type != VSDMO_TRI && elem_type != VSDMO_TET && elem_type != VSDMO_QUAD && elem_type != VSDMO_HEX)
         return fail(VSDMO_E_ARG, "bad element type");
-    if (elem_type == VSDMO_HEX) return fail(VSDMO_E_UNSUPPORTED, "hex meshes are not supported yet");
     if (!xyz || !elems || n_vertices <= 0 || n_elems <= 0) return fail(VSDMO_E_ARG, "empty mesh or null arrays");
     if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
-    const int k = elem_type == VSDMO_TRI ? 3 : 4;
+    const int k = elem_type == VSDMO_TRI ? 3 : elem_type == VSDMO_HEX ? 8 : 4;
     if ((long)n_elems * k > (long)INT32_MAX / 2 || (long)n_vertices * 4 > (long)INT32_MAX)
         return fail(VSDMO_E_ARG, "mesh too large for 32-bit indices");
     std::unique_ptr<vsdmo_mesh_s> h(new vsdmo_mesh_s);
@@ -235,8 +244,8 @@ VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_
     return VSDMO_OK;
 }
 
-VSDMO_API void vsdmo_mesh_destroy(vsdmo_mesh_t mesh) {
-    if (!mesh) return;
+namespace {
+void release_mesh(vsdmo_mesh_t mesh) {
     cudaStream_t s = mesh->m.stream;
     bool own = mesh->m.own_stream;
     cudaStreamSynchronize(s);
@@ -245,6 +254,17 @@ VSDMO_API void vsdmo_mesh_destroy(vsdmo_mesh_t mesh) {
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
     }
+}
+}  // namespace
+
+VSDMO_API void vsdmo_mesh_destroy(vsdmo_mesh_t mesh) {
+    if (!mesh) return;
+    // optimisers still hold the mesh: it is released with the last of them
+    if (mesh->n_opts > 0) {
+        mesh->destroy_requested = true;
+        return;
+    }
+    release_mesh(mesh);
 }
 
 VSDMO_API vsdmo_status vsdmo_mesh_sync(vsdmo_mesh_t mesh) {
@@ -283,7 +303,7 @@ VSDMO_API long vsdmo_mesh_array_len(vsdmo_mesh_t mesh, int id) {
     case VSDMO_A_HE_ROWPTR: return m.he_rowptr.p ? m.nSurf + 1L : 0;
     case VSDMO_A_HALFEDGES: return 4L * m.nHE;
     case VSDMO_A_HF_ROWPTR: return m.hf_rowptr.p ? m.nV + 1L : 0;
-    case VSDMO_A_HALFFACES: return m.hf.p ? 12L * m.nE : 0;
+    case VSDMO_A_HALFFACES: return m.hf.p ? 12L * m.nE : (m.hh.p ? 56L * m.nE : 0);
     case VSDMO_A_COL_FREE: return (long)m.col_free.size();
     case VSDMO_A_COL_FEATURE: return (long)m.col_feature.size();
     case VSDMO_A_COL_INNER: return (long)m.col_inner.size();
@@ -324,7 +344,8 @@ VSDMO_API vsdmo_status vsdmo_mesh_array(vsdmo_mesh_t mesh, int id, void* host_ou
         case VSDMO_A_HF_ROWPTR: d2h(m.hf_rowptr.p, sizeof(int) * n); break;
         case VSDMO_A_HALFFACES: {
             DBuf<int> t(n, s);
-            k_pack_hf<<<grid_for(n / 3, 256), 256, 0, s>>>(m.hf.p, n / 3, t.p);
+            if (m.hf.p) k_pack_hf<<<grid_for(n / 3, 256), 256, 0, s>>>(m.hf.p, n / 3, t.p);
+            else k_pack_hh<<<grid_for(n / 7, 256), 256, 0, s>>>(m.hh.p, n / 7, t.p);
             VSDMO_CHECK_LAUNCH();
             d2h(t.p, sizeof(int) * n);
             break;
@@ -407,6 +428,12 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->mode = MODE_TET;
         o->kind = MK_TET;
         for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
+    } else if (m.type == VSDMO_HEX) {
+        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "surface passes of volume meshes are not implemented yet; set fix_boundary=1");
+        if (m.maxTets > dmo_hex_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more hexahedra than the kernel's ring budget");
+        o->mode = MODE_HEX;
+        o->kind = MK_HEX;
+        for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
     } else if (m.type == VSDMO_TRI && (p.flat < 0 ? m.isFlat : p.flat)) {
         if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "sliding boundary vertices are not implemented yet; set fix_boundary=1");
         if (m.maxHE > dmo_tri2d_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
@@ -445,14 +472,17 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->last_min = h[0].min_q;
     });
     if (st != VSDMO_OK) return st;
+    ++mesh->n_opts;
     *out = o.release();
     return VSDMO_OK;
 }
 
 VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt) {
     if (!opt) return;
-    cudaStreamSynchronize(opt->mesh->m.stream);
+    vsdmo_mesh_s* mesh = opt->mesh;
+    cudaStreamSynchronize(mesh->m.stream);
     delete opt;
+    if (--mesh->n_opts == 0 && mesh->destroy_requested) release_mesh(mesh);
 }
 
 VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t o, int n_iter) {

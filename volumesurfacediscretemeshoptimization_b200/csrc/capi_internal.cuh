@@ -9,9 +9,11 @@ using namespace vsdmo;
 
 struct vsdmo_mesh_s {
     Mesh m;
+    int n_opts = 0;                 // optimisers that reference this mesh
+    bool destroy_requested = false; // vsdmo_mesh_destroy came while optimisers were alive
 };
 
-enum OptMode { MODE_TET = 0, MODE_TRI2D = 1, MODE_SURF = 2 };
+enum OptMode { MODE_TET = 0, MODE_TRI2D = 1, MODE_SURF = 2, MODE_HEX = 3 };
 
 struct vsdmo_opt_s {
     vsdmo_mesh_s* mesh = nullptr;

@@ -569,6 +569,269 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
     }
 }
 
+
+// ---- hexahedra ------------------------------------------------------------------------------------
+// k_optimizeHierarchicalInnerHex<128> (dmo/DMOHexImplCub.h:21-137) with shapeMetricHex
+// (dmo/DMOQualityHex.h:54-71). With the candidate p as corner 0 of a halfhex, sub-tets 1, 2, 3
+// and 6 of the metric do not depend on p, and sub-tets 0, 4, 5, 7, 8 have a determinant affine
+// in p and a Frobenius term quadratic in p; each halfhex is staged as 43 coefficients (the
+// constant part's key and 5 x {g, c, m, C}). min_j cbrt(s^2) / A is compared through s^2 / A^3
+// as a fraction. The reference block's 128 threads of 4 candidates, whose maxima carry across
+// levels, are kept: lane l owns threads 4l .. 4l+3 (fixed z, two y, eight x).
+constexpr int HEX_WARPS = 4;
+constexpr int HEX_MAX_RING = 64;
+constexpr int HEX_CO = 44;                      // floats per halfhex (43 used)
+constexpr float HEX_EPS = 1.19209e-07f;          // EPSILON of dmo/SurfaceCommon.h
+
+__device__ __forceinline__ void hcross(const float* a, const float* b, float* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ float hdot3(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+__device__ __forceinline__ void hex_frac(float s, float A, float es, float ea, float& N, float& D, bool& first, bool& zero) {
+    if (s < es || A < ea) { zero = true; return; }
+    const float num = s * s, den = (A * A) * A;
+    if (first) { N = num; D = den; first = false; return; }
+    if (num * D < N * den) { N = num; D = den; }
+}
+
+// coefficients of one halfhex from its seven corners r (scaled, relative to the vertex)
+__device__ void hex_coeffs(const float r[7][3], float es, float ea, float* out) {
+    const float* v1 = r[0]; const float* v2 = r[1]; const float* v3 = r[2]; const float* v4 = r[3];
+    const float* v5 = r[4]; const float* v6 = r[5]; const float* v7 = r[6];
+    float L0[3], L1[3], L2[3], L3[3], L5[3], L6[3], L7[3], L9[3], L10[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        L0[a] = v5[a] - v4[a]; L1[a] = v6[a] - v5[a]; L2[a] = v7[a] - v6[a]; L3[a] = v7[a] - v4[a];
+        L5[a] = v1[a] - v5[a]; L6[a] = v2[a] - v6[a]; L7[a] = v3[a] - v7[a]; L9[a] = v2[a] - v1[a];
+        L10[a] = v3[a] - v2[a];
+    }
+    float N = 0.f, D = 1.f;
+    bool first = true, zero = false;
+    // constant sub-tets 1 (L1, -L0, L5), 2 (L2, -L1, L6), 3 (-L3, -L2, L7), 6 (-L9, L10, -L6)
+    {
+        float e[4][3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            e[0][0][a] = L1[a]; e[0][1][a] = -L0[a]; e[0][2][a] = L5[a];
+            e[1][0][a] = L2[a]; e[1][1][a] = -L1[a]; e[1][2][a] = L6[a];
+            e[2][0][a] = -L3[a]; e[2][1][a] = -L2[a]; e[2][2][a] = L7[a];
+            e[3][0][a] = -L9[a]; e[3][1][a] = L10[a]; e[3][2][a] = -L6[a];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float x[3];
+            hcross(e[i][1], e[i][2], x);
+            const float sd = hdot3(e[i][0], x);
+            const float A = (hdot3(e[i][0], e[i][0]) + hdot3(e[i][1], e[i][1])) + hdot3(e[i][2], e[i][2]);
+            hex_frac(sd, A, es, ea, N, D, first, zero);
+        }
+    }
+    out[0] = N; out[1] = D; out[2] = zero ? 1.f : 0.f;
+    float* co = out + 3;
+    float g[3], t1[3], t2[3], t3[3];
+    // sub 0: det = (p - v4) . (L0 x L3)
+    hcross(L0, L3, g);
+    co[0] = g[0]; co[1] = g[1]; co[2] = g[2]; co[3] = -hdot3(v4, g);
+    co[4] = -2.f * v4[0]; co[5] = -2.f * v4[1]; co[6] = -2.f * v4[2];
+    co[7] = (hdot3(L0, L0) + hdot3(L3, L3)) + hdot3(v4, v4);
+    co += 8;
+    // sub 4: (v3 - p, v1 - p, v4 - p)
+    hcross(v1, v4, t1); hcross(v4, v3, t2); hcross(v3, v1, t3);
+    co[0] = -((t1[0] + t2[0]) + t3[0]); co[1] = -((t1[1] + t2[1]) + t3[1]); co[2] = -((t1[2] + t2[2]) + t3[2]);
+    co[3] = hdot3(v3, t1);
+    co[4] = -2.f * ((v3[0] + v1[0]) + v4[0]); co[5] = -2.f * ((v3[1] + v1[1]) + v4[1]); co[6] = -2.f * ((v3[2] + v1[2]) + v4[2]);
+    co[7] = (hdot3(v3, v3) + hdot3(v1, v1)) + hdot3(v4, v4);
+    co += 8;
+    // sub 5: (p - v1, L9, -L5)
+    const float mL5[3] = { -L5[0], -L5[1], -L5[2] };
+    hcross(L9, mL5, g);
+    co[0] = g[0]; co[1] = g[1]; co[2] = g[2]; co[3] = -hdot3(v1, g);
+    co[4] = -2.f * v1[0]; co[5] = -2.f * v1[1]; co[6] = -2.f * v1[2];
+    co[7] = hdot3(v1, v1) + (hdot3(L9, L9) + hdot3(L5, L5));
+    co += 8;
+    // sub 7: (-L10, p - v3, -L7): det = (p - v3) . (L7 x L10)
+    hcross(L7, L10, g);
+    co[0] = g[0]; co[1] = g[1]; co[2] = g[2]; co[3] = -hdot3(v3, g);
+    co[4] = -2.f * v3[0]; co[5] = -2.f * v3[1]; co[6] = -2.f * v3[2];
+    co[7] = hdot3(v3, v3) + (hdot3(L10, L10) + hdot3(L7, L7));
+    co += 8;
+    // sub 8: (Q0 - p, Q1 - p, Q2 + p)
+    float Q0[3], Q1[3], Q2[3], a1[3], a2[3], a3[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        Q0[a] = ((v5[a] - v4[a]) + (v6[a] - v7[a])) + (v1[a] + (v2[a] - v3[a]));
+        Q1[a] = ((v7[a] - v4[a]) + (v6[a] - v5[a])) + (v3[a] + (v2[a] - v1[a]));
+        Q2[a] = ((v1[a] - v5[a]) + (v2[a] - v6[a])) + ((v3[a] - v7[a]) - v4[a]);
+    }
+    hcross(Q0, Q1, a1); hcross(Q2, Q0, a2); hcross(Q1, Q2, a3);
+    co[0] = (a1[0] - a2[0]) - a3[0]; co[1] = (a1[1] - a2[1]) - a3[1]; co[2] = (a1[2] - a2[2]) - a3[2];
+    co[3] = hdot3(Q0, a3);
+    co[4] = 2.f * ((Q2[0] - Q0[0]) - Q1[0]); co[5] = 2.f * ((Q2[1] - Q0[1]) - Q1[1]); co[6] = 2.f * ((Q2[2] - Q0[2]) - Q1[2]);
+    co[7] = (hdot3(Q0, Q0) + hdot3(Q1, Q1)) + hdot3(Q2, Q2);
+}
+
+// ring key of one candidate (the current / old position)
+__device__ float hex_key1(const float* co, int k, float x, float y, float z, float es, float ea) {
+    const float t1x = x * x, t1y = y * y, t1z = z * z;
+    const float t3x = (3.f * x) * x, t3y = (3.f * y) * y, t3z = (3.f * z) * z;
+    float N = 0.f, D = 1.f;
+    bool first = true, zero = false;
+    for (int h = 0; h < k; ++h) {
+        const float* c = co + HEX_CO * h;
+        if (c[2] != 0.f) zero = true;
+        else if (first) { N = c[0]; D = c[1]; first = false; }
+        else if (c[0] * D < N * c[1]) { N = c[0]; D = c[1]; }
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+            const float* q = c + 3 + 8 * j;
+            const bool a3 = (j == 1 || j == 4);
+            const float s = fmaf(q[0], x, fmaf(q[1], y, fmaf(q[2], z, q[3])));
+            const float A = ((q[7] + fmaf(q[6], z, a3 ? t3z : t1z)) + fmaf(q[5], y, a3 ? t3y : t1y)) +
+                            fmaf(q[4], x, a3 ? t3x : t1x);
+            hex_frac(s, A, es, ea, N, D, first, zero);
+        }
+    }
+    return zero ? 0.f : N / D;
+}
+
+__global__ void __launch_bounds__(HEX_WARPS * 32)
+k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hh, int v0, int v1,
+          float grid_scale, int depth, int maxk) {
+    extern __shared__ float4 smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int v = v0 + blockIdx.x * HEX_WARPS + w;
+    if (v >= v1) return;
+    float* co = reinterpret_cast<float*>(smem) + (size_t)w * maxk * HEX_CO;
+    const int b = rowptr[v], k = rowptr[v + 1] - b;
+    if (k <= 0 || k > maxk) return;
+    const float4 c0 = pos[v];
+    // per-axis largest (scale) and smallest (grid extent, DMOHexImplCub.h:49-68) ring distance
+    float mx0 = 0.f, mx1 = 0.f, mx2 = 0.f, mn0 = FLT_MAX, mn1 = FLT_MAX, mn2 = FLT_MAX;
+    for (int idx = lane; idx < 7 * k; idx += 32) {
+        const int h = idx / 7, c = idx % 7;
+        const int4 q = hh[2 * (b + h) + (c >> 2)];
+        const int cc = c & 3;
+        const int u = cc == 0 ? q.x : (cc == 1 ? q.y : (cc == 2 ? q.z : q.w));
+        const float4 p = pos[u];
+        const float d0 = fabsf(p.x - c0.x), d1 = fabsf(p.y - c0.y), d2 = fabsf(p.z - c0.z);
+        mx0 = fmaxf(mx0, d0); mx1 = fmaxf(mx1, d1); mx2 = fmaxf(mx2, d2);
+        mn0 = fminf(mn0, d0); mn1 = fminf(mn1, d1); mn2 = fminf(mn2, d2);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        mx0 = fmaxf(mx0, __shfl_xor_sync(FULL, mx0, o)); mx1 = fmaxf(mx1, __shfl_xor_sync(FULL, mx1, o));
+        mx2 = fmaxf(mx2, __shfl_xor_sync(FULL, mx2, o)); mn0 = fminf(mn0, __shfl_xor_sync(FULL, mn0, o));
+        mn1 = fminf(mn1, __shfl_xor_sync(FULL, mn1, o)); mn2 = fminf(mn2, __shfl_xor_sync(FULL, mn2, o));
+    }
+    const float mm = fmaxf(mx0, fmaxf(mx1, mx2));
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) return;
+    int ex;
+    (void)frexpf(mm, &ex);
+    const float p2 = exp2_exact(-ex);
+    const float es = ldexpf(HEX_EPS, -3 * ex), ea = ldexpf(HEX_EPS, -2 * ex);
+    for (int h = lane; h < k; h += 32) {
+        const int4 qa = hh[2 * (b + h)], qb = hh[2 * (b + h) + 1];
+        const int us[7] = { qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z };
+        float r[7][3];
+#pragma unroll
+        for (int c = 0; c < 7; ++c) {
+            const float4 p = pos[us[c]];
+            r[c][0] = scale2(p.x - c0.x, p2, -ex); r[c][1] = scale2(p.y - c0.y, p2, -ex); r[c][2] = scale2(p.z - c0.z, p2, -ex);
+        }
+        hex_coeffs(r, es, ea, co + HEX_CO * h);
+    }
+    __syncwarp();
+    const float sx = scale2(mn0, p2, -ex), sy = scale2(mn1, p2, -ex), sz = scale2(mn2, p2, -ex);
+    // ring-wide: any constant part zero makes every candidate's key zero
+    bool czero = false;
+    for (int h = 0; h < k; ++h) czero |= co[HEX_CO * h + 2] != 0.f;
+    const int kz = lane >> 2, j0 = 2 * (lane & 3);
+    float qMax[4] = { -FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX };
+    float pX[4] = { 0.f, 0.f, 0.f, 0.f }, pY[4] = { 0.f, 0.f, 0.f, 0.f }, pZ[4] = { 0.f, 0.f, 0.f, 0.f };
+    float dx = 0.f, dy = 0.f, dz = 0.f;
+    float ds = grid_scale;
+    float qWin = -FLT_MAX;
+    for (int level = 0; level < depth; ++level) {
+        const float Sx = ds * sx, Sy = ds * sy, Sz = ds * sz;
+        const float qLast = hex_key1(co, k, dx, dy, dz, es, ea);
+        const float z = fmaf(grid_offset(kz), Sz, dz);
+        const float y[2] = { fmaf(grid_offset(j0), Sy, dy), fmaf(grid_offset(j0 + 1), Sy, dy) };
+        float x[NQ], t1x[NQ], t3x[NQ];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) { x[i] = fmaf(grid_offset(i), Sx, dx); t1x[i] = x[i] * x[i]; t3x[i] = (3.f * x[i]) * x[i]; }
+        const float t1z = z * z, t3z = (3.f * z) * z;
+        const float t1y[2] = { y[0] * y[0], y[1] * y[1] }, t3y[2] = { (3.f * y[0]) * y[0], (3.f * y[1]) * y[1] };
+        float N[2][NQ], D[2][NQ];
+        bool zr[2][NQ];
+        {
+            const float n0 = co[0], d0 = co[1];
+#pragma unroll
+            for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) { N[jj][i] = n0; D[jj][i] = d0; zr[jj][i] = czero; }
+        }
+        for (int h = 0; h < k; ++h) {
+            const float* c = co + HEX_CO * h;
+            if (h > 0) {
+                const float cn = c[0], cd = c[1];
+#pragma unroll
+                for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+                    for (int i = 0; i < NQ; ++i)
+                        if (cn * D[jj][i] < N[jj][i] * cd) { N[jj][i] = cn; D[jj][i] = cd; }
+            }
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const float* q = c + 3 + 8 * j;
+                const bool a3 = (j == 1 || j == 4);
+                const float sZ = fmaf(q[2], z, q[3]);
+                const float aZ = q[7] + fmaf(q[6], z, a3 ? t3z : t1z);
+#pragma unroll
+                for (int jj = 0; jj < 2; ++jj) {
+                    const float sY = fmaf(q[1], y[jj], sZ);
+                    const float aY = aZ + fmaf(q[5], y[jj], a3 ? t3y[jj] : t1y[jj]);
+#pragma unroll
+                    for (int i = 0; i < NQ; ++i) {
+                        const float sd = fmaf(q[0], x[i], sY);
+                        const float A = aY + fmaf(q[4], x[i], a3 ? t3x[i] : t1x[i]);
+                        if (sd < es || A < ea) { zr[jj][i] = true; continue; }
+                        const float num = sd * sd, den = (A * A) * A;
+                        if (num * D[jj][i] < N[jj][i] * den) { N[jj][i] = num; D[jj][i] = den; }
+                    }
+                }
+            }
+        }
+        // carried per-thread maxima of the reference's threads 4 lane + (0: x0-3 y0, 1: x4-7 y0,
+        // 2: x0-3 y1, 3: x4-7 y1), candidates in index order
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                const float key = zr[jj][i] ? 0.f : N[jj][i] / D[jj][i];
+                const int t = 2 * jj + (i >> 2);
+                if (key > qMax[t]) { qMax[t] = key; pX[t] = x[i]; pY[t] = y[jj]; pZ[t] = z; }
+            }
+        float bk = qMax[0];
+        int bi = 4 * lane;
+#pragma unroll
+        for (int t = 1; t < 4; ++t)
+            if (qMax[t] > bk) { bk = qMax[t]; bi = 4 * lane + t; }
+        warp_argmax(bk, bi);
+        const int src = bi >> 2, tt = bi & 3;
+        const float wx = __shfl_sync(FULL, tt == 0 ? pX[0] : (tt == 1 ? pX[1] : (tt == 2 ? pX[2] : pX[3])), src);
+        const float wy = __shfl_sync(FULL, tt == 0 ? pY[0] : (tt == 1 ? pY[1] : (tt == 2 ? pY[2] : pY[3])), src);
+        const float wz = __shfl_sync(FULL, tt == 0 ? pZ[0] : (tt == 1 ? pZ[1] : (tt == 2 ? pZ[2] : pZ[3])), src);
+        if (qLast < bk) { dx = wx; dy = wy; dz = wz; }
+        qWin = bk;
+        ds = ds * (2.0f / 7.0f);
+    }
+    const float qOld = hex_key1(co, k, 0.f, 0.f, 0.f, es, ea);
+    if (lane == 0 && qOld < qWin) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
+}
+
 // ---- flat triangles ---------------------------------------------------------------------------
 __device__ __forceinline__ float tri_key(const float4* co, int k, float x, float y) {
     const float tx = (2.0f * x) * x, ty = (2.0f * y) * y;
@@ -710,7 +973,50 @@ __device__ __forceinline__ float q_quad(float4 p0, float4 p1, float4 p2, float4 
     return (2.f * (a1 + a2)) / l;
 }
 
+// shapeMetricHex (dmo/DMOQualityHex.h:54-71) in the reference's operation order, with cbrtf
+__device__ float q_hex(const float4* __restrict__ pos, const int* __restrict__ h) {
+    float v[8][3];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) { const float4 p = pos[h[c]]; v[c][0] = p.x; v[c][1] = p.y; v[c][2] = p.z; }
+    const float* P[8] = { v[4], v[5], v[6], v[7], v[0], v[1], v[2], v[3] };
+    float L[12][3], X[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        L[0][a] = P[1][a] - P[0][a]; L[4][a] = P[4][a] - P[0][a]; L[8][a] = P[5][a] - P[4][a];
+        L[1][a] = P[2][a] - P[1][a]; L[5][a] = P[5][a] - P[1][a]; L[9][a] = P[6][a] - P[5][a];
+        L[2][a] = P[3][a] - P[2][a]; L[6][a] = P[6][a] - P[2][a]; L[10][a] = P[7][a] - P[6][a];
+        L[3][a] = P[3][a] - P[0][a]; L[7][a] = P[7][a] - P[3][a]; L[11][a] = P[7][a] - P[4][a];
+        X[0][a] = (((P[1][a] - P[0][a]) + (P[2][a] - P[3][a])) + (P[5][a] - P[4][a])) + (P[6][a] - P[7][a]);
+        X[1][a] = (((P[3][a] - P[0][a]) + (P[2][a] - P[1][a])) + (P[7][a] - P[4][a])) + (P[6][a] - P[5][a]);
+        X[2][a] = (((P[4][a] - P[0][a]) + (P[5][a] - P[1][a])) + (P[6][a] - P[2][a])) + (P[7][a] - P[3][a]);
+    }
+    const int T[9][3] = { { 0, 3, 4 }, { 1, 0, 5 }, { 2, 1, 6 }, { 3, 2, 7 }, { 11, 8, 4 },
+                          { 8, 9, 5 }, { 9, 10, 6 }, { 10, 11, 7 }, { 0, 1, 2 } };
+    const int S[9][3] = { { 1, 1, 1 }, { 1, -1, 1 }, { 1, -1, 1 }, { -1, -1, 1 }, { 1, 1, -1 },
+                          { -1, 1, -1 }, { -1, 1, -1 }, { -1, -1, -1 }, { 1, 1, 1 } };
+    float ret = 1e30f;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        float e[3][3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float val = i == 8 ? X[T[i][j]][a] : L[T[i][j]][a];
+                e[j][a] = S[i][j] < 0 ? -val : val;
+            }
+        float x[3];
+        hcross(e[1], e[2], x);
+        const float sj = hdot3(e[0], x);
+        const float Aj = (hdot3(e[0], e[0]) + hdot3(e[1], e[1])) + hdot3(e[2], e[2]);
+        if (sj < HEX_EPS || Aj < HEX_EPS) return 0.f;
+        ret = fminf(ret, cbrtf(sj * sj) / Aj);
+    }
+    return 3.f * ret;
+}
+
 __device__ __forceinline__ float element_quality(const int* __restrict__ el, int kind, const float4* __restrict__ pos, long e) {
+    if (kind == MK_HEX) return q_hex(pos, el + 8 * e);
     if (kind == MK_TET) {
         const int4 t = reinterpret_cast<const int4*>(el)[e];
         return q_tet(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
@@ -793,6 +1099,17 @@ __global__ void k_quality_histogram(const int* __restrict__ el, int kind, long n
 }  // namespace
 
 int dmo_tet_max_ring() { return TET_MAX_RING; }
+int dmo_hex_max_ring() { return HEX_MAX_RING; }
+
+void launch_dmo_hex(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxk = m.maxTets;
+    const size_t smem = (size_t)HEX_WARPS * maxk * HEX_CO * sizeof(float);
+    k_dmo_hex<<<(n + HEX_WARPS - 1) / HEX_WARPS, HEX_WARPS * 32, smem, s>>>(m.pos.p, m.hf_rowptr.p, m.hh.p, L.v0, L.v1,
+                                                                            L.grid_scale, L.depth, maxk);
+    VSDMO_CHECK_LAUNCH();
+}
 
 // Raises the dynamic shared-memory limit of the grid-search kernels (called once per
 // optimiser, outside any stream capture, on the current device).
@@ -805,6 +1122,8 @@ void prepare_dmo_kernels() {
                                     TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet_list, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_hex, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    HEX_WARPS * HEX_MAX_RING * HEX_CO * (int)sizeof(float)));
 }
 int dmo_tri2d_max_ring() { return TRI_MAX_RING; }
 int quality_stats_blocks() { return QS_BLOCKS; }

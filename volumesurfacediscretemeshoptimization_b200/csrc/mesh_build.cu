@@ -1,4 +1,4 @@
-// mesh_build.cu -- connectivity and colouring of tri / quad / tet meshes on the GPU.
+// mesh_build.cu -- connectivity and colouring of tri / quad / tet / hex meshes on the GPU.
 //
 // Produces, bit for bit, the layout the reference's MeshTetGPU::init / MeshTriGPU::init build
 // (mesh/MeshTetGPU.cu:35-42, mesh/MeshTriGPU.cu:37-50):
@@ -13,7 +13,9 @@
 //     the same with faces of four corners (mesh/MeshQuadGPU.cu), the fan walk stepping to the
 //     corner two after the target (getThirdVertex, mesh/MeshGPUCommon.cu:149-162) and the
 //     colouring adjacency holding both diagonals (:1067-1097);
-//   * halfface CSR, rows in tetrahedron order (mesh/MeshTetGPU.cu:113-142);
+//   * halfface CSR, rows in tetrahedron order (mesh/MeshTetGPU.cu:113-142); for hex meshes the
+//     boundary quads (mesh/MeshHexGPU.cu:141-164), the all-pairs colouring graph of a hexahedron
+//     and the halfhex CSR (mesh/MeshHexGPU.cu:116-139, mesh/MeshGPUCommon.cu:1334-1368);
 //   * boundary / feature flags (dihedral > 20 deg, mesh/MeshGPUCommon.cu:466-495) and face /
 //     vertex normals (:363-434).
 // Sorting uses the stable LSD radix sort of prim.cu. Colouring runs the reference's JPL round
@@ -108,6 +110,93 @@ __global__ void k_emit_boundary_tris(const int* idx, int nB, const uint32_t* s0,
         int a = s0[j], b = s1[j], c = s2[j];
         tris[3 * i] = a; tris[3 * i + 1] = b; tris[3 * i + 2] = c;
         isB2[a] = 1; isB2[b] = 1; isB2[c] = 1;
+    }
+}
+
+// ---- hexahedral boundary (MeshHexGPU::initBoundary2D, mesh/MeshHexGPU.cu:141-164) --------------
+// getQuadSmallestFirst: rotate so that the smallest index comes first (mesh/MeshGPUCommon.cu:37-54)
+__device__ __forceinline__ void quad_smallest_first(int a, int b, int c, int d, uint32_t* o) {
+    if (b < a && b < c && b < d) { o[0] = b; o[1] = c; o[2] = d; o[3] = a; }
+    else if (c < a && c < b && c < d) { o[0] = c; o[1] = d; o[2] = a; o[3] = b; }
+    else if (d < a && d < b && d < c) { o[0] = d; o[1] = a; o[2] = b; o[3] = c; }
+    else { o[0] = a; o[1] = b; o[2] = c; o[3] = d; }
+}
+
+// the six faces of a hexahedron (k_constructQuadsFromHexahedra, mesh/MeshGPUCommon.cu:1412-1430)
+__global__ void k_hex_faces(const int* hexes, int nH, uint32_t* f0, uint32_t* f1, uint32_t* f2, uint32_t* f3) {
+    const int F[6][4] = { {0, 1, 2, 3}, {1, 5, 6, 2}, {3, 2, 6, 7}, {4, 0, 3, 7}, {1, 0, 4, 5}, {5, 4, 7, 6} };
+    GRID_STRIDE(t, nH) {
+        const int* v = hexes + 8 * t;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            uint32_t o[4];
+            quad_smallest_first(v[F[f][0]], v[F[f][1]], v[F[f][2]], v[F[f][3]], o);
+            f0[6 * t + f] = o[0]; f1[6 * t + f] = o[1]; f2[6 * t + f] = o[2]; f3[6 * t + f] = o[3];
+        }
+    }
+}
+
+__device__ __forceinline__ int cmp4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0, uint32_t b1,
+                                    uint32_t b2, uint32_t b3) {
+    if (a0 != b0) return a0 < b0 ? -1 : 1;
+    if (a1 != b1) return a1 < b1 ? -1 : 1;
+    if (a2 != b2) return a2 < b2 ? -1 : 1;
+    if (a3 != b3) return a3 < b3 ? -1 : 1;
+    return 0;
+}
+
+// quads sorted lexicographically: (a,b,c,d) with b<d pairs with (a,d,c,b) (k_markDuplicateQuads)
+__global__ void k_pair_quads(const uint32_t* s0, const uint32_t* s1, const uint32_t* s2, const uint32_t* s3, long nF,
+                             uint8_t* paired, int* err) {
+    GRID_STRIDE(i, nF) {
+        const uint32_t a = s0[i], b = s1[i], c = s2[i], d = s3[i];
+        if (i + 1 < nF && s0[i + 1] == a && s1[i + 1] == b && s2[i + 1] == c && s3[i + 1] == d) atomicMax(err, BE_NONMANIFOLD);
+        if (b < d) {
+            long lo = i + 1, hi = nF;
+            while (lo < hi) {
+                const long mid = (lo + hi) >> 1;
+                if (cmp4(s0[mid], s1[mid], s2[mid], s3[mid], a, d, c, b) < 0) lo = mid + 1; else hi = mid;
+            }
+            if (lo < nF && s0[lo] == a && s1[lo] == d && s2[lo] == c && s3[lo] == b) { paired[i] = 1; paired[lo] = 1; }
+        }
+    }
+}
+
+__global__ void k_emit_boundary_quads(const int* idx, int nB, const uint32_t* s0, const uint32_t* s1, const uint32_t* s2,
+                                      const uint32_t* s3, int* quads, uint8_t* isB2) {
+    GRID_STRIDE(i, nB) {
+        const int j = idx[i];
+        const int a = s0[j], b = s1[j], c = s2[j], d = s3[j];
+        quads[4 * i] = a; quads[4 * i + 1] = b; quads[4 * i + 2] = c; quads[4 * i + 3] = d;
+        isB2[a] = 1; isB2[b] = 1; isB2[c] = 1; isB2[d] = 1;
+    }
+}
+
+// every vertex pair of a hexahedron within [lo, lo+num) (mesh/MeshGPUCommon.cu:936-1037)
+__global__ void k_hex_pairs(const int* hexes, int nH, int lo, int num, uint32_t* ks, uint32_t* vs, int* counter) {
+    GRID_STRIDE(t, nH) {
+        const int* v = hexes + 8 * t;
+        for (int i = 0; i < 7; ++i)
+            for (int j = i + 1; j < 8; ++j) {
+                const int a = v[i] - lo, b = v[j] - lo;
+                if (a >= 0 && a < num && b >= 0 && b < num) {
+                    const int p = atomicAdd(counter, 2);
+                    ks[p] = a; vs[p] = b; ks[p + 1] = b; vs[p + 1] = a;
+                }
+            }
+    }
+}
+
+// halfhex of corner j: the other seven corners (k_constructHalfhexesNew, mesh/MeshGPUCommon.cu:1334-1368),
+// two int4 per halfhex (the eighth value is -1)
+__global__ void k_halfhexes(const uint32_t* order, long nHH, const int* hexes, int4* hh) {
+    const int H[8][7] = { {1, 2, 3, 4, 5, 6, 7}, {5, 6, 2, 0, 4, 7, 3}, {6, 7, 3, 1, 5, 4, 0}, {7, 4, 0, 2, 6, 5, 1},
+                          {0, 3, 7, 5, 1, 2, 6}, {4, 7, 6, 1, 0, 3, 2}, {5, 4, 7, 2, 1, 0, 3}, {6, 5, 4, 3, 2, 1, 0} };
+    GRID_STRIDE(i, nHH) {
+        const int e = (int)order[i], t = e >> 3, j = e & 7;
+        const int* v = hexes + 8L * t;
+        hh[2 * i] = make_int4(v[H[j][0]], v[H[j][1]], v[H[j][2]], v[H[j][3]]);
+        hh[2 * i + 1] = make_int4(v[H[j][4]], v[H[j][5]], v[H[j][6]], -1);
     }
 }
 
@@ -557,7 +646,7 @@ struct Builder {
             DBuf<int> order;
             int nFree = stable_partition(m.isFeat.p, nS, 0, order);
             std::vector<std::pair<int*, long>> el = { {m.tris.p, (long)m.fk * m.nTris} };
-            if (m.type == VSDMO_TET) el.push_back({m.elems.p, 4L * m.nE});
+            if (m.type == VSDMO_TET || m.type == VSDMO_HEX) el.push_back({m.elems.p, (long)m.k * m.nE});
             permute_range(order.p, 0, nS, {&m.isB1, &m.isFeat}, el, nS);
             m.nFeature = nS - nFree;
         }
@@ -574,11 +663,13 @@ struct Builder {
                 nc = 0;
                 continue;
             }
-            long cap = m.type == VSDMO_TET ? 12L * m.nE : (m.fk == 4 ? 12L : 6L) * m.nTris;
+            long cap = m.type == VSDMO_TET ? 12L * m.nE : m.type == VSDMO_HEX ? 56L * m.nE : (m.fk == 4 ? 12L : 6L) * m.nTris;
             DBuf<uint32_t> ks(cap, s), vs(cap, s);
             DBuf<int> cnt(1, s);
             cnt.zero();
-            if (m.type == VSDMO_TET)
+            if (m.type == VSDMO_HEX)
+                k_hex_pairs<<<G(m.nE), 256, 0, s>>>(m.elems.p, m.nE, lo, num, ks.p, vs.p, cnt.p);
+            else if (m.type == VSDMO_TET)
                 k_tet_edge_pairs<<<G(m.nE), 256, 0, s>>>(m.elems.p, m.nE, lo, num, ks.p, vs.p, cnt.p);
             else if (m.fk == 4)
                 k_quad_edge_pairs<<<G(m.nTris), 256, 0, s>>>(m.tris.p, m.nTris, lo, num, ks.p, vs.p, cnt.p);
@@ -587,7 +678,7 @@ struct Builder {
             VSDMO_CHECK_LAUNCH();
             int np = read_scalar(cnt.p, s);
             std::vector<std::pair<int*, long>> el = { {m.tris.p, (long)m.fk * m.nTris} };
-            if (m.type == VSDMO_TET) el.push_back({m.elems.p, 4L * m.nE});
+            if (m.type == VSDMO_TET || m.type == VSDMO_HEX) el.push_back({m.elems.p, (long)m.k * m.nE});
             nc = color_range(lo, num, ks, vs, np, oh, od, {&m.isB1, &m.isFeat}, el);
         }
         final_halfedges();
@@ -685,6 +776,64 @@ struct Builder {
         VSDMO_CHECK_LAUNCH();
     }
 
+    void hex_boundary() {
+        const int nH = m.nE;
+        const long nF = 6L * nH;
+        DBuf<uint32_t> f0(nF, s), f1(nF, s), f2(nF, s), f3(nF, s), key(nF, s), order(nF, s);
+        k_hex_faces<<<G(nH), 256, 0, s>>>(m.elems.p, nH, f0.p, f1.p, f2.p, f3.p);
+        VSDMO_CHECK_LAUNCH();
+        k_iota<<<G(nF), 256, 0, s>>>(order.p, nF);
+        VSDMO_CHECK_LAUNCH();
+        const int bits = bits_for((uint32_t)(m.nV - 1));
+        const uint32_t* comps[4] = { f3.p, f2.p, f1.p, f0.p };
+        for (int c = 0; c < 4; ++c) {
+            k_gather_key<<<G(nF), 256, 0, s>>>(comps[c], order.p, key.p, nF);
+            VSDMO_CHECK_LAUNCH();
+            radix_sort_pairs(key.p, order.p, nF, bits, s);
+        }
+        DBuf<uint32_t> s0(nF, s), s1(nF, s), s2(nF, s), s3(nF, s);
+        k_gather_key<<<G(nF), 256, 0, s>>>(f0.p, order.p, s0.p, nF);
+        k_gather_key<<<G(nF), 256, 0, s>>>(f1.p, order.p, s1.p, nF);
+        k_gather_key<<<G(nF), 256, 0, s>>>(f2.p, order.p, s2.p, nF);
+        k_gather_key<<<G(nF), 256, 0, s>>>(f3.p, order.p, s3.p, nF);
+        VSDMO_CHECK_LAUNCH();
+        DBuf<uint8_t> paired(nF, s), unpaired(nF, s);
+        paired.zero();
+        err.zero();
+        k_pair_quads<<<G(nF), 256, 0, s>>>(s0.p, s1.p, s2.p, s3.p, nF, paired.p, err.p);
+        VSDMO_CHECK_LAUNCH();
+        check_err(err, s, "boundary faces");
+        k_not<<<G(nF), 256, 0, s>>>(paired.p, unpaired.p, nF);
+        VSDMO_CHECK_LAUNCH();
+        DBuf<int> bidx(nF, s);
+        const int nB = compact_flags(unpaired.p, nF, bidx.p, s);
+        m.nTris = nB;
+        m.tris.alloc(4L * nB, s);
+        m.isB2.alloc(m.nV, s);
+        m.isB2.zero();
+        k_emit_boundary_quads<<<G(nB), 256, 0, s>>>(bidx.p, nB, s0.p, s1.p, s2.p, s3.p, m.tris.p, m.isB2.p);
+        VSDMO_CHECK_LAUNCH();
+    }
+
+    void hex_halfhexes() {
+        const long nHH = 8L * m.nE;
+        DBuf<uint32_t> keys(nHH, s), order(nHH, s);
+        VSDMO_CUDA(cudaMemcpyAsync(keys.p, m.elems.p, sizeof(int) * nHH, cudaMemcpyDeviceToDevice, s));
+        k_iota<<<G(nHH), 256, 0, s>>>(order.p, nHH);
+        VSDMO_CHECK_LAUNCH();
+        radix_sort_pairs(keys.p, order.p, nHH, bits_for((uint32_t)(m.nV - 1)), s);
+        m.hf_rowptr.alloc(m.nV + 1, s);
+        rowptr_from_sorted(keys.p, nHH, m.nV, m.hf_rowptr.p, s);
+        m.hh.alloc(2 * nHH, s);
+        k_halfhexes<<<G(nHH), 256, 0, s>>>(order.p, nHH, m.elems.p, m.hh.p);
+        VSDMO_CHECK_LAUNCH();
+        DBuf<int> mx(1, s);
+        mx.zero();
+        k_max_row<<<G(m.nV), 256, 0, s>>>(m.hf_rowptr.p, m.nV, mx.p);
+        VSDMO_CHECK_LAUNCH();
+        m.maxTets = read_scalar(mx.p, s);
+    }
+
     void tet_halffaces() {
         const long nH = 4L * m.nE;
         DBuf<uint32_t> keys(nH, s), order(nH, s);
@@ -759,8 +908,34 @@ struct Builder {
             }
             if (m.nSurf > 0) surface_init();
             tet_halffaces();
-        } else {
-            throw Error(VSDMO_E_UNSUPPORTED, "hex meshes are not supported yet");
+        } else {  // VSDMO_HEX (MeshHexGPU::init, mesh/MeshHexGPU.cu:35-43)
+            m.fk = 4;
+            m.isFlat = 0;
+            hex_boundary();
+            {
+                DBuf<int> order;
+                int nS = stable_partition(m.isB2.p, m.nV, 1, order);
+                permute_range(order.p, 0, m.nV, {&m.isB2}, { {m.tris.p, 4L * m.nTris}, {m.elems.p, 8L * m.nE} }, m.nV);
+                m.nSurf = nS;
+            }
+            const int nI = m.nV - m.nSurf;
+            if (nI > 0) {
+                DBuf<uint32_t> ks(56L * m.nE, s), vs(56L * m.nE, s);
+                DBuf<int> cnt(1, s);
+                cnt.zero();
+                k_hex_pairs<<<G(m.nE), 256, 0, s>>>(m.elems.p, m.nE, m.nSurf, nI, ks.p, vs.p, cnt.p);
+                VSDMO_CHECK_LAUNCH();
+                int np = read_scalar(cnt.p, s);
+                m.nColInner = color_range(m.nSurf, nI, ks, vs, np, m.col_inner, m.d_col_inner, {&m.isB2},
+                                          { {m.tris.p, 4L * m.nTris}, {m.elems.p, 8L * m.nE} });
+            } else {
+                m.nColInner = 0;
+                m.col_inner.assign(1, m.nSurf);
+                m.d_col_inner.alloc(1, s);
+                VSDMO_CUDA(cudaMemcpyAsync(m.d_col_inner.p, m.col_inner.data(), sizeof(int), cudaMemcpyHostToDevice, s));
+            }
+            if (m.nSurf > 0) surface_init();
+            hex_halfhexes();
         }
         m.new_of_old.alloc(m.nV, s);
         k_final_perm<<<G(m.nV), 256, 0, s>>>(orig_of_cur.p, m.nV, m.new_of_old.p);

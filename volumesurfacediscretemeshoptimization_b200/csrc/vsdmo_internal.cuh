@@ -120,6 +120,7 @@ struct Mesh {
     DBuf<int4> he;            // [nHE] target, opposite, face, next
     DBuf<int> hf_rowptr;      // [nV+1]
     DBuf<int4> hf;            // [4nT] v0, v1, v2, tet
+    DBuf<int4> hh;            // hex: [8nH x 2] the other seven corners of each halfhex (+ -1)
     DBuf<uint8_t> isB1, isFeat, isB2;
     DBuf<float> fn, vn;       // [nTris*3], [nSurf*3]; quad normals from corners 0, 1, 3
     std::vector<int> col_free, col_feature, col_inner;  // host copies of colour offsets
@@ -145,6 +146,8 @@ void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s, uint8_t* 
                     unsigned long long* skipped = nullptr);
 void launch_dmo_tri2d(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
 int dmo_tet_max_ring();      // largest halfface row the tet kernel accepts
+void launch_dmo_hex(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
+int dmo_hex_max_ring();      // largest halfhex row the hex kernel accepts
 void prepare_dmo_kernels();
 int dmo_tri2d_max_ring();    // largest halfedge row the 2D kernel accepts
 
@@ -178,7 +181,7 @@ void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const 
 int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
 
 // Element metric used by the quality kernels.
-enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3 };
+enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4 };
 
 // Per-iteration statistics written by the quality kernel.
 struct IterStats {

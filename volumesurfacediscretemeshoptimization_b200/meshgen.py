@@ -94,9 +94,12 @@ def tet_cube(n: int = 48, seed: int | None = 0, jitter: float = 0.3):
 
 
 def hex_cube(n: int = 32, seed: int | None = 0, jitter: float = 0.3):
-    """Unit cube with ``n^3`` hexahedra. Corner order per cell: 0=(0,0,0) 1=(0,1,0)
-    2=(1,1,0) 3=(1,0,0) 4=(0,0,1) 5=(1,0,1) 6=(1,1,1) 7=(0,1,1), the OpenVolumeMesh order
-    under which ``shapeMetricHex`` of an undistorted cube is 1."""
+    """Unit cube with ``n^3`` hexahedra. Corner order per cell (offsets in cells):
+    0=(0,0,1) 1=(1,0,1) 2=(1,1,1) 3=(0,1,1) 4=(0,0,0) 5=(1,0,0) 6=(1,1,0) 7=(0,1,0): the
+    order under which every sub-tetrahedron of the reference's shapeMetricHex
+    (dmo/DMOQualityHex.h:54-71, which reads the corners as 4 5 6 7 0 1 2 3) is positive, the
+    metric of an undistorted cube is 1 and the six faces of k_constructQuadsFromHexahedra
+    (mesh/MeshGPUCommon.cu:1412-1430) point outwards."""
     m = n + 1
     h = 1.0 / n
     k, j, i = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
@@ -104,7 +107,7 @@ def hex_cube(n: int = 32, seed: int | None = 0, jitter: float = 0.3):
     ck, cj, ci = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
     b = ((ck * m + cj) * m + ci).ravel()
     X, Y, Z = 1, m, m * m
-    hexes = np.stack([b, b + Y, b + X + Y, b + X, b + Z, b + X + Z, b + X + Y + Z, b + Y + Z], 1)
+    hexes = np.stack([b + Z, b + X + Z, b + X + Y + Z, b + Y + Z, b, b + X, b + X + Y, b + Y], 1)
     if seed is not None and jitter > 0:
         inner = ((i > 0) & (i < n) & (j > 0) & (j < n) & (k > 0) & (k < n)).ravel()
         r = _rng(seed).uniform(-jitter * h, jitter * h, size=(inner.sum(), 3))
