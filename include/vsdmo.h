@@ -108,11 +108,12 @@ typedef struct vsdmo_params {
     int   quality;        /* vsdmo_quality                                                  */
     float grid_scale;     /* initial half-extent factor (0.5)                               */
     int   n_iter;         /* iterations run by vsdmo_opt_optimize (30)                      */
-    int   grid_n;         /* candidates per axis; only 8 is implemented                     */
+    int   grid_n;         /* candidates per axis: 8; flat tri / quad meshes also take 4     */
     int   depth;          /* refinement levels; 1..4 (3)                                    */
     int   fix_boundary;   /* 1: surface and feature passes are skipped (volume / flat runs  */
                           /*    with the boundary held fixed); 0: reference behaviour       */
-    int   flat;           /* tri meshes: -1 = from the mesh (all z == 0), 0 = surface, 1 = 2D */
+    int   flat;           /* tri / quad meshes: -1 = from the mesh (all z == 0), 0 = surface, */
+                          /*    1 = 2D                                                      */
     int   use_graph;      /* 1: each iteration is replayed from a captured CUDA graph       */
     int   check_monotone; /* 1: per-element check against the last minimum (reference       */
                           /*    k_updateCurrentQualities, dmo/DMOTet.cu:55-67)              */
@@ -164,8 +165,10 @@ VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* 
 /* ---- optimiser ------------------------------------------------------------------------- */
 /* Replaces DMOTetClass / DMOTriFlatClass / DMOTriClass / DMOQuadClass construction + init()
  * (dmo/DMOTet.cu:82-125, dmo/DMOTriFlat.cu:84-126, dmo/DMOTri.cu:80-126, dmo/DMOQuad.cu:78-123).
- * Tri meshes that are not flat (or flat = 0) and quad meshes get the surface optimiser; it
- * needs a mesh without feature vertices (VSDMO_E_UNSUPPORTED otherwise). Hex meshes get the
+ * Tri and quad meshes that are not flat (or flat = 0) get the surface optimiser; it needs a
+ * mesh without feature vertices (VSDMO_E_UNSUPPORTED otherwise). Flat quad meshes get the 2D
+ * search of DMOTriFlatClass with the quad mean ratio against +z (meanRatioMetricQuad(p, n),
+ * dmo/DMOQualityQuad.h:30-50; the reference has no flat-quad class). Hex meshes get the
  * interior search of DMOHexClass (dmo/DMOHex.cu, k_optimizeHierarchicalInnerHex). */
 VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* params, vsdmo_opt_t* out);
 VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt);
@@ -289,6 +292,59 @@ VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t opt, unsigned long
 /* Test entry point of the tensor-core GEMM: D [M x N] = bf16(A) [M x K] . bf16(B) [N x K]^T
  * in FP32, host arrays; N in {16, 32, 64, 96, 128}, K a multiple of 32. */
 VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int M, int N, int K, float* D);
+
+/* ---- batched flat meshes ------------------------------------------------------------------ */
+/* Many independent flat (z = 0) tri and quad meshes optimised together: one persistent launch
+ * per iteration takes (mesh, colour class, vertex chunk) work items in colour-major order, each
+ * mesh with its own grid (4 or 8 candidates per axis), refinement levels (1..4) and lanes per
+ * vertex (8, 16 or 32); iterations are replayed from a captured CUDA graph. The search per
+ * vertex is that of DMOTriFlatClass (dmo/DMOTriFlatImplCub.h:24-152, the reference runs one
+ * mesh per process). The reference has no batched mode: this replaces a loop over
+ * DMOTriFlatClass objects, one per mesh.
+ *
+ * n_meshes meshes; elem_types [n] (VSDMO_TRI or VSDMO_QUAD), n_vertices [n], n_elements [n]
+ * (host arrays); xyz: every mesh's vertices concatenated, float [sum n_vertices x 3];
+ * elems: every mesh's element list concatenated, int32 [sum k n_elements] with MESH-LOCAL
+ * vertex ids; mem_space applies to xyz and elems. Each mesh is built (connectivity and
+ * colouring) as vsdmo_mesh_create would with color_seed. Initial configuration: 8 / 3 / 32. */
+typedef struct vsdmo_batch_s* vsdmo_batch_t;
+VSDMO_API vsdmo_status vsdmo_batch_create(int n_meshes, const int32_t* elem_types, const int32_t* n_vertices,
+                                          const int32_t* n_elements, const float* xyz, const int32_t* elems,
+                                          int mem_space, uint32_t color_seed, void* cuda_stream,
+                                          vsdmo_batch_t* out);
+VSDMO_API void vsdmo_batch_destroy(vsdmo_batch_t batch);
+/* Queues n_iter iterations (graph replays) and waits for them; VSDMO_E_TIMEOUT when a
+ * colour-class wait of the persistent kernel expired (positions then are not a full
+ * iteration's result). */
+VSDMO_API vsdmo_status vsdmo_batch_iterate(vsdmo_batch_t batch, int n_iter);
+/* Queues n_iter iterations and returns without waiting (vsdmo_batch_sync waits and reports). */
+VSDMO_API vsdmo_status vsdmo_batch_iterate_async(vsdmo_batch_t batch, int n_iter);
+VSDMO_API vsdmo_status vsdmo_batch_sync(vsdmo_batch_t batch);
+/* Iteration count back to 0 and the per-mesh statistics of slot 0 from the current positions. */
+VSDMO_API vsdmo_status vsdmo_batch_restart(vsdmo_batch_t batch);
+/* Per-mesh statistics after `iteration` iterations since the restart (0 = at the restart):
+ * minimum and mean element quality, elements below the previous minimum; any output may be NULL. */
+VSDMO_API vsdmo_status vsdmo_batch_stats(vsdmo_batch_t batch, int iteration, float* min_q, double* mean_q,
+                                         int32_t* below_prev_min);
+/* Positions in the input numbering (concatenated, float [sum n_vertices x 3]). */
+VSDMO_API vsdmo_status vsdmo_batch_get_positions(vsdmo_batch_t batch, float* xyz, int mem_space);
+VSDMO_API vsdmo_status vsdmo_batch_set_positions(vsdmo_batch_t batch, const float* xyz, int mem_space);
+/* Per-mesh search configuration, host arrays [n_meshes]. */
+VSDMO_API vsdmo_status vsdmo_batch_get_config(vsdmo_batch_t batch, int32_t* grid_n, int32_t* depth, int32_t* lanes);
+VSDMO_API vsdmo_status vsdmo_batch_set_config(vsdmo_batch_t batch, const int32_t* grid_n, const int32_t* depth,
+                                              const int32_t* lanes);
+/* Autotuner: per size bucket (free vertices < 2,000 / < 10,000 / more) the configuration with
+ * the least device time to reach, within 1e-4, the mean and minimum quality that 8 / 3 / 32
+ * reaches in probe_iters iterations. Positions are left as they were. The report (one line per
+ * bucket) is written to `report` (truncated to report_len bytes, may be NULL). */
+VSDMO_API vsdmo_status vsdmo_batch_autotune(vsdmo_batch_t batch, int probe_iters, char* report, int report_len);
+/* Counts: 0 meshes, 1 vertices, 2 work items per iteration, 3 colour classes (all meshes),
+ * 4 iterations since the restart, 5 CTAs of the persistent launch, 6 largest halfedge row. */
+VSDMO_API long vsdmo_batch_info(vsdmo_batch_t batch, int which);
+/* Mesh m's layout in the batch: out8 = {first vertex, vertices, elements, vertices per
+ * element, colour classes, first free vertex (mesh-local), end of the free vertices,
+ * first halfedge}. */
+VSDMO_API vsdmo_status vsdmo_batch_mesh_info(vsdmo_batch_t batch, int mesh, int32_t* out8);
 
 #ifdef __cplusplus
 }

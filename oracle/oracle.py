@@ -74,6 +74,10 @@ def lib():
         L.or_surface_qualities_f64.argtypes = [P, P, P]
         L.or_optimize_surf_f32.argtypes = [P, P, I, F, I, P, P]
         L.or_optimize_surf_f64.argtypes = [P, P, I, D, I, P, P]
+        L.or_dmo_flat_f32.argtypes = [P, P, I, I, F, I, I, I]
+        L.or_dmo_quad2d_f64.argtypes = [P, P, I, I, D, P, I]
+        L.or_q_quad2d_f32.restype = F
+        L.or_q_quad2d_f32.argtypes = [P, P, P, P]
         L.or_dmo_hex_f32.argtypes = [P, P, I, I, F, I]
         L.or_dmo_hex_f64.argtypes = [P, P, I, I, D, P, I]
         L.or_hex_qualities_f32.argtypes = [P, P, P]
@@ -143,6 +147,18 @@ class OracleMesh:
         fn = {TET: lib().or_dmo_tet_f32, HEX: lib().or_dmo_hex_f32}.get(self.elem_type, lib().or_dmo_tri2d_f32)
         fn(self.h, _p(xyz), v0, v1, grid_scale, nthreads)
         return xyz
+
+    def dmo_flat_f32(self, xyz, v0, v1, nq=8, depth=3, grid_scale=0.5, nthreads=0):
+        """Flat tri / quad colour class with an nq x nq grid and `depth` levels (batched optimiser)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        lib().or_dmo_flat_f32(self.h, _p(xyz), v0, v1, grid_scale, nq, depth, nthreads)
+        return xyz
+
+    def dmo_quad2d_f64(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        margin = np.zeros(max(v1 - v0, 1), dtype=np.float64)
+        lib().or_dmo_quad2d_f64(self.h, _p(xyz), v0, v1, grid_scale, _p(margin), nthreads)
+        return xyz, margin[: v1 - v0]
 
     def dmo_color_ref32(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
         """The reference kernel's own float arithmetic (tet interior only)."""

@@ -101,6 +101,12 @@ void or_optimize_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale,
 void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
                      double* min_hist, double* mean_hist);
 
+/* ---- flat tri / quad meshes with a general grid (or_flat.c, the batched optimiser) ------ */
+void or_dmo_flat_f32(const or_mesh* m, float* xyz, int v0, int v1, float grid_scale, int nq, int depth, int nthreads);
+void or_dmo_quad2d_f64(const or_mesh* m, double* xyz, int v0, int v1, double grid_scale, double* margin, int nthreads);
+float  or_q_quad2d_f32(const float* p0, const float* p1, const float* p2, const float* p3);
+double or_q_quad2d_f64(const double* p0, const double* p1, const double* p2, const double* p3);
+
 /* ---- hexahedra (or_hex.c) ------------------------------------------------------------- */
 /* shapeMetricHex of corners v[0..7] (literal f64 / reference-order f32 with cbrtf) */
 double or_q_hex_f64(const double v[8][3]);

@@ -55,6 +55,18 @@ def test_host_only_calls(vsdmo):
     assert b"element type" in lib.vsdmo_last_error()
     assert lib.vsdmo_mesh_create(_capi.HEX, C.c_void_p(1), 1, C.c_void_p(1), 1, 5, 1, None, C.byref(h)) == _capi.E_ARG
     assert lib.vsdmo_opt_iterate(None, 1) == _capi.E_ARG
+    # batched meshes: argument errors before any CUDA call
+    import numpy as np
+    b = C.c_void_p()
+    one = np.ones(1, np.int32)
+    tet = np.full(1, _capi.TET, np.int32)
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert lib.vsdmo_batch_create(0, None, None, None, None, None, 0, 1, None, C.byref(b)) == _capi.E_ARG
+    assert lib.vsdmo_batch_create(1, ptr(tet), ptr(one), ptr(one), C.c_void_p(1), C.c_void_p(1), 0, 1, None,
+                                  C.byref(b)) == _capi.E_ARG
+    assert b"VSDMO_TRI or VSDMO_QUAD" in lib.vsdmo_last_error()
+    assert lib.vsdmo_batch_info(None, 0) == -1
+    assert lib.vsdmo_batch_iterate(None, 1) == _capi.E_ARG
 
 
 def test_python_api_raises_on_error(vsdmo):

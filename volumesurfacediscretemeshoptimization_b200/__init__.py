@@ -34,8 +34,8 @@ from ._capi import VSDMOError, Params, check
 
 __all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshQuad", "DMOMeshTet", "DMOMeshHex", "DMOMeshTriFactory",
            "DMOMeshQuadFactory", "DMOMeshTetFactory", "DMOMeshHexFactory", "DMOTetClass", "DMOHexClass",
-           "DMOTriFlatClass", "DMOTriClass", "DMOQuadClass", "ProposalModel", "VSDMOError", "Params",
-           "default_params", "version"]
+           "DMOTriFlatClass", "DMOTriClass", "DMOQuadClass", "DMOQuadFlatClass", "BatchDMO", "ProposalModel",
+           "VSDMOError", "Params", "default_params", "version"]
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -207,7 +207,7 @@ class _DMOBase:
 
     def __init__(self, dmo_mesh, qualityCriterium=QualityCriterium.MEAN_RATIO, gridScale: float = 0.5,
                  n_iter: int = 30, fix_boundary: bool = True, use_graph: bool = True, depth: int = 3,
-                 check_monotone: bool = True, active_set: bool = False):
+                 check_monotone: bool = True, active_set: bool = False, grid_n: int = 8):
         self.mesh = dmo_mesh
         p = default_params(dmo_mesh.elem_type)
         p.quality = int(qualityCriterium)
@@ -218,6 +218,7 @@ class _DMOBase:
         p.depth = int(depth)
         p.check_monotone = int(check_monotone)
         p.active_set = int(active_set)
+        p.grid_n = int(grid_n)
         p.flat = self._flat
         self.params = p
         h = C.c_void_p()
@@ -440,3 +441,106 @@ class DMOQuadClass(_DMOBase):
     """``DMO::DMOQuadClass`` (``dmo/DMOQuad.h``): surface quad DMO (meshes without feature
     vertices)."""
     _flat = 0
+
+
+class DMOQuadFlatClass(_DMOBase):
+    """Flat quad DMO: the 2D search of ``DMOTriFlatClass`` with the quad mean ratio against +z
+    (``meanRatioMetricQuad(p, n)``, ``dmo/DMOQualityQuad.h:30-50``); the reference has no
+    flat-quad class. ``grid_n`` 4 or 8."""
+    _flat = 1
+
+
+class BatchDMO:
+    """Many independent flat tri / quad meshes optimised together (one persistent launch per
+    iteration, replayed from a CUDA graph). ``meshes``: list of ``(elem_type, points [n x 3],
+    elems [m x k])`` with mesh-local vertex ids, ``elem_type`` ``TRI`` or ``QUAD``. Stands in
+    for a loop of ``DMOTriFlatClass`` objects, one per mesh."""
+
+    def __init__(self, meshes, color_seed: int = 1, stream=None):
+        types = np.array([int(t) for t, _, _ in meshes], np.int32)
+        nv = np.array([len(p) for _, p, _ in meshes], np.int32)
+        ne = np.array([len(e) for _, _, e in meshes], np.int32)
+        xyz = np.ascontiguousarray(np.concatenate([np.asarray(p, np.float32).reshape(-1, 3) for _, p, _ in meshes]))
+        el = np.ascontiguousarray(np.concatenate([np.asarray(e, np.int32).reshape(-1) for _, _, e in meshes]))
+        self.n_meshes = len(meshes)
+        self.n_vertices = int(nv.sum())
+        self.elem_types, self.nv, self.ne = types, nv, ne
+        h = C.c_void_p()
+        check(_capi.lib().vsdmo_batch_create(len(meshes), _ptr(types), _ptr(nv), _ptr(ne), _ptr(xyz), _ptr(el),
+                                              _capi.HOST, int(color_seed), C.c_void_p(stream), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _capi.lib().vsdmo_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self, _finalizing=sys.is_finalizing):
+        if _finalizing():
+            return
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def iterate(self, n: int = 1):
+        check(_capi.lib().vsdmo_batch_iterate(self.h, int(n)))
+
+    def iterate_async(self, n: int = 1):
+        check(_capi.lib().vsdmo_batch_iterate_async(self.h, int(n)))
+
+    def sync(self):
+        check(_capi.lib().vsdmo_batch_sync(self.h))
+
+    def restart(self):
+        check(_capi.lib().vsdmo_batch_restart(self.h))
+
+    def stats(self, iteration: int):
+        """(min quality, mean quality, elements below the previous minimum) per mesh."""
+        mn = np.zeros(self.n_meshes, np.float32)
+        mean = np.zeros(self.n_meshes, np.float64)
+        below = np.zeros(self.n_meshes, np.int32)
+        check(_capi.lib().vsdmo_batch_stats(self.h, int(iteration), _ptr(mn), _ptr(mean), _ptr(below)))
+        return mn, mean, below
+
+    def positions(self) -> np.ndarray:
+        out = np.zeros((self.n_vertices, 3), np.float32)
+        check(_capi.lib().vsdmo_batch_get_positions(self.h, _ptr(out), _capi.HOST))
+        return out
+
+    def mesh_positions(self, i: int) -> np.ndarray:
+        off = int(self.nv[:i].sum())
+        return self.positions()[off:off + int(self.nv[i])]
+
+    def set_positions(self, xyz):
+        xyz = np.ascontiguousarray(xyz, np.float32)
+        assert xyz.size == 3 * self.n_vertices
+        check(_capi.lib().vsdmo_batch_set_positions(self.h, _ptr(xyz), _capi.HOST))
+
+    def config(self):
+        """(grid_n, depth, lanes) arrays, one entry per mesh."""
+        n = np.zeros(self.n_meshes, np.int32)
+        d = np.zeros(self.n_meshes, np.int32)
+        l = np.zeros(self.n_meshes, np.int32)
+        check(_capi.lib().vsdmo_batch_get_config(self.h, _ptr(n), _ptr(d), _ptr(l)))
+        return n, d, l
+
+    def set_config(self, grid_n, depth, lanes):
+        b = lambda x: np.ascontiguousarray(np.broadcast_to(np.asarray(x, np.int32), (self.n_meshes,)))
+        n, d, l = b(grid_n), b(depth), b(lanes)
+        check(_capi.lib().vsdmo_batch_set_config(self.h, _ptr(n), _ptr(d), _ptr(l)))
+
+    def autotune(self, probe_iters: int = 3) -> str:
+        buf = C.create_string_buffer(4096)
+        check(_capi.lib().vsdmo_batch_autotune(self.h, int(probe_iters), buf, len(buf)))
+        return buf.value.decode()
+
+    def info(self) -> dict:
+        keys = ["meshes", "vertices", "items", "colors", "iterations", "blocks", "max_halfedges"]
+        return {k: int(_capi.lib().vsdmo_batch_info(self.h, i)) for i, k in enumerate(keys)}
+
+    def mesh_info(self, i: int) -> dict:
+        out = np.zeros(8, np.int32)
+        check(_capi.lib().vsdmo_batch_mesh_info(self.h, int(i), _ptr(out)))
+        keys = ["v_off", "nV", "nE", "k", "colors", "free_begin", "free_end", "he_off"]
+        return dict(zip(keys, (int(x) for x in out)))

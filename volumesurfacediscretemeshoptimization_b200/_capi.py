@@ -30,6 +30,10 @@ EXPORTED = [
     "vsdmo_model_get_params", "vsdmo_model_set_params", "vsdmo_model_forward", "vsdmo_model_gradients",
     "vsdmo_model_train", "vsdmo_opt_collect_pairs", "vsdmo_opt_set_model", "vsdmo_opt_learned_counters",
     "vsdmo_debug_gemm_bf16", "vsdmo_opt_proposals",
+    "vsdmo_batch_create", "vsdmo_batch_destroy", "vsdmo_batch_iterate", "vsdmo_batch_iterate_async",
+    "vsdmo_batch_sync", "vsdmo_batch_restart", "vsdmo_batch_stats", "vsdmo_batch_get_positions",
+    "vsdmo_batch_set_positions", "vsdmo_batch_get_config", "vsdmo_batch_set_config", "vsdmo_batch_autotune",
+    "vsdmo_batch_info", "vsdmo_batch_mesh_info",
 ]
 
 
@@ -138,6 +142,32 @@ def lib():
     L.vsdmo_opt_proposals.argtypes = [P, I, P]
     L.vsdmo_debug_gemm_bf16.restype = S
     L.vsdmo_debug_gemm_bf16.argtypes = [P, P, I, I, I, P]
+    L.vsdmo_batch_create.restype = S
+    L.vsdmo_batch_create.argtypes = [I, P, P, P, P, P, I, U, P, C.POINTER(P)]
+    L.vsdmo_batch_destroy.restype = None
+    L.vsdmo_batch_destroy.argtypes = [P]
+    for name in ("vsdmo_batch_iterate", "vsdmo_batch_iterate_async"):
+        getattr(L, name).restype = S
+        getattr(L, name).argtypes = [P, I]
+    for name in ("vsdmo_batch_sync", "vsdmo_batch_restart"):
+        getattr(L, name).restype = S
+        getattr(L, name).argtypes = [P]
+    L.vsdmo_batch_stats.restype = S
+    L.vsdmo_batch_stats.argtypes = [P, I, P, P, P]
+    L.vsdmo_batch_get_positions.restype = S
+    L.vsdmo_batch_get_positions.argtypes = [P, P, I]
+    L.vsdmo_batch_set_positions.restype = S
+    L.vsdmo_batch_set_positions.argtypes = [P, P, I]
+    L.vsdmo_batch_get_config.restype = S
+    L.vsdmo_batch_get_config.argtypes = [P, P, P, P]
+    L.vsdmo_batch_set_config.restype = S
+    L.vsdmo_batch_set_config.argtypes = [P, P, P, P]
+    L.vsdmo_batch_autotune.restype = S
+    L.vsdmo_batch_autotune.argtypes = [P, I, C.c_char_p, I]
+    L.vsdmo_batch_info.restype = C.c_long
+    L.vsdmo_batch_info.argtypes = [P, I]
+    L.vsdmo_batch_mesh_info.restype = S
+    L.vsdmo_batch_mesh_info.argtypes = [P, I, P]
     _lib = L
     return L
 

@@ -68,6 +68,7 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
         launch_dmo_hex(m, L, s);
     }
     else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
+    else if (o->mode == MODE_FLAT) launch_dmo_flat(m, L, o->p.grid_n, 32, s);
     else launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, s);
 }
 
@@ -415,7 +416,10 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     if (params) p = *params; else vsdmo_params_default(mesh->m.type, &p);
     const Mesh& m = mesh->m;
     if (p.quality != VSDMO_MEAN_RATIO) return fail(VSDMO_E_UNSUPPORTED, "only MEAN_RATIO is implemented");
-    if (p.grid_n != 8) return fail(VSDMO_E_UNSUPPORTED, "only an 8-point grid per axis is implemented");
+    const bool flat2d = (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) && (p.flat < 0 ? m.isFlat : p.flat);
+    if (p.grid_n != 8 && !(flat2d && p.grid_n == 4))
+        return fail(VSDMO_E_UNSUPPORTED, "only an 8-point grid per axis is implemented (4 or 8 for flat meshes)");
+    if (flat2d && p.grid_n == 4 && p.depth > 4) return fail(VSDMO_E_ARG, "depth must be in 1..4 with a 4-point grid");
     if (p.depth < 1 || p.depth > 8) return fail(VSDMO_E_ARG, "depth must be in 1..8");
     if (!(p.grid_scale > 0.f) || !std::isfinite(p.grid_scale)) return fail(VSDMO_E_ARG, "grid_scale must be positive");
     if (p.n_iter < 0) return fail(VSDMO_E_ARG, "n_iter must be >= 0");
@@ -434,11 +438,18 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->mode = MODE_HEX;
         o->kind = MK_HEX;
         for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
-    } else if (m.type == VSDMO_TRI && (p.flat < 0 ? m.isFlat : p.flat)) {
+    } else if (m.type == VSDMO_TRI && flat2d && p.grid_n == 8) {
         if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "sliding boundary vertices are not implemented yet; set fix_boundary=1");
         if (m.maxHE > dmo_tri2d_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
         o->mode = MODE_TRI2D;
         o->kind = MK_TRI2D;
+        for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+    } else if (flat2d) {
+        // flat quads (any grid) and flat triangles with a 4-point grid: the general 2D search
+        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "sliding boundary vertices are not implemented yet; set fix_boundary=1");
+        if (m.maxHE > flat_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
+        o->mode = MODE_FLAT;
+        o->kind = m.type == VSDMO_QUAD ? MK_QUAD2D : MK_TRI2D;
         for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
     } else if (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) {
         if (m.nFeature > 0)

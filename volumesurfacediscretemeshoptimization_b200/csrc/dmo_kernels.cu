@@ -973,6 +973,18 @@ __device__ __forceinline__ float q_quad(float4 p0, float4 p1, float4 p2, float4 
     return (2.f * (a1 + a2)) / l;
 }
 
+// meanRatioMetricQuad(p, n) with n = +z (dmo/DMOQualityQuad.h:30-50) for flat quads: -1 when a
+// corner turns clockwise, else 2 (A1 + A2) / sum |e|^2 (the corner areas are the z components)
+__device__ __forceinline__ float q_quad2d(float4 p0, float4 p1, float4 p2, float4 p3) {
+    const float e0x = p1.x - p0.x, e0y = p1.y - p0.y, e1x = p2.x - p1.x, e1y = p2.y - p1.y;
+    const float e2x = p3.x - p2.x, e2y = p3.y - p2.y, e3x = p0.x - p3.x, e3y = p0.y - p3.y;
+    const float l = (((e0x * e0x + e0y * e0y) + (e1x * e1x + e1y * e1y)) + (e2x * e2x + e2y * e2y)) + (e3x * e3x + e3y * e3y);
+    const float c1 = e1x * (-e0y) - e1y * (-e0x);
+    const float c2 = e3x * (-e2y) - e3y * (-e2x);
+    if (c1 < 0.f || c2 < 0.f) return -1.f;
+    return (2.f * (c1 + c2)) / l;
+}
+
 // shapeMetricHex (dmo/DMOQualityHex.h:54-71) in the reference's operation order, with cbrtf
 __device__ float q_hex(const float4* __restrict__ pos, const int* __restrict__ h) {
     float v[8][3];
@@ -1021,9 +1033,9 @@ __device__ __forceinline__ float element_quality(const int* __restrict__ el, int
         const int4 t = reinterpret_cast<const int4*>(el)[e];
         return q_tet(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
     }
-    if (kind == MK_QUAD) {
+    if (kind == MK_QUAD || kind == MK_QUAD2D) {
         const int4 t = reinterpret_cast<const int4*>(el)[e];
-        return q_quad(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
+        return kind == MK_QUAD ? q_quad(pos[t.x], pos[t.y], pos[t.z], pos[t.w]) : q_quad2d(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
     }
     const int* t = el + 3 * e;
     if (kind == MK_TRI3D) return q_tri3d(pos[t[0]], pos[t[1]], pos[t[2]]);

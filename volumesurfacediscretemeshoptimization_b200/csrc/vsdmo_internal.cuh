@@ -181,7 +181,7 @@ void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const 
 int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
 
 // Element metric used by the quality kernels.
-enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4 };
+enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4, MK_QUAD2D = 5 };
 
 // Per-iteration statistics written by the quality kernel.
 struct IterStats {

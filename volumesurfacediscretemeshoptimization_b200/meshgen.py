@@ -59,6 +59,24 @@ def tri_grid(n: int = 64, seed: int | None = 0, jitter: float = 0.4):
     return xyz.astype(np.float32), tris.astype(np.int32)
 
 
+def quad_grid(n: int = 64, seed: int | None = 0, jitter: float = 0.4):
+    """``n x n`` vertex grid on the unit square as counter-clockwise quads, interior vertices
+    displaced by ``U(-jitter*h, jitter*h)`` per axis, boundary exact, z = 0."""
+    h = 1.0 / (n - 1)
+    j, i = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    xyz = np.zeros((n * n, 3), dtype=np.float64)
+    xyz[:, 0] = (i * h).ravel()
+    xyz[:, 1] = (j * h).ravel()
+    cj, ci = np.meshgrid(np.arange(n - 1), np.arange(n - 1), indexing="ij")
+    v00 = (cj * n + ci).ravel()
+    quads = np.stack([v00, v00 + 1, v00 + n + 1, v00 + n], 1)
+    if seed is not None and jitter > 0:
+        inner = ((i > 0) & (i < n - 1) & (j > 0) & (j < n - 1)).ravel()
+        r = _rng(seed).uniform(-jitter * h, jitter * h, size=(inner.sum(), 2))
+        xyz[inner, :2] += r
+    return xyz.astype(np.float32), quads.astype(np.int32)
+
+
 _KUHN = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
 
 
@@ -245,6 +263,24 @@ def config3_quad(seed: int = 0, nu: int = 512, nv: int = 256):
     larger noise folds some of them into feature vertices under the 20 degree rule."""
     v, q = torus_quads(nu, nv)
     return perturb_surface(v, q, seed, tangential=0.2), q
+
+
+def config4(seed: int = 0, count: int = 256, v_min: int = 500, v_max: int = 50000):
+    """256 independent jittered structured 2D grids, triangles and quads alternating, vertex
+    counts log-uniform in [500, 50,000] (grid side round(sqrt(V))), interior jitter 0.4h.
+    Returns a list of (elem_type, xyz, elems) with elem_type 0 = triangles, 1 = quads."""
+    g = _rng(seed)
+    sizes = np.exp(g.uniform(np.log(v_min), np.log(v_max), size=count))
+    out = []
+    for m, v in enumerate(sizes):
+        n = max(4, int(round(np.sqrt(v))))
+        if m % 2 == 0:
+            xyz, el = tri_grid(n, seed=seed * 1000 + m, jitter=0.4)
+            out.append((0, xyz, el))
+        else:
+            xyz, el = quad_grid(n, seed=seed * 1000 + m, jitter=0.4)
+            out.append((1, xyz, el))
+    return out
 
 
 def config5(seed: int = 0, n: int = 100):
