@@ -317,6 +317,8 @@ def run_ours(args):
     mesh.close()
     if r == 0 and world == 1 and not args.no_learned:
         line["learned"] = learned_time_to_quality(dev, stream)
+    if r == 0 and world == 1 and not args.no_batched:
+        line["batched"] = batched_throughput(dev, stream)
     if r == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(xyz, tets)
     if r == 0:
@@ -326,40 +328,15 @@ def run_ours(args):
     return 0
 
 
-LEARNED_CFG = {"reduced_n": 4, "reduced_depth": 2, "reduced_scale": 0.012,
-               "train_steps": (6000, 2000), "train_lr": (1e-3, 2e-4), "batch": 4096}
-
-
 def learned_time_to_quality(dev, stream):
     """Trains the proposal network on plain-DMO pairs, then times plain vs learned DMO on the
     100^3 tet cube to plain's final (20-iteration) minimum quality."""
     import torch
     import volumesurfacediscretemeshoptimization_b200 as V
     from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+    from volumesurfacediscretemeshoptimization_b200.learned import DEFAULTS as LEARNED_CFG, train_proposal
     sp = stream.cuda_stream
-    t0 = time.perf_counter()
-    # training pairs from plain DMO on a separate seeded 48^3 cube
-    xyz, tets = G.config2(seed=1000)
-    tm = V.DMOMeshTet(xyz, tets, stream=sp)
-    topt = V.DMOTetClass(tm, n_iter=N_ITER)
-    cap = (tm.info["nV"] - tm.info["nSurf"]) * N_ITER
-    feats = torch.empty(cap * 96, dtype=torch.float32, device=dev)
-    targ = torch.empty(cap * 3, dtype=torch.float32, device=dev)
-    torch.cuda.synchronize()
-    n_pairs = topt.collect_pairs(N_ITER, feats.data_ptr(), targ.data_ptr(), cap)
-    t_collect = time.perf_counter() - t0
-    model = V.ProposalModel(seed=0, stream=sp)
-    t1 = time.perf_counter()
-    losses = []
-    for k, (steps, lr) in enumerate(zip(LEARNED_CFG["train_steps"], LEARNED_CFG["train_lr"])):
-        h = model.train(None, None, steps=steps, batch=LEARNED_CFG["batch"], lr=lr, seed=k,
-                        device_ptrs=(feats.data_ptr(), targ.data_ptr()), n_rows=n_pairs)
-        losses.append(float(h[-50:].mean()))
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t1
-    tvar = float(targ.view(-1, 3)[:n_pairs].var(0).mean().item())
-    topt.close(); tm.close()
-    del feats, targ
+    model, training = train_proposal(stream, LEARNED_CFG)
     # evaluation mesh
     xyz5, tets5 = G.config5()
     m5 = V.DMOMeshTet(xyz5, tets5, stream=sp)
@@ -405,12 +382,99 @@ def learned_time_to_quality(dev, stream):
         "reduced_accepted": acc, "fallbacks": fb, "fallbacks_moved": fb_moved,
         "reduced_accept_fraction": acc / max(1, acc + fb),
         "search": {k: LEARNED_CFG[k] for k in ("reduced_n", "reduced_depth", "reduced_scale")},
-        "training": {"pairs": n_pairs, "source": "20 plain iterations, tet cube 48^3 seed 1000",
-                     "steps": list(LEARNED_CFG["train_steps"]), "lr": list(LEARNED_CFG["train_lr"]),
-                     "batch": LEARNED_CFG["batch"], "final_mse": losses[-1], "target_variance": tvar,
-                     "collect_s": t_collect, "train_s": t_train},
+        "training": training,
         "plain_ms_per_iteration": tp, "learned_ms_per_iteration": tl,
         "timing": "sum of per-iteration CUDA-event times on the library stream",
+    }
+
+
+BATCH_ITERS = 10
+
+
+def batched_throughput(dev, stream):
+    """256 flat tri / quad meshes (vertex counts log-uniform in [500, 50,000], jitter 0.4h)
+    optimised together: one persistent launch per iteration replayed from a CUDA graph, with
+    the reference configuration (8 per axis, 3 levels, one warp per vertex) and with the
+    autotuned per-bucket configuration, against a loop over one single-mesh optimiser per mesh
+    (the reference runs one mesh per DMOTriFlatClass object). 10 iterations each, from the
+    same start; CUDA-event times on the library stream."""
+    import torch
+    import volumesurfacediscretemeshoptimization_b200 as V
+    from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+    sp = stream.cuda_stream
+    meshes = G.config4()
+    t0 = time.perf_counter()
+    b = V.BatchDMO(meshes, stream=sp)
+    build_s = time.perf_counter() - t0
+    x0 = b.positions()
+    infos = [b.mesh_info(i) for i in range(len(meshes))]
+    n_free = sum(m["free_end"] - m["free_begin"] for m in infos)
+
+    def timed(n):
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            b.iterate_async(n)
+            e.record(stream)
+        b.sync()
+        torch.cuda.synchronize()
+        return a.elapsed_time(e)
+
+    def summary():
+        mn, mean, _ = b.stats(BATCH_ITERS)
+        return {"min_of_min_quality": float(mn.min()), "mean_of_mean_quality": float(mean.mean())}
+
+    def run_config():
+        timed(2)                                  # warm-up (graph capture, clocks)
+        b.set_positions(x0); b.restart()
+        ms = timed(BATCH_ITERS)
+        return ms, summary()
+
+    ms_ref, q_ref = run_config()
+    t1 = time.perf_counter()
+    report = b.autotune(probe_iters=3)
+    tune_s = time.perf_counter() - t1
+    b.set_positions(x0); b.restart()
+    ms_tuned, q_tuned = run_config()
+    info = b.info()
+    nq, depth, lanes = b.config()
+    b.close()
+    # the per-mesh loop: one single-mesh optimiser per mesh, each iterated in turn
+    objs = []
+    for t, xyz, el in meshes:
+        m = (V.DMOMeshTri if t == 0 else V.DMOMeshQuad)(xyz, el, stream=sp)
+        o = (V.DMOTriFlatClass if t == 0 else V.DMOQuadFlatClass)(m, n_iter=BATCH_ITERS)
+        o.iterate(1)                              # warm-up (graph capture)
+        m.set_positions(xyz, original_order=True)
+        o.restart()
+        objs.append((m, o))
+    torch.cuda.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        a.record(stream)
+        for m, o in objs:
+            o.iterate(BATCH_ITERS)
+        e.record(stream)
+    torch.cuda.synchronize()
+    ms_loop = a.elapsed_time(e)
+    for m, o in objs:
+        o.close(); m.close()
+    ups = lambda ms: n_free * BATCH_ITERS / (ms / 1e3)
+    return {
+        "workload": "256 flat grids, tri and quad alternating, vertices log-uniform in [500, 50000] "
+                    "(3261948 vertices), jitter 0.4h, boundary fixed, seed 0",
+        "free_vertices": n_free, "iterations": BATCH_ITERS,
+        "reference_config": {"ms": ms_ref, "vertex_updates_per_s": ups(ms_ref), **q_ref,
+                             "grid": "8x8", "levels": 3, "lanes_per_vertex": 32},
+        "autotuned": {"ms": ms_tuned, "vertex_updates_per_s": ups(ms_tuned), **q_tuned,
+                      "buckets": report.strip().splitlines(), "autotune_s": tune_s,
+                      "configs_used": sorted({(int(a), int(b_), int(c)) for a, b_, c in zip(nq, depth, lanes)})},
+        "per_mesh_loop": {"ms": ms_loop, "vertex_updates_per_s": ups(ms_loop),
+                          "how": "256 single-mesh optimisers (8x8, 3 levels), each iterate(10) in turn"},
+        "speedup_batched_over_loop": ms_loop / ms_ref,
+        "work_items_per_iteration": info["items"], "colour_classes": info["colors"],
+        "persistent_ctas": info["blocks"], "build_s": build_s,
+        "timing": "CUDA events on the library stream; one graph replay per iteration",
     }
 
 
@@ -422,6 +486,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

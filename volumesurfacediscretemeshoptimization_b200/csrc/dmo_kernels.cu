@@ -217,6 +217,91 @@ __device__ __forceinline__ void tet_lane_best(const float4* __restrict__ co, int
     }
 }
 
+// ---- candidate filter of the tet search --------------------------------------------------------
+// The ring key of a candidate is a minimum over the ring's tets, so the minimum over any subset
+// of them bounds it from above. A level can only move the vertex to a candidate whose key
+// beats qLast, so a candidate whose key over a few tets is already below qLast can never be
+// chosen: the search evaluates the TET_CRIT tets with the smallest keys at the level's centre
+// for all 512 candidates, keeps the candidates that are not below qLast (with a relative
+// margin of 2^-14 that covers the rounding of the fraction comparisons), and evaluates the
+// full ring only for those, in the same operations and tet order as the plain search. The
+// winner, and whether the vertex moves, are the same as without the filter: every candidate
+// that beats qLast survives, and no discarded candidate can tie with or exceed one that does.
+constexpr int TET_CRIT = 4;      // tets of the filter
+constexpr int TET_LIST = 256;    // survivors per warp evaluated from a list (more: full search)
+
+// (num, den, det) of tet t at (x, y, z): the operations of tet_key1
+__device__ __forceinline__ float tet_piece_key(const float4* __restrict__ co, int t, float x, float y, float z) {
+    const float4 c0 = co[2 * t], c1 = co[2 * t + 1];
+    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    const float det = fmaf(c0.z, z, fmaf(c0.y, y, fmaf(c0.x, x, c0.w)));
+    const float L = ((c1.w + fmaf(c1.x, x, tx)) + fmaf(c1.y, y, ty)) + fmaf(c1.z, z, tz);
+    return det < 0.f ? det : (det * det) / ((L * L) * L);
+}
+
+// the TET_CRIT tets of smallest key at (x, y, z) (ties: lower tet index), the same on all lanes
+__device__ __forceinline__ void tet_critical(const float4* __restrict__ co, int k, float x, float y, float z, int lane,
+                                             int (&crit)[TET_CRIT]) {
+#pragma unroll
+    for (int r = 0; r < TET_CRIT; ++r) {
+        float bk = FLT_MAX;
+        int bt = 1 << 30;
+        for (int t = lane; t < k; t += 32) {
+            bool used = false;
+#pragma unroll
+            for (int q = 0; q < r; ++q) used |= (crit[q] == t);
+            if (used) continue;
+            const float kt = tet_piece_key(co, t, x, y, z);
+            if (kt < bk || (kt == bk && t < bt) || bt == (1 << 30)) { bk = kt; bt = t; }
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const float ok = __shfl_xor_sync(FULL, bk, o);
+            const int ot = __shfl_xor_sync(FULL, bt, o);
+            if (ot != (1 << 30) && (bt == (1 << 30) || ok < bk || (ok == bk && ot < bt))) { bk = ok; bt = ot; }
+        }
+        crit[r] = bt < k ? bt : 0;
+    }
+}
+
+// the lane's 16 candidates (fixed x, y[2], z[8]) over the critical tets: bit jj * 8 + q set when
+// the candidate survives (its key over the subset is not below thr)
+__device__ __forceinline__ unsigned tet_filter(const float4* __restrict__ co, const int (&crit)[TET_CRIT], int m,
+                                               float x, const float* y, const float* z, const float* tz, float thr) {
+    const float tx = (3.0f * x) * x;
+    const float ty[2] = { (3.0f * y[0]) * y[0], (3.0f * y[1]) * y[1] };
+    float N[2][NQ], D[2][NQ], dm[2][NQ];
+#pragma unroll
+    for (int r = 0; r < TET_CRIT; ++r) {
+        if (r >= m) break;
+        const int t = crit[r];
+        const float4 K0 = co[2 * t], K1 = co[2 * t + 1];
+        const float detA = fmaf(K0.x, x, K0.w);
+        const float LA = K1.w + fmaf(K1.x, x, tx);
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+            const float detB = fmaf(K0.y, y[jj], detA), LB = LA + fmaf(K1.y, y[jj], ty[jj]);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const float det = fmaf(K0.z, z[q], detB), L = LB + fmaf(K1.z, z[q], tz[q]);
+                const float num = det * det, den = (L * L) * L;
+                if (r == 0) { N[jj][q] = num; D[jj][q] = den; dm[jj][q] = det; continue; }
+                if (num * D[jj][q] < N[jj][q] * den) { N[jj][q] = num; D[jj][q] = den; }
+                dm[jj][q] = fminf(dm[jj][q], det);
+            }
+        }
+    }
+    unsigned alive = 0;
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const float key = dm[jj][q] < 0.f ? dm[jj][q] : N[jj][q] / D[jj][q];
+            if (!(key < thr)) alive |= 1u << (jj * 8 + q);
+        }
+    return alive;
+}
+
 // Setup of one tet vertex shared by the plain and the learned search: per-axis extent of the
 // ring (DMOTetImplCub.h:54-64), the exact power-of-two scale 2^ex and the element coefficients
 // in shared memory. Returns false when the ring is degenerate (the vertex is left alone).
@@ -259,9 +344,9 @@ __device__ __forceinline__ float4 tet_unscale(float4 c0, float dx, float dy, flo
 // The plain hierarchical search (DMOTetImplCub.h:66-136) from the local origin: depth levels
 // of 8 x 8 x 8 candidates, moving on strict improvement of the ring key qLast. Returns whether
 // the vertex moved; (dx, dy, dz) is the new position in scaled local coordinates.
-__device__ __forceinline__ bool tet_plain_search(const float4* __restrict__ co, int k, float sx, float sy, float sz,
-                                                 float grid_scale, int depth, int lane, float qLast, float& dx,
-                                                 float& dy, float& dz) {
+__device__ __forceinline__ bool tet_plain_search(const float4* __restrict__ co, int* __restrict__ list, int k, float sx,
+                                                 float sy, float sz, float grid_scale, int depth, int lane, float qLast,
+                                                 float& dx, float& dy, float& dz) {
     const int ci = lane & 7, cj = lane >> 3;
     const float oi = grid_offset(ci), oj0 = grid_offset(cj), oj1 = grid_offset(cj + 4);
     dx = 0.f; dy = 0.f; dz = 0.f;
@@ -276,12 +361,41 @@ __device__ __forceinline__ bool tet_plain_search(const float4* __restrict__ co, 
         for (int q = 0; q < NQ; ++q) { z[q] = fmaf(grid_offset(q), Sz, dz); tz[q] = (3.0f * z[q]) * z[q]; }
         float bk = -FLT_MAX;
         int bi = 1 << 30;
+        // filter: candidates already below qLast over the centre's critical tets are dropped
+        int crit[TET_CRIT];
+        tet_critical(co, k, dx, dy, dz, lane, crit);
+        const float thr = qLast - (fabsf(qLast) * 0x1p-14f + 1e-37f);
+        const unsigned alive = tet_filter(co, crit, min(TET_CRIT, k), x, y, z, tz, thr);
+        const int cnt = __popc(alive);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int n = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += n;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        if (total > TET_LIST) {
 #if TET_SPLIT_Y
-        tet_lane_best<1>(co, k, x, &y[0], z, tz, ci, cj, 0, bk, bi);
-        tet_lane_best<1>(co, k, x, &y[1], z, tz, ci, cj, 1, bk, bi);
+            tet_lane_best<1>(co, k, x, &y[0], z, tz, ci, cj, 0, bk, bi);
+            tet_lane_best<1>(co, k, x, &y[1], z, tz, ci, cj, 1, bk, bi);
 #else
-        tet_lane_best<2>(co, k, x, y, z, tz, ci, cj, 0, bk, bi);
+            tet_lane_best<2>(co, k, x, y, z, tz, ci, cj, 0, bk, bi);
 #endif
+        } else if (total > 0) {
+            int at = incl - cnt;
+            for (unsigned a = alive; a; a &= a - 1) {
+                const int bit = __ffs(a) - 1;
+                list[at++] = ci + 8 * (cj + 4 * (bit >> 3)) + 64 * (bit & 7);
+            }
+            __syncwarp();
+            for (int j = lane; j < total; j += 32) {
+                const int idx = list[j];
+                const float key = tet_key1(co, k, fmaf(grid_offset(idx & 7), Sx, dx),
+                                           fmaf(grid_offset((idx >> 3) & 7), Sy, dy), fmaf(grid_offset(idx >> 6), Sz, dz));
+                if (key > bk || (key == bk && idx < bi)) { bk = key; bi = idx; }
+            }
+            __syncwarp();
+        }
         warp_argmax(bk, bi);
         if (bi < NQ * NQ * NQ && qLast < bk) {
             const float nx = fmaf(grid_offset(bi & 7), Sx, dx);
@@ -322,6 +436,7 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
         return;
     }
     float4* co = smem + (size_t)w * maxk * 2;
+    int* list = reinterpret_cast<int*>(smem + (size_t)TET_WARPS * maxk * 2) + w * TET_LIST;
     const int b = rowptr[v], k = rowptr[v + 1] - b;
     if (k <= 0 || k > maxk) return;
     const float4 c0 = pos[v];
@@ -330,7 +445,7 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
     if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
     const float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
     float dx, dy, dz;
-    const bool moved = tet_plain_search(co, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
+    const bool moved = tet_plain_search(co, list, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
     if (moved && lane == 0) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
     if (dirty) {
         if (moved) tet_mark_ring(hf, b, k, lane, dirty);
@@ -347,6 +462,7 @@ k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
     extern __shared__ float4 smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     float4* co = smem + (size_t)w * maxk * 2;
+    int* slist = reinterpret_cast<int*>(smem + (size_t)TET_WARPS * maxk * 2) + w * TET_LIST;
     const int n = *count;
     for (int idx = blockIdx.x * TET_WARPS + w; idx < n; idx += gridDim.x * TET_WARPS) {
         const int v = list[idx];
@@ -358,7 +474,7 @@ k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
         if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) continue;
         const float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
         float dx, dy, dz;
-        const bool moved = tet_plain_search(co, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
+        const bool moved = tet_plain_search(co, slist, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
         if (moved && lane == 0) {
             pos[v] = tet_unscale(c0, dx, dy, dz, ex);
             atomicAdd(moved_count, 1ull);
@@ -1123,17 +1239,19 @@ void launch_dmo_hex(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
     VSDMO_CHECK_LAUNCH();
 }
 
+// coefficients of every warp's ring, then every warp's survivor list
+size_t tet_smem_bytes(int maxk) { return (size_t)TET_WARPS * maxk * 2 * sizeof(float4) + (size_t)TET_WARPS * TET_LIST * sizeof(int); }
+
 // Raises the dynamic shared-memory limit of the grid-search kernels (called once per
 // optimiser, outside any stream capture, on the current device).
 void prepare_dmo_kernels() {
-    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tet_smem_bytes(TET_MAX_RING)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tri2d, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TRI_WARPS * TRI_MAX_RING * 2 * (int)sizeof(float4)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet_learned, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet_list, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TET_WARPS * TET_MAX_RING * 2 * (int)sizeof(float4)));
+                                    (int)tet_smem_bytes(TET_MAX_RING)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_hex, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     HEX_WARPS * HEX_MAX_RING * HEX_CO * (int)sizeof(float)));
 }
@@ -1145,7 +1263,7 @@ void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s, uint8_t* 
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
     const int maxk = m.maxTets;
-    const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
+    const size_t smem = tet_smem_bytes(maxk);
     k_dmo_tet<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
         m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk, dirty, skipped);
     VSDMO_CHECK_LAUNCH();
@@ -1185,7 +1303,7 @@ void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, i
     VSDMO_CHECK_LAUNCH();
     // fallback: the plain search over the queued vertices, a fixed grid striding over the list
     const int blocks = std::min((n + TET_WARPS - 1) / TET_WARPS, 148 * 4);
-    k_dmo_tet_list<<<blocks, TET_WARPS * 32, smem, s>>>(m.pos.p, m.hf_rowptr.p, m.hf.p, fb_list, fb_count, L.grid_scale,
+    k_dmo_tet_list<<<blocks, TET_WARPS * 32, tet_smem_bytes(maxk), s>>>(m.pos.p, m.hf_rowptr.p, m.hf.p, fb_list, fb_count, L.grid_scale,
                                                        L.depth, maxk, dirty, counters + 2);
     VSDMO_CHECK_LAUNCH();
 }
