@@ -285,6 +285,15 @@ VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t opt, vsdmo_model_t model,
 /* Network proposals [n x 3] (host) of colour class `color` at the current positions, computed
  * by the fused inference kernel the learned search uses (for tests and inspection). */
 VSDMO_API vsdmo_status vsdmo_opt_proposals(vsdmo_opt_t opt, int color, float* out);
+/* When the learned mode runs the network (no counterpart in the reference, which has no
+ * learned mode). Iterations before once_after (counted from the last restart; all of them
+ * when once_after = -1, the default) run it before every colour class, from the positions
+ * that class sees. Iterations from once_after on run it once for all interior vertices, from
+ * the positions at the start of the iteration: one launch instead of one per class, but a
+ * class's proposals do not see the moves of the classes before it in the same iteration,
+ * which costs fallbacks while vertices still move far. The reduced search and the fallback
+ * always evaluate the current ring, so the minimum quality stays monotone either way. */
+VSDMO_API vsdmo_status vsdmo_opt_set_proposal_schedule(vsdmo_opt_t opt, int once_after);
 /* Counters since vsdmo_opt_set_model / vsdmo_opt_restart: [0] vertex updates accepted from the
  * reduced search, [1] fallbacks to the plain search, [2] fallbacks that moved the vertex,
  * [3] vertices skipped by the active set (plain and learned mode). */

@@ -189,3 +189,27 @@ def test_learned_mode_monotone_and_gain(vsdmo):
         res[name] = (acc, fb, mean[-1])
     # what training gains: more updates accepted from the cheap reduced search
     assert res["trained"][0] > 2 * res["untrained"][0] + 100, res
+
+
+def test_learned_proposals_once_per_iteration(vsdmo):
+    """One network launch per iteration (stale proposals for later colour classes): the
+    reduced search and the fallback judge the current ring, so the minimum stays monotone."""
+    trained, _ = _train_on_plain_pairs(vsdmo, seed=22)
+    xyz, tets = G.tet_cube(14, seed=6)
+    mesh = vsdmo.DMOMeshTet(xyz, tets)
+    opt = vsdmo.DMOTetClass(mesh, n_iter=5)
+    q0 = opt.getQuality()
+    opt.set_model(trained, 4, 2)
+    opt.set_proposal_schedule(2)          # iterations 0, 1 per colour class, then once
+    opt.optimize()
+    mn, mean = opt.history()
+    assert np.all(np.diff(mn) >= -1e-6)
+    assert mn[-1] > q0 and mean[-1] > mean[0]
+    acc, fb, _, _ = opt.learned_counters()
+    assert acc + fb == 5 * (mesh.info["nV"] - mesh.info["nSurf"]) and acc > fb
+    # the whole run with one launch per iteration
+    opt2 = vsdmo.DMOTetClass(vsdmo.DMOMeshTet(xyz, tets), n_iter=1)
+    opt2.set_model(trained, 4, 2)
+    opt2.set_proposal_schedule(0)
+    opt2.iterate(1)
+    assert opt2.learned_counters()[0] > 0

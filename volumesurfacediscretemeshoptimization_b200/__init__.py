@@ -336,6 +336,12 @@ class DMOTetClass(_DMOBase):
                                               reduced_scale))
         self._model = model
 
+    def set_proposal_schedule(self, once_after: int = -1):
+        """Iterations (since the restart) from ``once_after`` on run the network once for all
+        interior vertices from the positions at the iteration's start; earlier ones (all, with
+        -1) run it before every colour class."""
+        check(_capi.lib().vsdmo_opt_set_proposal_schedule(self.h, int(once_after)))
+
     def proposals(self, color: int) -> np.ndarray:
         """Network proposals [n x 3] of one colour class (fused inference kernel)."""
         r = self.mesh.array(A_COL_INNER)

@@ -29,7 +29,7 @@ EXPORTED = [
     "vsdmo_quality_reduce_noalloc", "vsdmo_model_num_params", "vsdmo_model_create", "vsdmo_model_destroy",
     "vsdmo_model_get_params", "vsdmo_model_set_params", "vsdmo_model_forward", "vsdmo_model_gradients",
     "vsdmo_model_train", "vsdmo_opt_collect_pairs", "vsdmo_opt_set_model", "vsdmo_opt_learned_counters",
-    "vsdmo_debug_gemm_bf16", "vsdmo_opt_proposals",
+    "vsdmo_debug_gemm_bf16", "vsdmo_opt_proposals", "vsdmo_opt_set_proposal_schedule",
     "vsdmo_batch_create", "vsdmo_batch_destroy", "vsdmo_batch_iterate", "vsdmo_batch_iterate_async",
     "vsdmo_batch_sync", "vsdmo_batch_restart", "vsdmo_batch_stats", "vsdmo_batch_get_positions",
     "vsdmo_batch_set_positions", "vsdmo_batch_get_config", "vsdmo_batch_set_config", "vsdmo_batch_autotune",
@@ -138,6 +138,8 @@ def lib():
     L.vsdmo_opt_set_model.argtypes = [P, P, I, I, F]
     L.vsdmo_opt_learned_counters.restype = S
     L.vsdmo_opt_learned_counters.argtypes = [P, P]
+    L.vsdmo_opt_set_proposal_schedule.restype = S
+    L.vsdmo_opt_set_proposal_schedule.argtypes = [P, I]
     L.vsdmo_opt_proposals.restype = S
     L.vsdmo_opt_proposals.argtypes = [P, I, P]
     L.vsdmo_debug_gemm_bf16.restype = S

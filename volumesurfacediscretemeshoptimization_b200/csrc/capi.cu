@@ -59,8 +59,10 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
         // learned proposal: ring features + network (one fused tensor-core kernel) -> reduced
         // grid around the proposal -> plain search for the vertices it did not improve
         const int n = L.v1 - L.v0;
-        o->model->m.infer_tet(m.pos.p, o->nb.p, o->nbn.p, o->nb_base, L.v0, n, o->ws.Y.p, mlp::OUTP, s);
-        launch_dmo_tet_learned(m, L, o->ws.Y.p, mlp::OUTP, o->reduced_n, o->reduced_depth, o->reduced_scale,
+        const float* Y = o->ws.Y.p;
+        if (o->proposals_once) Y = o->Yall.p + (size_t)(L.v0 - o->nb_base) * mlp::OUTP;
+        else o->model->m.infer_tet(m.pos.p, o->nb.p, o->nbn.p, o->nb_base, L.v0, n, o->ws.Y.p, mlp::OUTP, s);
+        launch_dmo_tet_learned(m, L, Y, mlp::OUTP, o->reduced_n, o->reduced_depth, o->reduced_scale,
                                o->counters.p, o->dirty.p, o->fb_list.p, o->fb_count.p, s);
     } else if (o->mode == MODE_TET) {
         launch_dmo_tet(m, L, s, o->dirty.p, o->dirty.p ? o->counters.p + 3 : nullptr);
@@ -89,6 +91,10 @@ namespace {
 
 void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
     const Mesh& m = o->mesh->m;
+    // proposals of every colour class from the positions at the start of the iteration
+    if (o->mode == MODE_TET && o->model && o->proposals_once)
+        o->model->m.infer_tet(m.pos.p, o->nb.p, o->nbn.p, o->nb_base, o->nb_base, m.nV - o->nb_base, o->Yall.p,
+                              mlp::OUTP, s);
     for (int c = 0; c < (int)o->ranges.size(); ++c) launch_color(o, c, s);
     if (o->mode == MODE_SURF) {
         launch_update_nn(m, o->X0.p, o->nn.p, s);
@@ -131,12 +137,12 @@ void ensure_capacity(vsdmo_opt_s* o, int need) {
         VSDMO_CUDA(cudaMemcpyAsync(ns.p, o->stats.p, sizeof(IterStats) * o->capacity, cudaMemcpyDeviceToDevice, s));
     o->stats = std::move(ns);
     o->capacity = cap;
-    if (o->exec) { cudaGraphExecDestroy(o->exec); o->exec = nullptr; }
-    if (o->graph) { cudaGraphDestroy(o->graph); o->graph = nullptr; }
+    o->drop_graphs();
 }
 
 void ensure_graph(vsdmo_opt_s* o) {
-    if (o->exec || !o->p.use_graph) return;
+    const int slot = o->proposals_once;
+    if (o->exec[slot] || !o->p.use_graph) return;
     cudaStream_t s = o->mesh->m.stream;
     VSDMO_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
@@ -147,8 +153,8 @@ void ensure_graph(vsdmo_opt_s* o) {
         if (g) cudaGraphDestroy(g);
         throw;
     }
-    VSDMO_CUDA(cudaStreamEndCapture(s, &o->graph));
-    VSDMO_CUDA(cudaGraphInstantiate(&o->exec, o->graph, 0));
+    VSDMO_CUDA(cudaStreamEndCapture(s, &o->graph[slot]));
+    VSDMO_CUDA(cudaGraphInstantiate(&o->exec[slot], o->graph[slot], 0));
 }
 
 std::vector<IterStats> read_stats(vsdmo_opt_s* o, int from, int count) {
@@ -504,9 +510,10 @@ VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t o, int n_iter) {
     vsdmo_status st = guarded([&] {
         cudaStream_t s = o->mesh->m.stream;
         ensure_capacity(o, o->iters_done + n_iter);
-        ensure_graph(o);
         for (int i = 0; i < n_iter; ++i) {
-            if (o->exec) VSDMO_CUDA(cudaGraphLaunch(o->exec, s));
+            o->proposals_once = (o->model && o->once_after >= 0 && o->iters_done + i >= o->once_after) ? 1 : 0;
+            ensure_graph(o);
+            if (o->exec[o->proposals_once]) VSDMO_CUDA(cudaGraphLaunch(o->exec[o->proposals_once], s));
             else run_iteration_body(o, s);
         }
         auto h = read_stats(o, o->iters_done + 1, n_iter);

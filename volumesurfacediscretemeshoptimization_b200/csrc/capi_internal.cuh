@@ -33,8 +33,16 @@ struct vsdmo_opt_s {
     DBuf<double> psum;
     DBuf<int> pfail;
     DBuf<unsigned> done;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    // captured iterations: [0] the default body, [1] the body with one network launch for all
+    // colour classes (learned mode, proposals_once)
+    cudaGraph_t graph[2] = { nullptr, nullptr };
+    cudaGraphExec_t exec[2] = { nullptr, nullptr };
+    void drop_graphs() {
+        for (int i = 0; i < 2; ++i) {
+            if (exec[i]) { cudaGraphExecDestroy(exec[i]); exec[i] = nullptr; }
+            if (graph[i]) { cudaGraphDestroy(graph[i]); graph[i] = nullptr; }
+        }
+    }
     float last_min = 0.f;
     // learned proposal (tet): model, feature rows of one colour class, proposals, counters
     struct vsdmo_model_s* model = nullptr;
@@ -45,13 +53,13 @@ struct vsdmo_opt_s {
     DBuf<uint8_t> dirty;                  // active-set flags [nV] (params.active_set)
     DBuf<int> nb, nbn;                    // ring vertices of the inner range [32 per vertex], counts
     DBuf<int> fb_list, fb_count;          // fallback queue of one colour class
+    int proposals_once = 0;               // body being run or captured: 1 = one network launch for all colours
+    int once_after = -1;                  // iterations from this one on (since the restart) use it; -1 never
+    DBuf<float> Yall;                     // its proposals [inner vertices x OUTP]
     int nb_base = 0;
     void ensure_neighbours();
     bool collect = false;
-    ~vsdmo_opt_s() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-    }
+    ~vsdmo_opt_s() { drop_graphs(); }
 };
 
 inline thread_local std::string g_last_error;

@@ -196,8 +196,20 @@ VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t o, vsdmo_model_t model, i
         }
         o->counters.zero();
         // the captured iteration changes
-        if (o->exec) { cudaGraphExecDestroy(o->exec); o->exec = nullptr; }
-        if (o->graph) { cudaGraphDestroy(o->graph); o->graph = nullptr; }
+        o->drop_graphs();
+        m.sync();
+    });
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_set_proposal_schedule(vsdmo_opt_t o, int once_after) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    if (o->mode != MODE_TET) return fail(VSDMO_E_UNSUPPORTED, "the learned proposal is implemented for tet meshes");
+    if (once_after < -1) return fail(VSDMO_E_ARG, "once_after must be -1 or an iteration index >= 0");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        o->once_after = once_after;
+        if (once_after >= 0 && !o->Yall.p) o->Yall.alloc((size_t)std::max(m.nV - m.nSurf, 1) * mlp::OUTP, m.stream);
+        if (once_after >= 0) o->ensure_neighbours();
         m.sync();
     });
 }

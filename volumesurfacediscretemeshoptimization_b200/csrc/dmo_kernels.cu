@@ -132,36 +132,6 @@ __device__ float tet_key1(const float4* co, int k, float x, float y, float z) {
     return dm < 0.f ? dm : N / D;
 }
 
-// tet_key1 with the k tets spread over the lanes and combined in tet order by shuffles: the
-// same operations in the same order, so the same bits, for about a third of the instructions
-__device__ float tet_key_lanes(const float4* co, int k, float x, float y, float z, int lane) {
-    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
-    float N = 0.f, D = 1.f, dm = 0.f;
-    for (int base = 0; base < k; base += 32) {
-        const int t = base + lane;
-        float num = 0.f, den = 1.f, det = 0.f;
-        if (t < k) {
-            const float4 c0 = co[2 * t], c1 = co[2 * t + 1];
-            const float detA = fmaf(c0.x, x, c0.w);
-            const float LA = c1.w + fmaf(c1.x, x, tx);
-            const float detB = fmaf(c0.y, y, detA);
-            const float LB = LA + fmaf(c1.y, y, ty);
-            det = fmaf(c0.z, z, detB);
-            const float L = LB + fmaf(c1.z, z, tz);
-            num = det * det;
-            den = (L * L) * L;
-        }
-        const int cnt = min(32, k - base);
-        for (int j = 0; j < cnt; ++j) {
-            const float nj = __shfl_sync(FULL, num, j), dj = __shfl_sync(FULL, den, j), mj = __shfl_sync(FULL, det, j);
-            if (base + j == 0) { N = nj; D = dj; dm = mj; continue; }
-            if (nj * D < N * dj) { N = nj; D = dj; }
-            dm = fminf(dm, mj);
-        }
-    }
-    return dm < 0.f ? dm : N / D;
-}
-
 // Ring minimum of the lane's candidates (fixed x, NJ y values, all NQ z values) over the k
 // tets of the ring; returns the lane's best (key, linear index), strict > in index order.
 template <int NJ>
@@ -300,6 +270,19 @@ __device__ __forceinline__ unsigned tet_filter(const float4* __restrict__ co, co
             if (!(key < thr)) alive |= 1u << (jj * 8 + q);
         }
     return alive;
+}
+
+// Ring key with the tets spread over the lanes and a warp minimum of the per-tet keys (det if
+// negative, else det^2 / L^3): the minimum needs no fixed order, so this costs one tet per lane
+// and five shuffles. It can differ from tet_key1 in the last bit when two tets' fractions are
+// within rounding of each other, so only the learned search, whose moves are judged by keys of
+// this same function, uses it.
+__device__ __forceinline__ float tet_key_min(const float4* __restrict__ co, int k, float x, float y, float z, int lane) {
+    float m = FLT_MAX;
+    for (int t = lane; t < k; t += 32) m = fminf(m, tet_piece_key(co, t, x, y, z));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(FULL, m, o));
+    return m;
 }
 
 // Setup of one tet vertex shared by the plain and the learned search: per-axis extent of the
@@ -604,7 +587,7 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
     float sx, sy, sz;
     int ex;
     if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
-    const float q0 = tet_key_lanes(co, k, 0.f, 0.f, 0.f, lane);
+    const float q0 = tet_key_min(co, k, 0.f, 0.f, 0.f, lane);
     // proposal in scaled local coordinates (the features were divided by mm = max(sx, sy, sz) 2^ex)
     const float mms = fmaxf(sx, fmaxf(sy, sz));
     const float* y = Y + (size_t)(v - v0) * ldy;
@@ -614,7 +597,7 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
     float best = -FLT_MAX, cx = 0.f, cy = 0.f, cz = 0.f;
     if (have) {
         px = fminf(fmaxf(px, -bx), bx); py = fminf(fmaxf(py, -by), by); pz = fminf(fmaxf(pz, -bz), bz);
-        best = tet_key_lanes(co, k, px, py, pz, lane);
+        best = tet_key_min(co, k, px, py, pz, lane);
         cx = px; cy = py; cz = pz;
         float rx = grid_scale * rscale * sx, ry = grid_scale * rscale * sy, rz = grid_scale * rscale * sz;
         const int nc = rn * rn * rn;
