@@ -44,7 +44,8 @@ typedef enum vsdmo_status {
     VSDMO_E_TIMEOUT = 6,      /* a bounded device-side wait gave up                    */
     VSDMO_E_NAN = 7,          /* non-finite coordinates                                */
     VSDMO_E_NOMEM = 8,        /* device allocation failed                              */
-    VSDMO_E_UNSUPPORTED = 9   /* combination of element type / options not supported   */
+    VSDMO_E_UNSUPPORTED = 9,  /* combination of element type / options not supported   */
+    VSDMO_E_IO = 10           /* a mesh file could not be opened, parsed or written     */
 } vsdmo_status;
 
 typedef enum vsdmo_elem_type {
@@ -92,7 +93,7 @@ typedef enum vsdmo_array_id {
 typedef enum vsdmo_info_id {
     VSDMO_I_NV = 0, VSDMO_I_NE, VSDMO_I_NSURF, VSDMO_I_NFEATURE, VSDMO_I_NTRIS, VSDMO_I_NHE,
     VSDMO_I_NCOL_FREE, VSDMO_I_NCOL_FEATURE, VSDMO_I_NCOL_INNER, VSDMO_I_MAX_HE,
-    VSDMO_I_MAX_TETS, VSDMO_I_IS_FLAT, VSDMO_I_COUNT
+    VSDMO_I_MAX_TETS, VSDMO_I_IS_FLAT, VSDMO_I_ELEM_TYPE, VSDMO_I_COUNT
 } vsdmo_info_id;
 
 typedef struct vsdmo_mesh_s* vsdmo_mesh_t;
@@ -161,6 +162,39 @@ VSDMO_API vsdmo_status vsdmo_mesh_get_positions(vsdmo_mesh_t mesh, float* xyz, i
  * without waiting; with a host source it returns after the copy. */
 VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* xyz, int original_order,
                                                 int mem_space);
+
+/* ---- mesh files -------------------------------------------------------------------------- */
+/* Formats of the reference's parsers and writers (io/ParserOFF.cu, io/ParserTetGen.cu,
+ * io/ParserHex.cu, io/FileWriter.cu): OFF (triangles or quads, decided by the first face),
+ * TetGen (<base>.node + <base>.ele, 0- or 1-based by the first node's number; attributes and
+ * boundary markers are read and not used), Medit .mesh (Vertices + Triangles / Quadrilaterals
+ * / Tetrahedra / Hexahedra, 1-based; hexahedra swap their two faces on reading and writing
+ * like the reference, so file order 0..7 = the library's 4 5 6 7 0 1 2 3). AUTO picks the
+ * format from the extension (.off, .mesh, .node / .ele, or a base name whose .node exists). */
+typedef enum vsdmo_file_format {
+    VSDMO_FMT_AUTO = 0, VSDMO_FMT_OFF = 1, VSDMO_FMT_TETGEN = 2, VSDMO_FMT_MEDIT = 3
+} vsdmo_file_format;
+/* Parses a file on the host (no device work). Call once with xyz = elems = NULL for the
+ * sizes, then with host buffers of 3 n_vertices floats and k n_elements ints. */
+VSDMO_API vsdmo_status vsdmo_file_read(const char* path, int format, int* elem_type, int* n_vertices, int* n_elements,
+                                       float* xyz, int32_t* elems);
+/* Writes host arrays (floats with 9 significant digits: a written mesh reads back bit for bit;
+ * the reference prints 6). TetGen writes 0-based <base>.node and <base>.ele. */
+VSDMO_API vsdmo_status vsdmo_file_write(const char* path, int format, int elem_type, const float* xyz, int n_vertices,
+                                        const int32_t* elems, int n_elements);
+/* DMOMeshTriFactory / DMOMeshQuadFactory / DMOMeshTetFactory / DMOMeshHexFactory::create(
+ * filename) (mesh/MeshFactory.cu:3-13,45-55,60-70,101-111): read, then vsdmo_mesh_create.
+ * VSDMO_E_IO (message in vsdmo_last_error) where the reference returns nullptr. */
+VSDMO_API vsdmo_status vsdmo_mesh_create_from_file(const char* path, int format, uint32_t color_seed, void* cuda_stream,
+                                                   vsdmo_mesh_t* out);
+/* writeOFF / writeTetgen / writeHex (io/FileWriter.cu:12-147) with the current positions, in
+ * the caller's vertex numbering and element order (the reference writes its internal order). */
+VSDMO_API vsdmo_status vsdmo_mesh_write_file(vsdmo_mesh_t mesh, const char* path, int format);
+/* DMOMeshTriFactory::create(DMOMeshTet&) / DMOMeshQuadFactory::create(DMOMeshHex&)
+ * (mesh/MeshFactory.cu:33-41,91-99): a new tri / quad mesh of a volume mesh's boundary faces
+ * and surface vertices (the volume's first nSurf vertices in its internal numbering). */
+VSDMO_API vsdmo_status vsdmo_mesh_create_surface(vsdmo_mesh_t volume, uint32_t color_seed, void* cuda_stream,
+                                                 vsdmo_mesh_t* out);
 
 /* ---- optimiser ------------------------------------------------------------------------- */
 /* Replaces DMOTetClass / DMOTriFlatClass / DMOTriClass / DMOQuadClass construction + init()

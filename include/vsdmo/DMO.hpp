@@ -1,7 +1,8 @@
 // DMO.hpp -- C++ host API with the reference's class names, over the C ABI of vsdmo.h.
 //
 // Mirrors the interface a user of DanielZint/VolumeSurfaceDiscreteMeshOptimization calls:
-//   DMOMeshTri/Quad/TetFactory::create              mesh/MeshFactory.h:17-40
+//   DMOMeshTri/Quad/Tet/HexFactory::create          mesh/MeshFactory.h:17-40 (arrays, files, boundaries)
+//   writeOFF / writeTetgen / writeHex               io/FileWriter.h
 //   DMOMeshTri / DMOMeshQuad / DMOMeshTet           mesh/DMOMeshTri.h:81-94, mesh/DMOMeshQuad.h,
 //                                                   mesh/DMOMeshTet.h:145-198
 //   DMO::QualityCriterium                           dmo/DMOQualityUtil.h:10-18
@@ -49,9 +50,24 @@ public:
         maxNumHalfedges = vsdmo_mesh_info(h_, VSDMO_I_MAX_HE);
         maxNumTetrahedra = vsdmo_mesh_info(h_, VSDMO_I_MAX_TETS);
     }
+    // adopts a handle made by vsdmo_mesh_create_from_file / vsdmo_mesh_create_surface
+    explicit DMOMesh(vsdmo_mesh_t adopted) : h_(adopted) {
+        nVertices_ = vsdmo_mesh_info(h_, VSDMO_I_NV);
+        nVerticesSurf = vsdmo_mesh_info(h_, VSDMO_I_NSURF);
+        nVerticesFeature = vsdmo_mesh_info(h_, VSDMO_I_NFEATURE);
+        nColorsFree = vsdmo_mesh_info(h_, VSDMO_I_NCOL_FREE);
+        nColorsFeature = vsdmo_mesh_info(h_, VSDMO_I_NCOL_FEATURE);
+        nColorsInner = vsdmo_mesh_info(h_, VSDMO_I_NCOL_INNER);
+        maxNumHalfedges = vsdmo_mesh_info(h_, VSDMO_I_MAX_HE);
+        maxNumTetrahedra = vsdmo_mesh_info(h_, VSDMO_I_MAX_TETS);
+    }
     DMOMesh(const DMOMesh&) = delete;
     DMOMesh& operator=(const DMOMesh&) = delete;
     virtual ~DMOMesh() { vsdmo_mesh_destroy(h_); }
+    // writes the current positions in the caller's numbering (io/FileWriter.cu)
+    void write(const std::string& filename, int format = VSDMO_FMT_AUTO) const {
+        check(vsdmo_mesh_write_file(h_, filename.c_str(), format));
+    }
 
     vsdmo_mesh_t handle() const { return h_; }
     int nVertices() const { return nVertices_; }
@@ -77,29 +93,59 @@ private:
 
 class DMOMeshTri : public DMOMesh {
 public:
+    explicit DMOMeshTri(vsdmo_mesh_t adopted) : DMOMesh(adopted) {}
     DMOMeshTri(int nVS, int nT, const float* points, const int32_t* tris, int memSpace = VSDMO_HOST)
         : DMOMesh(VSDMO_TRI, points, nVS, tris, nT, memSpace) {}
 };
 
 class DMOMeshQuad : public DMOMesh {
 public:
+    explicit DMOMeshQuad(vsdmo_mesh_t adopted) : DMOMesh(adopted) {}
     DMOMeshQuad(int nVS, int nQ, const float* points, const int32_t* quads, int memSpace = VSDMO_HOST)
         : DMOMesh(VSDMO_QUAD, points, nVS, quads, nQ, memSpace) {}
 };
 
 class DMOMeshTet : public DMOMesh {
 public:
+    explicit DMOMeshTet(vsdmo_mesh_t adopted) : DMOMesh(adopted) {}
     DMOMeshTet(int nV, int nT, const float* points, const int32_t* tets, int memSpace = VSDMO_HOST)
         : DMOMesh(VSDMO_TET, points, nV, tets, nT, memSpace) {}
 };
 
 class DMOMeshHex : public DMOMesh {
 public:
+    explicit DMOMeshHex(vsdmo_mesh_t adopted) : DMOMesh(adopted) {}
     DMOMeshHex(int nV, int nH, const float* points, const int32_t* hexes, int memSpace = VSDMO_HOST)
         : DMOMesh(VSDMO_HEX, points, nV, hexes, nH, memSpace) {}
 };
 
+namespace detail {
+// nullptr when the file cannot be opened or parsed (the reference's factories return nullptr)
+template <class M>
+std::shared_ptr<M> from_file(const std::string& filename, int expect) {
+    vsdmo_mesh_t h = nullptr;
+    const vsdmo_status st = vsdmo_mesh_create_from_file(filename.c_str(), VSDMO_FMT_AUTO, 1, nullptr, &h);
+    if (st == VSDMO_E_IO) return nullptr;
+    check(st);
+    if (vsdmo_mesh_info(h, VSDMO_I_ELEM_TYPE) != expect) {
+        vsdmo_mesh_destroy(h);
+        throw Error(VSDMO_E_ARG, filename + " holds another element type");
+    }
+    return std::make_shared<M>(h);
+}
+template <class M>
+std::shared_ptr<M> surface_of(const DMOMesh& volume) {
+    vsdmo_mesh_t h = nullptr;
+    check(vsdmo_mesh_create_surface(volume.handle(), 1, nullptr, &h));
+    return std::make_shared<M>(h);
+}
+}  // namespace detail
+
 struct DMOMeshTriFactory {
+    static std::shared_ptr<DMOMeshTri> create(const std::string& filename) {
+        return detail::from_file<DMOMeshTri>(filename, VSDMO_TRI);
+    }
+    static std::shared_ptr<DMOMeshTri> create(const DMOMeshTet& tetmesh) { return detail::surface_of<DMOMeshTri>(tetmesh); }
     static std::shared_ptr<DMOMeshTri> create(int nVS, int nT, const float* points, const int32_t* tris,
                                               int memSpace = VSDMO_HOST) {
         return std::make_shared<DMOMeshTri>(nVS, nT, points, tris, memSpace);
@@ -107,6 +153,10 @@ struct DMOMeshTriFactory {
 };
 
 struct DMOMeshQuadFactory {
+    static std::shared_ptr<DMOMeshQuad> create(const std::string& filename) {
+        return detail::from_file<DMOMeshQuad>(filename, VSDMO_QUAD);
+    }
+    static std::shared_ptr<DMOMeshQuad> create(const DMOMeshHex& hexmesh) { return detail::surface_of<DMOMeshQuad>(hexmesh); }
     static std::shared_ptr<DMOMeshQuad> create(int nVS, int nQ, const float* points, const int32_t* quads,
                                                int memSpace = VSDMO_HOST) {
         return std::make_shared<DMOMeshQuad>(nVS, nQ, points, quads, memSpace);
@@ -114,6 +164,9 @@ struct DMOMeshQuadFactory {
 };
 
 struct DMOMeshHexFactory {
+    static std::shared_ptr<DMOMeshHex> create(const std::string& filename) {
+        return detail::from_file<DMOMeshHex>(filename, VSDMO_HEX);
+    }
     static std::shared_ptr<DMOMeshHex> create(int nV, int nH, const float* points, const int32_t* hexes,
                                               int memSpace = VSDMO_HOST) {
         return std::make_shared<DMOMeshHex>(nV, nH, points, hexes, memSpace);
@@ -121,11 +174,20 @@ struct DMOMeshHexFactory {
 };
 
 struct DMOMeshTetFactory {
+    static std::shared_ptr<DMOMeshTet> create(const std::string& filename) {
+        return detail::from_file<DMOMeshTet>(filename, VSDMO_TET);
+    }
     static std::shared_ptr<DMOMeshTet> create(int nV, int nT, const float* points, const int32_t* tets,
                                               int memSpace = VSDMO_HOST) {
         return std::make_shared<DMOMeshTet>(nV, nT, points, tets, memSpace);
     }
 };
+
+// io/FileWriter.h names
+inline void writeOFF(const std::string& filename, const DMOMeshTri& mesh) { mesh.write(filename + ".off", VSDMO_FMT_OFF); }
+inline void writeOFF(const std::string& filename, const DMOMeshQuad& mesh) { mesh.write(filename + ".off", VSDMO_FMT_OFF); }
+inline void writeTetgen(const std::string& filename, const DMOMeshTet& mesh) { mesh.write(filename, VSDMO_FMT_TETGEN); }
+inline void writeHex(const std::string& filename, const DMOMeshHex& mesh) { mesh.write(filename + ".mesh", VSDMO_FMT_MEDIT); }
 
 class DMOBaseClass {
 public:

@@ -23,6 +23,7 @@ counterpart in the reference.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import enum
 import sys
 
@@ -35,7 +36,7 @@ from ._capi import VSDMOError, Params, check
 __all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshQuad", "DMOMeshTet", "DMOMeshHex", "DMOMeshTriFactory",
            "DMOMeshQuadFactory", "DMOMeshTetFactory", "DMOMeshHexFactory", "DMOTetClass", "DMOHexClass",
            "DMOTriFlatClass", "DMOTriClass", "DMOQuadClass", "DMOQuadFlatClass", "BatchDMO", "ProposalModel",
-           "VSDMOError", "Params", "default_params", "version"]
+           "VSDMOError", "Params", "default_params", "version", "read_mesh_file", "write_mesh_file"]
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -48,6 +49,7 @@ ARRAY_NAMES = {A_XYZ: "xyz", A_NEW_OF_OLD: "new_of_old", A_ELEMS: "elems", A_SUR
                A_VERTEX_NORMALS: "vertex_normals"}
 _F32 = {A_XYZ, A_FACE_NORMALS, A_VERTEX_NORMALS}
 _U8 = {A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D}
+I_ELEM_TYPE = 12
 INFO_NAMES = ["nV", "nE", "nSurf", "nFeature", "nTris", "nHE", "nColorsFree", "nColorsFeature",
               "nColorsInner", "maxNumHalfedges", "maxNumTetrahedra", "isFlat"]
 
@@ -81,10 +83,12 @@ class _Mesh:
     elem_type = -1
     k = 0
 
-    def __init__(self, points, elems, color_seed: int = 1, stream=None, device_ptrs=None):
+    def __init__(self, points, elems, color_seed: int = 1, stream=None, device_ptrs=None, handle=None):
         L = _capi.lib()
         h = C.c_void_p()
-        if device_ptrs is not None:
+        if handle is not None:
+            h = handle
+        elif device_ptrs is not None:
             xyz_ptr, el_ptr, nV, nE = device_ptrs
             check(L.vsdmo_mesh_create(self.elem_type, C.c_void_p(xyz_ptr), nV, C.c_void_p(el_ptr), nE,
                                       _capi.DEVICE, color_seed, C.c_void_p(stream or 0), C.byref(h)))
@@ -140,6 +144,11 @@ class _Mesh:
             raise ValueError("wrong number of vertices")
         check(_capi.lib().vsdmo_mesh_set_positions(self.h, _ptr(xyz), int(original_order), _capi.HOST))
 
+    def write(self, path: str, fmt: int = _capi.FMT_AUTO):
+        """writeOFF / writeTetgen / writeHex (``io/FileWriter.cu``): current positions in the
+        caller's numbering."""
+        check(_capi.lib().vsdmo_mesh_write_file(self.h, os.fsencode(path), int(fmt)))
+
     def positions_to_device(self, dev_ptr: int, original_order: bool = True):
         check(_capi.lib().vsdmo_mesh_get_positions(self.h, C.c_void_p(dev_ptr), int(original_order), _capi.DEVICE))
 
@@ -169,35 +178,100 @@ class DMOMeshHex(_Mesh):
     k = 8
 
 
+_MESH_CLASS = {_capi.TRI: DMOMeshTri, _capi.QUAD: DMOMeshQuad, _capi.TET: DMOMeshTet, _capi.HEX: DMOMeshHex}
+
+
+def _from_file(path, expect, color_seed, stream):
+    """``DMOMesh*Factory::create(filename)`` (``mesh/MeshFactory.cu:3-13,45-55,60-70,101-111``);
+    returns None where the reference returns nullptr (the file cannot be opened or parsed)."""
+    h = C.c_void_p()
+    st = _capi.lib().vsdmo_mesh_create_from_file(os.fsencode(path), _capi.FMT_AUTO, int(color_seed),
+                                                  C.c_void_p(stream or 0), C.byref(h))
+    if st == _capi.E_IO:
+        return None
+    check(st)
+    got = _capi.lib().vsdmo_mesh_info(h, I_ELEM_TYPE)
+    if got != expect:
+        _capi.lib().vsdmo_mesh_destroy(h)
+        raise VSDMOError(_capi.E_ARG, f"{path} holds element type {got}, this factory builds type {expect}")
+    cls = _MESH_CLASS[expect]
+    m = cls.__new__(cls)
+    _Mesh.__init__(m, None, None, handle=h)
+    return m
+
+
+def read_mesh_file(path, fmt: int = _capi.FMT_AUTO):
+    """Host parse of an OFF / TetGen / Medit file: (elem_type, points [n x 3], elems [m x k])."""
+    t, nv, ne = C.c_int(), C.c_int(), C.c_int()
+    b = os.fsencode(path)
+    check(_capi.lib().vsdmo_file_read(b, int(fmt), C.byref(t), C.byref(nv), C.byref(ne), None, None))
+    k = {_capi.TRI: 3, _capi.QUAD: 4, _capi.TET: 4, _capi.HEX: 8}[t.value]
+    xyz = np.zeros((nv.value, 3), np.float32)
+    el = np.zeros((ne.value, k), np.int32)
+    check(_capi.lib().vsdmo_file_read(b, int(fmt), C.byref(t), C.byref(nv), C.byref(ne), _ptr(xyz), _ptr(el)))
+    return t.value, xyz, el
+
+
+def write_mesh_file(path, elem_type: int, points, elems, fmt: int = _capi.FMT_AUTO):
+    xyz = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    el = np.ascontiguousarray(elems, np.int32)
+    check(_capi.lib().vsdmo_file_write(os.fsencode(path), int(fmt), int(elem_type), _ptr(xyz), len(xyz), _ptr(el),
+                                       len(el)))
+
+
+def _surface_of(volume, color_seed, stream, cls):
+    h = C.c_void_p()
+    check(_capi.lib().vsdmo_mesh_create_surface(volume.h, int(color_seed), C.c_void_p(stream or 0), C.byref(h)))
+    m = cls.__new__(cls)
+    _Mesh.__init__(m, None, None, handle=h)
+    return m
+
+
 class DMOMeshTriFactory:
-    """``DMOMeshTriFactory::create`` (``mesh/MeshFactory.cu:15-31``)."""
+    """``DMOMeshTriFactory::create`` (``mesh/MeshFactory.cu:3-41``): from arrays, from an OFF
+    file name, or the boundary of a ``DMOMeshTet``."""
 
     @staticmethod
-    def create(points, tris, color_seed: int = 1) -> DMOMeshTri:
-        return DMOMeshTri(points, tris, color_seed)
+    def create(points, tris=None, color_seed: int = 1, stream=None):
+        if isinstance(points, (str, os.PathLike)):
+            return _from_file(points, _capi.TRI, color_seed, stream)
+        if isinstance(points, DMOMeshTet):
+            return _surface_of(points, color_seed, stream, DMOMeshTri)
+        return DMOMeshTri(points, tris, color_seed, stream)
 
 
 class DMOMeshQuadFactory:
-    """``DMOMeshQuadFactory::create`` (``mesh/MeshFactory.cu``) from arrays."""
+    """``DMOMeshQuadFactory::create`` (``mesh/MeshFactory.cu:60-99``): from arrays, an OFF
+    file name, or the boundary of a ``DMOMeshHex``."""
 
     @staticmethod
-    def create(points, quads, color_seed: int = 1) -> DMOMeshQuad:
-        return DMOMeshQuad(points, quads, color_seed)
+    def create(points, quads=None, color_seed: int = 1, stream=None):
+        if isinstance(points, (str, os.PathLike)):
+            return _from_file(points, _capi.QUAD, color_seed, stream)
+        if isinstance(points, DMOMeshHex):
+            return _surface_of(points, color_seed, stream, DMOMeshQuad)
+        return DMOMeshQuad(points, quads, color_seed, stream)
 
 
 class DMOMeshHexFactory:
-    """``DMOMeshHexFactory::create`` (``mesh/MeshFactory.cu``) from arrays."""
+    """``DMOMeshHexFactory::create`` (``mesh/MeshFactory.cu:101-111``): from arrays or a Medit
+    file name."""
 
     @staticmethod
-    def create(points, hexes, color_seed: int = 1) -> DMOMeshHex:
-        return DMOMeshHex(points, hexes, color_seed)
+    def create(points, hexes=None, color_seed: int = 1, stream=None):
+        if isinstance(points, (str, os.PathLike)):
+            return _from_file(points, _capi.HEX, color_seed, stream)
+        return DMOMeshHex(points, hexes, color_seed, stream)
 
 
 class DMOMeshTetFactory:
-    """``DMOMeshTetFactory::create`` (``mesh/MeshFactory.cu:45-55``) from arrays."""
+    """``DMOMeshTetFactory::create`` (``mesh/MeshFactory.cu:45-55``): from arrays or a TetGen
+    base name (``base.node`` + ``base.ele``)."""
 
     @staticmethod
-    def create(points, tets, color_seed: int = 1) -> DMOMeshTet:
+    def create(points, tets=None, color_seed: int = 1, stream=None):
+        if isinstance(points, (str, os.PathLike)):
+            return _from_file(points, _capi.TET, color_seed, stream)
         return DMOMeshTet(points, tets, color_seed)
 
 

@@ -12,7 +12,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("VSDMO_LIB", os.path.join(HERE, "lib", "libvsdmo.so"))
 
-OK, E_ARG, E_CUDA, E_NONMANIFOLD, E_VALENCE, E_MONOTONE, E_TIMEOUT, E_NAN, E_NOMEM, E_UNSUPPORTED = range(10)
+OK, E_ARG, E_CUDA, E_NONMANIFOLD, E_VALENCE, E_MONOTONE, E_TIMEOUT, E_NAN, E_NOMEM, E_UNSUPPORTED, E_IO = range(11)
+FMT_AUTO, FMT_OFF, FMT_TETGEN, FMT_MEDIT = range(4)
 TRI, QUAD, TET, HEX = 0, 1, 2, 3
 HOST, DEVICE = 0, 1
 
@@ -34,6 +35,8 @@ EXPORTED = [
     "vsdmo_batch_sync", "vsdmo_batch_restart", "vsdmo_batch_stats", "vsdmo_batch_get_positions",
     "vsdmo_batch_set_positions", "vsdmo_batch_get_config", "vsdmo_batch_set_config", "vsdmo_batch_autotune",
     "vsdmo_batch_info", "vsdmo_batch_mesh_info",
+    "vsdmo_file_read", "vsdmo_file_write", "vsdmo_mesh_create_from_file", "vsdmo_mesh_write_file",
+    "vsdmo_mesh_create_surface",
 ]
 
 
@@ -168,6 +171,16 @@ def lib():
     L.vsdmo_batch_autotune.argtypes = [P, I, C.c_char_p, I]
     L.vsdmo_batch_info.restype = C.c_long
     L.vsdmo_batch_info.argtypes = [P, I]
+    L.vsdmo_file_read.restype = S
+    L.vsdmo_file_read.argtypes = [C.c_char_p, I, C.POINTER(I), C.POINTER(I), C.POINTER(I), P, P]
+    L.vsdmo_file_write.restype = S
+    L.vsdmo_file_write.argtypes = [C.c_char_p, I, I, P, I, P, I]
+    L.vsdmo_mesh_create_from_file.restype = S
+    L.vsdmo_mesh_create_from_file.argtypes = [C.c_char_p, I, U, P, C.POINTER(P)]
+    L.vsdmo_mesh_write_file.restype = S
+    L.vsdmo_mesh_write_file.argtypes = [P, C.c_char_p, I]
+    L.vsdmo_mesh_create_surface.restype = S
+    L.vsdmo_mesh_create_surface.argtypes = [P, U, P, C.POINTER(P)]
     L.vsdmo_batch_mesh_info.restype = S
     L.vsdmo_batch_mesh_info.argtypes = [P, I, P]
     _lib = L

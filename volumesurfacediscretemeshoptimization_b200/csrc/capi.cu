@@ -186,6 +186,7 @@ VSDMO_API const char* vsdmo_status_string(vsdmo_status s) {
     case VSDMO_E_NAN: return "non-finite coordinates";
     case VSDMO_E_NOMEM: return "out of memory";
     case VSDMO_E_UNSUPPORTED: return "unsupported";
+    case VSDMO_E_IO: return "mesh file error";
     }
     return "unknown status";
 }
@@ -295,6 +296,7 @@ VSDMO_API int vsdmo_mesh_info(vsdmo_mesh_t mesh, int which) {
     case VSDMO_I_MAX_HE: return m.maxHE;
     case VSDMO_I_MAX_TETS: return m.maxTets;
     case VSDMO_I_IS_FLAT: return m.isFlat;
+    case VSDMO_I_ELEM_TYPE: return m.type;
     default: return -1;
     }
 }
