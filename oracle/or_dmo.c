@@ -142,16 +142,19 @@ void or_element_qualities_f32(const or_mesh* m, const float* xyz, float* q) {
 /* f64: literal restatement of the reference kernels                                        */
 /* ======================================================================================= */
 
-static double ring_q_tet_f64(int k, const double* ring, const double* p) {
+typedef double (*tet_metric64)(const double*, const double*, const double*, const double*);
+typedef double (*tri_metric64)(const double*, const double*, const double*);
+
+static double ring_q_tet_f64(int k, const double* ring, const double* p, tet_metric64 metric) {
     double q = DBL_MAX;
     for (int t = 0; t < k; ++t) {
-        double v = or_q_tet_mean_ratio_f64(p, ring + 9 * t, ring + 9 * t + 3, ring + 9 * t + 6);
+        double v = metric(p, ring + 9 * t, ring + 9 * t + 3, ring + 9 * t + 6);
         q = fmin(q, v);
     }
     return q;
 }
 
-static void tet_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin) {
+static void tet_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin, tet_metric64 metric) {
     const int* rp = or__hf_rowptr(m);
     const int* hf = or__hf(m);
     int b = rp[v], k = rp[v + 1] - b;
@@ -176,7 +179,7 @@ static void tet_vertex_f64(const or_mesh* m, double* X, int v, double gs, double
     for (int d = 0; d < DEPTH; ++d) {
         double gmax[3], gmin[3];
         for (int a = 0; a < 3; ++a) { gmax[a] = cur[a] + ds * md[a]; gmin[a] = cur[a] - ds * md[a]; }
-        double qLast = ring_q_tet_f64(k, ring, cur);
+        double qLast = ring_q_tet_f64(k, ring, cur, metric);
         double best = -DBL_MAX, second = -DBL_MAX;
         for (int t = 0; t < 128; ++t) {
             for (int idx = 4 * t; idx < 4 * t + 4; ++idx) {
@@ -185,7 +188,7 @@ static void tet_vertex_f64(const or_mesh* m, double* X, int v, double gs, double
                 p[0] = aff * (i * gmin[0] + (NQ - 1 - i) * gmax[0]);
                 p[1] = aff * (j * gmin[1] + (NQ - 1 - j) * gmax[1]);
                 p[2] = aff * (kk * gmin[2] + (NQ - 1 - kk) * gmax[2]);
-                double q = ring_q_tet_f64(k, ring, p);
+                double q = ring_q_tet_f64(k, ring, p, metric);
                 if (q > best) { second = best; best = q; } else if (q > second) second = q;
                 if (q > qMax[t]) { qMax[t] = q; pMax[t][0] = p[0]; pMax[t][1] = p[1]; pMax[t][2] = p[2]; }
             }
@@ -198,20 +201,20 @@ static void tet_vertex_f64(const or_mesh* m, double* X, int v, double gs, double
         if (qLast < qMax[w]) { cur[0] = pMax[w][0]; cur[1] = pMax[w][1]; cur[2] = pMax[w][2]; }
         ds = ds * (2.0 / (NQ - 1));
     }
-    double qOld = ring_q_tet_f64(k, ring, p0);
+    double qOld = ring_q_tet_f64(k, ring, p0, metric);
     mg = fmin(mg, fabs(qMax[w] - qOld));
     if (qOld < qMax[w]) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; X[3 * v + 2] = cur[2]; }
     if (margin) *margin = mg;
     free(ring);
 }
 
-static double ring_q_tri2d_f64(int n1, const double* ring, const double* p) {
+static double ring_q_tri2d_f64(int n1, const double* ring, const double* p, tri_metric64 metric) {
     double q = DBL_MAX;
-    for (int i = 0; i < n1 - 1; ++i) q = fmin(q, or_q_tri2d_mean_ratio_f64(p, ring + 3 * i, ring + 3 * (i + 1)));
+    for (int i = 0; i < n1 - 1; ++i) q = fmin(q, metric(p, ring + 3 * i, ring + 3 * (i + 1)));
     return q;
 }
 
-static void tri2d_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin) {
+static void tri2d_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin, tri_metric64 metric) {
     const int* rp = or__he_rowptr(m);
     const int* he = or__he(m);
     int b = rp[v], k = rp[v + 1] - b;
@@ -232,14 +235,14 @@ static void tri2d_vertex_f64(const or_mesh* m, double* X, int v, double gs, doub
     for (int d = 0; d < DEPTH; ++d) {
         double gmax[2], gmin[2];
         for (int a = 0; a < 2; ++a) { gmax[a] = cur[a] + ds * md[a]; gmin[a] = cur[a] - ds * md[a]; }
-        double qLast = ring_q_tri2d_f64(n1, ring, cur);
+        double qLast = ring_q_tri2d_f64(n1, ring, cur, metric);
         double val[32], pp[32][2];
         double best = -DBL_MAX, second = -DBL_MAX;
         for (int t = 0; t < 32; ++t) {
             int i1 = t / NQ, j1 = t % NQ, i2 = i1 + 4;
             double p1[3] = { aff * (i1 * gmin[0] + (NQ - 1 - i1) * gmax[0]), aff * (j1 * gmin[1] + (NQ - 1 - j1) * gmax[1]), cur[2] };
             double p2[3] = { aff * (i2 * gmin[0] + (NQ - 1 - i2) * gmax[0]), aff * (j1 * gmin[1] + (NQ - 1 - j1) * gmax[1]), cur[2] };
-            double q1 = ring_q_tri2d_f64(n1, ring, p1), q2 = ring_q_tri2d_f64(n1, ring, p2);
+            double q1 = ring_q_tri2d_f64(n1, ring, p1, metric), q2 = ring_q_tri2d_f64(n1, ring, p2, metric);
             val[t] = q1; if (q2 > q1) val[t] = q2;
             if (q1 > q2) { pp[t][0] = p1[0]; pp[t][1] = p1[1]; } else { pp[t][0] = p2[0]; pp[t][1] = p2[1]; }
             double qs[2] = { q1, q2 };
@@ -253,7 +256,7 @@ static void tri2d_vertex_f64(const or_mesh* m, double* X, int v, double gs, doub
         lastMax = val[w];
         ds = ds * (2.0 / (NQ - 1));
     }
-    double qOld = ring_q_tri2d_f64(n1, ring, p0);
+    double qOld = ring_q_tri2d_f64(n1, ring, p0, metric);
     mg = fmin(mg, fabs(lastMax - qOld));
     if (qOld < lastMax) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; }
     if (margin) *margin = mg;
@@ -265,7 +268,7 @@ void or_dmo_tet_f64(const or_mesh* m, double* xyz, int v0, int v1, double gs, do
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 64)
 #endif
-    for (int v = v0; v < v1; ++v) tet_vertex_f64(m, xyz, v, gs, margin ? margin + (v - v0) : NULL);
+    for (int v = v0; v < v1; ++v) tet_vertex_f64(m, xyz, v, gs, margin ? margin + (v - v0) : NULL, or_q_tet_mean_ratio_f64);
 }
 
 void or_dmo_tri2d_f64(const or_mesh* m, double* xyz, int v0, int v1, double gs, double* margin, int nthreads) {
@@ -273,7 +276,7 @@ void or_dmo_tri2d_f64(const or_mesh* m, double* xyz, int v0, int v1, double gs, 
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 64)
 #endif
-    for (int v = v0; v < v1; ++v) tri2d_vertex_f64(m, xyz, v, gs, margin ? margin + (v - v0) : NULL);
+    for (int v = v0; v < v1; ++v) tri2d_vertex_f64(m, xyz, v, gs, margin ? margin + (v - v0) : NULL, or_q_tri2d_mean_ratio_f64);
 }
 
 /* literal float restatement of k_optimizeHierarchicalInnerTet (the reference's own FP32
@@ -573,4 +576,93 @@ void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double gs, int n
         }
     }
     free(q);
+}
+
+
+/* ======================================================================================= */
+/* angle criteria (MIN_ANGLE / MAX_ANGLE), literal in double                                */
+/* minAngleMetricTri2D / maxAngleMetricTri2D (dmo/DMOQualityTri.h:10-29,124-144),            */
+/* minAngleMetricTet / maxAngleMetricTet (dmo/DMOQualityTet.h:10-37,62-91), calcAngle        */
+/* (dmo/DMOQualityUtil.h:30-50): angles by acos of dot / sqrt(|u|^2 |v|^2).                  */
+/* ======================================================================================= */
+
+static double calc_angle(const double* u, const double* v, int dim) {
+    double d = 0.0, uu = 0.0, vv = 0.0;
+    for (int a = 0; a < dim; ++a) { d += u[a] * v[a]; uu += u[a] * u[a]; vv += v[a] * v[a]; }
+    return acos(d / sqrt(uu * vv));
+}
+
+static double tri2d_angle64(const double* p0, const double* p1, const double* p2, int max_angle) {
+    const double e0[2] = { p1[0] - p0[0], p1[1] - p0[1] }, e1[2] = { p2[0] - p1[0], p2[1] - p1[1] };
+    const double area = e0[0] * e1[1] - e0[1] * e1[0];
+    if (area < 0.0) return area;
+    const double a0[2] = { p0[0] - p1[0], p0[1] - p1[1] }, a1[2] = { p2[0] - p1[0], p2[1] - p1[1] };
+    const double b0[2] = { p1[0] - p2[0], p1[1] - p2[1] }, b1[2] = { p0[0] - p2[0], p0[1] - p2[1] };
+    const double c0[2] = { p2[0] - p0[0], p2[1] - p0[1] }, c1[2] = { p1[0] - p0[0], p1[1] - p0[1] };
+    const double a = calc_angle(a0, a1, 2), b = calc_angle(b0, b1, 2), c = calc_angle(c0, c1, 2);
+    if (max_angle) return 1.0 - fmax(fmax(a, b), c) / M_PI;
+    return 3.0 * fmin(fmin(a, b), c) / M_PI;
+}
+double or_q_tri2d_min_angle_f64(const double* p0, const double* p1, const double* p2) { return tri2d_angle64(p0, p1, p2, 0); }
+double or_q_tri2d_max_angle_f64(const double* p0, const double* p1, const double* p2) { return tri2d_angle64(p0, p1, p2, 1); }
+
+static void cross64(const double* u, const double* v, double* o) {
+    o[0] = u[1] * v[2] - u[2] * v[1];
+    o[1] = u[2] * v[0] - u[0] * v[2];
+    o[2] = u[0] * v[1] - u[1] * v[0];
+}
+
+static double tet_angle64(const double* p0, const double* p1, const double* p2, const double* p3, int max_angle) {
+    double e[6][3], n[4][3];
+    for (int a = 0; a < 3; ++a) {
+        e[0][a] = p1[a] - p0[a]; e[1][a] = p2[a] - p0[a]; e[2][a] = p3[a] - p0[a];
+        e[3][a] = p2[a] - p1[a]; e[4][a] = p3[a] - p1[a]; e[5][a] = p3[a] - p2[a];
+    }
+    double x[3];
+    cross64(e[1], e[2], x);
+    const double vol = (e[0][0] * x[0] + e[0][1] * x[1] + e[0][2] * x[2]) / 6.0;
+    if (vol < 0.0) return vol;
+    cross64(e[0], e[2], n[0]); cross64(e[3], e[4], n[1]); cross64(e[1], e[0], n[2]); cross64(e[2], e[1], n[3]);
+    for (int i = 0; i < 4; ++i) {
+        const double l = sqrt(n[i][0] * n[i][0] + n[i][1] * n[i][1] + n[i][2] * n[i][2]);
+        for (int a = 0; a < 3; ++a) n[i][a] /= l;
+    }
+    const int P[6][2] = { { 0, 1 }, { 0, 2 }, { 0, 3 }, { 1, 2 }, { 1, 3 }, { 2, 3 } };
+    double mn = DBL_MAX, mx = -DBL_MAX;
+    for (int q = 0; q < 6; ++q) {
+        const double m[3] = { -n[P[q][0]][0], -n[P[q][0]][1], -n[P[q][0]][2] };
+        const double ang = calc_angle(m, n[P[q][1]], 3);
+        mn = fmin(mn, ang); mx = fmax(mx, ang);
+    }
+    if (max_angle) return 1.0 - mx / M_PI;
+    return 3.0 * mn / M_PI;
+}
+double or_q_tet_min_angle_f64(const double* p0, const double* p1, const double* p2, const double* p3) { return tet_angle64(p0, p1, p2, p3, 0); }
+double or_q_tet_max_angle_f64(const double* p0, const double* p1, const double* p2, const double* p3) { return tet_angle64(p0, p1, p2, p3, 1); }
+
+void or_dmo_angle_f64(const or_mesh* m, double* xyz, int v0, int v1, double gs, int max_angle, double* margin, int nthreads) {
+    const int tet = or__hf_rowptr(m) != NULL;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+    for (int v = v0; v < v1; ++v) {
+        double* mg = margin ? margin + (v - v0) : NULL;
+        if (tet) tet_vertex_f64(m, xyz, v, gs, mg, max_angle ? or_q_tet_max_angle_f64 : or_q_tet_min_angle_f64);
+        else tri2d_vertex_f64(m, xyz, v, gs, mg, max_angle ? or_q_tri2d_max_angle_f64 : or_q_tri2d_min_angle_f64);
+    }
+}
+
+void or_angle_qualities_f64(const or_mesh* m, const double* xyz, int max_angle, double* q) {
+    const int nE = or_mesh_info(m, OR_I_NE);
+    const int* el = or__elems(m);
+    for (int t = 0; t < nE; ++t) {
+        if (or__hf_rowptr(m)) {
+            const int* v = el + 4 * t;
+            q[t] = tet_angle64(xyz + 3 * v[0], xyz + 3 * v[1], xyz + 3 * v[2], xyz + 3 * v[3], max_angle);
+        } else {
+            const int* v = el + 3 * t;
+            q[t] = tri2d_angle64(xyz + 3 * v[0], xyz + 3 * v[1], xyz + 3 * v[2], max_angle);
+        }
+    }
 }

@@ -84,6 +84,14 @@ def lib():
         L.or_hex_qualities_f64.argtypes = [P, P, P]
         L.or_optimize_hex_f32.argtypes = [P, P, I, F, I, P, P]
         L.or_optimize_hex_f64.argtypes = [P, P, I, D, I, P, P]
+        L.or_dmo_angle_f64.argtypes = [P, P, I, I, D, I, P, I]
+        L.or_angle_qualities_f64.argtypes = [P, P, I, P]
+        for n in ("or_q_tet_min_angle_f64", "or_q_tet_max_angle_f64"):
+            getattr(L, n).restype = D
+            getattr(L, n).argtypes = [P, P, P, P]
+        for n in ("or_q_tri2d_min_angle_f64", "or_q_tri2d_max_angle_f64"):
+            getattr(L, n).restype = D
+            getattr(L, n).argtypes = [P, P, P]
         L.or_q_tet_mean_ratio_f64.restype = D
         L.or_q_tet_mean_ratio_f64.argtypes = [P, P, P, P]
         L.or_q_tet_mean_ratio_f32.restype = F
@@ -159,6 +167,19 @@ class OracleMesh:
         margin = np.zeros(max(v1 - v0, 1), dtype=np.float64)
         lib().or_dmo_quad2d_f64(self.h, _p(xyz), v0, v1, grid_scale, _p(margin), nthreads)
         return xyz, margin[: v1 - v0]
+
+    def dmo_angle_f64(self, xyz, v0, v1, max_angle=False, grid_scale=0.5, nthreads=0):
+        """One colour class with the MIN_ANGLE (or MAX_ANGLE) criterion, literal in double."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        margin = np.zeros(max(v1 - v0, 1), dtype=np.float64)
+        lib().or_dmo_angle_f64(self.h, _p(xyz), v0, v1, grid_scale, int(max_angle), _p(margin), nthreads)
+        return xyz, margin[: v1 - v0]
+
+    def angle_qualities_f64(self, xyz, max_angle=False):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        q = np.zeros(self.info["nE"], dtype=np.float64)
+        lib().or_angle_qualities_f64(self.h, _p(xyz), int(max_angle), _p(q))
+        return q
 
     def dmo_color_ref32(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
         """The reference kernel's own float arithmetic (tet interior only)."""

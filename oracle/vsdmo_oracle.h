@@ -101,6 +101,16 @@ void or_optimize_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale,
 void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
                      double* min_hist, double* mean_hist);
 
+/* ---- angle criteria (MIN_ANGLE / MAX_ANGLE), literal in double (or_dmo.c) ---------------- */
+double or_q_tri2d_min_angle_f64(const double* p0, const double* p1, const double* p2);
+double or_q_tri2d_max_angle_f64(const double* p0, const double* p1, const double* p2);
+double or_q_tet_min_angle_f64(const double* p0, const double* p1, const double* p2, const double* p3);
+double or_q_tet_max_angle_f64(const double* p0, const double* p1, const double* p2, const double* p3);
+/* one colour class (tet interior or flat triangles) with the reference search and the angle metric */
+void or_dmo_angle_f64(const or_mesh* m, double* xyz, int v0, int v1, double grid_scale, int max_angle, double* margin,
+                      int nthreads);
+void or_angle_qualities_f64(const or_mesh* m, const double* xyz, int max_angle, double* q);
+
 /* ---- flat tri / quad meshes with a general grid (or_flat.c, the batched optimiser) ------ */
 void or_dmo_flat_f32(const or_mesh* m, float* xyz, int v0, int v1, float grid_scale, int nq, int depth, int nthreads);
 void or_dmo_quad2d_f64(const or_mesh* m, double* xyz, int v0, int v1, double grid_scale, double* margin, int nthreads);

@@ -71,6 +71,7 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
     }
     else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
     else if (o->mode == MODE_FLAT) launch_dmo_flat(m, L, o->p.grid_n, 32, s);
+    else if (o->mode == MODE_ANGLE) launch_dmo_angle(m, L, o->p.quality == VSDMO_MAX_ANGLE, s);
     else launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, s);
 }
 
@@ -423,7 +424,9 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     vsdmo_params p;
     if (params) p = *params; else vsdmo_params_default(mesh->m.type, &p);
     const Mesh& m = mesh->m;
-    if (p.quality != VSDMO_MEAN_RATIO) return fail(VSDMO_E_UNSUPPORTED, "only MEAN_RATIO is implemented");
+    const bool angle = p.quality == VSDMO_MIN_ANGLE || p.quality == VSDMO_MAX_ANGLE;
+    if (p.quality != VSDMO_MEAN_RATIO && !angle)
+        return fail(VSDMO_E_UNSUPPORTED, "MEAN_RATIO, MIN_ANGLE and MAX_ANGLE are implemented");
     const bool flat2d = (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) && (p.flat < 0 ? m.isFlat : p.flat);
     if (p.grid_n != 8 && !(flat2d && p.grid_n == 4))
         return fail(VSDMO_E_UNSUPPORTED, "only an 8-point grid per axis is implemented (4 or 8 for flat meshes)");
@@ -434,7 +437,21 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     std::unique_ptr<vsdmo_opt_s> o(new vsdmo_opt_s);
     o->mesh = mesh;
     o->p = p;
-    if (m.type == VSDMO_TET) {
+    if (angle) {
+        // angle criteria: tet interiors and flat triangle meshes (8-point grid)
+        const bool tet = m.type == VSDMO_TET;
+        if (!(tet || (m.type == VSDMO_TRI && flat2d)) || p.grid_n != 8)
+            return fail(VSDMO_E_UNSUPPORTED, "angle criteria are implemented for tet meshes and flat triangle meshes "
+                                             "with an 8-point grid");
+        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "set fix_boundary=1 (surface and boundary passes are not implemented)");
+        if ((tet ? m.maxTets : m.maxHE) > dmo_angle_max_ring(m.type))
+            return fail(VSDMO_E_VALENCE, "a vertex's ring exceeds the angle kernel's budget");
+        o->mode = MODE_ANGLE;
+        const bool mx = p.quality == VSDMO_MAX_ANGLE;
+        o->kind = tet ? (mx ? MK_TET_MAXA : MK_TET_MINA) : (mx ? MK_TRI2D_MAXA : MK_TRI2D_MINA);
+        if (tet) for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
+        else for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+    } else if (m.type == VSDMO_TET) {
         if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "surface passes of volume meshes are not implemented yet; set fix_boundary=1");
         if (m.maxTets > dmo_tet_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more tetrahedra than the kernel's ring budget");
         o->mode = MODE_TET;
@@ -478,6 +495,7 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->pfail.alloc(quality_stats_blocks(), s);
         o->done.alloc(1, s); o->done.zero();
         prepare_dmo_kernels();
+        if (o->mode == MODE_ANGLE) prepare_angle_kernels();
         if (o->mode == MODE_SURF) init_surface_state(o.get());
         o->counters.alloc(4, s);
         o->counters.zero();

@@ -14,7 +14,7 @@ struct vsdmo_mesh_s {
     bool destroy_requested = false; // vsdmo_mesh_destroy came while optimisers were alive
 };
 
-enum OptMode { MODE_TET = 0, MODE_TRI2D = 1, MODE_SURF = 2, MODE_HEX = 3, MODE_FLAT = 4 };
+enum OptMode { MODE_TET = 0, MODE_TRI2D = 1, MODE_SURF = 2, MODE_HEX = 3, MODE_FLAT = 4, MODE_ANGLE = 5 };
 
 struct vsdmo_opt_s {
     vsdmo_mesh_s* mesh = nullptr;

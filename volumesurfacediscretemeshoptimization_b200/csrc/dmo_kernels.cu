@@ -27,6 +27,7 @@
 // k_element_qualities replace k_qualityHistogram / k_getElementQualities (dmo/DMOTet.cu:31-43,69-75).
 #include "vsdmo_internal.cuh"
 #include "tc_gemm.cuh"
+#include "angle_metrics.cuh"
 #include <cfloat>
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -1128,6 +1129,18 @@ __device__ float q_hex(const float4* __restrict__ pos, const int* __restrict__ h
 
 __device__ __forceinline__ float element_quality(const int* __restrict__ el, int kind, const float4* __restrict__ pos, long e) {
     if (kind == MK_HEX) return q_hex(pos, el + 8 * e);
+    if (kind == MK_TET_MINA || kind == MK_TET_MAXA) {
+        const int4 t = reinterpret_cast<const int4*>(el)[e];
+        const float4 a = pos[t.x], b = pos[t.y], c = pos[t.z], d = pos[t.w];
+        const float pa[3] = { a.x, a.y, a.z }, pb[3] = { b.x, b.y, b.z }, pc[3] = { c.x, c.y, c.z }, pd[3] = { d.x, d.y, d.z };
+        return kind == MK_TET_MINA ? tet_angle<false>(pa, pb, pc, pd) : tet_angle<true>(pa, pb, pc, pd);
+    }
+    if (kind == MK_TRI2D_MINA || kind == MK_TRI2D_MAXA) {
+        const int* t = el + 3 * e;
+        const float4 a = pos[t[0]], b = pos[t[1]], c = pos[t[2]];
+        return kind == MK_TRI2D_MINA ? tri2d_angle<false>(a.x, a.y, b.x, b.y, c.x, c.y)
+                                     : tri2d_angle<true>(a.x, a.y, b.x, b.y, c.x, c.y);
+    }
     if (kind == MK_TET) {
         const int4 t = reinterpret_cast<const int4*>(el)[e];
         return q_tet(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);

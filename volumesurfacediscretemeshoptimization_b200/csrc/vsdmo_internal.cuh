@@ -181,7 +181,15 @@ void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const 
 int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
 
 // Element metric used by the quality kernels.
-enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4, MK_QUAD2D = 5 };
+enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4, MK_QUAD2D = 5,
+                  MK_TRI2D_MINA = 6, MK_TRI2D_MAXA = 7, MK_TET_MINA = 8, MK_TET_MAXA = 9 };
+
+// ---- angle criteria (angle.cu) ------------------------------------------------------------
+// one colour class with MIN_ANGLE (max_angle = false) or MAX_ANGLE for tet interiors and flat
+// triangle meshes
+void launch_dmo_angle(const Mesh& m, const DmoLaunch& L, bool max_angle, cudaStream_t s);
+int dmo_angle_max_ring(int elem_type);
+void prepare_angle_kernels();
 
 // Per-iteration statistics written by the quality kernel.
 struct IterStats {
