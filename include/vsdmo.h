@@ -336,6 +336,19 @@ VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t opt, unsigned long
  * in FP32, host arrays; N in {16, 32, 64, 96, 128}, K a multiple of 32. */
 VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int M, int N, int K, float* D);
 
+/* The GUI's surface views as sample grids (DMOTriClass / DMOQuadClass::getLocalSurfacePoints
+ * and getEstimateLocalSurfacePoints, dmo/DMOTri.cu:169-183, kernels dmo/DMOCommon.cu:73-150,
+ * dmo/DMOCommon.h:196-276): nu x nv points (xyz, sample i nu + j) around surface vertex vid
+ * (internal numbering) in the frame of its nearest initial vertex's local surface; local: the
+ * quadric itself over twice the search extent; estimate: the blended projection over the
+ * ring's surfaces that the search evaluates. out: 3 nu nv floats, host or device. Surface
+ * optimisers only; feature_sid is for per-sector surfaces of feature vertices, which the
+ * surface optimiser does not accept yet (ignored). */
+VSDMO_API vsdmo_status vsdmo_opt_local_surface_points(vsdmo_opt_t opt, int vid, int nu, int nv, float* out, int mem_space,
+                                                      int feature_sid);
+VSDMO_API vsdmo_status vsdmo_opt_estimate_surface_points(vsdmo_opt_t opt, int vid, int nu, int nv, float* out,
+                                                         int mem_space);
+
 /* ---- batched flat meshes ------------------------------------------------------------------ */
 /* Many independent flat (z = 0) tri and quad meshes optimised together: one persistent launch
  * per iteration takes (mesh, colour class, vertex chunk) work items in colour-major order, each

@@ -887,3 +887,38 @@ void or_optimize_surf_f64(const or_mesh* m, double* X, int n_iter, double gs, in
     }
     free(X0); free(fn); free(vn); free(LS); free(nn); free(q);
 }
+
+/* ======================================================================================== */
+/* sample grids of the surface views (dmo/DMOCommon.cu:73-150, dmo/DMOCommon.h:196-276)     */
+/* ======================================================================================== */
+void or_surface_points_f32(const or_mesh* m, const float* X, const float* X0, const float* LS, const int32_t* nn,
+                           int vid, int nu, int nv, float gs, int estimate_mode, float* out) {
+    const int* rp = or__he_rowptr(m);
+    const int* he = or__he(m);
+    surf32 S = { m, X0, LS, nn, NULL };
+    const float* c0 = X + 3 * (size_t)vid;
+    float md = -FLT_MAX;
+    for (int i = rp[vid]; i < rp[vid + 1]; ++i) {
+        const float* t = X + 3 * (size_t)he[4 * i];
+        float d[3] = { t[0] - c0[0], t[1] - c0[1], t[2] - c0[2] };
+        md = fmaxf(md, sqrtf(dot3f(d, d)));
+    }
+    const float* L = LS + LSF * (size_t)nn[vid];
+    float q[3] = { c0[0] - L[0], c0[1] - L[1], c0[2] - L[2] };
+    const float cu = dot3f(q, L + 4), cv = dot3f(q, L + 8);
+    float uMax = gs * md, uMin = -gs * md, vMax = gs * md, vMin = -gs * md;
+    if (!estimate_mode) { uMin *= 2.f; uMax *= 2.f; vMin *= 2.f; vMax *= 2.f; }
+    const float afU = 1.f / (float)(nu - 1), afV = 1.f / (float)(nv - 1);
+    for (int idx = 0; idx < nu * nv; ++idx) {
+        const int j = idx % nu, i = idx / nu;
+        const float u = cu + afU * ((float)i * uMin + (float)(nu - 1 - i) * uMax);
+        const float v = cv + afV * ((float)j * vMin + (float)(nv - 1 - j) * vMax);
+        float* o = out + 3 * (size_t)idx;
+        if (estimate_mode) {
+            est32(&S, vid, u, v, o);
+        } else {
+            const float w = poly32(L, u, v);
+            for (int a = 0; a < 3; ++a) o[a] = ((L[a] + u * L[4 + a]) + v * L[8 + a]) + w * L[12 + a];
+        }
+    }
+}

@@ -85,6 +85,7 @@ def lib():
         L.or_optimize_hex_f32.argtypes = [P, P, I, F, I, P, P]
         L.or_optimize_hex_f64.argtypes = [P, P, I, D, I, P, P]
         L.or_dmo_angle_f64.argtypes = [P, P, I, I, D, I, P, I]
+        L.or_surface_points_f32.argtypes = [P, P, P, P, P, I, I, I, F, I, P]
         L.or_angle_qualities_f64.argtypes = [P, P, I, P]
         for n in ("or_q_tet_min_angle_f64", "or_q_tet_max_angle_f64"):
             getattr(L, n).restype = D
@@ -174,6 +175,15 @@ class OracleMesh:
         margin = np.zeros(max(v1 - v0, 1), dtype=np.float64)
         lib().or_dmo_angle_f64(self.h, _p(xyz), v0, v1, grid_scale, int(max_angle), _p(margin), nthreads)
         return xyz, margin[: v1 - v0]
+
+    def surface_points_f32(self, xyz, state, vid, nu, nv, estimate, grid_scale=0.5):
+        """Sample grid of a surface view; state = (xyz_init, local_surfaces, nearest)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+        x0, ls, nn = (np.ascontiguousarray(a) for a in state)
+        out = np.zeros((nu * nv, 3), np.float32)
+        lib().or_surface_points_f32(self.h, _p(xyz), _p(x0), _p(ls), _p(nn), int(vid), int(nu), int(nv), grid_scale,
+                                    int(estimate), _p(out))
+        return out
 
     def angle_qualities_f64(self, xyz, max_angle=False):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)

@@ -159,6 +159,9 @@ void or_optimize_surf_f32(const or_mesh* m, float* xyz, int n_iter, float grid_s
                           double* min_hist, double* mean_hist);
 void or_optimize_surf_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
                           double* min_hist, double* mean_hist);
+/* nu x nv samples of vertex vid's own surface (estimate_mode 0) or of the blended estimate (1) */
+void or_surface_points_f32(const or_mesh* m, const float* xyz, const float* xyz_init, const float* local_surfaces,
+                           const int32_t* nearest, int vid, int nu, int nv, float grid_scale, int estimate_mode, float* out);
 float  or_q_tri3d_f32(const float* p0, const float* p1, const float* p2);
 double or_q_tri3d_f64(const double* p0, const double* p1, const double* p2);
 float  or_q_quad_f32(const float* p0, const float* p1, const float* p2, const float* p3, const float* n);

@@ -214,3 +214,23 @@ def test_surface_benchmark_mesh_properties(oracle_mod, vsdmo, cfg, kind, iters):
     mn, mean = opt.history()
     assert np.all(np.diff(mn) >= -1e-6)
     assert mean[-1] > mean[0]
+
+
+@pytest.mark.parametrize("name", ["ico3", "torus64x32"])
+def test_surface_view_samples_bitwise(oracle_mod, vsdmo, name):
+    """getLocalSurfacePoints / getEstimateLocalSurfacePoints: the sample grids of the GUI's
+    surface views, after two iterations (moved vertices, walked nearest neighbours), bitwise
+    against the oracle with the optimiser's own state."""
+    om, gm = _pair(oracle_mod, vsdmo, name)
+    opt = _opt(vsdmo, gm, n_iter=2)
+    opt.optimize()
+    state = opt.surface_state()
+    x = gm.positions()
+    for vid in (0, 7, gm.info["nSurf"] - 1):
+        for est, fn in ((False, opt.getLocalSurfacePoints), (True, opt.getEstimateLocalSurfacePoints)):
+            g = fn(vid, 5, 7)
+            o = om.surface_points_f32(x, state, vid, 5, 7, est)
+            assert g.shape == (35, 3) and np.all(np.isfinite(g))
+            assert same_bits(g, o), (vid, est)
+    with pytest.raises(vsdmo.VSDMOError):
+        opt.getLocalSurfacePoints(gm.info["nSurf"], 4, 4)

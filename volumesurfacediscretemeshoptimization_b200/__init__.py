@@ -382,6 +382,19 @@ class _DMOBase:
     def launches_per_iteration(self) -> int:
         return _capi.lib().vsdmo_opt_launches_per_iteration(self.h)
 
+    def getLocalSurfacePoints(self, vid: int, nu: int, nv: int, featureSid: int = 0) -> np.ndarray:
+        """Samples [nu * nv x 3] of vertex vid's (internal numbering) own local surface."""
+        out = np.zeros((nu * nv, 3), np.float32)
+        check(_capi.lib().vsdmo_opt_local_surface_points(self.h, int(vid), int(nu), int(nv), _ptr(out), _capi.HOST,
+                                                         int(featureSid)))
+        return out
+
+    def getEstimateLocalSurfacePoints(self, vid: int, nu: int, nv: int) -> np.ndarray:
+        """Samples [nu * nv x 3] of the blended surface estimate around vertex vid."""
+        out = np.zeros((nu * nv, 3), np.float32)
+        check(_capi.lib().vsdmo_opt_estimate_surface_points(self.h, int(vid), int(nu), int(nv), _ptr(out), _capi.HOST))
+        return out
+
     def surface_state(self):
         """(xyz_init [nSurf,3], local_surfaces [nSurf,16], nearest [nSurf]) of a surface
         optimiser, internal vertex numbering."""

@@ -36,7 +36,7 @@ EXPORTED = [
     "vsdmo_batch_set_positions", "vsdmo_batch_get_config", "vsdmo_batch_set_config", "vsdmo_batch_autotune",
     "vsdmo_batch_info", "vsdmo_batch_mesh_info",
     "vsdmo_file_read", "vsdmo_file_write", "vsdmo_mesh_create_from_file", "vsdmo_mesh_write_file",
-    "vsdmo_mesh_create_surface",
+    "vsdmo_mesh_create_surface", "vsdmo_opt_local_surface_points", "vsdmo_opt_estimate_surface_points",
 ]
 
 
@@ -181,6 +181,10 @@ def lib():
     L.vsdmo_mesh_write_file.argtypes = [P, C.c_char_p, I]
     L.vsdmo_mesh_create_surface.restype = S
     L.vsdmo_mesh_create_surface.argtypes = [P, U, P, C.POINTER(P)]
+    L.vsdmo_opt_local_surface_points.restype = S
+    L.vsdmo_opt_local_surface_points.argtypes = [P, I, I, I, P, I, I]
+    L.vsdmo_opt_estimate_surface_points.restype = S
+    L.vsdmo_opt_estimate_surface_points.argtypes = [P, I, I, I, P, I]
     L.vsdmo_batch_mesh_info.restype = S
     L.vsdmo_batch_mesh_info.argtypes = [P, I, P]
     _lib = L

@@ -417,6 +417,41 @@ VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* 
     });
 }
 
+namespace {
+vsdmo_status surface_points(vsdmo_opt_t o, int estimate_mode, int vid, int nu, int nv, float* out, int mem_space) {
+    if (!o || !out) return fail(VSDMO_E_ARG, "null argument");
+    if (o->mode != MODE_SURF) return fail(VSDMO_E_ARG, "not a surface optimiser");
+    const Mesh& m = o->mesh->m;
+    if (vid < 0 || vid >= m.nSurf) return fail(VSDMO_E_ARG, "vid must be a surface vertex (internal numbering)");
+    if (nu < 2 || nv < 2 || (long)nu * nv > (1L << 24)) return fail(VSDMO_E_ARG, "nu, nv must be >= 2 (at most 2^24 samples)");
+    if (mem_space != VSDMO_HOST && mem_space != VSDMO_DEVICE) return fail(VSDMO_E_ARG, "bad mem_space");
+    return guarded([&] {
+        cudaStream_t s = m.stream;
+        const size_t n = 3 * (size_t)nu * nv;
+        if (mem_space == VSDMO_DEVICE) {
+            launch_surface_samples(m, estimate_mode, vid, nu, nv, o->p.grid_scale, o->X0.p, o->LS.p, o->nn.p, out, s);
+            m.sync();
+            return;
+        }
+        DBuf<float> d(n, s);
+        launch_surface_samples(m, estimate_mode, vid, nu, nv, o->p.grid_scale, o->X0.p, o->LS.p, o->nn.p, d.p, s);
+        VSDMO_CUDA(cudaMemcpyAsync(out, d.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+        m.sync();
+    });
+}
+}  // namespace
+
+VSDMO_API vsdmo_status vsdmo_opt_local_surface_points(vsdmo_opt_t opt, int vid, int nu, int nv, float* out, int mem_space,
+                                                      int feature_sid) {
+    (void)feature_sid;   // meshes with feature vertices are not accepted by the surface optimiser yet
+    return surface_points(opt, 0, vid, nu, nv, out, mem_space);
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_estimate_surface_points(vsdmo_opt_t opt, int vid, int nu, int nv, float* out,
+                                                         int mem_space) {
+    return surface_points(opt, 1, vid, nu, nv, out, mem_space);
+}
+
 VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* params, vsdmo_opt_t* out) {
     if (!out) return fail(VSDMO_E_ARG, "null output handle");
     *out = nullptr;

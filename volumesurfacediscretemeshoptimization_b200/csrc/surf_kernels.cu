@@ -33,6 +33,7 @@
 // operation order, reproduced by the oracle's f32 mirror bit for bit (built with
 // --fmad=false here and without contraction there).
 #include "vsdmo_internal.cuh"
+#include <algorithm>
 #include <cfloat>
 
 namespace vsdmo {
@@ -352,7 +353,76 @@ k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4*
 
 }  // namespace
 
+// Sample grids of the GUI's surface views (DMOTriClass::getLocalSurfacePoints /
+// getEstimateLocalSurfacePoints, dmo/DMOTri.cu:169-183; kernels dmo/DMOCommon.cu:73-150 and
+// dmo/DMOCommon.h:196-276): nu x nv points around the vertex's current local coordinates in
+// the frame of its nearest initial vertex's surface, sample idx = i nu + j with u from i and v
+// from j, half-extent grid_scale x the ring's largest distance (twice that for the own
+// surface). estimate = 0: the own quadric (localToWorldCoords); 1: the blended projection over
+// the ring's surfaces, as the search evaluates candidates.
+__global__ void k_surface_samples(int estimate_mode, int vid, int nu, int nv, float grid_scale,
+                                  const float4* __restrict__ pos, const int* __restrict__ rowptr,
+                                  const int4* __restrict__ he, const float4* __restrict__ X0,
+                                  const float4* __restrict__ LS, const int* __restrict__ nn, float* __restrict__ out) {
+    extern __shared__ float4 ss[];
+    __shared__ float s_md;
+    const int b = rowptr[vid], k = rowptr[vid + 1] - b;
+    float4* nbL = ss;
+    float4* nbX = ss + 4 * k;
+    const float4 c0 = pos[vid];
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const int nnN = nn[he[b + i].x];
+        nbL[4 * i] = LS[4L * nnN]; nbL[4 * i + 1] = LS[4L * nnN + 1];
+        nbL[4 * i + 2] = LS[4L * nnN + 2]; nbL[4 * i + 3] = LS[4L * nnN + 3];
+        nbX[i] = X0[nnN];
+    }
+    if (threadIdx.x == 0) {
+        float md = -FLT_MAX;
+        for (int i = 0; i < k; ++i) {
+            const float4 t = pos[he[b + i].x];
+            const float dx = t.x - c0.x, dy = t.y - c0.y, dz = t.z - c0.z;
+            md = fmaxf(md, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+        }
+        s_md = md;
+    }
+    __syncthreads();
+    const int nnv = nn[vid];
+    Surf L;
+    L.l0 = LS[4L * nnv]; L.l1 = LS[4L * nnv + 1]; L.l2 = LS[4L * nnv + 2]; L.l3 = LS[4L * nnv + 3];
+    const float4 x0 = X0[nnv];
+    const float dx = c0.x - L.l0.x, dy = c0.y - L.l0.y, dz = c0.z - L.l0.z;
+    const float cu = dot3(dx, dy, dz, L.l1.x, L.l1.y, L.l1.z);
+    const float cv = dot3(dx, dy, dz, L.l2.x, L.l2.y, L.l2.z);
+    float uMax = grid_scale * s_md, uMin = -grid_scale * s_md;
+    float vMax = grid_scale * s_md, vMin = -grid_scale * s_md;
+    if (!estimate_mode) { uMin *= 2.f; uMax *= 2.f; vMin *= 2.f; vMax *= 2.f; }
+    const float afU = 1.f / (float)(nu - 1), afV = 1.f / (float)(nv - 1);
+    for (int idx = threadIdx.x; idx < nu * nv; idx += blockDim.x) {
+        const int j = idx % nu, i = idx / nu;
+        const float u = cu + afU * ((float)i * uMin + (float)(nu - 1 - i) * uMax);
+        const float v = cv + afV * ((float)j * vMin + (float)(nv - 1 - j) * vMax);
+        float3 p;
+        if (estimate_mode) {
+            p = estimate(L, x0, nbL, nbX, k, u, v);
+        } else {
+            const float w = poly(L.l0, L.l1, L.l2, u, v);
+            p = make_float3(((L.l0.x + u * L.l1.x) + v * L.l2.x) + w * L.l3.x,
+                            ((L.l0.y + u * L.l1.y) + v * L.l2.y) + w * L.l3.y,
+                            ((L.l0.z + u * L.l1.z) + v * L.l2.z) + w * L.l3.z);
+        }
+        out[3L * idx] = p.x; out[3L * idx + 1] = p.y; out[3L * idx + 2] = p.z;
+    }
+}
+
 int dmo_surf_max_ring() { return SURF_MAX_RING; }
+
+void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, int nv, float grid_scale,
+                            const float4* X0, const float4* LS, const int* nn, float* out, cudaStream_t s) {
+    const size_t smem = (size_t)5 * std::max(m.maxHE, 1) * sizeof(float4);
+    k_surface_samples<<<1, 256, smem, s>>>(estimate_mode, vid, nu, nv, grid_scale, m.pos.p, m.he_rowptr.p, m.he.p, X0,
+                                           LS, nn, out);
+    VSDMO_CHECK_LAUNCH();
+}
 
 void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, cudaStream_t s) {
     if (m.nSurf <= 0) return;

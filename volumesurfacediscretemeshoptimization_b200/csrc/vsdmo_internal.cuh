@@ -179,6 +179,9 @@ void launch_update_nn(const Mesh& m, const float4* X0, int* nn, cudaStream_t s);
 void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
                      cudaStream_t s);
 int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
+// nu x nv samples of vertex vid's own surface (estimate_mode 0) or of the blended estimate (1)
+void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, int nv, float grid_scale,
+                            const float4* X0, const float4* LS, const int* nn, float* out, cudaStream_t s);
 
 // Element metric used by the quality kernels.
 enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4, MK_QUAD2D = 5,
