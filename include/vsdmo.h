@@ -199,8 +199,10 @@ VSDMO_API vsdmo_status vsdmo_mesh_create_surface(vsdmo_mesh_t volume, uint32_t c
 /* ---- optimiser ------------------------------------------------------------------------- */
 /* Replaces DMOTetClass / DMOTriFlatClass / DMOTriClass / DMOQuadClass construction + init()
  * (dmo/DMOTet.cu:82-125, dmo/DMOTriFlat.cu:84-126, dmo/DMOTri.cu:80-126, dmo/DMOQuad.cu:78-123).
- * Tri and quad meshes that are not flat (or flat = 0) get the surface optimiser; it needs a
- * mesh without feature vertices (VSDMO_E_UNSUPPORTED otherwise). Flat quad meshes get the 2D
+ * Tri and quad meshes that are not flat (or flat = 0) get the surface optimiser (feature
+ * vertices: sector surfaces for their neighbours; with fix_boundary = 0 they slide along their
+ * feature curves, the reference's k_optimizeHierarchical1D). Flat triangle meshes with
+ * fix_boundary = 0 slide their boundary vertices (k_optimizeHierarchical1DFlat). Flat quad meshes get the 2D
  * search of DMOTriFlatClass with the quad mean ratio against +z (meanRatioMetricQuad(p, n),
  * dmo/DMOQualityQuad.h:30-50; the reference has no flat-quad class). Hex meshes get the
  * interior search of DMOHexClass (dmo/DMOHex.cu, k_optimizeHierarchicalInnerHex). */
@@ -336,6 +338,16 @@ VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t opt, unsigned long
  * in FP32, host arrays; N in {16, 32, 64, 96, 128}, K a multiple of 32. */
 VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int M, int N, int K, float* D);
 
+/* Feature-vertex state of an optimiser with feature vertices (surfaces with features, flat
+ * meshes with sliding boundaries), internal numbering: curves [nSurf x 12] (p0[3] a, e0[3] 0,
+ * e1[3] 0; computeLocalSurface1d, dmo/Surface1D.cu:41-82), fdeg [nSurf] (feature ring
+ * vertices), flags [nSurf] (the 1D pass moves the vertex; calcOptFeatureVec,
+ * dmo/DMOCommon.h:130-180); surfaces only: sector_rowptr [nFeature + 1], sector_table
+ * [nFeature x 20], sector_surfaces [n_sectors x 16] (initLocalSurfacesFeature,
+ * dmo/surfaceP/SurfaceFeature.h:79-106). Any output may be NULL. */
+VSDMO_API vsdmo_status vsdmo_opt_feature_state(vsdmo_opt_t opt, float* curves, int32_t* fdeg, uint8_t* flags,
+                                               int32_t* sector_rowptr, int32_t* sector_table, float* sector_surfaces,
+                                               int* n_sectors);
 /* The GUI's surface views as sample grids (DMOTriClass / DMOQuadClass::getLocalSurfacePoints
  * and getEstimateLocalSurfacePoints, dmo/DMOTri.cu:169-183, kernels dmo/DMOCommon.cu:73-150,
  * dmo/DMOCommon.h:196-276): nu x nv points (xyz, sample i nu + j) around surface vertex vid

@@ -486,7 +486,39 @@ typedef struct {
     const double* LS;   /* local surfaces of the initial positions */
     const int32_t* nn;  /* nearest initial vertex */
     const double* vn;   /* current vertex normals */
+    /* feature vertices' sector surfaces (NULL: the mesh has none) and the positions the sector
+       of a feature neighbour is chosen from (the positions at the start of the colour class) */
+    const int32_t* frow; const int32_t* ftab; const double* FS; const double* Xs;
 } surf64;
+
+/* sector surface of feature vertex f seen from vertex v: the sector of f's halfedge whose target
+   is closest to v (localSurfaceEstimationWithFeature, dmo/SurfaceEstimation.h:150-172) */
+static int sector_of(const or_mesh* m, const int32_t* frow, const int32_t* ftab, int f, int nFree, const double* Xs64,
+                     const float* Xs32, int v) {
+    const int* rp = or__he_rowptr(m);
+    const int* he = or__he(m);
+    int arg = 0, idx = 0;
+    if (Xs64) {
+        double best = DBL_MAX;
+        const double* pv = Xs64 + 3 * (size_t)v;
+        for (int i = rp[f]; i < rp[f + 1]; ++i, ++idx) {
+            const double* t = Xs64 + 3 * (size_t)he[4 * i];
+            double d[3] = { t[0] - pv[0], t[1] - pv[1], t[2] - pv[2] };
+            double s = dot3d(d, d);
+            if (s < best) { best = s; arg = idx; }
+        }
+    } else {
+        float best = FLT_MAX;
+        const float* pv = Xs32 + 3 * (size_t)v;
+        for (int i = rp[f]; i < rp[f + 1]; ++i, ++idx) {
+            const float* t = Xs32 + 3 * (size_t)he[4 * i];
+            float d[3] = { t[0] - pv[0], t[1] - pv[1], t[2] - pv[2] };
+            float s = dot3f(d, d);
+            if (s < best) { best = s; arg = idx; }
+        }
+    }
+    return frow[f - nFree] + ftab[TABLE_SIZE * (f - nFree) + arg];
+}
 
 static inline double poly64(const double* L, double u, double v) { return L[3] * u * u + L[7] * u * v + L[11] * v * v; }
 
@@ -512,7 +544,9 @@ static void est64(const surf64* S, int v, double u, double vv, double* out) {
         ++k;
         ids[k] = 1.0 / (dot3d(d, d) + EPS);
         isum += ids[k];
+        const int nFree = or_mesh_info(S->m, OR_I_NSURF) - or_mesh_info(S->m, OR_I_NFEATURE);
         const double* Ln = S->LS + LSF * (size_t)S->nn[vN];
+        if (S->FS && nnN >= nFree) Ln = S->FS + LSF * (size_t)sector_of(S->m, S->frow, S->ftab, nnN, nFree, S->Xs, NULL, v);
         double q[3] = { pw[0] - Ln[0], pw[1] - Ln[1], pw[2] - Ln[2] };
         double lu = q[0] * Ln[4] + q[1] * Ln[5] + q[2] * Ln[6];
         double lv = q[0] * Ln[8] + q[1] * Ln[9] + q[2] * Ln[10];
@@ -622,9 +656,24 @@ static void surf_vertex_f64(const surf64* S, double* X, int v, double gs, double
     free(ring);
 }
 
+void or_dmo_surf_feat_f64(const or_mesh* m, double* X, const double* X0, const double* LS, const int32_t* nn,
+                          const double* vn, const int32_t* frow, const int32_t* ftab, const double* FS, int v0, int v1,
+                          double gs, double* margin, int nthreads) {
+    const int nS = or_mesh_info(m, OR_I_NSURF);
+    double* Xs = FS ? (double*)malloc(sizeof(double) * 3 * (size_t)nS) : NULL;
+    if (Xs) memcpy(Xs, X, sizeof(double) * 3 * (size_t)nS);
+    surf64 S = { m, X0, LS, nn, vn, frow, ftab, FS, Xs };
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+    for (int v = v0; v < v1; ++v) surf_vertex_f64(&S, X, v, gs, margin ? margin + (v - v0) : NULL);
+    free(Xs);
+}
+
 void or_dmo_surf_f64(const or_mesh* m, double* X, const double* X0, const double* LS, const int32_t* nn,
                      const double* vn, int v0, int v1, double gs, double* margin, int nthreads) {
-    surf64 S = { m, X0, LS, nn, vn };
+    surf64 S = { m, X0, LS, nn, vn, NULL, NULL, NULL, NULL };
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 16)
@@ -641,6 +690,7 @@ typedef struct {
     const float* LS;
     const int32_t* nn;
     const float* vn;
+    const int32_t* frow; const int32_t* ftab; const float* FS; const float* Xs;
 } surf32;
 
 static inline float poly32(const float* L, float u, float v) { return (((L[3] * u) * u) + ((L[7] * u) * v)) + ((L[11] * v) * v); }
@@ -663,7 +713,10 @@ static void est32(const surf32* S, int v, float u, float vv, float* out) {
         float dn[3] = { xn[0] - pw[0], xn[1] - pw[1], xn[2] - pw[2] };
         float idn = 1.0f / (dot3f(dn, dn) + EPS);
         isum = isum + idn;
-        const float* Ln = S->LS + LSF * (size_t)S->nn[vN];
+        const int nnN = S->nn[vN];
+        const int nFree = or_mesh_info(S->m, OR_I_NSURF) - or_mesh_info(S->m, OR_I_NFEATURE);
+        const float* Ln = S->LS + LSF * (size_t)nnN;
+        if (S->FS && nnN >= nFree) Ln = S->FS + LSF * (size_t)sector_of(S->m, S->frow, S->ftab, nnN, nFree, NULL, S->Xs, v);
         float q[3] = { pw[0] - Ln[0], pw[1] - Ln[1], pw[2] - Ln[2] };
         float lu = dot3f(q, Ln + 4), lv = dot3f(q, Ln + 8);
         float lw = poly32(Ln, lu, lv);
@@ -769,9 +822,24 @@ static void surf_vertex_f32(const surf32* S, float* X, int v, float gs) {
     free(ring);
 }
 
+void or_dmo_surf_feat_f32(const or_mesh* m, float* X, const float* X0, const float* LS, const int32_t* nn,
+                          const float* vn, const int32_t* frow, const int32_t* ftab, const float* FS, int v0, int v1,
+                          float gs, int nthreads) {
+    const int nS = or_mesh_info(m, OR_I_NSURF);
+    float* Xs = FS ? (float*)malloc(sizeof(float) * 3 * (size_t)nS) : NULL;
+    if (Xs) memcpy(Xs, X, sizeof(float) * 3 * (size_t)nS);
+    surf32 S = { m, X0, LS, nn, vn, frow, ftab, FS, Xs };
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+    for (int v = v0; v < v1; ++v) surf_vertex_f32(&S, X, v, gs);
+    free(Xs);
+}
+
 void or_dmo_surf_f32(const or_mesh* m, float* X, const float* X0, const float* LS, const int32_t* nn,
                      const float* vn, int v0, int v1, float gs, int nthreads) {
-    surf32 S = { m, X0, LS, nn, vn };
+    surf32 S = { m, X0, LS, nn, vn, NULL, NULL, NULL, NULL };
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 16)

@@ -86,6 +86,17 @@ def lib():
         L.or_optimize_hex_f64.argtypes = [P, P, I, D, I, P, P]
         L.or_dmo_angle_f64.argtypes = [P, P, I, I, D, I, P, I]
         L.or_surface_points_f32.argtypes = [P, P, P, P, P, I, I, I, F, I, P]
+        L.or_feature_flags.argtypes = [P, P, P, P]
+        L.or_feature_surfaces_f32.restype = I
+        L.or_feature_surfaces_f32.argtypes = [P, P, P, P, P, P, I]
+        L.or_feature_surfaces_f64.restype = I
+        L.or_feature_surfaces_f64.argtypes = [P, P, P, P, P, P, I]
+        L.or_dmo_surf_feat_f32.argtypes = [P, P, P, P, P, P, P, P, P, I, I, F, I]
+        L.or_dmo_surf_feat_f64.argtypes = [P, P, P, P, P, P, P, P, P, I, I, D, P, I]
+        L.or_surface_fit_1d_f32.argtypes = [P, P, P, P]
+        L.or_surface_fit_1d_f64.argtypes = [P, P, P, P]
+        L.or_dmo_1d_f32.argtypes = [P, P, P, P, P, P, P, P, I, I, F, I]
+        L.or_dmo_1d_f64.argtypes = [P, P, P, P, P, P, P, P, I, I, D, P, I]
         L.or_angle_qualities_f64.argtypes = [P, P, I, P]
         for n in ("or_q_tet_min_angle_f64", "or_q_tet_max_angle_f64"):
             getattr(L, n).restype = D
@@ -184,6 +195,79 @@ class OracleMesh:
         lib().or_surface_points_f32(self.h, _p(xyz), _p(x0), _p(ls), _p(nn), int(vid), int(nu), int(nv), grid_scale,
                                     int(estimate), _p(out))
         return out
+
+    # ---- 1D feature / boundary pass ---------------------------------------------------------
+    def feature_flags(self, xyz):
+        """(fdeg [nSurf], opt [nSurf] uint8) from the positions."""
+        nS = self.info["nSurf"]
+        fdeg = np.zeros(nS, np.int32)
+        opt = np.zeros(nS, np.uint8)
+        lib().or_feature_flags(self.h, _p(np.ascontiguousarray(xyz, np.float32)), _p(fdeg), _p(opt))
+        return fdeg, opt
+
+    def sector_surfaces(self, xyz, fn, dtype=np.float32):
+        """Per-sector surfaces of the feature vertices: (rowptr [nFeature+1], table
+        [nFeature x 20], surfaces [nSectors x 16]); fn: face normals [nTris x 3]."""
+        nF = self.info["nFeature"]
+        cap = 20 * max(nF, 1)
+        rowptr = np.zeros(nF + 1, np.int32)
+        table = np.zeros(max(nF, 1) * 20, np.int32)
+        ls = np.zeros((cap, 16), dtype)
+        fn_ = lib().or_feature_surfaces_f32 if dtype == np.float32 else lib().or_feature_surfaces_f64
+        ns = fn_(self.h, _p(np.ascontiguousarray(xyz, dtype)), _p(np.ascontiguousarray(fn, dtype)), _p(rowptr),
+                 _p(table), _p(ls), cap)
+        if ns < 0:
+            raise ValueError("feature vertex beyond the sector table sizes")
+        return rowptr, table[: 20 * nF].reshape(nF, 20), ls[:ns]
+
+    def dmo_surf_feat_f32(self, xyz, x0, ls, nn, vn, sectors, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        rp, tab, fs = (np.ascontiguousarray(a) for a in sectors)
+        lib().or_dmo_surf_feat_f32(self.h, _p(xyz), _p(np.ascontiguousarray(x0, np.float32)),
+                                   _p(np.ascontiguousarray(ls, np.float32)), _p(np.ascontiguousarray(nn, np.int32)),
+                                   _p(np.ascontiguousarray(vn, np.float32)), _p(rp), _p(tab),
+                                   _p(np.ascontiguousarray(fs, np.float32)), v0, v1, grid_scale, nthreads)
+        return xyz
+
+    def dmo_surf_feat_f64(self, xyz, x0, ls, nn, vn, sectors, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        rp, tab, fs = sectors
+        margin = np.zeros(max(v1 - v0, 1))
+        lib().or_dmo_surf_feat_f64(self.h, _p(xyz), _p(np.ascontiguousarray(x0, np.float64)),
+                                   _p(np.ascontiguousarray(ls, np.float64)), _p(np.ascontiguousarray(nn, np.int32)),
+                                   _p(np.ascontiguousarray(vn, np.float64)), _p(np.ascontiguousarray(rp, np.int32)),
+                                   _p(np.ascontiguousarray(tab, np.int32)), _p(np.ascontiguousarray(fs, np.float64)),
+                                   v0, v1, grid_scale, _p(margin), nthreads)
+        return xyz, margin[: v1 - v0]
+
+    def curves_f32(self, xyz, vn):
+        nS = self.info["nSurf"]
+        out = np.zeros((nS, 12), np.float32)
+        lib().or_surface_fit_1d_f32(self.h, _p(np.ascontiguousarray(xyz, np.float32)),
+                                    _p(np.ascontiguousarray(vn, np.float32)), _p(out))
+        return out
+
+    def curves_f64(self, xyz, vn):
+        nS = self.info["nSurf"]
+        out = np.zeros((nS, 12), np.float64)
+        lib().or_surface_fit_1d_f64(self.h, _p(np.ascontiguousarray(xyz, np.float64)),
+                                    _p(np.ascontiguousarray(vn, np.float64)), _p(out))
+        return out
+
+    def dmo_1d_f32(self, xyz, x0, curves, nn, vn, fdeg, opt, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        a = [np.ascontiguousarray(x) for x in (x0, curves, nn, vn, fdeg, opt)]
+        lib().or_dmo_1d_f32(self.h, _p(xyz), *[_p(x) for x in a], v0, v1, grid_scale, nthreads)
+        return xyz
+
+    def dmo_1d_f64(self, xyz, x0, curves, nn, vn, fdeg, opt, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        a = [np.ascontiguousarray(x0, np.float64), np.ascontiguousarray(curves, np.float64),
+             np.ascontiguousarray(nn, np.int32), np.ascontiguousarray(vn, np.float64),
+             np.ascontiguousarray(fdeg, np.int32), np.ascontiguousarray(opt, np.uint8)]
+        margin = np.zeros(max(v1 - v0, 1), np.float64)
+        lib().or_dmo_1d_f64(self.h, _p(xyz), *[_p(x) for x in a], v0, v1, grid_scale, _p(margin), nthreads)
+        return xyz, margin[: v1 - v0]
 
     def angle_qualities_f64(self, xyz, max_angle=False):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)

@@ -117,6 +117,21 @@ void or_dmo_quad2d_f64(const or_mesh* m, double* xyz, int v0, int v1, double gri
 float  or_q_quad2d_f32(const float* p0, const float* p1, const float* p2, const float* p3);
 double or_q_quad2d_f64(const double* p0, const double* p1, const double* p2, const double* p3);
 
+/* ---- 1D feature / boundary pass (or_feat.c) ---------------------------------------------- */
+/* fdeg [nSurf]: feature ring vertices of every surface vertex; opt [nSurf]: feature vertices the
+ * pass moves (two feature neighbours at >= 160 degrees) */
+void or_feature_flags(const or_mesh* m, const float* xyz, int32_t* fdeg, uint8_t* opt);
+/* curves [nSurf x 12] (p0[3] a, e0[3] 0, e1[3] 0) of the feature vertices (zeros elsewhere) */
+void or_surface_fit_1d_f32(const or_mesh* m, const float* xyz, const float* vertex_normals, float* curves);
+void or_surface_fit_1d_f64(const or_mesh* m, const double* xyz, const double* vertex_normals, double* curves);
+/* one feature colour class [v0, v1) */
+void or_dmo_1d_f32(const or_mesh* m, float* xyz, const float* xyz_init, const float* curves, const int32_t* nearest,
+                   const float* vertex_normals, const int32_t* fdeg, const uint8_t* opt, int v0, int v1,
+                   float grid_scale, int nthreads);
+void or_dmo_1d_f64(const or_mesh* m, double* xyz, const double* xyz_init, const double* curves, const int32_t* nearest,
+                   const double* vertex_normals, const int32_t* fdeg, const uint8_t* opt, int v0, int v1,
+                   double grid_scale, double* margin, int nthreads);
+
 /* ---- hexahedra (or_hex.c) ------------------------------------------------------------- */
 /* shapeMetricHex of corners v[0..7] (literal f64 / reference-order f32 with cbrtf) */
 double or_q_hex_f64(const double v[8][3]);
@@ -153,6 +168,18 @@ void or_dmo_surf_f32(const or_mesh* m, float* xyz, const float* xyz_init, const 
 void or_dmo_surf_f64(const or_mesh* m, double* xyz, const double* xyz_init, const double* local_surfaces,
                      const int32_t* nearest, const double* vertex_normals, int v0, int v1, double grid_scale,
                      double* margin, int nthreads);
+/* the free-vertex surface search on meshes with feature vertices: the ring's feature neighbours
+ * project onto the sector surface (rowptr / table / surfaces of or_feature_surfaces_*) of the
+ * halfedge whose target is nearest to the vertex, nearest by the positions at the start of the
+ * colour class */
+void or_dmo_surf_feat_f32(const or_mesh* m, float* xyz, const float* xyz_init, const float* local_surfaces,
+                          const int32_t* nearest, const float* vertex_normals, const int32_t* rowptr,
+                          const int32_t* table, const float* sector_surfaces, int v0, int v1, float grid_scale,
+                          int nthreads);
+void or_dmo_surf_feat_f64(const or_mesh* m, double* xyz, const double* xyz_init, const double* local_surfaces,
+                          const int32_t* nearest, const double* vertex_normals, const int32_t* rowptr,
+                          const int32_t* table, const double* sector_surfaces, int v0, int v1, double grid_scale,
+                          double* margin, int nthreads);
 void or_surface_qualities_f32(const or_mesh* m, const float* xyz, float* q);
 void or_surface_qualities_f64(const or_mesh* m, const double* xyz, double* q);
 void or_optimize_surf_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale, int nthreads,

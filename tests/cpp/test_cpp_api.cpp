@@ -52,11 +52,21 @@ int main() {
         if (!(q1 > q0) || !dmo.isDone() || total != (int)tets.size() / 4) return 1;
         // an error surfaces as an exception carrying the status
         try {
-            DMO::DMOTetClass bad(*mesh, DMO::QualityCriterium::MIN_ANGLE);
+            DMO::DMOTetClass bad(*mesh, DMO::QualityCriterium::RADIUS_RATIO);
             return 2;
         } catch (const DMO::Error& e) {
             if (e.status != VSDMO_E_UNSUPPORTED) return 3;
         }
+        // files: write the optimised mesh, read it back through the factory, and a missing file
+        // gives nullptr like the reference's factories
+        const std::string base = "/tmp/vsdmo_cpp_api_mesh";
+        DMO::writeTetgen(base, static_cast<const DMO::DMOMeshTet&>(*mesh));
+        auto again = DMO::DMOMeshTetFactory::create(base);
+        if (!again || again->nVertices() != mesh->nVertices()) return 5;
+        if (again->getVertexPoints(true) != mesh->getVertexPoints(true)) return 6;
+        if (DMO::DMOMeshTetFactory::create(base + "_missing") != nullptr) return 7;
+        auto surf = DMO::DMOMeshTriFactory::create(*mesh);
+        if (!surf || surf->nVertices() != mesh->nVerticesSurf) return 8;
     } catch (const DMO::Error& e) {
         std::printf("error %d: %s\n", (int)e.status, e.what());
         return 4;

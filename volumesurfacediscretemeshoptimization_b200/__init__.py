@@ -395,6 +395,26 @@ class _DMOBase:
         check(_capi.lib().vsdmo_opt_estimate_surface_points(self.h, int(vid), int(nu), int(nv), _ptr(out), _capi.HOST))
         return out
 
+    def feature_state(self):
+        """(curves [nSurf x 12], fdeg [nSurf], flags [nSurf], (sector rowptr, table [nFeature x 20],
+        surfaces [n x 16]) or None) of an optimiser with feature vertices, internal numbering."""
+        nS, nF = self.mesh.info["nSurf"], self.mesh.info["nFeature"]
+        curves = np.zeros((nS, 12), np.float32)
+        fdeg = np.zeros(nS, np.int32)
+        flags = np.zeros(nS, np.uint8)
+        ns = C.c_int()
+        check(_capi.lib().vsdmo_opt_feature_state(self.h, _ptr(curves), _ptr(fdeg), _ptr(flags), None, None, None,
+                                                  C.byref(ns)))
+        sectors = None
+        if ns.value > 0:
+            rp = np.zeros(nF + 1, np.int32)
+            tab = np.zeros((nF, 20), np.int32)
+            fs = np.zeros((ns.value, 16), np.float32)
+            check(_capi.lib().vsdmo_opt_feature_state(self.h, None, None, None, _ptr(rp), _ptr(tab), _ptr(fs),
+                                                      C.byref(ns)))
+            sectors = (rp, tab, fs)
+        return curves, fdeg, flags, sectors
+
     def surface_state(self):
         """(xyz_init [nSurf,3], local_surfaces [nSurf,16], nearest [nSurf]) of a surface
         optimiser, internal vertex numbering."""
@@ -525,15 +545,23 @@ class DMOTriFlatClass(_DMOBase):
 
 
 class DMOTriClass(_DMOBase):
-    """``DMO::DMOTriClass`` (``dmo/DMOTri.h``): surface triangle DMO (meshes without feature
-    vertices)."""
+    """``DMO::DMOTriClass`` (``dmo/DMOTri.h``): surface triangle DMO; feature vertices slide
+    along their feature curves (``fix_boundary=True`` holds them)."""
     _flat = 0
+
+    def __init__(self, dmo_mesh, qualityCriterium=QualityCriterium.MEAN_RATIO, gridScale: float = 0.5,
+                 n_iter: int = 30, fix_boundary: bool = False, **kw):
+        super().__init__(dmo_mesh, qualityCriterium, gridScale, n_iter, fix_boundary, **kw)
 
 
 class DMOQuadClass(_DMOBase):
-    """``DMO::DMOQuadClass`` (``dmo/DMOQuad.h``): surface quad DMO (meshes without feature
-    vertices)."""
+    """``DMO::DMOQuadClass`` (``dmo/DMOQuad.h``): surface quad DMO; feature vertices slide
+    along their feature curves (``fix_boundary=True`` holds them)."""
     _flat = 0
+
+    def __init__(self, dmo_mesh, qualityCriterium=QualityCriterium.MEAN_RATIO, gridScale: float = 0.5,
+                 n_iter: int = 30, fix_boundary: bool = False, **kw):
+        super().__init__(dmo_mesh, qualityCriterium, gridScale, n_iter, fix_boundary, **kw)
 
 
 class DMOQuadFlatClass(_DMOBase):

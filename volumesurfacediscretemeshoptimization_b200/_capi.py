@@ -37,6 +37,7 @@ EXPORTED = [
     "vsdmo_batch_info", "vsdmo_batch_mesh_info",
     "vsdmo_file_read", "vsdmo_file_write", "vsdmo_mesh_create_from_file", "vsdmo_mesh_write_file",
     "vsdmo_mesh_create_surface", "vsdmo_opt_local_surface_points", "vsdmo_opt_estimate_surface_points",
+    "vsdmo_opt_feature_state",
 ]
 
 
@@ -181,6 +182,8 @@ def lib():
     L.vsdmo_mesh_write_file.argtypes = [P, C.c_char_p, I]
     L.vsdmo_mesh_create_surface.restype = S
     L.vsdmo_mesh_create_surface.argtypes = [P, U, P, C.POINTER(P)]
+    L.vsdmo_opt_feature_state.restype = S
+    L.vsdmo_opt_feature_state.argtypes = [P, P, P, P, P, P, P, C.POINTER(I)]
     L.vsdmo_opt_local_surface_points.restype = S
     L.vsdmo_opt_local_surface_points.argtypes = [P, I, I, I, P, I, I]
     L.vsdmo_opt_estimate_surface_points.restype = S

@@ -72,7 +72,11 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
     else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
     else if (o->mode == MODE_FLAT) launch_dmo_flat(m, L, o->p.grid_n, 32, s);
     else if (o->mode == MODE_ANGLE) launch_dmo_angle(m, L, o->p.quality == VSDMO_MAX_ANGLE, s);
-    else launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, s);
+    else {
+        SectorSurfaces sec{o->srow.p, o->stab.p, o->FS.p, o->Xs.p};
+        if (o->feat) VSDMO_CUDA(cudaMemcpyAsync(o->Xs.p, m.pos.p, sizeof(float4) * m.nSurf, cudaMemcpyDeviceToDevice, s));
+        launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, o->feat ? &sec : nullptr, s);
+    }
 }
 
 }  // namespace
@@ -97,10 +101,18 @@ void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
         o->model->m.infer_tet(m.pos.p, o->nb.p, o->nbn.p, o->nb_base, o->nb_base, m.nV - o->nb_base, o->Yall.p,
                               mlp::OUTP, s);
     for (int c = 0; c < (int)o->ranges.size(); ++c) launch_color(o, c, s);
-    if (o->mode == MODE_SURF) {
-        launch_update_nn(m, o->X0.p, o->nn.p, s);
-        update_normals(m, s);
+    if (o->pass1d) {
+        // feature vertices along their curves (flat meshes: only while the last minimum quality is
+        // positive, dmo/DMOTriFlat.cu:140)
+        const int mode = o->slide ? 0 : (m.fk == 3 ? 1 : 2);
+        for (const auto& r : o->franges) {
+            DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
+            launch_dmo_1d(m, mode, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p,
+                          o->slide ? o->stats.p : nullptr, o->slide ? o->d_iter.p : nullptr, s);
+        }
     }
+    if (o->mode == MODE_SURF || o->slide) launch_update_nn(m, o->X0.p, o->nn.p, s);
+    if (o->mode == MODE_SURF) update_normals(m, s);
     launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p,
                          o->p.check_monotone ? 1 : 0, s);
 }
@@ -114,18 +126,34 @@ __global__ void k_surface_state(const float4* pos, int nS, float4* X0, int* nn) 
 
 // initial positions, normals, local surfaces and nn = identity from the current positions
 // (the constructor of DMOTriClass / DMOQuadClass, dmo/DMOTri.cu:80-126)
+// With feature vertices also their curves and 1D flags (computeLocalSurfaces1d,
+// calcOptFeatureVec) and, on surfaces, the per-sector surfaces (initLocalSurfacesFeature).
 void init_surface_state(vsdmo_opt_s* o) {
     const Mesh& m = o->mesh->m;
     cudaStream_t s = m.stream;
     if (!o->X0.p) {
         o->X0.alloc(m.nSurf, s);
-        o->LS.alloc(4L * m.nSurf, s);
         o->nn.alloc(m.nSurf, s);
+        if (o->mode == MODE_SURF) o->LS.alloc(4L * m.nSurf, s);
     }
     k_surface_state<<<grid_for(m.nSurf, 256), 256, 0, s>>>(m.pos.p, m.nSurf, o->X0.p, o->nn.p);
     VSDMO_CHECK_LAUNCH();
-    update_normals(m, s);
-    launch_surface_fit(m, o->X0.p, o->LS.p, s);
+    if (o->mode == MODE_SURF) {
+        update_normals(m, s);
+        launch_surface_fit(m, o->X0.p, o->LS.p, s);
+    }
+    if (o->feat) {
+        if (!o->LS1.p) {
+            o->LS1.alloc(3L * m.nSurf, s);
+            o->fdeg.alloc(m.nSurf, s);
+            o->fopt.alloc(m.nSurf, s);
+        }
+        init_feature_state(m, o->slide ? 1 : 0, o->LS1.p, o->fdeg.p, o->fopt.p, s);
+        if (o->mode == MODE_SURF) {
+            o->nsect = build_sectors(m, o->srow, o->stab, o->FS, s);
+            if (!o->Xs.p) o->Xs.alloc(m.nSurf, s);
+        }
+    }
 }
 
 void ensure_capacity(vsdmo_opt_s* o, int need) {
@@ -499,11 +527,16 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->kind = MK_HEX;
         for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
     } else if (m.type == VSDMO_TRI && flat2d && p.grid_n == 8) {
-        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "sliding boundary vertices are not implemented yet; set fix_boundary=1");
-        if (m.maxHE > dmo_tri2d_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
+        if (m.maxHE > dmo_tri2d_max_ring() || (!p.fix_boundary && m.maxHE > dmo_surf_max_ring()))
+            return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
         o->mode = MODE_TRI2D;
         o->kind = MK_TRI2D;
         for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+        if (!p.fix_boundary && m.nFeature > 0) {
+            // boundary vertices slide along their boundary curves (DMOTriFlatClass::doIteration)
+            o->slide = o->feat = o->pass1d = true;
+            for (int c = 0; c < m.nColFeature; ++c) o->franges.push_back({m.col_feature[c], m.col_feature[c + 1]});
+        }
     } else if (flat2d) {
         // flat quads (any grid) and flat triangles with a 4-point grid: the general 2D search
         if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "sliding boundary vertices are not implemented yet; set fix_boundary=1");
@@ -512,13 +545,17 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->kind = m.type == VSDMO_QUAD ? MK_QUAD2D : MK_TRI2D;
         for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
     } else if (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) {
-        if (m.nFeature > 0)
-            return fail(VSDMO_E_UNSUPPORTED, "surface meshes with feature or boundary vertices need the feature passes, "
-                                             "which are not implemented yet");
         if (m.maxHE > dmo_surf_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
         o->mode = MODE_SURF;
         o->kind = m.type == VSDMO_QUAD ? MK_QUAD : MK_TRI3D;
         for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+        if (m.nFeature > 0) {
+            // feature neighbours project onto their sector surfaces; the feature vertices themselves
+            // slide along their feature curves unless fix_boundary holds them
+            o->feat = true;
+            o->pass1d = !p.fix_boundary;
+            for (int c = 0; c < m.nColFeature; ++c) o->franges.push_back({m.col_feature[c], m.col_feature[c + 1]});
+        }
     } else {
         return fail(VSDMO_E_UNSUPPORTED, "element type not supported");
     }
@@ -531,7 +568,7 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->done.alloc(1, s); o->done.zero();
         prepare_dmo_kernels();
         if (o->mode == MODE_ANGLE) prepare_angle_kernels();
-        if (o->mode == MODE_SURF) init_surface_state(o.get());
+        if (o->mode == MODE_SURF || o->slide) init_surface_state(o.get());
         o->counters.alloc(4, s);
         o->counters.zero();
         if (o->mode == MODE_TET && p.active_set) {
@@ -588,7 +625,7 @@ VSDMO_API vsdmo_status vsdmo_opt_restart(vsdmo_opt_t o) {
         const Mesh& m = o->mesh->m;
         o->iters_done = 0;
         o->d_iter.zero();
-        if (o->mode == MODE_SURF) init_surface_state(o);
+        if (o->mode == MODE_SURF || o->slide) init_surface_state(o);
         o->counters.zero();
         if (o->dirty.p) o->dirty.fill_bytes(1);
         launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1,
@@ -612,13 +649,36 @@ VSDMO_API int vsdmo_opt_iterations_done(vsdmo_opt_t o) { return o ? o->iters_don
 VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t o) {
     if (!o) return -1;
     // colour launches + quality kernel (+ nearest-neighbour walk and two normal kernels)
-    return (int)o->ranges.size() + 1 + (o->mode == MODE_SURF ? 3 : 0);
+    return (int)o->ranges.size() + 1 + (o->mode == MODE_SURF ? 3 : 0) + (o->slide ? 1 : 0) +
+           (o->pass1d ? (int)o->franges.size() : 0);
+}
+
+VSDMO_API vsdmo_status vsdmo_opt_feature_state(vsdmo_opt_t o, float* curves, int32_t* fdeg, uint8_t* flags,
+                                               int32_t* sector_rowptr, int32_t* sector_table, float* sector_surfaces,
+                                               int* n_sectors) {
+    if (!o) return fail(VSDMO_E_ARG, "null optimiser");
+    if (!o->feat) return fail(VSDMO_E_ARG, "the optimiser has no feature vertices");
+    return guarded([&] {
+        const Mesh& m = o->mesh->m;
+        cudaStream_t s = m.stream;
+        if (n_sectors) *n_sectors = o->nsect;
+        if (curves) VSDMO_CUDA(cudaMemcpyAsync(curves, o->LS1.p, sizeof(float4) * 3L * m.nSurf, cudaMemcpyDeviceToHost, s));
+        if (fdeg) VSDMO_CUDA(cudaMemcpyAsync(fdeg, o->fdeg.p, sizeof(int) * m.nSurf, cudaMemcpyDeviceToHost, s));
+        if (flags) VSDMO_CUDA(cudaMemcpyAsync(flags, o->fopt.p, m.nSurf, cudaMemcpyDeviceToHost, s));
+        if (o->nsect > 0) {
+            if (sector_rowptr) VSDMO_CUDA(cudaMemcpyAsync(sector_rowptr, o->srow.p, sizeof(int) * (m.nFeature + 1), cudaMemcpyDeviceToHost, s));
+            if (sector_table) VSDMO_CUDA(cudaMemcpyAsync(sector_table, o->stab.p, sizeof(int) * 20L * m.nFeature, cudaMemcpyDeviceToHost, s));
+            if (sector_surfaces) VSDMO_CUDA(cudaMemcpyAsync(sector_surfaces, o->FS.p, sizeof(float4) * 4L * o->nsect, cudaMemcpyDeviceToHost, s));
+        }
+        m.sync();
+    });
 }
 
 VSDMO_API vsdmo_status vsdmo_opt_surface_state(vsdmo_opt_t o, float* xyz_init, float* local_surfaces,
                                                int32_t* nearest) {
     if (!o) return fail(VSDMO_E_ARG, "null optimiser");
-    if (o->mode != MODE_SURF) return fail(VSDMO_E_ARG, "not a surface optimiser");
+    if (o->mode != MODE_SURF && !o->slide) return fail(VSDMO_E_ARG, "not a surface optimiser");
+    if (local_surfaces && !o->LS.p) return fail(VSDMO_E_ARG, "this optimiser has no local surfaces");
     return guarded([&] {
         const Mesh& m = o->mesh->m;
         cudaStream_t s = m.stream;

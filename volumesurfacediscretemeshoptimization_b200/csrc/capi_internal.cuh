@@ -24,6 +24,17 @@ struct vsdmo_opt_s {
     int mode = MODE_TET;
     int kind = MK_TET;                         // element metric of the quality kernels
     std::vector<std::pair<int, int>> ranges;  // colour classes in launch order
+    // feature / boundary pass: slide = flat triangles with sliding boundary vertices; feat = the
+    // mesh has feature vertices (surface: sector surfaces always, the 1D pass unless fix_boundary)
+    bool slide = false, feat = false, pass1d = false;
+    DBuf<float4> LS1;                          // curves of the feature vertices [3 nSurf]
+    DBuf<int> fdeg;                            // feature ring vertices [nSurf]
+    DBuf<uint8_t> fopt;                        // the 1D pass moves the vertex [nSurf]
+    DBuf<int> srow, stab;                      // sector rows [nFeature + 1], table [nFeature x 20]
+    DBuf<float4> FS;                           // sector surfaces [4 per sector]
+    DBuf<float4> Xs;                           // positions at the start of a colour class [nSurf]
+    int nsect = 0;
+    std::vector<std::pair<int, int>> franges;  // feature colour classes
     DBuf<float4> X0;                           // surface mode: initial surface positions [nSurf]
     DBuf<float4> LS;                           // local surfaces [4 nSurf]
     DBuf<int> nn;                              // nearest initial vertex [nSurf]

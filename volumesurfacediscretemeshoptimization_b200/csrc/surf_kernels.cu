@@ -43,6 +43,8 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int SURF_WARPS = 4;
 constexpr int SURF_MAX_RING = 64;
 constexpr float SURF_EPS = 1.19209e-07f;   // EPSILON of the reference's surface code
+constexpr int SECT_TABLE = 20;              // TABLE_SIZE of dmo/surfaceP/SurfaceCommon.h: halfedges of a feature vertex
+constexpr int SECT_LIST = 40;               // MAX_NEIGHBORS: points of one sector
 
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
     return (ax * bx + ay * by) + az * bz;
@@ -267,7 +269,9 @@ template <int FK>
 __global__ void __launch_bounds__(SURF_WARPS * 32)
 k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
            const float4* __restrict__ X0, const float4* __restrict__ LS, const int* __restrict__ nn,
-           const float* __restrict__ vn, int v0, int v1, float grid_scale, int depth, int maxk) {
+           const float* __restrict__ vn, int v0, int v1, float grid_scale, int depth, int maxk,
+           const int* __restrict__ srow, const int* __restrict__ stab, const float4* __restrict__ FS,
+           const float4* __restrict__ Xs, int nFree) {
     extern __shared__ float4 smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int v = v0 + blockIdx.x * SURF_WARPS + warp;
@@ -294,10 +298,25 @@ k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4*
             md = fmaxf(md, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
         }
         const int nnN = nn[h.x];
-        nbL[4 * i] = LS[4L * nnN];
-        nbL[4 * i + 1] = LS[4L * nnN + 1];
-        nbL[4 * i + 2] = LS[4L * nnN + 2];
-        nbL[4 * i + 3] = LS[4L * nnN + 3];
+        const float4* Ls = LS + 4L * nnN;
+        if (FS && nnN >= nFree) {
+            // a feature neighbour projects onto the sector surface of its halfedge whose target is
+            // nearest to this vertex (positions at the start of the colour class)
+            const float4 pv = Xs[v];
+            float best = FLT_MAX;
+            int arg = 0;
+            for (int j = rowptr[nnN], idx = 0; j < rowptr[nnN + 1]; ++j, ++idx) {
+                const float4 t = Xs[he[j].x];
+                const float ex = t.x - pv.x, ey = t.y - pv.y, ez = t.z - pv.z;
+                const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+                if (d2 < best) { best = d2; arg = idx; }
+            }
+            Ls = FS + 4L * (srow[nnN - nFree] + stab[SECT_TABLE * (nnN - nFree) + arg]);
+        }
+        nbL[4 * i] = Ls[0];
+        nbL[4 * i + 1] = Ls[1];
+        nbL[4 * i + 2] = Ls[2];
+        nbL[4 * i + 3] = Ls[3];
         nbX[i] = X0[nnN];
     }
 #pragma unroll
@@ -348,6 +367,328 @@ k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4*
         lastMax = bv;
         ds = ds * (2.0f / 7.0f);
     }
+    if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
+}
+
+// ---- feature vertices ---------------------------------------------------------------------------
+// fdeg[v]: feature vertices in the ring of surface vertex v; opt[v]: the 1D pass moves feature
+// vertex v (two feature ring vertices at >= 160 degrees; k_calcOptFeatureVec, dmo/DMOCommon.h:130-180)
+__global__ void k_feature_flags(int nS, int nFree, const int* __restrict__ rowptr, const int4* __restrict__ he,
+                                const float4* __restrict__ pos, int* __restrict__ fdeg, uint8_t* __restrict__ opt) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nS; v += gridDim.x * blockDim.x) {
+        int cnt = 0, a = -1, b = -1;
+        for (int i = rowptr[v]; i < rowptr[v + 1]; ++i) {
+            const int d = he[i].x;
+            if (d >= nFree) {
+                if (cnt == 0) a = d; else if (cnt == 1) b = d;
+                ++cnt;
+            }
+        }
+        fdeg[v] = cnt;
+        uint8_t o = 0;
+        if (v >= nFree && cnt == 2) {
+            const float4 p0 = pos[v], pa = pos[a], pb = pos[b];
+            const float ux = pa.x - p0.x, uy = pa.y - p0.y, uz = pa.z - p0.z;
+            const float wx = pb.x - p0.x, wy = pb.y - p0.y, wz = pb.z - p0.z;
+            const float dt = dot3(ux, uy, uz, wx, wy, wz);
+            const float len = sqrtf(dot3(ux, uy, uz, ux, uy, uz) * dot3(wx, wy, wz, wx, wy, wz));
+            const double ang = 180.0 / 3.14159265358979323846 * (double)acosf(dt / len);
+            o = ang >= 160.0 ? 1 : 0;
+        }
+        opt[v] = o;
+    }
+}
+
+// computeLocalSurface1d (dmo/Surface1D.cu:8-82): curve v = a u^2 in the frame (t2, n), t2 = n x (n x r)
+// with r towards the last feature ring vertex; LS1[3v] = (p0, a), (t2, 0), (n, 0)
+__global__ void k_surface_fit_1d(int nS, int nFree, int flat, const int* __restrict__ rowptr,
+                                 const int4* __restrict__ he, const float4* __restrict__ pos,
+                                 const float* __restrict__ vn, float4* __restrict__ LS1) {
+    for (int v = nFree + blockIdx.x * blockDim.x + threadIdx.x; v < nS; v += gridDim.x * blockDim.x) {
+        int last = -1;
+        for (int i = rowptr[v]; i < rowptr[v + 1]; ++i) if (he[i].x >= nFree) last = he[i].x;
+        if (last < 0) {
+            LS1[3L * v] = make_float4(0.f, 0.f, 0.f, 0.f);
+            LS1[3L * v + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            LS1[3L * v + 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const float4 c = pos[v];
+        float n[3] = { 0.f, 0.f, 1.f };
+        if (!flat) { n[0] = vn[3L * v]; n[1] = vn[3L * v + 1]; n[2] = vn[3L * v + 2]; }
+        const float4 q = pos[last];
+        float r[3] = { q.x - c.x, q.y - c.y, q.z - c.z };
+        const float cr[3] = { n[1] * r[2] - n[2] * r[1], n[2] * r[0] - n[0] * r[2], n[0] * r[1] - n[1] * r[0] };
+        if (sqrtf(dot3(cr[0], cr[1], cr[2], cr[0], cr[1], cr[2])) < 10.f * SURF_EPS) { r[0] = n[0]; r[1] = n[2]; r[2] = -n[1]; }
+        float t1[3] = { n[1] * r[2] - n[2] * r[1], n[2] * r[0] - n[0] * r[2], n[0] * r[1] - n[1] * r[0] };
+        float t2[3] = { n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0] };
+        const float ln = sqrtf(dot3(n[0], n[1], n[2], n[0], n[1], n[2]));
+        const float l1 = sqrtf(dot3(t1[0], t1[1], t1[2], t1[0], t1[1], t1[2]));
+        const float l2 = sqrtf(dot3(t2[0], t2[1], t2[2], t2[0], t2[1], t2[2]));
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { n[a] = n[a] / ln; t1[a] = t1[a] / l1; t2[a] = t2[a] / l2; }
+        float ATA = 0.f, ATb = 0.f;
+        for (int i = rowptr[v]; i < rowptr[v + 1]; ++i) {
+            const int d = he[i].x;
+            if (d < nFree) continue;
+            const float4 pp = pos[d];
+            const float px = pp.x - c.x, py = pp.y - c.y, pz = pp.z - c.z;
+            const float u = dot3(t2[0], t2[1], t2[2], px, py, pz), w = dot3(n[0], n[1], n[2], px, py, pz);
+            ATb += (u * u) * w;
+            ATA += ((u * u) * u) * u;
+        }
+        LS1[3L * v] = make_float4(c.x, c.y, c.z, ATb / ATA);
+        LS1[3L * v + 1] = make_float4(t2[0], t2[1], t2[2], 0.f);
+        LS1[3L * v + 2] = make_float4(n[0], n[1], n[2], 0.f);
+    }
+}
+
+// sectors of a feature vertex (SurfaceFeature.cu:12-85): split of its fan at the feature ring
+// vertices; count per feature vertex (plus one closing sector when it is not on a boundary)
+__global__ void k_sector_count(int nFeat, int nFree, const int* __restrict__ rowptr, const int4* __restrict__ he,
+                               const uint8_t* __restrict__ isB1, int* __restrict__ cnt, int* __restrict__ err) {
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nFeat; idx += gridDim.x * blockDim.x) {
+        const int vid = nFree + idx, b = rowptr[vid], e = rowptr[vid + 1];
+        if (e - b > SECT_TABLE) { atomicExch(err, 1); cnt[idx] = 0; continue; }
+        int sid = 0;
+        for (int i = b + 1; i < e; ++i) if (he[i].x >= nFree) ++sid;
+        if (!isB1[vid]) ++sid;
+        cnt[idx] = sid;
+    }
+}
+
+// one sector's quadric (computeLocalSurfacesFeature1/2, SurfaceFeature.cu:134-221): the frame of
+// the face of the sector's first edge, least squares over the sector's points (+ the midpoint of
+// points 2 and 3 when it has 5)
+__device__ void sector_fit(const int* L, int np, const int* __restrict__ rowptr, const int4* __restrict__ he,
+                           const float4* __restrict__ pos, const float* __restrict__ fn, float4* out) {
+    const int vid = L[0];
+    const float4 c = pos[vid];
+    float P[SECT_LIST + 1][3];
+    for (int i = 0; i < np; ++i) { const float4 q = pos[L[i]]; P[i][0] = q.x; P[i][1] = q.y; P[i][2] = q.z; }
+    if (np == 5) {
+        for (int a = 0; a < 3; ++a) P[5][a] = 0.5f * (P[2][a] + P[3][a]);
+        np = 6;
+    }
+    int f = -1;
+    for (int i = rowptr[vid]; i < rowptr[vid + 1]; ++i) if (he[i].x == L[1]) f = he[i].z;
+    float n[3] = { fn[3L * f], fn[3L * f + 1], fn[3L * f + 2] };
+    const float4 q0 = pos[L[1]];
+    float rv[3] = { q0.x - c.x, q0.y - c.y, q0.z - c.z };
+    const float cr[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+    if (sqrtf(dot3(cr[0], cr[1], cr[2], cr[0], cr[1], cr[2])) < 10.f * SURF_EPS) { rv[0] = n[0]; rv[1] = n[2]; rv[2] = -n[1]; }
+    float t1[3] = { n[1] * rv[2] - n[2] * rv[1], n[2] * rv[0] - n[0] * rv[2], n[0] * rv[1] - n[1] * rv[0] };
+    float t2[3] = { n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0] };
+    const float ln = sqrtf(dot3(n[0], n[1], n[2], n[0], n[1], n[2]));
+    const float l1 = sqrtf(dot3(t1[0], t1[1], t1[2], t1[0], t1[1], t1[2]));
+    const float l2 = sqrtf(dot3(t2[0], t2[1], t2[2], t2[0], t2[1], t2[2]));
+    for (int a = 0; a < 3; ++a) { n[a] = n[a] / ln; t1[a] = t1[a] / l1; t2[a] = t2[a] / l2; }
+    float M00 = 0.f, M01 = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, r0 = 0.f, r1 = 0.f, r2 = 0.f;
+    for (int i = 0; i < np; ++i) {
+        const float px = P[i][0] - c.x, py = P[i][1] - c.y, pz = P[i][2] - c.z;
+        const float u = dot3(t1[0], t1[1], t1[2], px, py, pz);
+        const float vv = dot3(t2[0], t2[1], t2[2], px, py, pz);
+        const float w = dot3(n[0], n[1], n[2], px, py, pz);
+        const float uu = u * u, uv = u * vv, v2 = vv * vv;
+        r0 = r0 + uu * w; r1 = r1 + uv * w; r2 = r2 + v2 * w;
+        M00 = M00 + uu * uu; M01 = M01 + uu * uv; M11 = M11 + uu * v2; M12 = M12 + uv * v2; M22 = M22 + v2 * v2;
+    }
+    float A[3][3] = { { M00, M01, M11 }, { M01, M11, M12 }, { M11, M12, M22 } };
+    float sv[3] = { r0, r1, r2 };
+    solve3(A, sv);
+    if (np <= 4) { sv[0] = 0.f; sv[1] = 0.f; sv[2] = 0.f; }
+    for (int a = 0; a < 3; ++a) if (sv[a] != sv[a]) sv[a] = 0.f;
+    out[0] = make_float4(c.x, c.y, c.z, sv[0]);
+    out[1] = make_float4(t1[0], t1[1], t1[2], sv[1]);
+    out[2] = make_float4(t2[0], t2[1], t2[2], sv[2]);
+    out[3] = make_float4(n[0], n[1], n[2], (float)np);
+}
+
+// sector table [nFeat x 20] (sector of every halfedge of a feature vertex, -1 unused) and the
+// sector surfaces FS [4 per sector], one thread per feature vertex
+__global__ void k_sector_fit(int nFeat, int nFree, const int* __restrict__ rowptr, const int4* __restrict__ he,
+                             const uint8_t* __restrict__ isB1, const float4* __restrict__ pos, const float* __restrict__ fn,
+                             const int* __restrict__ srow, int* __restrict__ stab, float4* __restrict__ FS,
+                             int* __restrict__ err) {
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nFeat; idx += gridDim.x * blockDim.x) {
+        const int vid = nFree + idx, b = rowptr[vid], e = rowptr[vid + 1];
+        int* T = stab + (size_t)SECT_TABLE * idx;
+        for (int i = 0; i < SECT_TABLE; ++i) T[i] = -1;
+        if (e - b > SECT_TABLE) continue;
+        T[0] = 0;
+        int L[SECT_LIST + 1];
+        int sid = 0, nn = 0, lastHE = b, vindex = 1;
+        bool last = true;
+        for (int i = b + 1; i < e; ++i) {
+            const int vdst = he[i].x;
+            if (last) { nn = 0; L[nn++] = vid; L[nn++] = he[lastHE].x; }
+            if (vdst >= nFree) {
+                T[vindex] = sid;
+                L[nn++] = vdst;
+                sector_fit(L, nn, rowptr, he, pos, fn, FS + 4L * (srow[idx] + sid));
+                ++sid;
+                nn = 0;
+                last = true;
+            } else {
+                if (nn >= SECT_LIST) { atomicExch(err, 1); break; }
+                T[vindex] = sid;
+                L[nn++] = vdst;
+                last = false;
+            }
+            ++lastHE;
+            ++vindex;
+        }
+        if (!isB1[vid]) {
+            if (last) { nn = 0; L[nn++] = vid; L[nn++] = he[lastHE].x; }
+            L[nn++] = he[b].x;
+            sector_fit(L, nn, rowptr, he, pos, fn, FS + 4L * (srow[idx] + sid));
+        }
+    }
+}
+
+// 2D mean ratio of (p, a, b) (meanRatioMetricTri2D, dmo/DMOQualityTri.h:243-257)
+__device__ __forceinline__ float q2d(float px, float py, float4 a, float4 b) {
+    const float e0x = a.x - px, e0y = a.y - py, e1x = b.x - a.x, e1y = b.y - a.y, e2x = px - b.x, e2y = py - b.y;
+    const float l = ((e0x * e0x + e0y * e0y) + (e1x * e1x + e1y * e1y)) + (e2x * e2x + e2y * e2y);
+    const float area = e0x * e1y - e0y * e1x;
+    if (area < 0.f) return area;
+    return ((2.f * sqrtf(3.f)) * area) / l;
+}
+
+// MODE 0: flat (2D mean ratio), 1: surface triangles, 2: surface quads
+template <int MODE, bool SIGNED>
+__device__ __forceinline__ float ring_q1d(const float4* ring, int ne, float px, float py, float pz, float3 n) {
+    if (MODE == 0) {
+        float q = FLT_MAX;
+        for (int i = 0; i < ne; ++i) q = fminf(q, q2d(px, py, ring[i], ring[i + 1]));
+        return q;
+    }
+    if (MODE == 1) return ring_key_tri<SIGNED>(ring, ne, px, py, pz, n);
+    return ring_key_quad<SIGNED>(ring, ne, px, py, pz, n);
+}
+
+// localSurfaceEstimation1d (dmo/Surface1D.h:52-93)
+__device__ __forceinline__ float3 est1d(const float4* __restrict__ LS1, const float4* __restrict__ X0,
+                                        const int* __restrict__ nn, int nnv, const int* surf, int ns, float u) {
+    const float4 l0 = LS1[3L * nnv], l1 = LS1[3L * nnv + 1], l2 = LS1[3L * nnv + 2];
+    const float w = (l0.w * u) * u;
+    const float pwx = (l0.x + u * l1.x) + w * l2.x;
+    const float pwy = (l0.y + u * l1.y) + w * l2.y;
+    const float pwz = (l0.z + u * l1.z) + w * l2.z;
+    const float4 x0 = X0[nnv];
+    const float dx = x0.x - pwx, dy = x0.y - pwy, dz = x0.z - pwz;
+    const float id = 1.0f / (dot3(dx, dy, dz, dx, dy, dz) + SURF_EPS);
+    float isum = id;
+    float ax = pwx * id, ay = pwy * id, az = pwz * id;
+    for (int i = 0; i < ns; ++i) {
+        const int nnN = nn[surf[i]];
+        const float4 xn = X0[nnN];
+        const float ex = xn.x - pwx, ey = xn.y - pwy, ez = xn.z - pwz;
+        const float idn = 1.0f / (dot3(ex, ey, ez, ex, ey, ez) + SURF_EPS);
+        isum = isum + idn;
+        const float4 m0 = LS1[3L * nnN], m1 = LS1[3L * nnN + 1], m2 = LS1[3L * nnN + 2];
+        const float qx = pwx - m0.x, qy = pwy - m0.y, qz = pwz - m0.z;
+        const float lu = dot3(qx, qy, qz, m1.x, m1.y, m1.z);
+        const float lw = (m0.w * lu) * lu;
+        ax = ax + ((m0.x + lu * m1.x) + lw * m2.x) * idn;
+        ay = ay + ((m0.y + lu * m1.y) + lw * m2.y) * idn;
+        az = az + ((m0.z + lu * m1.z) + lw * m2.z) * idn;
+    }
+    const float inv = 1.0f / isum;
+    return make_float3(ax * inv, ay * inv, az * inv);
+}
+
+// The 1D pass over one colour class of feature vertices (k_optimizeHierarchical1DFlat,
+// dmo/DMOTriFlatImplCub.h:159-330; k_optimizeHierarchical1D, dmo/DMOTriImplCub.h:205-380,
+// dmo/DMOQuadImplCub.h:219-400): lanes 0-7 take the 8 candidates along u of the vertex's curve,
+// the first maximum in lane order wins, moves on strict improvement, written when the last
+// level's best beats the current position (surfaces: its unsigned ring quality). gate: the
+// flat pass runs only while the last minimum quality (stats[*iter]) is positive.
+template <int MODE>
+__global__ void __launch_bounds__(SURF_WARPS * 32)
+k_dmo_1d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
+         const uint8_t* __restrict__ isB1, const float4* __restrict__ X0, const float4* __restrict__ LS1,
+         const int* __restrict__ nn, const float* __restrict__ vn, const int* __restrict__ fdeg,
+         const uint8_t* __restrict__ opt, int nFree, int v0, int v1, float grid_scale, int maxk,
+         const IterStats* __restrict__ stats, const int* __restrict__ iter) {
+    extern __shared__ float4 s1d[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int v = v0 + blockIdx.x * SURF_WARPS + warp;
+    if (v >= v1 || !opt[v]) return;
+    if (stats && !(stats[*iter].min_q > 0.f)) return;
+    const int b = rowptr[v], k = rowptr[v + 1] - b;
+    if (k <= 0 || k > maxk) return;
+    float4* ring = s1d + (size_t)warp * (2 * maxk + 1 + (maxk + 3) / 4);
+    int* surf = reinterpret_cast<int*>(ring + 2 * maxk + 1);
+    const float4 c0 = pos[v];
+    float md = -FLT_MAX;
+    int ns = 0;
+    for (int base = 0; base < k; base += 32) {
+        const int i = base + lane;
+        bool flag = false;
+        if (i < k) {
+            const int4 h = he[b + i];
+            const float4 t = pos[h.x];
+            float dx = fabsf(c0.x - t.x), dy = fabsf(c0.y - t.y), dz = fabsf(c0.z - t.z);
+            md = fmaxf(md, sqrtf((dx * dx + dy * dy) + dz * dz));
+            if (MODE == 2) {
+                const float4 t2 = pos[he[h.w].x];
+                ring[2 * i] = t;
+                ring[2 * i + 1] = t2;
+                dx = fabsf(c0.x - t2.x); dy = fabsf(c0.y - t2.y); dz = fabsf(c0.z - t2.z);
+                md = fmaxf(md, sqrtf((dx * dx + dy * dy) + dz * dz));
+            } else {
+                ring[i] = t;
+            }
+            flag = h.x >= nFree && fdeg[h.x] == 2;
+        }
+        const unsigned bal = __ballot_sync(FULL, flag);
+        if (flag) surf[ns + __popc(bal & ((1u << lane) - 1u))] = he[b + i].x;
+        ns += __popc(bal);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) md = fmaxf(md, __shfl_xor_sync(FULL, md, o));
+    const bool closed = !isB1[v];
+    const int ne = closed ? k : k - 1;
+    __syncwarp();
+    if (lane == 0 && closed) ring[MODE == 2 ? 2 * k : k] = ring[0];
+    __syncwarp();
+    const int nnv = nn[v];
+    const float4 l0 = LS1[3L * nnv], l1 = LS1[3L * nnv + 1];
+    float cu;
+    {
+        const float qx = c0.x - l0.x, qy = c0.y - l0.y, qz = c0.z - l0.z;
+        cu = dot3(qx, qy, qz, l1.x, l1.y, l1.z);
+    }
+    float3 n = make_float3(0.f, 0.f, 0.f);
+    if (MODE != 0) n = make_float3(vn[3L * nnv], vn[3L * nnv + 1], vn[3L * nnv + 2]);
+    float cx = c0.x, cy = c0.y, cz = c0.z;
+    const float aff = 1.f / 7.f;
+    float ds = grid_scale, lastMax = -FLT_MAX;
+    for (int d = 0; d < 3; ++d) {
+        const float uMax = ds * md, uMin = -ds * md;
+        const int i = lane & 7;
+        const float u = cu + aff * ((float)i * uMin + (float)(7 - i) * uMax);
+        float3 p = make_float3(0.f, 0.f, 0.f);
+        float q = -FLT_MAX;
+        if (lane < 8) {
+            p = est1d(LS1, X0, nn, nnv, surf, ns, u);
+            q = ring_q1d<MODE, true>(ring, ne, p.x, p.y, p.z, n);
+        }
+        float bv = __shfl_sync(FULL, q, 0);
+        int bt = 0;
+        for (int t = 1; t < 8; ++t) {
+            const float qt = __shfl_sync(FULL, q, t);
+            if (qt > bv) { bv = qt; bt = t; }
+        }
+        const float qLast = ring_q1d<MODE, true>(ring, ne, cx, cy, cz, n);
+        const float bu = __shfl_sync(FULL, u, bt);
+        const float bx = __shfl_sync(FULL, p.x, bt), by = __shfl_sync(FULL, p.y, bt), bz = __shfl_sync(FULL, p.z, bt);
+        if (qLast < bv) { cx = bx; cy = by; cz = bz; cu = bu; }
+        lastMax = bv;
+        ds = ds * (2.f / 7.f);
+    }
+    const float qOld = ring_q1d<MODE, false>(ring, ne, c0.x, c0.y, c0.z, n);
     if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
 }
 
@@ -438,7 +779,7 @@ void launch_update_nn(const Mesh& m, const float4* X0, int* nn, cudaStream_t s) 
 }
 
 void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
-                     cudaStream_t s) {
+                     const SectorSurfaces* sec, cudaStream_t s) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
     const int maxk = m.maxHE;
@@ -446,10 +787,66 @@ void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const 
     const int blocks = (n + SURF_WARPS - 1) / SURF_WARPS;
     if (m.fk == 4)
         k_dmo_surf<4><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0,
-                                                            L.v1, L.grid_scale, L.depth, maxk);
+                                                            L.v1, L.grid_scale, L.depth, maxk, sec ? sec->srow : nullptr,
+                                                            sec ? sec->stab : nullptr, sec ? sec->FS : nullptr,
+                                                            sec ? sec->Xs : nullptr, m.nSurf - m.nFeature);
     else
         k_dmo_surf<3><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0,
-                                                            L.v1, L.grid_scale, L.depth, maxk);
+                                                            L.v1, L.grid_scale, L.depth, maxk, sec ? sec->srow : nullptr,
+                                                            sec ? sec->stab : nullptr, sec ? sec->FS : nullptr,
+                                                            sec ? sec->Xs : nullptr, m.nSurf - m.nFeature);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void init_feature_state(const Mesh& m, int flat, float4* LS1, int* fdeg, uint8_t* opt, cudaStream_t s) {
+    const int nFree = m.nSurf - m.nFeature;
+    k_feature_flags<<<grid_for(m.nSurf, 256), 256, 0, s>>>(m.nSurf, nFree, m.he_rowptr.p, m.he.p, m.pos.p, fdeg, opt);
+    VSDMO_CHECK_LAUNCH();
+    VSDMO_CUDA(cudaMemsetAsync(LS1, 0, sizeof(float4) * 3 * (size_t)m.nSurf, s));
+    if (m.nFeature > 0) {
+        k_surface_fit_1d<<<grid_for(m.nFeature, 128), 128, 0, s>>>(m.nSurf, nFree, flat, m.he_rowptr.p, m.he.p, m.pos.p,
+                                                                   m.vn.p, LS1);
+        VSDMO_CHECK_LAUNCH();
+    }
+}
+
+int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>& FS, cudaStream_t s) {
+    const int nFeat = m.nFeature, nFree = m.nSurf - m.nFeature;
+    if (nFeat <= 0) return 0;
+    DBuf<int> cnt(nFeat, s), err(1, s);
+    err.zero();
+    srow.alloc(nFeat + 1, s);
+    k_sector_count<<<grid_for(nFeat, 128), 128, 0, s>>>(nFeat, nFree, m.he_rowptr.p, m.he.p, m.isB1.p, cnt.p, err.p);
+    VSDMO_CHECK_LAUNCH();
+    exclusive_scan(cnt.p, srow.p, nFeat, srow.p + nFeat, s);
+    const int nSect = read_scalar(srow.p + nFeat, s);
+    stab.alloc((size_t)SECT_TABLE * nFeat, s);
+    FS.alloc(4 * (size_t)std::max(nSect, 1), s);
+    k_sector_fit<<<grid_for(nFeat, 64), 64, 0, s>>>(nFeat, nFree, m.he_rowptr.p, m.he.p, m.isB1.p, m.pos.p, m.fn.p,
+                                                   srow.p, stab.p, FS.p, err.p);
+    VSDMO_CHECK_LAUNCH();
+    if (read_scalar(err.p, s))
+        throw Error(VSDMO_E_VALENCE, "a feature vertex has more than 20 halfedges or a sector more than 40 points");
+    return nSect;
+}
+
+void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
+                   const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
+                   cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxk = std::max(m.maxHE, 1);
+    const size_t smem = (size_t)SURF_WARPS * (2 * maxk + 1 + (maxk + 3) / 4) * sizeof(float4);
+    const int blocks = (n + SURF_WARPS - 1) / SURF_WARPS;
+    const int nFree = m.nSurf - m.nFeature;
+#define VSDMO_1D(MODE)                                                                                              \
+    k_dmo_1d<MODE><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, m.isB1.p, X0, LS1, nn, m.vn.p, \
+                                                         fdeg, opt, nFree, L.v0, L.v1, L.grid_scale, maxk, gate_stats, \
+                                                         gate_iter)
+    if (mode == 0) VSDMO_1D(0);
+    else if (mode == 1) VSDMO_1D(1);
+    else VSDMO_1D(2);
+#undef VSDMO_1D
     VSDMO_CHECK_LAUNCH();
 }
 

@@ -175,9 +175,29 @@ void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, i
 void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, cudaStream_t s);
 // nn [nSurf]: nearest initial vertex of every surface vertex, walked from its previous value.
 void launch_update_nn(const Mesh& m, const float4* X0, int* nn, cudaStream_t s);
-// One colour class of free surface vertices (triangles when m.fk == 3, quads when 4).
+struct IterStats;
+// Sector surfaces of the feature vertices (per-sector quadrics) and the positions the sector of
+// a feature neighbour is chosen from (a copy of the positions taken at the start of the colour).
+struct SectorSurfaces {
+    const int* srow;      // [nFeature + 1]
+    const int* stab;      // [nFeature x 20]
+    const float4* FS;     // [4 per sector]
+    const float4* Xs;     // [nSurf]
+};
+// One colour class of free surface vertices (triangles when m.fk == 3, quads when 4); sec:
+// null for meshes without feature vertices.
 void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
-                     cudaStream_t s);
+                     const SectorSurfaces* sec, cudaStream_t s);
+// Feature vertices: fdeg, the 1D-pass flags and the curves LS1 [3 nSurf] from the current
+// positions and vertex normals (flat: +z).
+void init_feature_state(const Mesh& m, int flat, float4* LS1, int* fdeg, uint8_t* opt, cudaStream_t s);
+// per-sector surfaces; returns the sector count (VSDMO_E_VALENCE beyond the table sizes)
+int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>& FS, cudaStream_t s);
+// One colour class of feature vertices: mode 0 flat (gated on the last minimum quality being
+// positive when gate_stats is set), 1 surface triangles, 2 surface quads.
+void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
+                   const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
+                   cudaStream_t s);
 int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
 // nu x nv samples of vertex vid's own surface (estimate_mode 0) or of the blended estimate (1)
 void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, int nv, float grid_scale,
