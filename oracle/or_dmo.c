@@ -666,3 +666,7 @@ void or_angle_qualities_f64(const or_mesh* m, const double* xyz, int max_angle, 
         }
     }
 }
+
+/* the f32 tet ring key for the boundary-surface passes (or_surf.c, or_feat.c) */
+void or__tet_coeffs_f32(const float* a, const float* b, const float* c, float* K) { tet_coeffs(a, b, c, K); }
+float or__tet_key_f32(int k, const float* K, float x, float y, float z) { return tet_key(k, K, x, y, z); }

@@ -180,6 +180,15 @@ void or_dmo_surf_feat_f64(const or_mesh* m, double* xyz, const double* xyz_init,
                           const int32_t* nearest, const double* vertex_normals, const int32_t* rowptr,
                           const int32_t* table, const double* sector_surfaces, int v0, int v1, double grid_scale,
                           double* margin, int nthreads);
+/* boundary-surface pass of a tet mesh: one colour class of free boundary vertices, the surface
+ * search judged by the ring of tets (sector data may be NULL) */
+void or_dmo_tet_surf_f32(const or_mesh* m, float* xyz, const float* xyz_init, const float* local_surfaces,
+                         const int32_t* nearest, const int32_t* rowptr, const int32_t* table,
+                         const float* sector_surfaces, int v0, int v1, float grid_scale, int nthreads);
+void or_dmo_tet_surf_f64(const or_mesh* m, double* xyz, const double* xyz_init, const double* local_surfaces,
+                         const int32_t* nearest, const int32_t* rowptr, const int32_t* table,
+                         const double* sector_surfaces, int v0, int v1, double grid_scale, double* margin,
+                         int nthreads);
 void or_surface_qualities_f32(const or_mesh* m, const float* xyz, float* q);
 void or_surface_qualities_f64(const or_mesh* m, const double* xyz, double* q);
 void or_optimize_surf_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale, int nthreads,

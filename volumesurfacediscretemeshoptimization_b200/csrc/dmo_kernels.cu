@@ -28,6 +28,7 @@
 #include "vsdmo_internal.cuh"
 #include "tc_gemm.cuh"
 #include "angle_metrics.cuh"
+#include "tet_key.cuh"
 #include <cfloat>
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -69,11 +70,6 @@ __device__ __forceinline__ float grid_offset(int i) {
     }
 }
 
-// 2^e as a float when it is a normal number, else 0. Multiplying by it is exactly ldexpf(x, e)
-// (both are the correctly rounded value of x 2^e), at the cost of one multiply.
-__device__ __forceinline__ float exp2_exact(int e) { return (e >= -126 && e <= 127) ? __int_as_float((e + 127) << 23) : 0.f; }
-__device__ __forceinline__ float scale2(float x, float p, int e) { return p != 0.f ? x * p : ldexpf(x, e); }
-
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
     for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(FULL, v, o));
@@ -88,49 +84,6 @@ __device__ __forceinline__ void warp_argmax(float& k, int& i) {
         int oi = __shfl_xor_sync(FULL, i, o);
         if (ok > k || (ok == k && oi < i)) { k = ok; i = oi; }
     }
-}
-
-// ---- tetrahedra ------------------------------------------------------------------------------
-// coefficients of tet (p, a, b, c) in scaled local coordinates
-__device__ __forceinline__ void tet_coeffs(float ax, float ay, float az, float bx, float by, float bz,
-                                           float cx, float cy, float cz, float4& K0, float4& K1) {
-    float ux = bx - ax, uy = by - ay, uz = bz - az;
-    float wx = cx - ax, wy = cy - ay, wz = cz - az;
-    float vx = cx - bx, vy = cy - by, vz = cz - bz;
-    float nx = uy * wz - uz * wy;
-    float ny = uz * wx - ux * wz;
-    float nz = ux * wy - uy * wx;
-    float d0 = (ax * nx + ay * ny) + az * nz;
-    float sx = (ax + bx) + cx, sy = (ay + by) + cy, sz = (az + bz) + cz;
-    float a2 = (ax * ax + ay * ay) + az * az;
-    float b2 = (bx * bx + by * by) + bz * bz;
-    float c2 = (cx * cx + cy * cy) + cz * cz;
-    float u2 = (ux * ux + uy * uy) + uz * uz;
-    float w2 = (wx * wx + wy * wy) + wz * wz;
-    float v2 = (vx * vx + vy * vy) + vz * vz;
-    K0 = make_float4(-nx, -ny, -nz, d0);
-    K1 = make_float4(-2.0f * sx, -2.0f * sy, -2.0f * sz, ((((a2 + b2) + c2) + u2) + w2) + v2);
-}
-
-// key of one candidate (used for the current position)
-__device__ float tet_key1(const float4* co, int k, float x, float y, float z) {
-    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
-    float N = 0.f, D = 1.f, dm = 0.f;
-    for (int t = 0; t < k; ++t) {
-        const float4 c0 = co[2 * t], c1 = co[2 * t + 1];
-        float detA = fmaf(c0.x, x, c0.w);
-        float LA = c1.w + fmaf(c1.x, x, tx);
-        float detB = fmaf(c0.y, y, detA);
-        float LB = LA + fmaf(c1.y, y, ty);
-        float det = fmaf(c0.z, z, detB);
-        float L = LB + fmaf(c1.z, z, tz);
-        float num = det * det;
-        float den = (L * L) * L;
-        if (t == 0) { N = num; D = den; dm = det; continue; }
-        if (num * D < N * den) { N = num; D = den; }
-        dm = fminf(dm, det);
-    }
-    return dm < 0.f ? dm : N / D;
 }
 
 // Ring minimum of the lane's candidates (fixed x, NJ y values, all NQ z values) over the k
@@ -1262,6 +1215,24 @@ void launch_dmo_tet(const Mesh& m, const DmoLaunch& L, cudaStream_t s, uint8_t* 
     const size_t smem = tet_smem_bytes(maxk);
     k_dmo_tet<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
         m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, L.depth, maxk, dirty, skipped);
+    VSDMO_CHECK_LAUNCH();
+}
+
+// Active set with a free boundary: the boundary passes move vertices whose rings hold interior
+// vertices; flagging the rings of all boundary vertices [v0, v1) keeps "skipping changes no
+// result" without tracking which boundary vertex moved. One warp per vertex.
+__global__ void k_mark_rings(const int* __restrict__ rowptr, const int4* __restrict__ hf, int v0, int v1,
+                             uint8_t* __restrict__ dirty) {
+    const int v = v0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (v >= v1) return;
+    const int b = rowptr[v];
+    tet_mark_ring(hf, b, rowptr[v + 1] - b, threadIdx.x & 31, dirty);
+}
+
+void launch_mark_rings(const Mesh& m, int v0, int v1, uint8_t* dirty, cudaStream_t s) {
+    if (v1 <= v0 || !dirty) return;
+    const long threads = 32L * (v1 - v0);
+    k_mark_rings<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m.hf_rowptr.p, m.hf.p, v0, v1, dirty);
     VSDMO_CHECK_LAUNCH();
 }
 

@@ -33,6 +33,7 @@
 // operation order, reproduced by the oracle's f32 mirror bit for bit (built with
 // --fmad=false here and without contraction there).
 #include "vsdmo_internal.cuh"
+#include "tet_key.cuh"
 #include <algorithm>
 #include <cfloat>
 
@@ -45,6 +46,7 @@ constexpr int SURF_MAX_RING = 64;
 constexpr float SURF_EPS = 1.19209e-07f;   // EPSILON of the reference's surface code
 constexpr int SECT_TABLE = 20;              // TABLE_SIZE of dmo/surfaceP/SurfaceCommon.h: halfedges of a feature vertex
 constexpr int SECT_LIST = 40;               // MAX_NEIGHBORS: points of one sector
+constexpr int TET_SURF_MAX_RING = 256;      // tets of a boundary vertex in the boundary passes
 
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
     return (ax * bx + ay * by) + az * bz;
@@ -265,6 +267,74 @@ __device__ __forceinline__ float ring_key(const float4* ring, int k, float px, f
 // shared memory per warp, in float4: ring [2 maxk + 1], neighbour surfaces [4 maxk], X0 [maxk]
 __host__ __device__ constexpr int surf_warp_f4(int maxk) { return 7 * maxk + 1; }
 
+// surface of ring neighbour vN for vertex v: its nearest initial vertex's surface, or for a feature
+// nearest initial vertex the sector surface of its halfedge whose target is nearest to v
+// (positions Xs taken at the start of the colour class)
+__device__ __forceinline__ const float4* neighbour_surface(int v, int nnN, const float4* __restrict__ LS,
+                                                           const int* __restrict__ rowptr, const int4* __restrict__ he,
+                                                           const int* __restrict__ srow, const int* __restrict__ stab,
+                                                           const float4* __restrict__ FS, const float4* __restrict__ Xs,
+                                                           int nFree) {
+    if (!FS || nnN < nFree) return LS + 4L * nnN;
+    const float4 pv = Xs[v];
+    float best = FLT_MAX;
+    int arg = 0;
+    for (int j = rowptr[nnN], idx = 0; j < rowptr[nnN + 1]; ++j, ++idx) {
+        const float4 t = Xs[he[j].x];
+        const float ex = t.x - pv.x, ey = t.y - pv.y, ez = t.z - pv.z;
+        const float d2 = dot3(ex, ey, ez, ex, ey, ez);
+        if (d2 < best) { best = d2; arg = idx; }
+    }
+    return FS + 4L * (srow[nnN - nFree] + stab[SECT_TABLE * (nnN - nFree) + arg]);
+}
+
+// the ring of tets of vertex v, scaled by 2^-ex like the interior search: coefficients in co
+// (2 per tet); returns false for a degenerate ring. md: the largest distance to a ring point.
+__device__ __forceinline__ bool stage_tets(const float4* __restrict__ pos, const int* __restrict__ hf_rowptr,
+                                           const int4* __restrict__ hf, int v, float4 c0, int lane, float4* co,
+                                           int& kt, float& md, int& ex, float& pinv) {
+    const int b = hf_rowptr[v];
+    kt = hf_rowptr[v + 1] - b;
+    float mm = 0.f, me = -FLT_MAX;
+    for (int t = lane; t < kt; t += 32) {
+        const int4 h = hf[b + t];
+        const int ids[3] = { h.x, h.y, h.z };
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float4 q = pos[ids[j]];
+            const float dx = q.x - c0.x, dy = q.y - c0.y, dz = q.z - c0.z;
+            mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
+            me = fmaxf(me, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        mm = fmaxf(mm, __shfl_xor_sync(FULL, mm, o));
+        me = fmaxf(me, __shfl_xor_sync(FULL, me, o));
+    }
+    md = me;
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) return false;
+    (void)frexpf(mm, &ex);
+    pinv = exp2_exact(-ex);
+    for (int t = lane; t < kt; t += 32) {
+        const int4 h = hf[b + t];
+        const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
+        float4 K0, K1;
+        tet_coeffs(scale2(pa.x - c0.x, pinv, -ex), scale2(pa.y - c0.y, pinv, -ex), scale2(pa.z - c0.z, pinv, -ex),
+                   scale2(pb.x - c0.x, pinv, -ex), scale2(pb.y - c0.y, pinv, -ex), scale2(pb.z - c0.z, pinv, -ex),
+                   scale2(pc.x - c0.x, pinv, -ex), scale2(pc.y - c0.y, pinv, -ex), scale2(pc.z - c0.z, pinv, -ex), K0, K1);
+        co[2 * t] = K0;
+        co[2 * t + 1] = K1;
+    }
+    __syncwarp();
+    return true;
+}
+
+__device__ __forceinline__ float tet_key_at(const float4* co, int kt, float4 c0, float pinv, int ex, float px, float py,
+                                            float pz) {
+    return tet_key1(co, kt, scale2(px - c0.x, pinv, -ex), scale2(py - c0.y, pinv, -ex), scale2(pz - c0.z, pinv, -ex));
+}
+
 template <int FK>
 __global__ void __launch_bounds__(SURF_WARPS * 32)
 k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
@@ -298,21 +368,7 @@ k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4*
             md = fmaxf(md, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
         }
         const int nnN = nn[h.x];
-        const float4* Ls = LS + 4L * nnN;
-        if (FS && nnN >= nFree) {
-            // a feature neighbour projects onto the sector surface of its halfedge whose target is
-            // nearest to this vertex (positions at the start of the colour class)
-            const float4 pv = Xs[v];
-            float best = FLT_MAX;
-            int arg = 0;
-            for (int j = rowptr[nnN], idx = 0; j < rowptr[nnN + 1]; ++j, ++idx) {
-                const float4 t = Xs[he[j].x];
-                const float ex = t.x - pv.x, ey = t.y - pv.y, ez = t.z - pv.z;
-                const float d2 = dot3(ex, ey, ez, ex, ey, ez);
-                if (d2 < best) { best = d2; arg = idx; }
-            }
-            Ls = FS + 4L * (srow[nnN - nFree] + stab[SECT_TABLE * (nnN - nFree) + arg]);
-        }
+        const float4* Ls = neighbour_surface(v, nnN, LS, rowptr, he, srow, stab, FS, Xs, nFree);
         nbL[4 * i] = Ls[0];
         nbL[4 * i + 1] = Ls[1];
         nbL[4 * i + 2] = Ls[2];
@@ -692,6 +748,150 @@ k_dmo_1d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* _
     if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
 }
 
+// Boundary-surface pass of a tet mesh (k_optimizeHierarchical2DTet, dmo/DMOTetImplCub.h:140-325):
+// the surface search of k_dmo_surf over the boundary vertex's surface ring, judged by the key of
+// the vertex's ring of tets; only while the last minimum quality is positive (dmo/DMOTet.cu:139).
+__global__ void __launch_bounds__(SURF_WARPS * 32)
+k_dmo_surf_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
+               const int* __restrict__ hf_rowptr, const int4* __restrict__ hf, const float4* __restrict__ X0,
+               const float4* __restrict__ LS, const int* __restrict__ nn, int v0, int v1, float grid_scale, int depth,
+               int maxkt, int maxks, const int* __restrict__ srow, const int* __restrict__ stab,
+               const float4* __restrict__ FS, const float4* __restrict__ Xs, int nFree,
+               const IterStats* __restrict__ stats, const int* __restrict__ iter) {
+    extern __shared__ float4 sst[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int v = v0 + blockIdx.x * SURF_WARPS + warp;
+    if (v >= v1) return;
+    if (!(stats[*iter].min_q > 0.f)) return;
+    const int b = rowptr[v], ks = rowptr[v + 1] - b;
+    if (ks <= 0 || ks > maxks || hf_rowptr[v + 1] - hf_rowptr[v] > maxkt) return;
+    float4* co = sst + (size_t)warp * (2 * maxkt + 5 * maxks);
+    float4* nbL = co + 2 * maxkt;
+    float4* nbX = nbL + 4 * maxks;
+    const float4 c0 = pos[v];
+    int kt, ex;
+    float md, pinv;
+    if (!stage_tets(pos, hf_rowptr, hf, v, c0, lane, co, kt, md, ex, pinv)) return;
+    for (int i = lane; i < ks; i += 32) {
+        const int nnN = nn[he[b + i].x];
+        const float4* Ls = neighbour_surface(v, nnN, LS, rowptr, he, srow, stab, FS, Xs, nFree);
+        nbL[4 * i] = Ls[0]; nbL[4 * i + 1] = Ls[1]; nbL[4 * i + 2] = Ls[2]; nbL[4 * i + 3] = Ls[3];
+        nbX[i] = X0[nnN];
+    }
+    __syncwarp();
+    const int nnv = nn[v];
+    Surf L;
+    L.l0 = LS[4L * nnv]; L.l1 = LS[4L * nnv + 1]; L.l2 = LS[4L * nnv + 2]; L.l3 = LS[4L * nnv + 3];
+    const float4 x0 = X0[nnv];
+    float cu, cv;
+    {
+        const float dx = c0.x - L.l0.x, dy = c0.y - L.l0.y, dz = c0.z - L.l0.z;
+        cu = dot3(dx, dy, dz, L.l1.x, L.l1.y, L.l1.z);
+        cv = dot3(dx, dy, dz, L.l2.x, L.l2.y, L.l2.z);
+    }
+    const float qOld = tet_key_at(co, kt, c0, pinv, ex, c0.x, c0.y, c0.z);
+    const int i1 = lane >> 3, j1 = lane & 7, i2 = i1 + 4;
+    const float o1 = (float)(7 - 2 * i1) / 7.f, oj = (float)(7 - 2 * j1) / 7.f, o2 = (float)(7 - 2 * i2) / 7.f;
+    float cx = c0.x, cy = c0.y, cz = c0.z;
+    float ds = grid_scale, lastMax = -FLT_MAX;
+    for (int d = 0; d < depth; ++d) {
+        const float S = ds * md;
+        const float u1 = fmaf(o1, S, cu), vv = fmaf(oj, S, cv), u2 = fmaf(o2, S, cu);
+        const float3 p1 = estimate(L, x0, nbL, nbX, ks, u1, vv);
+        const float3 p2 = estimate(L, x0, nbL, nbX, ks, u2, vv);
+        const float q1 = tet_key_at(co, kt, c0, pinv, ex, p1.x, p1.y, p1.z);
+        const float q2 = tet_key_at(co, kt, c0, pinv, ex, p2.x, p2.y, p2.z);
+        const bool second = q2 > q1;
+        const float val = second ? q2 : q1;
+        float bv = __shfl_sync(FULL, val, 0);
+        int bt = 0;
+        for (int t = 1; t < 32; ++t) {
+            const float vt = __shfl_sync(FULL, val, t);
+            if (vt > bv) { bv = vt; bt = t; }
+        }
+        const float qLast = tet_key_at(co, kt, c0, pinv, ex, cx, cy, cz);
+        const float bu = __shfl_sync(FULL, second ? u2 : u1, bt);
+        const float bw = __shfl_sync(FULL, vv, bt);
+        const float bx = __shfl_sync(FULL, second ? p2.x : p1.x, bt);
+        const float by = __shfl_sync(FULL, second ? p2.y : p1.y, bt);
+        const float bz = __shfl_sync(FULL, second ? p2.z : p1.z, bt);
+        if (qLast < bv) { cx = bx; cy = by; cz = bz; cu = bu; cv = bw; }
+        lastMax = bv;
+        ds = ds * (2.0f / 7.0f);
+    }
+    if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
+}
+
+// 1D pass of the feature vertices on a tet mesh's boundary (k_optimizeHierarchical1DTet,
+// dmo/DMOTetImplCub.h:327-494): k_dmo_1d with the key of the ring of tets
+__global__ void __launch_bounds__(SURF_WARPS * 32)
+k_dmo_1d_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
+             const int* __restrict__ hf_rowptr, const int4* __restrict__ hf, const float4* __restrict__ X0,
+             const float4* __restrict__ LS1, const int* __restrict__ nn, const int* __restrict__ fdeg,
+             const uint8_t* __restrict__ opt, int nFree, int v0, int v1, float grid_scale, int maxkt, int maxks,
+             const IterStats* __restrict__ stats, const int* __restrict__ iter) {
+    extern __shared__ float4 s1t[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int v = v0 + blockIdx.x * SURF_WARPS + warp;
+    if (v >= v1 || !opt[v]) return;
+    if (!(stats[*iter].min_q > 0.f)) return;
+    const int b = rowptr[v], ks = rowptr[v + 1] - b;
+    if (ks <= 0 || ks > maxks || hf_rowptr[v + 1] - hf_rowptr[v] > maxkt) return;
+    float4* co = s1t + (size_t)warp * (2 * maxkt + (maxks + 3) / 4);
+    int* surf = reinterpret_cast<int*>(co + 2 * maxkt);
+    const float4 c0 = pos[v];
+    int kt, ex;
+    float md, pinv;
+    if (!stage_tets(pos, hf_rowptr, hf, v, c0, lane, co, kt, md, ex, pinv)) return;
+    int ns = 0;
+    for (int base = 0; base < ks; base += 32) {
+        const int i = base + lane;
+        bool flag = false;
+        int t = 0;
+        if (i < ks) { t = he[b + i].x; flag = t >= nFree && fdeg[t] == 2; }
+        const unsigned bal = __ballot_sync(FULL, flag);
+        if (flag) surf[ns + __popc(bal & ((1u << lane) - 1u))] = t;
+        ns += __popc(bal);
+    }
+    __syncwarp();
+    const int nnv = nn[v];
+    const float4 l0 = LS1[3L * nnv], l1 = LS1[3L * nnv + 1];
+    float cu;
+    {
+        const float qx = c0.x - l0.x, qy = c0.y - l0.y, qz = c0.z - l0.z;
+        cu = dot3(qx, qy, qz, l1.x, l1.y, l1.z);
+    }
+    float cx = c0.x, cy = c0.y, cz = c0.z;
+    const float aff = 1.f / 7.f;
+    float ds = grid_scale, lastMax = -FLT_MAX;
+    for (int d = 0; d < 3; ++d) {
+        const float uMax = ds * md, uMin = -ds * md;
+        const int i = lane & 7;
+        const float u = cu + aff * ((float)i * uMin + (float)(7 - i) * uMax);
+        float3 p = make_float3(0.f, 0.f, 0.f);
+        float q = -FLT_MAX;
+        if (lane < 8) {
+            p = est1d(LS1, X0, nn, nnv, surf, ns, u);
+            q = tet_key_at(co, kt, c0, pinv, ex, p.x, p.y, p.z);
+        }
+        float bv = __shfl_sync(FULL, q, 0);
+        int bt = 0;
+        for (int t = 1; t < 8; ++t) {
+            const float qt = __shfl_sync(FULL, q, t);
+            if (qt > bv) { bv = qt; bt = t; }
+        }
+        const float qLast = tet_key_at(co, kt, c0, pinv, ex, cx, cy, cz);
+        const float bu = __shfl_sync(FULL, u, bt);
+        const float bx = __shfl_sync(FULL, p.x, bt), by = __shfl_sync(FULL, p.y, bt), bz = __shfl_sync(FULL, p.z, bt);
+        if (qLast < bv) { cx = bx; cy = by; cz = bz; cu = bu; }
+        lastMax = bv;
+        ds = ds * (2.f / 7.f);
+    }
+    const float qOld = tet_key_at(co, kt, c0, pinv, ex, c0.x, c0.y, c0.z);
+    if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
+}
+
+
 }  // namespace
 
 // Sample grids of the GUI's surface views (DMOTriClass::getLocalSurfacePoints /
@@ -828,6 +1028,40 @@ int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>&
     if (read_scalar(err.p, s))
         throw Error(VSDMO_E_VALENCE, "a feature vertex has more than 20 halfedges or a sector more than 40 points");
     return nSect;
+}
+
+void launch_dmo_surf_tet(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
+                         const SectorSurfaces* sec, const IterStats* gate_stats, const int* gate_iter, cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxkt = std::max(m.maxTets, 1), maxks = std::max(m.maxHE, 1);
+    const size_t smem = (size_t)SURF_WARPS * (2 * maxkt + 5 * maxks) * sizeof(float4);
+    k_dmo_surf_tet<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
+        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, m.hf.p, X0, LS, nn, L.v0, L.v1, L.grid_scale, L.depth, maxkt, maxks,
+        sec ? sec->srow : nullptr, sec ? sec->stab : nullptr, sec ? sec->FS : nullptr, sec ? sec->Xs : nullptr,
+        m.nSurf - m.nFeature, gate_stats, gate_iter);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void launch_dmo_1d_tet(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
+                       const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
+                       cudaStream_t s) {
+    const int n = L.v1 - L.v0;
+    if (n <= 0) return;
+    const int maxkt = std::max(m.maxTets, 1), maxks = std::max(m.maxHE, 1);
+    const size_t smem = (size_t)SURF_WARPS * (2 * maxkt + (maxks + 3) / 4) * sizeof(float4);
+    k_dmo_1d_tet<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
+        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, m.hf.p, X0, LS1, nn, fdeg, opt, m.nSurf - m.nFeature, L.v0, L.v1,
+        L.grid_scale, maxkt, maxks, gate_stats, gate_iter);
+    VSDMO_CHECK_LAUNCH();
+}
+
+int surf_tet_max_ring() { return TET_SURF_MAX_RING; }
+
+void prepare_surf_kernels() {
+    const int mx = (int)((size_t)SURF_WARPS * (2 * TET_SURF_MAX_RING + 5 * SURF_MAX_RING) * sizeof(float4));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_surf_tet, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_tet, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
 }
 
 void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
