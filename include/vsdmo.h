@@ -205,7 +205,11 @@ VSDMO_API vsdmo_status vsdmo_mesh_create_surface(vsdmo_mesh_t volume, uint32_t c
  * fix_boundary = 0 slide their boundary vertices (k_optimizeHierarchical1DFlat). Flat quad meshes get the 2D
  * search of DMOTriFlatClass with the quad mean ratio against +z (meanRatioMetricQuad(p, n),
  * dmo/DMOQualityQuad.h:30-50; the reference has no flat-quad class). Hex meshes get the
- * interior search of DMOHexClass (dmo/DMOHex.cu, k_optimizeHierarchicalInnerHex). */
+ * interior search of DMOHexClass (dmo/DMOHex.cu, k_optimizeHierarchicalInnerHex). Tet and hex
+ * meshes with fix_boundary = 0 add the boundary passes of DMOTetClass / DMOHexClass::doIteration
+ * (dmo/DMOTet.cu:128-170, dmo/DMOHex.cu:131-185): free boundary vertices on their local
+ * surfaces and feature vertices on their curves, judged by their volume rings, while the last
+ * minimum quality is positive. */
 VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* params, vsdmo_opt_t* out);
 VSDMO_API void vsdmo_opt_destroy(vsdmo_opt_t opt);
 /* n_iter calls of doIteration() (dmo/DMOTet.cu:128-170, dmo/DMOTriFlat.cu:129-166,

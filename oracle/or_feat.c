@@ -231,48 +231,12 @@ typedef struct {
 } feat_ctx;
 
 static int ring_mode(const or_mesh* m) {
-    if (or__hf_rowptr(m)) return 3;          /* boundary of a tet mesh: the ring of tets */
+    if (or__hf_rowptr(m)) return 3;          /* boundary of a volume mesh: its ring of tets / halfhexes */
     if (or_mesh_info(m, OR_I_IS_FLAT)) return 0;
     return or__fk(m) == 3 ? 1 : 2;
 }
 
-/* mode 3: the vertex's tets, scaled like the interior search (tet_key of or_dmo.c) */
-void or__tet_coeffs_f32(const float* a, const float* b, const float* c, float* K);
-float or__tet_key_f32(int k, const float* K, float x, float y, float z);
-double or_q_tet_mean_ratio_f64(const double* p0, const double* p1, const double* p2, const double* p3);
-
-static int tet_ring_f32(const or_mesh* m, const float* X, int v, float* K, int* ex, float* md) {
-    const int* rp = or__hf_rowptr(m);
-    const int* hf = or__hf(m);
-    const int b = rp[v], k = rp[v + 1] - b;
-    if (k > 4 * MAXR) return -1;
-    const float* c0 = X + 3 * (size_t)v;
-    float r[9 * 4 * MAXR];
-    float mm = 0.f, me = -FLT_MAX;
-    for (int t = 0; t < k; ++t) for (int j = 0; j < 3; ++j) {
-        const float* q = X + 3 * (size_t)hf[3 * (b + t) + j];
-        float d[3] = { q[0] - c0[0], q[1] - c0[1], q[2] - c0[2] };
-        for (int a = 0; a < 3; ++a) { r[9 * t + 3 * j + a] = d[a]; mm = fmaxf(mm, fabsf(d[a])); }
-        me = fmaxf(me, sqrtf(d3f(d, d)));
-    }
-    *md = me;
-    if (!(mm > 0.f) || !(mm < FLT_MAX)) return -1;
-    (void)frexpf(mm, ex);
-    for (int i = 0; i < 9 * k; ++i) r[i] = ldexpf(r[i], -*ex);
-    for (int t = 0; t < k; ++t) or__tet_coeffs_f32(r + 9 * t, r + 9 * t + 3, r + 9 * t + 6, K + 8 * t);
-    return k;
-}
-
-static double tet_ring_f64(const or_mesh* m, const double* X, int v, const double* p) {
-    const int* rp = or__hf_rowptr(m);
-    const int* hf = or__hf(m);
-    double q = DBL_MAX;
-    for (int i = rp[v]; i < rp[v + 1]; ++i)
-        q = fmin(q, or_q_tet_mean_ratio_f64(p, X + 3 * (size_t)hf[3 * i], X + 3 * (size_t)hf[3 * i + 1],
-                                            X + 3 * (size_t)hf[3 * i + 2]));
-    return q;
-}
-
+/* mode 3: the vertex's ring of tets / halfhexes (or_vring.c) */
 /* collects the quality ring (returns the element count), the extent and the surf neighbours */
 #define COLLECT(T, SQRT, FABS, FMAX)                                                                       \
     const int* rp = or__he_rowptr(C->m);                                                                  \
@@ -336,14 +300,12 @@ static void feat_vertex_32(const feat_ctx* C, float* X, int v, float gs) {
     if (!C->opt[v]) return;
     COLLECT(float, sqrtf, fabsf, fmaxf)
     if (k > MAXR) return;
-    float TK[8 * 4 * MAXR];
-    int tex = 0, kt = 0;
+    or_vring32 R = { 0 };
     if (C->mode == 3) {
-        kt = tet_ring_f32(C->m, X, v, TK, &tex, &md);
-        if (kt < 0) return;
+        if (!or__vring32_init(&R, C->m, X, v)) { or__vring32_free(&R); return; }
+        md = R.md;
     }
-#define RQ(P, N) (C->mode == 3 ? or__tet_key_f32(kt, TK, ldexpf((P)[0] - c0[0], -tex), ldexpf((P)[1] - c0[1], -tex), \
-                                                 ldexpf((P)[2] - c0[2], -tex)) : ringq32(C->mode, ne, ring, P, N))
+#define RQ(P, N) (C->mode == 3 ? or__vring32_key(&R, P) : ringq32(C->mode, ne, ring, P, N))
     const float* LS = (const float*)C->LS1;
     const float* L = LS + LS1F * (size_t)C->nn[v];
     float q[3] = { c0[0] - L[0], c0[1] - L[1], c0[2] - L[2] };
@@ -374,6 +336,7 @@ static void feat_vertex_32(const feat_ctx* C, float* X, int v, float gs) {
     const float qOld = RQ(c0, NULL);
 #undef RQ
     if (qOld < lastMax) { X[3 * (size_t)v] = cur[0]; X[3 * (size_t)v + 1] = cur[1]; X[3 * (size_t)v + 2] = cur[2]; }
+    or__vring32_free(&R);
 }
 
 void or_dmo_1d_f32(const or_mesh* m, float* X, const float* X0, const float* LS1, const int32_t* nn, const float* vn,
@@ -418,17 +381,8 @@ static void feat_vertex_64(const feat_ctx* C, double* X, int v, double gs, doubl
     if (!C->opt[v]) return;
     COLLECT(double, sqrt, fabs, fmax)
     if (k > MAXR) return;
-    if (C->mode == 3) {
-        const int* hrp = or__hf_rowptr(C->m);
-        const int* hfa = or__hf(C->m);
-        md = -DBL_MAX;
-        for (int i = hrp[v]; i < hrp[v + 1]; ++i) for (int j = 0; j < 3; ++j) {
-            const double* q = X + 3 * (size_t)hfa[3 * i + j];
-            double d[3] = { q[0] - c0[0], q[1] - c0[1], q[2] - c0[2] };
-            md = fmax(md, sqrt(d3d(d, d)));
-        }
-    }
-#define RQ(P, N) (C->mode == 3 ? tet_ring_f64(C->m, X, v, P) : ringq64(C->mode, ne, ring, P, N))
+    if (C->mode == 3) md = or__vring64_extent(C->m, X, v);
+#define RQ(P, N) (C->mode == 3 ? or__vring64_q(C->m, X, v, P) : ringq64(C->mode, ne, ring, P, N))
     const double* LS = (const double*)C->LS1;
     const double* L = LS + LS1F * (size_t)C->nn[v];
     double q[3] = { c0[0] - L[0], c0[1] - L[1], c0[2] - L[2] };
@@ -445,18 +399,19 @@ static void feat_vertex_64(const feat_ctx* C, double* X, int v, double gs, doubl
             double p[3];
             est1d_64(C, v, surf, ns, u, p);
             const double qv = RQ(p, nv);
-            if (qv > best) { second = best; best = qv; bu = u; } else if (qv > second) second = qv;
+            if (qv > best) { second = best; best = qv; bu = u; }
+            else if ((C->mode != 3 || qv < best) && qv > second) second = qv;
         }
         const double qLast = RQ(cur, nv);
         mg = fmin(mg, best - second);
-        mg = fmin(mg, fabs(best - qLast));
+        mg = fmin(mg, C->mode == 3 ? or__gap64(best, qLast) : fabs(best - qLast));
         if (qLast < best) { est1d_64(C, v, surf, ns, bu, cur); cu = bu; }
         lastMax = best;
         ds = ds * (2.0 / (NQ - 1));
     }
     const double qOld = RQ(c0, NULL);
 #undef RQ
-    mg = fmin(mg, fabs(lastMax - qOld));
+    mg = fmin(mg, C->mode == 3 ? or__gap64(lastMax, qOld) : fabs(lastMax - qOld));
     if (qOld < lastMax) { X[3 * (size_t)v] = cur[0]; X[3 * (size_t)v + 1] = cur[1]; X[3 * (size_t)v + 2] = cur[2]; }
     if (margin) *margin = mg;
 }

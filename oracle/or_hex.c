@@ -132,19 +132,20 @@ static void hex_vertex_f64(const or_mesh* m, double* X, int v, double gs, double
                 p[1] = aff * (j * gmin[1] + (NQ - 1 - j) * gmax[1]);
                 p[2] = aff * (kk * gmin[2] + (NQ - 1 - kk) * gmax[2]);
                 const double q = ring_hex64(k, ring, p);
-                if (q > best) { second = best; best = q; } else if (q > second) second = q;
+                if (q > best) { second = best; best = q; }
+                else if (q < best && q > second) second = q;   /* exact ties: see or__gap64 */
                 if (q > qMax[t]) { qMax[t] = q; pMax[t][0] = p[0]; pMax[t][1] = p[1]; pMax[t][2] = p[2]; }
             }
         key = 0;
         for (int t = 1; t < 128; ++t) if (qMax[t] > qMax[key]) key = t;
         mg = fmin(mg, best - second);
         if (carried > -DBL_MAX && best != carried) mg = fmin(mg, fabs(best - carried));
-        mg = fmin(mg, fabs(qMax[key] - qLast));
+        mg = fmin(mg, or__gap64(qMax[key], qLast));
         if (qLast < qMax[key]) { curr[0] = pMax[key][0]; curr[1] = pMax[key][1]; curr[2] = pMax[key][2]; }
         ds = ds * (2.0 / (NQ - 1));
     }
     const double qOld = ring_hex64(k, ring, c0);
-    mg = fmin(mg, fabs(qMax[key] - qOld));
+    mg = fmin(mg, or__gap64(qMax[key], qOld));
     if (qOld < qMax[key]) { X[3 * v] = curr[0]; X[3 * v + 1] = curr[1]; X[3 * v + 2] = curr[2]; }
     if (margin) *margin = mg;
     free(ring);
@@ -271,6 +272,10 @@ static float hex_key32(int k, const float* co, float x, float y, float z, float 
         }
     }
     return zero ? 0.f : N / D;
+}
+
+float or__hex_key_f32(int k, const float* co, float x, float y, float z, float es, float ea) {
+    return hex_key32(k, co, x, y, z, es, ea);
 }
 
 static inline float grid_offset(int i) { return (float)(NQ - 1 - 2 * i) / (float)(NQ - 1); }

@@ -993,58 +993,23 @@ void or_surface_points_f32(const or_mesh* m, const float* X, const float* X0, co
 
 
 /* ======================================================================================== */
-/* boundary-surface pass of tet meshes (k_optimizeHierarchical2DTet, DMOTetImplCub.h:140-325): */
-/* the surface search of the free boundary vertices with the ring quality of their tets        */
+/* boundary-surface pass of volume meshes (k_optimizeHierarchical2DTet, dmo/DMOTetImplCub.h:  */
+/* 142-325; k_optimizeHierarchical2DHex, dmo/DMOHexImplCub.h:142-317): the surface search of   */
+/* the free boundary vertices judged by their ring of tets / halfhexes (or_vring.c)            */
 /* ======================================================================================== */
 extern const int* or__hf_rowptr(const or_mesh* m);
-extern const int* or__hf(const or_mesh* m);
-void or__tet_coeffs_f32(const float* a, const float* b, const float* c, float* K);
-float or__tet_key_f32(int k, const float* K, float x, float y, float z);
-double or_q_tet_mean_ratio_f64(const double* p0, const double* p1, const double* p2, const double* p3);
 
-/* the scaled tet ring of vertex v: coefficients K [8 k], exponent, Euclidean extent */
-static int tet_ring32(const or_mesh* m, const float* X, int v, float* K, int* ex, float* md) {
-    const int* rp = or__hf_rowptr(m);
-    const int* hf = or__hf(m);
-    const int b = rp[v], k = rp[v + 1] - b;
-    const float* c0 = X + 3 * (size_t)v;
-    float mm = 0.f, me = -FLT_MAX;
-    float* r = (float*)malloc(sizeof(float) * 9 * (size_t)(k > 0 ? k : 1));
-    for (int t = 0; t < k; ++t) for (int j = 0; j < 3; ++j) {
-        const float* q = X + 3 * (size_t)hf[3 * (b + t) + j];
-        float d[3] = { q[0] - c0[0], q[1] - c0[1], q[2] - c0[2] };
-        for (int a = 0; a < 3; ++a) { r[9 * t + 3 * j + a] = d[a]; mm = fmaxf(mm, fabsf(d[a])); }
-        me = fmaxf(me, sqrtf(dot3f(d, d)));
-    }
-    *md = me;
-    if (!(mm > 0.f) || !(mm < FLT_MAX)) { free(r); return -1; }
-    (void)frexpf(mm, ex);
-    for (int i = 0; i < 9 * k; ++i) r[i] = ldexpf(r[i], -*ex);
-    for (int t = 0; t < k; ++t) or__tet_coeffs_f32(r + 9 * t, r + 9 * t + 3, r + 9 * t + 6, K + 8 * t);
-    free(r);
-    return k;
-}
-
-static float tet_key_at(int k, const float* K, int ex, const float* c0, const float* p) {
-    return or__tet_key_f32(k, K, ldexpf(p[0] - c0[0], -ex), ldexpf(p[1] - c0[1], -ex), ldexpf(p[2] - c0[2], -ex));
-}
-
-static void tet_surf_vertex_f32(const surf32* S, float* X, int v, float gs) {
+static void vol_surf_vertex_f32(const surf32* S, float* X, int v, float gs) {
     const or_mesh* m = S->m;
-    const int* hrp = or__hf_rowptr(m);
-    const int kt = hrp[v + 1] - hrp[v];
-    if (kt <= 0) return;
-    float* K = (float*)malloc(sizeof(float) * 8 * (size_t)kt);
-    int ex;
-    float md;
-    if (tet_ring32(m, X, v, K, &ex, &md) < 0) { free(K); return; }
+    or_vring32 R;
+    if (!or__vring32_init(&R, m, X, v)) { or__vring32_free(&R); return; }
+    const float md = R.md;
     float c0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
     float cur[3] = { c0[0], c0[1], c0[2] };
     const float* L = S->LS + LSF * (size_t)S->nn[v];
     float dl[3] = { c0[0] - L[0], c0[1] - L[1], c0[2] - L[2] };
     float cu = dot3f(dl, L + 4), cv = dot3f(dl, L + 8);
-    float qLast = tet_key_at(kt, K, ex, c0, c0);
-    const float qOld = qLast;
+    const float qOld = or__vring32_key(&R, c0);
     float ds = gs, lastMax = -FLT_MAX;
     for (int d = 0; d < DEPTH; ++d) {
         float S_ = ds * md;
@@ -1057,7 +1022,7 @@ static void tet_surf_vertex_f32(const surf32* S, float* X, int v, float gs) {
             float pw1[3], pw2[3];
             est32(S, v, us[i1], vs[j1], pw1);
             est32(S, v, us[i2], vs[j1], pw2);
-            float q1 = tet_key_at(kt, K, ex, c0, pw1), q2 = tet_key_at(kt, K, ex, c0, pw2);
+            float q1 = or__vring32_key(&R, pw1), q2 = or__vring32_key(&R, pw2);
             float val = q1; int second = 0;
             if (q2 > q1) { val = q2; second = 1; }
             if (bt < 0 || val > bv) {
@@ -1067,16 +1032,16 @@ static void tet_surf_vertex_f32(const surf32* S, float* X, int v, float gs) {
                 bp[0] = pp[0]; bp[1] = pp[1]; bp[2] = pp[2];
             }
         }
-        qLast = tet_key_at(kt, K, ex, c0, cur);
+        const float qLast = or__vring32_key(&R, cur);
         if (qLast < bv) { cur[0] = bp[0]; cur[1] = bp[1]; cur[2] = bp[2]; cu = bu; cv = bvv; }
         lastMax = bv;
         ds = ds * (2.0f / (float)(NQ - 1));
     }
     if (qOld < lastMax) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; X[3 * v + 2] = cur[2]; }
-    free(K);
+    or__vring32_free(&R);
 }
 
-void or_dmo_tet_surf_f32(const or_mesh* m, float* X, const float* X0, const float* LS, const int32_t* nn,
+void or_dmo_vol_surf_f32(const or_mesh* m, float* X, const float* X0, const float* LS, const int32_t* nn,
                          const int32_t* frow, const int32_t* ftab, const float* FS, int v0, int v1, float gs,
                          int nthreads) {
     const int nS = or_mesh_info(m, OR_I_NSURF);
@@ -1088,33 +1053,17 @@ void or_dmo_tet_surf_f32(const or_mesh* m, float* X, const float* X0, const floa
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 16)
 #endif
-    for (int v = v0; v < v1; ++v) tet_surf_vertex_f32(&S, X, v, gs);
+    for (int v = v0; v < v1; ++v) vol_surf_vertex_f32(&S, X, v, gs);
     free(Xs);
 }
 
-static double tet_ring64(const or_mesh* m, const double* X, int v, const double* p) {
-    const int* rp = or__hf_rowptr(m);
-    const int* hf = or__hf(m);
-    double q = DBL_MAX;
-    for (int i = rp[v]; i < rp[v + 1]; ++i)
-        q = fmin(q, or_q_tet_mean_ratio_f64(p, X + 3 * (size_t)hf[3 * i], X + 3 * (size_t)hf[3 * i + 1],
-                                            X + 3 * (size_t)hf[3 * i + 2]));
-    return q;
-}
-
-static void tet_surf_vertex_f64(const surf64* S, double* X, int v, double gs, double* margin) {
+static void vol_surf_vertex_f64(const surf64* S, double* X, int v, double gs, double* margin) {
     const or_mesh* m = S->m;
     const int* rp = or__hf_rowptr(m);
-    const int* hf = or__hf(m);
     if (rp[v + 1] - rp[v] <= 0) { if (margin) *margin = DBL_MAX; return; }
     double p0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
     double cur[3] = { p0[0], p0[1], p0[2] };
-    double md = -DBL_MAX;
-    for (int i = rp[v]; i < rp[v + 1]; ++i) for (int j = 0; j < 3; ++j) {
-        const double* q = X + 3 * (size_t)hf[3 * i + j];
-        double d[3] = { q[0] - p0[0], q[1] - p0[1], q[2] - p0[2] };
-        md = fmax(md, sqrt(dot3d(d, d)));
-    }
+    const double md = or__vring64_extent(m, X, v);
     const double* L = S->LS + LSF * (size_t)S->nn[v];
     double dl[3] = { p0[0] - L[0], p0[1] - L[1], p0[2] - L[2] };
     double cu = dot3d(dl, L + 4), cv = dot3d(dl, L + 8);
@@ -1132,29 +1081,32 @@ static void tet_surf_vertex_f64(const surf64* S, double* X, int v, double gs, do
             double pw1[3], pw2[3];
             est64(S, v, u1, v1, pw1);
             est64(S, v, u2, v1, pw2);
-            double q1 = tet_ring64(m, X, v, pw1), q2 = tet_ring64(m, X, v, pw2);
+            double q1 = or__vring64_q(m, X, v, pw1), q2 = or__vring64_q(m, X, v, pw2);
             val[t] = q1; uvs[t][0] = u1; uvs[t][1] = v1;
             for (int a = 0; a < 3; ++a) pts[t][a] = pw1[a];
             if (q2 > q1) { val[t] = q2; uvs[t][0] = u2; for (int a = 0; a < 3; ++a) pts[t][a] = pw2[a]; }
             double qs[2] = { q1, q2 };
-            for (int s_ = 0; s_ < 2; ++s_) { if (qs[s_] > best) { second = best; best = qs[s_]; } else if (qs[s_] > second) second = qs[s_]; }
+            for (int s_ = 0; s_ < 2; ++s_) {
+                if (qs[s_] > best) { second = best; best = qs[s_]; }
+                else if (qs[s_] < best && qs[s_] > second) second = qs[s_];
+            }
         }
-        double qLast = tet_ring64(m, X, v, cur);
+        double qLast = or__vring64_q(m, X, v, cur);
         int w = 0;
         for (int t = 1; t < 32; ++t) if (val[t] > val[w]) w = t;
         mg = fmin(mg, best - second);
-        mg = fmin(mg, fabs(best - qLast));
+        mg = fmin(mg, or__gap64(best, qLast));
         if (qLast < val[w]) { for (int a = 0; a < 3; ++a) cur[a] = pts[w][a]; cu = uvs[w][0]; cv = uvs[w][1]; }
         lastMax = val[w];
         ds = ds * (2.0 / (NQ - 1));
     }
-    double qOld = tet_ring64(m, X, v, p0);
-    mg = fmin(mg, fabs(lastMax - qOld));
+    double qOld = or__vring64_q(m, X, v, p0);
+    mg = fmin(mg, or__gap64(lastMax, qOld));
     if (qOld < lastMax) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; X[3 * v + 2] = cur[2]; }
     if (margin) *margin = mg;
 }
 
-void or_dmo_tet_surf_f64(const or_mesh* m, double* X, const double* X0, const double* LS, const int32_t* nn,
+void or_dmo_vol_surf_f64(const or_mesh* m, double* X, const double* X0, const double* LS, const int32_t* nn,
                          const int32_t* frow, const int32_t* ftab, const double* FS, int v0, int v1, double gs,
                          double* margin, int nthreads) {
     double* Xs = FS ? (double*)malloc(sizeof(double) * 3 * (size_t)or_mesh_info(m, OR_I_NV)) : NULL;
@@ -1164,6 +1116,6 @@ void or_dmo_tet_surf_f64(const or_mesh* m, double* X, const double* X0, const do
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 16)
 #endif
-    for (int v = v0; v < v1; ++v) tet_surf_vertex_f64(&S, X, v, gs, margin ? margin + (v - v0) : NULL);
+    for (int v = v0; v < v1; ++v) vol_surf_vertex_f64(&S, X, v, gs, margin ? margin + (v - v0) : NULL);
     free(Xs);
 }

@@ -92,8 +92,8 @@ def lib():
         L.or_feature_surfaces_f64.restype = I
         L.or_feature_surfaces_f64.argtypes = [P, P, P, P, P, P, I]
         L.or_dmo_surf_feat_f32.argtypes = [P, P, P, P, P, P, P, P, P, I, I, F, I]
-        L.or_dmo_tet_surf_f32.argtypes = [P, P, P, P, P, P, P, P, I, I, F, I]
-        L.or_dmo_tet_surf_f64.argtypes = [P, P, P, P, P, P, P, P, I, I, D, P, I]
+        L.or_dmo_vol_surf_f32.argtypes = [P, P, P, P, P, P, P, P, I, I, F, I]
+        L.or_dmo_vol_surf_f64.argtypes = [P, P, P, P, P, P, P, P, I, I, D, P, I]
         L.or_dmo_surf_feat_f64.argtypes = [P, P, P, P, P, P, P, P, P, I, I, D, P, I]
         L.or_surface_fit_1d_f32.argtypes = [P, P, P, P]
         L.or_surface_fit_1d_f64.argtypes = [P, P, P, P]
@@ -242,24 +242,24 @@ class OracleMesh:
                                    v0, v1, grid_scale, _p(margin), nthreads)
         return xyz, margin[: v1 - v0]
 
-    def dmo_tet_surf_f32(self, xyz, x0, ls, nn, sectors, v0, v1, grid_scale=0.5, nthreads=0):
-        """Boundary-surface pass of a tet mesh over the free boundary class [v0, v1)."""
+    def dmo_vol_surf_f32(self, xyz, x0, ls, nn, sectors, v0, v1, grid_scale=0.5, nthreads=0):
+        """Boundary-surface pass of a tet or hex mesh over the free boundary class [v0, v1)."""
         xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
         rp, tab, fs = (None, None, None) if sectors is None else (np.ascontiguousarray(a) for a in sectors)
-        lib().or_dmo_tet_surf_f32(self.h, _p(xyz), _p(np.ascontiguousarray(x0, np.float32)),
+        lib().or_dmo_vol_surf_f32(self.h, _p(xyz), _p(np.ascontiguousarray(x0, np.float32)),
                                   _p(np.ascontiguousarray(ls, np.float32)), _p(np.ascontiguousarray(nn, np.int32)),
                                   None if rp is None else _p(rp), None if tab is None else _p(tab),
                                   None if fs is None else _p(np.ascontiguousarray(fs, np.float32)), v0, v1,
                                   grid_scale, nthreads)
         return xyz
 
-    def dmo_tet_surf_f64(self, xyz, x0, ls, nn, sectors, v0, v1, grid_scale=0.5, nthreads=0):
+    def dmo_vol_surf_f64(self, xyz, x0, ls, nn, sectors, v0, v1, grid_scale=0.5, nthreads=0):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
         margin = np.zeros(max(v1 - v0, 1))
         a = [None, None, None] if sectors is None else [np.ascontiguousarray(sectors[0], np.int32),
                                                        np.ascontiguousarray(sectors[1], np.int32),
                                                        np.ascontiguousarray(sectors[2], np.float64)]
-        lib().or_dmo_tet_surf_f64(self.h, _p(xyz), _p(np.ascontiguousarray(x0, np.float64)),
+        lib().or_dmo_vol_surf_f64(self.h, _p(xyz), _p(np.ascontiguousarray(x0, np.float64)),
                                   _p(np.ascontiguousarray(ls, np.float64)), _p(np.ascontiguousarray(nn, np.int32)),
                                   *[None if x is None else _p(x) for x in a], v0, v1, grid_scale, _p(margin), nthreads)
         return xyz, margin[: v1 - v0]

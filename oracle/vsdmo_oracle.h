@@ -180,15 +180,23 @@ void or_dmo_surf_feat_f64(const or_mesh* m, double* xyz, const double* xyz_init,
                           const int32_t* nearest, const double* vertex_normals, const int32_t* rowptr,
                           const int32_t* table, const double* sector_surfaces, int v0, int v1, double grid_scale,
                           double* margin, int nthreads);
-/* boundary-surface pass of a tet mesh: one colour class of free boundary vertices, the surface
- * search judged by the ring of tets (sector data may be NULL) */
-void or_dmo_tet_surf_f32(const or_mesh* m, float* xyz, const float* xyz_init, const float* local_surfaces,
+/* boundary-surface pass of a tet or hex mesh: one colour class of free boundary vertices, the
+ * surface search judged by the vertex's ring of tets / halfhexes (sector data may be NULL) */
+void or_dmo_vol_surf_f32(const or_mesh* m, float* xyz, const float* xyz_init, const float* local_surfaces,
                          const int32_t* nearest, const int32_t* rowptr, const int32_t* table,
                          const float* sector_surfaces, int v0, int v1, float grid_scale, int nthreads);
-void or_dmo_tet_surf_f64(const or_mesh* m, double* xyz, const double* xyz_init, const double* local_surfaces,
+void or_dmo_vol_surf_f64(const or_mesh* m, double* xyz, const double* xyz_init, const double* local_surfaces,
                          const int32_t* nearest, const int32_t* rowptr, const int32_t* table,
                          const double* sector_surfaces, int v0, int v1, double grid_scale, double* margin,
                          int nthreads);
+/* the volume ring of a boundary vertex (or_vring.c; internal to the oracle) */
+typedef struct { int hex, k, ex; float es, ea, md; float* co; float c0[3]; } or_vring32;
+int    or__vring32_init(or_vring32* R, const or_mesh* m, const float* xyz, int v);  /* 0: degenerate */
+float  or__vring32_key(const or_vring32* R, const float* p);
+void   or__vring32_free(or_vring32* R);
+double or__vring64_q(const or_mesh* m, const double* xyz, int v, const double* p);
+double or__vring64_extent(const or_mesh* m, const double* xyz, int v);
+double or__gap64(double a, double b);
 void or_surface_qualities_f32(const or_mesh* m, const float* xyz, float* q);
 void or_surface_qualities_f64(const or_mesh* m, const double* xyz, double* q);
 void or_optimize_surf_f32(const or_mesh* m, float* xyz, int n_iter, float grid_scale, int nthreads,

@@ -101,9 +101,9 @@ def test_hex_against_fp64_reference(oracle_mod, vsdmo):
         checked += int(clear.sum())
         total += v1 - v0
         x = g
-    # the shape metric is 0 for every candidate of a ring that holds a degenerate corner and
-    # the grid extent is the per-axis minimum ring distance, so exact ties are common here
-    assert checked > 0.2 * total
+    # exact ties in double (a ring minimum held by a constant sub-tet, or 0) are structural and
+    # decide nothing; the remaining decisions are clear for most vertices
+    assert checked > 0.6 * total
     xyz, el = HEXES["hex8"]()
     gm2 = vsdmo.DMOMeshHex(xyz, el)
     opt2 = vsdmo.DMOHexClass(gm2, n_iter=3)

@@ -1,11 +1,11 @@
-"""GPU parity tests of the boundary passes of tet meshes (DMOTetClass with a free boundary,
-dmo/DMOTet.cu:128-170): the interior classes, then — while the minimum quality after the
-previous iteration is positive — the free boundary classes on their local surfaces judged by
-their tet rings (k_optimizeHierarchical2DTet) and the feature classes on their curves
-(k_optimizeHierarchical1DTet), then the nearest-initial-vertex walk and the normals.
-Bitwise against the oracle's f32 restatement over whole iterations, within the FP64
-restatement's tolerance for one iteration, and the known answer of a cube: boundary vertices
-stay on their faces and edges."""
+"""GPU parity tests of the boundary passes of volume meshes (DMOTetClass / DMOHexClass with a
+free boundary, dmo/DMOTet.cu:128-170, dmo/DMOHex.cu:131-185): the interior classes, then —
+while the minimum quality after the previous iteration is positive — the free boundary
+classes on their local surfaces judged by their volume rings (k_optimizeHierarchical2DTet /
+2DHex) and the feature classes on their curves (k_optimizeHierarchical1DTet / 1DHex), then the
+nearest-initial-vertex walk and the normals. Bitwise against the oracle's f32 restatement over
+whole iterations, within the FP64 restatement's tolerance for one iteration, and the known
+answer of a cube: boundary vertices stay on their faces and edges."""
 import ctypes as C
 
 import numpy as np
@@ -14,7 +14,7 @@ import pytest
 from volumesurfacediscretemeshoptimization_b200 import meshgen as G
 
 pytestmark = pytest.mark.gpu
-TET = 2
+TET, HEX = 2, 3
 
 
 def same_bits(a, b):
@@ -29,21 +29,29 @@ def _p(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def jittered_tet_cube(n=6, seed=4):
-    """Tet cube with interior vertices jittered by up to 0.3h and boundary vertices displaced
-    within their face plane / along their edge by up to 0.25h (corners fixed)."""
+def jittered_cube(kind="tet", n=None, seed=4):
+    """Tet (n = 6) or hex (n = 5) cube with interior vertices jittered by up to 0.3h (hex 0.2h)
+    and boundary vertices displaced within their face plane / along their edge by up to 0.25h
+    (hex 0.2h), corners fixed."""
+    hex_ = kind == "hex"
+    n = n or (5 if hex_ else 6)
     h = 1.0 / n
-    xyz, tets = G.tet_cube(n, seed=None)
+    ji, jb = (0.2, 0.2) if hex_ else (0.3, 0.25)
+    xyz, el = (G.hex_cube if hex_ else G.tet_cube)(n, seed=None)
     xyz = xyz.astype(np.float64)
     rng = np.random.default_rng(seed)
     for i in range(len(xyz)):
         on = (np.abs(xyz[i]) < 1e-9) | (np.abs(xyz[i] - 1) < 1e-9)
         for a in range(3):
             if on.sum() == 0:
-                xyz[i, a] += rng.uniform(-0.3 * h, 0.3 * h)
+                xyz[i, a] += rng.uniform(-ji * h, ji * h)
             elif not on[a] and on.sum() < 3:
-                xyz[i, a] += rng.uniform(-0.25 * h, 0.25 * h)
-    return xyz.astype(np.float32), tets
+                xyz[i, a] += rng.uniform(-jb * h, jb * h)
+    return xyz.astype(np.float32), el, h
+
+
+def _classes(vsdmo, kind):
+    return (HEX, vsdmo.DMOMeshHex, vsdmo.DMOHexClass) if kind == "hex" else (TET, vsdmo.DMOMeshTet, vsdmo.DMOTetClass)
 
 
 def _ranges(arr):
@@ -51,14 +59,14 @@ def _ranges(arr):
 
 
 def _oracle_iteration(oracle_mod, om, x, st):
-    """One DMOTetClass iteration with a free boundary on the oracle (f32)."""
+    """One DMOTetClass / DMOHexClass iteration with a free boundary on the oracle (f32)."""
     L = oracle_mod.lib()
     gate = om.element_qualities_f32(x).min() > 0
     for v0, v1 in _ranges(om.array(oracle_mod.A_COL_INNER)):
         x = om.dmo_color_f32(x, v0, v1)
     if gate:
         for v0, v1 in _ranges(om.array(oracle_mod.A_COL_FREE)):
-            x = om.dmo_tet_surf_f32(x, st["x0"], st["ls"], st["nn"], st["sectors"], v0, v1)
+            x = om.dmo_vol_surf_f32(x, st["x0"], st["ls"], st["nn"], st["sectors"], v0, v1)
         for v0, v1 in _ranges(om.array(oracle_mod.A_COL_FEATURE)):
             x = om.dmo_1d_f32(x, st["x0"], st["curves"], st["nn"], st["vn"], st["fdeg"], st["opt"], v0, v1)
     nn = st["nn"].copy()
@@ -69,12 +77,14 @@ def _oracle_iteration(oracle_mod, om, x, st):
     return x
 
 
-def test_tet_free_boundary_bitwise(oracle_mod, vsdmo):
-    xyz, tets = jittered_tet_cube()
-    om = oracle_mod.OracleMesh(TET, xyz, tets)
-    gm = vsdmo.DMOMeshTet(xyz, tets)
+@pytest.mark.parametrize("kind", ["tet", "hex"])
+def test_free_boundary_bitwise(oracle_mod, vsdmo, kind):
+    xyz, el, _ = jittered_cube(kind)
+    et, Mesh, Opt = _classes(vsdmo, kind)
+    om = oracle_mod.OracleMesh(et, xyz, el)
+    gm = Mesh(xyz, el)
     assert gm.info == om.info and gm.info["nFeature"] > 0
-    opt = vsdmo.DMOTetClass(gm, n_iter=3, fix_boundary=False)
+    opt = Opt(gm, n_iter=3, fix_boundary=False)
     x = om.xyz
     x0, ls, nn, fn, vn = om.surface_state_f32(x)
     sectors_o = om.sector_surfaces(x, fn)
@@ -109,35 +119,38 @@ def test_tet_free_boundary_bitwise(oracle_mod, vsdmo):
     assert np.all(np.diff(mn) >= -1e-6) and mean[-1] > mean[0]
 
 
-def test_tet_free_boundary_against_fp64_reference(oracle_mod, vsdmo):
-    """One iteration (interior classes, free boundary classes, feature classes) against the
-    literal double restatement: positions within 1e-5 h wherever the double decisions are
-    clear (a vertex is comparable when its decisions and those of its tet ring are)."""
-    n = 6
-    h = 1.0 / n
-    xyz, tets = jittered_tet_cube(n, seed=4)
-    om = oracle_mod.OracleMesh(TET, xyz, tets)
-    gm = vsdmo.DMOMeshTet(xyz, tets)
-    opt = vsdmo.DMOTetClass(gm, n_iter=1, fix_boundary=False)
+@pytest.mark.parametrize("kind", ["tet", "hex"])
+def test_free_boundary_against_fp64_reference(oracle_mod, vsdmo, kind):
+    """The boundary passes of one iteration against the literal double restatement: from the
+    positions after the interior classes (the f32 restatement's, bitwise the product's), the
+    free boundary classes and the feature classes in double; positions within 1e-5 h wherever
+    the double decisions are clear (a vertex is comparable when its own decisions and those of
+    the boundary vertices of its volume ring are)."""
+    xyz, el, h = jittered_cube(kind)
+    et, Mesh, Opt = _classes(vsdmo, kind)
+    om = oracle_mod.OracleMesh(et, xyz, el)
+    gm = Mesh(xyz, el)
+    opt = Opt(gm, n_iter=1, fix_boundary=False)
     x32 = om.xyz
-    x = x32.astype(np.float64)
-    assert om.element_qualities_f64(x).min() > 0
+    assert om.element_qualities_f64(x32.astype(np.float64)).min() > 0
+    xi = x32
+    for v0, v1 in _ranges(om.array(oracle_mod.A_COL_INNER)):
+        xi = om.dmo_color_f32(xi, v0, v1)
+    x = xi.astype(np.float64)
+    nS = om.info["nSurf"]
     rp = om.array(oracle_mod.A_HF_ROWPTR)
-    hf = om.array(oracle_mod.A_HALFFACES).reshape(-1, 3)
+    hf = om.array(oracle_mod.A_HALFFACES).reshape(-1, 7 if kind == "hex" else 3)
     clear = np.ones(len(x), bool)
 
     def ring_clear(v0, v1):
         for v in range(v0, v1):
             clear[v] &= bool(np.all(clear[hf[rp[v]:rp[v + 1]].ravel()]))
 
-    for v0, v1 in _ranges(om.array(oracle_mod.A_COL_INNER)):
-        x, mg = om.dmo_color_f64(x, v0, v1)
-        clear[v0:v1] &= mg > 1e-5
     x0, ls, nn, vn = om.surface_state_f64(x32)
     fn = om.array(oracle_mod.A_FACE_NORMALS).reshape(-1, 3).astype(np.float64)
     sectors = om.sector_surfaces(x32, fn, dtype=np.float64)
     for v0, v1 in _ranges(om.array(oracle_mod.A_COL_FREE)):
-        x, mg = om.dmo_tet_surf_f64(x, x0, ls, nn, sectors, v0, v1)
+        x, mg = om.dmo_vol_surf_f64(x, x0, ls, nn, sectors, v0, v1)
         clear[v0:v1] &= mg > 1e-5
         ring_clear(v0, v1)
     fdeg, flags = om.feature_flags(x32)
@@ -147,19 +160,23 @@ def test_tet_free_boundary_against_fp64_reference(oracle_mod, vsdmo):
         clear[v0:v1] &= mg > 1e-5
         ring_clear(v0, v1)
     opt.iterate(1)
-    d = np.abs(gm.positions().astype(np.float64) - x).max(1)
-    assert np.all(d[clear] < 1e-5 * h), float(d[clear].max())
-    nS = om.info["nSurf"]
-    assert clear[:nS].sum() > 0.5 * nS
+    g = gm.positions()
+    assert same_bits(g[nS:], xi[nS:])
+    d = np.abs(g[:nS].astype(np.float64) - x[:nS]).max(1)
+    c = clear[:nS]
+    assert np.all(d[c] < 1e-5 * h), float(d[c].max())
+    assert c.sum() > 0.5 * nS
     assert np.any(x[:nS] != x32[:nS])
 
 
-def test_tet_boundary_fixed_by_default(vsdmo):
-    xyz, tets = jittered_tet_cube()
-    gm = vsdmo.DMOMeshTet(xyz, tets)
+@pytest.mark.parametrize("kind", ["tet", "hex"])
+def test_boundary_fixed_by_default(vsdmo, kind):
+    xyz, el, _ = jittered_cube(kind)
+    _, Mesh, Opt = _classes(vsdmo, kind)
+    gm = Mesh(xyz, el)
     nS = gm.info["nSurf"]
     x = gm.positions()
-    vsdmo.DMOTetClass(gm, n_iter=2).optimize()
+    Opt(gm, n_iter=2).optimize()
     g = gm.positions()
     assert np.array_equal(g[:nS], x[:nS]) and np.any(g[nS:] != x[nS:])
 
@@ -167,7 +184,7 @@ def test_tet_boundary_fixed_by_default(vsdmo):
 def test_tet_boundary_pass_waits_for_a_valid_mesh(oracle_mod, vsdmo):
     """With an inverted tet at the start the boundary stays where it is in the first iteration
     and the interior classes still move."""
-    xyz, tets = jittered_tet_cube()
+    xyz, tets, _ = jittered_cube("tet")
     gm0 = vsdmo.DMOMeshTet(xyz, tets)
     nS = gm0.info["nSurf"]
     # push an interior vertex through a neighbouring boundary face
@@ -187,17 +204,10 @@ def test_tet_boundary_pass_waits_for_a_valid_mesh(oracle_mod, vsdmo):
 def test_tet_free_boundary_with_active_set(vsdmo):
     """The active set skips only searches whose result cannot change: with the boundary passes
     (which move vertices of interior rings) the positions equal those of the full search."""
-    xyz, tets = jittered_tet_cube()
+    xyz, tets, _ = jittered_cube("tet")
     out = []
     for active in (False, True):
         gm = vsdmo.DMOMeshTet(xyz, tets)
         vsdmo.DMOTetClass(gm, n_iter=6, fix_boundary=False, active_set=active).optimize()
         out.append(gm.positions())
     assert same_bits(out[0], out[1])
-
-
-def test_hex_free_boundary_unsupported(vsdmo):
-    xyz, hexes = G.hex_cube(3, seed=None)
-    gm = vsdmo.DMOMeshHex(xyz, hexes)
-    with pytest.raises(Exception, match="boundary passes of hex meshes"):
-        vsdmo.DMOHexClass(gm, n_iter=1, fix_boundary=False)

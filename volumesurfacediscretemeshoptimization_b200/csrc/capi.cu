@@ -101,20 +101,21 @@ void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
         o->model->m.infer_tet(m.pos.p, o->nb.p, o->nbn.p, o->nb_base, o->nb_base, m.nV - o->nb_base, o->Yall.p,
                               mlp::OUTP, s);
     for (int c = 0; c < (int)o->ranges.size(); ++c) launch_color(o, c, s);
-    if (o->tetsurf) {
-        // boundary passes of a tet mesh, only while the last minimum quality is positive
-        // (DMOTetClass::doIteration, dmo/DMOTet.cu:128-170): free boundary classes on their
-        // surfaces, feature classes on their curves
+    if (o->volsurf) {
+        // boundary passes of a volume mesh, only while the last minimum quality is positive
+        // (DMOTetClass::doIteration, dmo/DMOTet.cu:128-170; DMOHexClass::doIteration,
+        // dmo/DMOHex.cu:131-185): free boundary classes on their surfaces, feature classes on
+        // their curves
         SectorSurfaces sec{o->srow.p, o->stab.p, o->FS.p, o->Xs.p};
         for (const auto& r : o->sranges) {
             DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
             if (o->feat) VSDMO_CUDA(cudaMemcpyAsync(o->Xs.p, m.pos.p, sizeof(float4) * m.nSurf, cudaMemcpyDeviceToDevice, s));
-            launch_dmo_surf_tet(m, L, o->X0.p, o->LS.p, o->nn.p, o->feat ? &sec : nullptr, o->stats.p, o->d_iter.p, s);
+            launch_dmo_surf_vol(m, L, o->X0.p, o->LS.p, o->nn.p, o->feat ? &sec : nullptr, o->stats.p, o->d_iter.p, s);
         }
         if (o->pass1d)
             for (const auto& r : o->franges) {
                 DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
-                launch_dmo_1d_tet(m, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p, o->stats.p, o->d_iter.p, s);
+                launch_dmo_1d_vol(m, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p, o->stats.p, o->d_iter.p, s);
             }
         launch_mark_rings(m, 0, m.nSurf, o->dirty.p, s);
         launch_update_nn(m, o->X0.p, o->nn.p, s);
@@ -149,7 +150,7 @@ __global__ void k_surface_state(const float4* pos, int nS, float4* X0, int* nn) 
 void init_surface_state(vsdmo_opt_s* o) {
     const Mesh& m = o->mesh->m;
     cudaStream_t s = m.stream;
-    const bool surfaces = o->mode == MODE_SURF || o->tetsurf;
+    const bool surfaces = o->mode == MODE_SURF || o->volsurf;
     if (!o->X0.p) {
         o->X0.alloc(m.nSurf, s);
         o->nn.alloc(m.nSurf, s);
@@ -467,7 +468,7 @@ VSDMO_API vsdmo_status vsdmo_mesh_set_positions(vsdmo_mesh_t mesh, const float* 
 namespace {
 vsdmo_status surface_points(vsdmo_opt_t o, int estimate_mode, int vid, int nu, int nv, float* out, int mem_space) {
     if (!o || !out) return fail(VSDMO_E_ARG, "null argument");
-    if (o->mode != MODE_SURF && !o->tetsurf) return fail(VSDMO_E_ARG, "not a surface optimiser");
+    if (o->mode != MODE_SURF && !o->volsurf) return fail(VSDMO_E_ARG, "not a surface optimiser");
     const Mesh& m = o->mesh->m;
     if (vid < 0 || vid >= m.nSurf) return fail(VSDMO_E_ARG, "vid must be a surface vertex (internal numbering)");
     if (nu < 2 || nv < 2 || (long)nu * nv > (1L << 24)) return fail(VSDMO_E_ARG, "nu, nv must be >= 2 (at most 2^24 samples)");
@@ -541,9 +542,9 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         if (!p.fix_boundary) {
             // the boundary vertices move on the boundary surface (and feature vertices on their
             // feature curves) after the interior classes, like DMOTetClass
-            if (m.maxTets > surf_tet_max_ring() || m.maxHE > dmo_surf_max_ring())
+            if (m.maxTets > surf_vol_max_ring(VSDMO_TET) || m.maxHE > dmo_surf_max_ring())
                 return fail(VSDMO_E_VALENCE, "a boundary vertex's ring exceeds the boundary kernels' budget");
-            o->tetsurf = true;
+            o->volsurf = true;
             for (int c = 0; c < m.nColFree; ++c) o->sranges.push_back({m.col_free[c], m.col_free[c + 1]});
             if (m.nFeature > 0) {
                 o->feat = o->pass1d = true;
@@ -551,11 +552,21 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
             }
         }
     } else if (m.type == VSDMO_HEX) {
-        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "boundary passes of hex meshes are not implemented; set fix_boundary=1");
         if (m.maxTets > dmo_hex_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more hexahedra than the kernel's ring budget");
         o->mode = MODE_HEX;
         o->kind = MK_HEX;
         for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
+        if (!p.fix_boundary) {
+            // boundary and feature passes after the interior classes, like DMOHexClass
+            if (m.maxTets > surf_vol_max_ring(VSDMO_HEX) || m.maxHE > dmo_surf_max_ring())
+                return fail(VSDMO_E_VALENCE, "a boundary vertex's ring exceeds the boundary kernels' budget");
+            o->volsurf = true;
+            for (int c = 0; c < m.nColFree; ++c) o->sranges.push_back({m.col_free[c], m.col_free[c + 1]});
+            if (m.nFeature > 0) {
+                o->feat = o->pass1d = true;
+                for (int c = 0; c < m.nColFeature; ++c) o->franges.push_back({m.col_feature[c], m.col_feature[c + 1]});
+            }
+        }
     } else if (m.type == VSDMO_TRI && flat2d && p.grid_n == 8) {
         if (m.maxHE > dmo_tri2d_max_ring() || (!p.fix_boundary && m.maxHE > dmo_surf_max_ring()))
             return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
@@ -598,8 +609,8 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->done.alloc(1, s); o->done.zero();
         prepare_dmo_kernels();
         if (o->mode == MODE_ANGLE) prepare_angle_kernels();
-        if (o->tetsurf) prepare_surf_kernels();
-        if (o->mode == MODE_SURF || o->slide || o->tetsurf) init_surface_state(o.get());
+        if (o->volsurf) prepare_surf_kernels();
+        if (o->mode == MODE_SURF || o->slide || o->volsurf) init_surface_state(o.get());
         o->counters.alloc(4, s);
         o->counters.zero();
         if (o->mode == MODE_TET && p.active_set) {
@@ -656,7 +667,7 @@ VSDMO_API vsdmo_status vsdmo_opt_restart(vsdmo_opt_t o) {
         const Mesh& m = o->mesh->m;
         o->iters_done = 0;
         o->d_iter.zero();
-        if (o->mode == MODE_SURF || o->slide || o->tetsurf) init_surface_state(o);
+        if (o->mode == MODE_SURF || o->slide || o->volsurf) init_surface_state(o);
         o->counters.zero();
         if (o->dirty.p) o->dirty.fill_bytes(1);
         launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1,
@@ -680,8 +691,8 @@ VSDMO_API int vsdmo_opt_iterations_done(vsdmo_opt_t o) { return o ? o->iters_don
 VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t o) {
     if (!o) return -1;
     // colour launches + quality kernel (+ nearest-neighbour walk and two normal kernels)
-    return (int)o->ranges.size() + 1 + (o->mode == MODE_SURF || o->tetsurf ? 3 : 0) + (o->slide ? 1 : 0) +
-           (o->tetsurf && o->dirty.p ? 1 : 0) +
+    return (int)o->ranges.size() + 1 + (o->mode == MODE_SURF || o->volsurf ? 3 : 0) + (o->slide ? 1 : 0) +
+           (o->volsurf && o->dirty.p ? 1 : 0) +
            (o->pass1d ? (int)o->franges.size() : 0) + (int)o->sranges.size();
 }
 
@@ -709,7 +720,7 @@ VSDMO_API vsdmo_status vsdmo_opt_feature_state(vsdmo_opt_t o, float* curves, int
 VSDMO_API vsdmo_status vsdmo_opt_surface_state(vsdmo_opt_t o, float* xyz_init, float* local_surfaces,
                                                int32_t* nearest) {
     if (!o) return fail(VSDMO_E_ARG, "null optimiser");
-    if (o->mode != MODE_SURF && !o->slide && !o->tetsurf) return fail(VSDMO_E_ARG, "not a surface optimiser");
+    if (o->mode != MODE_SURF && !o->slide && !o->volsurf) return fail(VSDMO_E_ARG, "not a surface optimiser");
     if (local_surfaces && !o->LS.p) return fail(VSDMO_E_ARG, "this optimiser has no local surfaces");
     return guarded([&] {
         const Mesh& m = o->mesh->m;

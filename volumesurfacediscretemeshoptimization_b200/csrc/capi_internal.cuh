@@ -27,7 +27,7 @@ struct vsdmo_opt_s {
     // feature / boundary pass: slide = flat triangles with sliding boundary vertices; feat = the
     // mesh has feature vertices (surface: sector surfaces always, the 1D pass unless fix_boundary)
     bool slide = false, feat = false, pass1d = false;
-    bool tetsurf = false;                      // tet mesh with its boundary passes (fix_boundary = 0)
+    bool volsurf = false;                      // tet / hex mesh with its boundary passes (fix_boundary = 0)
     std::vector<std::pair<int, int>> sranges;  // free boundary colour classes of a tet mesh
     DBuf<float4> LS1;                          // curves of the feature vertices [3 nSurf]
     DBuf<int> fdeg;                            // feature ring vertices [nSurf]

@@ -34,6 +34,7 @@
 // --fmad=false here and without contraction there).
 #include "vsdmo_internal.cuh"
 #include "tet_key.cuh"
+#include "hex_key.cuh"
 #include <algorithm>
 #include <cfloat>
 
@@ -47,6 +48,7 @@ constexpr float SURF_EPS = 1.19209e-07f;   // EPSILON of the reference's surface
 constexpr int SECT_TABLE = 20;              // TABLE_SIZE of dmo/surfaceP/SurfaceCommon.h: halfedges of a feature vertex
 constexpr int SECT_LIST = 40;               // MAX_NEIGHBORS: points of one sector
 constexpr int TET_SURF_MAX_RING = 256;      // tets of a boundary vertex in the boundary passes
+constexpr int HEX_SURF_MAX_RING = 64;       // hexahedra of a boundary vertex in the boundary passes
 
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
     return (ax * bx + ay * by) + az * bz;
@@ -288,52 +290,122 @@ __device__ __forceinline__ const float4* neighbour_surface(int v, int nnN, const
     return FS + 4L * (srow[nnN - nFree] + stab[SECT_TABLE * (nnN - nFree) + arg]);
 }
 
-// the ring of tets of vertex v, scaled by 2^-ex like the interior search: coefficients in co
-// (2 per tet); returns false for a degenerate ring. md: the largest distance to a ring point.
-__device__ __forceinline__ bool stage_tets(const float4* __restrict__ pos, const int* __restrict__ hf_rowptr,
-                                           const int4* __restrict__ hf, int v, float4 c0, int lane, float4* co,
-                                           int& kt, float& md, int& ex, float& pinv) {
-    const int b = hf_rowptr[v];
-    kt = hf_rowptr[v + 1] - b;
-    float mm = 0.f, me = -FLT_MAX;
-    for (int t = lane; t < kt; t += 32) {
-        const int4 h = hf[b + t];
-        const int ids[3] = { h.x, h.y, h.z };
+// Volume rings of a boundary vertex for the boundary passes of volume meshes. stage() reads
+// the vertex's ring from pos, scales it by 2^-ex like the interior search (ex from the largest
+// per-axis ring distance) and writes its coefficients to co; key(p) is the ring key at the
+// absolute position p; md is the grid extent of the reference kernel. stage() returns false
+// for a degenerate ring.
+struct TetRing {
+    // k_optimizeHierarchical2DTet / 1DTet: extent = largest distance to a ring point
+    // (dmo/DMOTetImplCub.h:246, 455); 2 float4 of coefficients per tet (tet_key.cuh)
+    static constexpr int F4 = 2;
+    const float4* co;
+    int k, ex;
+    float pinv, md;
+    float4 c0;
+    __device__ bool stage(const float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
+                          int v, float4 c, int lane, float4* buf) {
+        c0 = c;
+        co = buf;
+        const int b = rowptr[v];
+        k = rowptr[v + 1] - b;
+        float mm = 0.f, me = -FLT_MAX;
+        for (int t = lane; t < k; t += 32) {
+            const int4 h = hf[b + t];
+            const int ids[3] = { h.x, h.y, h.z };
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const float4 q = pos[ids[j]];
-            const float dx = q.x - c0.x, dy = q.y - c0.y, dz = q.z - c0.z;
-            mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
-            me = fmaxf(me, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+            for (int j = 0; j < 3; ++j) {
+                const float4 q = pos[ids[j]];
+                const float dx = q.x - c0.x, dy = q.y - c0.y, dz = q.z - c0.z;
+                mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
+                me = fmaxf(me, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+            }
         }
-    }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        mm = fmaxf(mm, __shfl_xor_sync(FULL, mm, o));
-        me = fmaxf(me, __shfl_xor_sync(FULL, me, o));
+        for (int o = 16; o; o >>= 1) {
+            mm = fmaxf(mm, __shfl_xor_sync(FULL, mm, o));
+            me = fmaxf(me, __shfl_xor_sync(FULL, me, o));
+        }
+        md = me;
+        if (!(mm > 0.f) || !(mm < FLT_MAX)) return false;
+        (void)frexpf(mm, &ex);
+        pinv = exp2_exact(-ex);
+        for (int t = lane; t < k; t += 32) {
+            const int4 h = hf[b + t];
+            const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
+            float4 K0, K1;
+            tet_coeffs(scale2(pa.x - c0.x, pinv, -ex), scale2(pa.y - c0.y, pinv, -ex), scale2(pa.z - c0.z, pinv, -ex),
+                       scale2(pb.x - c0.x, pinv, -ex), scale2(pb.y - c0.y, pinv, -ex), scale2(pb.z - c0.z, pinv, -ex),
+                       scale2(pc.x - c0.x, pinv, -ex), scale2(pc.y - c0.y, pinv, -ex), scale2(pc.z - c0.z, pinv, -ex),
+                       K0, K1);
+            buf[2 * t] = K0;
+            buf[2 * t + 1] = K1;
+        }
+        __syncwarp();
+        return true;
     }
-    md = me;
-    if (!(mm > 0.f) || !(mm < FLT_MAX)) return false;
-    (void)frexpf(mm, &ex);
-    pinv = exp2_exact(-ex);
-    for (int t = lane; t < kt; t += 32) {
-        const int4 h = hf[b + t];
-        const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
-        float4 K0, K1;
-        tet_coeffs(scale2(pa.x - c0.x, pinv, -ex), scale2(pa.y - c0.y, pinv, -ex), scale2(pa.z - c0.z, pinv, -ex),
-                   scale2(pb.x - c0.x, pinv, -ex), scale2(pb.y - c0.y, pinv, -ex), scale2(pb.z - c0.z, pinv, -ex),
-                   scale2(pc.x - c0.x, pinv, -ex), scale2(pc.y - c0.y, pinv, -ex), scale2(pc.z - c0.z, pinv, -ex), K0, K1);
-        co[2 * t] = K0;
-        co[2 * t + 1] = K1;
+    __device__ float key(float px, float py, float pz) const {
+        return tet_key1(co, k, scale2(px - c0.x, pinv, -ex), scale2(py - c0.y, pinv, -ex), scale2(pz - c0.z, pinv, -ex));
     }
-    __syncwarp();
-    return true;
-}
+};
 
-__device__ __forceinline__ float tet_key_at(const float4* co, int kt, float4 c0, float pinv, int ex, float px, float py,
-                                            float pz) {
-    return tet_key1(co, kt, scale2(px - c0.x, pinv, -ex), scale2(py - c0.y, pinv, -ex), scale2(pz - c0.z, pinv, -ex));
-}
+struct HexRing {
+    // k_optimizeHierarchical2DHex / 1DHex: extent = smallest distance to a ring point
+    // (dmo/DMOHexImplCub.h:246, 448); 43 floats of coefficients per halfhex (hex_key.cuh)
+    static constexpr int F4 = HEX_CO / 4;
+    const float* co;
+    int k, ex;
+    float pinv, md, es, ea;
+    float4 c0;
+    __device__ bool stage(const float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hh,
+                          int v, float4 c, int lane, float4* buf) {
+        c0 = c;
+        float* cf = reinterpret_cast<float*>(buf);
+        co = cf;
+        const int b = rowptr[v];
+        k = rowptr[v + 1] - b;
+        float mm = 0.f, me = FLT_MAX;
+        for (int idx = lane; idx < 7 * k; idx += 32) {
+            const int h = idx / 7, c7 = idx % 7;
+            const int4 q = hh[2 * (b + h) + (c7 >> 2)];
+            const int cc = c7 & 3;
+            const float4 p = pos[cc == 0 ? q.x : (cc == 1 ? q.y : (cc == 2 ? q.z : q.w))];
+            const float dx = p.x - c0.x, dy = p.y - c0.y, dz = p.z - c0.z;
+            mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
+            me = fminf(me, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            mm = fmaxf(mm, __shfl_xor_sync(FULL, mm, o));
+            me = fminf(me, __shfl_xor_sync(FULL, me, o));
+        }
+        md = me;
+        if (!(mm > 0.f) || !(mm < FLT_MAX)) return false;
+        (void)frexpf(mm, &ex);
+        pinv = exp2_exact(-ex);
+        es = ldexpf(HEX_EPS, -3 * ex);
+        ea = ldexpf(HEX_EPS, -2 * ex);
+        for (int h = lane; h < k; h += 32) {
+            const int4 qa = hh[2 * (b + h)], qb = hh[2 * (b + h) + 1];
+            const int us[7] = { qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z };
+            float r[7][3];
+#pragma unroll
+            for (int c7 = 0; c7 < 7; ++c7) {
+                const float4 p = pos[us[c7]];
+                r[c7][0] = scale2(p.x - c0.x, pinv, -ex);
+                r[c7][1] = scale2(p.y - c0.y, pinv, -ex);
+                r[c7][2] = scale2(p.z - c0.z, pinv, -ex);
+            }
+            hex_coeffs(r, es, ea, cf + HEX_CO * h);
+        }
+        __syncwarp();
+        return true;
+    }
+    __device__ float key(float px, float py, float pz) const {
+        return hex_key1(co, k, scale2(px - c0.x, pinv, -ex), scale2(py - c0.y, pinv, -ex), scale2(pz - c0.z, pinv, -ex),
+                        es, ea);
+    }
+};
 
 template <int FK>
 __global__ void __launch_bounds__(SURF_WARPS * 32)
@@ -748,11 +820,14 @@ k_dmo_1d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* _
     if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
 }
 
-// Boundary-surface pass of a tet mesh (k_optimizeHierarchical2DTet, dmo/DMOTetImplCub.h:140-325):
-// the surface search of k_dmo_surf over the boundary vertex's surface ring, judged by the key of
-// the vertex's ring of tets; only while the last minimum quality is positive (dmo/DMOTet.cu:139).
+// Boundary-surface pass of a volume mesh (k_optimizeHierarchical2DTet,
+// dmo/DMOTetImplCub.h:142-325; k_optimizeHierarchical2DHex, dmo/DMOHexImplCub.h:142-317): the
+// surface search of k_dmo_surf over the boundary vertex's surface ring, judged by the key of the
+// vertex's volume ring; only while the last minimum quality is positive (dmo/DMOTet.cu:139,
+// dmo/DMOHex.cu:152).
+template <class R>
 __global__ void __launch_bounds__(SURF_WARPS * 32)
-k_dmo_surf_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
+k_dmo_surf_vol(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
                const int* __restrict__ hf_rowptr, const int4* __restrict__ hf, const float4* __restrict__ X0,
                const float4* __restrict__ LS, const int* __restrict__ nn, int v0, int v1, float grid_scale, int depth,
                int maxkt, int maxks, const int* __restrict__ srow, const int* __restrict__ stab,
@@ -765,13 +840,13 @@ k_dmo_surf_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
     if (!(stats[*iter].min_q > 0.f)) return;
     const int b = rowptr[v], ks = rowptr[v + 1] - b;
     if (ks <= 0 || ks > maxks || hf_rowptr[v + 1] - hf_rowptr[v] > maxkt) return;
-    float4* co = sst + (size_t)warp * (2 * maxkt + 5 * maxks);
-    float4* nbL = co + 2 * maxkt;
+    float4* co = sst + (size_t)warp * (R::F4 * maxkt + 5 * maxks);
+    float4* nbL = co + R::F4 * maxkt;
     float4* nbX = nbL + 4 * maxks;
     const float4 c0 = pos[v];
-    int kt, ex;
-    float md, pinv;
-    if (!stage_tets(pos, hf_rowptr, hf, v, c0, lane, co, kt, md, ex, pinv)) return;
+    R ring;
+    if (!ring.stage(pos, hf_rowptr, hf, v, c0, lane, co)) return;
+    const float md = ring.md;
     for (int i = lane; i < ks; i += 32) {
         const int nnN = nn[he[b + i].x];
         const float4* Ls = neighbour_surface(v, nnN, LS, rowptr, he, srow, stab, FS, Xs, nFree);
@@ -789,7 +864,7 @@ k_dmo_surf_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
         cu = dot3(dx, dy, dz, L.l1.x, L.l1.y, L.l1.z);
         cv = dot3(dx, dy, dz, L.l2.x, L.l2.y, L.l2.z);
     }
-    const float qOld = tet_key_at(co, kt, c0, pinv, ex, c0.x, c0.y, c0.z);
+    const float qOld = ring.key(c0.x, c0.y, c0.z);
     const int i1 = lane >> 3, j1 = lane & 7, i2 = i1 + 4;
     const float o1 = (float)(7 - 2 * i1) / 7.f, oj = (float)(7 - 2 * j1) / 7.f, o2 = (float)(7 - 2 * i2) / 7.f;
     float cx = c0.x, cy = c0.y, cz = c0.z;
@@ -799,8 +874,8 @@ k_dmo_surf_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
         const float u1 = fmaf(o1, S, cu), vv = fmaf(oj, S, cv), u2 = fmaf(o2, S, cu);
         const float3 p1 = estimate(L, x0, nbL, nbX, ks, u1, vv);
         const float3 p2 = estimate(L, x0, nbL, nbX, ks, u2, vv);
-        const float q1 = tet_key_at(co, kt, c0, pinv, ex, p1.x, p1.y, p1.z);
-        const float q2 = tet_key_at(co, kt, c0, pinv, ex, p2.x, p2.y, p2.z);
+        const float q1 = ring.key(p1.x, p1.y, p1.z);
+        const float q2 = ring.key(p2.x, p2.y, p2.z);
         const bool second = q2 > q1;
         const float val = second ? q2 : q1;
         float bv = __shfl_sync(FULL, val, 0);
@@ -809,7 +884,7 @@ k_dmo_surf_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
             const float vt = __shfl_sync(FULL, val, t);
             if (vt > bv) { bv = vt; bt = t; }
         }
-        const float qLast = tet_key_at(co, kt, c0, pinv, ex, cx, cy, cz);
+        const float qLast = ring.key(cx, cy, cz);
         const float bu = __shfl_sync(FULL, second ? u2 : u1, bt);
         const float bw = __shfl_sync(FULL, vv, bt);
         const float bx = __shfl_sync(FULL, second ? p2.x : p1.x, bt);
@@ -822,10 +897,12 @@ k_dmo_surf_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
     if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
 }
 
-// 1D pass of the feature vertices on a tet mesh's boundary (k_optimizeHierarchical1DTet,
-// dmo/DMOTetImplCub.h:327-494): k_dmo_1d with the key of the ring of tets
+// 1D pass of the feature vertices on a volume mesh's boundary (k_optimizeHierarchical1DTet,
+// dmo/DMOTetImplCub.h:327-494; k_optimizeHierarchical1DHex, dmo/DMOHexImplCub.h:319-487):
+// k_dmo_1d with the key of the vertex's volume ring
+template <class R>
 __global__ void __launch_bounds__(SURF_WARPS * 32)
-k_dmo_1d_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
+k_dmo_1d_vol(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
              const int* __restrict__ hf_rowptr, const int4* __restrict__ hf, const float4* __restrict__ X0,
              const float4* __restrict__ LS1, const int* __restrict__ nn, const int* __restrict__ fdeg,
              const uint8_t* __restrict__ opt, int nFree, int v0, int v1, float grid_scale, int maxkt, int maxks,
@@ -837,12 +914,12 @@ k_dmo_1d_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int
     if (!(stats[*iter].min_q > 0.f)) return;
     const int b = rowptr[v], ks = rowptr[v + 1] - b;
     if (ks <= 0 || ks > maxks || hf_rowptr[v + 1] - hf_rowptr[v] > maxkt) return;
-    float4* co = s1t + (size_t)warp * (2 * maxkt + (maxks + 3) / 4);
-    int* surf = reinterpret_cast<int*>(co + 2 * maxkt);
+    float4* co = s1t + (size_t)warp * (R::F4 * maxkt + (maxks + 3) / 4);
+    int* surf = reinterpret_cast<int*>(co + R::F4 * maxkt);
     const float4 c0 = pos[v];
-    int kt, ex;
-    float md, pinv;
-    if (!stage_tets(pos, hf_rowptr, hf, v, c0, lane, co, kt, md, ex, pinv)) return;
+    R ring;
+    if (!ring.stage(pos, hf_rowptr, hf, v, c0, lane, co)) return;
+    const float md = ring.md;
     int ns = 0;
     for (int base = 0; base < ks; base += 32) {
         const int i = base + lane;
@@ -872,7 +949,7 @@ k_dmo_1d_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int
         float q = -FLT_MAX;
         if (lane < 8) {
             p = est1d(LS1, X0, nn, nnv, surf, ns, u);
-            q = tet_key_at(co, kt, c0, pinv, ex, p.x, p.y, p.z);
+            q = ring.key(p.x, p.y, p.z);
         }
         float bv = __shfl_sync(FULL, q, 0);
         int bt = 0;
@@ -880,14 +957,14 @@ k_dmo_1d_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int
             const float qt = __shfl_sync(FULL, q, t);
             if (qt > bv) { bv = qt; bt = t; }
         }
-        const float qLast = tet_key_at(co, kt, c0, pinv, ex, cx, cy, cz);
+        const float qLast = ring.key(cx, cy, cz);
         const float bu = __shfl_sync(FULL, u, bt);
         const float bx = __shfl_sync(FULL, p.x, bt), by = __shfl_sync(FULL, p.y, bt), bz = __shfl_sync(FULL, p.z, bt);
         if (qLast < bv) { cx = bx; cy = by; cz = bz; cu = bu; }
         lastMax = bv;
         ds = ds * (2.f / 7.f);
     }
-    const float qOld = tet_key_at(co, kt, c0, pinv, ex, c0.x, c0.y, c0.z);
+    const float qOld = ring.key(c0.x, c0.y, c0.z);
     if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
 }
 
@@ -1030,38 +1107,50 @@ int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>&
     return nSect;
 }
 
-void launch_dmo_surf_tet(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
+// ring array and per-element shared memory of a volume mesh's boundary passes
+static const int4* vol_ring(const Mesh& m) { return m.type == VSDMO_HEX ? m.hh.p : m.hf.p; }
+
+void launch_dmo_surf_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
                          const SectorSurfaces* sec, const IterStats* gate_stats, const int* gate_iter, cudaStream_t s) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
+    const bool hex = m.type == VSDMO_HEX;
+    const int f4 = hex ? HexRing::F4 : TetRing::F4;
     const int maxkt = std::max(m.maxTets, 1), maxks = std::max(m.maxHE, 1);
-    const size_t smem = (size_t)SURF_WARPS * (2 * maxkt + 5 * maxks) * sizeof(float4);
-    k_dmo_surf_tet<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
-        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, m.hf.p, X0, LS, nn, L.v0, L.v1, L.grid_scale, L.depth, maxkt, maxks,
-        sec ? sec->srow : nullptr, sec ? sec->stab : nullptr, sec ? sec->FS : nullptr, sec ? sec->Xs : nullptr,
+    const size_t smem = (size_t)SURF_WARPS * (f4 * maxkt + 5 * maxks) * sizeof(float4);
+    auto k = hex ? k_dmo_surf_vol<HexRing> : k_dmo_surf_vol<TetRing>;
+    k<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
+        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, vol_ring(m), X0, LS, nn, L.v0, L.v1, L.grid_scale, L.depth, maxkt,
+        maxks, sec ? sec->srow : nullptr, sec ? sec->stab : nullptr, sec ? sec->FS : nullptr, sec ? sec->Xs : nullptr,
         m.nSurf - m.nFeature, gate_stats, gate_iter);
     VSDMO_CHECK_LAUNCH();
 }
 
-void launch_dmo_1d_tet(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
+void launch_dmo_1d_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
                        const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
                        cudaStream_t s) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
+    const bool hex = m.type == VSDMO_HEX;
+    const int f4 = hex ? HexRing::F4 : TetRing::F4;
     const int maxkt = std::max(m.maxTets, 1), maxks = std::max(m.maxHE, 1);
-    const size_t smem = (size_t)SURF_WARPS * (2 * maxkt + (maxks + 3) / 4) * sizeof(float4);
-    k_dmo_1d_tet<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
-        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, m.hf.p, X0, LS1, nn, fdeg, opt, m.nSurf - m.nFeature, L.v0, L.v1,
-        L.grid_scale, maxkt, maxks, gate_stats, gate_iter);
+    const size_t smem = (size_t)SURF_WARPS * (f4 * maxkt + (maxks + 3) / 4) * sizeof(float4);
+    auto k = hex ? k_dmo_1d_vol<HexRing> : k_dmo_1d_vol<TetRing>;
+    k<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
+        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, vol_ring(m), X0, LS1, nn, fdeg, opt, m.nSurf - m.nFeature, L.v0,
+        L.v1, L.grid_scale, maxkt, maxks, gate_stats, gate_iter);
     VSDMO_CHECK_LAUNCH();
 }
 
-int surf_tet_max_ring() { return TET_SURF_MAX_RING; }
+int surf_vol_max_ring(int elem_type) { return elem_type == VSDMO_HEX ? HEX_SURF_MAX_RING : TET_SURF_MAX_RING; }
 
 void prepare_surf_kernels() {
-    const int mx = (int)((size_t)SURF_WARPS * (2 * TET_SURF_MAX_RING + 5 * SURF_MAX_RING) * sizeof(float4));
-    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_surf_tet, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_tet, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    const int tet = (int)((size_t)SURF_WARPS * (TetRing::F4 * TET_SURF_MAX_RING + 5 * SURF_MAX_RING) * sizeof(float4));
+    const int hex = (int)((size_t)SURF_WARPS * (HexRing::F4 * HEX_SURF_MAX_RING + 5 * SURF_MAX_RING) * sizeof(float4));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_surf_vol<TetRing>, cudaFuncAttributeMaxDynamicSharedMemorySize, tet));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_vol<TetRing>, cudaFuncAttributeMaxDynamicSharedMemorySize, tet));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_surf_vol<HexRing>, cudaFuncAttributeMaxDynamicSharedMemorySize, hex));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_vol<HexRing>, cudaFuncAttributeMaxDynamicSharedMemorySize, hex));
 }
 
 void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,

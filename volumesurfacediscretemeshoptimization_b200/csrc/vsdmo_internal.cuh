@@ -194,14 +194,15 @@ void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const 
 void init_feature_state(const Mesh& m, int flat, float4* LS1, int* fdeg, uint8_t* opt, cudaStream_t s);
 // per-sector surfaces; returns the sector count (VSDMO_E_VALENCE beyond the table sizes)
 int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>& FS, cudaStream_t s);
-// Boundary passes of a tet mesh (run only while the last minimum quality is positive): one colour
-// class of free boundary vertices on their surfaces, one of feature vertices on their curves.
-void launch_dmo_surf_tet(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
+// Boundary passes of a tet or hex mesh (run only while the last minimum quality is positive):
+// one colour class of free boundary vertices on their surfaces, one of feature vertices on their
+// curves, each judged by the vertex's volume ring.
+void launch_dmo_surf_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
                          const SectorSurfaces* sec, const IterStats* gate_stats, const int* gate_iter, cudaStream_t s);
-void launch_dmo_1d_tet(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
+void launch_dmo_1d_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
                        const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
                        cudaStream_t s);
-int surf_tet_max_ring();
+int surf_vol_max_ring(int elem_type);
 void prepare_surf_kernels();
 // One colour class of feature vertices: mode 0 flat (gated on the last minimum quality being
 // positive when gate_stats is set), 1 surface triangles, 2 surface quads.
