@@ -102,9 +102,9 @@ typedef struct vsdmo_model_s* vsdmo_model_t;
 
 /* Optimiser parameters. Defaults (vsdmo_params_default) follow the reference constructors:
  * DMOTetClass(mesh, MEAN_RATIO, 0.5f, 30)  dmo/DMOTet.h:24,
- * DMOTriFlatClass(mesh, MIN_ANGLE, 0.5f, 30) dmo/DMOTriFlat.h:25 (MEAN_RATIO is the only
- * criterion implemented here so far, and the default), DMO_NQ = 8, DMO_DEPTH = 3
- * (dmo/DMOConfig.h:4-6). */
+ * DMOTriFlatClass(mesh, MIN_ANGLE, 0.5f, 30) dmo/DMOTriFlat.h:25 (the default here is
+ * MEAN_RATIO for every element type; MIN_ANGLE / MAX_ANGLE run on tet and triangle meshes),
+ * DMO_NQ = 8, DMO_DEPTH = 3 (dmo/DMOConfig.h:4-6). */
 typedef struct vsdmo_params {
     int   quality;        /* vsdmo_quality                                                  */
     float grid_scale;     /* initial half-extent factor (0.5)                               */

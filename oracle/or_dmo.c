@@ -603,6 +603,32 @@ static double tri2d_angle64(const double* p0, const double* p1, const double* p2
     if (max_angle) return 1.0 - fmax(fmax(a, b), c) / M_PI;
     return 3.0 * fmin(fmin(a, b), c) / M_PI;
 }
+/* minAngleMetricTri(p, n) / maxAngleMetricTri(p, n) (dmo/DMOQualityTri.h:50-71,166-189); n == NULL:
+ * the unsigned metric (minAngleMetricTri(p), :31-47) */
+double or_q_tri3d_angle_f64(const double* p0, const double* p1, const double* p2, const double* n, int max_angle) {
+    double a0[3], a1[3], b0[3], b1[3], c0[3], c1[3], e0[3], e1[3];
+    for (int i = 0; i < 3; ++i) {
+        a0[i] = p0[i] - p1[i]; a1[i] = p2[i] - p1[i];
+        b0[i] = p1[i] - p2[i]; b1[i] = p0[i] - p2[i];
+        c0[i] = p2[i] - p0[i]; c1[i] = p1[i] - p0[i];
+        e0[i] = p1[i] - p0[i]; e1[i] = p2[i] - p1[i];
+    }
+    const double a = calc_angle(a0, a1, 3), b = calc_angle(b0, b1, 3), c = calc_angle(c0, c1, 3);
+    double q = max_angle ? 1.0 - fmax(fmax(a, b), c) / M_PI : 3.0 * fmin(fmin(a, b), c) / M_PI;
+    if (n) {
+        const double t[3] = { e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2], e0[0] * e1[1] - e0[1] * e1[0] };
+        const double len = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        if ((t[0] / len) * n[0] + (t[1] / len) * n[1] + (t[2] / len) * n[2] < 0.0) q = -q;
+    }
+    return q;
+}
+
+/* the quality criterion of the surface, 1D and boundary restatements (OR_MEAN_RATIO,
+ * OR_MIN_ANGLE, OR_MAX_ANGLE); process-wide test state, set before the calls it governs */
+static int g_criterion = 0;
+void or_set_criterion(int c) { g_criterion = c; }
+int or__criterion(void) { return g_criterion; }
+
 double or_q_tri2d_min_angle_f64(const double* p0, const double* p1, const double* p2) { return tri2d_angle64(p0, p1, p2, 0); }
 double or_q_tri2d_max_angle_f64(const double* p0, const double* p1, const double* p2) { return tri2d_angle64(p0, p1, p2, 1); }
 

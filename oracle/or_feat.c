@@ -203,9 +203,15 @@ static float ringq32(int mode, int k, const float* ring, const float* p, const f
 
 static double ringq64(int mode, int k, const double* ring, const double* p, const double* n) {
     double q = DBL_MAX;
+    const int crit = or__criterion();
     for (int i = 0; i < k; ++i) {
         double v;
-        if (mode == 0) v = or_q_tri2d_mean_ratio_f64(p, ring + 3 * i, ring + 3 * (i + 1));
+        if (mode == 0 && crit != OR_MEAN_RATIO)
+            v = crit == OR_MAX_ANGLE ? or_q_tri2d_max_angle_f64(p, ring + 3 * i, ring + 3 * (i + 1))
+                                     : or_q_tri2d_min_angle_f64(p, ring + 3 * i, ring + 3 * (i + 1));
+        else if (mode == 1 && crit != OR_MEAN_RATIO)
+            v = or_q_tri3d_angle_f64(p, ring + 3 * i, ring + 3 * (i + 1), n, crit == OR_MAX_ANGLE);
+        else if (mode == 0) v = or_q_tri2d_mean_ratio_f64(p, ring + 3 * i, ring + 3 * (i + 1));
         else if (mode == 1) {
             const double* a = ring + 3 * i; const double* b = ring + 3 * (i + 1);
             double e0[3] = { a[0] - p[0], a[1] - p[1], a[2] - p[2] };

@@ -563,7 +563,10 @@ static double ring64(int fk, int k, const double* ring, const double* p, const d
     double q = DBL_MAX;
     for (int i = 0; i < k; ++i) {
         double v;
-        if (fk == 3) {
+        const int crit = or__criterion();
+        if (fk == 3 && crit != OR_MEAN_RATIO) {
+            v = or_q_tri3d_angle_f64(p, ring + 3 * i, ring + 3 * (i + 1), n, crit == OR_MAX_ANGLE);
+        } else if (fk == 3) {
             const double* a = ring + 3 * i; const double* b = ring + 3 * (i + 1);
             double e0[3], e1[3], e2[3];
             for (int c = 0; c < 3; ++c) { e0[c] = a[c] - p[c]; e1[c] = b[c] - p[c]; e2[c] = b[c] - a[c]; }
@@ -855,8 +858,12 @@ void or_surface_qualities_f64(const or_mesh* m, const double* X, double* q) {
     const int* F = or__faces(m);
     for (int t = 0; t < nF; ++t) {
         const int* f = F + fk * (size_t)t;
-        q[t] = fk == 3 ? or_q_tri3d_f64(X + 3 * f[0], X + 3 * f[1], X + 3 * f[2])
-                       : or_q_quad_f64(X + 3 * f[0], X + 3 * f[1], X + 3 * f[2], X + 3 * f[3], NULL);
+        const int crit = or__criterion();
+        if (fk == 3 && crit != OR_MEAN_RATIO)
+            q[t] = or_q_tri3d_angle_f64(X + 3 * f[0], X + 3 * f[1], X + 3 * f[2], NULL, crit == OR_MAX_ANGLE);
+        else
+            q[t] = fk == 3 ? or_q_tri3d_f64(X + 3 * f[0], X + 3 * f[1], X + 3 * f[2])
+                           : or_q_quad_f64(X + 3 * f[0], X + 3 * f[1], X + 3 * f[2], X + 3 * f[3], NULL);
     }
 }
 

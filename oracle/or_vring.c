@@ -7,7 +7,8 @@
  * coefficients once (tets: the 8 of or_dmo.c's tet key; halfhexes: the 43 of or_hex.c's hex
  * key); the key of a candidate p is that of (p - c0) 2^-e.
  * f64 (the reference literally): the ring minimum of the element metric with p as the vertex
- * (qualityTetRing / qualityHexRing, dmo/DMOQualityTet.h, dmo/DMOQualityHex.h:75-112).
+ * (qualityTetRing / qualityHexRing, dmo/DMOQualityTet.h:165-177, dmo/DMOQualityHex.h:75-112), tets
+ * under the criterion of or_set_criterion (mean ratio, min or max angle).
  * Grid extent: tets the LARGEST Euclidean distance to a ring point (dmo/DMOTetImplCub.h:246,
  * 455), hexes the SMALLEST (dmo/DMOHexImplCub.h:246, 448).
  */
@@ -85,9 +86,11 @@ double or__vring64_q(const or_mesh* m, const double* X, int v, const double* p) 
         }
         return q;
     }
+    const int crit = or__criterion();
+    double (*metric)(const double*, const double*, const double*, const double*) =
+        crit == OR_MIN_ANGLE ? or_q_tet_min_angle_f64 : (crit == OR_MAX_ANGLE ? or_q_tet_max_angle_f64 : or_q_tet_mean_ratio_f64);
     for (int i = rp[v]; i < rp[v + 1]; ++i)
-        q = fmin(q, or_q_tet_mean_ratio_f64(p, X + 3 * (size_t)hf[3 * i], X + 3 * (size_t)hf[3 * i + 1],
-                                            X + 3 * (size_t)hf[3 * i + 2]));
+        q = fmin(q, metric(p, X + 3 * (size_t)hf[3 * i], X + 3 * (size_t)hf[3 * i + 1], X + 3 * (size_t)hf[3 * i + 2]));
     return q;
 }
 

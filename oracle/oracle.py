@@ -100,6 +100,8 @@ def lib():
         L.or_dmo_1d_f32.argtypes = [P, P, P, P, P, P, P, P, I, I, F, I]
         L.or_dmo_1d_f64.argtypes = [P, P, P, P, P, P, P, P, I, I, D, P, I]
         L.or_angle_qualities_f64.argtypes = [P, P, I, P]
+        L.or_set_criterion.argtypes = [I]
+        L.or_set_criterion.restype = None
         for n in ("or_q_tet_min_angle_f64", "or_q_tet_max_angle_f64"):
             getattr(L, n).restype = D
             getattr(L, n).argtypes = [P, P, P, P]
@@ -385,6 +387,25 @@ class OracleMesh:
             fn = lib().or_hex_qualities_f32
         fn(self.h, _p(xyz), _p(q))
         return q
+
+
+MEAN_RATIO, MIN_ANGLE, MAX_ANGLE = 0, 4, 6
+
+
+class criterion:
+    """Context manager: the criterion of the f64 surface, 1D and boundary restatements and of
+    the surface element qualities (process-wide oracle state; mean ratio outside the block)."""
+
+    def __init__(self, c):
+        self.c = int(c)
+
+    def __enter__(self):
+        lib().or_set_criterion(self.c)
+        return self
+
+    def __exit__(self, *exc):
+        lib().or_set_criterion(MEAN_RATIO)
+        return False
 
 
 def color_jpl(rowptr, col, seed=1):

@@ -539,8 +539,9 @@ class DMOHexClass(_DMOBase):
 
 
 class DMOTriFlatClass(_DMOBase):
-    """``DMO::DMOTriFlatClass`` (``dmo/DMOTriFlat.h:19-51``); MEAN_RATIO is the implemented
-    criterion (the reference's default argument is MIN_ANGLE)."""
+    """``DMO::DMOTriFlatClass`` (``dmo/DMOTriFlat.h:19-51``). The default criterion here is
+    MEAN_RATIO; the reference's default argument, MIN_ANGLE (with ``fix_boundary=False`` for its
+    sliding boundary), is passed explicitly."""
     _flat = 1
 
 

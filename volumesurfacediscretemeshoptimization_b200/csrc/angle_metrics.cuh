@@ -47,6 +47,31 @@ __device__ __forceinline__ float tri2d_angle(float ax, float ay, float bx, float
     return angle_q<MAXA>(fmaxf(fmaxf(c1, c2), c3), fminf(fminf(c1, c2), c3));
 }
 
+// triangle (p0, p1, p2) in space; SIGNED: negated when its normal e0 x e1 (normalised) points
+// away from n (minAngleMetricTri(p, n) / maxAngleMetricTri(p, n); without n the unsigned metric)
+template <bool MAXA, bool SIGNED>
+__device__ __forceinline__ float tri3d_angle(const float* p0, const float* p1, const float* p2, float nx, float ny,
+                                             float nz) {
+    float u[3], v[3], w[3], e0[3], e1[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        e0[a] = p1[a] - p0[a]; e1[a] = p2[a] - p1[a];
+        u[a] = p0[a] - p1[a];   // angle at p1: (p0 - p1, p2 - p1) = (u, e1)
+        v[a] = p1[a] - p2[a];   // angle at p2: (p1 - p2, p0 - p2) = (v, w)
+        w[a] = p0[a] - p2[a];
+    }
+    const float m0[3] = { -w[0], -w[1], -w[2] };   // angle at p0: (p2 - p0, p1 - p0) = (-w, e0)
+    const float c1 = ang_cos3(u, e1), c2 = ang_cos3(v, w), c3 = ang_cos3(m0, e0);
+    float q = angle_q<MAXA>(fmaxf(fmaxf(c1, c2), c3), fminf(fminf(c1, c2), c3));
+    if (SIGNED) {
+        const float tx = e0[1] * e1[2] - e0[2] * e1[1], ty = e0[2] * e1[0] - e0[0] * e1[2], tz = e0[0] * e1[1] - e0[1] * e1[0];
+        const float len = sqrtf((tx * tx + ty * ty) + tz * tz);
+        const float nd = ((tx / len) * nx + (ty / len) * ny) + (tz / len) * nz;
+        if (nd < 0.f) q = -q;
+    }
+    return q;
+}
+
 // tetrahedron (p0, p1, p2, p3): dihedral angles between the face normals
 template <bool MAXA>
 __device__ __forceinline__ float tet_angle(const float* p0, const float* p1, const float* p2, const float* p3) {

@@ -75,7 +75,7 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
     else {
         SectorSurfaces sec{o->srow.p, o->stab.p, o->FS.p, o->Xs.p};
         if (o->feat) VSDMO_CUDA(cudaMemcpyAsync(o->Xs.p, m.pos.p, sizeof(float4) * m.nSurf, cudaMemcpyDeviceToDevice, s));
-        launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, o->feat ? &sec : nullptr, s);
+        launch_dmo_surf(m, L, o->X0.p, o->LS.p, o->nn.p, o->feat ? &sec : nullptr, criterion_of(o->kind), s);
     }
 }
 
@@ -110,12 +110,14 @@ void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
         for (const auto& r : o->sranges) {
             DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
             if (o->feat) VSDMO_CUDA(cudaMemcpyAsync(o->Xs.p, m.pos.p, sizeof(float4) * m.nSurf, cudaMemcpyDeviceToDevice, s));
-            launch_dmo_surf_vol(m, L, o->X0.p, o->LS.p, o->nn.p, o->feat ? &sec : nullptr, o->stats.p, o->d_iter.p, s);
+            launch_dmo_surf_vol(m, L, o->X0.p, o->LS.p, o->nn.p, o->feat ? &sec : nullptr, criterion_of(o->kind),
+                                o->stats.p, o->d_iter.p, s);
         }
         if (o->pass1d)
             for (const auto& r : o->franges) {
                 DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
-                launch_dmo_1d_vol(m, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p, o->stats.p, o->d_iter.p, s);
+                launch_dmo_1d_vol(m, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p, criterion_of(o->kind),
+                                  o->stats.p, o->d_iter.p, s);
             }
         launch_mark_rings(m, 0, m.nSurf, o->dirty.p, s);
         launch_update_nn(m, o->X0.p, o->nn.p, s);
@@ -126,7 +128,7 @@ void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
         const int mode = o->slide ? 0 : (m.fk == 3 ? 1 : 2);
         for (const auto& r : o->franges) {
             DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
-            launch_dmo_1d(m, mode, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p,
+            launch_dmo_1d(m, mode, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p, criterion_of(o->kind),
                           o->slide ? o->stats.p : nullptr, o->slide ? o->d_iter.p : nullptr, s);
         }
     }
@@ -521,19 +523,46 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     o->mesh = mesh;
     o->p = p;
     if (angle) {
-        // angle criteria: tet interiors and flat triangle meshes (8-point grid)
-        const bool tet = m.type == VSDMO_TET;
-        if (!(tet || (m.type == VSDMO_TRI && flat2d)) || p.grid_n != 8)
-            return fail(VSDMO_E_UNSUPPORTED, "angle criteria are implemented for tet meshes and flat triangle meshes "
-                                             "with an 8-point grid");
-        if (!p.fix_boundary) return fail(VSDMO_E_UNSUPPORTED, "set fix_boundary=1 (surface and boundary passes are not implemented)");
-        if ((tet ? m.maxTets : m.maxHE) > dmo_angle_max_ring(m.type))
-            return fail(VSDMO_E_VALENCE, "a vertex's ring exceeds the angle kernel's budget");
-        o->mode = MODE_ANGLE;
+        // angle criteria (dmo/DMOQualityTri.h:10-237, dmo/DMOQualityTet.h:10-115): tet meshes
+        // (interior search; boundary passes with fix_boundary = 0), flat triangle meshes (interior
+        // search; sliding boundary with fix_boundary = 0) and triangle surfaces; 8-point grid
+        const bool tet = m.type == VSDMO_TET, tri = m.type == VSDMO_TRI;
+        if (!(tet || tri) || p.grid_n != 8)
+            return fail(VSDMO_E_UNSUPPORTED, "angle criteria are implemented for tet and triangle meshes with an "
+                                             "8-point grid");
         const bool mx = p.quality == VSDMO_MAX_ANGLE;
-        o->kind = tet ? (mx ? MK_TET_MAXA : MK_TET_MINA) : (mx ? MK_TRI2D_MAXA : MK_TRI2D_MINA);
-        if (tet) for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
-        else for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+        if (tri && !flat2d) {
+            if (m.maxHE > dmo_surf_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
+            o->mode = MODE_SURF;
+            o->kind = mx ? MK_TRI3D_MAXA : MK_TRI3D_MINA;
+            for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+            if (m.nFeature > 0) {
+                o->feat = true;
+                o->pass1d = !p.fix_boundary;
+                for (int c = 0; c < m.nColFeature; ++c) o->franges.push_back({m.col_feature[c], m.col_feature[c + 1]});
+            }
+        } else {
+            if ((tet ? m.maxTets : m.maxHE) > dmo_angle_max_ring(m.type))
+                return fail(VSDMO_E_VALENCE, "a vertex's ring exceeds the angle kernel's budget");
+            o->mode = MODE_ANGLE;
+            o->kind = tet ? (mx ? MK_TET_MAXA : MK_TET_MINA) : (mx ? MK_TRI2D_MAXA : MK_TRI2D_MINA);
+            if (tet) for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
+            else for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
+            if (!p.fix_boundary && tet) {
+                if (m.maxTets > surf_vol_max_ring(VSDMO_TET) || m.maxHE > dmo_surf_max_ring())
+                    return fail(VSDMO_E_VALENCE, "a boundary vertex's ring exceeds the boundary kernels' budget");
+                o->volsurf = true;
+                for (int c = 0; c < m.nColFree; ++c) o->sranges.push_back({m.col_free[c], m.col_free[c + 1]});
+                if (m.nFeature > 0) {
+                    o->feat = o->pass1d = true;
+                    for (int c = 0; c < m.nColFeature; ++c) o->franges.push_back({m.col_feature[c], m.col_feature[c + 1]});
+                }
+            } else if (!p.fix_boundary && m.nFeature > 0) {
+                if (m.maxHE > dmo_surf_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
+                o->slide = o->feat = o->pass1d = true;
+                for (int c = 0; c < m.nColFeature; ++c) o->franges.push_back({m.col_feature[c], m.col_feature[c + 1]});
+            }
+        }
     } else if (m.type == VSDMO_TET) {
         if (m.maxTets > dmo_tet_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more tetrahedra than the kernel's ring budget");
         o->mode = MODE_TET;

@@ -979,6 +979,13 @@ __device__ __forceinline__ float element_quality(const int* __restrict__ el, int
         return kind == MK_TRI2D_MINA ? tri2d_angle<false>(a.x, a.y, b.x, b.y, c.x, c.y)
                                      : tri2d_angle<true>(a.x, a.y, b.x, b.y, c.x, c.y);
     }
+    if (kind == MK_TRI3D_MINA || kind == MK_TRI3D_MAXA) {
+        const int* t = el + 3 * e;
+        const float4 a = pos[t[0]], b = pos[t[1]], c = pos[t[2]];
+        const float pa[3] = { a.x, a.y, a.z }, pb[3] = { b.x, b.y, b.z }, pc[3] = { c.x, c.y, c.z };
+        return kind == MK_TRI3D_MINA ? tri3d_angle<false, false>(pa, pb, pc, 0.f, 0.f, 0.f)
+                                     : tri3d_angle<true, false>(pa, pb, pc, 0.f, 0.f, 0.f);
+    }
     if (kind == MK_TET) {
         const int4 t = reinterpret_cast<const int4*>(el)[e];
         return q_tet(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);

@@ -13,7 +13,7 @@
 //                   batched cuBLAS getrf/getrs; the published algorithm is restated here).
 //   k_update_nn     k_updateNearestNeighbor (dmo/DMOCommon.cu:11-42): greedy walk over the
 //                   initial positions to the initial vertex nearest to the current position.
-//   k_dmo_surf<FK>  k_optimizeHierarchical2D (dmo/DMOTriImplCub.h:26-201 for FK = 3,
+//   k_dmo_surf<FK,Q> k_optimizeHierarchical2D (dmo/DMOTriImplCub.h:26-201 for FK = 3,
 //                   dmo/DMOQuadImplCub.h:24-209 for FK = 4): 8 x 8 grid in the (u, v) frame of
 //                   the surface of nn[v], each candidate projected by the inverse-distance blend
 //                   over the 1-ring surfaces (localSurfaceEstimationWithFeature,
@@ -35,6 +35,7 @@
 #include "vsdmo_internal.cuh"
 #include "tet_key.cuh"
 #include "hex_key.cuh"
+#include "angle_metrics.cuh"
 #include <algorithm>
 #include <cfloat>
 
@@ -260,8 +261,27 @@ __device__ __forceinline__ float ring_key_quad(const float4* __restrict__ ring, 
     return q;
 }
 
-template <int FK, bool SIGNED>
+// angle criteria on a triangle fan: min over the fan of minAngleMetricTri / maxAngleMetricTri
+// of (p, ring[i], ring[i + 1]) (qualityShapeMinAMTri / MaxAMTri, dmo/DMOQualityTri.h:89-121,
+// 205-237), signed by n when SIGNED
+template <bool MAXA, bool SIGNED>
+__device__ __forceinline__ float ring_angle_tri(const float4* __restrict__ ring, int k, float px, float py, float pz,
+                                                float3 n) {
+    const float p[3] = { px, py, pz };
+    float q = FLT_MAX;
+    for (int i = 0; i < k; ++i) {
+        const float4 a = ring[i], b = ring[i + 1];
+        const float pa[3] = { a.x, a.y, a.z }, pb[3] = { b.x, b.y, b.z };
+        q = fminf(q, tri3d_angle<MAXA, SIGNED>(p, pa, pb, n.x, n.y, n.z));
+    }
+    return q;
+}
+
+// ring quality of a surface vertex; Q: 0 mean ratio, 1 min angle, 2 max angle (triangles only)
+template <int FK, bool SIGNED, int Q = 0>
 __device__ __forceinline__ float ring_key(const float4* ring, int k, float px, float py, float pz, float3 n) {
+    if (FK == 3 && Q == 1) return ring_angle_tri<false, SIGNED>(ring, k, px, py, pz, n);
+    if (FK == 3 && Q == 2) return ring_angle_tri<true, SIGNED>(ring, k, px, py, pz, n);
     if (FK == 3) return ring_key_tri<SIGNED>(ring, k, px, py, pz, n);
     return ring_key_quad<SIGNED>(ring, k, px, py, pz, n);
 }
@@ -407,7 +427,57 @@ struct HexRing {
     }
 };
 
-template <int FK>
+template <bool MAXA>
+struct TetAngleRing {
+    // angle criteria on the ring of tets (qualityTetRing with MIN_ANGLE / MAX_ANGLE,
+    // dmo/DMOQualityTet.h:165-177): the literal metric per tet (angle_metrics.cuh) on positions
+    // relative to the vertex; extent as TetRing
+    static constexpr int F4 = 3;
+    const float4* r;
+    int k;
+    float md;
+    float4 c0;
+    __device__ bool stage(const float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
+                          int v, float4 c, int lane, float4* buf) {
+        c0 = c;
+        r = buf;
+        const int b = rowptr[v];
+        k = rowptr[v + 1] - b;
+        float mm = 0.f, me = -FLT_MAX;
+        for (int t = lane; t < k; t += 32) {
+            const int4 h = hf[b + t];
+            const int ids[3] = { h.x, h.y, h.z };
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const float4 q = pos[ids[j]];
+                const float dx = q.x - c0.x, dy = q.y - c0.y, dz = q.z - c0.z;
+                mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
+                me = fmaxf(me, sqrtf(dot3(dx, dy, dz, dx, dy, dz)));
+                buf[3 * t + j] = make_float4(dx, dy, dz, 0.f);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            mm = fmaxf(mm, __shfl_xor_sync(FULL, mm, o));
+            me = fmaxf(me, __shfl_xor_sync(FULL, me, o));
+        }
+        md = me;
+        __syncwarp();
+        return mm > 0.f && mm < FLT_MAX;
+    }
+    __device__ float key(float px, float py, float pz) const {
+        const float p[3] = { px - c0.x, py - c0.y, pz - c0.z };
+        float q = FLT_MAX;
+        for (int t = 0; t < k; ++t) {
+            const float4 a = r[3 * t], b = r[3 * t + 1], c = r[3 * t + 2];
+            const float pa[3] = { a.x, a.y, a.z }, pb[3] = { b.x, b.y, b.z }, pc[3] = { c.x, c.y, c.z };
+            q = fminf(q, tet_angle<MAXA>(p, pa, pb, pc));
+        }
+        return q;
+    }
+};
+
+template <int FK, int Q>
 __global__ void __launch_bounds__(SURF_WARPS * 32)
 k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
            const float4* __restrict__ X0, const float4* __restrict__ LS, const int* __restrict__ nn,
@@ -464,8 +534,8 @@ k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4*
         cu = dot3(dx, dy, dz, L.l1.x, L.l1.y, L.l1.z);
         cv = dot3(dx, dy, dz, L.l2.x, L.l2.y, L.l2.z);
     }
-    float qLast = ring_key<FK, true>(ring, k, c0.x, c0.y, c0.z, n);
-    const float qOld = ring_key<FK, false>(ring, k, c0.x, c0.y, c0.z, n);
+    float qLast = ring_key<FK, true, Q>(ring, k, c0.x, c0.y, c0.z, n);
+    const float qOld = ring_key<FK, false, Q>(ring, k, c0.x, c0.y, c0.z, n);
 
     const int i1 = lane >> 3, j1 = lane & 7, i2 = i1 + 4;
     const float o1 = (float)(7 - 2 * i1) / 7.f, oj = (float)(7 - 2 * j1) / 7.f, o2 = (float)(7 - 2 * i2) / 7.f;
@@ -476,8 +546,8 @@ k_dmo_surf(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4*
         const float u1 = fmaf(o1, S, cu), vv = fmaf(oj, S, cv), u2 = fmaf(o2, S, cu);
         const float3 p1 = estimate(L, x0, nbL, nbX, k, u1, vv);
         const float3 p2 = estimate(L, x0, nbL, nbX, k, u2, vv);
-        const float q1 = ring_key<FK, true>(ring, k, p1.x, p1.y, p1.z, n);
-        const float q2 = ring_key<FK, true>(ring, k, p2.x, p2.y, p2.z, n);
+        const float q1 = ring_key<FK, true, Q>(ring, k, p1.x, p1.y, p1.z, n);
+        const float q2 = ring_key<FK, true, Q>(ring, k, p2.x, p2.y, p2.z, n);
         const bool second = q2 > q1;
         const float val = second ? q2 : q1;
         float bv = __shfl_sync(FULL, val, 0);
@@ -683,16 +753,21 @@ __device__ __forceinline__ float q2d(float px, float py, float4 a, float4 b) {
     return ((2.f * sqrtf(3.f)) * area) / l;
 }
 
-// MODE 0: flat (2D mean ratio), 1: surface triangles, 2: surface quads
-template <int MODE, bool SIGNED>
+// MODE 0: flat (2D mean ratio; Q 1 / 2: minAngleMetricTri2D / maxAngleMetricTri2D), 1: surface
+// triangles, 2: surface quads
+template <int MODE, bool SIGNED, int Q>
 __device__ __forceinline__ float ring_q1d(const float4* ring, int ne, float px, float py, float pz, float3 n) {
     if (MODE == 0) {
         float q = FLT_MAX;
-        for (int i = 0; i < ne; ++i) q = fminf(q, q2d(px, py, ring[i], ring[i + 1]));
+        for (int i = 0; i < ne; ++i) {
+            const float4 a = ring[i], b = ring[i + 1];
+            q = fminf(q, Q == 0 ? q2d(px, py, a, b)
+                                : (Q == 1 ? tri2d_angle<false>(px, py, a.x, a.y, b.x, b.y)
+                                          : tri2d_angle<true>(px, py, a.x, a.y, b.x, b.y)));
+        }
         return q;
     }
-    if (MODE == 1) return ring_key_tri<SIGNED>(ring, ne, px, py, pz, n);
-    return ring_key_quad<SIGNED>(ring, ne, px, py, pz, n);
+    return ring_key<MODE == 1 ? 3 : 4, SIGNED, Q>(ring, ne, px, py, pz, n);
 }
 
 // localSurfaceEstimation1d (dmo/Surface1D.h:52-93)
@@ -732,7 +807,7 @@ __device__ __forceinline__ float3 est1d(const float4* __restrict__ LS1, const fl
 // the first maximum in lane order wins, moves on strict improvement, written when the last
 // level's best beats the current position (surfaces: its unsigned ring quality). gate: the
 // flat pass runs only while the last minimum quality (stats[*iter]) is positive.
-template <int MODE>
+template <int MODE, int Q>
 __global__ void __launch_bounds__(SURF_WARPS * 32)
 k_dmo_1d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ he,
          const uint8_t* __restrict__ isB1, const float4* __restrict__ X0, const float4* __restrict__ LS1,
@@ -801,7 +876,7 @@ k_dmo_1d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* _
         float q = -FLT_MAX;
         if (lane < 8) {
             p = est1d(LS1, X0, nn, nnv, surf, ns, u);
-            q = ring_q1d<MODE, true>(ring, ne, p.x, p.y, p.z, n);
+            q = ring_q1d<MODE, true, Q>(ring, ne, p.x, p.y, p.z, n);
         }
         float bv = __shfl_sync(FULL, q, 0);
         int bt = 0;
@@ -809,14 +884,14 @@ k_dmo_1d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* _
             const float qt = __shfl_sync(FULL, q, t);
             if (qt > bv) { bv = qt; bt = t; }
         }
-        const float qLast = ring_q1d<MODE, true>(ring, ne, cx, cy, cz, n);
+        const float qLast = ring_q1d<MODE, true, Q>(ring, ne, cx, cy, cz, n);
         const float bu = __shfl_sync(FULL, u, bt);
         const float bx = __shfl_sync(FULL, p.x, bt), by = __shfl_sync(FULL, p.y, bt), bz = __shfl_sync(FULL, p.z, bt);
         if (qLast < bv) { cx = bx; cy = by; cz = bz; cu = bu; }
         lastMax = bv;
         ds = ds * (2.f / 7.f);
     }
-    const float qOld = ring_q1d<MODE, false>(ring, ne, c0.x, c0.y, c0.z, n);
+    const float qOld = ring_q1d<MODE, false, Q>(ring, ne, c0.x, c0.y, c0.z, n);
     if (lane == 0 && qOld < lastMax) pos[v] = make_float4(cx, cy, cz, c0.w);
 }
 
@@ -1056,22 +1131,16 @@ void launch_update_nn(const Mesh& m, const float4* X0, int* nn, cudaStream_t s) 
 }
 
 void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
-                     const SectorSurfaces* sec, cudaStream_t s) {
+                     const SectorSurfaces* sec, int crit, cudaStream_t s) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
     const int maxk = m.maxHE;
     const size_t smem = (size_t)SURF_WARPS * surf_warp_f4(maxk) * sizeof(float4);
     const int blocks = (n + SURF_WARPS - 1) / SURF_WARPS;
-    if (m.fk == 4)
-        k_dmo_surf<4><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0,
-                                                            L.v1, L.grid_scale, L.depth, maxk, sec ? sec->srow : nullptr,
-                                                            sec ? sec->stab : nullptr, sec ? sec->FS : nullptr,
-                                                            sec ? sec->Xs : nullptr, m.nSurf - m.nFeature);
-    else
-        k_dmo_surf<3><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0,
-                                                            L.v1, L.grid_scale, L.depth, maxk, sec ? sec->srow : nullptr,
-                                                            sec ? sec->stab : nullptr, sec ? sec->FS : nullptr,
-                                                            sec ? sec->Xs : nullptr, m.nSurf - m.nFeature);
+    auto k = m.fk == 4 ? k_dmo_surf<4, 0> : (crit == 1 ? k_dmo_surf<3, 1> : (crit == 2 ? k_dmo_surf<3, 2> : k_dmo_surf<3, 0>));
+    k<<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0, L.v1, L.grid_scale,
+                                            L.depth, maxk, sec ? sec->srow : nullptr, sec ? sec->stab : nullptr,
+                                            sec ? sec->FS : nullptr, sec ? sec->Xs : nullptr, m.nSurf - m.nFeature);
     VSDMO_CHECK_LAUNCH();
 }
 
@@ -1107,39 +1176,51 @@ int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>&
     return nSect;
 }
 
-// ring array and per-element shared memory of a volume mesh's boundary passes
-static const int4* vol_ring(const Mesh& m) { return m.type == VSDMO_HEX ? m.hh.p : m.hf.p; }
-
-void launch_dmo_surf_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
-                         const SectorSurfaces* sec, const IterStats* gate_stats, const int* gate_iter, cudaStream_t s) {
+template <class R>
+static void surf_vol_launch(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
+                            const SectorSurfaces* sec, const IterStats* gate_stats, const int* gate_iter,
+                            cudaStream_t s) {
     const int n = L.v1 - L.v0;
-    if (n <= 0) return;
-    const bool hex = m.type == VSDMO_HEX;
-    const int f4 = hex ? HexRing::F4 : TetRing::F4;
     const int maxkt = std::max(m.maxTets, 1), maxks = std::max(m.maxHE, 1);
-    const size_t smem = (size_t)SURF_WARPS * (f4 * maxkt + 5 * maxks) * sizeof(float4);
-    auto k = hex ? k_dmo_surf_vol<HexRing> : k_dmo_surf_vol<TetRing>;
-    k<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
-        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, vol_ring(m), X0, LS, nn, L.v0, L.v1, L.grid_scale, L.depth, maxkt,
-        maxks, sec ? sec->srow : nullptr, sec ? sec->stab : nullptr, sec ? sec->FS : nullptr, sec ? sec->Xs : nullptr,
-        m.nSurf - m.nFeature, gate_stats, gate_iter);
+    const size_t smem = (size_t)SURF_WARPS * (R::F4 * maxkt + 5 * maxks) * sizeof(float4);
+    k_dmo_surf_vol<R><<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
+        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, m.type == VSDMO_HEX ? m.hh.p : m.hf.p, X0, LS, nn, L.v0, L.v1,
+        L.grid_scale, L.depth, maxkt, maxks, sec ? sec->srow : nullptr, sec ? sec->stab : nullptr,
+        sec ? sec->FS : nullptr, sec ? sec->Xs : nullptr, m.nSurf - m.nFeature, gate_stats, gate_iter);
     VSDMO_CHECK_LAUNCH();
 }
 
-void launch_dmo_1d_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
-                       const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
-                       cudaStream_t s) {
+template <class R>
+static void vol_1d_launch(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
+                          const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
+                          cudaStream_t s) {
     const int n = L.v1 - L.v0;
-    if (n <= 0) return;
-    const bool hex = m.type == VSDMO_HEX;
-    const int f4 = hex ? HexRing::F4 : TetRing::F4;
     const int maxkt = std::max(m.maxTets, 1), maxks = std::max(m.maxHE, 1);
-    const size_t smem = (size_t)SURF_WARPS * (f4 * maxkt + (maxks + 3) / 4) * sizeof(float4);
-    auto k = hex ? k_dmo_1d_vol<HexRing> : k_dmo_1d_vol<TetRing>;
-    k<<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
-        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, vol_ring(m), X0, LS1, nn, fdeg, opt, m.nSurf - m.nFeature, L.v0,
-        L.v1, L.grid_scale, maxkt, maxks, gate_stats, gate_iter);
+    const size_t smem = (size_t)SURF_WARPS * (R::F4 * maxkt + (maxks + 3) / 4) * sizeof(float4);
+    k_dmo_1d_vol<R><<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
+        m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, m.type == VSDMO_HEX ? m.hh.p : m.hf.p, X0, LS1, nn, fdeg, opt,
+        m.nSurf - m.nFeature, L.v0, L.v1, L.grid_scale, maxkt, maxks, gate_stats, gate_iter);
     VSDMO_CHECK_LAUNCH();
+}
+
+void launch_dmo_surf_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
+                         const SectorSurfaces* sec, int crit, const IterStats* gate_stats, const int* gate_iter,
+                         cudaStream_t s) {
+    if (L.v1 <= L.v0) return;
+    if (m.type == VSDMO_HEX) surf_vol_launch<HexRing>(m, L, X0, LS, nn, sec, gate_stats, gate_iter, s);
+    else if (crit == 1) surf_vol_launch<TetAngleRing<false>>(m, L, X0, LS, nn, sec, gate_stats, gate_iter, s);
+    else if (crit == 2) surf_vol_launch<TetAngleRing<true>>(m, L, X0, LS, nn, sec, gate_stats, gate_iter, s);
+    else surf_vol_launch<TetRing>(m, L, X0, LS, nn, sec, gate_stats, gate_iter, s);
+}
+
+void launch_dmo_1d_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
+                       const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
+                       cudaStream_t s) {
+    if (L.v1 <= L.v0) return;
+    if (m.type == VSDMO_HEX) vol_1d_launch<HexRing>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
+    else if (crit == 1) vol_1d_launch<TetAngleRing<false>>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
+    else if (crit == 2) vol_1d_launch<TetAngleRing<true>>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
+    else vol_1d_launch<TetRing>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
 }
 
 int surf_vol_max_ring(int elem_type) { return elem_type == VSDMO_HEX ? HEX_SURF_MAX_RING : TET_SURF_MAX_RING; }
@@ -1151,10 +1232,16 @@ void prepare_surf_kernels() {
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_vol<TetRing>, cudaFuncAttributeMaxDynamicSharedMemorySize, tet));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_surf_vol<HexRing>, cudaFuncAttributeMaxDynamicSharedMemorySize, hex));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_vol<HexRing>, cudaFuncAttributeMaxDynamicSharedMemorySize, hex));
+    const int ang = (int)((size_t)SURF_WARPS * (TetAngleRing<false>::F4 * TET_SURF_MAX_RING + 5 * SURF_MAX_RING) *
+                          sizeof(float4));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_surf_vol<TetAngleRing<false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ang));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_surf_vol<TetAngleRing<true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ang));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_vol<TetAngleRing<false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ang));
+    VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_1d_vol<TetAngleRing<true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ang));
 }
 
 void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
-                   const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
+                   const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
                    cudaStream_t s) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
@@ -1162,14 +1249,11 @@ void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0
     const size_t smem = (size_t)SURF_WARPS * (2 * maxk + 1 + (maxk + 3) / 4) * sizeof(float4);
     const int blocks = (n + SURF_WARPS - 1) / SURF_WARPS;
     const int nFree = m.nSurf - m.nFeature;
-#define VSDMO_1D(MODE)                                                                                              \
-    k_dmo_1d<MODE><<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, m.isB1.p, X0, LS1, nn, m.vn.p, \
-                                                         fdeg, opt, nFree, L.v0, L.v1, L.grid_scale, maxk, gate_stats, \
-                                                         gate_iter)
-    if (mode == 0) VSDMO_1D(0);
-    else if (mode == 1) VSDMO_1D(1);
-    else VSDMO_1D(2);
-#undef VSDMO_1D
+    auto k = mode == 2 ? k_dmo_1d<2, 0>
+           : mode == 1 ? (crit == 1 ? k_dmo_1d<1, 1> : (crit == 2 ? k_dmo_1d<1, 2> : k_dmo_1d<1, 0>))
+                       : (crit == 1 ? k_dmo_1d<0, 1> : (crit == 2 ? k_dmo_1d<0, 2> : k_dmo_1d<0, 0>));
+    k<<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, m.isB1.p, X0, LS1, nn, m.vn.p, fdeg, opt,
+                                            nFree, L.v0, L.v1, L.grid_scale, maxk, gate_stats, gate_iter);
     VSDMO_CHECK_LAUNCH();
 }
 

@@ -188,7 +188,7 @@ struct SectorSurfaces {
 // One colour class of free surface vertices (triangles when m.fk == 3, quads when 4); sec:
 // null for meshes without feature vertices.
 void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
-                     const SectorSurfaces* sec, cudaStream_t s);
+                     const SectorSurfaces* sec, int crit, cudaStream_t s);
 // Feature vertices: fdeg, the 1D-pass flags and the curves LS1 [3 nSurf] from the current
 // positions and vertex normals (flat: +z).
 void init_feature_state(const Mesh& m, int flat, float4* LS1, int* fdeg, uint8_t* opt, cudaStream_t s);
@@ -197,17 +197,19 @@ int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>&
 // Boundary passes of a tet or hex mesh (run only while the last minimum quality is positive):
 // one colour class of free boundary vertices on their surfaces, one of feature vertices on their
 // curves, each judged by the vertex's volume ring.
+// crit: criterion_of(kind) (tets only; hex rings use the shape metric)
 void launch_dmo_surf_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
-                         const SectorSurfaces* sec, const IterStats* gate_stats, const int* gate_iter, cudaStream_t s);
+                         const SectorSurfaces* sec, int crit, const IterStats* gate_stats, const int* gate_iter,
+                         cudaStream_t s);
 void launch_dmo_1d_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
-                       const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
+                       const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
                        cudaStream_t s);
 int surf_vol_max_ring(int elem_type);
 void prepare_surf_kernels();
 // One colour class of feature vertices: mode 0 flat (gated on the last minimum quality being
 // positive when gate_stats is set), 1 surface triangles, 2 surface quads.
 void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
-                   const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
+                   const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
                    cudaStream_t s);
 int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
 // nu x nv samples of vertex vid's own surface (estimate_mode 0) or of the blended estimate (1)
@@ -216,7 +218,14 @@ void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, i
 
 // Element metric used by the quality kernels.
 enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4, MK_QUAD2D = 5,
-                  MK_TRI2D_MINA = 6, MK_TRI2D_MAXA = 7, MK_TET_MINA = 8, MK_TET_MAXA = 9 };
+                  MK_TRI2D_MINA = 6, MK_TRI2D_MAXA = 7, MK_TET_MINA = 8, MK_TET_MAXA = 9,
+                  MK_TRI3D_MINA = 10, MK_TRI3D_MAXA = 11 };
+// ring criterion of the surface, 1D and boundary passes: 0 mean ratio, 1 min angle, 2 max angle
+inline int criterion_of(int kind) {
+    if (kind == MK_TRI2D_MINA || kind == MK_TET_MINA || kind == MK_TRI3D_MINA) return 1;
+    if (kind == MK_TRI2D_MAXA || kind == MK_TET_MAXA || kind == MK_TRI3D_MAXA) return 2;
+    return 0;
+}
 
 // ---- angle criteria (angle.cu) ------------------------------------------------------------
 // one colour class with MIN_ANGLE (max_angle = false) or MAX_ANGLE for tet interiors and flat
