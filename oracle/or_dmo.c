@@ -435,6 +435,110 @@ static void tet_vertex_f32(const or_mesh* m, float* X, int v, float gs) {
     free(r); free(K);
 }
 
+/* ---- learned reduced search (the product's addition; restated from its design) ---------- */
+/* The network's displacement y (units of the largest per-axis ring extent) centres a grid of
+ * rn^3 candidates per level, rdepth levels, offsets (rn-1-2i)/(rn-1), first half-extent
+ * grid_scale * rscale * the per-axis extent, shrinking by 2/(rn-1); the proposal is clamped to
+ * +-grid_scale * extent per axis. Keys: the ring minimum of the per-tet keys (det if negative,
+ * else det^2 / L^3) for the current position and the proposal, the ordered fraction minimum
+ * (tet_key) for the grid candidates; the best candidate of a level (largest key, lowest index
+ * on ties) becomes the centre when it beats the best so far. The vertex moves when the best
+ * beats the key of its current position; otherwise it is queued for the plain search. */
+static float tet_key_piecemin(int k, const float* K, float x, float y, float z) {
+    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    float m = FLT_MAX;
+    for (int t = 0; t < k; ++t) {
+        const float* c = K + 8 * t;
+        const float det = fmaf(c[2], z, fmaf(c[1], y, fmaf(c[0], x, c[3])));
+        const float L = ((c[7] + fmaf(c[4], x, tx)) + fmaf(c[5], y, ty)) + fmaf(c[6], z, tz);
+        m = fminf(m, det < 0.f ? det : (det * det) / ((L * L) * L));
+    }
+    return m;
+}
+
+static int tet_learned_vertex_f32(const or_mesh* m, float* X, int v, const float* yv, float gs, int rn, int rdepth,
+                                  float rscale) {
+    const int* rp = or__hf_rowptr(m);
+    const int* hf = or__hf(m);
+    int b = rp[v], k = rp[v + 1] - b;
+    if (k <= 0) return 0;
+    float c0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
+    float* r = (float*)malloc(sizeof(float) * 9 * (size_t)k);
+    float* K = (float*)malloc(sizeof(float) * 8 * (size_t)k);
+    float md[3] = { 0.f, 0.f, 0.f };
+    for (int t = 0; t < k; ++t) for (int j = 0; j < 3; ++j) {
+        int u = hf[3 * (b + t) + j];
+        for (int a = 0; a < 3; ++a) {
+            float d = X[3 * u + a] - c0[a];
+            r[9 * t + 3 * j + a] = d;
+            md[a] = fmaxf(md[a], fabsf(d));
+        }
+    }
+    float mm = fmaxf(md[0], fmaxf(md[1], md[2]));
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) { free(r); free(K); return 0; }
+    int ex; (void)frexpf(mm, &ex);
+    for (int i = 0; i < 9 * k; ++i) r[i] = ldexpf(r[i], -ex);
+    for (int a = 0; a < 3; ++a) md[a] = ldexpf(md[a], -ex);
+    for (int t = 0; t < k; ++t) tet_coeffs(r + 9 * t, r + 9 * t + 3, r + 9 * t + 6, K + 8 * t);
+    const float q0 = tet_key_piecemin(k, K, 0.f, 0.f, 0.f);
+    const float mms = fmaxf(md[0], fmaxf(md[1], md[2]));
+    float p[3] = { yv[0] * mms, yv[1] * mms, yv[2] * mms };
+    const int have = isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]);
+    float best = -FLT_MAX, c[3] = { 0.f, 0.f, 0.f };
+    if (have) {
+        for (int a = 0; a < 3; ++a) { const float bnd = gs * md[a]; p[a] = fminf(fmaxf(p[a], -bnd), bnd); c[a] = p[a]; }
+        best = tet_key_piecemin(k, K, p[0], p[1], p[2]);
+        float rr[3] = { gs * rscale * md[0], gs * rscale * md[1], gs * rscale * md[2] };
+        const int nc = rn * rn * rn;
+        for (int level = 0; level < rdepth; ++level) {
+            float bk = -FLT_MAX;
+            int bi = -1;
+            for (int ci = 0; ci < nc; ++ci) {
+                const int ix = ci % rn, iy = (ci / rn) % rn, iz = ci / (rn * rn);
+                const float q = tet_key(k, K, fmaf((float)(rn - 1 - 2 * ix) / (float)(rn - 1), rr[0], c[0]),
+                                        fmaf((float)(rn - 1 - 2 * iy) / (float)(rn - 1), rr[1], c[1]),
+                                        fmaf((float)(rn - 1 - 2 * iz) / (float)(rn - 1), rr[2], c[2]));
+                if (bi < 0 || q > bk) { bk = q; bi = ci; }
+            }
+            if (bk > best) {
+                const int ix = bi % rn, iy = (bi / rn) % rn, iz = bi / (rn * rn);
+                const float n0 = fmaf((float)(rn - 1 - 2 * ix) / (float)(rn - 1), rr[0], c[0]);
+                const float n1 = fmaf((float)(rn - 1 - 2 * iy) / (float)(rn - 1), rr[1], c[1]);
+                const float n2 = fmaf((float)(rn - 1 - 2 * iz) / (float)(rn - 1), rr[2], c[2]);
+                c[0] = n0; c[1] = n1; c[2] = n2;
+                best = bk;
+            }
+            const float sh = 2.0f / (float)(rn - 1);
+            rr[0] *= sh; rr[1] *= sh; rr[2] *= sh;
+        }
+    }
+    int moved = 0;
+    if (have && best > q0) {
+        X[3 * v] = c0[0] + ldexpf(c[0], ex);
+        X[3 * v + 1] = c0[1] + ldexpf(c[1], ex);
+        X[3 * v + 2] = c0[2] + ldexpf(c[2], ex);
+        moved = 1;
+    }
+    free(r); free(K);
+    return moved;
+}
+
+/* one colour class [v0, v1) of the learned mode: the reduced search with proposals Y
+ * [(v1 - v0) x ldy], then the plain search (tet_vertex_f32) of the vertices it did not move;
+ * queued[i] = 1 for those */
+void or_dmo_tet_learned_f32(const or_mesh* m, float* X, int v0, int v1, const float* Y, int ldy, float gs, int rn,
+                            int rdepth, float rscale, uint8_t* queued, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+    for (int v = v0; v < v1; ++v) {
+        const int mv = tet_learned_vertex_f32(m, X, v, Y + (size_t)(v - v0) * ldy, gs, rn, rdepth, rscale);
+        if (queued) queued[v - v0] = (uint8_t)!mv;
+        if (!mv) tet_vertex_f32(m, X, v, gs);
+    }
+}
+
 /* per triangle (p, a, b): (nA.x, nA.y, A0, m.x, m.y, C) */
 static void tri_coeffs(const float* a, const float* b, float* K) {
     float ux = b[0] - a[0], uy = b[1] - a[1];

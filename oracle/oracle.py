@@ -100,6 +100,7 @@ def lib():
         L.or_dmo_1d_f32.argtypes = [P, P, P, P, P, P, P, P, I, I, F, I]
         L.or_dmo_1d_f64.argtypes = [P, P, P, P, P, P, P, P, I, I, D, P, I]
         L.or_angle_qualities_f64.argtypes = [P, P, I, P]
+        L.or_dmo_tet_learned_f32.argtypes = [P, P, I, I, P, I, F, I, I, F, P, I]
         L.or_set_criterion.argtypes = [I]
         L.or_set_criterion.restype = None
         for n in ("or_q_tet_min_angle_f64", "or_q_tet_max_angle_f64"):
@@ -171,6 +172,15 @@ class OracleMesh:
         fn = {TET: lib().or_dmo_tet_f32, HEX: lib().or_dmo_hex_f32}.get(self.elem_type, lib().or_dmo_tri2d_f32)
         fn(self.h, _p(xyz), v0, v1, grid_scale, nthreads)
         return xyz
+
+    def dmo_tet_learned_f32(self, xyz, v0, v1, Y, rn=4, rdepth=2, rscale=0.012, grid_scale=0.5, nthreads=0):
+        """Learned mode, one colour class: (positions, queued mask of the plain-search fallbacks)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        queued = np.zeros(max(v1 - v0, 1), np.uint8)
+        lib().or_dmo_tet_learned_f32(self.h, _p(xyz), v0, v1, _p(Y), Y.shape[1], grid_scale, rn, rdepth, rscale,
+                                     _p(queued), nthreads)
+        return xyz, queued[: v1 - v0].astype(bool)
 
     def dmo_flat_f32(self, xyz, v0, v1, nq=8, depth=3, grid_scale=0.5, nthreads=0):
         """Flat tri / quad colour class with an nq x nq grid and `depth` levels (batched optimiser)."""

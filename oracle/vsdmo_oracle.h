@@ -102,6 +102,10 @@ void or_optimize_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scal
                      double* min_hist, double* mean_hist);
 
 /* ---- angle criteria (MIN_ANGLE / MAX_ANGLE), literal in double (or_dmo.c) ---------------- */
+/* learned mode, one colour class: reduced search around the proposals Y [(v1-v0) x ldy], plain
+ * search for the vertices it does not move (queued[i] = 1) */
+void or_dmo_tet_learned_f32(const or_mesh* m, float* xyz, int v0, int v1, const float* Y, int ldy, float grid_scale,
+                            int rn, int rdepth, float rscale, uint8_t* queued, int nthreads);
 double or_q_tri2d_min_angle_f64(const double* p0, const double* p1, const double* p2);
 double or_q_tri3d_angle_f64(const double* p0, const double* p1, const double* p2, const double* n, int max_angle);
 /* criterion of the f64 surface / 1D / boundary restatements and of or_surface_qualities_f64:

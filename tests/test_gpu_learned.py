@@ -213,3 +213,29 @@ def test_learned_proposals_once_per_iteration(vsdmo):
     opt2.set_proposal_schedule(0)
     opt2.iterate(1)
     assert opt2.learned_counters()[0] > 0
+
+
+def test_learned_colour_launches_match_oracle(vsdmo, oracle_mod):
+    """Learned mode, colour class by colour class, bitwise against the oracle's f32
+    restatement (or_dmo_tet_learned_f32): the reduced 4^3 x 2 search around the network's
+    proposals, then the plain search for the vertices it did not move."""
+    trained, _ = _train_on_plain_pairs(vsdmo, seed=23)
+    xyz, tets = G.tet_cube(10, seed=7)
+    mesh = vsdmo.DMOMeshTet(xyz, tets)
+    om = oracle_mod.OracleMesh(2, xyz, tets)
+    assert mesh.info == om.info
+    opt = vsdmo.DMOTetClass(mesh, n_iter=2)
+    opt.set_model(trained, 4, 2, 0.012)
+    x = mesh.positions()
+    queued_total = 0
+    for sweep in range(2):
+        for c, (v0, v1) in enumerate(om.color_ranges()):
+            Y = opt.proposals(c)
+            xo, queued = om.dmo_tet_learned_f32(x, v0, v1, Y, 4, 2, 0.012)
+            opt.run_color(c)
+            g = mesh.positions()
+            assert np.array_equal(g.view(np.uint32), xo.view(np.uint32)), (sweep, c)
+            queued_total += int(queued.sum())
+            x = g
+    acc, fb, _, _ = opt.learned_counters()
+    assert fb == queued_total and acc + fb == 2 * (mesh.info["nV"] - mesh.info["nSurf"]) and acc > fb

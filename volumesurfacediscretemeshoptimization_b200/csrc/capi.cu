@@ -698,6 +698,7 @@ VSDMO_API vsdmo_status vsdmo_opt_restart(vsdmo_opt_t o) {
         o->d_iter.zero();
         if (o->mode == MODE_SURF || o->slide || o->volsurf) init_surface_state(o);
         o->counters.zero();
+        if (o->fb_count.p) o->fb_count.zero();
         if (o->dirty.p) o->dirty.fill_bytes(1);
         launch_quality_stats(m, o->kind, o->stats.p, o->d_iter.p, o->pmin.p, o->psum.p, o->pfail.p, o->done.p, -1,
                              m.stream);

@@ -65,7 +65,7 @@ struct vsdmo_opt_s {
     DBuf<unsigned long long> counters;    // [0] reduced accepted, [1] fallback, [2] fallback moved, [3] skipped
     DBuf<uint8_t> dirty;                  // active-set flags [nV] (params.active_set)
     DBuf<int> nb, nbn;                    // ring vertices of the inner range [32 per vertex], counts
-    DBuf<int> fb_list, fb_count;          // fallback queue of one colour class
+    DBuf<int> fb_list, fb_count;          // fallback queue of one colour class: entries, {length, blocks done}
     int proposals_once = 0;               // body being run or captured: 1 = one network launch for all colours
     int once_after = -1;                  // iterations from this one on (since the restart) use it; -1 never
     DBuf<float> Yall;                     // its proposals [inner vertices x OUTP]

@@ -192,7 +192,8 @@ VSDMO_API vsdmo_status vsdmo_opt_set_model(vsdmo_opt_t o, vsdmo_model_t model, i
             o->ws.ensure(maxn, false, s);
             o->ensure_neighbours();
             if (!o->fb_list.p || (int)o->fb_list.n < maxn) o->fb_list.alloc(maxn, s);
-            if (!o->fb_count.p) o->fb_count.alloc(1, s);
+            if (!o->fb_count.p) o->fb_count.alloc(2, s);
+            o->fb_count.zero();
         }
         o->counters.zero();
         // the captured iteration changes

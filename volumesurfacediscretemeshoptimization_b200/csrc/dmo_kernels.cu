@@ -392,10 +392,12 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
 }
 
 // The plain search over a list of vertices of one colour class (the learned mode's fallback):
-// warps stride over list[0 .. *count).
+// warps stride over list[0 .. count[0]). The last block to finish sets the queue back to empty
+// (count[0] = 0; count[1] counts the finished blocks), so the next class's learned search
+// appends to an empty queue without a separate reset launch.
 __global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
 k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
-               const int* __restrict__ list, const int* __restrict__ count, float grid_scale, int depth, int maxk,
+               const int* __restrict__ list, int* __restrict__ count, float grid_scale, int depth, int maxk,
                uint8_t* __restrict__ dirty, unsigned long long* __restrict__ moved_count) {
     extern __shared__ float4 smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -422,6 +424,15 @@ k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
             else if (lane == 0) dirty[v] = 0;
         }
         __syncwarp();
+    }
+    // every thread of this block has read count[0]; the last block resets the queue
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned* done = reinterpret_cast<unsigned*>(count + 1);
+        if (atomicAdd(done, 1u) == gridDim.x - 1) {
+            count[0] = 0;
+            *done = 0u;
+        }
     }
 }
 
@@ -1155,15 +1166,14 @@ void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, i
     if (n <= 0) return;
     const int maxk = m.maxTets;
     const size_t smem = (size_t)TET_WARPS * maxk * 2 * sizeof(float4);
-    VSDMO_CUDA(cudaMemsetAsync(fb_count, 0, sizeof(int), s));
     k_dmo_tet_learned<<<(n + TET_WARPS - 1) / TET_WARPS, TET_WARPS * 32, smem, s>>>(
         m.pos.p, m.hf_rowptr.p, m.hf.p, L.v0, L.v1, L.grid_scale, maxk, Y, ldy, rn, rdepth, rscale, counters, dirty,
         fb_list, fb_count);
     VSDMO_CHECK_LAUNCH();
     // fallback: the plain search over the queued vertices, a fixed grid striding over the list
     const int blocks = std::min((n + TET_WARPS - 1) / TET_WARPS, 148 * 4);
-    k_dmo_tet_list<<<blocks, TET_WARPS * 32, tet_smem_bytes(maxk), s>>>(m.pos.p, m.hf_rowptr.p, m.hf.p, fb_list, fb_count, L.grid_scale,
-                                                       L.depth, maxk, dirty, counters + 2);
+    k_dmo_tet_list<<<blocks, TET_WARPS * 32, tet_smem_bytes(maxk), s>>>(m.pos.p, m.hf_rowptr.p, m.hf.p, fb_list, fb_count,
+                                                                        L.grid_scale, L.depth, maxk, dirty, counters + 2);
     VSDMO_CHECK_LAUNCH();
 }
 

@@ -166,7 +166,8 @@ void launch_tet_targets(const Mesh& m, int v0, int v1, const float* scale, const
                         cudaStream_t s);
 // reduced grid around the network's proposal (Y [n x ldy], first 3 columns), plain fallback;
 // counters [4], dirty: optional active-set flags
-// fb_list [colour size] / fb_count: scratch of the fallback queue
+// fb_list [colour size] / fb_count [2]: the fallback queue (its length and a block counter,
+// both zero between launches: the fallback kernel leaves them so)
 void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, int ldy, int rn, int rdepth,
                             float rscale, unsigned long long* counters, uint8_t* dirty, int* fb_list, int* fb_count,
                             cudaStream_t s);

@@ -11,7 +11,7 @@ import time
 
 # training and reduced-search settings used for the 100^3 tet cube measurements
 DEFAULTS = {"reduced_n": 4, "reduced_depth": 2, "reduced_scale": 0.012,
-            "train_steps": (6000, 2000), "train_lr": (1e-3, 2e-4), "batch": 4096,
+            "train_steps": (20000, 6000), "train_lr": (1e-3, 2e-4), "batch": 8192,
             "pairs_mesh": "tet cube 48^3, jitter 0.3h", "pairs_seed": 1000, "pairs_iterations": 20}
 
 
