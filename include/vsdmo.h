@@ -63,7 +63,9 @@ typedef enum vsdmo_quality {
     VSDMO_JACOBIAN = 3,
     VSDMO_MIN_ANGLE = 4,
     VSDMO_RADIUS_RATIO = 5,
-    VSDMO_MAX_ANGLE = 6
+    VSDMO_MAX_ANGLE = 6,
+    VSDMO_CONDITION = 7        /* hex meshes: inverse condition number of the corner Jacobians  */
+                               /* (an addition; the reference judges hexes by shapeMetricHex)    */
 } vsdmo_quality;
 
 typedef enum vsdmo_mem_space { VSDMO_HOST = 0, VSDMO_DEVICE = 1 } vsdmo_mem_space;
@@ -121,6 +123,9 @@ typedef struct vsdmo_params {
     int   active_set;     /* tet: 1 = skip a vertex whose last search found no improvement   */
                           /*    while none of its ring vertices moved since (the result is   */
                           /*    the same with or without skipping); 0 = search every vertex  */
+    int   fit_ring;       /* local quadric surfaces: 1 = fitted over the vertex and its       */
+                          /*    1-ring (dmo/surfaceP/Surface.cu:11-104, the reference), 2 =    */
+                          /*    over its 2-ring as well (an addition; at most 63 points)      */
 } vsdmo_params;
 
 /* ---- library --------------------------------------------------------------------------- */

@@ -33,7 +33,7 @@ inline void check(vsdmo_status s) {
     if (s != VSDMO_OK) throw Error(s, std::string(vsdmo_status_string(s)) + ": " + vsdmo_last_error());
 }
 
-enum class QualityCriterium { MEAN_RATIO = 0, AREA, RIGHT_ANGLE, JACOBIAN, MIN_ANGLE, RADIUS_RATIO, MAX_ANGLE };
+enum class QualityCriterium { MEAN_RATIO = 0, AREA, RIGHT_ANGLE, JACOBIAN, MIN_ANGLE, RADIUS_RATIO, MAX_ANGLE, CONDITION };
 
 // Owns a device mesh (connectivity, colouring, positions) built from host or device arrays.
 class DMOMesh {

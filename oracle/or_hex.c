@@ -83,20 +83,22 @@ double or_q_hex_f64(const double v[8][3]) {
     return 3.0 * ret;
 }
 
-static double ring_hex64(int k, const double* ring, const double* p) {
+typedef double (*hex_metric64)(const double v[8][3]);
+
+static double ring_hex64(int k, const double* ring, const double* p, hex_metric64 metric) {
     double q = DBL_MAX;
     for (int h = 0; h < k; ++h) {
         double v[8][3];
         for (int a = 0; a < 3; ++a) v[0][a] = p[a];
         for (int c = 0; c < 7; ++c)
             for (int a = 0; a < 3; ++a) v[1 + c][a] = ring[21 * h + 3 * c + a];
-        double x = or_q_hex_f64(v);
+        double x = metric(v);
         q = fmin(q, x);
     }
     return q;
 }
 
-static void hex_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin) {
+static void hex_vertex_f64(const or_mesh* m, double* X, int v, double gs, double* margin, hex_metric64 metric) {
     const int* rp = or__hf_rowptr(m);
     const int* hf = or__hf(m);
     const int b = rp[v], k = rp[v + 1] - b;
@@ -121,7 +123,7 @@ static void hex_vertex_f64(const or_mesh* m, double* X, int v, double gs, double
     for (int d = 0; d < DEPTH; ++d) {
         double gmax[3], gmin[3];
         for (int a = 0; a < 3; ++a) { gmax[a] = curr[a] + ds * minD[a]; gmin[a] = curr[a] - ds * minD[a]; }
-        const double qLast = ring_hex64(k, ring, curr);
+        const double qLast = ring_hex64(k, ring, curr, metric);
         double best = -DBL_MAX, second = -DBL_MAX, carried = -DBL_MAX;
         for (int t = 0; t < 128; ++t) carried = fmax(carried, qMax[t]);
         for (int t = 0; t < 128; ++t)
@@ -131,7 +133,7 @@ static void hex_vertex_f64(const or_mesh* m, double* X, int v, double gs, double
                 p[0] = aff * (i * gmin[0] + (NQ - 1 - i) * gmax[0]);
                 p[1] = aff * (j * gmin[1] + (NQ - 1 - j) * gmax[1]);
                 p[2] = aff * (kk * gmin[2] + (NQ - 1 - kk) * gmax[2]);
-                const double q = ring_hex64(k, ring, p);
+                const double q = ring_hex64(k, ring, p, metric);
                 if (q > best) { second = best; best = q; }
                 else if (q < best && q > second) second = q;   /* exact ties: see or__gap64 */
                 if (q > qMax[t]) { qMax[t] = q; pMax[t][0] = p[0]; pMax[t][1] = p[1]; pMax[t][2] = p[2]; }
@@ -144,7 +146,7 @@ static void hex_vertex_f64(const or_mesh* m, double* X, int v, double gs, double
         if (qLast < qMax[key]) { curr[0] = pMax[key][0]; curr[1] = pMax[key][1]; curr[2] = pMax[key][2]; }
         ds = ds * (2.0 / (NQ - 1));
     }
-    const double qOld = ring_hex64(k, ring, c0);
+    const double qOld = ring_hex64(k, ring, c0, metric);
     mg = fmin(mg, or__gap64(qMax[key], qOld));
     if (qOld < qMax[key]) { X[3 * v] = curr[0]; X[3 * v + 1] = curr[1]; X[3 * v + 2] = curr[2]; }
     if (margin) *margin = mg;
@@ -156,7 +158,7 @@ void or_dmo_hex_f64(const or_mesh* m, double* X, int v0, int v1, double gs, doub
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 8)
 #endif
-    for (int v = v0; v < v1; ++v) hex_vertex_f64(m, X, v, gs, margin ? margin + (v - v0) : NULL);
+    for (int v = v0; v < v1; ++v) hex_vertex_f64(m, X, v, gs, margin ? margin + (v - v0) : NULL, or_q_hex_f64);
 }
 
 /* ======================================================================================== */
@@ -444,4 +446,197 @@ void or_optimize_hex_f64(const or_mesh* m, double* X, int n_iter, double gs, int
         if (mean_hist) mean_hist[it] = s / nE;
     }
     free(q);
+}
+
+/* ======================================================================================== */
+/* condition-number quality of hexahedra (an addition to the reference's criteria)            */
+/* ======================================================================================== */
+/* Corner Jacobians of the hex read in the reference's order P = v4 v5 v6 v7 v0 v1 v2 v3:
+ * c0 (P1-P0, P3-P0, P4-P0), c1 (P2-P1, P0-P1, P5-P1), c2 (P3-P2, P1-P2, P6-P2),
+ * c3 (P0-P3, P2-P3, P7-P3), c4 (P7-P4, P5-P4, P0-P4), c5 (P4-P5, P6-P5, P1-P5),
+ * c6 (P5-P6, P7-P6, P2-P6), c7 (P6-P7, P4-P7, P3-P7); corner quality 3 det A /
+ * (|A|_F |adj A|_F) (the inverse condition number, signed; 0 for a degenerate corner); element
+ * quality = minimum over the corners. f64: literally; f32: the product's arithmetic (the key
+ * det |det| / (|A|_F^2 |adj A|_F^2) in the search, the ring scaled as for the shape metric). */
+static const int HC_CORNER[8][4] = { { 0, 1, 3, 4 }, { 1, 2, 0, 5 }, { 2, 3, 1, 6 }, { 3, 0, 2, 7 },
+                                     { 4, 7, 5, 0 }, { 5, 4, 6, 1 }, { 6, 5, 7, 2 }, { 7, 6, 4, 3 } };
+
+double or_q_hex_cond_f64(const double v[8][3]) {
+    const double* P[8] = { v[4], v[5], v[6], v[7], v[0], v[1], v[2], v[3] };
+    double q = DBL_MAX;
+    for (int c = 0; c < 8; ++c) {
+        double e[3][3];
+        for (int j = 0; j < 3; ++j)
+            for (int a = 0; a < 3; ++a) e[j][a] = P[HC_CORNER[c][j + 1]][a] - P[HC_CORNER[c][0]][a];
+        const double det = det3d(e[0], e[1], e[2]);
+        double x[3][3];
+        for (int j = 0; j < 3; ++j) {
+            const double* u = e[(j + 1) % 3]; const double* w = e[(j + 2) % 3];
+            x[j][0] = u[1] * w[2] - u[2] * w[1]; x[j][1] = u[2] * w[0] - u[0] * w[2]; x[j][2] = u[0] * w[1] - u[1] * w[0];
+        }
+        const double F2 = nrm2d(e[0]) + nrm2d(e[1]) + nrm2d(e[2]);
+        const double G2 = nrm2d(x[0]) + nrm2d(x[1]) + nrm2d(x[2]);
+        const double qc = F2 * G2 > 0.0 ? 3.0 * det / sqrt(F2 * G2) : 0.0;
+        q = fmin(q, qc);
+    }
+    return q;
+}
+
+/* f32: fixed operation order */
+static void hcf_cross(const float* a, const float* b, float* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+static float hcf_dot(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+static void hcf_corner(const float* o, const float* a, const float* b, const float* c, float* det, float* den) {
+    const float e1[3] = { a[0] - o[0], a[1] - o[1], a[2] - o[2] };
+    const float e2[3] = { b[0] - o[0], b[1] - o[1], b[2] - o[2] };
+    const float e3[3] = { c[0] - o[0], c[1] - o[1], c[2] - o[2] };
+    float x[3], y[3], z[3];
+    hcf_cross(e2, e3, x);
+    *det = hcf_dot(e1, x);
+    const float F2 = (hcf_dot(e1, e1) + hcf_dot(e2, e2)) + hcf_dot(e3, e3);
+    hcf_cross(e3, e1, y);
+    hcf_cross(e1, e2, z);
+    const float G2 = (hcf_dot(x, x) + hcf_dot(y, y)) + hcf_dot(z, z);
+    *den = F2 * G2;
+}
+static float hcf_key(const float* o, const float* a, const float* b, const float* c) {
+    float det, den;
+    hcf_corner(o, a, b, c, &det, &den);
+    return den > 0.f ? (det * fabsf(det)) / den : 0.f;
+}
+static float hcf_quality(const float* o, const float* a, const float* b, const float* c) {
+    float det, den;
+    hcf_corner(o, a, b, c, &det, &den);
+    return den > 0.f ? (3.f * det) / sqrtf(den) : 0.f;
+}
+
+float or_q_hex_cond_f32(const float v[8][3]) {
+    const float* P[8] = { v[4], v[5], v[6], v[7], v[0], v[1], v[2], v[3] };
+    float q = hcf_quality(P[0], P[1], P[3], P[4]);
+    for (int c = 1; c < 8; ++c)
+        q = fminf(q, hcf_quality(P[HC_CORNER[c][0]], P[HC_CORNER[c][1]], P[HC_CORNER[c][2]], P[HC_CORNER[c][3]]));
+    return q;
+}
+
+/* halfhex (p, r0..r6): P4 = p, P5..P7 = r0..r2, P0..P3 = r3..r6 */
+static float hcf_const_key(const float (*r)[3]) {
+    float k = hcf_key(r[4], r[5], r[3], r[0]);
+    k = fminf(k, hcf_key(r[5], r[6], r[4], r[1]));
+    k = fminf(k, hcf_key(r[6], r[3], r[5], r[2]));
+    k = fminf(k, hcf_key(r[1], r[0], r[2], r[5]));
+    return k;
+}
+static float hcf_halfhex_key(const float (*r)[3], float ck, const float* p) {
+    float k = fminf(ck, hcf_key(p, r[2], r[0], r[3]));
+    k = fminf(k, hcf_key(r[3], r[4], r[6], p));
+    k = fminf(k, hcf_key(r[0], p, r[1], r[4]));
+    k = fminf(k, hcf_key(r[2], r[1], p, r[6]));
+    return k;
+}
+static float hcf_ring_key(int k, const float* R, const float* CK, const float* p) {
+    float q = FLT_MAX;
+    for (int h = 0; h < k; ++h) q = fminf(q, hcf_halfhex_key((const float(*)[3])(R + 21 * h), CK[h], p));
+    return q;
+}
+
+static void hex_cond_vertex_f32(const or_mesh* m, float* X, int v, float gs) {
+    const int* rp = or__hf_rowptr(m);
+    const int* hf = or__hf(m);
+    const int b = rp[v], k = rp[v + 1] - b;
+    if (k <= 0) return;
+    const float c0[3] = { X[3 * v], X[3 * v + 1], X[3 * v + 2] };
+    float mx[3] = { 0.f, 0.f, 0.f }, mn[3] = { FLT_MAX, FLT_MAX, FLT_MAX };
+    for (int h = 0; h < k; ++h)
+        for (int c = 0; c < 7; ++c) {
+            const int u = hf[7 * (b + h) + c];
+            for (int a = 0; a < 3; ++a) {
+                const float d = fabsf(X[3 * u + a] - c0[a]);
+                mx[a] = fmaxf(mx[a], d);
+                mn[a] = fminf(mn[a], d);
+            }
+        }
+    const float mm = fmaxf(mx[0], fmaxf(mx[1], mx[2]));
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) return;
+    int ex;
+    (void)frexpf(mm, &ex);
+    float* R = (float*)malloc(sizeof(float) * 21 * (size_t)k);
+    float* CK = (float*)malloc(sizeof(float) * (size_t)k);
+    for (int h = 0; h < k; ++h) {
+        for (int c = 0; c < 7; ++c) {
+            const int u = hf[7 * (b + h) + c];
+            for (int a = 0; a < 3; ++a) R[21 * h + 3 * c + a] = ldexpf(X[3 * u + a] - c0[a], -ex);
+        }
+        CK[h] = hcf_const_key((const float(*)[3])(R + 21 * h));
+    }
+    const float S[3] = { ldexpf(mn[0], -ex), ldexpf(mn[1], -ex), ldexpf(mn[2], -ex) };
+    float qMax[128], pMax[128][3];
+    for (int t = 0; t < 128; ++t) { qMax[t] = -FLT_MAX; pMax[t][0] = pMax[t][1] = pMax[t][2] = 0.f; }
+    float d[3] = { 0.f, 0.f, 0.f };
+    float ds = gs;
+    int key = 0;
+    for (int lv = 0; lv < DEPTH; ++lv) {
+        const float Sx = ds * S[0], Sy = ds * S[1], Sz = ds * S[2];
+        const float qLast = hcf_ring_key(k, R, CK, d);
+        for (int t = 0; t < 128; ++t)
+            for (int idx = 4 * t; idx < 4 * t + 4; ++idx) {
+                const int i = idx % NQ, j = (idx / NQ) % NQ, kk = idx / (NQ * NQ);
+                const float p[3] = { fmaf(grid_offset(i), Sx, d[0]), fmaf(grid_offset(j), Sy, d[1]),
+                                     fmaf(grid_offset(kk), Sz, d[2]) };
+                const float q = hcf_ring_key(k, R, CK, p);
+                if (q > qMax[t]) { qMax[t] = q; pMax[t][0] = p[0]; pMax[t][1] = p[1]; pMax[t][2] = p[2]; }
+            }
+        key = 0;
+        for (int t = 1; t < 128; ++t) if (qMax[t] > qMax[key]) key = t;
+        if (qLast < qMax[key]) { d[0] = pMax[key][0]; d[1] = pMax[key][1]; d[2] = pMax[key][2]; }
+        ds = ds * (2.0f / (float)(NQ - 1));
+    }
+    const float z0[3] = { 0.f, 0.f, 0.f };
+    const float qOld = hcf_ring_key(k, R, CK, z0);
+    if (qOld < qMax[key]) {
+        X[3 * v] = c0[0] + ldexpf(d[0], ex);
+        X[3 * v + 1] = c0[1] + ldexpf(d[1], ex);
+        X[3 * v + 2] = c0[2] + ldexpf(d[2], ex);
+    }
+    free(R); free(CK);
+}
+
+void or_dmo_hex_cond_f32(const or_mesh* m, float* X, int v0, int v1, float gs, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 8)
+#endif
+    for (int v = v0; v < v1; ++v) hex_cond_vertex_f32(m, X, v, gs);
+}
+
+void or_dmo_hex_cond_f64(const or_mesh* m, double* X, int v0, int v1, double gs, double* margin, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 8)
+#endif
+    for (int v = v0; v < v1; ++v) hex_vertex_f64(m, X, v, gs, margin ? margin + (v - v0) : NULL, or_q_hex_cond_f64);
+}
+
+void or_hex_cond_qualities_f64(const or_mesh* m, const double* X, double* q) {
+    const int nE = or_mesh_info(m, OR_I_NE);
+    const int* el = or__elems(m);
+    for (int e = 0; e < nE; ++e) {
+        double v[8][3];
+        for (int c = 0; c < 8; ++c)
+            for (int a = 0; a < 3; ++a) v[c][a] = X[3 * (size_t)el[8 * e + c] + a];
+        q[e] = or_q_hex_cond_f64(v);
+    }
+}
+
+void or_hex_cond_qualities_f32(const or_mesh* m, const float* X, float* q) {
+    const int nE = or_mesh_info(m, OR_I_NE);
+    const int* el = or__elems(m);
+    for (int e = 0; e < nE; ++e) {
+        float v[8][3];
+        for (int c = 0; c < 8; ++c)
+            for (int a = 0; a < 3; ++a) v[c][a] = X[3 * (size_t)el[8 * e + c] + a];
+        q[e] = or_q_hex_cond_f32(v);
+    }
 }

@@ -120,19 +120,43 @@ static void solve3_f64(double A[3][3], double b[3]) {
     b[0] = (b[0] - A[0][1] * b[1] - A[0][2] * b[2]) / A[0][0];
 }
 
+/* the fit's points after the centre: the 1-ring (halfedge targets in row order), and with
+ * ring == 2 then the ring vertices of each 1-ring vertex in row order, each vertex once, the
+ * centre excluded; at most 62 */
+static int fit_ids(const or_mesh* m, int v, int ring, int* ids) {
+    const int* rp = or__he_rowptr(m);
+    const int* he = or__he(m);
+    int nb = 0;
+    for (int i = rp[v]; i < rp[v + 1] && nb < 62; ++i) ids[nb++] = he[4 * i];
+    if (ring == 2) {
+        const int n1 = nb;
+        for (int i = 0; i < n1 && nb < 62; ++i) {
+            const int u = ids[i];
+            for (int j = rp[u]; j < rp[u + 1] && nb < 62; ++j) {
+                const int w = he[4 * j];
+                int seen = w == v;
+                for (int a = 0; a < nb && !seen; ++a) seen = ids[a] == w;
+                if (!seen) ids[nb++] = w;
+            }
+        }
+    }
+    return nb;
+}
+
 /* returns number of vertices whose frame failed the orthonormality check */
-int or_surface_fit_f32(const or_mesh* m, const float* X, const float* vn, float* LS) {
+int or_surface_fit_ring_f32(const or_mesh* m, const float* X, const float* vn, float* LS, int ring) {
     const int nS = or_mesh_info(m, OR_I_NSURF);
     const int* rp = or__he_rowptr(m);
     const int* he = or__he(m);
     int bad = 0;
     for (int v = 0; v < nS; ++v) {
         const float* c = X + 3 * (size_t)v;
-        int b = rp[v], k = rp[v + 1] - b;
+        int b = rp[v];
         float P[64][3];
-        int np = 0;
+        int np = 0, ids[62];
+        const int nb = fit_ids(m, v, ring, ids);
         P[np][0] = c[0]; P[np][1] = c[1]; P[np][2] = c[2]; np++;
-        for (int i = 0; i < k && np < 63; ++i) { const float* q = X + 3 * (size_t)he[4 * (b + i)]; P[np][0] = q[0]; P[np][1] = q[1]; P[np][2] = q[2]; np++; }
+        for (int i = 0; i < nb; ++i) { const float* q = X + 3 * (size_t)ids[i]; P[np][0] = q[0]; P[np][1] = q[1]; P[np][2] = q[2]; np++; }
         if (np == 5) { for (int a = 0; a < 3; ++a) P[np][a] = 0.5f * (P[2][a] + P[3][a]); np++; }
         /* frame */
         float n[3] = { vn[3 * v], vn[3 * v + 1], vn[3 * v + 2] };
@@ -168,18 +192,19 @@ int or_surface_fit_f32(const or_mesh* m, const float* X, const float* vn, float*
     return bad;
 }
 
-int or_surface_fit_f64(const or_mesh* m, const double* X, const double* vn, double* LS) {
+int or_surface_fit_ring_f64(const or_mesh* m, const double* X, const double* vn, double* LS, int ring) {
     const int nS = or_mesh_info(m, OR_I_NSURF);
     const int* rp = or__he_rowptr(m);
     const int* he = or__he(m);
     int bad = 0;
     for (int v = 0; v < nS; ++v) {
         const double* c = X + 3 * (size_t)v;
-        int b = rp[v], k = rp[v + 1] - b;
+        int b = rp[v];
         double P[64][3];
-        int np = 0;
+        int np = 0, ids[62];
+        const int nb = fit_ids(m, v, ring, ids);
         P[np][0] = c[0]; P[np][1] = c[1]; P[np][2] = c[2]; np++;
-        for (int i = 0; i < k && np < 63; ++i) { const double* q = X + 3 * (size_t)he[4 * (b + i)]; P[np][0] = q[0]; P[np][1] = q[1]; P[np][2] = q[2]; np++; }
+        for (int i = 0; i < nb; ++i) { const double* q = X + 3 * (size_t)ids[i]; P[np][0] = q[0]; P[np][1] = q[1]; P[np][2] = q[2]; np++; }
         if (np == 5) { for (int a = 0; a < 3; ++a) P[np][a] = 0.5 * (P[2][a] + P[3][a]); np++; }
         double n[3] = { vn[3 * v], vn[3 * v + 1], vn[3 * v + 2] };
         const double* q0 = X + 3 * (size_t)he[4 * b];
@@ -211,6 +236,13 @@ int or_surface_fit_f64(const or_mesh* m, const double* X, const double* vn, doub
         o[12] = n[0]; o[13] = n[1]; o[14] = n[2]; o[15] = (double)np;
     }
     return bad;
+}
+
+int or_surface_fit_f32(const or_mesh* m, const float* X, const float* vn, float* LS) {
+    return or_surface_fit_ring_f32(m, X, vn, LS, 1);
+}
+int or_surface_fit_f64(const or_mesh* m, const double* X, const double* vn, double* LS) {
+    return or_surface_fit_ring_f64(m, X, vn, LS, 1);
 }
 
 /* ======================================================================================== */

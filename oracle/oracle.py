@@ -66,6 +66,8 @@ def lib():
         L.or_surface_normals_f32.argtypes = [P, P, P, P]
         L.or_surface_fit_f32.argtypes = [P, P, P, P]
         L.or_surface_fit_f64.argtypes = [P, P, P, P]
+        L.or_surface_fit_ring_f32.argtypes = [P, P, P, P, I]
+        L.or_surface_fit_ring_f64.argtypes = [P, P, P, P, I]
         L.or_update_nn_f32.argtypes = [P, P, P, P]
         L.or_update_nn_f64.argtypes = [P, P, P, P]
         L.or_dmo_surf_f32.argtypes = [P, P, P, P, P, P, I, I, F, I]
@@ -101,6 +103,10 @@ def lib():
         L.or_dmo_1d_f64.argtypes = [P, P, P, P, P, P, P, P, I, I, D, P, I]
         L.or_angle_qualities_f64.argtypes = [P, P, I, P]
         L.or_dmo_tet_learned_f32.argtypes = [P, P, I, I, P, I, F, I, I, F, P, I]
+        L.or_dmo_hex_cond_f32.argtypes = [P, P, I, I, F, I]
+        L.or_dmo_hex_cond_f64.argtypes = [P, P, I, I, D, P, I]
+        L.or_hex_cond_qualities_f32.argtypes = [P, P, P]
+        L.or_hex_cond_qualities_f64.argtypes = [P, P, P]
         L.or_set_criterion.argtypes = [I]
         L.or_set_criterion.restype = None
         for n in ("or_q_tet_min_angle_f64", "or_q_tet_max_angle_f64"):
@@ -172,6 +178,25 @@ class OracleMesh:
         fn = {TET: lib().or_dmo_tet_f32, HEX: lib().or_dmo_hex_f32}.get(self.elem_type, lib().or_dmo_tri2d_f32)
         fn(self.h, _p(xyz), v0, v1, grid_scale, nthreads)
         return xyz
+
+    def dmo_hex_cond_f32(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
+        """One colour class of interior hex vertices under the condition-number quality (f32)."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).copy()
+        lib().or_dmo_hex_cond_f32(self.h, _p(xyz), v0, v1, grid_scale, nthreads)
+        return xyz
+
+    def dmo_hex_cond_f64(self, xyz, v0, v1, grid_scale=0.5, nthreads=0):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        margin = np.zeros(max(v1 - v0, 1))
+        lib().or_dmo_hex_cond_f64(self.h, _p(xyz), v0, v1, grid_scale, _p(margin), nthreads)
+        return xyz, margin[: v1 - v0]
+
+    def hex_cond_qualities(self, xyz, dtype=np.float64):
+        xyz = np.ascontiguousarray(xyz, dtype=dtype)
+        q = np.zeros(self.info["nE"], dtype=dtype)
+        fn = lib().or_hex_cond_qualities_f64 if dtype == np.float64 else lib().or_hex_cond_qualities_f32
+        fn(self.h, _p(xyz), _p(q))
+        return q
 
     def dmo_tet_learned_f32(self, xyz, v0, v1, Y, rn=4, rdepth=2, rscale=0.012, grid_scale=0.5, nthreads=0):
         """Learned mode, one colour class: (positions, queued mask of the plain-search fallbacks)."""
@@ -348,22 +373,22 @@ class OracleMesh:
         return xyz, mn, mean
 
     # ---- surface state (quadric fit, nearest initial vertex, normals) --------------------
-    def surface_state_f32(self, xyz):
+    def surface_state_f32(self, xyz, ring=1):
         """(xyz_init, local_surfaces[nSurf,16], nearest[nSurf], face_normals, vertex_normals)"""
         xyz = np.ascontiguousarray(xyz, dtype=np.float32)
         nS, nF = self.info["nSurf"], self.info["nTris"]
         fn = np.zeros((nF, 3), np.float32); vn = np.zeros((nS, 3), np.float32)
         lib().or_surface_normals_f32(self.h, _p(xyz), _p(fn), _p(vn))
         ls = np.zeros((nS, 16), np.float32)
-        lib().or_surface_fit_f32(self.h, _p(xyz), _p(vn), _p(ls))
+        lib().or_surface_fit_ring_f32(self.h, _p(xyz), _p(vn), _p(ls), int(ring))
         return xyz.copy(), ls, np.arange(nS, dtype=np.int32), fn, vn
 
-    def surface_state_f64(self, xyz):
+    def surface_state_f64(self, xyz, ring=1):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         nS = self.info["nSurf"]
         vn = self.array(A_VERTEX_NORMALS).reshape(-1, 3).astype(np.float64)
         ls = np.zeros((nS, 16), np.float64)
-        lib().or_surface_fit_f64(self.h, _p(xyz), _p(vn), _p(ls))
+        lib().or_surface_fit_ring_f64(self.h, _p(xyz), _p(vn), _p(ls), int(ring))
         return xyz.copy(), ls, np.arange(nS, dtype=np.int32), vn
 
     def dmo_surf_color_f32(self, xyz, state, v0, v1, grid_scale=0.5, nthreads=0):

@@ -156,6 +156,15 @@ void or_optimize_hex_f32(const or_mesh* m, float* xyz, int n_iter, float grid_sc
                          double* min_hist, double* mean_hist);
 void or_optimize_hex_f64(const or_mesh* m, double* xyz, int n_iter, double grid_scale, int nthreads,
                          double* min_hist, double* mean_hist);
+/* condition-number quality of hexahedra (an addition): corner inverse condition numbers,
+ * element minimum; search of one colour class of interior hex vertices under it */
+double or_q_hex_cond_f64(const double v[8][3]);
+float  or_q_hex_cond_f32(const float v[8][3]);
+void or_dmo_hex_cond_f32(const or_mesh* m, float* xyz, int v0, int v1, float grid_scale, int nthreads);
+void or_dmo_hex_cond_f64(const or_mesh* m, double* xyz, int v0, int v1, double grid_scale, double* margin,
+                         int nthreads);
+void or_hex_cond_qualities_f64(const or_mesh* m, const double* xyz, double* q);
+void or_hex_cond_qualities_f32(const or_mesh* m, const float* xyz, float* q);
 /* per-halfhex coefficients of the product arithmetic (43 floats, see or_hex.c) */
 void or_hex_coeffs_f32(const float r[7][3], float eps_s, float eps_a, float* out);
 
@@ -164,6 +173,11 @@ void or_hex_coeffs_f32(const float r[7][3], float eps_s, float eps_a, float* out
 void or_surface_normals_f32(const or_mesh* m, const float* xyz, float* face_normals, float* vertex_normals);
 int  or_surface_fit_f32(const or_mesh* m, const float* xyz, const float* vertex_normals, float* local_surfaces);
 int  or_surface_fit_f64(const or_mesh* m, const double* xyz, const double* vertex_normals, double* local_surfaces);
+/* ring 1: the fits above (centre + 1-ring, the reference); ring 2: centre + 1-ring + 2-ring */
+int  or_surface_fit_ring_f32(const or_mesh* m, const float* xyz, const float* vertex_normals, float* local_surfaces,
+                             int ring);
+int  or_surface_fit_ring_f64(const or_mesh* m, const double* xyz, const double* vertex_normals, double* local_surfaces,
+                             int ring);
 /* per-sector surfaces of feature vertices: rowptr [nFeature+1], table [nFeature*20] (sector of
  * each halfedge of a feature vertex, -1 unused), local_surfaces [cap*16]; returns the sector
  * count, -1 when a feature vertex exceeds 20 halfedges / 40 sector points or cap is too small */

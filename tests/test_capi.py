@@ -43,7 +43,7 @@ def test_host_only_calls(vsdmo):
     assert b"sm_100a" in lib.vsdmo_version()
     p = _capi.Params()
     assert lib.vsdmo_params_default(_capi.TET, C.byref(p)) == 0
-    assert (p.grid_n, p.depth, p.n_iter) == (8, 3, 30)
+    assert (p.grid_n, p.depth, p.n_iter, p.fit_ring) == (8, 3, 30, 1)
     assert abs(p.grid_scale - 0.5) < 1e-7
     assert lib.vsdmo_params_default(99, C.byref(p)) == _capi.E_ARG
     assert lib.vsdmo_status_string(_capi.E_MONOTONE) == b"quality decreased"

@@ -140,3 +140,81 @@ def test_hex_benchmark_mesh_properties(oracle_mod, vsdmo):
     # the reference's extent is the per-axis MINIMUM ring distance, tiny on a jittered lattice:
     # the mean quality rises, hexes with a degenerate corner can stay at 0
     assert np.all(np.diff(mn) >= -1e-6) and mean[-1] > mean[0]
+
+
+# ---- condition-number quality (QualityCriterium.CONDITION, an addition) -------------------
+
+def test_hex_condition_qualities(oracle_mod, vsdmo):
+    """Element qualities: 1 on the unit cube, bitwise against the oracle's f32 restatement and
+    within 1e-6 of its double one on a jittered cube (with inverted corners)."""
+    for name in ("hex7_clean", "hex8"):
+        om, gm = _pair(oracle_mod, vsdmo, name)
+        opt = vsdmo.DMOHexClass(gm, qualityCriterium=vsdmo.QualityCriterium.CONDITION, n_iter=1)
+        q = opt.getElementQualities()
+        x = gm.positions()
+        assert same_bits(q, om.hex_cond_qualities(x, np.float32))
+        np.testing.assert_allclose(q, om.hex_cond_qualities(x.astype(np.float64)), rtol=0, atol=1e-6)
+        if name == "hex7_clean":
+            assert np.all(np.abs(q - 1.0) < 1e-6)
+        else:
+            assert q.min() < 0
+
+
+@pytest.mark.parametrize("name", ["hex3", "hex5", "hex8"])
+def test_hex_condition_colour_launches_bitwise(oracle_mod, vsdmo, name):
+    om, gm = _pair(oracle_mod, vsdmo, name)
+    opt = vsdmo.DMOHexClass(gm, qualityCriterium=vsdmo.QualityCriterium.CONDITION, n_iter=2)
+    x = om.xyz
+    moved = 0
+    for sweep in range(2):
+        for c, (v0, v1) in enumerate(om.color_ranges()):
+            y = om.dmo_hex_cond_f32(x, v0, v1)
+            moved += int(np.any(y != x, axis=1).sum())
+            x = y
+            opt.run_color(c)
+            assert same_bits(gm.positions(), x), (sweep, c)
+    assert moved > 0
+
+
+def test_hex_condition_against_fp64_and_known_answers(oracle_mod, vsdmo):
+    """Colour launches within 1e-5 h of the literal double search where its decisions are
+    clear (exact ties of constant corners decide nothing); a full run raises the minimum from
+    inverted to valid monotonically; the unit-cube grid is a fixed point."""
+    om, gm = _pair(oracle_mod, vsdmo, "hex8")
+    h = 1.0 / 8
+    opt = vsdmo.DMOHexClass(gm, qualityCriterium=vsdmo.QualityCriterium.CONDITION, n_iter=4)
+    x = om.xyz
+    checked = total = 0
+    for c, (v0, v1) in enumerate(om.color_ranges()):
+        x64, margin = om.dmo_hex_cond_f64(x.astype(np.float64), v0, v1)
+        opt.run_color(c)
+        g = gm.positions()
+        clear = margin > 1e-5
+        d = np.abs(g[v0:v1].astype(np.float64) - x64[v0:v1]).max(1)
+        assert np.all(d[clear] < 1e-5 * h), float(d[clear].max())
+        checked += int(clear.sum())
+        total += v1 - v0
+        x = g
+    assert checked > 0.6 * total
+    xyz, el = HEXES["hex8"]()
+    opt2 = vsdmo.DMOHexClass(vsdmo.DMOMeshHex(xyz, el), qualityCriterium=vsdmo.QualityCriterium.CONDITION, n_iter=4,
+                             check_monotone=False)
+    q0 = opt2.getQuality()
+    opt2.optimize()
+    mn, mean = opt2.history()
+    assert q0 < 0 < mn[-1] and np.all(np.diff(mn) >= -1e-6) and mean[-1] > mean[0]
+    xyz, el = HEXES["hex7_clean"]()
+    gm3 = vsdmo.DMOMeshHex(xyz, el)
+    x3 = gm3.positions()
+    vsdmo.DMOHexClass(gm3, qualityCriterium=vsdmo.QualityCriterium.CONDITION, n_iter=2).optimize()
+    assert np.array_equal(gm3.positions(), x3)
+
+
+def test_hex_condition_requires_fixed_boundary(vsdmo):
+    xyz, el = HEXES["hex3"]()
+    with pytest.raises(vsdmo.VSDMOError):
+        vsdmo.DMOHexClass(vsdmo.DMOMeshHex(xyz, el), qualityCriterium=vsdmo.QualityCriterium.CONDITION,
+                          fix_boundary=False)
+    xyz, el = G.tet_cube(3, seed=1)
+    with pytest.raises(vsdmo.VSDMOError):
+        vsdmo.DMOTetClass(vsdmo.DMOMeshTet(xyz, el), qualityCriterium=vsdmo.QualityCriterium.CONDITION)

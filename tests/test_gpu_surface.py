@@ -235,3 +235,41 @@ def test_surface_view_samples_bitwise(oracle_mod, vsdmo, name):
             assert same_bits(g, o), (vid, est)
     with pytest.raises(vsdmo.VSDMOError):
         opt.getLocalSurfacePoints(gm.info["nSurf"], 4, 4)
+
+
+@pytest.mark.parametrize("name", ["ico3", "torus40x40"])
+def test_two_ring_fit_bitwise(oracle_mod, vsdmo, name):
+    """fit_ring=2 (an addition: the reference fits over the 1-ring): the quadrics over the
+    2-ring bitwise against the oracle (or_surface_fit_ring_f32), within 1e-4 (relative) of its
+    double fit, and colour launches on them bitwise."""
+    om, gm = _pair(oracle_mod, vsdmo, name)
+    opt = _opt(vsdmo, gm, n_iter=1, fit_ring=2)
+    _, ls, _ = opt.surface_state()
+    state = om.surface_state_f32(om.xyz, ring=2)
+    assert same_bits(ls, state[1])
+    # triangles: 1 + 6 + 12 points around a valence-6 vertex; quads: 1 + 4 + 8 (no midpoint)
+    npts = ls[:, 15]
+    assert npts.min() >= (13 if gm.elem_type == QUAD else 16)
+    ls64 = om.surface_state_f64(om.xyz, ring=2)[1]
+    # the 3 x 3 normal equations in float: relative error ~1e-5 of the coefficients
+    np.testing.assert_allclose(ls[:, [3, 7, 11]], ls64[:, [3, 7, 11]], rtol=1e-4, atol=1e-5)
+    ls1 = om.surface_state_f32(om.xyz, ring=1)[1]
+    assert not same_bits(ls, ls1)
+    x = om.xyz
+    for c, (v0, v1) in enumerate(om.color_ranges()):
+        x = om.dmo_surf_color_f32(x, state, v0, v1)
+        opt.run_color(c)
+        assert same_bits(gm.positions(), x), c
+
+
+def test_two_ring_fit_on_a_sphere(oracle_mod, vsdmo):
+    """Known answer: on the unit icosphere the quadric w = a u^2 + b uv + c v^2 of the sphere
+    around a vertex has a = c = -1/2, b = 0 (w along the outward normal); both fits find it
+    within the icosphere's chord error."""
+    xyz, f = G.icosphere(4)
+    for ring in (1, 2):
+        gm = vsdmo.DMOMeshTri(xyz, f)
+        opt = vsdmo.DMOTriClass(gm, n_iter=1, fit_ring=ring)
+        ls = opt.surface_state()[1]
+        assert np.all(np.abs(ls[:, 3] + 0.5) < 0.03) and np.all(np.abs(ls[:, 11] + 0.5) < 0.03)
+        assert np.all(np.abs(ls[:, 7]) < 0.03)

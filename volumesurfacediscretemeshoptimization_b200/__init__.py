@@ -63,6 +63,7 @@ class QualityCriterium(enum.IntEnum):
     MIN_ANGLE = 4
     RADIUS_RATIO = 5
     MAX_ANGLE = 6
+    CONDITION = 7   # hex meshes: inverse condition number of the corner Jacobians (an addition)
 
 
 def version() -> str:
@@ -281,7 +282,7 @@ class _DMOBase:
 
     def __init__(self, dmo_mesh, qualityCriterium=QualityCriterium.MEAN_RATIO, gridScale: float = 0.5,
                  n_iter: int = 30, fix_boundary: bool = True, use_graph: bool = True, depth: int = 3,
-                 check_monotone: bool = True, active_set: bool = False, grid_n: int = 8):
+                 check_monotone: bool = True, active_set: bool = False, grid_n: int = 8, fit_ring: int = 1):
         self.mesh = dmo_mesh
         p = default_params(dmo_mesh.elem_type)
         p.quality = int(qualityCriterium)
@@ -292,6 +293,7 @@ class _DMOBase:
         p.depth = int(depth)
         p.check_monotone = int(check_monotone)
         p.active_set = int(active_set)
+        p.fit_ring = int(fit_ring)
         p.grid_n = int(grid_n)
         p.flat = self._flat
         self.params = p

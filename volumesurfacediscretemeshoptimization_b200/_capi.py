@@ -51,7 +51,7 @@ class Params(C.Structure):
     _fields_ = [("quality", C.c_int), ("grid_scale", C.c_float), ("n_iter", C.c_int),
                 ("grid_n", C.c_int), ("depth", C.c_int), ("fix_boundary", C.c_int),
                 ("flat", C.c_int), ("use_graph", C.c_int), ("check_monotone", C.c_int),
-                ("active_set", C.c_int)]
+                ("active_set", C.c_int), ("fit_ring", C.c_int)]
 
 
 _lib = None

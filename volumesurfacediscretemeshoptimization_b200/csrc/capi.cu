@@ -67,7 +67,8 @@ void launch_color(vsdmo_opt_s* o, int c, cudaStream_t s) {
     } else if (o->mode == MODE_TET) {
         launch_dmo_tet(m, L, s, o->dirty.p, o->dirty.p ? o->counters.p + 3 : nullptr);
     } else if (o->mode == MODE_HEX) {
-        launch_dmo_hex(m, L, s);
+        if (o->kind == MK_HEX_COND) launch_dmo_hex_cond(m, L, s);
+        else launch_dmo_hex(m, L, s);
     }
     else if (o->mode == MODE_TRI2D) launch_dmo_tri2d(m, L, s);
     else if (o->mode == MODE_FLAT) launch_dmo_flat(m, L, o->p.grid_n, 32, s);
@@ -162,7 +163,7 @@ void init_surface_state(vsdmo_opt_s* o) {
     VSDMO_CHECK_LAUNCH();
     if (surfaces) {
         update_normals(m, s);
-        launch_surface_fit(m, o->X0.p, o->LS.p, s);
+        launch_surface_fit(m, o->X0.p, o->LS.p, o->p.fit_ring, s);
     }
     if (o->feat) {
         if (!o->LS1.p) {
@@ -255,6 +256,7 @@ VSDMO_API vsdmo_status vsdmo_params_default(int elem_type, vsdmo_params* out) {
     out->use_graph = 1;
     out->check_monotone = 1;
     out->active_set = 0;
+    out->fit_ring = 1;
     return VSDMO_OK;
 }
 
@@ -510,8 +512,9 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     if (params) p = *params; else vsdmo_params_default(mesh->m.type, &p);
     const Mesh& m = mesh->m;
     const bool angle = p.quality == VSDMO_MIN_ANGLE || p.quality == VSDMO_MAX_ANGLE;
-    if (p.quality != VSDMO_MEAN_RATIO && !angle)
-        return fail(VSDMO_E_UNSUPPORTED, "MEAN_RATIO, MIN_ANGLE and MAX_ANGLE are implemented");
+    const bool cond = p.quality == VSDMO_CONDITION;
+    if (p.quality != VSDMO_MEAN_RATIO && !angle && !(cond && m.type == VSDMO_HEX))
+        return fail(VSDMO_E_UNSUPPORTED, "MEAN_RATIO, MIN_ANGLE and MAX_ANGLE are implemented, and CONDITION for hex meshes");
     const bool flat2d = (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) && (p.flat < 0 ? m.isFlat : p.flat);
     if (p.grid_n != 8 && !(flat2d && p.grid_n == 4))
         return fail(VSDMO_E_UNSUPPORTED, "only an 8-point grid per axis is implemented (4 or 8 for flat meshes)");
@@ -519,6 +522,7 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     if (p.depth < 1 || p.depth > 8) return fail(VSDMO_E_ARG, "depth must be in 1..8");
     if (!(p.grid_scale > 0.f) || !std::isfinite(p.grid_scale)) return fail(VSDMO_E_ARG, "grid_scale must be positive");
     if (p.n_iter < 0) return fail(VSDMO_E_ARG, "n_iter must be >= 0");
+    if (p.fit_ring != 1 && p.fit_ring != 2) return fail(VSDMO_E_ARG, "fit_ring must be 1 or 2");
     std::unique_ptr<vsdmo_opt_s> o(new vsdmo_opt_s);
     o->mesh = mesh;
     o->p = p;
@@ -581,9 +585,13 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
             }
         }
     } else if (m.type == VSDMO_HEX) {
-        if (m.maxTets > dmo_hex_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more hexahedra than the kernel's ring budget");
+        if (m.maxTets > (cond ? dmo_hex_cond_max_ring() : dmo_hex_max_ring()))
+            return fail(VSDMO_E_VALENCE, "a vertex has more hexahedra than the kernel's ring budget");
+        if (cond && !p.fix_boundary)
+            return fail(VSDMO_E_UNSUPPORTED, "the boundary passes of hex meshes use the shape metric; set fix_boundary=1 "
+                                             "with CONDITION");
         o->mode = MODE_HEX;
-        o->kind = MK_HEX;
+        o->kind = cond ? MK_HEX_COND : MK_HEX;
         for (int c = 0; c < m.nColInner; ++c) o->ranges.push_back({m.col_inner[c], m.col_inner[c + 1]});
         if (!p.fix_boundary) {
             // boundary and feature passes after the interior classes, like DMOHexClass
@@ -638,6 +646,7 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
         o->done.alloc(1, s); o->done.zero();
         prepare_dmo_kernels();
         if (o->mode == MODE_ANGLE) prepare_angle_kernels();
+        if (o->kind == MK_HEX_COND) prepare_hex_cond_kernels();
         if (o->volsurf) prepare_surf_kernels();
         if (o->mode == MODE_SURF || o->slide || o->volsurf) init_surface_state(o.get());
         o->counters.alloc(4, s);

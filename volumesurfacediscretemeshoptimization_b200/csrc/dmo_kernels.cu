@@ -30,6 +30,7 @@
 #include "angle_metrics.cuh"
 #include "tet_key.cuh"
 #include "hex_key.cuh"
+#include "hex_cond.cuh"
 #include <cfloat>
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -978,6 +979,15 @@ __device__ float q_hex(const float4* __restrict__ pos, const int* __restrict__ h
 
 __device__ __forceinline__ float element_quality(const int* __restrict__ el, int kind, const float4* __restrict__ pos, long e) {
     if (kind == MK_HEX) return q_hex(pos, el + 8 * e);
+    if (kind == MK_HEX_COND) {
+        float v[8][3];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float4 p = pos[el[8 * e + c]];
+            v[c][0] = p.x; v[c][1] = p.y; v[c][2] = p.z;
+        }
+        return hc_element_quality(v);
+    }
     if (kind == MK_TET_MINA || kind == MK_TET_MAXA) {
         const int4 t = reinterpret_cast<const int4*>(el)[e];
         const float4 a = pos[t.x], b = pos[t.y], c = pos[t.z], d = pos[t.w];

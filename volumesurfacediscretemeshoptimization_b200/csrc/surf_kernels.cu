@@ -8,7 +8,8 @@
 //   k_surface_fit   computeLocalCoordinates + computeLocalSurface1/2 (dmo/surfaceP/Surface.h:66-93,
 //                   Surface.cu:11-104): frame t1 = n x (q0 - p), t2 = n x t1, least squares
 //                   quadric w = a u^2 + b uv + c v^2 over the centre and its 1-ring (plus the
-//                   midpoint of neighbours 1 and 2 for valence 4); the 3x3 normal equations are
+//                   midpoint of neighbours 1 and 2 for valence 4; optionally the 2-ring as
+//                   well, an addition the reference does not have); the 3x3 normal equations are
 //                   solved by LU with partial pivoting in registers (the reference calls the
 //                   batched cuBLAS getrf/getrs; the published algorithm is restated here).
 //   k_update_nn     k_updateNearestNeighbor (dmo/DMOCommon.cu:11-42): greedy walk over the
@@ -82,12 +83,30 @@ __device__ void solve3(float A[3][3], float b[3]) {
 }
 
 // LS[4v + 0..3] = (p0, a), (t1, b), (t2, c), (n, numPoints)
+// ring2 = 1: the fit takes the 2-ring too -- after the 1-ring, the ring vertices of each 1-ring
+// vertex in row order, each vertex once (the first occurrence), the vertex itself excluded;
+// at most 63 points either way.
 __global__ void k_surface_fit(int nS, const int* __restrict__ rowptr, const int4* __restrict__ he,
-                              const float4* __restrict__ pos, const float* __restrict__ vn, float4* __restrict__ LS) {
+                              const float4* __restrict__ pos, const float* __restrict__ vn, float4* __restrict__ LS,
+                              int ring2) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nS; v += gridDim.x * blockDim.x) {
         const float4 c = pos[v];
         const int b = rowptr[v], k = rowptr[v + 1] - b;
-        const int nb = k < 62 ? k : 62;            // the reference keeps at most 63 points
+        int ids[62];
+        int nb = 0;
+        for (int i = 0; i < k && nb < 62; ++i) ids[nb++] = he[b + i].x;   // the reference keeps at most 63 points
+        if (ring2) {
+            const int n1 = nb;
+            for (int i = 0; i < n1 && nb < 62; ++i) {
+                const int u = ids[i];
+                for (int j = rowptr[u]; j < rowptr[u + 1] && nb < 62; ++j) {
+                    const int w = he[j].x;
+                    bool seen = w == v;
+                    for (int a = 0; a < nb && !seen; ++a) seen = ids[a] == w;
+                    if (!seen) ids[nb++] = w;
+                }
+            }
+        }
         const int np = 1 + nb + (1 + nb == 5 ? 1 : 0);
         float n[3] = { vn[3 * v], vn[3 * v + 1], vn[3 * v + 2] };
         const float4 q0 = pos[he[b].x];
@@ -109,10 +128,10 @@ __global__ void k_surface_fit(int nS, const int* __restrict__ rowptr, const int4
             if (i == 0) {
                 px = c.x; py = c.y; pz = c.z;
             } else if (i <= nb) {
-                const float4 q = pos[he[b + i - 1].x];
+                const float4 q = pos[ids[i - 1]];
                 px = q.x; py = q.y; pz = q.z;
             } else {  // valence 4: midpoint of points 2 and 3 (neighbours 1 and 2)
-                const float4 qa = pos[he[b + 1].x], qb = pos[he[b + 2].x];
+                const float4 qa = pos[ids[1]], qb = pos[ids[2]];
                 px = 0.5f * (qa.x + qb.x); py = 0.5f * (qa.y + qb.y); pz = 0.5f * (qa.z + qb.z);
             }
             const float dx = px - c.x, dy = py - c.y, dz = pz - c.z;
@@ -1117,9 +1136,9 @@ void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, i
     VSDMO_CHECK_LAUNCH();
 }
 
-void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, cudaStream_t s) {
+void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, int ring, cudaStream_t s) {
     if (m.nSurf <= 0) return;
-    k_surface_fit<<<grid_for(m.nSurf, 128), 128, 0, s>>>(m.nSurf, m.he_rowptr.p, m.he.p, pos, m.vn.p, LS);
+    k_surface_fit<<<grid_for(m.nSurf, 128), 128, 0, s>>>(m.nSurf, m.he_rowptr.p, m.he.p, pos, m.vn.p, LS, ring == 2 ? 1 : 0);
     VSDMO_CHECK_LAUNCH();
 }
 

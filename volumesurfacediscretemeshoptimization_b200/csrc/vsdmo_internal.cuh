@@ -174,7 +174,12 @@ void launch_dmo_tet_learned(const Mesh& m, const DmoLaunch& L, const float* Y, i
 
 // ---- surface DMO (surf_kernels.cu) ----------------------------------------------------------
 // Local quadric surfaces LS [4 nSurf] float4 fitted to pos with the mesh's vertex normals.
-void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, cudaStream_t s);
+// hex interiors under the condition-number quality (hex_cond.cu)
+void launch_dmo_hex_cond(const Mesh& m, const DmoLaunch& L, cudaStream_t s);
+int dmo_hex_cond_max_ring();
+void prepare_hex_cond_kernels();
+// ring: 1 = centre + 1-ring (the reference), 2 = centre + 1-ring + 2-ring
+void launch_surface_fit(const Mesh& m, const float4* pos, float4* LS, int ring, cudaStream_t s);
 // nn [nSurf]: nearest initial vertex of every surface vertex, walked from its previous value.
 void launch_update_nn(const Mesh& m, const float4* X0, int* nn, cudaStream_t s);
 struct IterStats;
@@ -220,7 +225,7 @@ void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, i
 // Element metric used by the quality kernels.
 enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4, MK_QUAD2D = 5,
                   MK_TRI2D_MINA = 6, MK_TRI2D_MAXA = 7, MK_TET_MINA = 8, MK_TET_MAXA = 9,
-                  MK_TRI3D_MINA = 10, MK_TRI3D_MAXA = 11 };
+                  MK_TRI3D_MINA = 10, MK_TRI3D_MAXA = 11, MK_HEX_COND = 12 };
 // ring criterion of the surface, 1D and boundary passes: 0 mean ratio, 1 min angle, 2 max angle
 inline int criterion_of(int kind) {
     if (kind == MK_TRI2D_MINA || kind == MK_TET_MINA || kind == MK_TRI3D_MINA) return 1;
