@@ -643,24 +643,30 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
 // in p and a Frobenius term quadratic in p; each halfhex is staged as 43 coefficients (the
 // constant part's key and 5 x {g, c, m, C}). min_j cbrt(s^2) / A is compared through s^2 / A^3
 // as a fraction. The reference block's 128 threads of 4 candidates, whose maxima carry across
-// levels, are kept: lane l owns threads 4l .. 4l+3 (fixed z, two y, eight x).
-constexpr int HEX_WARPS = 4;
+// levels, are kept as one block of 128 threads per vertex: thread t takes candidates
+// 4t .. 4t+3 (x = 4 (t & 1) .. +3, y = (t >> 1) & 7, z = t >> 4). (The colour classes of a hex
+// mesh hold ~600-1,200 vertices: one warp per vertex left ~8 warps per SM.)
+constexpr int HEX_THREADS = 128;
 constexpr int HEX_MAX_RING = 64;
 
-__global__ void __launch_bounds__(HEX_WARPS * 32)
-k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hh, int v0, int v1,
+__global__ void __launch_bounds__(HEX_THREADS)
+k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hh, int v0,
           float grid_scale, int depth, int maxk) {
     extern __shared__ float4 smem[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int v = v0 + blockIdx.x * HEX_WARPS + w;
-    if (v >= v1) return;
-    float* co = reinterpret_cast<float*>(smem) + (size_t)w * maxk * HEX_CO;
+    __shared__ float red[6][HEX_THREADS / 32];
+    __shared__ float s_k[HEX_THREADS / 32];
+    __shared__ int s_i[HEX_THREADS / 32];
+    __shared__ float s_win[3];
+    __shared__ int s_czero;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int v = v0 + blockIdx.x;
+    float* co = reinterpret_cast<float*>(smem);
     const int b = rowptr[v], k = rowptr[v + 1] - b;
     if (k <= 0 || k > maxk) return;
     const float4 c0 = pos[v];
     // per-axis largest (scale) and smallest (grid extent, DMOHexImplCub.h:49-68) ring distance
     float mx0 = 0.f, mx1 = 0.f, mx2 = 0.f, mn0 = FLT_MAX, mn1 = FLT_MAX, mn2 = FLT_MAX;
-    for (int idx = lane; idx < 7 * k; idx += 32) {
+    for (int idx = t; idx < 7 * k; idx += HEX_THREADS) {
         const int h = idx / 7, c = idx % 7;
         const int4 q = hh[2 * (b + h) + (c >> 2)];
         const int cc = c & 3;
@@ -676,13 +682,21 @@ k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
         mx2 = fmaxf(mx2, __shfl_xor_sync(FULL, mx2, o)); mn0 = fminf(mn0, __shfl_xor_sync(FULL, mn0, o));
         mn1 = fminf(mn1, __shfl_xor_sync(FULL, mn1, o)); mn2 = fminf(mn2, __shfl_xor_sync(FULL, mn2, o));
     }
+    if (lane == 0) { red[0][w] = mx0; red[1][w] = mx1; red[2][w] = mx2; red[3][w] = mn0; red[4][w] = mn1; red[5][w] = mn2; }
+    if (t == 0) s_czero = 0;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < HEX_THREADS / 32; ++i) {
+        mx0 = fmaxf(mx0, red[0][i]); mx1 = fmaxf(mx1, red[1][i]); mx2 = fmaxf(mx2, red[2][i]);
+        mn0 = fminf(mn0, red[3][i]); mn1 = fminf(mn1, red[4][i]); mn2 = fminf(mn2, red[5][i]);
+    }
     const float mm = fmaxf(mx0, fmaxf(mx1, mx2));
-    if (!(mm > 0.f) || !(mm < FLT_MAX)) return;
+    if (!(mm > 0.f) || !(mm < FLT_MAX)) return;   // uniform over the block
     int ex;
     (void)frexpf(mm, &ex);
     const float p2 = exp2_exact(-ex);
     const float es = ldexpf(HEX_EPS, -3 * ex), ea = ldexpf(HEX_EPS, -2 * ex);
-    for (int h = lane; h < k; h += 32) {
+    for (int h = t; h < k; h += HEX_THREADS) {
         const int4 qa = hh[2 * (b + h)], qb = hh[2 * (b + h) + 1];
         const int us[7] = { qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z };
         float r[7][3];
@@ -692,94 +706,83 @@ k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
             r[c][0] = scale2(p.x - c0.x, p2, -ex); r[c][1] = scale2(p.y - c0.y, p2, -ex); r[c][2] = scale2(p.z - c0.z, p2, -ex);
         }
         hex_coeffs(r, es, ea, co + HEX_CO * h);
+        if (co[HEX_CO * h + 2] != 0.f) s_czero = 1;
     }
-    __syncwarp();
+    __syncthreads();
     const float sx = scale2(mn0, p2, -ex), sy = scale2(mn1, p2, -ex), sz = scale2(mn2, p2, -ex);
     // ring-wide: any constant part zero makes every candidate's key zero
-    bool czero = false;
-    for (int h = 0; h < k; ++h) czero |= co[HEX_CO * h + 2] != 0.f;
-    const int kz = lane >> 2, j0 = 2 * (lane & 3);
-    float qMax[4] = { -FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX };
-    float pX[4] = { 0.f, 0.f, 0.f, 0.f }, pY[4] = { 0.f, 0.f, 0.f, 0.f }, pZ[4] = { 0.f, 0.f, 0.f, 0.f };
+    const bool czero = s_czero != 0;
+    const int ci = 4 * (t & 1), cj = (t >> 1) & 7, ck = t >> 4;
+    float qMax = -FLT_MAX, pX = 0.f, pY = 0.f, pZ = 0.f;
     float dx = 0.f, dy = 0.f, dz = 0.f;
     float ds = grid_scale;
     float qWin = -FLT_MAX;
     for (int level = 0; level < depth; ++level) {
         const float Sx = ds * sx, Sy = ds * sy, Sz = ds * sz;
         const float qLast = hex_key1(co, k, dx, dy, dz, es, ea);
-        const float z = fmaf(grid_offset(kz), Sz, dz);
-        const float y[2] = { fmaf(grid_offset(j0), Sy, dy), fmaf(grid_offset(j0 + 1), Sy, dy) };
-        float x[NQ], t1x[NQ], t3x[NQ];
+        const float z = fmaf(grid_offset(ck), Sz, dz);
+        const float y = fmaf(grid_offset(cj), Sy, dy);
+        float x[4], t1x[4], t3x[4];
 #pragma unroll
-        for (int i = 0; i < NQ; ++i) { x[i] = fmaf(grid_offset(i), Sx, dx); t1x[i] = x[i] * x[i]; t3x[i] = (3.f * x[i]) * x[i]; }
+        for (int i = 0; i < 4; ++i) { x[i] = fmaf(grid_offset(ci + i), Sx, dx); t1x[i] = x[i] * x[i]; t3x[i] = (3.f * x[i]) * x[i]; }
         const float t1z = z * z, t3z = (3.f * z) * z;
-        const float t1y[2] = { y[0] * y[0], y[1] * y[1] }, t3y[2] = { (3.f * y[0]) * y[0], (3.f * y[1]) * y[1] };
-        float N[2][NQ], D[2][NQ];
-        bool zr[2][NQ];
+        const float t1y = y * y, t3y = (3.f * y) * y;
+        float N[4], D[4];
+        bool zr[4];
         {
             const float n0 = co[0], d0 = co[1];
 #pragma unroll
-            for (int jj = 0; jj < 2; ++jj)
-#pragma unroll
-                for (int i = 0; i < NQ; ++i) { N[jj][i] = n0; D[jj][i] = d0; zr[jj][i] = czero; }
+            for (int i = 0; i < 4; ++i) { N[i] = n0; D[i] = d0; zr[i] = czero; }
         }
         for (int h = 0; h < k; ++h) {
             const float* c = co + HEX_CO * h;
             if (h > 0) {
                 const float cn = c[0], cd = c[1];
 #pragma unroll
-                for (int jj = 0; jj < 2; ++jj)
-#pragma unroll
-                    for (int i = 0; i < NQ; ++i)
-                        if (cn * D[jj][i] < N[jj][i] * cd) { N[jj][i] = cn; D[jj][i] = cd; }
+                for (int i = 0; i < 4; ++i)
+                    if (cn * D[i] < N[i] * cd) { N[i] = cn; D[i] = cd; }
             }
 #pragma unroll
             for (int j = 0; j < 5; ++j) {
                 const float* q = c + 3 + 8 * j;
                 const bool a3 = (j == 1 || j == 4);
-                const float sZ = fmaf(q[2], z, q[3]);
-                const float aZ = q[7] + fmaf(q[6], z, a3 ? t3z : t1z);
+                const float sY = fmaf(q[1], y, fmaf(q[2], z, q[3]));
+                const float aY = (q[7] + fmaf(q[6], z, a3 ? t3z : t1z)) + fmaf(q[5], y, a3 ? t3y : t1y);
 #pragma unroll
-                for (int jj = 0; jj < 2; ++jj) {
-                    const float sY = fmaf(q[1], y[jj], sZ);
-                    const float aY = aZ + fmaf(q[5], y[jj], a3 ? t3y[jj] : t1y[jj]);
-#pragma unroll
-                    for (int i = 0; i < NQ; ++i) {
-                        const float sd = fmaf(q[0], x[i], sY);
-                        const float A = aY + fmaf(q[4], x[i], a3 ? t3x[i] : t1x[i]);
-                        if (sd < es || A < ea) { zr[jj][i] = true; continue; }
-                        const float num = sd * sd, den = (A * A) * A;
-                        if (num * D[jj][i] < N[jj][i] * den) { N[jj][i] = num; D[jj][i] = den; }
-                    }
+                for (int i = 0; i < 4; ++i) {
+                    const float sd = fmaf(q[0], x[i], sY);
+                    const float A = aY + fmaf(q[4], x[i], a3 ? t3x[i] : t1x[i]);
+                    if (sd < es || A < ea) { zr[i] = true; continue; }
+                    const float num = sd * sd, den = (A * A) * A;
+                    if (num * D[i] < N[i] * den) { N[i] = num; D[i] = den; }
                 }
             }
         }
-        // carried per-thread maxima of the reference's threads 4 lane + (0: x0-3 y0, 1: x4-7 y0,
-        // 2: x0-3 y1, 3: x4-7 y1), candidates in index order
+        // the thread's maximum carries across levels (candidates in index order, strict >)
 #pragma unroll
-        for (int jj = 0; jj < 2; ++jj)
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) {
-                const float key = zr[jj][i] ? 0.f : N[jj][i] / D[jj][i];
-                const int t = 2 * jj + (i >> 2);
-                if (key > qMax[t]) { qMax[t] = key; pX[t] = x[i]; pY[t] = y[jj]; pZ[t] = z; }
-            }
-        float bk = qMax[0];
-        int bi = 4 * lane;
-#pragma unroll
-        for (int t = 1; t < 4; ++t)
-            if (qMax[t] > bk) { bk = qMax[t]; bi = 4 * lane + t; }
+        for (int i = 0; i < 4; ++i) {
+            const float key = zr[i] ? 0.f : N[i] / D[i];
+            if (key > qMax) { qMax = key; pX = x[i]; pY = y; pZ = z; }
+        }
+        // block arg-max, the lowest thread on ties
+        float bk = qMax;
+        int bi = t;
         warp_argmax(bk, bi);
-        const int src = bi >> 2, tt = bi & 3;
-        const float wx = __shfl_sync(FULL, tt == 0 ? pX[0] : (tt == 1 ? pX[1] : (tt == 2 ? pX[2] : pX[3])), src);
-        const float wy = __shfl_sync(FULL, tt == 0 ? pY[0] : (tt == 1 ? pY[1] : (tt == 2 ? pY[2] : pY[3])), src);
-        const float wz = __shfl_sync(FULL, tt == 0 ? pZ[0] : (tt == 1 ? pZ[1] : (tt == 2 ? pZ[2] : pZ[3])), src);
-        if (qLast < bk) { dx = wx; dy = wy; dz = wz; }
+        if (lane == 0) { s_k[w] = bk; s_i[w] = bi; }
+        __syncthreads();
+        bk = s_k[0]; bi = s_i[0];
+#pragma unroll
+        for (int i = 1; i < HEX_THREADS / 32; ++i)
+            if (s_k[i] > bk || (s_k[i] == bk && s_i[i] < bi)) { bk = s_k[i]; bi = s_i[i]; }
+        if (t == bi) { s_win[0] = pX; s_win[1] = pY; s_win[2] = pZ; }
+        __syncthreads();
+        if (qLast < bk) { dx = s_win[0]; dy = s_win[1]; dz = s_win[2]; }
         qWin = bk;
         ds = ds * (2.0f / 7.0f);
+        __syncthreads();   // s_k / s_win are rewritten by the next level
     }
     const float qOld = hex_key1(co, k, 0.f, 0.f, 0.f, es, ea);
-    if (lane == 0 && qOld < qWin) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
+    if (t == 0 && qOld < qWin) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
 }
 
 // ---- flat triangles ---------------------------------------------------------------------------
@@ -1095,9 +1098,8 @@ void launch_dmo_hex(const Mesh& m, const DmoLaunch& L, cudaStream_t s) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
     const int maxk = m.maxTets;
-    const size_t smem = (size_t)HEX_WARPS * maxk * HEX_CO * sizeof(float);
-    k_dmo_hex<<<(n + HEX_WARPS - 1) / HEX_WARPS, HEX_WARPS * 32, smem, s>>>(m.pos.p, m.hf_rowptr.p, m.hh.p, L.v0, L.v1,
-                                                                            L.grid_scale, L.depth, maxk);
+    const size_t smem = (size_t)maxk * HEX_CO * sizeof(float);
+    k_dmo_hex<<<n, HEX_THREADS, smem, s>>>(m.pos.p, m.hf_rowptr.p, m.hh.p, L.v0, L.grid_scale, L.depth, maxk);
     VSDMO_CHECK_LAUNCH();
 }
 
@@ -1115,7 +1117,7 @@ void prepare_dmo_kernels() {
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_tet_list, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)tet_smem_bytes(TET_MAX_RING)));
     VSDMO_CUDA(cudaFuncSetAttribute(k_dmo_hex, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    HEX_WARPS * HEX_MAX_RING * HEX_CO * (int)sizeof(float)));
+                                    HEX_MAX_RING * HEX_CO * (int)sizeof(float)));
 }
 int dmo_tri2d_max_ring() { return TRI_MAX_RING; }
 int quality_stats_blocks() { return QS_BLOCKS; }

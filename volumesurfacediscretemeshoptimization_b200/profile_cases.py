@@ -9,8 +9,9 @@ library stream, not under a profiler's replay).
     flat_quad   flat quad grid 181^2 (32,761 vertices), k_dmo_flat<4>
     surf_tri    icosphere level 7 with surface noise (163,842 vertices), k_dmo_surf<3>
     surf_quad   torus 512x256 quads with surface noise (131,072 vertices), k_dmo_surf<4>
+                (surface cases: --fit-ring 2 fits the quadrics over the 2-ring)
     tet         Kuhn tet cube 48^3 (117,649 vertices), k_dmo_tet
-    hex         hex cube 32^3 (35,937 vertices), k_dmo_hex
+    hex         hex cube 32^3 (35,937 vertices), k_dmo_hex (--quality CONDITION: k_dmo_hex_cond)
     learned     Kuhn tet cube 100^3 (1,030,301 vertices) with the proposal network (trained
                 first with --train, else untrained): k_mlp_tet_infer, k_dmo_tet_learned,
                 k_dmo_tet_list
@@ -30,6 +31,8 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--meshes", type=int, default=256)
     ap.add_argument("--train", action="store_true", help="learned: train the network first (else untrained)")
+    ap.add_argument("--quality", default="MEAN_RATIO", help="QualityCriterium name (e.g. CONDITION for hex)")
+    ap.add_argument("--fit-ring", type=int, default=1, help="surface cases: quadric fit over the 1- or 2-ring")
     a = ap.parse_args(argv)
     import torch
     import volumesurfacediscretemeshoptimization_b200 as V
@@ -63,7 +66,8 @@ def main(argv=None):
         else:
             xyz, el = G.config5()
             mesh, cls = V.DMOMeshTet(xyz, el, stream=sp), V.DMOTetClass
-        opt = cls(mesh, n_iter=10 ** 6)
+        kw = {"fit_ring": a.fit_ring} if c in ("surf_tri", "surf_quad") else {}
+        opt = cls(mesh, qualityCriterium=getattr(V.QualityCriterium, a.quality), n_iter=10 ** 6, **kw)
         if c == "learned":
             from volumesurfacediscretemeshoptimization_b200.learned import DEFAULTS, train_proposal
             model = train_proposal(stream)[0] if a.train else V.ProposalModel(seed=0, stream=sp)
@@ -78,8 +82,11 @@ def main(argv=None):
         it(a.iters)
         e1.record(stream)
     torch.cuda.synchronize()
-    print(json.dumps({"case": c, "iters": a.iters, "ms_per_iteration": e0.elapsed_time(e1) / a.iters,
-                      "wall_s": time.perf_counter() - t0}), flush=True)
+    line = {"case": c, "iters": a.iters, "ms_per_iteration": e0.elapsed_time(e1) / a.iters,
+            "wall_s": time.perf_counter() - t0}
+    if c != "batched":
+        line.update(quality=a.quality, min_quality=opt.getQuality(), fit_ring=a.fit_ring)
+    print(json.dumps(line), flush=True)
     return 0
 
 
