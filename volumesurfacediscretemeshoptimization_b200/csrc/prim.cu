@@ -4,6 +4,7 @@
 // (e.g. mesh/MeshTriGPU.cu:142,162-170, mesh/MeshTetGPU.cu:125) and k_find_first_n
 // (mesh/SortUtil.cu:3-35). The build runs once per mesh; these kernels are HBM-bound.
 #include "vsdmo_internal.cuh"
+#include <mutex>
 
 namespace vsdmo {
 
@@ -195,6 +196,28 @@ void rowptr_from_sorted(const uint32_t* d_sorted_keys, long n, int K, int* d_row
         VSDMO_CHECK_LAUNCH();
     }
     exclusive_scan(counts.p, d_rowptr, (long)K + 1, nullptr, s);
+}
+
+cudaMemPool_t device_pool() {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    int dev = 0;
+    VSDMO_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        VSDMO_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = 8ull << 30;
+        VSDMO_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools[dev] = pool;
+    }
+    return pools[dev];
 }
 
 }  // namespace vsdmo

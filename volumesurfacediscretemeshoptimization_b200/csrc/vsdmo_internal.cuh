@@ -32,7 +32,14 @@ struct Error : std::runtime_error {
 
 #define VSDMO_CHECK_LAUNCH() VSDMO_CUDA(cudaGetLastError())
 
-// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync on the owning stream).
+// The library's stream-ordered memory pool on the current device (created on first use). It
+// keeps up to 8 GiB of freed memory cached across stream synchronisations, where the default
+// pool hands it back to the driver at every synchronisation and the next build maps it again
+// (measured: mesh build of the 48^3 tet cube 9-88 ms with the default pool, 5 ms with this one).
+cudaMemPool_t device_pool();
+
+// Stream-ordered device buffer (allocated from device_pool() / cudaFreeAsync on the owning
+// stream).
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -52,7 +59,7 @@ struct DBuf {
         release();
         s = st;
         n = count;
-        if (count) VSDMO_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+        if (count) VSDMO_CUDA(cudaMallocFromPoolAsync((void**)&p, count * sizeof(T), device_pool(), st));
     }
     void release() {
         if (p) cudaFreeAsync(p, s);
