@@ -57,10 +57,8 @@ def workload_config(extra=None):
 
 
 def rank_info():
-    r = int(os.environ.get("RANK", "0"))
-    w = int(os.environ.get("WORLD_SIZE", "1"))
-    lr = int(os.environ.get("LOCAL_RANK", "0"))
-    return r, w, lr
+    from volumesurfacediscretemeshoptimization_b200 import replicas
+    return replicas.rank_info()
 
 
 class ClockSampler:
@@ -160,12 +158,9 @@ def run_reference(args):
 
 def run_ours(args):
     import torch
+    from volumesurfacediscretemeshoptimization_b200 import replicas
     r, world, lr = rank_info()
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = replicas.init("nccl", timeout_s=120)
     torch.cuda.set_device(lr)
     dev = torch.device("cuda", lr)
     from volumesurfacediscretemeshoptimization_b200 import build as B
@@ -177,7 +172,7 @@ def run_ours(args):
     lib = _capi.lib()
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
-    xyz, tets = G.config2(seed=r)
+    xyz, tets = G.config2(seed=replicas.replica_seed(r))
     # ---- device-resident workload -------------------------------------------------------------
     mesh = V._Mesh.__new__(V.DMOMeshTet)
     with torch.cuda.stream(stream):
@@ -206,8 +201,7 @@ def run_ours(args):
     q_final = opt.getQuality()
     # ---- timed region ----------------------------------------------------------------------------
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     torch.cuda.synchronize()
     with ClockSampler(lr) as clk:
         for i in range(args.steps):
@@ -217,15 +211,10 @@ def run_ours(args):
                 step()
                 ev[i][1].record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    total_updates = n_inner * N_ITER * args.steps * world
-    value = total_updates / (ms_max / 1e3)
+    ms_max = replicas.max_over_ranks(ms, dist, dev)
+    value = replicas.whole_job_rate(n_inner * N_ITER * args.steps, ms_max, world)
 
     # ---- roofline of the grid-search kernel (separate pass, same stream) -----------------------------
     reset()
@@ -288,8 +277,8 @@ def run_ours(args):
         m2.close()
         if i > 0:  # first one is a warm-up
             e2e_ms.append(a.elapsed_time(b))
-    e2e_ms_med = statistics.median(e2e_ms)
-    e2e_value = n_inner * N_ITER * world / (e2e_ms_med / 1e3)
+    e2e_ms_med = replicas.max_over_ranks(statistics.median(e2e_ms), dist, dev)
+    e2e_value = replicas.whole_job_rate(n_inner * N_ITER, e2e_ms_med, world)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -323,8 +312,7 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_baseline_sample(xyz, tets)
     if r == 0:
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    replicas.finish(dist)
     return 0
 
 
