@@ -64,8 +64,9 @@ typedef enum vsdmo_quality {
     VSDMO_MIN_ANGLE = 4,
     VSDMO_RADIUS_RATIO = 5,
     VSDMO_MAX_ANGLE = 6,
-    VSDMO_CONDITION = 7        /* hex meshes: inverse condition number of the corner Jacobians  */
-                               /* (an addition; the reference judges hexes by shapeMetricHex)    */
+    VSDMO_CONDITION = 7        /* hex meshes and quad surfaces: inverse condition number of the */
+                               /* corner Jacobians (an addition; the reference judges hexes by   */
+                               /* shapeMetricHex and quads by meanRatioMetricQuad)               */
 } vsdmo_quality;
 
 typedef enum vsdmo_mem_space { VSDMO_HOST = 0, VSDMO_DEVICE = 1 } vsdmo_mem_space;

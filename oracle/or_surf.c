@@ -478,7 +478,28 @@ float or_q_tri3d_f32(const float* p0, const float* p1, const float* p2) {
 }
 
 /* meanRatioMetricQuad(p) / (p, n) (DMOQualityQuad.h:13-50); n == NULL: unsigned variant */
+/* condition-number quality of a quad (an addition; or_set_criterion(OR_CONDITION)): per corner
+ * with edges e1, e2 to its neighbours 2 det / (|e1|^2 + |e2|^2), det = (e1 x e2) . n, or
+ * |e1 x e2| without n; the smallest corner */
+static double qcond_corner64(const double* o, const double* a, const double* b, const double* n) {
+    const double e1[3] = { a[0] - o[0], a[1] - o[1], a[2] - o[2] }, e2[3] = { b[0] - o[0], b[1] - o[1], b[2] - o[2] };
+    const double c[3] = { e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0] };
+    const double F2 = dot3d(e1, e1) + dot3d(e2, e2);
+    const double det = n ? dot3d(c, n) : sqrt(dot3d(c, c));
+    return F2 > 0.0 ? 2.0 * det / F2 : 0.0;
+}
+static float qcond_corner32(const float* o, const float* a, const float* b, const float* n) {
+    const float e1[3] = { a[0] - o[0], a[1] - o[1], a[2] - o[2] }, e2[3] = { b[0] - o[0], b[1] - o[1], b[2] - o[2] };
+    const float c[3] = { e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0] };
+    const float F2 = dot3f(e1, e1) + dot3f(e2, e2);
+    const float det = n ? dot3f(c, n) : sqrtf(dot3f(c, c));
+    return F2 > 0.f ? (2.f * det) / F2 : 0.f;
+}
+
 double or_q_quad_f64(const double* p0, const double* p1, const double* p2, const double* p3, const double* n) {
+    if (or__criterion() == OR_CONDITION)
+        return fmin(fmin(qcond_corner64(p0, p1, p3, n), qcond_corner64(p1, p2, p0, n)),
+                    fmin(qcond_corner64(p2, p3, p1, n), qcond_corner64(p3, p0, p2, n)));
     double e[4][3];
     for (int a = 0; a < 3; ++a) { e[0][a] = p1[a] - p0[a]; e[1][a] = p2[a] - p1[a]; e[2][a] = p3[a] - p2[a]; e[3][a] = p0[a] - p3[a]; }
     double l = dot3d(e[0], e[0]) + dot3d(e[1], e[1]) + dot3d(e[2], e[2]) + dot3d(e[3], e[3]);
@@ -495,6 +516,12 @@ double or_q_quad_f64(const double* p0, const double* p1, const double* p2, const
 }
 
 float or_q_quad_f32(const float* p0, const float* p1, const float* p2, const float* p3, const float* n) {
+    if (or__criterion() == OR_CONDITION) {
+        float q = qcond_corner32(p0, p1, p3, n);
+        q = fminf(q, qcond_corner32(p1, p2, p0, n));
+        q = fminf(q, qcond_corner32(p2, p3, p1, n));
+        return fminf(q, qcond_corner32(p3, p0, p2, n));
+    }
     float e[4][3];
     for (int a = 0; a < 3; ++a) { e[0][a] = p1[a] - p0[a]; e[1][a] = p2[a] - p1[a]; e[2][a] = p3[a] - p2[a]; e[3][a] = p0[a] - p3[a]; }
     float l = ((dot3f(e[0], e[0]) + dot3f(e[1], e[1])) + dot3f(e[2], e[2])) + dot3f(e[3], e[3]);
@@ -654,6 +681,9 @@ static void surf_vertex_f64(const surf64* S, double* X, int v, double gs, double
     double cv = dl[0] * L[8] + dl[1] * L[9] + dl[2] * L[10];
     const double aff = 1.0 / (NQ - 1);
     double ds = gs, lastMax = -DBL_MAX, mg = DBL_MAX;
+    /* the quad condition number has a corner that does not touch the vertex (the diagonal
+       one): exact ties at its value are structural (or__gap64) */
+    const int ties = or__criterion() == OR_CONDITION;
     for (int d = 0; d < DEPTH; ++d) {
         double uMax = ds * md, uMin = -ds * md;
         double val[32], uvs[32][2];
@@ -670,13 +700,16 @@ static void surf_vertex_f64(const surf64* S, double* X, int v, double gs, double
             val[t] = q1; uvs[t][0] = u1; uvs[t][1] = v1;
             if (q2 > q1) { val[t] = q2; uvs[t][0] = u2; }
             double qs[2] = { q1, q2 };
-            for (int s = 0; s < 2; ++s) { if (qs[s] > best) { second = best; best = qs[s]; } else if (qs[s] > second) second = qs[s]; }
+            for (int s = 0; s < 2; ++s) {
+                if (qs[s] > best) { second = best; best = qs[s]; }
+                else if ((!ties || qs[s] < best) && qs[s] > second) second = qs[s];
+            }
         }
         double qLast = ring64(fk, k, ring, cur, n);
         int w = 0;
         for (int t = 1; t < 32; ++t) if (val[t] > val[w]) w = t;
         mg = fmin(mg, best - second);
-        mg = fmin(mg, fabs(best - qLast));
+        mg = fmin(mg, ties ? or__gap64(best, qLast) : fabs(best - qLast));
         if (qLast < val[w]) {
             est64(S, v, uvs[w][0], uvs[w][1], cur);
             cu = uvs[w][0]; cv = uvs[w][1];
@@ -685,7 +718,7 @@ static void surf_vertex_f64(const surf64* S, double* X, int v, double gs, double
         ds = ds * (2.0 / (NQ - 1));
     }
     double qOld = ring64(fk, k, ring, p0, NULL);
-    mg = fmin(mg, fabs(lastMax - qOld));
+    mg = fmin(mg, ties ? or__gap64(lastMax, qOld) : fabs(lastMax - qOld));
     if (qOld < lastMax) { X[3 * v] = cur[0]; X[3 * v + 1] = cur[1]; X[3 * v + 2] = cur[2]; }
     if (margin) *margin = mg;
     free(ring);

@@ -424,7 +424,7 @@ class OracleMesh:
         return q
 
 
-MEAN_RATIO, MIN_ANGLE, MAX_ANGLE = 0, 4, 6
+MEAN_RATIO, MIN_ANGLE, MAX_ANGLE, CONDITION = 0, 4, 6, 7
 
 
 class criterion:

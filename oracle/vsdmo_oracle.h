@@ -109,8 +109,9 @@ void or_dmo_tet_learned_f32(const or_mesh* m, float* xyz, int v0, int v1, const 
 double or_q_tri2d_min_angle_f64(const double* p0, const double* p1, const double* p2);
 double or_q_tri3d_angle_f64(const double* p0, const double* p1, const double* p2, const double* n, int max_angle);
 /* criterion of the f64 surface / 1D / boundary restatements and of or_surface_qualities_f64:
- * OR_MEAN_RATIO (default), OR_MIN_ANGLE or OR_MAX_ANGLE (process-wide test state) */
-enum { OR_MEAN_RATIO = 0, OR_MIN_ANGLE = 4, OR_MAX_ANGLE = 6 };
+ * OR_MEAN_RATIO (default), OR_MIN_ANGLE or OR_MAX_ANGLE, OR_CONDITION for quads (process-wide
+ * test state) */
+enum { OR_MEAN_RATIO = 0, OR_MIN_ANGLE = 4, OR_MAX_ANGLE = 6, OR_CONDITION = 7 };
 void or_set_criterion(int criterion);
 int  or__criterion(void);
 double or_q_tri2d_max_angle_f64(const double* p0, const double* p1, const double* p2);

@@ -273,3 +273,65 @@ def test_two_ring_fit_on_a_sphere(oracle_mod, vsdmo):
         ls = opt.surface_state()[1]
         assert np.all(np.abs(ls[:, 3] + 0.5) < 0.03) and np.all(np.abs(ls[:, 11] + 0.5) < 0.03)
         assert np.all(np.abs(ls[:, 7]) < 0.03)
+
+
+@pytest.mark.parametrize("name", ["torus64x32", "torus40x40"])
+def test_quad_condition_bitwise(oracle_mod, vsdmo, name):
+    """QualityCriterium.CONDITION on quad surfaces (an addition: per corner 2 det / (|e1|^2 +
+    |e2|^2), det signed by the vertex normal in the search): element qualities, single colour
+    launches and whole runs bitwise against the oracle's f32 restatement under
+    oracle.criterion(CONDITION)."""
+    om, gm = _pair(oracle_mod, vsdmo, name)
+    cond = vsdmo.QualityCriterium.CONDITION
+    with oracle_mod.criterion(oracle_mod.CONDITION):
+        opt = _opt(vsdmo, gm, qualityCriterium=cond, n_iter=1)
+        assert same_bits(opt.getElementQualities(), om.element_qualities_f32(om.xyz))
+        state = om.surface_state_f32(om.xyz)
+        x = om.xyz
+        for c, (v0, v1) in enumerate(om.color_ranges()):
+            x = om.dmo_surf_color_f32(x, state, v0, v1)
+            opt.run_color(c)
+            assert same_bits(gm.positions(), x), c
+        om2, gm2 = _pair(oracle_mod, vsdmo, name)
+        opt2 = _opt(vsdmo, gm2, qualityCriterium=cond, n_iter=3)
+        x32, mn32, me32 = om2.optimize_f32(om2.xyz, 3)
+        opt2.optimize()
+        assert same_bits(gm2.positions(), x32)
+        mn, mean = opt2.history()
+        np.testing.assert_allclose(mn[1:], mn32, rtol=0, atol=2e-6)
+        assert np.all(np.diff(mn) >= -1e-6) and mean[-1] > mean[0]
+
+
+def test_quad_condition_against_fp64_and_known_answers(oracle_mod, vsdmo):
+    om, gm = _pair(oracle_mod, vsdmo, "torus64x32")
+    h = SURF["torus64x32"][2]
+    cond = vsdmo.QualityCriterium.CONDITION
+    opt = _opt(vsdmo, gm, qualityCriterium=cond, n_iter=1)
+    with oracle_mod.criterion(oracle_mod.CONDITION):
+        np.testing.assert_allclose(opt.getElementQualities(), om.element_qualities_f64(om.xyz.astype(np.float64)),
+                                   rtol=0, atol=1e-6)
+        x0, ls, nn, vn = om.surface_state_f64(om.xyz)
+        x = om.xyz
+        checked = total = 0
+        for c, (v0, v1) in enumerate(om.color_ranges()):
+            x64, margin = om.dmo_surf_color_f64(x.astype(np.float64), x0, ls, nn, vn, v0, v1)
+            opt.run_color(c)
+            g = gm.positions()
+            clear = margin > 1e-5
+            d = np.abs(g[v0:v1].astype(np.float64) - x64[v0:v1]).max(1)
+            assert np.all(d[clear] < 1e-5 * h), float(d[clear].max())
+            checked += int(clear.sum())
+            total += v1 - v0
+            x = g
+    assert checked > 0.5 * total
+    # a square grid treated as a surface: every corner is square (quality 1), a fixed point
+    xyz, q = G.quad_grid(12, seed=None)
+    gq = vsdmo.DMOMeshQuad(xyz, q)
+    oq = vsdmo.DMOQuadClass(gq, qualityCriterium=cond, n_iter=2)
+    assert np.all(np.abs(oq.getElementQualities() - 1.0) < 1e-6)
+    x = gq.positions()
+    oq.optimize()
+    assert np.array_equal(gq.positions(), x)
+    # flat quad meshes (the 2D search) keep the mean ratio only
+    with pytest.raises(vsdmo.VSDMOError):
+        vsdmo.DMOQuadFlatClass(vsdmo.DMOMeshQuad(xyz, q), qualityCriterium=cond)

@@ -63,7 +63,7 @@ class QualityCriterium(enum.IntEnum):
     MIN_ANGLE = 4
     RADIUS_RATIO = 5
     MAX_ANGLE = 6
-    CONDITION = 7   # hex meshes: inverse condition number of the corner Jacobians (an addition)
+    CONDITION = 7   # hex meshes, quad surfaces: inverse condition number of the corner Jacobians (an addition)
 
 
 def version() -> str:

@@ -513,9 +513,10 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     const Mesh& m = mesh->m;
     const bool angle = p.quality == VSDMO_MIN_ANGLE || p.quality == VSDMO_MAX_ANGLE;
     const bool cond = p.quality == VSDMO_CONDITION;
-    if (p.quality != VSDMO_MEAN_RATIO && !angle && !(cond && m.type == VSDMO_HEX))
-        return fail(VSDMO_E_UNSUPPORTED, "MEAN_RATIO, MIN_ANGLE and MAX_ANGLE are implemented, and CONDITION for hex meshes");
     const bool flat2d = (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) && (p.flat < 0 ? m.isFlat : p.flat);
+    if (p.quality != VSDMO_MEAN_RATIO && !angle && !(cond && (m.type == VSDMO_HEX || (m.type == VSDMO_QUAD && !flat2d))))
+        return fail(VSDMO_E_UNSUPPORTED, "MEAN_RATIO, MIN_ANGLE and MAX_ANGLE are implemented, and CONDITION for hex "
+                                         "meshes and quad surfaces");
     if (p.grid_n != 8 && !(flat2d && p.grid_n == 4))
         return fail(VSDMO_E_UNSUPPORTED, "only an 8-point grid per axis is implemented (4 or 8 for flat meshes)");
     if (flat2d && p.grid_n == 4 && p.depth > 4) return fail(VSDMO_E_ARG, "depth must be in 1..4 with a 4-point grid");
@@ -625,7 +626,7 @@ VSDMO_API vsdmo_status vsdmo_opt_create(vsdmo_mesh_t mesh, const vsdmo_params* p
     } else if (m.type == VSDMO_TRI || m.type == VSDMO_QUAD) {
         if (m.maxHE > dmo_surf_max_ring()) return fail(VSDMO_E_VALENCE, "a vertex has more halfedges than the kernel's ring budget");
         o->mode = MODE_SURF;
-        o->kind = m.type == VSDMO_QUAD ? MK_QUAD : MK_TRI3D;
+        o->kind = m.type == VSDMO_QUAD ? (cond ? MK_QUAD_COND : MK_QUAD) : MK_TRI3D;
         for (int c = 0; c < m.nColFree; ++c) o->ranges.push_back({m.col_free[c], m.col_free[c + 1]});
         if (m.nFeature > 0) {
             // feature neighbours project onto their sector surfaces; the feature vertices themselves

@@ -31,6 +31,7 @@
 #include "tet_key.cuh"
 #include "hex_key.cuh"
 #include "hex_cond.cuh"
+#include "quad_cond.cuh"
 #include <cfloat>
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -1017,6 +1018,11 @@ __device__ __forceinline__ float element_quality(const int* __restrict__ el, int
     if (kind == MK_QUAD || kind == MK_QUAD2D) {
         const int4 t = reinterpret_cast<const int4*>(el)[e];
         return kind == MK_QUAD ? q_quad(pos[t.x], pos[t.y], pos[t.z], pos[t.w]) : q_quad2d(pos[t.x], pos[t.y], pos[t.z], pos[t.w]);
+    }
+    if (kind == MK_QUAD_COND) {
+        const int4 t = reinterpret_cast<const int4*>(el)[e];
+        const float4 a = pos[t.x];
+        return quad_cond<false>(a.x, a.y, a.z, pos[t.y], pos[t.z], pos[t.w], make_float3(0.f, 0.f, 0.f));
     }
     const int* t = el + 3 * e;
     if (kind == MK_TRI3D) return q_tri3d(pos[t[0]], pos[t[1]], pos[t[2]]);

@@ -37,6 +37,7 @@
 #include "tet_key.cuh"
 #include "hex_key.cuh"
 #include "angle_metrics.cuh"
+#include "quad_cond.cuh"
 #include <algorithm>
 #include <cfloat>
 
@@ -270,6 +271,17 @@ __device__ __forceinline__ float quad_metric(float p0x, float p0y, float p0z, fl
 }
 
 template <bool SIGNED>
+__device__ __forceinline__ float ring_key_quad_cond(const float4* __restrict__ ring, int k, float px, float py,
+                                                    float pz, float3 n) {
+    float q = 0.f;
+    for (int i = 0; i < k; ++i) {
+        const float v = quad_cond<SIGNED>(px, py, pz, ring[2 * i], ring[2 * i + 1], ring[2 * i + 2], n);
+        q = i == 0 ? v : fminf(q, v);
+    }
+    return q;
+}
+
+template <bool SIGNED>
 __device__ __forceinline__ float ring_key_quad(const float4* __restrict__ ring, int k, float px, float py, float pz,
                                                float3 n) {
     float q = 0.f;
@@ -296,12 +308,14 @@ __device__ __forceinline__ float ring_angle_tri(const float4* __restrict__ ring,
     return q;
 }
 
-// ring quality of a surface vertex; Q: 0 mean ratio, 1 min angle, 2 max angle (triangles only)
+// ring quality of a surface vertex; Q: 0 mean ratio, 1 min angle, 2 max angle (triangles),
+// 3 condition number (quads)
 template <int FK, bool SIGNED, int Q = 0>
 __device__ __forceinline__ float ring_key(const float4* ring, int k, float px, float py, float pz, float3 n) {
     if (FK == 3 && Q == 1) return ring_angle_tri<false, SIGNED>(ring, k, px, py, pz, n);
     if (FK == 3 && Q == 2) return ring_angle_tri<true, SIGNED>(ring, k, px, py, pz, n);
     if (FK == 3) return ring_key_tri<SIGNED>(ring, k, px, py, pz, n);
+    if (Q == 3) return ring_key_quad_cond<SIGNED>(ring, k, px, py, pz, n);
     return ring_key_quad<SIGNED>(ring, k, px, py, pz, n);
 }
 
@@ -1156,7 +1170,8 @@ void launch_dmo_surf(const Mesh& m, const DmoLaunch& L, const float4* X0, const 
     const int maxk = m.maxHE;
     const size_t smem = (size_t)SURF_WARPS * surf_warp_f4(maxk) * sizeof(float4);
     const int blocks = (n + SURF_WARPS - 1) / SURF_WARPS;
-    auto k = m.fk == 4 ? k_dmo_surf<4, 0> : (crit == 1 ? k_dmo_surf<3, 1> : (crit == 2 ? k_dmo_surf<3, 2> : k_dmo_surf<3, 0>));
+    auto k = m.fk == 4 ? (crit == 3 ? k_dmo_surf<4, 3> : k_dmo_surf<4, 0>)
+                       : (crit == 1 ? k_dmo_surf<3, 1> : (crit == 2 ? k_dmo_surf<3, 2> : k_dmo_surf<3, 0>));
     k<<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, X0, LS, nn, m.vn.p, L.v0, L.v1, L.grid_scale,
                                             L.depth, maxk, sec ? sec->srow : nullptr, sec ? sec->stab : nullptr,
                                             sec ? sec->FS : nullptr, sec ? sec->Xs : nullptr, m.nSurf - m.nFeature);
@@ -1268,7 +1283,7 @@ void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0
     const size_t smem = (size_t)SURF_WARPS * (2 * maxk + 1 + (maxk + 3) / 4) * sizeof(float4);
     const int blocks = (n + SURF_WARPS - 1) / SURF_WARPS;
     const int nFree = m.nSurf - m.nFeature;
-    auto k = mode == 2 ? k_dmo_1d<2, 0>
+    auto k = mode == 2 ? (crit == 3 ? k_dmo_1d<2, 3> : k_dmo_1d<2, 0>)
            : mode == 1 ? (crit == 1 ? k_dmo_1d<1, 1> : (crit == 2 ? k_dmo_1d<1, 2> : k_dmo_1d<1, 0>))
                        : (crit == 1 ? k_dmo_1d<0, 1> : (crit == 2 ? k_dmo_1d<0, 2> : k_dmo_1d<0, 0>));
     k<<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, m.isB1.p, X0, LS1, nn, m.vn.p, fdeg, opt,

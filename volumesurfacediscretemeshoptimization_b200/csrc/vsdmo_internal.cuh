@@ -232,11 +232,13 @@ void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, i
 // Element metric used by the quality kernels.
 enum MetricKind { MK_TRI2D = 0, MK_TRI3D = 1, MK_QUAD = 2, MK_TET = 3, MK_HEX = 4, MK_QUAD2D = 5,
                   MK_TRI2D_MINA = 6, MK_TRI2D_MAXA = 7, MK_TET_MINA = 8, MK_TET_MAXA = 9,
-                  MK_TRI3D_MINA = 10, MK_TRI3D_MAXA = 11, MK_HEX_COND = 12 };
-// ring criterion of the surface, 1D and boundary passes: 0 mean ratio, 1 min angle, 2 max angle
+                  MK_TRI3D_MINA = 10, MK_TRI3D_MAXA = 11, MK_HEX_COND = 12, MK_QUAD_COND = 13 };
+// ring criterion of the surface, 1D and boundary passes: 0 mean ratio, 1 min angle, 2 max angle,
+// 3 condition number
 inline int criterion_of(int kind) {
     if (kind == MK_TRI2D_MINA || kind == MK_TET_MINA || kind == MK_TRI3D_MINA) return 1;
     if (kind == MK_TRI2D_MAXA || kind == MK_TET_MAXA || kind == MK_TRI3D_MAXA) return 2;
+    if (kind == MK_HEX_COND || kind == MK_QUAD_COND) return 3;
     return 0;
 }
 
