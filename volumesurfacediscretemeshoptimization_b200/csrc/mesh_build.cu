@@ -580,21 +580,25 @@ struct Builder {
             rowptr.zero();
             col.alloc(1, s);
         }
-        // JPL rounds
-        DBuf<int> colors(num, s), remaining(1, s);
+        // JPL rounds, CH per host read: round c leaves remaining[c % CH] uncoloured vertices; the
+        // rounds after the last one find nobody uncoloured and change nothing
+        constexpr int CH = 16;
+        DBuf<int> colors(num, s), remaining(CH, s);
         k_fill_int<<<G(num), 256, 0, s>>>(colors.p, num, -1);
         VSDMO_CHECK_LAUNCH();
-        int c = 0;
-        while (true) {
+        int nc = -1;
+        for (int c0 = 0; nc < 0; c0 += CH) {
+            if (c0 > num + 1) throw Error(VSDMO_E_CUDA, "colouring did not terminate");
             remaining.zero();
-            k_jpl_round<<<G(num), 256, 0, s>>>(num, rowptr.p, col.p, m.seed, c, colors.p, remaining.p);
-            VSDMO_CHECK_LAUNCH();
-            ++c;
-            int left = read_scalar(remaining.p, s);
-            if (left == 0) break;
-            if (c > num + 1) throw Error(VSDMO_E_CUDA, "colouring did not terminate");
+            for (int i = 0; i < CH; ++i) {
+                k_jpl_round<<<G(num), 256, 0, s>>>(num, rowptr.p, col.p, m.seed, c0 + i, colors.p, remaining.p + i);
+                VSDMO_CHECK_LAUNCH();
+            }
+            const std::vector<int> left = remaining.to_host();
+            for (int i = 0; i < CH && nc < 0; ++i)
+                if (left[i] == 0) nc = c0 + i + 1;
         }
-        const int nc = c;  // JPL colours are dense: every round colours the top-priority vertex left
+        // JPL colours are dense: every round colours the top-priority vertex left
         // stable sort of the range by colour
         DBuf<uint32_t> ck(num, s), order(num, s);
         VSDMO_CUDA(cudaMemcpyAsync(ck.p, colors.p, sizeof(int) * num, cudaMemcpyDeviceToDevice, s));
