@@ -17,6 +17,8 @@ library stream, not under a profiler's replay).
                 k_dmo_tet_list
     batched     --meshes flat tri / quad grids of 500-50,000 vertices in one persistent
                 launch per iteration, k_batch_iter
+    build       the connectivity build of the tet cube 48^3 from pinned host arrays (radix
+                sorts, CSR, colouring); --iters builds after one warm-up build
 """
 from __future__ import annotations
 
@@ -27,7 +29,8 @@ import time
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["tri2d", "flat_quad", "surf_tri", "surf_quad", "tet", "hex", "learned", "batched"])
+    ap.add_argument("case", choices=["tri2d", "flat_quad", "surf_tri", "surf_quad", "tet", "hex", "learned", "batched",
+                                     "build"])
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--meshes", type=int, default=256)
     ap.add_argument("--train", action="store_true", help="learned: train the network first (else untrained)")
@@ -41,6 +44,31 @@ def main(argv=None):
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     c = a.case
+    if c == "build":
+        # the connectivity build of the 48^3 tet cube from pinned host arrays, --iters times
+        # after one warm-up build
+        import ctypes as C
+        from volumesurfacediscretemeshoptimization_b200 import _capi
+        xyz, el = G.config2()
+        lib = _capi.lib()
+        px = torch.from_numpy(xyz).pin_memory()
+        pe = torch.from_numpy(el).pin_memory()
+        ms = []
+        for rep in range(a.iters + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                h = C.c_void_p()
+                _capi.check(lib.vsdmo_mesh_create(_capi.TET, C.c_void_p(px.data_ptr()), len(xyz), C.c_void_p(pe.data_ptr()),
+                                                  len(el), _capi.HOST, 1, C.c_void_p(sp), C.byref(h)))
+                e1.record(stream)
+            torch.cuda.synchronize()
+            lib.vsdmo_mesh_destroy(h)
+            if rep:
+                ms.append(e0.elapsed_time(e1))
+        print(json.dumps({"case": c, "iters": a.iters, "ms_per_build": sum(ms) / len(ms)}), flush=True)
+        return 0
     if c == "batched":
         opt = V.BatchDMO(G.config4(count=a.meshes), stream=sp)
         it = lambda n: opt.iterate(n)
