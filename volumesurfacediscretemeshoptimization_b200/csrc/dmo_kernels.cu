@@ -394,8 +394,8 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
 }
 
 // The plain search over a list of vertices of one colour class (the learned mode's fallback):
-// warps stride over list[0 .. count[0]). The last block to finish sets the queue back to empty
-// (count[0] = 0; count[1] counts the finished blocks), so the next class's learned search
+// warps stride over list[0 .. count[0]). The last warp to finish sets the queue back to empty
+// (count[0] = 0; count[1] counts the finished warps), so the next class's learned search
 // appends to an empty queue without a separate reset launch.
 __global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
 k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
@@ -427,11 +427,12 @@ k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
         }
         __syncwarp();
     }
-    // every thread of this block has read count[0]; the last block resets the queue
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    // every lane of this warp has read count[0]; the last warp of the grid resets the queue (a
+    // warp count, not a block barrier: the warps of a block finish their strides apart)
+    __syncwarp();
+    if (lane == 0) {
         unsigned* done = reinterpret_cast<unsigned*>(count + 1);
-        if (atomicAdd(done, 1u) == gridDim.x - 1) {
+        if (atomicAdd(done, 1u) == gridDim.x * TET_WARPS - 1) {
             count[0] = 0;
             *done = 0u;
         }
