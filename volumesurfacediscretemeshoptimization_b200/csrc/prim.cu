@@ -76,42 +76,79 @@ __global__ void k_radix_hist(const uint32_t* keys, long n, int shift, int* count
     counts[(long)threadIdx.x * nTiles + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void k_radix_scatter(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout,
-                                long n, int shift, const int* offs, int nTiles) {
-    __shared__ int base[256];
+// One tile of RS_TILE pairs: the stable rank of every pair within the tile, computed 256 pairs at
+// a time (a warp match per digit, warp counts, a running base per digit), places the pair in
+// shared memory in tile-local digit order; then consecutive threads write consecutive pairs of
+// a digit run to consecutive global positions (the tile's run of digit d starts at its global
+// offset offs[d * nTiles + tile]), so the writes coalesce.
+__global__ void __launch_bounds__(RS_THREADS)
+k_radix_scatter(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, long n, int shift,
+                const int* offs, int nTiles) {
+    __shared__ uint32_t sk[RS_TILE], sv[RS_TILE];
+    __shared__ int gbase[256], lstart[256], run[256];
     __shared__ int wcnt[RS_WARPS][257];
-    base[threadIdx.x] = offs[(long)threadIdx.x * nTiles + blockIdx.x];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __shared__ int wsum[RS_WARPS];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const long tile = (long)blockIdx.x * RS_TILE;
+    const int tile_n = (int)min((long)RS_TILE, n - tile);
+    // the tile's count of digit tid, from the scanned (digit-major) offsets
+    const long idx = (long)tid * nTiles + blockIdx.x;
+    const int g = offs[idx];
+    const int next = (idx + 1 < 256L * nTiles) ? offs[idx + 1] : (int)n;
+    const int cnt = next - g;
+    gbase[tid] = g;
+    // exclusive scan of the counts over the digits: the tile-local run starts
+    int x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    int before = 0;
+#pragma unroll
+    for (int i = 0; i < RS_WARPS; ++i) before += i < w ? wsum[i] : 0;
+    lstart[tid] = before + x - cnt;
+    run[tid] = before + x - cnt;
+    __syncthreads();
     for (int r = 0; r < RS_ROUNDS; ++r) {
-        for (int j = threadIdx.x; j < RS_WARPS * 257; j += RS_THREADS) (&wcnt[0][0])[j] = 0;
+        for (int j = tid; j < RS_WARPS * 257; j += RS_THREADS) (&wcnt[0][0])[j] = 0;
         __syncthreads();
-        const long idx = tile + (long)r * RS_THREADS + threadIdx.x;
-        const bool valid = idx < n;
-        uint32_t k = valid ? kin[idx] : 0u;
-        int d = valid ? (int)((k >> shift) & 255u) : 256;
-        unsigned peers = __match_any_sync(FULL, d);
-        int rank = __popc(peers & lt);
+        const long i = tile + (long)r * RS_THREADS + tid;
+        const bool valid = i < n;
+        const uint32_t k = valid ? kin[i] : 0u;
+        const uint32_t v = valid ? vin[i] : 0u;
+        const int d = valid ? (int)((k >> shift) & 255u) : 256;
+        const unsigned peers = __match_any_sync(FULL, d);
+        const int rank = __popc(peers & lt);
         if (lane == __ffs(peers) - 1) wcnt[w][d] = __popc(peers);
         __syncthreads();
         {
-            int s = base[threadIdx.x];
+            int s = run[tid];
 #pragma unroll
             for (int ww = 0; ww < RS_WARPS; ++ww) {
-                int t = wcnt[ww][threadIdx.x];
-                wcnt[ww][threadIdx.x] = s;
+                const int t = wcnt[ww][tid];
+                wcnt[ww][tid] = s;
                 s += t;
             }
-            base[threadIdx.x] = s;
+            run[tid] = s;
         }
         __syncthreads();
         if (valid) {
-            int pos = wcnt[w][d] + rank;
-            kout[pos] = k;
-            vout[pos] = vin[idx];
+            const int p = wcnt[w][d] + rank;
+            sk[p] = k;
+            sv[p] = v;
         }
         __syncthreads();
+    }
+    for (int j = tid; j < tile_n; j += RS_THREADS) {
+        const uint32_t k = sk[j];
+        const int d = (int)((k >> shift) & 255u);
+        const int p = gbase[d] + (j - lstart[d]);
+        kout[p] = k;
+        vout[p] = sv[j];
     }
 }
 
