@@ -35,7 +35,9 @@ _lib = None
 
 
 def build():
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """The oracle library, and the reference's own quality functions where its sources are
+    present (oracle/_ref/, Makefile target ``ref``)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all", "ref-if-present"], check=True)
 
 
 def lib():
@@ -123,6 +125,14 @@ def lib():
         L.or_q_tri2d_mean_ratio_f64.argtypes = [P, P, P]
         L.or_q_tri2d_mean_ratio_f32.restype = F
         L.or_q_tri2d_mean_ratio_f32.argtypes = [P, P, P]
+        L.or_q_hex_f64.restype = D
+        L.or_q_hex_f64.argtypes = [P]
+        L.or_q_tri3d_f64.restype = D
+        L.or_q_tri3d_f64.argtypes = [P, P, P]
+        L.or_q_tri3d_angle_f64.restype = D
+        L.or_q_tri3d_angle_f64.argtypes = [P, P, P, P, I]
+        L.or_q_quad_f64.restype = D
+        L.or_q_quad_f64.argtypes = [P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -462,3 +472,76 @@ def q_tri2d(p, dtype=np.float64):
     p = [np.ascontiguousarray(x, dtype=dtype) for x in p]
     f = lib().or_q_tri2d_mean_ratio_f64 if dtype == np.float64 else lib().or_q_tri2d_mean_ratio_f32
     return f(*[_p(x) for x in p])
+
+
+# ---- the reference's own element quality functions (oracle/_ref/libref_quality.so) ----------
+# Built by ``make ref`` from the reference's dmo/DMOQuality.h as it lies (ref_quality.cu); they
+# run on the GPU. Item kinds (ref_quality.cu RefFn) and the reference's QualityCriterium values:
+RQ_TET, RQ_HEX, RQ_QUAD, RQ_TRI, RQ_TRI2D, RQ_TRI_N, RQ_QUAD_N = range(7)
+REF_MEAN_RATIO, REF_MIN_ANGLE, REF_MAX_ANGLE = 0, 4, 6
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libref_quality.so")
+_ref = None
+
+
+def ref_lib():
+    """The compiled reference quality functions, or None where they were not built (the
+    reference sources were absent when ``build()`` ran)."""
+    global _ref
+    if _ref is None and os.path.exists(REF_LIB_PATH):
+        L = C.CDLL(REF_LIB_PATH)
+        L.refq_eval.restype = C.c_int
+        L.refq_eval.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        _ref = L
+    return _ref
+
+
+def ref_quality(fn, crit, pts, nrm=None):
+    """The reference function ``fn`` (RQ_*) with criterion ``crit`` on each item: pts has shape
+    (n, corners, 3), nrm (n, 3) for RQ_TRI_N / RQ_QUAD_N. Float32 results from the GPU."""
+    pts = np.ascontiguousarray(pts, dtype=np.float32)
+    n = pts.shape[0]
+    out = np.zeros(n, dtype=np.float32)
+    nr = None if nrm is None else np.ascontiguousarray(nrm, dtype=np.float32)
+    st = ref_lib().refq_eval(fn, crit, _p(pts), None if nr is None else _p(nr), n, _p(out))
+    if st != 0:
+        raise RuntimeError(f"refq_eval failed with CUDA error {st}")
+    return out
+
+
+def element_metric_f64(fn, crit, pts, nrm=None):
+    """The oracle's FP64 restatement of the same reference function on each item (the
+    functions the oracle's DMO and quality restatements use)."""
+    L = lib()
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    nrm = None if nrm is None else np.ascontiguousarray(nrm, dtype=np.float64)
+    out = np.zeros(pts.shape[0])
+    for i, e in enumerate(pts):
+        c = [_p(e[j]) for j in range(e.shape[0])]
+        if fn == RQ_TET:
+            f = {REF_MEAN_RATIO: L.or_q_tet_mean_ratio_f64, REF_MIN_ANGLE: L.or_q_tet_min_angle_f64,
+                 REF_MAX_ANGLE: L.or_q_tet_max_angle_f64}[crit]
+            out[i] = f(*c)
+        elif fn == RQ_HEX:
+            out[i] = L.or_q_hex_f64(_p(e))
+        elif fn == RQ_QUAD:
+            out[i] = L.or_q_quad_f64(*c, None)
+        elif fn == RQ_QUAD_N:
+            out[i] = L.or_q_quad_f64(*c, _p(nrm[i]))
+        elif fn == RQ_TRI2D:
+            f = {REF_MEAN_RATIO: L.or_q_tri2d_mean_ratio_f64, REF_MIN_ANGLE: L.or_q_tri2d_min_angle_f64,
+                 REF_MAX_ANGLE: L.or_q_tri2d_max_angle_f64}[crit]
+            out[i] = f(*c)
+        elif fn in (RQ_TRI, RQ_TRI_N):
+            nv = None if fn == RQ_TRI else _p(nrm[i])
+            if crit == REF_MEAN_RATIO:
+                q = L.or_q_tri3d_f64(*c)
+                if fn == RQ_TRI_N:
+                    t = np.cross(e[1] - e[0], e[2] - e[0])
+                    d = float(np.dot(t / np.linalg.norm(t), nrm[i]))
+                    q = q if d > 0 else (-q if d < 0 else 0.0)
+                out[i] = q
+            else:
+                out[i] = L.or_q_tri3d_angle_f64(*c, nv, int(crit == REF_MAX_ANGLE))
+        else:
+            raise ValueError(fn)
+    return out

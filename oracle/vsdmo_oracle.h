@@ -10,9 +10,12 @@
  * no sample meshes, and its live colouring is the closed cusparseScsrcolor. The restatement
  * is pinned by (a) known-answer cases the reference's formulas fix exactly (regular
  * simplices / unit cube = quality 1, flipped elements return their signed volume/area,
- * unperturbed structured meshes are fixed points) and (b) golden fixtures produced by this
- * restatement and committed under tests/golden/. See the file header of each .c file for
- * the reference lines each function follows.
+ * unperturbed structured meshes are fixed points), (b) golden fixtures produced by this
+ * restatement and committed under tests/golden/, and (c) the reference's own element quality
+ * functions (dmo/DMOQuality.h compiled unmodified into oracle/_ref/ by the Makefile target
+ * `ref`, through ref_quality.cu): every element metric restated here matches them on the GPU
+ * within FP32 rounding (tests/test_gpu_reference_metrics.py). See the file header of each .c
+ * file for the reference lines each function follows.
  *
  * Two arithmetic modes of the DMO grid search are provided:
  *   *_f64 : the reference kernels' algorithm and formulas (mean ratio with cbrt, candidate

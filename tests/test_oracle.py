@@ -261,3 +261,14 @@ def test_hex_oracle_fixed_point_and_progress(oracle_mod):
     x64, mn64, me64 = m.optimize_f64(m.xyz.astype(np.float64), 3)
     assert me32[-1] > q0.mean() and mn32[-1] >= q0.min()
     assert abs(mn32[-1] - mn64[-1]) < 1e-4 and abs(me32[-1] - me64[-1]) < 1e-4
+
+
+def test_reference_quality_library_exports():
+    """Where the reference's sources were present at build time, its own quality functions
+    (dmo/DMOQuality.h, compiled unmodified by oracle/Makefile target ``ref``) load and export
+    the entry point the GPU tests evaluate them through."""
+    from oracle import oracle as O
+    L = O.ref_lib()
+    if L is None:
+        pytest.skip("the reference's quality functions were not built here")
+    assert hasattr(L, "refq_eval")
