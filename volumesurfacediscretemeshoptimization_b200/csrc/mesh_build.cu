@@ -546,14 +546,7 @@ struct Builder {
     // stable partition of [0, n): flag == first_value first; returns the number of those
     int stable_partition(const uint8_t* d_flags, int n, int first_value, DBuf<int>& order) {
         order.alloc(n, s);
-        DBuf<uint8_t> inv(n, s);
-        k_not<<<G(n), 256, 0, s>>>(d_flags, inv.p, n);
-        VSDMO_CHECK_LAUNCH();
-        const uint8_t* a = first_value ? d_flags : inv.p;
-        const uint8_t* b = first_value ? inv.p : d_flags;
-        int na = compact_flags(a, n, order.p, s);
-        compact_flags(b, n, order.p + na, s);
-        return na;
+        return stable_partition_flags(d_flags, n, first_value, order.p, s);
     }
 
     // colour the range [lo, lo+num) given its adjacency pairs; sort it by colour

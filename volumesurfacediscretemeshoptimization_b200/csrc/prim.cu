@@ -162,6 +162,23 @@ __global__ void k_compact_scatter(const uint8_t* f, const int* pos, long n, int*
         if (f[i]) out[pos[i]] = (int)i;
 }
 
+// flag == first ? 1 : 0
+__global__ void k_match_to_int(const uint8_t* f, int first, int* o, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        o[i] = ((f[i] != 0) == (first != 0)) ? 1 : 0;
+}
+
+// stable partition: matching index i goes to pos[i], the others after the *total matching
+// ones, in index order (i - pos[i] non-matching indices precede i)
+__global__ void k_partition_scatter(const uint8_t* f, int first, const int* pos, const int* total, long n,
+                                    int* out) {
+    const int nm = *total;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const bool match = (f[i] != 0) == (first != 0);
+        out[match ? pos[i] : nm + (int)(i - pos[i])] = (int)i;
+    }
+}
+
 __global__ void k_count_keys(const uint32_t* keys, long n, int* counts) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         atomicAdd(&counts[keys[i]], 1);
@@ -221,6 +238,17 @@ int compact_flags(const uint8_t* d_flags, long n, int* d_out_index, cudaStream_t
     VSDMO_CHECK_LAUNCH();
     exclusive_scan(pos.p, pos.p, n, tot.p, s);
     k_compact_scatter<<<grid_for(n, 256), 256, 0, s>>>(d_flags, pos.p, n, d_out_index);
+    VSDMO_CHECK_LAUNCH();
+    return read_scalar(tot.p, s);
+}
+
+int stable_partition_flags(const uint8_t* d_flags, long n, int first_value, int* d_order, cudaStream_t s) {
+    if (n <= 0) return 0;
+    DBuf<int> pos(n, s), tot(1, s);
+    k_match_to_int<<<grid_for(n, 256), 256, 0, s>>>(d_flags, first_value, pos.p, n);
+    VSDMO_CHECK_LAUNCH();
+    exclusive_scan(pos.p, pos.p, n, tot.p, s);
+    k_partition_scatter<<<grid_for(n, 256), 256, 0, s>>>(d_flags, first_value, pos.p, tot.p, n, d_order);
     VSDMO_CHECK_LAUNCH();
     return read_scalar(tot.p, s);
 }

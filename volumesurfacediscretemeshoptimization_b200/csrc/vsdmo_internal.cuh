@@ -102,6 +102,9 @@ void exclusive_scan(const int* d_in, int* d_out, long n, int* d_total, cudaStrea
 void radix_sort_pairs(uint32_t* keys, uint32_t* vals, long n, int bits, cudaStream_t s);
 // Stable compaction: out[j] = i for the flagged positions i, in increasing order; returns count.
 int compact_flags(const uint8_t* d_flags, long n, int* d_out_index, cudaStream_t s);
+// stable partition of [0, n) into d_order: indices with (flag != 0) == first_value first, then
+// the rest, each in index order; returns the number of the first group (one host read)
+int stable_partition_flags(const uint8_t* d_flags, long n, int first_value, int* d_order, cudaStream_t s);
 // CSR offsets [K+1] from n keys already sorted ascending (keys < K).
 void rowptr_from_sorted(const uint32_t* d_sorted_keys, long n, int K, int* d_rowptr, cudaStream_t s);
 int bits_for(uint32_t maxval);
