@@ -281,14 +281,6 @@ __global__ void k_quad_edge_pairs(const int* quads, int nQ, int lo, int num, uin
     }
 }
 
-__global__ void k_unique_flags(const uint32_t* ks, const uint32_t* vs, long n, uint8_t* f) {
-    GRID_STRIDE(i, n) f[i] = (i == 0 || ks[i] != ks[i - 1] || vs[i] != vs[i - 1]) ? 1 : 0;
-}
-
-__global__ void k_gather_pairs(const int* idx, int n, const uint32_t* ks, const uint32_t* vs, uint32_t* ko, int* vo) {
-    GRID_STRIDE(i, n) { ko[i] = ks[idx[i]]; vo[i] = (int)vs[idx[i]]; }
-}
-
 // ---- JPL colouring ---------------------------------------------------------------------------
 __global__ void k_fill_int(int* a, long n, int v) { GRID_STRIDE(i, n) a[i] = v; }
 
@@ -556,19 +548,8 @@ struct Builder {
         DBuf<int> rowptr(num + 1, s);
         DBuf<int> col;
         if (npairs > 0) {
-            int bits = bits_for((uint32_t)(num - 1));
-            radix_sort_pairs(vs.p, ks.p, npairs, bits, s);   // by neighbour
-            radix_sort_pairs(ks.p, vs.p, npairs, bits, s);   // then stably by source
-            DBuf<uint8_t> uf(npairs, s);
-            k_unique_flags<<<G(npairs), 256, 0, s>>>(ks.p, vs.p, npairs, uf.p);
-            VSDMO_CHECK_LAUNCH();
-            DBuf<int> uidx(npairs, s);
-            int nu = compact_flags(uf.p, npairs, uidx.p, s);
-            DBuf<uint32_t> uk(nu, s);
-            col.alloc(nu, s);
-            k_gather_pairs<<<G(nu), 256, 0, s>>>(uidx.p, nu, ks.p, vs.p, uk.p, col.p);
-            VSDMO_CHECK_LAUNCH();
-            rowptr_from_sorted(uk.p, nu, num, rowptr.p, s);
+            col.alloc(npairs, s);
+            csr_unique_from_pairs(ks.p, vs.p, npairs, num, rowptr.p, col.p, s);
         } else {
             rowptr.zero();
             col.alloc(1, s);

@@ -183,6 +183,55 @@ __global__ void k_count_keys(const uint32_t* keys, long n, int* counts) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
         atomicAdd(&counts[keys[i]], 1);
 }
+// ---- CSR of the distinct pairs ------------------------------------------------------------------
+// bucket the values by key: each pair takes the next free slot of its key's row (the order
+// inside a row is arbitrary; k_row_unique makes the row canonical)
+__global__ void k_bucket_scatter(const uint32_t* keys, const uint32_t* vals, long n, int* cursor, uint32_t* out) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[atomicAdd(&cursor[keys[i]], 1)] = vals[i];
+}
+
+// one warp per row (grid-stride over rows): the row's distinct values in ascending order to
+// out[rs[r] ...] and their number to u[r]. A value is kept at its first occurrence in the row,
+// and its place is the number of kept values below it. Rows are short (the edges of one
+// vertex's ring), so the quadratic scans cost less than sorting the rows.
+__global__ void k_row_unique(const int* rs, const uint32_t* v, long K, uint8_t* keep, uint32_t* out, int* u) {
+    const int lane = threadIdx.x & 31;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < K; r += nw) {
+        const int b = rs[r], n = rs[r + 1] - b;
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t x = v[b + i];
+            bool first = true;
+            for (int j = 0; j < i && first; ++j) first = v[b + j] != x;
+            keep[b + i] = first ? 1 : 0;
+        }
+        __syncwarp();
+        int cnt = 0;
+        for (int i = lane; i < n; i += 32) {
+            if (!keep[b + i]) continue;
+            const uint32_t x = v[b + i];
+            int rank = 0;
+            for (int j = 0; j < n; ++j) rank += (keep[b + j] && v[b + j] < x) ? 1 : 0;
+            out[b + rank] = x;
+            ++cnt;
+        }
+        cnt = __reduce_add_sync(FULL, cnt);
+        if (lane == 0) u[r] = cnt;
+        __syncwarp();
+    }
+}
+
+// one warp per row: the distinct values of row r to col[rowptr[r] ...]
+__global__ void k_row_copy(const int* rs, const int* rowptr, const uint32_t* src, long K, int* col) {
+    const int lane = threadIdx.x & 31;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < K; r += nw) {
+        const int b = rs[r], o = rowptr[r], n = rowptr[r + 1] - o;
+        for (int j = lane; j < n; j += 32) col[o + j] = (int)src[b + j];
+    }
+}
+
 }  // namespace
 
 int bits_for(uint32_t maxval) {
@@ -261,6 +310,34 @@ void rowptr_from_sorted(const uint32_t* d_sorted_keys, long n, int K, int* d_row
         VSDMO_CHECK_LAUNCH();
     }
     exclusive_scan(counts.p, d_rowptr, (long)K + 1, nullptr, s);
+}
+
+void csr_unique_from_pairs(const uint32_t* d_keys, const uint32_t* d_vals, long n, int K, int* d_rowptr, int* d_col,
+                           cudaStream_t s) {
+    if (K <= 0) {
+        VSDMO_CUDA(cudaMemsetAsync(d_rowptr, 0, sizeof(int), s));
+        return;
+    }
+    const long cap = std::max(n, 1L);
+    DBuf<int> counts(K, s), rs((long)K + 1, s), cursor(K, s), u(K, s);
+    DBuf<uint32_t> bucket(cap, s), uniq(cap, s);
+    DBuf<uint8_t> keep(cap, s);
+    counts.zero();
+    if (n > 0) {
+        k_count_keys<<<grid_for(n, 256), 256, 0, s>>>(d_keys, n, counts.p);
+        VSDMO_CHECK_LAUNCH();
+    }
+    exclusive_scan(counts.p, rs.p, K, rs.p + K, s);
+    VSDMO_CUDA(cudaMemcpyAsync(cursor.p, rs.p, sizeof(int) * K, cudaMemcpyDeviceToDevice, s));
+    if (n > 0) {
+        k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(d_keys, d_vals, n, cursor.p, bucket.p);
+        VSDMO_CHECK_LAUNCH();
+    }
+    k_row_unique<<<grid_for((long)K * 32, 256), 256, 0, s>>>(rs.p, bucket.p, K, keep.p, uniq.p, u.p);
+    VSDMO_CHECK_LAUNCH();
+    exclusive_scan(u.p, d_rowptr, K, d_rowptr + K, s);
+    k_row_copy<<<grid_for((long)K * 32, 256), 256, 0, s>>>(rs.p, d_rowptr, uniq.p, K, d_col);
+    VSDMO_CHECK_LAUNCH();
 }
 
 cudaMemPool_t device_pool() {

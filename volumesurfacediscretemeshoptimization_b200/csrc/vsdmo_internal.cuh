@@ -105,6 +105,11 @@ int compact_flags(const uint8_t* d_flags, long n, int* d_out_index, cudaStream_t
 // stable partition of [0, n) into d_order: indices with (flag != 0) == first_value first, then
 // the rest, each in index order; returns the number of the first group (one host read)
 int stable_partition_flags(const uint8_t* d_flags, long n, int first_value, int* d_order, cudaStream_t s);
+// CSR (rows 0..K-1) of the distinct (key, value) pairs, each row's values ascending: the same
+// arrays as a stable sort by (key, value) followed by dropping repeats. d_rowptr holds K + 1
+// ints, d_col at least n.
+void csr_unique_from_pairs(const uint32_t* d_keys, const uint32_t* d_vals, long n, int K, int* d_rowptr, int* d_col,
+                           cudaStream_t s);
 // CSR offsets [K+1] from n keys already sorted ascending (keys < K).
 void rowptr_from_sorted(const uint32_t* d_sorted_keys, long n, int K, int* d_rowptr, cudaStream_t s);
 int bits_for(uint32_t maxval);
