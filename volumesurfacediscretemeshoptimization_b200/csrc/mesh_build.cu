@@ -39,6 +39,9 @@ __device__ __forceinline__ uint32_t priority(uint32_t i, uint32_t seed) {
 }
 
 #define GRID_STRIDE(i, n) for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long)gridDim.x * blockDim.x)
+constexpr unsigned FULL = 0xffffffffu;
+
+__global__ void k_count_keys_u32(const uint32_t* keys, long n, int* counts) { GRID_STRIDE(i, n) atomicAdd(&counts[keys[i]], 1); }
 
 __global__ void k_input(const float* xyz, int nV, const int* elems, long nIdx, float4* pos, int* err, int* nonzero_z) {
     GRID_STRIDE(i, nV) {
@@ -80,36 +83,65 @@ __global__ void k_tet_faces(const int* tets, int nT, uint32_t* f0, uint32_t* f1,
     }
 }
 
-__device__ __forceinline__ int cmp3(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t b0, uint32_t b1, uint32_t b2) {
-    if (a0 != b0) return a0 < b0 ? -1 : 1;
-    if (a1 != b1) return a1 < b1 ? -1 : 1;
-    if (a2 != b2) return a2 < b2 ? -1 : 1;
-    return 0;
+// faces bucketed by their first vertex: row f0 holds (f1 << 32 | f2) of every face (f0, f1, f2)
+__global__ void k_face_bucket(const uint32_t* f0, const uint32_t* f1, const uint32_t* f2, long nF, int* cursor,
+                              unsigned long long* out) {
+    GRID_STRIDE(i, nF) out[atomicAdd(&cursor[f0[i]], 1)] = ((unsigned long long)f1[i] << 32) | f2[i];
 }
 
-// faces sorted lexicographically: an ascending face (a,b,c), b<c, pairs with the first (a,c,b)
-__global__ void k_pair_faces(const uint32_t* s0, const uint32_t* s1, const uint32_t* s2, long nF, uint8_t* paired, int* err) {
-    GRID_STRIDE(i, nF) {
-        uint32_t a = s0[i], b = s1[i], c = s2[i];
-        if (i + 1 < nF && s0[i + 1] == a && s1[i + 1] == b && s2[i + 1] == c) atomicMax(err, BE_NONMANIFOLD);
-        if (b < c) {
-            long lo = i + 1, hi = nF;
-            while (lo < hi) {
-                long mid = (lo + hi) >> 1;
-                if (cmp3(s0[mid], s1[mid], s2[mid], a, c, b) < 0) lo = mid + 1; else hi = mid;
+// one warp per row a (grid-stride over rows): face (a, b, c) is a boundary face unless the row
+// also holds its twin (a, c, b) (k_markDuplicateTris, mesh/MeshGPUCommon.cu:56-74); an exact
+// repeat is a non-manifold input. The boundary faces get their place among the row's boundary
+// faces in (b, c) order, so rows in vertex order give the lexicographic order of a sort.
+__global__ void k_face_rows(const int* rs, const unsigned long long* fb, long K, uint8_t* bnd, int* rank, int* u,
+                            int* err) {
+    const int lane = threadIdx.x & 31;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < K; r += nw) {
+        const int b0 = rs[r], n = rs[r + 1] - b0;
+        for (int i = lane; i < n; i += 32) {
+            const unsigned long long x = fb[b0 + i], twin = (x << 32) | (x >> 32);
+            bool paired = false, repeat = false;
+            for (int j = 0; j < n; ++j) {
+                if (j == i) continue;
+                const unsigned long long y = fb[b0 + j];
+                repeat |= y == x;
+                paired |= y == twin;
             }
-            if (lo < nF && s0[lo] == a && s1[lo] == c && s2[lo] == b) { paired[i] = 1; paired[lo] = 1; }
+            if (repeat) atomicMax(err, BE_NONMANIFOLD);
+            bnd[b0 + i] = paired ? 0 : 1;
         }
+        __syncwarp();
+        int cnt = 0;
+        for (int i = lane; i < n; i += 32) {
+            if (!bnd[b0 + i]) continue;
+            const unsigned long long x = fb[b0 + i];
+            int k = 0;
+            for (int j = 0; j < n; ++j) k += (bnd[b0 + j] && fb[b0 + j] < x) ? 1 : 0;
+            rank[b0 + i] = k;
+            ++cnt;
+        }
+        cnt = __reduce_add_sync(FULL, cnt);
+        if (lane == 0) u[r] = cnt;
+        __syncwarp();
     }
 }
 
-__global__ void k_emit_boundary_tris(const int* idx, int nB, const uint32_t* s0, const uint32_t* s1, const uint32_t* s2,
-                                     int* tris, uint8_t* isB2) {
-    GRID_STRIDE(i, nB) {
-        int j = idx[i];
-        int a = s0[j], b = s1[j], c = s2[j];
-        tris[3 * i] = a; tris[3 * i + 1] = b; tris[3 * i + 2] = c;
-        isB2[a] = 1; isB2[b] = 1; isB2[c] = 1;
+// one warp per row: the row's boundary faces to tris[offs[a] + rank], their vertices flagged
+__global__ void k_face_emit(const int* rs, const unsigned long long* fb, const uint8_t* bnd, const int* rank,
+                            const int* offs, long K, int* tris, uint8_t* isB2) {
+    const int lane = threadIdx.x & 31;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < K; r += nw) {
+        const int b0 = rs[r], n = rs[r + 1] - b0;
+        for (int i = lane; i < n; i += 32) {
+            if (!bnd[b0 + i]) continue;
+            const long p = offs[r] + rank[b0 + i];
+            const unsigned long long x = fb[b0 + i];
+            const int b = (int)(x >> 32), c = (int)(x & 0xffffffffu);
+            tris[3 * p] = (int)r; tris[3 * p + 1] = b; tris[3 * p + 2] = c;
+            isB2[r] = 1; isB2[b] = 1; isB2[c] = 1;
+        }
     }
 }
 
@@ -717,40 +749,33 @@ struct Builder {
     }
 
     void tet_boundary() {
-        const int nT = m.nE;
+        const int nT = m.nE, nV = m.nV;
         const long nF = 4L * nT;
-        DBuf<uint32_t> f0(nF, s), f1(nF, s), f2(nF, s), key(nF, s), order(nF, s);
+        DBuf<uint32_t> f0(nF, s), f1(nF, s), f2(nF, s);
         k_tet_faces<<<G(nT), 256, 0, s>>>(m.elems.p, nT, f0.p, f1.p, f2.p);
         VSDMO_CHECK_LAUNCH();
-        k_iota<<<G(nF), 256, 0, s>>>(order.p, nF);
+        // bucket the faces by first vertex (counting sort), then pair each row's faces in place
+        DBuf<int> counts(nV, s), rs((long)nV + 1, s), cursor(nV, s), u(nV, s), offs((long)nV + 1, s), rank(nF, s);
+        DBuf<unsigned long long> fb(nF, s);
+        DBuf<uint8_t> bnd(nF, s);
+        counts.zero();
+        k_count_keys_u32<<<G(nF), 256, 0, s>>>(f0.p, nF, counts.p);
         VSDMO_CHECK_LAUNCH();
-        const int bits = bits_for((uint32_t)(m.nV - 1));
-        const uint32_t* comps[3] = { f2.p, f1.p, f0.p };
-        for (int c = 0; c < 3; ++c) {
-            k_gather_key<<<G(nF), 256, 0, s>>>(comps[c], order.p, key.p, nF);
-            VSDMO_CHECK_LAUNCH();
-            radix_sort_pairs(key.p, order.p, nF, bits, s);
-        }
-        DBuf<uint32_t> s0(nF, s), s1(nF, s), s2(nF, s);
-        k_gather_key<<<G(nF), 256, 0, s>>>(f0.p, order.p, s0.p, nF);
-        k_gather_key<<<G(nF), 256, 0, s>>>(f1.p, order.p, s1.p, nF);
-        k_gather_key<<<G(nF), 256, 0, s>>>(f2.p, order.p, s2.p, nF);
+        exclusive_scan(counts.p, rs.p, nV, rs.p + nV, s);
+        VSDMO_CUDA(cudaMemcpyAsync(cursor.p, rs.p, sizeof(int) * nV, cudaMemcpyDeviceToDevice, s));
+        k_face_bucket<<<G(nF), 256, 0, s>>>(f0.p, f1.p, f2.p, nF, cursor.p, fb.p);
         VSDMO_CHECK_LAUNCH();
-        DBuf<uint8_t> paired(nF, s), unpaired(nF, s);
-        paired.zero();
         err.zero();
-        k_pair_faces<<<G(nF), 256, 0, s>>>(s0.p, s1.p, s2.p, nF, paired.p, err.p);
+        k_face_rows<<<G(32L * nV), 256, 0, s>>>(rs.p, fb.p, nV, bnd.p, rank.p, u.p, err.p);
         VSDMO_CHECK_LAUNCH();
         check_err(err, s, "boundary faces");
-        k_not<<<G(nF), 256, 0, s>>>(paired.p, unpaired.p, nF);
-        VSDMO_CHECK_LAUNCH();
-        DBuf<int> bidx(nF, s);
-        const int nB = compact_flags(unpaired.p, nF, bidx.p, s);
+        exclusive_scan(u.p, offs.p, nV, offs.p + nV, s);
+        const int nB = read_scalar(offs.p + nV, s);
         m.nTris = nB;
         m.tris.alloc(3L * nB, s);
         m.isB2.alloc(m.nV, s);
         m.isB2.zero();
-        k_emit_boundary_tris<<<G(nB), 256, 0, s>>>(bidx.p, nB, s0.p, s1.p, s2.p, m.tris.p, m.isB2.p);
+        k_face_emit<<<G(32L * nV), 256, 0, s>>>(rs.p, fb.p, bnd.p, rank.p, offs.p, nV, m.tris.p, m.isB2.p);
         VSDMO_CHECK_LAUNCH();
     }
 
