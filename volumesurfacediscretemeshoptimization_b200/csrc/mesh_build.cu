@@ -632,11 +632,8 @@ struct Builder {
         {
             DBuf<uint32_t> keys(nHE1, s), order(nHE1, s);
             VSDMO_CUDA(cudaMemcpyAsync(keys.p, m.tris.p, sizeof(int) * nHE1, cudaMemcpyDeviceToDevice, s));
-            k_iota<<<G(nHE1), 256, 0, s>>>(order.p, nHE1);
-            VSDMO_CHECK_LAUNCH();
-            radix_sort_pairs(keys.p, order.p, nHE1, bits_for((uint32_t)(nS - 1)), s);
             DBuf<int> rowptr(nS + 1, s);
-            rowptr_from_sorted(keys.p, nHE1, nS, rowptr.p, s);
+            stable_sort_short_rows(keys.p, order.p, nHE1, nS, rowptr.p, s);
             DBuf<int4> he(nHE1, s);
             k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, m.fk, he.p);
             VSDMO_CHECK_LAUNCH();
@@ -702,12 +699,8 @@ struct Builder {
         const long nHE1 = (long)m.fk * m.nTris;
         DBuf<uint32_t> keys(nHE1, s), order(nHE1, s);
         VSDMO_CUDA(cudaMemcpyAsync(keys.p, m.tris.p, sizeof(int) * nHE1, cudaMemcpyDeviceToDevice, s));
-        k_iota<<<G(nHE1), 256, 0, s>>>(order.p, nHE1);
-        VSDMO_CHECK_LAUNCH();
-        const int bits = bits_for((uint32_t)(nS - 1));
-        radix_sort_pairs(keys.p, order.p, nHE1, bits, s);
         DBuf<int> rowptr1(nS + 1, s);
-        rowptr_from_sorted(keys.p, nHE1, nS, rowptr1.p, s);
+        stable_sort_short_rows(keys.p, order.p, nHE1, nS, rowptr1.p, s);
         DBuf<int4> he1(nHE1, s);
         k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, m.fk, he1.p);
         VSDMO_CHECK_LAUNCH();
@@ -723,11 +716,8 @@ struct Builder {
         DBuf<int4> rec(nHE, s);
         k_with_dummies<<<G(nHE), 256, 0, s>>>(keys.p, he1.p, nHE1, didx.p, nD, k2.p, rec.p);
         VSDMO_CHECK_LAUNCH();
-        k_iota<<<G(nHE), 256, 0, s>>>(o2.p, nHE);
-        VSDMO_CHECK_LAUNCH();
-        radix_sort_pairs(k2.p, o2.p, nHE, bits, s);
         m.he_rowptr.alloc(nS + 1, s);
-        rowptr_from_sorted(k2.p, nHE, nS, m.he_rowptr.p, s);
+        stable_sort_short_rows(k2.p, o2.p, nHE, nS, m.he_rowptr.p, s);
         DBuf<int4> in(nHE, s);
         k_gather<int4><<<G(nHE), 256, 0, s>>>(rec.p, o2.p, in.p, nHE);
         VSDMO_CHECK_LAUNCH();
@@ -841,11 +831,8 @@ struct Builder {
         const long nH = 4L * m.nE;
         DBuf<uint32_t> keys(nH, s), order(nH, s);
         VSDMO_CUDA(cudaMemcpyAsync(keys.p, m.elems.p, sizeof(int) * nH, cudaMemcpyDeviceToDevice, s));
-        k_iota<<<G(nH), 256, 0, s>>>(order.p, nH);
-        VSDMO_CHECK_LAUNCH();
-        radix_sort_pairs(keys.p, order.p, nH, bits_for((uint32_t)(m.nV - 1)), s);
         m.hf_rowptr.alloc(m.nV + 1, s);
-        rowptr_from_sorted(keys.p, nH, m.nV, m.hf_rowptr.p, s);
+        stable_sort_short_rows(keys.p, order.p, nH, m.nV, m.hf_rowptr.p, s);
         m.hf.alloc(nH, s);
         k_halffaces<<<G(nH), 256, 0, s>>>(order.p, nH, m.elems.p, m.hf.p);
         VSDMO_CHECK_LAUNCH();

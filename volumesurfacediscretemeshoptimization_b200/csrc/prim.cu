@@ -232,6 +232,29 @@ __global__ void k_row_copy(const int* rs, const int* rowptr, const uint32_t* src
     }
 }
 
+// bucket the indices [0, n) by key (arbitrary order inside a row)
+__global__ void k_bucket_index(const uint32_t* keys, long n, int* cursor, uint32_t* out) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[atomicAdd(&cursor[keys[i]], 1)] = (uint32_t)i;
+}
+
+// one warp per row (grid-stride): the row's indices in ascending order (each placed by the
+// number of smaller indices in the row: they are distinct), and the row's key beside each
+__global__ void k_row_order(const int* rs, const uint32_t* idx, long K, uint32_t* order, uint32_t* keys) {
+    const int lane = threadIdx.x & 31;
+    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long r = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < K; r += nw) {
+        const int b = rs[r], n = rs[r + 1] - b;
+        for (int i = lane; i < n; i += 32) {
+            const uint32_t x = idx[b + i];
+            int k = 0;
+            for (int j = 0; j < n; ++j) k += idx[b + j] < x ? 1 : 0;
+            order[b + k] = x;
+            keys[b + i] = (uint32_t)r;
+        }
+    }
+}
+
 }  // namespace
 
 int bits_for(uint32_t maxval) {
@@ -337,6 +360,24 @@ void csr_unique_from_pairs(const uint32_t* d_keys, const uint32_t* d_vals, long 
     VSDMO_CHECK_LAUNCH();
     exclusive_scan(u.p, d_rowptr, K, d_rowptr + K, s);
     k_row_copy<<<grid_for((long)K * 32, 256), 256, 0, s>>>(rs.p, d_rowptr, uniq.p, K, d_col);
+    VSDMO_CHECK_LAUNCH();
+}
+
+void stable_sort_short_rows(uint32_t* d_keys, uint32_t* d_order, long n, int K, int* d_rowptr, cudaStream_t s) {
+    if (K <= 0) return;
+    DBuf<int> counts(K, s), cursor(K, s);
+    DBuf<uint32_t> bucket(std::max(n, 1L), s);
+    counts.zero();
+    if (n > 0) {
+        k_count_keys<<<grid_for(n, 256), 256, 0, s>>>(d_keys, n, counts.p);
+        VSDMO_CHECK_LAUNCH();
+    }
+    exclusive_scan(counts.p, d_rowptr, K, d_rowptr + K, s);
+    if (n <= 0) return;
+    VSDMO_CUDA(cudaMemcpyAsync(cursor.p, d_rowptr, sizeof(int) * K, cudaMemcpyDeviceToDevice, s));
+    k_bucket_index<<<grid_for(n, 256), 256, 0, s>>>(d_keys, n, cursor.p, bucket.p);
+    VSDMO_CHECK_LAUNCH();
+    k_row_order<<<grid_for((long)K * 32, 256), 256, 0, s>>>(d_rowptr, bucket.p, K, d_order, d_keys);
     VSDMO_CHECK_LAUNCH();
 }
 

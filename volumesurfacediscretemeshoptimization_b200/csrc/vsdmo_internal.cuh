@@ -108,6 +108,12 @@ int stable_partition_flags(const uint8_t* d_flags, long n, int first_value, int*
 // CSR (rows 0..K-1) of the distinct (key, value) pairs, each row's values ascending: the same
 // arrays as a stable sort by (key, value) followed by dropping repeats. d_rowptr holds K + 1
 // ints, d_col at least n.
+// stable sort of [0, n) by d_keys (values in [0, K)): d_order receives the original indices in
+// (key, index) order, d_keys the keys in that order and d_rowptr (K + 1 ints) the row starts,
+// the same arrays as radix_sort_pairs over (keys, 0..n-1) followed by rowptr_from_sorted. For
+// keys whose rows are short (a vertex's elements or halfedges): each row is ordered by one warp
+// in time quadratic in its length.
+void stable_sort_short_rows(uint32_t* d_keys, uint32_t* d_order, long n, int K, int* d_rowptr, cudaStream_t s);
 void csr_unique_from_pairs(const uint32_t* d_keys, const uint32_t* d_vals, long n, int K, int* d_rowptr, int* d_col,
                            cudaStream_t s);
 // CSR offsets [K+1] from n keys already sorted ascending (keys < K).
