@@ -316,7 +316,11 @@ __global__ void k_quad_edge_pairs(const int* quads, int nQ, int lo, int num, uin
 // ---- JPL colouring ---------------------------------------------------------------------------
 __global__ void k_fill_int(int* a, long n, int v) { GRID_STRIDE(i, n) a[i] = v; }
 
-__global__ void k_jpl_round(int n, const int* rowptr, const int* col, uint32_t seed, int c, int* colors, int* remaining) {
+// prev: the previous round's count of uncoloured vertices in the same host read (null for the
+// first round of one); when it is 0 every vertex has its colour and the round has nothing to do
+__global__ void k_jpl_round(int n, const int* rowptr, const int* col, uint32_t seed, int c, int* colors, int* remaining,
+                            const int* prev) {
+    if (prev && *prev == 0) return;
     GRID_STRIDE(i, n) {
         if (colors[i] != -1) continue;
         uint32_t pi = priority((uint32_t)i, seed);
@@ -597,7 +601,8 @@ struct Builder {
             if (c0 > num + 1) throw Error(VSDMO_E_CUDA, "colouring did not terminate");
             remaining.zero();
             for (int i = 0; i < CH; ++i) {
-                k_jpl_round<<<G(num), 256, 0, s>>>(num, rowptr.p, col.p, m.seed, c0 + i, colors.p, remaining.p + i);
+                k_jpl_round<<<G(num), 256, 0, s>>>(num, rowptr.p, col.p, m.seed, c0 + i, colors.p, remaining.p + i,
+                                                   i > 0 ? remaining.p + i - 1 : nullptr);
                 VSDMO_CHECK_LAUNCH();
             }
             const std::vector<int> left = remaining.to_host();
