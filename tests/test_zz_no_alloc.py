@@ -80,3 +80,77 @@ def test_no_alloc_rejects_oversized_meshes(vsdmo):
     st = _run_noalloc(lib, _capi.TET, 0, d, 4, di, 8_388_609, 0.5, d, dd, di, 0)
     assert st == _capi.E_ARG
     assert b"8388608" in lib.vsdmo_last_error()
+
+
+def _outputs(dev):
+    import torch
+    return (torch.empty(1, dtype=torch.float32, device=dev), torch.empty(1, dtype=torch.float64, device=dev),
+            torch.empty(1, dtype=torch.int32, device=dev))
+
+
+def test_no_alloc_skips_elements_outside_the_mesh(vsdmo):
+    """One index past the last vertex and one negative index: nothing outside the caller's
+    arrays is read, the results say so (-1 and NaN), and the next call is correct again."""
+    import torch
+    from volumesurfacediscretemeshoptimization_b200 import _capi
+    lib = _capi.lib()
+    xyz, el = G.tet_cube(6, seed=3)
+    mesh = vsdmo.DMOMeshTet(xyz, el)
+    ref_min, ref_mean = vsdmo.DMOTetClass(mesh, n_iter=1).quality_stats()
+    dev = torch.device("cuda", 0)
+    d_xyz = torch.from_numpy(xyz).to(dev).contiguous()
+    bad = el.copy()
+    bad[5, 2] = len(xyz)
+    bad[9, 0] = -3
+    d_bad = torch.from_numpy(bad).to(dev).contiguous()
+    d_el = torch.from_numpy(el).to(dev).contiguous()
+    out_min, out_sum, out_below = _outputs(dev)
+    st = _run_noalloc(lib, _capi.TET, 0, d_xyz, len(xyz), d_bad, len(el), 0.5, out_min, out_sum, out_below, 0)
+    assert st == 0, lib.vsdmo_last_error()
+    torch.cuda.synchronize(dev)
+    assert int(out_below.item()) == -1
+    assert np.isnan(float(out_min.item())) and np.isnan(float(out_sum.item()))
+    st = _run_noalloc(lib, _capi.TET, 0, d_xyz, len(xyz), d_el, len(el), 0.5, out_min, out_sum, out_below, 0)
+    assert st == 0, lib.vsdmo_last_error()
+    torch.cuda.synchronize(dev)
+    assert abs(float(out_min.item()) - ref_min) <= TOL
+    assert abs(float(out_sum.item()) / len(el) - ref_mean) <= TOL
+    assert int(out_below.item()) >= 0
+
+
+def test_no_alloc_large_mesh_with_clamped_blocks(vsdmo):
+    """4.37 M tetrahedra: more than 256 threads x 32 elements x 1024 blocks / 2, so the grid is
+    clamped to its 1024 blocks and every thread strides over more than 16 elements."""
+    import torch
+    from volumesurfacediscretemeshoptimization_b200 import _capi
+    lib = _capi.lib()
+    xyz, el = G.tet_cube(90, seed=4)
+    assert len(el) > 256 * 32 * 1024 // 2
+    mesh = vsdmo.DMOMeshTet(xyz, el)
+    ref_min, ref_mean = vsdmo.DMOTetClass(mesh, n_iter=1).quality_stats()
+    dev = torch.device("cuda", 0)
+    d_xyz = torch.from_numpy(xyz).to(dev).contiguous()
+    d_el = torch.from_numpy(el).to(dev).contiguous()
+    out_min, out_sum, out_below = _outputs(dev)
+    for _ in range(2):
+        st = _run_noalloc(lib, _capi.TET, 0, d_xyz, len(xyz), d_el, len(el), 0.5, out_min, out_sum, out_below, 0)
+        assert st == 0, lib.vsdmo_last_error()
+        torch.cuda.synchronize(dev)
+        assert abs(float(out_min.item()) - ref_min) <= TOL
+        assert abs(float(out_sum.item()) / len(el) - ref_mean) <= TOL
+
+
+def test_no_alloc_accepts_the_limit(vsdmo):
+    """Exactly 8,388,608 elements (all corners at vertex 0) is accepted and runs."""
+    import torch
+    from volumesurfacediscretemeshoptimization_b200 import _capi
+    lib = _capi.lib()
+    dev = torch.device("cuda", 0)
+    n = 8_388_608
+    d_xyz = torch.zeros(12, dtype=torch.float32, device=dev)
+    d_el = torch.zeros(4 * n, dtype=torch.int32, device=dev)
+    out_min, out_sum, out_below = _outputs(dev)
+    st = _run_noalloc(lib, _capi.TET, 0, d_xyz, 4, d_el, n, 0.5, out_min, out_sum, out_below, 0)
+    assert st == 0, lib.vsdmo_last_error()
+    torch.cuda.synchronize(dev)
+    assert int(out_below.item()) == 0   # degenerate tetrahedra give NaN qualities, never below

@@ -895,8 +895,8 @@ VSDMO_API vsdmo_status vsdmo_quality_reduce_noalloc(int elem_type, int flat, con
         return fail(VSDMO_E_ARG, "n_elems " + std::to_string(n_elems) + " exceeds the no-alloc limit of " +
                                      std::to_string(noalloc_max_elements()) + " elements per call");
     return guarded([&] {
-        quality_reduce_noalloc(elem_type == VSDMO_TET ? 4 : 3, d_xyz, d_elems, n_elems, threshold, d_min, d_sum, d_below,
-                               (cudaStream_t)cuda_stream);
+        quality_reduce_noalloc(elem_type == VSDMO_TET ? 4 : 3, d_xyz, n_vertices, d_elems, n_elems, threshold, d_min,
+                               d_sum, d_below, (cudaStream_t)cuda_stream);
     });
 }
 

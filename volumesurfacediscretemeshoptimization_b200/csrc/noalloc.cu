@@ -21,12 +21,13 @@ constexpr long NA_MAX_ELEMS = (long)NA_MAX_BLOCKS * NA_THREADS * NA_ELEMS_PER_TH
 constexpr int NA_MAX_DEVICES = 64;
 
 // Layout of the scratch array: one done-counter, then per block a float minimum, an int
-// count and a double sum.
+// count, a double sum and an int count of elements skipped for an index outside the mesh.
 constexpr size_t NA_OFF_COUNTER = 0;
 constexpr size_t NA_OFF_MIN = 256;
 constexpr size_t NA_OFF_BELOW = NA_OFF_MIN + sizeof(float) * NA_MAX_BLOCKS;
 constexpr size_t NA_OFF_SUM = NA_OFF_BELOW + sizeof(int) * NA_MAX_BLOCKS;
-constexpr size_t NA_SCRATCH_BYTES = NA_OFF_SUM + sizeof(double) * NA_MAX_BLOCKS;  // 16,640 bytes
+constexpr size_t NA_OFF_BAD = NA_OFF_SUM + sizeof(double) * NA_MAX_BLOCKS;
+constexpr size_t NA_SCRATCH_BYTES = NA_OFF_BAD + sizeof(int) * NA_MAX_BLOCKS;  // 20,736 bytes
 
 // Shared by every call on a device and kept for the life of the process. In host code this
 // name is only a host-side stand-in; kernels get its device address from cudaGetSymbolAddress.
@@ -74,22 +75,30 @@ __device__ __forceinline__ float na_q_tri2d(const float* X, const int* t) {
     return ((2.f * sqrtf(3.f)) * area) / l;
 }
 
+// Elements with an index outside [0, nV) are skipped before any of their corners is loaded
+// and counted; when there is one, the results are *out_below = -1 and NaN minimum and sum.
 __global__ void __launch_bounds__(NA_THREADS)
-k_quality_reduce_noalloc(const float* __restrict__ X, const int* __restrict__ el, int k, long nE, float threshold,
-                         unsigned char* scratch, float* out_min, double* out_sum, int* out_below) {
+k_quality_reduce_noalloc(const float* __restrict__ X, int nV, const int* __restrict__ el, int k, long nE,
+                         float threshold, unsigned char* scratch, float* out_min, double* out_sum, int* out_below) {
     unsigned* counter = reinterpret_cast<unsigned*>(scratch + NA_OFF_COUNTER);
     float* pmin = reinterpret_cast<float*>(scratch + NA_OFF_MIN);
     int* pbelow = reinterpret_cast<int*>(scratch + NA_OFF_BELOW);
     double* psum = reinterpret_cast<double*>(scratch + NA_OFF_SUM);
+    int* pbad = reinterpret_cast<int*>(scratch + NA_OFF_BAD);
     __shared__ float smin[NA_THREADS / 32];
     __shared__ int sbelow[NA_THREADS / 32];
     __shared__ double ssum[NA_THREADS / 32];
+    __shared__ int sbad[NA_THREADS / 32];
     __shared__ bool last;
     float mn = FLT_MAX;
     double sm = 0.0;
-    int below = 0;
+    int below = 0, bad = 0;
     for (long e = (long)blockIdx.x * NA_THREADS + threadIdx.x; e < nE; e += (long)gridDim.x * NA_THREADS) {
-        const float q = k == 4 ? na_q_tet(X, el + 4 * e) : na_q_tri2d(X, el + 3 * e);
+        const int* t = el + (long)k * e;
+        bool inside = true;
+        for (int c = 0; c < k; ++c) inside &= (unsigned)t[c] < (unsigned)nV;
+        if (!inside) { ++bad; continue; }
+        const float q = k == 4 ? na_q_tet(X, t) : na_q_tri2d(X, t);
         mn = fminf(mn, q);
         sm += (double)q;
         below += q < threshold ? 1 : 0;
@@ -99,40 +108,43 @@ k_quality_reduce_noalloc(const float* __restrict__ X, const int* __restrict__ el
         mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
         sm += __shfl_xor_sync(0xffffffffu, sm, o);
         below += __shfl_xor_sync(0xffffffffu, below, o);
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) { smin[w] = mn; ssum[w] = sm; sbelow[w] = below; }
+    if (lane == 0) { smin[w] = mn; ssum[w] = sm; sbelow[w] = below; sbad[w] = bad; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        float a = smin[0]; double s = ssum[0]; int b = sbelow[0];
-        for (int i = 1; i < NA_THREADS / 32; ++i) { a = fminf(a, smin[i]); s += ssum[i]; b += sbelow[i]; }
-        pmin[blockIdx.x] = a; psum[blockIdx.x] = s; pbelow[blockIdx.x] = b;
+        float a = smin[0]; double s = ssum[0]; int b = sbelow[0], x = sbad[0];
+        for (int i = 1; i < NA_THREADS / 32; ++i) { a = fminf(a, smin[i]); s += ssum[i]; b += sbelow[i]; x += sbad[i]; }
+        pmin[blockIdx.x] = a; psum[blockIdx.x] = s; pbelow[blockIdx.x] = b; pbad[blockIdx.x] = x;
         __threadfence();
         last = atomicAdd(counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if (last && threadIdx.x == 0) {
         __threadfence();
-        float a = FLT_MAX; double s = 0.0; int b = 0;
+        float a = FLT_MAX; double s = 0.0; int b = 0, x = 0;
         for (unsigned i = 0; i < gridDim.x; ++i) {
             a = fminf(a, ((volatile float*)pmin)[i]);
             s += ((volatile double*)psum)[i];
             b += ((volatile int*)pbelow)[i];
+            x += ((volatile int*)pbad)[i];
         }
-        *out_min = a;
-        *out_sum = s;
-        *out_below = b;
+        *out_min = x ? __int_as_float(0x7fc00000) : a;
+        *out_sum = x ? __longlong_as_double(0x7ff8000000000000LL) : s;
+        *out_below = x ? -1 : b;
         *counter = 0u;
     }
 }
 
-bool is_device_memory(const void* p) {
+// device (or managed) memory of the current device: the kernel and the scratch lookup run there
+bool is_device_memory(const void* p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
 }
 
 }  // namespace
@@ -155,19 +167,21 @@ void* noalloc_scratch_for_current_device() {
     return g_scratch_ptr[dev];
 }
 
-void quality_reduce_noalloc(int k, const float* d_xyz, const int* d_elems, long n_elems, float threshold,
-                            float* d_min, double* d_sum, int* d_below, cudaStream_t s) {
-    if (!is_device_memory(d_xyz) || !is_device_memory(d_elems) || !is_device_memory(d_min) ||
-        !is_device_memory(d_sum) || !is_device_memory(d_below))
-        throw Error(VSDMO_E_ARG, "the no-alloc reduction takes device pointers only");
+void quality_reduce_noalloc(int k, const float* d_xyz, int n_vertices, const int* d_elems, long n_elems,
+                            float threshold, float* d_min, double* d_sum, int* d_below, cudaStream_t s) {
+    int dev = 0;
+    VSDMO_CUDA(cudaGetDevice(&dev));
+    if (!is_device_memory(d_xyz, dev) || !is_device_memory(d_elems, dev) || !is_device_memory(d_min, dev) ||
+        !is_device_memory(d_sum, dev) || !is_device_memory(d_below, dev))
+        throw Error(VSDMO_E_ARG, "the no-alloc reduction takes device pointers of the current device only");
     unsigned char* scratch = static_cast<unsigned char*>(noalloc_scratch_for_current_device());
     // the counter must start at zero even if an earlier call on this device was cut short
     VSDMO_CUDA(cudaMemsetAsync(scratch + NA_OFF_COUNTER, 0, sizeof(unsigned), s));
     long blocks = (n_elems + (long)NA_THREADS * NA_ELEMS_PER_THREAD - 1) / ((long)NA_THREADS * NA_ELEMS_PER_THREAD);
     if (blocks < 1) blocks = 1;
     if (blocks > NA_MAX_BLOCKS) blocks = NA_MAX_BLOCKS;
-    k_quality_reduce_noalloc<<<(unsigned)blocks, NA_THREADS, 0, s>>>(d_xyz, d_elems, k, n_elems, threshold, scratch,
-                                                                     d_min, d_sum, d_below);
+    k_quality_reduce_noalloc<<<(unsigned)blocks, NA_THREADS, 0, s>>>(d_xyz, n_vertices, d_elems, k, n_elems,
+                                                                     threshold, scratch, d_min, d_sum, d_below);
     VSDMO_CHECK_LAUNCH();
 }
 
