@@ -140,7 +140,10 @@ VSDMO_API vsdmo_status vsdmo_params_default(int elem_type, vsdmo_params* out);
  * (mesh/MeshFactory.cu:15-31), DMOMeshTetFactory::create (mesh/MeshFactory.cu:45-55, minus the
  * file parsing) and the MeshTetGPU::init / MeshTriGPU::init builds they run
  * (mesh/MeshTetGPU.cu:35-42, mesh/MeshTriGPU.cu:37-50). color_seed seeds the colouring
- * priorities (the reference's live colouring is cusparseScsrcolor, VertexColoring.cu:128-153). */
+ * priorities (the reference's live colouring is cusparseScsrcolor, VertexColoring.cu:128-153);
+ * VSDMO_COLOR_REFERENCE instead selects the priorities of the reference's own JPL colouring,
+ * n - i for local index i of the n vertices coloured together (VertexColoring.cu:107-125). */
+#define VSDMO_COLOR_REFERENCE 0xFFFFFFFFu
 VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_vertices,
                                          const int32_t* elems, int n_elems, int mem_space,
                                          uint32_t color_seed, void* cuda_stream, vsdmo_mesh_t* out);
@@ -271,10 +274,13 @@ VSDMO_API vsdmo_status vsdmo_mesh_sync(vsdmo_mesh_t mesh);
  * element), the minimum element quality (mean ratio, the formula of vsdmo_opt_find_min_quality),
  * the double-precision sum of the qualities and the number of elements whose quality is below
  * `threshold`, written to the caller's device pointers d_min / d_sum / d_below.
- *   - Allocates nothing: the per-block partial results live in a fixed 16,640-byte
+ *   - Allocates nothing: the per-block partial results live in a fixed 20,736-byte
  *     __device__ array inside the library that every GPU loading the library holds until the
  *     process exits. At most 8,388,608 elements per call; larger meshes are rejected with
- *     VSDMO_E_ARG.
+ *     VSDMO_E_ARG. All pointers must be device memory of the current device (VSDMO_E_ARG).
+ *   - An element with an index outside [0, n_vertices) is skipped before any of its corners
+ *     is read; when there is one, the results are *d_below = -1 and a NaN minimum and sum (the
+ *     call is asynchronous, so the check is reported through the results, not the status).
  *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress)
  *     with that device current; make that first call before any stream capture.
  *   - Asynchronous on cuda_stream (NULL = legacy default stream); results are valid after the

@@ -83,7 +83,11 @@ uint32_t or_priority(uint32_t i, uint32_t seed) {
 int or_color_jpl(int n, const int32_t* rowptr, const int32_t* col, uint32_t seed, int32_t* colors) {
     uint32_t* pr = (uint32_t*)xc((size_t)n, sizeof(uint32_t));
     uint8_t* win = (uint8_t*)xc((size_t)n, 1);
-    for (int i = 0; i < n; ++i) { pr[i] = or_priority((uint32_t)i, seed); colors[i] = -1; }
+    for (int i = 0; i < n; ++i) {
+        /* OR_COLOR_REFERENCE: the reference's priorities randoms[i] = n - i (VertexColoring.cu:112) */
+        pr[i] = seed == OR_COLOR_REFERENCE ? (uint32_t)(n - i) : or_priority((uint32_t)i, seed);
+        colors[i] = -1;
+    }
     int left = n, c = 0;
     while (left > 0) {
         for (int i = 0; i < n; ++i) {

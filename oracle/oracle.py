@@ -16,6 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
 TRI, QUAD, TET, HEX = 0, 1, 2, 3
+# color_seed value selecting the reference's JPL priorities n - i (OR_COLOR_REFERENCE)
+COLOR_REFERENCE = 0xFFFFFFFF
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -34,10 +36,18 @@ I_NAMES = ["nV", "nE", "nSurf", "nFeature", "nTris", "nHE", "nColorsFree", "nCol
 _lib = None
 
 
+# where the reference's sources lie when they are present (this container; not the GPU box,
+# which uses the builds under oracle/_ref/ that travel with the tree)
+REF_SRC = os.environ.get("VSDMO_REFERENCE_SRC", "/root/reference/VSDMO/src")
+
+
 def build():
-    """The oracle library, and the reference's own quality functions where its sources are
-    present (oracle/_ref/, Makefile target ``ref``)."""
-    subprocess.run(["make", "-s", "-C", HERE, "all", "ref-if-present"], check=True)
+    """The oracle library, and, where the reference's sources are present, the reference's own
+    quality functions and mesh build / DMO as checkers (oracle/_ref/, Makefile target ``ref``)."""
+    args = ["make", "-s", "-j8", "-C", HERE, "all"]
+    if os.path.isdir(os.path.join(REF_SRC, "dmo")):
+        args += ["ref-if-present", "REF=" + REF_SRC]
+    subprocess.run(args, check=True)
 
 
 def lib():
@@ -545,3 +555,150 @@ def element_metric_f64(fn, crit, pts, nrm=None):
         else:
             raise ValueError(fn)
     return out
+
+
+# ---- the reference's own mesh build and DMO (oracle/_ref/libref_vsdmo.so) --------------------
+# Built by ``make ref`` from the reference's mesh/ and dmo/ sources as they lie (ref_vsdmo.cu,
+# ref_prelude_vsdmo.h); it runs on the GPU. Colouring: the reference's color_jpl (priorities
+# n - i) stands in for its closed cusparseScsrcolor, unless COLOURING_CUSPARSE (the closed one)
+# or COLOURING_HASHED (the reference's JPL rounds with the library's hashed priorities) is asked.
+REFVS_LIB_PATH = os.path.join(HERE, "_ref", "libref_vsdmo.so")
+COLOURING_JPL, COLOURING_CUSPARSE, COLOURING_HASHED = 0, 1, 2
+_refvs = None
+
+
+def refvs_lib():
+    """The reference's compiled mesh build and DMO, or None where they were not built."""
+    global _refvs
+    if _refvs is None and os.path.exists(REFVS_LIB_PATH):
+        L = C.CDLL(REFVS_LIB_PATH)
+        P, I, F = C.c_void_p, C.c_int, C.c_float
+        L.refvs_set_colouring.argtypes = [I, C.c_uint32]
+        L.refvs_set_colouring.restype = None
+        L.refvs_mesh_create.argtypes = [I, P, I, P, I]
+        L.refvs_mesh_create.restype = P
+        L.refvs_mesh_destroy.argtypes = [P]
+        L.refvs_mesh_destroy.restype = None
+        L.refvs_mesh_info.argtypes = [P, I]
+        L.refvs_mesh_info.restype = I
+        L.refvs_mesh_array.argtypes = [P, I, P]
+        L.refvs_mesh_array.restype = C.c_long
+        L.refvs_set_positions.argtypes = [P, P]
+        L.refvs_set_positions.restype = None
+        L.refvs_colour_launch.argtypes = [P, I, F]
+        L.refvs_colour_sweeps.argtypes = [P, I, F, C.POINTER(F)]
+        L.refvs_opt_create.argtypes = [P, I, F, I]
+        L.refvs_opt_iterate.argtypes = [P, I]
+        L.refvs_opt_quality.argtypes = [P]
+        L.refvs_opt_quality.restype = F
+        L.refvs_opt_element_qualities.argtypes = [P, P]
+        L.refvs_opt_surface_state.argtypes = [P, P, P, P]
+        L.refvs_opt_surface_colour.argtypes = [P, I]
+        _refvs = L
+    return _refvs
+
+
+class RefMesh:
+    """A mesh built by the reference's own code (MeshXxxGPU::init + DMOMeshXxx) on the GPU, with
+    its interior / flat colour launches and its optimiser classes. Arrays, info items and the
+    internal vertex order are in the library's formats (VSDMO_A_*)."""
+
+    def __init__(self, kind, xyz, elems, colouring=COLOURING_JPL, color_seed=1):
+        L = refvs_lib()
+        L.refvs_set_colouring(int(colouring), int(color_seed))
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        k = {TRI: 3, QUAD: 4, TET: 4, HEX: 8}[kind]
+        el = np.ascontiguousarray(elems, dtype=np.int32).reshape(-1, k)
+        self.kind, self.k = kind, k
+        self.h = L.refvs_mesh_create(kind, _p(xyz), len(xyz), _p(el), len(el))
+        L.refvs_set_colouring(COLOURING_JPL, 1)
+        if not self.h:
+            raise RuntimeError("the reference did not build the mesh")
+        self.info = {n: L.refvs_mesh_info(self.h, i) for i, n in enumerate(I_NAMES)}
+
+    def close(self):
+        if self.h:
+            refvs_lib().refvs_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def array(self, aid):
+        L = refvs_lib()
+        n = L.refvs_mesh_array(self.h, aid, None)
+        if n < 0:
+            return None
+        a = np.zeros(max(n, 0), dtype=ARRAY_DTYPES.get(aid, np.int32))
+        if n > 0:
+            L.refvs_mesh_array(self.h, aid, _p(a))
+        return a
+
+    def arrays(self):
+        out = {}
+        for aid in ARRAY_NAMES:
+            if aid == A_NEW_OF_OLD:
+                continue
+            a = self.array(aid)
+            if a is not None:
+                out[ARRAY_NAMES[aid]] = a
+        return out
+
+    def positions(self):
+        return self.array(A_XYZ).reshape(-1, 3)
+
+    def set_positions(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        refvs_lib().refvs_set_positions(self.h, _p(xyz))
+
+    def colour_launch(self, cid, grid_scale=0.5):
+        st = refvs_lib().refvs_colour_launch(self.h, int(cid), float(grid_scale))
+        if st != 0:
+            raise RuntimeError(f"reference colour launch failed ({st})")
+
+    def colour_sweeps(self, n_iter, grid_scale=0.5):
+        ms = C.c_float(0)
+        st = refvs_lib().refvs_colour_sweeps(self.h, int(n_iter), float(grid_scale), C.byref(ms))
+        if st != 0:
+            raise RuntimeError(f"reference colour sweeps failed ({st})")
+        return ms.value
+
+    def opt_create(self, crit=REF_MEAN_RATIO, grid_scale=0.5, n_iter=30):
+        st = refvs_lib().refvs_opt_create(self.h, int(crit), float(grid_scale), int(n_iter))
+        if st != 0:
+            raise RuntimeError(f"reference optimiser creation failed ({st})")
+
+    def iterate(self, n=1):
+        st = refvs_lib().refvs_opt_iterate(self.h, int(n))
+        if st != 0:
+            raise RuntimeError(f"reference iteration failed ({st})")
+
+    def quality(self):
+        return refvs_lib().refvs_opt_quality(self.h)
+
+    def surface_state(self):
+        """(initial positions [nSurf, 3], local surfaces [nSurf, 16] in the reference's layout
+        p0, e0, e1, e2, a, b, c, numPoints (an int's bits), nearest initial vertex [nSurf])."""
+        nS = self.info["nSurf"]
+        x0 = np.zeros((nS, 3), np.float32)
+        ls = np.zeros((nS, 16), np.float32)
+        nn = np.zeros(nS, np.int32)
+        st = refvs_lib().refvs_opt_surface_state(self.h, _p(x0), _p(ls), _p(nn))
+        if st != 0:
+            raise RuntimeError(f"reference surface state failed ({st})")
+        return x0, ls, nn
+
+    def surface_colour(self, cid):
+        st = refvs_lib().refvs_opt_surface_colour(self.h, int(cid))
+        if st != 0:
+            raise RuntimeError(f"reference surface colour launch failed ({st})")
+
+    def element_qualities(self):
+        q = np.zeros(self.info["nE"], dtype=np.float32)
+        st = refvs_lib().refvs_opt_element_qualities(self.h, _p(q))
+        if st != 0:
+            raise RuntimeError(f"reference element qualities failed ({st})")
+        return q

@@ -72,7 +72,9 @@ int      or_mesh_info(const or_mesh* m, int which);
 long     or_mesh_array_len(const or_mesh* m, int id);          /* elements of the array   */
 int      or_mesh_array(const or_mesh* m, int id, void* out);    /* copies; 0 on success    */
 
-/* JPL colouring of a CSR graph with the seeded priorities; returns number of colours. */
+/* JPL colouring of a CSR graph with the seeded priorities, or with the reference's priorities
+ * n - i when seed == OR_COLOR_REFERENCE; returns number of colours. */
+#define OR_COLOR_REFERENCE 0xFFFFFFFFu
 int      or_color_jpl(int n, const int32_t* rowptr, const int32_t* col, uint32_t seed, int32_t* colors);
 uint32_t or_priority(uint32_t i, uint32_t seed);
 

@@ -1,0 +1,412 @@
+"""GPU tests against the reference itself: its own mesh build and DMO, compiled from its sources
+(oracle/_ref/libref_vsdmo.so, Makefile target ``ref``) and run on the same inputs.
+
+* connectivity and colouring: with the reference's JPL priorities (``COLOR_REFERENCE``), every
+  array the library exports equals the reference's bit for bit (positions in the internal
+  vertex order, elements, surface faces, halfedge / halfface / halfhex CSR, colour offsets,
+  flags); normals within float rounding (the reference is compiled with fused multiply-adds,
+  the library without). The oracle's restatement is held to the same arrays. With the library's
+  default hashed priorities given to the reference's own JPL kernel, the same holds.
+* the grid search: one colour launch of the reference's kernel (interior tet / hex, flat
+  triangles, triangle and quad surfaces) from the same state as the library's, compared vertex
+  by vertex wherever the FP64 oracle's decision margin is clear of the reference's FP32 rounding
+  (2e-6 / h, see _clear_margin): the reference's FP32 kernel and
+  the library are each within 1e-5 h of the FP64 restatement, so within 2e-5 h of each other
+  (at config 1's h = 1/63, 1e-5 h is 1.3 float ulps of a unit coordinate, below the rounding of
+  the reference kernel's candidate coordinates: there the bound is 5e-7);
+* the surface state the reference's optimiser builds (initial positions, local quadric
+  surfaces from its cuBLAS batched LU, nearest initial vertices) against the library's;
+* whole runs, both sides coloured with the library's default priorities (the reference's
+  n - i priorities make chains of hundreds of colours, one vertex each on the torus, along
+  which a single near-tie decision propagates within one iteration): the first iteration of the
+  reference (its interior sweeps with the boundary held; DMOTetClass / DMOHexClass with their
+  boundary passes) against the FP64 restatement on the vertices whose decisions, and those of
+  the ring vertices they read, are clear of rounding; its surface classes against the library
+  after one iteration. Over several iterations the near-tie decisions of the reference's own
+  FP32 arithmetic compound (on tet_cube17 its minimum after 3 iterations is 1.9e-3 below the
+  FP64 restatement's, which the library matches within 1e-4), so whole runs of the library are
+  held to the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+
+pytestmark = pytest.mark.gpu
+
+TRI, QUAD, TET, HEX = 0, 1, 2, 3
+
+
+def _ico(level, seed, t):
+    v, f = G.icosphere(level)
+    return G.perturb_surface(v, f, seed=seed, tangential=t), f
+
+
+def _torus(nu, nv, seed, t):
+    v, q = G.torus_quads(nu, nv)
+    return G.perturb_surface(v, q, seed=seed, tangential=t), q
+
+
+def _cube_free_boundary(hex_, n, seed):
+    """cube whose interior vertices are jittered by up to 0.3h (hex 0.2h) and whose boundary
+    vertices move within their face plane or along their edge by up to 0.25h (hex 0.2h),
+    corners fixed: every boundary pass has work"""
+    h = 1.0 / n
+    ji, jb = (0.2, 0.2) if hex_ else (0.3, 0.25)
+    xyz, el = (G.hex_cube if hex_ else G.tet_cube)(n, seed=None)
+    xyz = xyz.astype(np.float64)
+    rng = np.random.default_rng(seed)
+    for i in range(len(xyz)):
+        on = (np.abs(xyz[i]) < 1e-9) | (np.abs(xyz[i] - 1) < 1e-9)
+        for a in range(3):
+            if on.sum() == 0:
+                xyz[i, a] += rng.uniform(-ji * h, ji * h)
+            elif not on[a] and on.sum() < 3:
+                xyz[i, a] += rng.uniform(-jb * h, jb * h)
+    return xyz.astype(np.float32), el
+
+
+# name: (kind, generator, h = grid spacing of the mesh)
+MESHES = {
+    "tri_grid8": (TRI, lambda: G.tri_grid(8, seed=3), 1 / 7),
+    "config1": (TRI, lambda: G.config1(), 1 / 63),
+    "tri_grid_odd": (TRI, lambda: G.tri_grid(37, seed=11, jitter=0.45), 1 / 36),
+    "ico3": (TRI, lambda: _ico(3, 1, 0.3), 0.15),
+    "torus40x40": (QUAD, lambda: _torus(40, 40, 2, 0.15), 0.15),
+    "tet_cube4": (TET, lambda: G.tet_cube(4, seed=5), 1 / 4),
+    "tet_cube12": (TET, lambda: G.tet_cube(12, seed=0), 1 / 12),
+    "tet_cube17": (TET, lambda: G.tet_cube(17, seed=2, jitter=0.35), 1 / 17),
+    "hex5": (HEX, lambda: G.hex_cube(5, seed=2), 1 / 5),
+    "hex8": (HEX, lambda: G.hex_cube(8, seed=4), 1 / 8),
+    "tet_free7": (TET, lambda: _cube_free_boundary(False, 7, 4), 1 / 7),
+    "hex_free5": (HEX, lambda: _cube_free_boundary(True, 5, 4), 1 / 5),
+}
+
+
+@pytest.fixture(scope="module")
+def ref(oracle_mod):
+    if oracle_mod.refvs_lib() is None:
+        pytest.skip("the reference's mesh build and DMO were not built (oracle/_ref)")
+    return oracle_mod
+
+
+def _lib_mesh(vsdmo, kind, xyz, el, seed=None):
+    cls = {TRI: vsdmo.DMOMeshTri, QUAD: vsdmo.DMOMeshQuad, TET: vsdmo.DMOMeshTet, HEX: vsdmo.DMOMeshHex}[kind]
+    return cls(xyz, el, color_seed=vsdmo.COLOR_REFERENCE if seed is None else seed)
+
+
+def _hashed_pair(ref, vsdmo, kind, xyz, el, seed=1):
+    """the reference's build with its JPL kernel on the library's hashed priorities, and the
+    library's default build"""
+    return (ref.RefMesh(kind, xyz, el, colouring=ref.COLOURING_HASHED, color_seed=seed),
+            _lib_mesh(vsdmo, kind, xyz, el, seed), ref.OracleMesh(kind, xyz, el, color_seed=seed))
+
+
+def _clear_margin(h):
+    """The FP64 decision margin above which the reference's FP32 kernel must decide the same:
+    its candidate coordinates carry up to ~5e-7 of rounding (see _tol), which moves a
+    candidate's quality by up to |grad q| x 5e-7, about 4 / h x 5e-7 for elements of size h."""
+    return 2e-6 / h
+
+
+def _tol(h):
+    """1e-5 h, or 5e-7 where that is larger: the reference forms each candidate coordinate as
+    (1/7) (i min + (7 - i) max), whose FP32 rounding reaches about 4 ulps of a unit coordinate
+    (at config 1's h = 1/63, 1e-5 h is 1.3 ulps)"""
+    return max(1e-5 * h, 5e-7)
+
+
+def _norm_info(info):
+    """zero colours are an empty offset list in the reference (nColors = -1) and a single offset
+    in the library (0)"""
+    return {k: (max(v, 0) if k.startswith("nColors") else v) for k, v in info.items()}
+
+
+def _compare_arrays(A, B, where):
+    for k, a in A.items():
+        b = B[k]
+        if k.startswith("col_") and min(a.size, b.size) == 0 and max(a.size, b.size) <= 1:
+            continue   # no colour class: [] (reference) or [start] (library)
+        assert a.shape == b.shape, (where, k, a.shape, b.shape)
+        if k in ("face_normals", "vertex_normals"):
+            na, nb = np.isnan(a), np.isnan(b)
+            assert np.array_equal(na, nb), (where, k)
+            np.testing.assert_allclose(a[~na], b[~nb], rtol=0, atol=2e-6, err_msg=f"{where} {k}")
+        elif a.dtype == np.float32:
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (where, k)
+        else:
+            assert np.array_equal(a, b), (where, k, np.flatnonzero(a != b)[:5])
+
+
+@pytest.mark.parametrize("priorities", ["reference", "hashed"])
+@pytest.mark.parametrize("name", list(MESHES))
+def test_connectivity_equals_reference(ref, vsdmo, name, priorities):
+    kind, gen, _ = MESHES[name]
+    xyz, el = gen()
+    if priorities == "reference":
+        rm = ref.RefMesh(kind, xyz, el)
+        gm = _lib_mesh(vsdmo, kind, xyz, el)
+        om = ref.OracleMesh(kind, xyz, el, color_seed=ref.COLOR_REFERENCE)
+    else:
+        rm, gm, om = _hashed_pair(ref, vsdmo, kind, xyz, el)
+    R = rm.arrays()
+    assert R["col_inner"].size > 0 or kind in (TRI, QUAD)
+    assert _norm_info(gm.info) == _norm_info(rm.info)
+    assert _norm_info(om.info) == _norm_info(rm.info)
+    G_ = gm.arrays()
+    O_ = om.arrays()
+    _compare_arrays(R, G_, "library")
+    _compare_arrays(R, O_, "oracle")
+
+
+def test_reference_colouring_of_the_benchmark_mesh(ref, vsdmo):
+    """config 2 (48^3 Kuhn cube): the whole connectivity, colouring included, against the
+    reference's build of the same mesh."""
+    xyz, el = G.config2()
+    rm = ref.RefMesh(TET, xyz, el)
+    gm = _lib_mesh(vsdmo, TET, xyz, el)
+    assert _norm_info(gm.info) == _norm_info(rm.info)
+    _compare_arrays(rm.arrays(), gm.arrays(), "library")
+
+
+@pytest.mark.parametrize("name", ["tri_grid8", "config1", "tet_cube12", "tet_cube17", "hex5", "hex8"])
+def test_colour_launches_against_reference_kernel(ref, vsdmo, name):
+    kind, gen, h = MESHES[name]
+    xyz, el = gen()
+    rm = ref.RefMesh(kind, xyz, el)
+    gm = _lib_mesh(vsdmo, kind, xyz, el)
+    om = ref.OracleMesh(kind, xyz, el, color_seed=ref.COLOR_REFERENCE)
+    cls = {TRI: vsdmo.DMOTriFlatClass, TET: vsdmo.DMOTetClass, HEX: vsdmo.DMOHexClass}[kind]
+    opt = cls(gm, n_iter=1)
+    x = gm.positions()
+    assert np.array_equal(rm.positions(), x)
+    checked = total = 0
+    for c, (v0, v1) in enumerate(om.color_ranges()):
+        rm.set_positions(x)
+        rm.colour_launch(c)
+        xr = rm.positions()
+        x64, margin = om.dmo_color_f64(x.astype(np.float64), v0, v1)
+        opt.run_color(c)
+        xg = gm.positions()
+        clear = margin > _clear_margin(h)
+        cols = slice(0, 2) if kind == TRI else slice(0, 3)
+        dr = np.abs(xr[v0:v1, cols].astype(np.float64) - x64[v0:v1, cols]).max(1)
+        dg = np.abs(xg[v0:v1, cols].astype(np.float64) - xr[v0:v1, cols]).max(1)
+        # the reference's kernel against the FP64 restatement of it, and against the library
+        assert np.all(dr[clear] < _tol(h)), (c, float(dr[clear].max()))
+        assert np.all(dg[clear] < 2 * _tol(h)), (c, float(dg[clear].max()))
+        # vertices outside v0:v1 are untouched by both
+        assert np.array_equal(np.delete(xr, np.s_[v0:v1], 0), np.delete(x, np.s_[v0:v1], 0))
+        checked += int(clear.sum())
+        total += v1 - v0
+        x = xg
+    assert checked > 0.3 * total
+
+
+def _quality_min_mean(q):
+    q = np.asarray(q, dtype=np.float64)
+    return float(q.min()), float(q.mean())
+
+
+def _neighbours(om, kind):
+    """per vertex, the vertices whose positions its search reads (its element ring)"""
+    if kind in (TET, HEX):
+        rp = om.array(O.A_HF_ROWPTR)
+        hf = om.array(O.A_HALFFACES).reshape(-1, 7 if kind == HEX else 3)
+        return [hf[rp[v]:rp[v + 1]].ravel() for v in range(len(rp) - 1)]
+    rp = om.array(O.A_HE_ROWPTR)
+    he = om.array(O.A_HALFEDGES).reshape(-1, 4)
+    return [he[rp[v]:rp[v + 1], 0] for v in range(len(rp) - 1)]
+
+
+def _ranges(off):
+    return [(int(off[c]), int(off[c + 1])) for c in range(len(off) - 1)]
+
+
+def _fp64_iteration(om, kind, free_boundary, thr):
+    """One iteration of the FP64 restatement from the initial state, colour by colour in
+    doIteration's order, and the vertices whose result is clear of rounding: a vertex is clear
+    when each of its FP64 decisions has a margin over thr and every ring vertex it read was
+    clear when it was read."""
+    x32 = om.xyz
+    x = x32.astype(np.float64)
+    clear = np.ones(len(x), bool)
+    nb = _neighbours(om, kind)
+
+    def settle(v0, v1, mg):
+        clear[v0:v1] &= mg > thr
+        for v in range(v0, v1):
+            clear[v] &= bool(np.all(clear[nb[v]])) if len(nb[v]) else True
+
+    inner = om.array(O.A_COL_INNER) if kind in (TET, HEX) else om.array(O.A_COL_FREE)
+    for v0, v1 in _ranges(inner):
+        x, mg = om.dmo_color_f64(x, v0, v1)
+        settle(v0, v1, mg)
+    if free_boundary and kind in (TET, HEX):
+        x0, ls, nn, vn = om.surface_state_f64(x32)
+        fn = om.array(O.A_FACE_NORMALS).reshape(-1, 3).astype(np.float64)
+        sectors = om.sector_surfaces(x32, fn, dtype=np.float64)
+        for v0, v1 in _ranges(om.array(O.A_COL_FREE)):
+            x, mg = om.dmo_vol_surf_f64(x, x0, ls, nn, sectors, v0, v1)
+            settle(v0, v1, mg)
+        fdeg, flags = om.feature_flags(x32)
+        curves = om.curves_f64(x32, vn)
+        for v0, v1 in _ranges(om.array(O.A_COL_FEATURE)):
+            x, mg = om.dmo_1d_f64(x, x0, curves, nn, vn, fdeg, flags, v0, v1)
+            settle(v0, v1, mg)
+    return x, clear
+
+
+@pytest.mark.parametrize("name,iters", [("config1", 10), ("tet_cube12", 5), ("tet_cube17", 3), ("hex8", 5)])
+def test_fixed_boundary_runs_against_reference(ref, vsdmo, name, iters):
+    """The benchmark mode (boundary held). Iteration 1: the reference kernel's sweep over every
+    colour against the FP64 restatement, on the vertices whose decisions are clear of rounding.
+    Whole runs: the library within 1e-4 of the FP64 restatement's minimum and mean; the
+    reference's own FP32 run near them (its near-tie decisions compound)."""
+    kind, gen, h = MESHES[name]
+    xyz, el = gen()
+    rm, gm, om = _hashed_pair(ref, vsdmo, kind, xyz, el)
+    cls = {TRI: vsdmo.DMOTriFlatClass, TET: vsdmo.DMOTetClass, HEX: vsdmo.DMOHexClass}[kind]
+    opt = cls(gm, n_iter=iters)
+    cols = slice(0, 2) if kind == TRI else slice(0, 3)
+    x64, clear = _fp64_iteration(om, kind, False, _clear_margin(h))
+    rm.colour_sweeps(1)
+    opt.iterate(1)
+    d = np.abs(rm.positions()[:, cols].astype(np.float64) - x64[:, cols]).max(1)
+    assert np.all(d[clear] < _tol(h)), float(d[clear].max())
+    assert clear.sum() > 0.3 * (d > 0).sum()
+    rm.colour_sweeps(iters - 1)
+    opt.iterate(iters - 1)
+    _, mn64, me64 = om.optimize_f64(om.xyz, iters)
+    gmin, gmean = _quality_min_mean(om.element_qualities_f64(gm.positions()))
+    rmin, rmean = _quality_min_mean(om.element_qualities_f64(rm.positions()))
+    assert abs(gmin - mn64[-1]) < 1e-4 and abs(gmean - me64[-1]) < 1e-4, (gmin, mn64[-1], gmean, me64[-1])
+    assert abs(rmin - mn64[-1]) < 5e-3 and abs(rmean - me64[-1]) < 1e-3, (rmin, mn64[-1], rmean, me64[-1])
+    q0 = om.element_qualities_f64(om.xyz)
+    assert gmean > q0.mean() and gmin >= q0.min()
+
+
+@pytest.mark.parametrize("name", ["tet_free7", "hex_free5"])
+def test_volume_optimiser_free_boundary_iteration(ref, vsdmo, name):
+    """DMOTetClass / DMOHexClass::doIteration as the reference runs it (interior colours, then the
+    surface passes of the boundary and the feature curves): its first iteration against the FP64
+    restatement on the vertices clear of rounding; the library's is held to the same restatement
+    by test_gpu_volume_boundary.py."""
+    kind, gen, h = MESHES[name]
+    xyz, el = gen()
+    rm, gm, om = _hashed_pair(ref, vsdmo, kind, xyz, el)
+    assert om.element_qualities_f64(om.xyz).min() > 0     # the surface passes run (lastMinQuality > 0)
+    x64, clear = _fp64_iteration(om, kind, True, _clear_margin(h))
+    rm.opt_create(ref.REF_MEAN_RATIO, 0.5, 1)
+    rm.iterate(1)
+    d = np.abs(rm.positions().astype(np.float64) - x64).max(1)
+    assert np.all(d[clear] < _tol(h)), (float(d[clear].max()), np.flatnonzero(clear & (d >= _tol(h)))[:5])
+    # hex moves are short (the per-axis minimum ring distance): few hex decisions are clear
+    assert clear.sum() >= (3 if kind == HEX else 50)
+    # the library's iteration: the same minimum; the mean within 1e-3 (a near-tie between two
+    # candidates of the same ring minimum can leave the mean of the ring's elements apart)
+    opt = _free_boundary_opt(vsdmo, gm, kind, 1)
+    opt.iterate(1)
+    (rmin, rmean), (gmin, gmean) = _quality_min_mean(rm.element_qualities()), _quality_min_mean(opt.getElementQualities())
+    assert abs(rmin - gmin) < 1e-4, (rmin, gmin)
+    assert abs(rmean - gmean) < 1e-3, (rmean, gmean)
+
+
+def _free_boundary_opt(vsdmo, gm, kind, iters):
+    if kind == TRI and gm.info["isFlat"]:
+        return vsdmo.DMOTriFlatClass(gm, n_iter=iters, fix_boundary=False)
+    cls = {TRI: vsdmo.DMOTriClass, QUAD: vsdmo.DMOQuadClass, TET: vsdmo.DMOTetClass, HEX: vsdmo.DMOHexClass}[kind]
+    return cls(gm, n_iter=iters, fix_boundary=False)
+
+
+# the reference's surface optimiser classes and the flat one with its sliding boundary
+# (their defaults); the library with fix_boundary=False
+@pytest.mark.parametrize("name", ["tri_grid_odd", "ico3", "torus40x40"])
+def test_reference_optimiser_classes_first_iteration(ref, vsdmo, name):
+    kind, gen, h = MESHES[name]
+    xyz, el = gen()
+    rm, gm, _ = _hashed_pair(ref, vsdmo, kind, xyz, el)
+    opt = _free_boundary_opt(vsdmo, gm, kind, 1)
+    q0 = float(np.min(opt.getElementQualities()))
+    rm.opt_create(ref.REF_MEAN_RATIO, 0.5, 1)
+    rm.iterate(1)
+    opt.iterate(1)
+    flat = kind == TRI and gm.info["isFlat"]
+    cols = slice(0, 2) if flat else slice(0, 3)
+    d = np.abs(rm.positions()[:, cols].astype(np.float64) - gm.positions()[:, cols]).max(1)
+    assert np.mean(d < 2 * _tol(h)) > 0.95, (int((d >= 2 * _tol(h)).sum()), len(d))
+    (rmin, rmean), (gmin, gmean) = _quality_min_mean(rm.element_qualities()), _quality_min_mean(opt.getElementQualities())
+    assert abs(rmin - gmin) < 1e-4, (rmin, gmin)
+    assert abs(rmean - gmean) < 1e-4, (rmean, gmean)
+    assert abs(rm.quality() - gmin) < 1e-4
+    assert gmin >= q0 - 1e-6
+
+
+SURFACES = ["ico3", "torus40x40"]
+
+
+def _ours_from_reference_layout(ls):
+    """the reference's localSurface (p0, e0, e1, e2, a, b, c, numPoints) in the library's layout
+    (p0, a, e0, b, e1, c, e2, numPoints)"""
+    out = np.zeros_like(ls)
+    out[:, 0:3], out[:, 3] = ls[:, 0:3], ls[:, 12]
+    out[:, 4:7], out[:, 7] = ls[:, 3:6], ls[:, 13]
+    out[:, 8:11], out[:, 11] = ls[:, 6:9], ls[:, 14]
+    out[:, 12:15] = ls[:, 9:12]
+    out[:, 15] = ls[:, 15].view(np.int32).astype(np.float32)
+    return out
+
+
+@pytest.mark.parametrize("name", SURFACES)
+def test_surface_state_against_reference(ref, vsdmo, name):
+    kind, gen, _ = MESHES[name]
+    xyz, el = gen()
+    rm = ref.RefMesh(kind, xyz, el)
+    gm = _lib_mesh(vsdmo, kind, xyz, el)
+    opt = _free_boundary_opt(vsdmo, gm, kind, 1)
+    rm.opt_create(ref.REF_MEAN_RATIO, 0.5, 1)
+    rx0, rls, rnn = rm.surface_state()
+    gx0, gls, gnn = opt.surface_state()
+    assert np.array_equal(rx0.view(np.uint32), gx0.view(np.uint32))
+    assert np.array_equal(rnn, gnn)
+    r = _ours_from_reference_layout(rls)
+    assert np.array_equal(r[:, 15], gls[:, 15])                       # points in each fit
+    assert np.array_equal(r[:, 0:3].view(np.uint32), gls[:, 0:3].view(np.uint32))   # origins
+    for c in (slice(4, 7), slice(8, 11), slice(12, 15)):               # frame axes
+        np.testing.assert_allclose(r[:, c], gls[:, c], rtol=0, atol=2e-6)
+    # the quadric coefficients: the reference solves with cuBLAS's batched LU, the library with
+    # its own LU with partial pivoting; both solve the same 3x3 system in FP32
+    abc_r, abc_g = r[:, [3, 7, 11]], gls[:, [3, 7, 11]]
+    scale = np.maximum(np.abs(abc_r).max(1, keepdims=True), 1e-3)
+    assert np.all(np.abs(abc_r - abc_g) <= 1e-4 * scale + 1e-6), float((np.abs(abc_r - abc_g) / scale).max())
+
+
+@pytest.mark.parametrize("name", SURFACES)
+def test_surface_colour_launches_against_reference_kernel(ref, vsdmo, name):
+    kind, gen, h = MESHES[name]
+    xyz, el = gen()
+    rm = ref.RefMesh(kind, xyz, el)
+    gm = _lib_mesh(vsdmo, kind, xyz, el)
+    om = ref.OracleMesh(kind, xyz, el, color_seed=ref.COLOR_REFERENCE)
+    opt = _free_boundary_opt(vsdmo, gm, kind, 1)
+    rm.opt_create(ref.REF_MEAN_RATIO, 0.5, 1)
+    x0, ls, nn, vn = om.surface_state_f64(om.xyz)
+    x = gm.positions()
+    checked = total = 0
+    for c, (v0, v1) in enumerate(om.color_ranges()):
+        rm.set_positions(x)
+        rm.surface_colour(c)
+        xr = rm.positions()
+        x64, margin = om.dmo_surf_color_f64(x.astype(np.float64), x0, ls, nn, vn, v0, v1)
+        opt.run_color(c)
+        xg = gm.positions()
+        clear = margin > _clear_margin(h)
+        dr = np.abs(xr[v0:v1].astype(np.float64) - x64[v0:v1]).max(1)
+        dg = np.abs(xg[v0:v1].astype(np.float64) - xr[v0:v1]).max(1)
+        assert np.all(dr[clear] < _tol(h)), (c, float(dr[clear].max()))
+        assert np.all(dg[clear] < 2 * _tol(h)), (c, float(dg[clear].max()))
+        checked += int(clear.sum())
+        total += v1 - v0
+        x = xg
+    assert checked > 0.3 * total

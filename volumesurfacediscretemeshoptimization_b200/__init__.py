@@ -36,7 +36,8 @@ from ._capi import VSDMOError, Params, check
 __all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshQuad", "DMOMeshTet", "DMOMeshHex", "DMOMeshTriFactory",
            "DMOMeshQuadFactory", "DMOMeshTetFactory", "DMOMeshHexFactory", "DMOTetClass", "DMOHexClass",
            "DMOTriFlatClass", "DMOTriClass", "DMOQuadClass", "DMOQuadFlatClass", "BatchDMO", "ProposalModel",
-           "VSDMOError", "Params", "default_params", "version", "read_mesh_file", "write_mesh_file"]
+           "VSDMOError", "Params", "default_params", "version", "read_mesh_file", "write_mesh_file",
+           "COLOR_REFERENCE"]
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -50,6 +51,9 @@ ARRAY_NAMES = {A_XYZ: "xyz", A_NEW_OF_OLD: "new_of_old", A_ELEMS: "elems", A_SUR
 _F32 = {A_XYZ, A_FACE_NORMALS, A_VERTEX_NORMALS}
 _U8 = {A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D}
 I_ELEM_TYPE = 12
+# color_seed value selecting the reference's own JPL priorities n - i (VSDMO_COLOR_REFERENCE)
+# instead of the seeded hash; the reference's mesh/VertexColoring.cu:107-125
+COLOR_REFERENCE = 0xFFFFFFFF
 INFO_NAMES = ["nV", "nE", "nSurf", "nFeature", "nTris", "nHE", "nColorsFree", "nColorsFeature",
               "nColorsInner", "maxNumHalfedges", "maxNumTetrahedra", "isFlat"]
 

@@ -19,7 +19,8 @@
 //   * boundary / feature flags (dihedral > 20 deg, mesh/MeshGPUCommon.cu:466-495) and face /
 //     vertex normals (:363-434).
 // Sorting uses the stable LSD radix sort of prim.cu. Colouring runs the reference's JPL round
-// rule (mesh/VertexColoring.cu:76-105) with seeded hash priorities.
+// rule (mesh/VertexColoring.cu:76-105) with seeded hash priorities, or with the reference's own
+// priorities n - i (VertexColoring.cu:107-125) when the seed is VSDMO_COLOR_REFERENCE.
 #include "vsdmo_internal.cuh"
 #include <climits>
 #include <cmath>
@@ -30,12 +31,20 @@ namespace {
 enum BuildErr { BE_OK = 0, BE_INDEX = 1, BE_NAN = 2, BE_DEGENERATE = 3, BE_NONMANIFOLD = 4,
                 BE_FAN = 5, BE_FEATURE_START = 6 };
 
-__device__ __forceinline__ uint32_t priority(uint32_t i, uint32_t seed) {
+// n: the number of vertices coloured together (i is local to them)
+__device__ __forceinline__ uint32_t priority(uint32_t i, uint32_t seed, uint32_t n) {
+    if (seed == VSDMO_COLOR_REFERENCE) return n - i;
     uint32_t h = i + seed * 0x9E3779B9u;
     h ^= h >> 16; h *= 0x85EBCA6Bu;
     h ^= h >> 13; h *= 0xC2B2AE35u;
     h ^= h >> 16;
     return h;
+}
+
+// the halfedge fans are walked by one thread per vertex in time quadratic in the fan's length
+// (k_ccw, like the reference's k_sortCCWDummyOpposite): longer fans are refused
+[[noreturn]] void throw_long_fan() {
+    throw Error(VSDMO_E_VALENCE, "a vertex has more than " + std::to_string(SHORT_ROW_MAX) + " halfedges");
 }
 
 #define GRID_STRIDE(i, n) for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long)gridDim.x * blockDim.x)
@@ -323,13 +332,13 @@ __global__ void k_jpl_round(int n, const int* rowptr, const int* col, uint32_t s
     if (prev && *prev == 0) return;
     GRID_STRIDE(i, n) {
         if (colors[i] != -1) continue;
-        uint32_t pi = priority((uint32_t)i, seed);
+        uint32_t pi = priority((uint32_t)i, seed, (uint32_t)n);
         bool f = true;
         for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
             int j = col[e];
             int jc = colors[j];
             if ((jc != -1 && jc != c) || (int)i == j) continue;
-            if (pi <= priority((uint32_t)j, seed)) { f = false; break; }
+            if (pi <= priority((uint32_t)j, seed, (uint32_t)n)) { f = false; break; }
         }
         if (f) colors[i] = c; else atomicAdd(remaining, 1);
     }
@@ -638,7 +647,7 @@ struct Builder {
             DBuf<uint32_t> keys(nHE1, s), order(nHE1, s);
             VSDMO_CUDA(cudaMemcpyAsync(keys.p, m.tris.p, sizeof(int) * nHE1, cudaMemcpyDeviceToDevice, s));
             DBuf<int> rowptr(nS + 1, s);
-            stable_sort_short_rows(keys.p, order.p, nHE1, nS, rowptr.p, s);
+            if (stable_sort_short_rows(keys.p, order.p, nHE1, nS, rowptr.p, s) > SHORT_ROW_MAX) throw_long_fan();
             DBuf<int4> he(nHE1, s);
             k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, m.fk, he.p);
             VSDMO_CHECK_LAUNCH();
@@ -705,7 +714,7 @@ struct Builder {
         DBuf<uint32_t> keys(nHE1, s), order(nHE1, s);
         VSDMO_CUDA(cudaMemcpyAsync(keys.p, m.tris.p, sizeof(int) * nHE1, cudaMemcpyDeviceToDevice, s));
         DBuf<int> rowptr1(nS + 1, s);
-        stable_sort_short_rows(keys.p, order.p, nHE1, nS, rowptr1.p, s);
+        if (stable_sort_short_rows(keys.p, order.p, nHE1, nS, rowptr1.p, s) > SHORT_ROW_MAX) throw_long_fan();
         DBuf<int4> he1(nHE1, s);
         k_he_records<<<G(nHE1), 256, 0, s>>>(order.p, nHE1, m.tris.p, m.fk, he1.p);
         VSDMO_CHECK_LAUNCH();
@@ -722,7 +731,7 @@ struct Builder {
         k_with_dummies<<<G(nHE), 256, 0, s>>>(keys.p, he1.p, nHE1, didx.p, nD, k2.p, rec.p);
         VSDMO_CHECK_LAUNCH();
         m.he_rowptr.alloc(nS + 1, s);
-        stable_sort_short_rows(k2.p, o2.p, nHE, nS, m.he_rowptr.p, s);
+        if (stable_sort_short_rows(k2.p, o2.p, nHE, nS, m.he_rowptr.p, s) > SHORT_ROW_MAX) throw_long_fan();
         DBuf<int4> in(nHE, s);
         k_gather<int4><<<G(nHE), 256, 0, s>>>(rec.p, o2.p, in.p, nHE);
         VSDMO_CHECK_LAUNCH();
@@ -757,6 +766,9 @@ struct Builder {
         k_count_keys_u32<<<G(nF), 256, 0, s>>>(f0.p, nF, counts.p);
         VSDMO_CHECK_LAUNCH();
         exclusive_scan(counts.p, rs.p, nV, rs.p + nV, s);
+        if (longest_row(rs.p, nV, s) > SHORT_ROW_MAX)
+            throw Error(VSDMO_E_VALENCE, "a vertex is the first corner of more than " + std::to_string(SHORT_ROW_MAX) +
+                                             " tetrahedron faces (more than ~1365 tetrahedra around one vertex)");
         VSDMO_CUDA(cudaMemcpyAsync(cursor.p, rs.p, sizeof(int) * nV, cudaMemcpyDeviceToDevice, s));
         k_face_bucket<<<G(nF), 256, 0, s>>>(f0.p, f1.p, f2.p, nF, cursor.p, fb.p);
         VSDMO_CHECK_LAUNCH();

@@ -255,7 +255,44 @@ __global__ void k_row_order(const int* rs, const uint32_t* idx, long K, uint32_t
     }
 }
 
+// the longest row of a CSR row pointer rs[0..K] to *out (atomic maximum; *out starts at 0)
+__global__ void k_longest_row(const int* rs, long K, int* out) {
+    int m = 0;
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < K; r += (long)gridDim.x * blockDim.x)
+        m = max(m, rs[r + 1] - rs[r]);
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+}
+
+__global__ void k_iota_u32(uint32_t* a, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        a[i] = (uint32_t)i;
+}
+
+// in (key, value)-sorted pairs: 1 where a pair differs from the one before it, counted per key
+__global__ void k_flag_distinct(const uint32_t* k, const uint32_t* v, long n, uint8_t* flag, int* per_key) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const bool d = i == 0 || k[i] != k[i - 1] || v[i] != v[i - 1];
+        flag[i] = d ? 1 : 0;
+        if (d) atomicAdd(&per_key[k[i]], 1);
+    }
+}
+
+__global__ void k_gather_col(const uint32_t* v, const int* idx, long n, int* col) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        col[i] = (int)v[idx[i]];
+}
+
 }  // namespace
+
+int longest_row(const int* d_rowptr, long K, cudaStream_t s) {
+    if (K <= 0) return 0;
+    DBuf<int> m(1, s);
+    m.zero();
+    k_longest_row<<<grid_for(K, 256), 256, 0, s>>>(d_rowptr, K, m.p);
+    VSDMO_CHECK_LAUNCH();
+    return read_scalar(m.p, s);
+}
 
 int bits_for(uint32_t maxval) {
     int b = 1;
@@ -351,6 +388,26 @@ void csr_unique_from_pairs(const uint32_t* d_keys, const uint32_t* d_vals, long 
         VSDMO_CHECK_LAUNCH();
     }
     exclusive_scan(counts.p, rs.p, K, rs.p + K, s);
+    if (n > 0 && longest_row(rs.p, K, s) > SHORT_ROW_MAX) {
+        // a row too long for one warp's quadratic scans: the same CSR from two stable radix sorts
+        // (by value, then by key) and the first pair of every run of equal pairs
+        DBuf<uint32_t> kk(n, s), vv(n, s);
+        DBuf<int> idx(n, s);
+        VSDMO_CUDA(cudaMemcpyAsync(kk.p, d_keys, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+        VSDMO_CUDA(cudaMemcpyAsync(vv.p, d_vals, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+        radix_sort_pairs(vv.p, kk.p, n, 32, s);
+        radix_sort_pairs(kk.p, vv.p, n, bits_for((uint32_t)(K > 1 ? K - 1 : 1)), s);
+        u.zero();
+        k_flag_distinct<<<grid_for(n, 256), 256, 0, s>>>(kk.p, vv.p, n, keep.p, u.p);
+        VSDMO_CHECK_LAUNCH();
+        exclusive_scan(u.p, d_rowptr, K, d_rowptr + K, s);
+        const int nu = compact_flags(keep.p, n, idx.p, s);
+        if (nu > 0) {
+            k_gather_col<<<grid_for(nu, 256), 256, 0, s>>>(vv.p, idx.p, nu, d_col);
+            VSDMO_CHECK_LAUNCH();
+        }
+        return;
+    }
     VSDMO_CUDA(cudaMemcpyAsync(cursor.p, rs.p, sizeof(int) * K, cudaMemcpyDeviceToDevice, s));
     if (n > 0) {
         k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(d_keys, d_vals, n, cursor.p, bucket.p);
@@ -363,8 +420,8 @@ void csr_unique_from_pairs(const uint32_t* d_keys, const uint32_t* d_vals, long 
     VSDMO_CHECK_LAUNCH();
 }
 
-void stable_sort_short_rows(uint32_t* d_keys, uint32_t* d_order, long n, int K, int* d_rowptr, cudaStream_t s) {
-    if (K <= 0) return;
+int stable_sort_short_rows(uint32_t* d_keys, uint32_t* d_order, long n, int K, int* d_rowptr, cudaStream_t s) {
+    if (K <= 0) return 0;
     DBuf<int> counts(K, s), cursor(K, s);
     DBuf<uint32_t> bucket(std::max(n, 1L), s);
     counts.zero();
@@ -373,12 +430,21 @@ void stable_sort_short_rows(uint32_t* d_keys, uint32_t* d_order, long n, int K, 
         VSDMO_CHECK_LAUNCH();
     }
     exclusive_scan(counts.p, d_rowptr, K, d_rowptr + K, s);
-    if (n <= 0) return;
+    if (n <= 0) return 0;
+    const int longest = longest_row(d_rowptr, K, s);
+    if (longest > SHORT_ROW_MAX) {
+        // a row too long for one warp's quadratic scan: the stable radix sort gives the same arrays
+        k_iota_u32<<<grid_for(n, 256), 256, 0, s>>>(d_order, n);
+        VSDMO_CHECK_LAUNCH();
+        radix_sort_pairs(d_keys, d_order, n, bits_for((uint32_t)(K > 1 ? K - 1 : 1)), s);
+        return longest;
+    }
     VSDMO_CUDA(cudaMemcpyAsync(cursor.p, d_rowptr, sizeof(int) * K, cudaMemcpyDeviceToDevice, s));
     k_bucket_index<<<grid_for(n, 256), 256, 0, s>>>(d_keys, n, cursor.p, bucket.p);
     VSDMO_CHECK_LAUNCH();
     k_row_order<<<grid_for((long)K * 32, 256), 256, 0, s>>>(d_rowptr, bucket.p, K, d_order, d_keys);
     VSDMO_CHECK_LAUNCH();
+    return longest;
 }
 
 cudaMemPool_t device_pool() {

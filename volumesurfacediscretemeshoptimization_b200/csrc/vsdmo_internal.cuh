@@ -112,12 +112,19 @@ int stable_partition_flags(const uint8_t* d_flags, long n, int first_value, int*
 // (key, index) order, d_keys the keys in that order and d_rowptr (K + 1 ints) the row starts,
 // the same arrays as radix_sort_pairs over (keys, 0..n-1) followed by rowptr_from_sorted. For
 // keys whose rows are short (a vertex's elements or halfedges): each row is ordered by one warp
-// in time quadratic in its length.
-void stable_sort_short_rows(uint32_t* d_keys, uint32_t* d_order, long n, int K, int* d_rowptr, cudaStream_t s);
+// in time quadratic in its length; above SHORT_ROW_MAX entries in a row, by the radix sort.
+// Returns the longest row (one host read).
+int stable_sort_short_rows(uint32_t* d_keys, uint32_t* d_order, long n, int K, int* d_rowptr, cudaStream_t s);
 void csr_unique_from_pairs(const uint32_t* d_keys, const uint32_t* d_vals, long n, int K, int* d_rowptr, int* d_col,
                            cudaStream_t s);
 // CSR offsets [K+1] from n keys already sorted ascending (keys < K).
 void rowptr_from_sorted(const uint32_t* d_sorted_keys, long n, int K, int* d_rowptr, cudaStream_t s);
+// Rows longer than this are not ordered by one warp's quadratic scans: stable_sort_short_rows and
+// csr_unique_from_pairs switch to radix sorts, and the tet face pairing rejects the mesh
+// (VSDMO_E_VALENCE). The kernels' ring budgets (at most 512 elements around a vertex) stay far below.
+constexpr int SHORT_ROW_MAX = 4096;
+// longest row of a CSR row pointer d_rowptr[0..K] (one host read)
+int longest_row(const int* d_rowptr, long K, cudaStream_t s);
 int bits_for(uint32_t maxval);
 
 // ---- mesh (mesh_build.cu) ----------------------------------------------------------------
@@ -280,7 +287,7 @@ int quality_stats_blocks();
 
 // ---- allocation-free quality reduction (noalloc.cu) -----------------------------------------
 long noalloc_max_elements();
-void quality_reduce_noalloc(int k, const float* d_xyz, const int* d_elems, long n_elems, float threshold,
-                            float* d_min, double* d_sum, int* d_below, cudaStream_t s);
+void quality_reduce_noalloc(int k, const float* d_xyz, int n_vertices, const int* d_elems, long n_elems,
+                            float threshold, float* d_min, double* d_sum, int* d_below, cudaStream_t s);
 
 }  // namespace vsdmo
