@@ -115,13 +115,47 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def host_cpu():
+    """(model name, physical cores, logical CPUs usable by this process)."""
+    model, cores = None, set()
+    try:
+        cur = {}
+        for line in open("/proc/cpuinfo"):
+            if ":" not in line:
+                if cur.get("processor") is not None:
+                    cores.add((cur.get("physical id", "0"), cur.get("core id", cur["processor"])))
+                cur = {}
+                continue
+            k, v = [x.strip() for x in line.split(":", 1)]
+            cur[k] = v
+            if k == "model name" and model is None:
+                model = v
+        if cur.get("processor") is not None:
+            cores.add((cur.get("physical id", "0"), cur.get("core id", cur["processor"])))
+    except OSError:
+        pass
+    logical = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    physical = min(len(cores), logical) if cores else logical
+    return model, max(1, physical), logical
+
+
+def pin_openmp(threads):
+    """One OpenMP thread per physical core, bound to it; set before the oracle library (and its
+    OpenMP runtime) is loaded."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    os.environ.setdefault("OMP_PLACES", "cores")
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+
+
 def cpu_baseline_sample(xyz, tets, max_seconds=20.0):
     """Times the oracle's literal FP32 restatement of k_optimizeHierarchicalInnerTet on the
-    host cores over the first colour class(es) of the first iteration."""
+    host cores (one pinned OpenMP thread per physical core) over the first colour class(es) of
+    the first iteration."""
+    model, cores, logical = host_cpu()
+    pin_openmp(cores)
     from oracle import oracle as O
     m = O.OracleMesh(O.TET, xyz, tets, color_seed=1)
     x = m.xyz
-    cores = os.cpu_count() or 1
     done = 0
     t0 = time.perf_counter()
     classes = 0
@@ -134,32 +168,70 @@ def cpu_baseline_sample(xyz, tets, max_seconds=20.0):
         classes += 1
     dt = time.perf_counter() - t0
     return {"value": done / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "cpu_model": model, "logical_cpus": logical,
+            "threads": f"{cores} OpenMP threads, OMP_PLACES={os.environ.get('OMP_PLACES')} "
+                       f"OMP_PROC_BIND={os.environ.get('OMP_PROC_BIND')}",
+            "seconds": dt, "vertex_updates": done,
             "sample": f"first {classes} colour classes ({done} vertex updates) of iteration 1, "
-                      f"literal FP32 restatement of the reference kernel, OpenMP over {cores} threads, {dt:.1f} s"}
+                      f"literal FP32 restatement of the reference kernel (the reference has no CPU DMO), "
+                      f"{cores} pinned threads, {dt:.1f} s"}
+
+
+def reference_gpu_row(xyz, tets):
+    """The reference's own CUDA path built from its sources (oracle/_ref/libref_vsdmo.so): its
+    mesh build, then its k_optimizeHierarchicalInnerTet<128> over every interior colour for 20
+    iterations with its host loop's per-launch synchronisation (the surface passes off: boundary
+    fixed), timed with CUDA events. Colouring: its live cusparseScsrcolor, and its own JPL."""
+    from oracle import oracle as O
+    if O.refvs_lib() is None:
+        return {"unavailable": "the reference's CUDA sources were not built into oracle/_ref"}
+    out = {"what": "reference kernels on this B200: k_optimizeHierarchicalInnerTet<128>, one block of 128 "
+                   "threads per vertex, cudaDeviceSynchronize after each colour launch (dmo/DMOTet.cu:129-136)",
+           "workload": "tet cube 48^3, 20 iterations, boundary fixed"}
+    for name, mode in (("cusparse_colouring", O.COLOURING_CUSPARSE), ("jpl_colouring", O.COLOURING_JPL)):
+        rm = O.RefMesh(O.TET, xyz, tets, colouring=mode)
+        n_inner = rm.info["nV"] - rm.info["nSurf"]
+        x0 = rm.positions()
+        rm.colour_sweeps(3)                    # warm-up
+        rm.set_positions(x0)
+        ms = rm.colour_sweeps(N_ITER)
+        out[name] = {"colours": rm.info["nColorsInner"], "ms": ms,
+                     "vertex_updates_per_s": n_inner * N_ITER / (ms / 1e3)}
+        rm.close()
+    return out
 
 
 def run_reference(args):
+    """The reference arm: each step is one bounded sample (about 8 s) of the CPU restatement of
+    the reference kernel on the host cores; value = vertex updates / time over the timed steps.
+    The reference's own CUDA path on this GPU is reported beside it (reference_gpu)."""
     r, w, _ = rank_info()
     if r != 0:
         return 0
     from volumesurfacediscretemeshoptimization_b200 import meshgen as G
     xyz, tets = G.config2()
-    vals = []
+    done = secs = 0.0
     base = None
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline_sample(xyz, tets, max_seconds=8.0 if args.steps > 3 else 15.0)
+        b = cpu_baseline_sample(xyz, tets, max_seconds=8.0)
         if i >= args.warmup:
-            vals.append(b["value"])
+            done += b["vertex_updates"]
+            secs += b["seconds"]
             base = b
-    v = statistics.median(vals)
+    v = done / secs
     base["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 103823 * N_ITER / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Kuhn tet cube; the reference ships no meshes)",
-            "config": workload_config({"sample": "bounded CPU sample, see cpu_baseline"}),
+            "config": workload_config({"step": "one bounded CPU sample of the workload (see cpu_baseline)"}),
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:
+        try:
+            line["reference_gpu"] = reference_gpu_row(xyz, tets)
+        except Exception as e:  # a checker row: its absence must not lose the reference line
+            line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -208,7 +280,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     q_final = opt.getQuality()
     # ---- timed region ----------------------------------------------------------------------------
+    # events around every step and around every iteration inside it (one graph replay: the colour
+    # launches of k_dmo_tet and the quality reduction)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    it_ev = [[torch.cuda.Event(enable_timing=True) for _ in range(N_ITER + 1)] for _ in range(args.steps)]
     replicas.barrier(dist)
     torch.cuda.synchronize()
     with ClockSampler(lr) as clk:
@@ -216,47 +291,68 @@ def run_ours(args):
             with torch.cuda.stream(stream):
                 flush.fill_(float(i))
                 ev[i][0].record(stream)
-                step()
+                reset()
+                opt.restart()
+                it_ev[i][0].record(stream)
+                for k in range(N_ITER):
+                    opt.iterate(1)
+                    it_ev[i][k + 1].record(stream)
                 ev[i][1].record(stream)
         torch.cuda.synchronize()
     replicas.barrier(dist)
     ms = sum(a.elapsed_time(b) for a, b in ev)
     ms_max = replicas.max_over_ranks(ms, dist, dev)
     value = replicas.whole_job_rate(n_inner * N_ITER * args.steps, ms_max, world)
+    iter_ms = sum(it_ev[i][0].elapsed_time(it_ev[i][N_ITER]) for i in range(args.steps)) / args.steps
+    clocks = clk.summary()
 
-    # ---- roofline of the grid-search kernel (separate pass, same stream) -----------------------------
-    reset()
-    opt.restart()
+    # ---- roofline of the grid-search kernel, inside the timed steps ------------------------------------
     n_col = mesh.info["nColorsInner"]
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-        for it in range(3):
-            for c in range(n_col):
-                _capi.check(lib.vsdmo_opt_run_color(opt.h, c))
-        e1.record(stream)
-    torch.cuda.synchronize()
-    dmo_ms = e0.elapsed_time(e1) / 3.0
-    bytes_per_update = 488  # 20 + 12k + 12|N| + 12 with k = 24 tets and |N| = 14 neighbours (interior Kuhn vertex)
-    bytes_iter = bytes_per_update * n_inner
-    achieved_gbs = bytes_iter / (dmo_ms / 1e3) / 1e9
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
-    hbm_peak = peaks.get("hbm_gbs") or 6650.0
-    traffic = None
+    prof = {}
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "dmo_tet_config2_traffic.json")))
-        # ncu DRAM bytes per vertex update, scaled to one iteration (the unit `achieved` uses)
-        traffic = prof["dram_bytes_per_vertex_update"] * n_inner
     except Exception:
         pass
-    # FP32 work of the search as the reference formulates it: 3 levels x 512 candidates x 24
-    # tets x ~80 FP32 operations per mean-ratio evaluation (plus cbrt) per vertex update
-    ref_flop_per_update = 3 * 512 * 24 * 80
-    fp32_nominal_tflops = 148 * 128 * 2 * 1.965e9 / 1e12
+    # k_dmo_tet's share of an iteration's device time (33 colour launches + 1 quality reduction),
+    # from the ncu launch list of this bench (profiles/launches_bench_config2.md)
+    share = prof.get("share_of_iteration", 0.988)
+    kern_ms_step = iter_ms * share
+    launches_step = n_col * N_ITER
+    avg_launch_s = kern_ms_step / launches_step / 1e3
+    upd_per_launch = n_inner / n_col
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    inst_per_update = prof.get("warp_instructions_per_vertex_update")
+    bytes_per_update = 488  # 20 + 12k + 12|N| + 12 with k = 24 tets and |N| = 14 neighbours (interior Kuhn vertex)
+    hbm_peak = peaks.get("hbm_gbs") or 6650.0
+    hbm_achieved = bytes_per_update * upd_per_launch / avg_launch_s / 1e9
+    issue_peak = 148 * 4 * sm_mhz * 1e6  # warp instructions per second: 4 schedulers x 148 SMs x clock
+    issue_achieved = inst_per_update * upd_per_launch / avg_launch_s if inst_per_update else None
+    traffic = prof.get("dram_bytes_per_vertex_update")
+    roofline = {
+        "bound": "issue", "kernel": "k_dmo_tet",
+        "achieved": issue_achieved, "peak": issue_peak, "unit": "warp-instructions/s",
+        "frac": issue_achieved / issue_peak if issue_achieved else None,
+        "traffic": traffic * upd_per_launch if traffic else None,
+        "per": "one launch (one colour class, average over the timed steps)",
+        "how": "achieved = warp instructions per vertex update (ncu smsp__inst_executed.sum on this workload, "
+               "profiles/k_dmo_tet_config2.md) x vertex updates per launch / average launch time; peak = 148 SMs "
+               "x 4 schedulers x median SM clock during the timed region; launch time = per-iteration CUDA "
+               "events inside the timed steps x k_dmo_tet's share of an iteration (ncu launch list)",
+        "warp_instructions_per_vertex_update": inst_per_update,
+        "kernel_ms_per_step": kern_ms_step, "iteration_ms_per_step": iter_ms,
+        "share_of_iteration": share, "launches_per_step": launches_step,
+        "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,
+                "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+                "algorithmic_bytes_per_vertex_update": bytes_per_update,
+                "dram_bytes_per_vertex_update": traffic,
+                "traffic_over_algorithmic": traffic / bytes_per_update if traffic else None},
+    }
+    assert kern_ms_step <= ms_max / args.steps * 1.0001 or world > 1
 
     # ---- end to end through the public API with host buffers ---------------------------------------------
     pin_xyz = torch.from_numpy(xyz).pin_memory()
@@ -294,34 +390,78 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Kuhn tet cube; the reference ships no meshes)",
         "config": workload_config({"final_min_quality": q_final, "colours": n_col}),
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "gpu_launches": (launches_per_iter * N_ITER + 2) * args.steps,
         "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": e2e_ms_med,
                 "h2d_bytes_per_step": int(xyz.nbytes + tets.nbytes), "d2h_bytes_per_step": int(xyz.nbytes),
                 "includes": "mesh build (connectivity + colouring) from pinned host arrays, 20 iterations, positions back to host"},
-        "roofline": {"bound": "hbm", "kernel": "k_dmo_tet", "achieved": achieved_gbs, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                     "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
-                     "algorithmic_bytes_per_vertex_update": bytes_per_update,
-                     "per": "one iteration (all colour launches); achieved = algorithmic bytes / kernel time",
-                     "kernel_ms_per_iteration": dmo_ms,
-                     "note": "compute-bound kernel: HBM fraction is reported as asked; see fp32"},
-        "fp32": {"reference_formulation_flop_per_vertex_update": ref_flop_per_update,
-                 "equivalent_tflops": ref_flop_per_update * n_inner / (dmo_ms / 1e3) / 1e12,
-                 "nominal_peak_tflops": fp32_nominal_tflops},
+        "roofline": roofline,
     }
     opt.close()
     mesh.close()
+    if r == 0 and world == 1 and not args.no_colour_priority:
+        line["colour_priority"] = colour_priority_rates(dev, stream, xyz, tets, value, n_col)
     if r == 0 and world == 1 and not args.no_learned:
         line["learned"] = learned_time_to_quality(dev, stream)
     if r == 0 and world == 1 and not args.no_batched:
         line["batched"] = batched_throughput(dev, stream)
     if r == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(xyz, tets)
+    # compact summaries last, where a tail of the line still shows them
+    summary = {"vertex_updates_per_s": value, "e2e_vertex_updates_per_s": e2e_value,
+               "issue_frac": roofline["frac"], "hbm_frac": roofline["hbm"]["frac"]}
+    if "learned" in line:
+        L = line["learned"]
+        summary["learned"] = {"time_ratio_learned_over_plain": L["time_ratio_learned_over_plain"],
+                              "learned_reached": L["learned_reached"], "learned_iterations": L["learned_iterations"],
+                              "plain_ms": L["plain_ms"], "learned_ms": L["learned_ms"],
+                              "excludes": "training (" + str(L["training"].get("train_s")) + " s) and pair "
+                                          "collection: one-off, on a separate 48^3 mesh"}
+    if "batched" in line:
+        B = line["batched"]
+        summary["batched"] = {"reference_config_vertex_updates_per_s": B["reference_config"]["vertex_updates_per_s"],
+                              "autotuned_vertex_updates_per_s": B["autotuned"]["vertex_updates_per_s"],
+                              "per_mesh_loop_vertex_updates_per_s": B["per_mesh_loop"]["vertex_updates_per_s"]}
+    if "colour_priority" in line:
+        summary["colour_priority"] = {k: line["colour_priority"][k]["vertex_updates_per_s"]
+                                      for k in ("hash", "reference")}
+    line["summary"] = summary
     if r == 0:
         print(json.dumps(line), flush=True)
     replicas.finish(dist)
     return 0
+
+
+def colour_priority_rates(dev, stream, xyz, tets, hash_value, hash_colours):
+    """The same 20-iteration plain DMO with the reference's JPL priorities n - i
+    (COLOR_REFERENCE) instead of the hashed ones: one warm-up and one timed run."""
+    import torch
+    import volumesurfacediscretemeshoptimization_b200 as V
+    sp = stream.cuda_stream
+    m = V.DMOMeshTet(xyz, tets, color_seed=V.COLOR_REFERENCE, stream=sp)
+    n_inner = m.info["nV"] - m.info["nSurf"]
+    o = V.DMOTetClass(m, n_iter=10 ** 9)
+    x0 = m.positions()
+    o.iterate(3)
+    m.set_positions(x0)
+    o.restart()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        a.record(stream)
+        o.iterate(N_ITER)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    q = o.getQuality()
+    out = {"hash": {"colours": hash_colours, "vertex_updates_per_s": hash_value},
+           "reference": {"colours": m.info["nColorsInner"], "vertex_updates_per_s": n_inner * N_ITER / (ms / 1e3),
+                         "ms": ms, "final_min_quality": q},
+           "how": "reference = priorities n - i of the reference's color_jpl (mesh/VertexColoring.cu:107-125); "
+                  "hash = the default seeded hash; same mesh, 20 iterations, no L2 flush"}
+    o.close()
+    m.close()
+    return out
 
 
 ONCE_AFTER = 1   # first iteration of the one-launch-per-iteration proposal schedule (variant)
@@ -506,6 +646,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--no-colour-priority", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
