@@ -44,7 +44,7 @@ constexpr unsigned FULL = 0xffffffffu;
 
 // packed position of feature (row, col) in the network's 96-column input operand
 __device__ __forceinline__ size_t learned_pk_off(long row, int col) { return tc::pk_off(row, col, 96); }
-// launch shape of the tet kernel (tuned on B200, see profiles/)
+// launch shape of the tet kernel: 4 warps per block, measured fastest on B200 against 2 and 8
 #ifndef TET_WARPS_CFG
 #define TET_WARPS_CFG 4
 #endif
@@ -154,7 +154,10 @@ __device__ __forceinline__ void tet_lane_best(const float4* __restrict__ co, int
 // full ring only for those, in the same operations and tet order as the plain search. The
 // winner, and whether the vertex moves, are the same as without the filter: every candidate
 // that beats qLast survives, and no discarded candidate can tie with or exceed one that does.
-constexpr int TET_CRIT = 4;      // tets of the filter
+#ifndef TET_CRIT_CFG
+#define TET_CRIT_CFG 6
+#endif
+constexpr int TET_CRIT = TET_CRIT_CFG;   // tets of the filter
 constexpr int TET_LIST = 256;    // survivors per warp evaluated from a list (more: full search)
 
 // (num, den, det) of tet t at (x, y, z): the operations of tet_key1
@@ -166,28 +169,54 @@ __device__ __forceinline__ float tet_piece_key(const float4* __restrict__ co, in
     return det < 0.f ? det : (det * det) / ((L * L) * L);
 }
 
-// the TET_CRIT tets of smallest key at (x, y, z) (ties: lower tet index), the same on all lanes
+// The TET_CRIT tets of smallest key at (x, y, z), the same on all lanes. Any choice of tets gives
+// an exact filter (the key over any subset bounds the ring key from above), so the choice needs
+// no exact arithmetic: a ring of up to 32 tets keys each tet once on its lane (fast division),
+// orders the keys as unsigned integers whose low 5 bits are the tet index and takes the minimum
+// TET_CRIT times with one warp reduction each. Larger rings scan their tets per round.
+__device__ __forceinline__ unsigned tet_order_key(float key, int t) {
+    const unsigned b = __float_as_uint(key);
+    const unsigned o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);   // float order as unsigned order
+    return (o & ~31u) | (unsigned)t;
+}
+
+__device__ __forceinline__ float tet_piece_key_fast(const float4* __restrict__ co, int t, float x, float y, float z) {
+    const float4 c0 = co[2 * t], c1 = co[2 * t + 1];
+    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    const float det = fmaf(c0.z, z, fmaf(c0.y, y, fmaf(c0.x, x, c0.w)));
+    const float L = ((c1.w + fmaf(c1.x, x, tx)) + fmaf(c1.y, y, ty)) + fmaf(c1.z, z, tz);
+    return det < 0.f ? det : __fdividef(det * det, (L * L) * L);
+}
+
 __device__ __forceinline__ void tet_critical(const float4* __restrict__ co, int k, float x, float y, float z, int lane,
                                              int (&crit)[TET_CRIT]) {
+    if (k <= 32) {
+        unsigned mine = lane < k ? tet_order_key(tet_piece_key_fast(co, lane, x, y, z), lane) : 0xffffffffu;
+#pragma unroll
+        for (int r = 0; r < TET_CRIT; ++r) {
+            const unsigned m = __reduce_min_sync(FULL, mine);
+            const int t = (int)(m & 31u);
+            crit[r] = t < k ? t : 0;
+            if (lane == t) mine = 0xffffffffu;
+        }
+        return;
+    }
 #pragma unroll
     for (int r = 0; r < TET_CRIT; ++r) {
-        float bk = FLT_MAX;
-        int bt = 1 << 30;
+        unsigned best = 0xffffffffu;
+        int bt = 0;
         for (int t = lane; t < k; t += 32) {
             bool used = false;
 #pragma unroll
             for (int q = 0; q < r; ++q) used |= (crit[q] == t);
             if (used) continue;
-            const float kt = tet_piece_key(co, t, x, y, z);
-            if (kt < bk || (kt == bk && t < bt) || bt == (1 << 30)) { bk = kt; bt = t; }
+            const unsigned kt = tet_order_key(tet_piece_key_fast(co, t, x, y, z), t & 31);
+            if (kt < best || (kt == best && t < bt)) { best = kt; bt = t; }
         }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            const float ok = __shfl_xor_sync(FULL, bk, o);
-            const int ot = __shfl_xor_sync(FULL, bt, o);
-            if (ot != (1 << 30) && (bt == (1 << 30) || ok < bk || (ok == bk && ot < bt))) { bk = ok; bt = ot; }
-        }
-        crit[r] = bt < k ? bt : 0;
+        // the warp's smallest (key, tet) pair: reduce the key, then the tet among the lanes holding it
+        const unsigned m = __reduce_min_sync(FULL, best);
+        const unsigned tt = __reduce_min_sync(FULL, best == m ? (unsigned)bt : 0xffffffffu);
+        crit[r] = tt < (unsigned)k ? (int)tt : 0;
     }
 }
 
@@ -223,8 +252,10 @@ __device__ __forceinline__ unsigned tet_filter(const float4* __restrict__ co, co
     for (int jj = 0; jj < 2; ++jj)
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
-            const float key = dm[jj][q] < 0.f ? dm[jj][q] : N[jj][q] / D[jj][q];
-            if (!(key < thr)) alive |= 1u << (jj * 8 + q);
+            // key < thr, with the fraction compared by cross-multiplication (its rounding is
+            // far inside thr's margin)
+            const bool below = dm[jj][q] < 0.f ? dm[jj][q] < thr : N[jj][q] < thr * D[jj][q];
+            if (!below) alive |= 1u << (jj * 8 + q);
         }
     return alive;
 }
