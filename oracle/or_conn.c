@@ -407,8 +407,9 @@ static int surface_init(or_mesh* m, int* old_of_cur, uint32_t seed, char* err, i
                 const float* f2 = m->fn + 3 * (size_t)h1[4 * opp + 2];
                 float dot = f1[0] * f2[0] + f1[1] * f2[1] + f1[2] * f2[2];
                 float len = sqrtf((f1[0] * f1[0] + f1[1] * f1[1] + f1[2] * f1[2]) * (f2[0] * f2[0] + f2[1] * f2[1] + f2[2] * f2[2]));
-                double angle = 180.0 / M_PI * (double)acosf(dot / len);
-                if (angle > 20.0) { m->isFeat[v] = 1; m->isFeat[dst] = 1; }
+                /* a float angle, as in the reference (MeshGPUCommon.cu:485-488) */
+                float angle = (float)(180.0 / M_PI * (double)acosf(dot / len));
+                if (angle > 20.f) { m->isFeat[v] = 1; m->isFeat[dst] = 1; }
             }
     }
     free(r1); free(h1);

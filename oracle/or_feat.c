@@ -78,8 +78,9 @@ void or_feature_flags(const or_mesh* m, const float* X, int32_t* fdeg, uint8_t* 
             for (int c = 0; c < 3; ++c) { u[c] = X[3 * (size_t)a + c] - p0[c]; w[c] = X[3 * (size_t)b + c] - p0[c]; }
             const float dot = d3f(u, w);
             const float len = sqrtf(d3f(u, u) * d3f(w, w));
-            const double ang = 180.0 / 3.14159265358979323846 * (double)acosf(dot / len);
-            opt[v] = ang >= 160.0;
+            /* a float angle, as in the reference (DMOCommon.h:157-158) */
+            const float ang = (float)(180.0 / 3.14159265358979323846 * (double)acosf(dot / len));
+            opt[v] = ang >= 160.f;
         }
     }
 }

@@ -998,6 +998,9 @@ static void normals_f64(const or_mesh* m, const double* X, double* fn, double* v
     }
 }
 
+/* face and vertex normals in double (MeshGPUCommon.cu:363-434), for the f64 iteration loops */
+void or_surface_normals_f64(const or_mesh* m, const double* X, double* fn, double* vn) { normals_f64(m, X, fn, vn); }
+
 void or_optimize_surf_f64(const or_mesh* m, double* X, int n_iter, double gs, int nthreads,
                           double* min_hist, double* mean_hist) {
     const int nS = or_mesh_info(m, OR_I_NSURF), nF = or_mesh_info(m, OR_I_NTRIS);

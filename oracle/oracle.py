@@ -76,6 +76,7 @@ def lib():
         L.or_optimize_f32.argtypes = [P, P, I, F, I, P, P]
         L.or_optimize_f64.argtypes = [P, P, I, D, I, P, P]
         L.or_surface_normals_f32.argtypes = [P, P, P, P]
+        L.or_surface_normals_f64.argtypes = [P, P, P, P]
         L.or_surface_fit_f32.argtypes = [P, P, P, P]
         L.or_surface_fit_f64.argtypes = [P, P, P, P]
         L.or_surface_fit_ring_f32.argtypes = [P, P, P, P, I]
@@ -402,6 +403,47 @@ class OracleMesh:
         ls = np.zeros((nS, 16), np.float32)
         lib().or_surface_fit_ring_f32(self.h, _p(xyz), _p(vn), _p(ls), int(ring))
         return xyz.copy(), ls, np.arange(nS, dtype=np.int32), fn, vn
+
+    def surface_normals_f64(self, xyz):
+        """(face normals [nTris, 3], vertex normals [nSurf, 3]) in double."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        fn = np.zeros((self.info["nTris"], 3)); vn = np.zeros((self.info["nSurf"], 3))
+        lib().or_surface_normals_f64(self.h, _p(xyz), _p(fn), _p(vn))
+        return fn, vn
+
+    def optimize_surf_features_f64(self, xyz, n_iter, grid_scale=0.5, nthreads=0):
+        """DMOTriClass / DMOQuadClass::doIteration (dmo/DMOTri.cu:128-165, dmo/DMOQuad.cu:125-162)
+        in double for a surface with feature vertices: free colours on their local (or sector)
+        surfaces, then the feature colours along their curves, the nearest-initial-vertex walk and
+        new normals; the quadric, sector and curve fits from the initial positions. Returns
+        (positions, per-iteration minimum, per-iteration mean)."""
+        x32 = np.ascontiguousarray(xyz, np.float32)
+        x = x32.astype(np.float64)
+        x0, ls, nn, vn = self.surface_state_f64(x32)
+        fn, vn = self.surface_normals_f64(x)
+        feat = self.info["nFeature"] > 0
+        sectors = self.sector_surfaces(x32, fn, dtype=np.float64) if feat else None
+        fdeg, flags = self.feature_flags(x32)
+        curves = self.curves_f64(x32, vn)
+        free = self.array(A_COL_FREE)
+        cf = self.array(A_COL_FEATURE)
+        mn, mean = [], []
+        for _ in range(n_iter):
+            for c in range(len(free) - 1):
+                v0, v1 = int(free[c]), int(free[c + 1])
+                if feat:
+                    x, _ = self.dmo_surf_feat_f64(x, x0, ls, nn, vn, sectors, v0, v1, grid_scale, nthreads)
+                else:
+                    x, _ = self.dmo_surf_color_f64(x, x0, ls, nn, vn, v0, v1, grid_scale, nthreads)
+            for c in range(len(cf) - 1):
+                x, _ = self.dmo_1d_f64(x, x0, curves, nn, vn, fdeg, flags, int(cf[c]), int(cf[c + 1]),
+                                       grid_scale, nthreads)
+            nn = nn.copy()
+            lib().or_update_nn_f64(self.h, _p(x), _p(x0), _p(nn))
+            fn, vn = self.surface_normals_f64(x)
+            q = self.element_qualities_f64(x)
+            mn.append(float(q.min())); mean.append(float(q.mean()))
+        return x, np.array(mn), np.array(mean)
 
     def surface_state_f64(self, xyz, ring=1):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)

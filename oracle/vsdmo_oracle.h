@@ -177,6 +177,7 @@ void or_hex_coeffs_f32(const float r[7][3], float eps_s, float eps_a, float* out
 /* ---- surfaces (tri / quad meshes without feature vertices) ----------------------------- */
 /* local surfaces: 16 values per surface vertex: p0[3] a, e0[3] b, e1[3] c, e2[3] numPoints  */
 void or_surface_normals_f32(const or_mesh* m, const float* xyz, float* face_normals, float* vertex_normals);
+void or_surface_normals_f64(const or_mesh* m, const double* xyz, double* face_normals, double* vertex_normals);
 int  or_surface_fit_f32(const or_mesh* m, const float* xyz, const float* vertex_normals, float* local_surfaces);
 int  or_surface_fit_f64(const or_mesh* m, const double* xyz, const double* vertex_normals, double* local_surfaces);
 /* ring 1: the fits above (centre + 1-ring, the reference); ring 2: centre + 1-ring + 2-ring */

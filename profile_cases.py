@@ -1,5 +1,5 @@
 """Small, self-contained workloads of each kernel family, for profiling one family at a time
-(``ncu -k <kernel> python -m volumesurfacediscretemeshoptimization_b200.profile_cases <case>``).
+(``ncu -k <kernel> python profile_cases.py <case>``).
 
 Every case builds its mesh, runs one warm-up iteration (graph capture) and then ``--iters``
 iterations, and prints one line with the case's time per iteration (CUDA events on the

@@ -4,7 +4,7 @@
 * connectivity and colouring: with the reference's JPL priorities (``COLOR_REFERENCE``), every
   array the library exports equals the reference's bit for bit (positions in the internal
   vertex order, elements, surface faces, halfedge / halfface / halfhex CSR, colour offsets,
-  flags); normals within float rounding (the reference is compiled with fused multiply-adds,
+  flags); normals within 1e-5 (the reference is compiled with fused multiply-adds,
   the library without). The oracle's restatement is held to the same arrays. With the library's
   default hashed priorities given to the reference's own JPL kernel, the same holds.
 * the grid search: one colour launch of the reference's kernel (interior tet / hex, flat
@@ -132,7 +132,7 @@ def _compare_arrays(A, B, where):
         if k in ("face_normals", "vertex_normals"):
             na, nb = np.isnan(a), np.isnan(b)
             assert np.array_equal(na, nb), (where, k)
-            np.testing.assert_allclose(a[~na], b[~nb], rtol=0, atol=2e-6, err_msg=f"{where} {k}")
+            np.testing.assert_allclose(a[~na], b[~nb], rtol=0, atol=1e-5, err_msg=f"{where} {k}")
         elif a.dtype == np.float32:
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (where, k)
         else:
@@ -160,12 +160,16 @@ def test_connectivity_equals_reference(ref, vsdmo, name, priorities):
     _compare_arrays(R, O_, "oracle")
 
 
-def test_reference_colouring_of_the_benchmark_mesh(ref, vsdmo):
-    """config 2 (48^3 Kuhn cube): the whole connectivity, colouring included, against the
-    reference's build of the same mesh."""
-    xyz, el = G.config2()
-    rm = ref.RefMesh(TET, xyz, el)
-    gm = _lib_mesh(vsdmo, TET, xyz, el)
+@pytest.mark.parametrize("cfg", ["config2", "config3_tri", "config3_quad"])
+def test_reference_connectivity_of_the_benchmark_meshes(ref, vsdmo, cfg):
+    """The full-size benchmark meshes (the 48^3 Kuhn cube; the icosphere and the torus with the
+    specified noise and their ~110 k / ~94 k feature vertices): the whole connectivity, colouring
+    and feature flags included, against the reference's build of the same mesh. Both evaluate the
+    dihedral rule with CUDA's acosf, so even the edge within an ulp of 20 degrees agrees."""
+    kind = {"config2": TET, "config3_tri": TRI, "config3_quad": QUAD}[cfg]
+    xyz, el = getattr(G, cfg)()
+    rm = ref.RefMesh(kind, xyz, el)
+    gm = _lib_mesh(vsdmo, kind, xyz, el)
     assert _norm_info(gm.info) == _norm_info(rm.info)
     _compare_arrays(rm.arrays(), gm.arrays(), "library")
 

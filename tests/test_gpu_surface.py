@@ -197,7 +197,9 @@ def test_surface_restart_rebuilds_state(oracle_mod, vsdmo):
 
 @pytest.mark.parametrize("cfg,kind,iters", [("config3_tri", TRI, 15), ("config3_quad", QUAD, 15)])
 def test_surface_benchmark_mesh_properties(oracle_mod, vsdmo, cfg, kind, iters):
-    xyz, el = getattr(G, cfg)()
+    """the feature-free variant of the config 3 meshes (the specified noise is covered by
+    test_gpu_full_size.py)"""
+    xyz, el = getattr(G, cfg)(variant="feature_free")
     om = oracle_mod.OracleMesh(kind, xyz, el)
     assert om.info["nFeature"] == 0
     gm = (vsdmo.DMOMeshQuad if kind == QUAD else vsdmo.DMOMeshTri)(xyz, el)

@@ -397,8 +397,10 @@ __global__ void k_flags_b1_feat(const uint32_t* srcs, const int4* he, long nHE, 
         const float* f2 = fn + 3 * (long)he[h.y].z;
         float dot = f1[0] * f2[0] + f1[1] * f2[1] + f1[2] * f2[2];
         float len = sqrtf((f1[0] * f1[0] + f1[1] * f1[1] + f1[2] * f1[2]) * (f2[0] * f2[0] + f2[1] * f2[1] + f2[2] * f2[2]));
-        double angle = 180.0 / 3.14159265358979323846 * (double)acosf(dot / len);
-        if (angle > 20.0) { isFeat[src] = 1; isFeat[h.x] = 1; }
+        // the reference keeps the angle as a float (float angle = 180.f / M_PI * acosf(..),
+        // MeshGPUCommon.cu:485-488): the double product is rounded before the compare
+        const float angle = (float)(180.0 / 3.14159265358979323846 * (double)acosf(dot / len));
+        if (angle > 20.f) { isFeat[src] = 1; isFeat[h.x] = 1; }
     }
 }
 

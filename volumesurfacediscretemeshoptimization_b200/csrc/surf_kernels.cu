@@ -623,8 +623,9 @@ __global__ void k_feature_flags(int nS, int nFree, const int* __restrict__ rowpt
             const float wx = pb.x - p0.x, wy = pb.y - p0.y, wz = pb.z - p0.z;
             const float dt = dot3(ux, uy, uz, wx, wy, wz);
             const float len = sqrtf(dot3(ux, uy, uz, ux, uy, uz) * dot3(wx, wy, wz, wx, wy, wz));
-            const double ang = 180.0 / 3.14159265358979323846 * (double)acosf(dt / len);
-            o = ang >= 160.0 ? 1 : 0;
+            // a float angle, as the reference keeps it (DMOCommon.h:157-158)
+            const float ang = (float)(180.0 / 3.14159265358979323846 * (double)acosf(dt / len));
+            o = ang >= 160.f ? 1 : 0;
         }
         opt[v] = o;
     }

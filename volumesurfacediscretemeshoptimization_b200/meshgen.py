@@ -191,12 +191,13 @@ def torus_quads(nu: int = 512, nv: int = 256, R: float = 1.0, r: float = 0.35):
     return xyz.astype(np.float32), q.astype(np.int32)
 
 
-def perturb_surface(xyz, elems, seed: int = 0, tangential: float = 0.35, normal_sigma: float = 1e-3):
+def perturb_surface(xyz, elems, seed: int = 0, tangential: float = 0.35, normal_sigma: float = 1e-3,
+                    normal_absolute: bool = False):
     """Tangential noise ``U(-t*l, t*l)`` (``l`` = mean incident edge length) in the tangent
-    plane of the area-weighted vertex normal, plus ``N(0, normal_sigma * l)`` along it. The
-    normal noise is relative to the edge length: an absolute sigma of 1e-3 on edges of ~0.01
-    tilts neighbouring faces by more than 20 degrees and turns most vertices into feature
-    vertices under the reference's dihedral rule (mesh/MeshTriGPU.cu:506)."""
+    plane of the area-weighted vertex normal, plus normal noise along it: ``N(0, normal_sigma)``
+    with ``normal_absolute``, else ``N(0, normal_sigma * l)``. An absolute sigma of 1e-3 on edges
+    of ~0.01 tilts neighbouring faces by more than 20 degrees and turns many vertices into
+    feature vertices under the reference's dihedral rule (mesh/MeshTriGPU.cu:506)."""
     xyz = xyz.astype(np.float64)
     k = elems.shape[1]
     nV = len(xyz)
@@ -218,7 +219,7 @@ def perturb_surface(xyz, elems, seed: int = 0, tangential: float = 0.35, normal_
     g = _rng(seed)
     a = g.uniform(-tangential, tangential, size=(nV, 2)) * lmean[:, None]
     nn = g.normal(0.0, normal_sigma, size=nV)
-    out = xyz + a[:, :1] * t1 + a[:, 1:] * t2 + (nn * lmean)[:, None] * vn
+    out = xyz + a[:, :1] * t1 + a[:, 1:] * t2 + (nn if normal_absolute else nn * lmean)[:, None] * vn
     return out.astype(np.float32)
 
 
@@ -246,22 +247,29 @@ def config2_hex(seed: int = 0, n: int = 32):
     return hex_cube(n, seed, 0.3)
 
 
-def config3_tri(seed: int = 0, level: int = 7):
-    """Icosphere level 7 (163,842 vertices / 327,680 triangles) with surface noise.
+def config3_tri(seed: int = 0, level: int = 7, variant: str = "as_written"):
+    """Icosphere level 7 (163,842 vertices / 327,680 triangles), radius 1, with surface noise.
 
-    Tangential noise 0.3 l: at 0.35 l a few triangles fold past the reference's 20 degree
-    dihedral rule and their vertices become feature vertices; at 0.3 l the sphere stays free
-    of features for every seed tried, as a smooth surface should."""
+    ``as_written``: tangential noise U(+-0.35 l) and normal noise N(0, 1e-3), absolute, as the
+    workload is specified; the normal noise makes many vertices feature vertices under the
+    reference's 20 degree dihedral rule, which the feature passes then move along their curves.
+    ``feature_free``: tangential 0.3 l and N(0, 1e-3 l), which keeps the sphere free of
+    feature vertices (a smooth-surface variant)."""
     v, f = icosphere(level)
+    if variant == "as_written":
+        return perturb_surface(v, f, seed, tangential=0.35, normal_sigma=1e-3, normal_absolute=True), f
     return perturb_surface(v, f, seed, tangential=0.3), f
 
 
-def config3_quad(seed: int = 0, nu: int = 512, nv: int = 256):
+def config3_quad(seed: int = 0, nu: int = 512, nv: int = 256, variant: str = "as_written"):
     """Torus R=1, r=0.35 with 512x256 quads and surface noise.
 
-    Tangential noise 0.2 l: the quads are up to 2:1 anisotropic (edges 0.008-0.017), and
-    larger noise folds some of them into feature vertices under the 20 degree rule."""
+    ``as_written``: tangential U(+-0.35 l) and absolute normal noise N(0, 1e-3), as specified.
+    ``feature_free``: tangential 0.2 l and N(0, 1e-3 l): the quads are up to 2:1 anisotropic
+    (edges 0.008-0.017) and larger noise folds some of them into feature vertices."""
     v, q = torus_quads(nu, nv)
+    if variant == "as_written":
+        return perturb_surface(v, q, seed, tangential=0.35, normal_sigma=1e-3, normal_absolute=True), q
     return perturb_surface(v, q, seed, tangential=0.2), q
 
 
