@@ -428,7 +428,10 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
 // warps stride over list[0 .. count[0]). The last warp to finish sets the queue back to empty
 // (count[0] = 0; count[1] counts the finished warps), so the next class's learned search
 // appends to an empty queue without a separate reset launch.
-__global__ void __launch_bounds__(TET_WARPS * 32, TET_MIN_BLOCKS)
+#ifndef TET_LIST_MIN_BLOCKS
+#define TET_LIST_MIN_BLOCKS 4   // 128 registers: four blocks per SM (164 unconstrained, three blocks)
+#endif
+__global__ void __launch_bounds__(TET_WARPS * 32, TET_LIST_MIN_BLOCKS)
 k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* __restrict__ hf,
                const int* __restrict__ list, int* __restrict__ count, float grid_scale, int depth, int maxk,
                uint8_t* __restrict__ dirty, unsigned long long* __restrict__ moved_count) {

@@ -265,19 +265,20 @@ __global__ void k_sum(const float* a, int n, float* out) {
 }
 
 // ---- fused inference for the learned tet search --------------------------------------------------
-// One persistent CTA per SM keeps the packed BF16 weights in shared memory (loaded once by bulk
-// copies) and runs FI_GROUPS independent groups of four warps. A group owns one 128-column
-// TMEM accumulator and one 32 KB activation buffer and loops over tiles of 128 vertices: each
-// thread builds its vertex's 96 inputs from the ring-vertex table straight into the packed A
-// operand, then the four layers run back to back on the tensor cores, every layer's
-// epilogue overwriting the buffer its own MMAs have finished reading. Groups synchronise on
-// their own named barrier, so one group's tensor-core phase overlaps another's feature gather.
-constexpr int FI_GROUPS = 4;
-constexpr int FI_THREADS = 128 * FI_GROUPS;
+// One persistent CTA of 16 warps per SM keeps the packed BF16 weights in shared memory (loaded
+// once by bulk copies) and runs tiles of 128 vertices one after the other, all warps on the same
+// tile so that a tile's latency chain is short (one class of a few hundred tiles is a single
+// wave): the four threads of a row build its 96 inputs from the ring-vertex table, eight ring
+// vertices each, straight into the packed A operand; then the four layers run back to back on
+// the tensor cores, and each layer's epilogue is split over the warps by TMEM lane quadrant
+// (rows) and 32-column block, overwriting the buffer its own MMAs have finished reading.
+constexpr int FI_THREADS = 512;
 constexpr uint32_t FI_W1 = 0, FI_W2 = FI_W1 + 3 * 8192, FI_W3 = FI_W2 + 4 * 8192, FI_W4 = FI_W3 + 4 * 8192;
 constexpr uint32_t FI_WBYTES = FI_W4 + 4 * 1024;                    // weights: 94,208 bytes
-constexpr uint32_t FI_BUF = FI_WBYTES;                              // + 32 KB per group
-constexpr uint32_t FI_SMEM = FI_BUF + FI_GROUPS * 4 * 8192;         // 225,280 bytes
+constexpr uint32_t FI_BUF = FI_WBYTES;                              // + one 32 KB activation tile
+constexpr uint32_t FI_SMEM = FI_BUF + 4 * 8192;                     // 126,976 bytes
+constexpr int FI_PARTS = FI_THREADS / 128;                          // threads per row of the tile
+constexpr int FI_NB_PART = MAX_NB / FI_PARTS;                       // ring vertices per thread
 
 // packed offset of (row, col) inside one 128-row tile held in shared memory
 __device__ __forceinline__ uint32_t tile_off(int r, int c) {
@@ -290,10 +291,6 @@ __device__ __forceinline__ void fi_store8(uint8_t* base, uint32_t off, const flo
 #pragma unroll
     for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16_rn(v[i]);
     *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(h);
-}
-
-__device__ __forceinline__ void group_sync(int g) {
-    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(128) : "memory");
 }
 
 // issue one layer: D[128 x N] = A (K columns, tile in smem) . B^T; b_chunk: bytes between the
@@ -314,23 +311,25 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
                 const uint8_t* __restrict__ W3p, const uint8_t* __restrict__ W4p, const float* __restrict__ params,
                 float* __restrict__ Y, int ldy, int* err) {
     extern __shared__ __align__(1024) uint8_t sm[];
-    __shared__ __align__(8) uint64_t bars[1 + FI_GROUPS];
+    __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t tmem_slot;
-    __shared__ int fail[FI_GROUPS];
+    __shared__ int s_fail;
+    __shared__ float s_max[FI_PARTS][128];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = threadIdx.x >> 7, r = threadIdx.x & 127;       // group, row of the tile
+    const int row = threadIdx.x & 127, part = threadIdx.x >> 7;
     const uint32_t sb = tc::smem_u32(sm);
-    const uint32_t bar_w = tc::smem_u32(&bars[0]), bar_m = tc::smem_u32(&bars[1 + g]);
+    const uint32_t bar_w = tc::smem_u32(&bars[0]), bar_m = tc::smem_u32(&bars[1]);
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 1 + FI_GROUPS; ++i) tc::mbar_init(tc::smem_u32(&bars[i]), 1);
+        tc::mbar_init(bar_w, 1);
+        tc::mbar_init(bar_m, 1);
         tc::mbar_init_fence();
-        for (int i = 0; i < FI_GROUPS; ++i) fail[i] = 0;
+        s_fail = 0;
     }
-    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128 * FI_GROUPS);
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
-    const uint32_t tmem = tmem_slot + 128u * g;
+    const uint32_t tmem = tmem_slot;
     if (threadIdx.x == 0) {
         tc::mbar_expect_tx(bar_w, FI_WBYTES);
         tc::bulk_g2s(sb + FI_W1, W1p, 3 * 8192, bar_w);
@@ -338,102 +337,133 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
         tc::bulk_g2s(sb + FI_W3, W3p, 4 * 8192, bar_w);
         for (int c = 0; c < 4; ++c) tc::bulk_g2s(sb + FI_W4 + 1024u * c, W4p + (size_t)c * 8192, 1024, bar_w);
     }
-    if (!tc::mbar_wait(bar_w, 0) && lane == 0) {
+    bool weights = tc::mbar_wait(bar_w, 0);
+    if (!weights && lane == 0) {
         atomicExch(err, tc::TC_TIMEOUT_LOAD);
-        fail[g] = 1;
+        s_fail = 1;
     }
     __syncthreads();
-    uint8_t* buf = sm + FI_BUF + (uint32_t)g * 4 * 8192;
-    const uint32_t sbuf = sb + FI_BUF + (uint32_t)g * 4 * 8192;
+    uint8_t* buf = sm + FI_BUF;
+    const uint32_t sbuf = sb + FI_BUF;
     const uint32_t id128 = tc::idesc_bf16(HID), id16 = tc::idesc_bf16(OUTP);
-    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    const bool issuer = r == 0;
+    const int q = warp & 3, cb = warp >> 2;                             // lane quadrant, column block
+    const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
+    const int erow = q * 32 + lane;                                     // this thread's row in the epilogue
     uint32_t phase = 0;
+    bool pending = false;                                               // an MMA commit not yet seen
     const int ntiles = (n + 127) / 128;
-    // group-major tile order: every CTA's first group gets a tile before any second group does
-    for (int tile = g * gridDim.x + blockIdx.x; tile < ntiles && !fail[g]; tile += gridDim.x * FI_GROUPS) {
-        // ---- inputs of this thread's vertex -> packed rows of X (in the group's buffer)
-        const int i = tile * 128 + r;
+    for (int tile = blockIdx.x; tile < ntiles && !s_fail; tile += gridDim.x) {
+        // ---- inputs: ring vertices FI_NB_PART * part .. + FI_NB_PART of this row's vertex
         {
+            const int i = tile * 128 + row;
             float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f);
-            const int* list = nullptr;
-            int cnt = 0;
+            int cnt = 0, self = 0;
+            int idx[FI_NB_PART];
             if (i < n) {
-                c0 = pos[v0 + i];
-                list = nb + (size_t)(v0 + i - nb_base) * MAX_NB;
-                cnt = nbn[v0 + i - nb_base];
+                self = v0 + i;
+                c0 = pos[self];
+                cnt = nbn[self - nb_base];
+                const int4* rw = reinterpret_cast<const int4*>(nb + (size_t)(self - nb_base) * MAX_NB) +
+                                 part * (FI_NB_PART / 4);
+#pragma unroll
+                for (int k = 0; k < FI_NB_PART / 4; ++k) {
+                    const int4 t = rw[k];
+                    idx[4 * k] = t.x; idx[4 * k + 1] = t.y; idx[4 * k + 2] = t.z; idx[4 * k + 3] = t.w;
+                }
+            } else {
+#pragma unroll
+                for (int a = 0; a < FI_NB_PART; ++a) idx[a] = 0;
             }
-            // each ring vertex loaded once; the 96 inputs stay in registers (fully unrolled)
-            float f[IN];
+            // unpredicated loads (slots past the ring load the vertex itself and contribute zeros)
+            float f[3 * FI_NB_PART];
             float mm = 0.f;
 #pragma unroll
-            for (int a = 0; a < MAX_NB; ++a) {
-                float dx = 0.f, dy = 0.f, dz = 0.f;
-                if (a < cnt) {
-                    const float4 q = pos[list[a]];
-                    dx = q.x - c0.x; dy = q.y - c0.y; dz = q.z - c0.z;
-                    mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
-                }
+            for (int a = 0; a < FI_NB_PART; ++a) {
+                const bool ok = part * FI_NB_PART + a < cnt;
+                const float4 p = pos[ok ? idx[a] : self];
+                const float dx = ok ? p.x - c0.x : 0.f, dy = ok ? p.y - c0.y : 0.f, dz = ok ? p.z - c0.z : 0.f;
+                mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
                 f[3 * a] = dx; f[3 * a + 1] = dy; f[3 * a + 2] = dz;
             }
+            s_max[part][row] = mm;
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < FI_PARTS; ++k) mm = fmaxf(mm, s_max[k][row]);
             const float inv = mm > 0.f ? 1.f / mm : 0.f;
 #pragma unroll
-            for (int c = 0; c < IN; ++c) f[c] = f[c] * inv;
+            for (int c = 0; c < 3 * FI_NB_PART; ++c) f[c] = f[c] * inv;
 #pragma unroll
-            for (int q = 0; q < IN / 8; ++q) fi_store8(buf, tile_off(r, 8 * q), f + 8 * q);
+            for (int k = 0; k < 3 * FI_NB_PART / 8; ++k)
+                fi_store8(buf, tile_off(row, 3 * FI_NB_PART * part + 8 * k), f + 8 * k);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc::tc_fence_before();
-        group_sync(g);
+        __syncthreads();
         const uint32_t srcW[3] = { FI_W1, FI_W2, FI_W3 };
         const int Ks[3] = { IN, HID, HID };
         const int boff[3] = { OFF_B1, OFF_B2, OFF_B3 };
         for (int l = 0; l < 4; ++l) {
-            if (issuer) {
+            if (threadIdx.x == 0) {
                 tc::tc_fence_after();
                 if (l < 3) fi_layer_issue(tmem, sbuf, sb + srcW[l], Ks[l], 8192u, id128, bar_m);
                 else fi_layer_issue(tmem, sbuf, sb + FI_W4, HID, 1024u, id16, bar_m);
             }
-            __syncwarp();
-            if (!tc::mbar_wait(bar_m, phase) && lane == 0) {
-                atomicExch(err, tc::TC_TIMEOUT_MMA);
-                fail[g] = 1;
-            }
-            phase ^= 1u;
-            tc::tc_fence_after();
-            if (l < 3) {
-                // the MMAs are done with the buffer: the activations overwrite it
-                const float* bias = params + boff[l];
-#pragma unroll 1
-                for (int c = 0; c < HID; c += 16) {
-                    float v[16];
-                    tc::tmem_ld16(lane_addr + (uint32_t)c, v);
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) v[e] = i < n ? fmaxf(v[e] + bias[c + e], 0.f) : 0.f;
-                    fi_store8(buf, tile_off(r, c), v);
-                    fi_store8(buf, tile_off(r, c + 8), v + 8);
+            pending = true;
+            if (!tc::mbar_wait(bar_m, phase)) {
+                if (lane == 0) {
+                    atomicExch(err, tc::TC_TIMEOUT_MMA);
+                    s_fail = 1;
                 }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             } else {
-                float v[16];
-                tc::tmem_ld16(lane_addr, v);
-                if (i < n) {
-                    const float* b4 = params + OFF_B4;
-                    float* y = Y + (size_t)i * ldy;
-                    y[0] = v[0] + b4[0];
-                    y[1] = v[1] + b4[1];
-                    y[2] = v[2] + b4[2];
+                pending = false;
+                phase ^= 1u;
+            }
+            tc::tc_fence_after();
+            const int i = tile * 128 + erow;
+            if (!pending) {
+                if (l < 3) {
+                    // the MMAs are done with the buffer: this warp's 32 rows x 32 columns of the
+                    // activations overwrite it
+                    const int c = 32 * cb;
+                    float v[32];
+                    tc::tmem_ld32(lane_addr + (uint32_t)c, v);
+                    const float4* b4 = reinterpret_cast<const float4*>(params + boff[l] + c);   // 16-byte aligned
+#pragma unroll
+                    for (int e = 0; e < 32; e += 4) {
+                        const float4 bb = __ldg(b4 + e / 4);
+                        v[e] = i < n ? fmaxf(v[e] + bb.x, 0.f) : 0.f;
+                        v[e + 1] = i < n ? fmaxf(v[e + 1] + bb.y, 0.f) : 0.f;
+                        v[e + 2] = i < n ? fmaxf(v[e + 2] + bb.z, 0.f) : 0.f;
+                        v[e + 3] = i < n ? fmaxf(v[e + 3] + bb.w, 0.f) : 0.f;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) fi_store8(buf, tile_off(erow, c + 8 * k), v + 8 * k);
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                } else if (cb == 0) {
+                    float v[16];
+                    tc::tmem_ld16(lane_addr, v);
+                    if (i < n) {
+                        const float* b4 = params + OFF_B4;
+                        float* y = Y + (size_t)i * ldy;
+                        y[0] = v[0] + b4[0];
+                        y[1] = v[1] + b4[1];
+                        y[2] = v[2] + b4[2];
+                    }
                 }
             }
             tc::tc_fence_before();
-            group_sync(g);
-            if (fail[g]) break;
+            __syncthreads();
+            if (s_fail) break;
         }
     }
+    // after a timed-out wait, give the copies and MMAs in flight a bounded time to land before
+    // the shared and tensor memory are released
+    if (!weights) (void)tc::mbar_wait(bar_w, 0);
+    if (pending) (void)tc::mbar_wait(bar_m, phase);
     __syncthreads();
     if (warp == 0) {
         tc::tc_fence_after();
-        tc::tmem_dealloc(tmem_slot, 128 * FI_GROUPS);
+        tc::tmem_dealloc(tmem_slot, 128);
     }
 }
 
