@@ -405,6 +405,8 @@ def run_ours(args):
         line["learned"] = learned_time_to_quality(dev, stream)
     if r == 0 and world == 1 and not args.no_batched:
         line["batched"] = batched_throughput(dev, stream)
+    if r == 0 and world == 1 and not args.no_surface:
+        line["surface"] = surface_rates(dev, stream)
     if r == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(xyz, tets)
     # compact summaries last, where a tail of the line still shows them
@@ -425,6 +427,9 @@ def run_ours(args):
     if "colour_priority" in line:
         summary["colour_priority"] = {k: line["colour_priority"][k]["vertex_updates_per_s"]
                                       for k in ("hash", "reference")}
+    if "surface" in line:
+        summary["surface_vertex_updates_per_s"] = {k: v["vertex_updates_per_s"] for k, v in line["surface"].items()
+                                                   if isinstance(v, dict)}
     line["summary"] = summary
     if r == 0:
         print(json.dumps(line), flush=True)
@@ -548,6 +553,48 @@ def learned_time_to_quality(dev, stream):
 
 
 BATCH_ITERS = 10
+SURF_ITERS = 15
+
+
+def surface_rates(dev, stream):
+    """The surface workloads with their feature passes on: the level-7 icosphere (triangles,
+    DMOTriClass) and the 512 x 256 torus (quads, DMOQuadClass), tangential noise 0.35 of the
+    local edge length and normal noise N(0, 1e-3), 15 iterations. One warm-up iteration (graph
+    capture), positions reset, then the 15 timed iterations (CUDA events on the library stream).
+    A vertex update is one vertex moved by its pass: every surface vertex is visited once per
+    iteration, free vertices by the surface search and feature vertices by the curve search."""
+    import torch
+    import volumesurfacediscretemeshoptimization_b200 as V
+    from volumesurfacediscretemeshoptimization_b200 import meshgen as G
+    sp = stream.cuda_stream
+    out = {}
+    for name, gen, mcls, ocls in (("config3_tri", G.config3_tri, V.DMOMeshTri, V.DMOTriClass),
+                                  ("config3_quad", G.config3_quad, V.DMOMeshQuad, V.DMOQuadClass)):
+        xyz, el = gen()
+        m = mcls(xyz, el, stream=sp)
+        o = ocls(m, n_iter=SURF_ITERS)
+        o.iterate(1)
+        m.set_positions(xyz, original_order=True)
+        o.restart()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            o.iterate(SURF_ITERS)
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        mn, mean = o.quality_stats()
+        n_upd = m.info["nSurf"]
+        out[name] = {"vertices": m.info["nV"], "feature_vertices": m.info["nFeature"], "iterations": SURF_ITERS,
+                     "ms": ms, "vertex_updates_per_s": n_upd * SURF_ITERS / (ms / 1e3),
+                     "final_min_quality": mn, "final_mean_quality": mean,
+                     "launches_per_iteration": o.launches_per_iteration}
+        o.close()
+        m.close()
+    out["workload"] = ("icosphere level 7 (163842 vertices) and torus 512x256 quads (131072 vertices), tangential "
+                       "noise 0.35 local edge, normal N(0, 1e-3), seed 0, feature vertices sliding on their curves")
+    return out
 
 
 def batched_throughput(dev, stream):
@@ -648,6 +695,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-colour-priority", action="store_true")
+    ap.add_argument("--no-surface", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -350,9 +350,19 @@ VSDMO_API vsdmo_status vsdmo_opt_set_proposal_schedule(vsdmo_opt_t opt, int once
  * reduced search, [1] fallbacks to the plain search, [2] fallbacks that moved the vertex,
  * [3] vertices skipped by the active set (plain and learned mode). */
 VSDMO_API vsdmo_status vsdmo_opt_learned_counters(vsdmo_opt_t opt, unsigned long long* counters4);
-/* Test entry point of the tensor-core GEMM: D [M x N] = bf16(A) [M x K] . bf16(B) [N x K]^T
- * in FP32, host arrays; N in {16, 32, 64, 96, 128}, K a multiple of 32. */
+/* TEST-ONLY: the tensor-core GEMM alone, D [M x N] = bf16(A) [M x K] . bf16(B) [N x K]^T in
+ * FP32, host arrays; N in {16, 32, 64, 96, 128}, K a multiple of 32. It allocates and
+ * synchronises per call; no product path uses it. */
 VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int M, int N, int K, float* D);
+/* TEST-ONLY: lowers the limit of the bounded device waits that report VSDMO_E_TIMEOUT -- the
+ * colour-class waits of the batched iteration, the stage waits of the tensor-core GEMM and the
+ * weight / MMA waits of the proposal inference -- on the current device, so that a test can make
+ * them expire. ns = 0 makes the GEMM and inference waits expire at once and a batch colour wait
+ * as soon as it is entered (a colour class still being searched); ns < 0 restores the default of
+ * 1 s; above 1 s is refused (VSDMO_E_ARG). The
+ * waits that let copies and MMAs in flight land after an expiry keep 1 s. Synchronises the
+ * device; call it with none of the library's work in flight. */
+VSDMO_API vsdmo_status vsdmo_debug_set_wait_limit_ns(int64_t ns);
 
 /* Feature-vertex state of an optimiser with feature vertices (surfaces with features, flat
  * meshes with sliding boundaries), internal numbering: curves [nSurf x 12] (p0[3] a, e0[3] 0,

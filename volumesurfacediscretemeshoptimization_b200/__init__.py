@@ -540,6 +540,13 @@ def debug_gemm_bf16(A, B) -> np.ndarray:
     return D
 
 
+def debug_set_wait_limit_ns(ns: int) -> None:
+    """Test entry point: limit of the bounded device waits that report a timeout (batched
+    colour-class waits, tensor-core GEMM and inference waits) on the current device; 0 makes
+    them expire, a negative value restores the default of 1 s."""
+    check(_capi.lib().vsdmo_debug_set_wait_limit_ns(int(ns)))
+
+
 class DMOHexClass(_DMOBase):
     """``DMO::DMOHexClass`` (``dmo/DMOHex.h``): interior hex DMO with ``shapeMetricHex``."""
 

@@ -30,7 +30,7 @@ EXPORTED = [
     "vsdmo_quality_reduce_noalloc", "vsdmo_model_num_params", "vsdmo_model_create", "vsdmo_model_destroy",
     "vsdmo_model_get_params", "vsdmo_model_set_params", "vsdmo_model_forward", "vsdmo_model_gradients",
     "vsdmo_model_train", "vsdmo_opt_collect_pairs", "vsdmo_opt_set_model", "vsdmo_opt_learned_counters",
-    "vsdmo_debug_gemm_bf16", "vsdmo_opt_proposals", "vsdmo_opt_set_proposal_schedule",
+    "vsdmo_debug_gemm_bf16", "vsdmo_debug_set_wait_limit_ns", "vsdmo_opt_proposals", "vsdmo_opt_set_proposal_schedule",
     "vsdmo_batch_create", "vsdmo_batch_destroy", "vsdmo_batch_iterate", "vsdmo_batch_iterate_async",
     "vsdmo_batch_sync", "vsdmo_batch_restart", "vsdmo_batch_stats", "vsdmo_batch_get_positions",
     "vsdmo_batch_set_positions", "vsdmo_batch_get_config", "vsdmo_batch_set_config", "vsdmo_batch_autotune",
@@ -148,6 +148,8 @@ def lib():
     L.vsdmo_opt_proposals.argtypes = [P, I, P]
     L.vsdmo_debug_gemm_bf16.restype = S
     L.vsdmo_debug_gemm_bf16.argtypes = [P, P, I, I, I, P]
+    L.vsdmo_debug_set_wait_limit_ns.restype = S
+    L.vsdmo_debug_set_wait_limit_ns.argtypes = [C.c_int64]
     L.vsdmo_batch_create.restype = S
     L.vsdmo_batch_create.argtypes = [I, P, P, P, P, P, I, U, P, C.POINTER(P)]
     L.vsdmo_batch_destroy.restype = None

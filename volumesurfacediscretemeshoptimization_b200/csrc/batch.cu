@@ -34,6 +34,9 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int BCO = 9;                 // coefficient floats per ring element
 constexpr int BATCH_WARPS = 8;
 constexpr unsigned long long BWAIT_NS = 1000000000ull;
+// limit of a colour-class wait: BWAIT_NS unless the test-only vsdmo_debug_set_wait_limit_ns
+// lowered it to make waits expire
+__device__ unsigned long long g_batch_wait_ns = BWAIT_NS;
 
 __device__ __forceinline__ unsigned long long bnow() {
     unsigned long long t;
@@ -224,10 +227,11 @@ k_batch_iter(float4* __restrict__ pos, const int* __restrict__ rowptr, const int
                 const int need = csize[mh.col_base + it.color - 1];
                 if (*d < need) {
                     const unsigned long long t0 = bnow();
+                    const unsigned long long lim = *(volatile unsigned long long*)&g_batch_wait_ns;
                     while (*d < need) {
                         if (*ve) { ok = 0; break; }
                         __nanosleep(128);
-                        if (bnow() - t0 > BWAIT_NS) { ok = 0; atomicExch(err, 1); break; }
+                        if (bnow() - t0 >= lim) { ok = 0; atomicExch(err, 1); break; }
                     }
                 }
                 __threadfence();
@@ -602,6 +606,12 @@ void Batch::iterate(int n) {
     }
     for (int i = 0; i < n; ++i) VSDMO_CUDA(cudaGraphLaunch(exec, stream));
     iters_done += n;
+}
+
+void batch_set_wait_limit(unsigned long long ns) {
+    VSDMO_CUDA(cudaDeviceSynchronize());
+    VSDMO_CUDA(cudaMemcpyToSymbol(g_batch_wait_ns, &ns, sizeof(ns)));
+    VSDMO_CUDA(cudaDeviceSynchronize());
 }
 
 void Batch::check_errors() {

@@ -99,4 +99,7 @@ struct Batch {
     void quality(BatchStats* out, int* d_it, int init, cudaStream_t s) const;
 };
 
+// limit of the colour-class waits of the batched iteration on the current device (test-only lowering)
+void batch_set_wait_limit(unsigned long long ns);
+
 }  // namespace vsdmo

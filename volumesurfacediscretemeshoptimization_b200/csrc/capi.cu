@@ -690,10 +690,12 @@ VSDMO_API vsdmo_status vsdmo_opt_iterate(vsdmo_opt_t o, int n_iter) {
             else run_iteration_body(o, s);
         }
         auto h = read_stats(o, o->iters_done + 1, n_iter);
-        if (o->model) o->model->m.check(s);
         for (auto& x : h) failures += x.fail_count;
         o->iters_done += n_iter;
         o->last_min = h.back().min_q;
+        // an expired network wait is reported after the iterations are counted: they ran, and
+        // every move was evaluated on the current ring whatever the proposals held
+        if (o->model) o->model->m.check(s);
     });
     if (st != VSDMO_OK) return st;
     if (failures) return fail(VSDMO_E_MONOTONE, "minimum quality decreased during the iteration");

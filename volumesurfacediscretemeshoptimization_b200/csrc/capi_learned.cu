@@ -36,6 +36,15 @@ VSDMO_API vsdmo_status vsdmo_debug_gemm_bf16(const float* A, const float* B, int
     });
 }
 
+VSDMO_API vsdmo_status vsdmo_debug_set_wait_limit_ns(int64_t ns) {
+    if (ns > 1000000000ll) return fail(VSDMO_E_ARG, "the wait limit can only be lowered (at most 1e9 ns)");
+    const unsigned long long lim = ns < 0 ? 1000000000ull : (unsigned long long)ns;
+    return guarded([&] {
+        mlp::set_wait_limit(lim);
+        batch_set_wait_limit(lim);
+    });
+}
+
 VSDMO_API int vsdmo_model_num_params(void) { return mlp::N_PARAMS; }
 
 VSDMO_API vsdmo_status vsdmo_model_create(uint64_t seed, void* cuda_stream, vsdmo_model_t* out) {

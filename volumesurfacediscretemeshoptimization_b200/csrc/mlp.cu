@@ -337,7 +337,7 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
         tc::bulk_g2s(sb + FI_W3, W3p, 4 * 8192, bar_w);
         for (int c = 0; c < 4; ++c) tc::bulk_g2s(sb + FI_W4 + 1024u * c, W4p + (size_t)c * 8192, 1024, bar_w);
     }
-    bool weights = tc::mbar_wait(bar_w, 0);
+    bool weights = tc::mbar_wait_reported(bar_w, 0);
     if (!weights && lane == 0) {
         atomicExch(err, tc::TC_TIMEOUT_LOAD);
         s_fail = 1;
@@ -409,7 +409,7 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
                 else fi_layer_issue(tmem, sbuf, sb + FI_W4, HID, 1024u, id16, bar_m);
             }
             pending = true;
-            if (!tc::mbar_wait(bar_m, phase)) {
+            if (!tc::mbar_wait_reported(bar_m, phase)) {
                 if (lane == 0) {
                     atomicExch(err, tc::TC_TIMEOUT_MMA);
                     s_fail = 1;
@@ -692,7 +692,18 @@ void Model::infer_tet(const float4* pos, const int* nb, const int* nbn, int nb_b
 
 void Model::check(cudaStream_t s) {
     const int e = read_scalar(err.p, s);
-    if (e) throw Error(VSDMO_E_TIMEOUT, "tensor-core GEMM wait expired (code " + std::to_string(e) + ")");
+    if (e) {
+        // the report is consumed: the next launch on this model starts from a clear flag
+        VSDMO_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+        VSDMO_CUDA(cudaStreamSynchronize(s));
+        throw Error(VSDMO_E_TIMEOUT, "tensor-core wait expired (code " + std::to_string(e) + ")");
+    }
+}
+
+void set_wait_limit(unsigned long long ns) {
+    VSDMO_CUDA(cudaDeviceSynchronize());
+    VSDMO_CUDA(cudaMemcpyToSymbol(tc::g_wait_limit_ns, &ns, sizeof(ns)));
+    VSDMO_CUDA(cudaDeviceSynchronize());
 }
 
 // Prepares every GEMM instantiation (dynamic shared-memory limits) outside stream capture.

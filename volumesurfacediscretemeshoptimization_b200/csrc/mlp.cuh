@@ -65,6 +65,8 @@ struct Model {
 
 void prepare(cudaStream_t s);
 void debug_gemm(const float* hA, const float* hB, int M, int N, int K, float* hD, cudaStream_t s);
+// limit of the reported tensor-core waits on the current device (test-only lowering)
+void set_wait_limit(unsigned long long ns);
 
 }  // namespace mlp
 }  // namespace vsdmo

@@ -75,14 +75,39 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// bounded wait for the phase with the given parity; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    if (mbar_try(bar, parity)) return true;
+// non-blocking test of the phase with the given parity
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// wait of at most limit_ns for the phase with the given parity; false on timeout. The first
+// check does not block, so a zero limit expires unless the phase has already completed.
+__device__ __forceinline__ bool mbar_wait_for(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
+    if (mbar_test(bar, parity)) return true;
     const unsigned long long t0 = now_ns();
-    while (true) {
+    while (now_ns() - t0 < limit_ns)
         if (mbar_try(bar, parity)) return true;
-        if (now_ns() - t0 > WAIT_NS) return false;
-    }
+    return false;
+}
+
+// the limit of the waits whose expiry a kernel reports (the GEMM's stage waits, the inference
+// kernel's weight and MMA waits): WAIT_NS unless the test-only vsdmo_debug_set_wait_limit_ns
+// lowered it to make them expire; 0 makes them expire at once, whatever the barrier's state,
+// so that a test does not depend on how fast a copy or an MMA lands. The waits that drain
+// copies and MMAs in flight after an expiry, before shared and tensor memory are released,
+// always use WAIT_NS.
+static __device__ unsigned long long g_wait_limit_ns = WAIT_NS;
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) { return mbar_wait_for(bar, parity, WAIT_NS); }
+__device__ __forceinline__ bool mbar_wait_reported(uint32_t bar, uint32_t parity) {
+    const unsigned long long lim = *(volatile unsigned long long*)&g_wait_limit_ns;
+    return lim != 0 && mbar_wait_for(bar, parity, lim);
 }
 
 // global -> shared bulk copy, completion counted on an mbarrier (no multicast)
@@ -234,7 +259,7 @@ __device__ bool gemm_tile(const uint8_t* __restrict__ A, const uint8_t* __restri
         for (int i = 0; i < nk; ++i) {
             const int s = i % STAGES;
             const uint32_t ph = (uint32_t)(i / STAGES) & 1u;
-            if (!mbar_wait(full0 + 8u * s, ph)) { code = TC_TIMEOUT_LOAD; break; }
+            if (!mbar_wait_reported(full0 + 8u * s, ph)) { code = TC_TIMEOUT_LOAD; break; }
             ++consumed;
             tc_fence_after();
             const uint32_t a = sbase + (uint32_t)s * STAGE_BYTES, b = a + CHUNK_BYTES;
@@ -243,7 +268,7 @@ __device__ bool gemm_tile(const uint8_t* __restrict__ A, const uint8_t* __restri
                 mma_bf16(tmem, smem_desc(a + 256u * j), smem_desc(b + 256u * j), idesc, (i > 0 || j > 0) ? 1u : 0u);
             mma_commit(empty0 + 8u * s);
             if (i + STAGES < nk) {
-                if (!mbar_wait(empty0 + 8u * s, ph)) { code = TC_TIMEOUT_MMA; break; }
+                if (!mbar_wait_reported(empty0 + 8u * s, ph)) { code = TC_TIMEOUT_MMA; break; }
                 load(i + STAGES);
             }
         }
