@@ -266,18 +266,22 @@ __global__ void k_sum(const float* a, int n, float* out) {
 
 // ---- fused inference for the learned tet search --------------------------------------------------
 // One persistent CTA of 16 warps per SM keeps the packed BF16 weights in shared memory (loaded
-// once by bulk copies) and runs tiles of 128 vertices one after the other, all warps on the same
-// tile so that a tile's latency chain is short (one class of a few hundred tiles is a single
-// wave): the four threads of a row build its 96 inputs from the ring-vertex table, eight ring
-// vertices each, straight into the packed A operand; then the four layers run back to back on
-// the tensor cores, and each layer's epilogue is split over the warps by TMEM lane quadrant
-// (rows) and 32-column block, overwriting the buffer its own MMAs have finished reading.
+// once by bulk copies) and runs two tiles of 128 vertices at a time: the CTA is two groups of
+// 8 warps, each with its own activation buffer, 128 TMEM columns and MMA barrier, so one
+// group's ring gathers (global loads) overlap the other group's layer chain (MMAs and
+// epilogues). Within a group the two threads of a row build its 96 inputs from the ring-vertex
+// table, sixteen ring vertices each, straight into the packed A operand; the four layers then
+// run back to back on the tensor cores, each layer's epilogue split over the group's warps by
+// TMEM lane quadrant (rows) and 64-column half, overwriting the buffer its own MMAs have
+// finished reading. Groups synchronise on their own named barrier.
 constexpr int FI_THREADS = 512;
+constexpr int FI_GROUPS = 2;
+constexpr int FI_GTHREADS = FI_THREADS / FI_GROUPS;                 // threads of a group
 constexpr uint32_t FI_W1 = 0, FI_W2 = FI_W1 + 3 * 8192, FI_W3 = FI_W2 + 4 * 8192, FI_W4 = FI_W3 + 4 * 8192;
 constexpr uint32_t FI_WBYTES = FI_W4 + 4 * 1024;                    // weights: 94,208 bytes
-constexpr uint32_t FI_BUF = FI_WBYTES;                              // + one 32 KB activation tile
-constexpr uint32_t FI_SMEM = FI_BUF + 4 * 8192;                     // 126,976 bytes
-constexpr int FI_PARTS = FI_THREADS / 128;                          // threads per row of the tile
+constexpr uint32_t FI_BUF = FI_WBYTES;                              // + one 32 KB activation tile per group
+constexpr uint32_t FI_SMEM = FI_BUF + FI_GROUPS * 4 * 8192;         // 159,744 bytes
+constexpr int FI_PARTS = FI_GTHREADS / 128;                         // threads per row of the tile
 constexpr int FI_NB_PART = MAX_NB / FI_PARTS;                       // ring vertices per thread
 
 // packed offset of (row, col) inside one 128-row tile held in shared memory
@@ -305,31 +309,40 @@ __device__ __forceinline__ void fi_layer_issue(uint32_t tmem, uint32_t a, uint32
     tc::mma_commit(bar);
 }
 
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(FI_GTHREADS) : "memory");
+}
+
 __global__ void __launch_bounds__(FI_THREADS, 1)
 k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, const int* __restrict__ nbn, int nb_base,
                 int v0, int n, const uint8_t* __restrict__ W1p, const uint8_t* __restrict__ W2p,
                 const uint8_t* __restrict__ W3p, const uint8_t* __restrict__ W4p, const float* __restrict__ params,
                 float* __restrict__ Y, int ldy, int* err) {
     extern __shared__ __align__(1024) uint8_t sm[];
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[1 + FI_GROUPS];
     __shared__ uint32_t tmem_slot;
-    __shared__ int s_fail;
-    __shared__ float s_max[FI_PARTS][128];
+    __shared__ int s_wfail;
+    // expired MMA waits of a group, one slot per step parity: a slot written in step s is read
+    // after the group barrier of step s and next written in step s + 2, after every thread of
+    // the group has passed the barrier of step s + 1, so all threads of a group read the same value
+    __shared__ int s_fail[FI_GROUPS][2];
+    __shared__ float s_max[FI_GROUPS][FI_PARTS][128];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = threadIdx.x & 127, part = threadIdx.x >> 7;
+    const int g = warp >> 3, gt = threadIdx.x & (FI_GTHREADS - 1);  // group, thread in the group
+    const int row = gt & 127, part = gt >> 7;
     const uint32_t sb = tc::smem_u32(sm);
-    const uint32_t bar_w = tc::smem_u32(&bars[0]), bar_m = tc::smem_u32(&bars[1]);
+    const uint32_t bar_w = tc::smem_u32(&bars[0]), bar_m = tc::smem_u32(&bars[1 + g]);
     if (threadIdx.x == 0) {
-        tc::mbar_init(bar_w, 1);
-        tc::mbar_init(bar_m, 1);
+        for (int b = 0; b < 1 + FI_GROUPS; ++b) tc::mbar_init(tc::smem_u32(&bars[b]), 1);
         tc::mbar_init_fence();
-        s_fail = 0;
+        s_wfail = 0;
+        for (int b = 0; b < FI_GROUPS; ++b) s_fail[b][0] = s_fail[b][1] = 0;
     }
-    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128);
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tmem_slot), 128 * FI_GROUPS);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
-    const uint32_t tmem = tmem_slot;
+    const uint32_t tmem = tmem_slot + 128u * (uint32_t)g;             // this group's 128 columns
     if (threadIdx.x == 0) {
         tc::mbar_expect_tx(bar_w, FI_WBYTES);
         tc::bulk_g2s(sb + FI_W1, W1p, 3 * 8192, bar_w);
@@ -340,19 +353,23 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
     bool weights = tc::mbar_wait_reported(bar_w, 0);
     if (!weights && lane == 0) {
         atomicExch(err, tc::TC_TIMEOUT_LOAD);
-        s_fail = 1;
+        s_wfail = 1;
     }
     __syncthreads();
-    uint8_t* buf = sm + FI_BUF;
-    const uint32_t sbuf = sb + FI_BUF;
+    uint8_t* buf = sm + FI_BUF + (uint32_t)g * 4u * 8192u;
+    const uint32_t sbuf = sb + FI_BUF + (uint32_t)g * 4u * 8192u;
     const uint32_t id128 = tc::idesc_bf16(HID), id16 = tc::idesc_bf16(OUTP);
-    const int q = warp & 3, cb = warp >> 2;                             // lane quadrant, column block
+    const int q = warp & 3, ch = (warp >> 2) & 1;                      // lane quadrant, 64-column half
     const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
     const int erow = q * 32 + lane;                                     // this thread's row in the epilogue
+    const bool issuer = gt == 0;
     uint32_t phase = 0;
     bool pending = false;                                               // an MMA commit not yet seen
+    int step = 0;
     const int ntiles = (n + 127) / 128;
-    for (int tile = blockIdx.x; tile < ntiles && !s_fail; tile += gridDim.x) {
+    const int stride = FI_GROUPS * gridDim.x;
+    bool stop = s_wfail != 0;
+    for (int tile = blockIdx.x + g * gridDim.x; tile < ntiles && !stop; tile += stride) {
         // ---- inputs: ring vertices FI_NB_PART * part .. + FI_NB_PART of this row's vertex
         {
             const int i = tile * 128 + row;
@@ -385,10 +402,10 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
                 mm = fmaxf(mm, fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))));
                 f[3 * a] = dx; f[3 * a + 1] = dy; f[3 * a + 2] = dz;
             }
-            s_max[part][row] = mm;
-            __syncthreads();
+            s_max[g][part][row] = mm;
+            group_sync(g);
 #pragma unroll
-            for (int k = 0; k < FI_PARTS; ++k) mm = fmaxf(mm, s_max[k][row]);
+            for (int k = 0; k < FI_PARTS; ++k) mm = fmaxf(mm, s_max[g][k][row]);
             const float inv = mm > 0.f ? 1.f / mm : 0.f;
 #pragma unroll
             for (int c = 0; c < 3 * FI_NB_PART; ++c) f[c] = f[c] * inv;
@@ -398,12 +415,12 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc::tc_fence_before();
-        __syncthreads();
+        group_sync(g);
         const uint32_t srcW[3] = { FI_W1, FI_W2, FI_W3 };
         const int Ks[3] = { IN, HID, HID };
         const int boff[3] = { OFF_B1, OFF_B2, OFF_B3 };
-        for (int l = 0; l < 4; ++l) {
-            if (threadIdx.x == 0) {
+        for (int l = 0; l < 4; ++l, ++step) {
+            if (issuer) {
                 tc::tc_fence_after();
                 if (l < 3) fi_layer_issue(tmem, sbuf, sb + srcW[l], Ks[l], 8192u, id128, bar_m);
                 else fi_layer_issue(tmem, sbuf, sb + FI_W4, HID, 1024u, id16, bar_m);
@@ -412,7 +429,7 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
             if (!tc::mbar_wait_reported(bar_m, phase)) {
                 if (lane == 0) {
                     atomicExch(err, tc::TC_TIMEOUT_MMA);
-                    s_fail = 1;
+                    s_fail[g][step & 1] = 1;
                 }
             } else {
                 pending = false;
@@ -422,24 +439,27 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
             const int i = tile * 128 + erow;
             if (!pending) {
                 if (l < 3) {
-                    // the MMAs are done with the buffer: this warp's 32 rows x 32 columns of the
+                    // the MMAs are done with the buffer: this warp's 32 rows x 64 columns of the
                     // activations overwrite it
-                    const int c = 32 * cb;
-                    float v[32];
-                    tc::tmem_ld32(lane_addr + (uint32_t)c, v);
-                    const float4* b4 = reinterpret_cast<const float4*>(params + boff[l] + c);   // 16-byte aligned
 #pragma unroll
-                    for (int e = 0; e < 32; e += 4) {
-                        const float4 bb = __ldg(b4 + e / 4);
-                        v[e] = i < n ? fmaxf(v[e] + bb.x, 0.f) : 0.f;
-                        v[e + 1] = i < n ? fmaxf(v[e + 1] + bb.y, 0.f) : 0.f;
-                        v[e + 2] = i < n ? fmaxf(v[e + 2] + bb.z, 0.f) : 0.f;
-                        v[e + 3] = i < n ? fmaxf(v[e + 3] + bb.w, 0.f) : 0.f;
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = 64 * ch + 32 * h;
+                        float v[32];
+                        tc::tmem_ld32(lane_addr + (uint32_t)c, v);
+                        const float4* b4 = reinterpret_cast<const float4*>(params + boff[l] + c);   // 16-byte aligned
+#pragma unroll
+                        for (int e = 0; e < 32; e += 4) {
+                            const float4 bb = __ldg(b4 + e / 4);
+                            v[e] = i < n ? fmaxf(v[e] + bb.x, 0.f) : 0.f;
+                            v[e + 1] = i < n ? fmaxf(v[e + 1] + bb.y, 0.f) : 0.f;
+                            v[e + 2] = i < n ? fmaxf(v[e + 2] + bb.z, 0.f) : 0.f;
+                            v[e + 3] = i < n ? fmaxf(v[e + 3] + bb.w, 0.f) : 0.f;
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) fi_store8(buf, tile_off(erow, c + 8 * k), v + 8 * k);
                     }
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) fi_store8(buf, tile_off(erow, c + 8 * k), v + 8 * k);
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                } else if (cb == 0) {
+                } else if (ch == 0) {
                     float v[16];
                     tc::tmem_ld16(lane_addr, v);
                     if (i < n) {
@@ -452,8 +472,8 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
                 }
             }
             tc::tc_fence_before();
-            __syncthreads();
-            if (s_fail) break;
+            group_sync(g);
+            if (s_fail[g][step & 1]) { stop = true; ++step; break; }
         }
     }
     // after a timed-out wait, give the copies and MMAs in flight a bounded time to land before
@@ -463,7 +483,7 @@ k_mlp_tet_infer(const float4* __restrict__ pos, const int* __restrict__ nb, cons
     __syncthreads();
     if (warp == 0) {
         tc::tc_fence_after();
-        tc::tmem_dealloc(tmem_slot, 128);
+        tc::tmem_dealloc(tmem_slot, 128 * FI_GROUPS);
     }
 }
 
