@@ -276,15 +276,31 @@ __device__ __forceinline__ float tet_key_min(const float4* __restrict__ co, int 
 // Setup of one tet vertex shared by the plain and the learned search: per-axis extent of the
 // ring (DMOTetImplCub.h:54-64), the exact power-of-two scale 2^ex and the element coefficients
 // in shared memory. Returns false when the ring is degenerate (the vertex is left alone).
+// KEEP: rings of up to 32 tets (all of a Kuhn cube's) keep their lane's corners in registers
+// between the extent and the coefficients (one register more than the learned search can spare
+// at seven blocks per SM); otherwise the corners are loaded again.
+template <bool KEEP>
 __device__ __forceinline__ bool tet_setup(const float4* __restrict__ pos, const int4* __restrict__ hf, int b, int k,
                                           float4 c0, int lane, float4* co, float& sx, float& sy, float& sz, int& ex) {
     float mdx = 0.f, mdy = 0.f, mdz = 0.f;
-    for (int t = lane; t < k; t += 32) {
-        const int4 h = hf[b + t];
-        const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
-        mdx = fmaxf(mdx, fabsf(pa.x - c0.x)); mdy = fmaxf(mdy, fabsf(pa.y - c0.y)); mdz = fmaxf(mdz, fabsf(pa.z - c0.z));
-        mdx = fmaxf(mdx, fabsf(pb.x - c0.x)); mdy = fmaxf(mdy, fabsf(pb.y - c0.y)); mdz = fmaxf(mdz, fabsf(pb.z - c0.z));
-        mdx = fmaxf(mdx, fabsf(pc.x - c0.x)); mdy = fmaxf(mdy, fabsf(pc.y - c0.y)); mdz = fmaxf(mdz, fabsf(pc.z - c0.z));
+    const bool one = KEEP && k <= 32;
+    float4 qa = c0, qb = c0, qc = c0;
+    if (one) {
+        if (lane < k) {
+            const int4 h = hf[b + lane];
+            qa = pos[h.x]; qb = pos[h.y]; qc = pos[h.z];
+        }
+        mdx = fmaxf(fabsf(qa.x - c0.x), fmaxf(fabsf(qb.x - c0.x), fabsf(qc.x - c0.x)));
+        mdy = fmaxf(fabsf(qa.y - c0.y), fmaxf(fabsf(qb.y - c0.y), fabsf(qc.y - c0.y)));
+        mdz = fmaxf(fabsf(qa.z - c0.z), fmaxf(fabsf(qb.z - c0.z), fabsf(qc.z - c0.z)));
+    } else {
+        for (int t = lane; t < k; t += 32) {
+            const int4 h = hf[b + t];
+            const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
+            mdx = fmaxf(mdx, fabsf(pa.x - c0.x)); mdy = fmaxf(mdy, fabsf(pa.y - c0.y)); mdz = fmaxf(mdz, fabsf(pa.z - c0.z));
+            mdx = fmaxf(mdx, fabsf(pb.x - c0.x)); mdy = fmaxf(mdy, fabsf(pb.y - c0.y)); mdz = fmaxf(mdz, fabsf(pb.z - c0.z));
+            mdx = fmaxf(mdx, fabsf(pc.x - c0.x)); mdy = fmaxf(mdy, fabsf(pc.y - c0.y)); mdz = fmaxf(mdz, fabsf(pc.z - c0.z));
+        }
     }
     mdx = warp_max(mdx); mdy = warp_max(mdy); mdz = warp_max(mdz);
     const float mm = fmaxf(mdx, fmaxf(mdy, mdz));
@@ -292,8 +308,11 @@ __device__ __forceinline__ bool tet_setup(const float4* __restrict__ pos, const 
     (void)frexpf(mm, &ex);
     const float p = exp2_exact(-ex);
     for (int t = lane; t < k; t += 32) {
-        const int4 h = hf[b + t];
-        const float4 pa = pos[h.x], pb = pos[h.y], pc = pos[h.z];
+        float4 pa = qa, pb = qb, pc = qc;
+        if (!one) {
+            const int4 h = hf[b + t];
+            pa = pos[h.x]; pb = pos[h.y]; pc = pos[h.z];
+        }
         float4 K0, K1;
         tet_coeffs(scale2(pa.x - c0.x, p, -ex), scale2(pa.y - c0.y, p, -ex), scale2(pa.z - c0.z, p, -ex),
                    scale2(pb.x - c0.x, p, -ex), scale2(pb.y - c0.y, p, -ex), scale2(pb.z - c0.z, p, -ex),
@@ -413,8 +432,8 @@ k_dmo_tet(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
     const float4 c0 = pos[v];
     float sx, sy, sz;
     int ex;
-    if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
-    const float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
+    if (!tet_setup<true>(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
+    const float qLast = tet_key_origin(co, k);
     float dx, dy, dz;
     const bool moved = tet_plain_search(co, list, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
     if (moved && lane == 0) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
@@ -447,8 +466,8 @@ k_dmo_tet_list(float4* __restrict__ pos, const int* __restrict__ rowptr, const i
         const float4 c0 = pos[v];
         float sx, sy, sz;
         int ex;
-        if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) continue;
-        const float qLast = tet_key1(co, k, 0.f, 0.f, 0.f);
+        if (!tet_setup<true>(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) continue;
+        const float qLast = tet_key_origin(co, k);
         float dx, dy, dz;
         const bool moved = tet_plain_search(co, slist, k, sx, sy, sz, grid_scale, depth, lane, qLast, dx, dy, dz);
         if (moved && lane == 0) {
@@ -589,7 +608,7 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
     const float4 c0 = pos[v];
     float sx, sy, sz;
     int ex;
-    if (!tet_setup(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
+    if (!tet_setup<false>(pos, hf, b, k, c0, lane, co, sx, sy, sz, ex)) return;
     const float q0 = tet_key_min(co, k, 0.f, 0.f, 0.f, lane);
     // proposal in scaled local coordinates (the features were divided by mm = max(sx, sy, sz) 2^ex)
     const float mms = fmaxf(sx, fmaxf(sy, sz));

@@ -58,5 +58,20 @@ static __device__ float tet_key1(const float4* co, int k, float x, float y, floa
     return dm < 0.f ? dm : N / D;
 }
 
+// tet_key1 at the local origin (the vertex itself): det = d0 and L = C exactly there (every term
+// that carries the candidate is a product with +-0 added to them), so the same fold runs on the
+// constant coefficients alone and returns the same key
+static __device__ float tet_key_origin(const float4* co, int k) {
+    float N = 0.f, D = 1.f, dm = 0.f;
+    for (int t = 0; t < k; ++t) {
+        const float det = co[2 * t].w, L = co[2 * t + 1].w;
+        const float num = det * det;
+        const float den = (L * L) * L;
+        if (t == 0) { N = num; D = den; dm = det; continue; }
+        if (num * D < N * den) { N = num; D = den; }
+        dm = fminf(dm, det);
+    }
+    return dm < 0.f ? dm : N / D;
+}
 
 }  // namespace vsdmo
