@@ -115,8 +115,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+_HOST_CPU = None
+
+
 def host_cpu():
-    """(model name, physical cores, logical CPUs usable by this process)."""
+    """(model name, physical cores, logical CPUs usable by this process), read once: after the
+    first OpenMP region with OMP_PROC_BIND the main thread is bound to one core, so a later
+    sched_getaffinity would report that core alone."""
+    global _HOST_CPU
+    if _HOST_CPU is None:
+        _HOST_CPU = _read_host_cpu()
+    return _HOST_CPU
+
+
+def _read_host_cpu():
     model, cores = None, set()
     try:
         cur = {}
