@@ -115,10 +115,10 @@ void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
                                 o->stats.p, o->d_iter.p, s);
         }
         if (o->pass1d)
-            for (const auto& r : o->franges) {
+            for (const auto& r : o->fmranges) {
                 DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
                 launch_dmo_1d_vol(m, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p, criterion_of(o->kind),
-                                  o->stats.p, o->d_iter.p, s);
+                                  o->stats.p, o->d_iter.p, s, o->fmove.p);
             }
         launch_mark_rings(m, 0, m.nSurf, o->dirty.p, s);
         launch_update_nn(m, o->X0.p, o->nn.p, s);
@@ -127,10 +127,10 @@ void run_iteration_body(vsdmo_opt_s* o, cudaStream_t s) {
         // feature vertices along their curves (flat meshes: only while the last minimum quality is
         // positive, dmo/DMOTriFlat.cu:140)
         const int mode = o->slide ? 0 : (m.fk == 3 ? 1 : 2);
-        for (const auto& r : o->franges) {
+        for (const auto& r : o->fmranges) {
             DmoLaunch L{r.first, r.second, o->p.grid_scale, o->p.depth};
             launch_dmo_1d(m, mode, L, o->X0.p, o->LS1.p, o->nn.p, o->fdeg.p, o->fopt.p, criterion_of(o->kind),
-                          o->slide ? o->stats.p : nullptr, o->slide ? o->d_iter.p : nullptr, s);
+                          o->slide ? o->stats.p : nullptr, o->slide ? o->d_iter.p : nullptr, s, o->fmove.p);
         }
     }
     if (o->mode == MODE_SURF || o->slide) launch_update_nn(m, o->X0.p, o->nn.p, s);
@@ -144,6 +144,33 @@ __global__ void k_surface_state(const float4* pos, int nS, float4* X0, int* nn) 
         X0[i] = pos[i];
         nn[i] = i;
     }
+}
+
+// The 1D pass only moves the feature vertices whose flag is set (two feature ring vertices at
+// 160 degrees or more); the others return at once. Their ids, class by class, let the pass
+// launch one warp per movable vertex and skip classes without any. A rebuild can change the
+// launch sizes, so captured iterations are dropped.
+void build_feature_movers(vsdmo_opt_s* o) {
+    const Mesh& m = o->mesh->m;
+    cudaStream_t s = m.stream;
+    const int nFree = m.nSurf - m.nFeature;
+    std::vector<uint8_t> flags(std::max(m.nFeature, 1));
+    if (m.nFeature > 0)
+        VSDMO_CUDA(cudaMemcpyAsync(flags.data(), o->fopt.p + nFree, m.nFeature, cudaMemcpyDeviceToHost, s));
+    VSDMO_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> ids;
+    o->fmranges.clear();
+    for (const auto& r : o->franges) {
+        const int b = (int)ids.size();
+        for (int v = r.first; v < r.second; ++v)
+            if (flags[v - nFree]) ids.push_back(v);
+        if ((int)ids.size() > b) o->fmranges.push_back({b, (int)ids.size()});
+    }
+    o->fmove.alloc(std::max<size_t>(ids.size(), 1), s);
+    if (!ids.empty())
+        VSDMO_CUDA(cudaMemcpyAsync(o->fmove.p, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, s));
+    VSDMO_CUDA(cudaStreamSynchronize(s));
+    o->drop_graphs();
 }
 
 // initial positions, normals, local surfaces and nn = identity from the current positions
@@ -172,6 +199,7 @@ void init_surface_state(vsdmo_opt_s* o) {
             o->fopt.alloc(m.nSurf, s);
         }
         init_feature_state(m, o->slide ? 1 : 0, o->LS1.p, o->fdeg.p, o->fopt.p, s);
+        build_feature_movers(o);
         if (surfaces) {
             o->nsect = build_sectors(m, o->srow, o->stab, o->FS, s);
             if (!o->Xs.p) o->Xs.alloc(m.nSurf, s);
@@ -735,7 +763,7 @@ VSDMO_API int vsdmo_opt_launches_per_iteration(vsdmo_opt_t o) {
     // colour launches + quality kernel (+ nearest-neighbour walk and two normal kernels)
     return (int)o->ranges.size() + 1 + (o->mode == MODE_SURF || o->volsurf ? 3 : 0) + (o->slide ? 1 : 0) +
            (o->volsurf && o->dirty.p ? 1 : 0) +
-           (o->pass1d ? (int)o->franges.size() : 0) + (int)o->sranges.size();
+           (o->pass1d ? (int)o->fmranges.size() : 0) + (int)o->sranges.size();
 }
 
 VSDMO_API vsdmo_status vsdmo_opt_feature_state(vsdmo_opt_t o, float* curves, int32_t* fdeg, uint8_t* flags,

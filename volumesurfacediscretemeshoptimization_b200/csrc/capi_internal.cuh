@@ -37,6 +37,10 @@ struct vsdmo_opt_s {
     DBuf<float4> Xs;                           // positions at the start of a colour class [nSurf]
     int nsect = 0;
     std::vector<std::pair<int, int>> franges;  // feature colour classes
+    // movable feature vertices (the 1D pass moves them, fopt set), class by class: fmove holds
+    // their ids, fmranges[c] the range of class c in it (rebuilt with the flags)
+    DBuf<int> fmove;
+    std::vector<std::pair<int, int>> fmranges;
     DBuf<float4> X0;                           // surface mode: initial surface positions [nSurf]
     DBuf<float4> LS;                           // local surfaces [4 nSurf]
     DBuf<int> nn;                              // nearest initial vertex [nSurf]

@@ -847,11 +847,13 @@ k_dmo_1d(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* _
          const uint8_t* __restrict__ isB1, const float4* __restrict__ X0, const float4* __restrict__ LS1,
          const int* __restrict__ nn, const float* __restrict__ vn, const int* __restrict__ fdeg,
          const uint8_t* __restrict__ opt, int nFree, int v0, int v1, float grid_scale, int maxk,
-         const IterStats* __restrict__ stats, const int* __restrict__ iter) {
+         const IterStats* __restrict__ stats, const int* __restrict__ iter, const int* __restrict__ list) {
     extern __shared__ float4 s1d[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int v = v0 + blockIdx.x * SURF_WARPS + warp;
-    if (v >= v1 || !opt[v]) return;
+    const int i = v0 + blockIdx.x * SURF_WARPS + warp;
+    if (i >= v1) return;
+    const int v = list ? list[i] : i;
+    if (!opt[v]) return;
     if (stats && !(stats[*iter].min_q > 0.f)) return;
     const int b = rowptr[v], k = rowptr[v + 1] - b;
     if (k <= 0 || k > maxk) return;
@@ -1015,11 +1017,13 @@ k_dmo_1d_vol(float4* __restrict__ pos, const int* __restrict__ rowptr, const int
              const int* __restrict__ hf_rowptr, const int4* __restrict__ hf, const float4* __restrict__ X0,
              const float4* __restrict__ LS1, const int* __restrict__ nn, const int* __restrict__ fdeg,
              const uint8_t* __restrict__ opt, int nFree, int v0, int v1, float grid_scale, int maxkt, int maxks,
-             const IterStats* __restrict__ stats, const int* __restrict__ iter) {
+             const IterStats* __restrict__ stats, const int* __restrict__ iter, const int* __restrict__ list) {
     extern __shared__ float4 s1t[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int v = v0 + blockIdx.x * SURF_WARPS + warp;
-    if (v >= v1 || !opt[v]) return;
+    const int i = v0 + blockIdx.x * SURF_WARPS + warp;
+    if (i >= v1) return;
+    const int v = list ? list[i] : i;
+    if (!opt[v]) return;
     if (!(stats[*iter].min_q > 0.f)) return;
     const int b = rowptr[v], ks = rowptr[v + 1] - b;
     if (ks <= 0 || ks > maxks || hf_rowptr[v + 1] - hf_rowptr[v] > maxkt) return;
@@ -1228,13 +1232,13 @@ static void surf_vol_launch(const Mesh& m, const DmoLaunch& L, const float4* X0,
 template <class R>
 static void vol_1d_launch(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
                           const int* fdeg, const uint8_t* opt, const IterStats* gate_stats, const int* gate_iter,
-                          cudaStream_t s) {
+                          cudaStream_t s, const int* list) {
     const int n = L.v1 - L.v0;
     const int maxkt = std::max(m.maxTets, 1), maxks = std::max(m.maxHE, 1);
     const size_t smem = (size_t)SURF_WARPS * (R::F4 * maxkt + (maxks + 3) / 4) * sizeof(float4);
     k_dmo_1d_vol<R><<<(n + SURF_WARPS - 1) / SURF_WARPS, SURF_WARPS * 32, smem, s>>>(
         m.pos.p, m.he_rowptr.p, m.he.p, m.hf_rowptr.p, m.type == VSDMO_HEX ? m.hh.p : m.hf.p, X0, LS1, nn, fdeg, opt,
-        m.nSurf - m.nFeature, L.v0, L.v1, L.grid_scale, maxkt, maxks, gate_stats, gate_iter);
+        m.nSurf - m.nFeature, L.v0, L.v1, L.grid_scale, maxkt, maxks, gate_stats, gate_iter, list);
     VSDMO_CHECK_LAUNCH();
 }
 
@@ -1250,12 +1254,12 @@ void launch_dmo_surf_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, co
 
 void launch_dmo_1d_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
                        const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
-                       cudaStream_t s) {
+                       cudaStream_t s, const int* list) {
     if (L.v1 <= L.v0) return;
-    if (m.type == VSDMO_HEX) vol_1d_launch<HexRing>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
-    else if (crit == 1) vol_1d_launch<TetAngleRing<false>>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
-    else if (crit == 2) vol_1d_launch<TetAngleRing<true>>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
-    else vol_1d_launch<TetRing>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s);
+    if (m.type == VSDMO_HEX) vol_1d_launch<HexRing>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s, list);
+    else if (crit == 1) vol_1d_launch<TetAngleRing<false>>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s, list);
+    else if (crit == 2) vol_1d_launch<TetAngleRing<true>>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s, list);
+    else vol_1d_launch<TetRing>(m, L, X0, LS1, nn, fdeg, opt, gate_stats, gate_iter, s, list);
 }
 
 int surf_vol_max_ring(int elem_type) { return elem_type == VSDMO_HEX ? HEX_SURF_MAX_RING : TET_SURF_MAX_RING; }
@@ -1277,7 +1281,7 @@ void prepare_surf_kernels() {
 
 void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
                    const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
-                   cudaStream_t s) {
+                   cudaStream_t s, const int* list) {
     const int n = L.v1 - L.v0;
     if (n <= 0) return;
     const int maxk = std::max(m.maxHE, 1);
@@ -1288,7 +1292,7 @@ void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0
            : mode == 1 ? (crit == 1 ? k_dmo_1d<1, 1> : (crit == 2 ? k_dmo_1d<1, 2> : k_dmo_1d<1, 0>))
                        : (crit == 1 ? k_dmo_1d<0, 1> : (crit == 2 ? k_dmo_1d<0, 2> : k_dmo_1d<0, 0>));
     k<<<blocks, SURF_WARPS * 32, smem, s>>>(m.pos.p, m.he_rowptr.p, m.he.p, m.isB1.p, X0, LS1, nn, m.vn.p, fdeg, opt,
-                                            nFree, L.v0, L.v1, L.grid_scale, maxk, gate_stats, gate_iter);
+                                            nFree, L.v0, L.v1, L.grid_scale, maxk, gate_stats, gate_iter, list);
     VSDMO_CHECK_LAUNCH();
 }
 

@@ -235,16 +235,18 @@ int build_sectors(const Mesh& m, DBuf<int>& srow, DBuf<int>& stab, DBuf<float4>&
 void launch_dmo_surf_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS, const int* nn,
                          const SectorSurfaces* sec, int crit, const IterStats* gate_stats, const int* gate_iter,
                          cudaStream_t s);
+// list (optional): the vertices of the class, L.v0 .. L.v1 then index the list instead of the
+// vertices (the movable feature vertices of the class; the others would return at once)
 void launch_dmo_1d_vol(const Mesh& m, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
                        const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
-                       cudaStream_t s);
+                       cudaStream_t s, const int* list = nullptr);
 int surf_vol_max_ring(int elem_type);
 void prepare_surf_kernels();
 // One colour class of feature vertices: mode 0 flat (gated on the last minimum quality being
 // positive when gate_stats is set), 1 surface triangles, 2 surface quads.
 void launch_dmo_1d(const Mesh& m, int mode, const DmoLaunch& L, const float4* X0, const float4* LS1, const int* nn,
                    const int* fdeg, const uint8_t* opt, int crit, const IterStats* gate_stats, const int* gate_iter,
-                   cudaStream_t s);
+                   cudaStream_t s, const int* list = nullptr);
 int dmo_surf_max_ring();     // largest halfedge row the surface kernel accepts
 // nu x nv samples of vertex vid's own surface (estimate_mode 0) or of the blended estimate (1)
 void launch_surface_samples(const Mesh& m, int estimate_mode, int vid, int nu, int nv, float grid_scale,
