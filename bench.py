@@ -412,7 +412,7 @@ def run_ours(args):
     opt.close()
     mesh.close()
     if r == 0 and world == 1 and not args.no_colour_priority:
-        line["colour_priority"] = colour_priority_rates(dev, stream, xyz, tets, value, n_col)
+        line["colour_priority"] = colour_priority_rates(dev, stream, xyz, tets, value, n_col, q_final)
     if r == 0 and world == 1 and not args.no_learned:
         line["learned"] = learned_time_to_quality(dev, stream)
     if r == 0 and world == 1 and not args.no_batched:
@@ -438,7 +438,7 @@ def run_ours(args):
                               "per_mesh_loop_vertex_updates_per_s": B["per_mesh_loop"]["vertex_updates_per_s"]}
     if "colour_priority" in line:
         summary["colour_priority"] = {k: line["colour_priority"][k]["vertex_updates_per_s"]
-                                      for k in ("hash", "reference")}
+                                      for k in ("default", "hash_rounds", "reference")}
     if "surface" in line:
         summary["surface_vertex_updates_per_s"] = {k: v["vertex_updates_per_s"] for k, v in line["surface"].items()
                                                    if isinstance(v, dict)}
@@ -449,35 +449,38 @@ def run_ours(args):
     return 0
 
 
-def colour_priority_rates(dev, stream, xyz, tets, hash_value, hash_colours):
-    """The same 20-iteration plain DMO with the reference's JPL priorities n - i
-    (COLOR_REFERENCE) instead of the hashed ones: one warm-up and one timed run."""
+def colour_priority_rates(dev, stream, xyz, tets, hash_value, hash_colours, hash_min_q):
+    """The same 20-iteration plain DMO under the other colourings: round colours (the
+    reference's rule) with the default hashed priorities (COLOR_ROUNDS | 1), and with the
+    reference's own priorities n - i (COLOR_REFERENCE); one warm-up and one timed run each."""
     import torch
     import volumesurfacediscretemeshoptimization_b200 as V
     sp = stream.cuda_stream
-    m = V.DMOMeshTet(xyz, tets, color_seed=V.COLOR_REFERENCE, stream=sp)
-    n_inner = m.info["nV"] - m.info["nSurf"]
-    o = V.DMOTetClass(m, n_iter=10 ** 9)
-    x0 = m.positions()
-    o.iterate(3)
-    m.set_positions(x0)
-    o.restart()
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        a.record(stream)
-        o.iterate(N_ITER)
-        b.record(stream)
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b)
-    q = o.getQuality()
-    out = {"hash": {"colours": hash_colours, "vertex_updates_per_s": hash_value},
-           "reference": {"colours": m.info["nColorsInner"], "vertex_updates_per_s": n_inner * N_ITER / (ms / 1e3),
-                         "ms": ms, "final_min_quality": q},
-           "how": "reference = priorities n - i of the reference's color_jpl (mesh/VertexColoring.cu:107-125); "
-                  "hash = the default seeded hash; same mesh, 20 iterations, no L2 flush"}
-    o.close()
-    m.close()
+    out = {"default": {"colours": hash_colours, "vertex_updates_per_s": hash_value, "final_min_quality": hash_min_q}}
+    for name, seed in (("hash_rounds", V.COLOR_ROUNDS | 1), ("reference", V.COLOR_REFERENCE)):
+        m = V.DMOMeshTet(xyz, tets, color_seed=seed, stream=sp)
+        n_inner = m.info["nV"] - m.info["nSurf"]
+        o = V.DMOTetClass(m, n_iter=10 ** 9)
+        x0 = m.positions()
+        o.iterate(3)
+        m.set_positions(x0)
+        o.restart()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            o.iterate(N_ITER)
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        out[name] = {"colours": m.info["nColorsInner"], "vertex_updates_per_s": n_inner * N_ITER / (ms / 1e3),
+                     "ms": ms, "final_min_quality": o.getQuality()}
+        o.close()
+        m.close()
+    out["how"] = ("default = the seeded hash priorities, each vertex taking the smallest colour its higher-priority "
+                  "neighbours leave free; hash_rounds = the same priorities, colour = JPL round (the reference's rule, "
+                  "mesh/VertexColoring.cu:76-105); reference = round colours with the reference's priorities n - i "
+                  "(mesh/VertexColoring.cu:107-125); same mesh, 20 iterations, no L2 flush")
     return out
 
 

@@ -139,10 +139,16 @@ VSDMO_API vsdmo_status vsdmo_params_default(int elem_type, vsdmo_params* out);
 /* Replaces DMOMeshTriFactory::create(int nVS, int nT, CudaArray<Vec3f>&, CudaArray<Triangle>&)
  * (mesh/MeshFactory.cu:15-31), DMOMeshTetFactory::create (mesh/MeshFactory.cu:45-55, minus the
  * file parsing) and the MeshTetGPU::init / MeshTriGPU::init builds they run
- * (mesh/MeshTetGPU.cu:35-42, mesh/MeshTriGPU.cu:37-50). color_seed seeds the colouring
- * priorities (the reference's live colouring is cusparseScsrcolor, VertexColoring.cu:128-153);
- * VSDMO_COLOR_REFERENCE instead selects the priorities of the reference's own JPL colouring,
- * n - i for local index i of the n vertices coloured together (VertexColoring.cu:107-125). */
+ * (mesh/MeshTetGPU.cu:35-42, mesh/MeshTriGPU.cu:37-50). Colouring (the reference's live
+ * colouring is cusparseScsrcolor, VertexColoring.cu:128-153) runs the rounds of the reference's
+ * JPL rule (VertexColoring.cu:76-105) with priorities hashed from color_seed; by default a vertex
+ * takes the smallest colour none of its higher-priority neighbours has (the greedy colouring in
+ * priority order: 11 classes on the 48^3 tet cube where round colours give 33). Two values
+ * select the reference's own rule, colour = round:
+ *   VSDMO_COLOR_ROUNDS | s  round colours, priorities hashed from s (the low 31 bits);
+ *   VSDMO_COLOR_REFERENCE   round colours with the reference's priorities n - i for local
+ *                           index i of the n vertices coloured together (VertexColoring.cu:107-125). */
+#define VSDMO_COLOR_ROUNDS 0x80000000u
 #define VSDMO_COLOR_REFERENCE 0xFFFFFFFFu
 VSDMO_API vsdmo_status vsdmo_mesh_create(int elem_type, const float* xyz, int n_vertices,
                                          const int32_t* elems, int n_elems, int mem_space,

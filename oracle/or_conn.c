@@ -32,10 +32,12 @@
  * Colouring: the reference's live path calls the closed cusparseScsrcolor
  * (mesh/VertexColoring.cu:128-153), whose result cannot be restated. The build uses the
  * reference's own Jones-Plassmann-Luby round rule (k_color_jpl_kernel, VertexColoring.cu:76-105:
- * an uncoloured vertex takes colour c iff its priority beats every neighbour that is uncoloured
- * or already has colour c) with priorities from a seeded 32-bit bijective hash instead of the
- * index-based priorities of VertexColoring.cu:54-72/107-125 (those make every round colour a
- * single vertex on structured meshes, i.e. one colour per vertex).
+ * an uncoloured vertex is coloured in round c iff its priority beats every neighbour that is
+ * uncoloured or coloured in round c) with priorities from a seeded 32-bit bijective hash instead
+ * of the index-based priorities of VertexColoring.cu:54-72/107-125 (those make every round colour
+ * a single vertex on structured meshes, i.e. one colour per vertex); by default the vertex takes
+ * the smallest colour its coloured neighbours do not have, with OR_COLOR_ROUNDS in the seed (and
+ * with OR_COLOR_REFERENCE) the round itself, as the reference does.
  */
 #include "vsdmo_oracle.h"
 #include <stdlib.h>
@@ -80,33 +82,58 @@ uint32_t or_priority(uint32_t i, uint32_t seed) {
     return h;
 }
 
+/* Round c colours every uncoloured vertex whose priority beats all its neighbours that are
+ * uncoloured or coloured in round c (rnd: the round of each vertex, -1 before). The colour is c
+ * (round colours: OR_COLOR_REFERENCE and OR_COLOR_ROUNDS seeds) or, by default, the smallest
+ * colour that none of the vertex's coloured neighbours has (all of them have higher priorities),
+ * i.e. the greedy colouring in priority order. Returns the number of colours. */
 int or_color_jpl(int n, const int32_t* rowptr, const int32_t* col, uint32_t seed, int32_t* colors) {
     uint32_t* pr = (uint32_t*)xc((size_t)n, sizeof(uint32_t));
     uint8_t* win = (uint8_t*)xc((size_t)n, 1);
+    int* rnd = (int*)xc((size_t)n, sizeof(int));
+    const int first_fit = seed != OR_COLOR_REFERENCE && !(seed & OR_COLOR_ROUNDS);
     for (int i = 0; i < n; ++i) {
         /* OR_COLOR_REFERENCE: the reference's priorities randoms[i] = n - i (VertexColoring.cu:112) */
-        pr[i] = seed == OR_COLOR_REFERENCE ? (uint32_t)(n - i) : or_priority((uint32_t)i, seed);
+        pr[i] = seed == OR_COLOR_REFERENCE ? (uint32_t)(n - i) : or_priority((uint32_t)i, seed & ~OR_COLOR_ROUNDS);
         colors[i] = -1;
+        rnd[i] = -1;
     }
-    int left = n, c = 0;
+    int left = n, c = 0, ncol = 0;
     while (left > 0) {
         for (int i = 0; i < n; ++i) {
             win[i] = 0;
-            if (colors[i] != -1) continue;
+            if (rnd[i] != -1) continue;
             int f = 1;
             for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
                 int j = col[e];
-                int jc = colors[j];
-                if ((jc != -1 && jc != c) || i == j) continue;
+                int jr = rnd[j];
+                if ((jr != -1 && jr != c) || i == j) continue;
                 if (pr[i] <= pr[j]) { f = 0; break; }
             }
             win[i] = (uint8_t)f;
         }
-        for (int i = 0; i < n; ++i) if (win[i]) { colors[i] = c; --left; }
+        for (int i = 0; i < n; ++i) {
+            if (!win[i]) continue;
+            int colour = c;
+            if (first_fit) {
+                for (colour = 0;; ++colour) {
+                    int taken = 0;
+                    for (int e = rowptr[i]; e < rowptr[i + 1] && !taken; ++e) {
+                        int j = col[e];
+                        taken = j != i && rnd[j] != -1 && rnd[j] != c && colors[j] == colour;
+                    }
+                    if (!taken) break;
+                }
+            }
+            colors[i] = colour;
+            if (colour + 1 > ncol) ncol = colour + 1;
+            --left;
+        }
+        for (int i = 0; i < n; ++i) if (win[i]) rnd[i] = c;
         ++c;
     }
-    free(pr); free(win);
-    return c;
+    free(pr); free(win); free(rnd);
+    return first_fit ? ncol : c;
 }
 
 /* stable order (new -> old) putting elements with flag == first_value first */

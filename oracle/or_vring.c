@@ -110,7 +110,15 @@ double or__vring64_extent(const or_mesh* m, const double* X, int v) {
     return me;
 }
 
-/* decision margin of a comparison of two ring values: an exact tie in double is structural (the
- * ring minimum of both is a part that does not depend on the candidate -- a halfhex's constant
- * sub-tets, or 0), and the f32 keys tie exactly too, so it decides nothing */
-double or__gap64(double a, double b) { return a == b ? DBL_MAX : fabs(a - b); }
+/* decision margin of a comparison of two ring values: under the shape metrics an exact tie in
+ * double is structural (the ring minimum of both is a part that does not depend on the candidate
+ * -- a halfhex's constant sub-tets, or 0), and the f32 keys tie exactly too, so it decides
+ * nothing. Under the angle criteria an exact tie is not safe: the dihedral angle at a ring edge
+ * that lies on the line a boundary vertex slides along is constant along the line, but its float
+ * evaluations at two positions differ in the last bits, so the float search can decide either
+ * way -- such a comparison has no margin. */
+double or__gap64(double a, double b) {
+    if (a != b) return fabs(a - b);
+    const int c = or__criterion();
+    return c == OR_MIN_ANGLE || c == OR_MAX_ANGLE ? 0.0 : DBL_MAX;
+}

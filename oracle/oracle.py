@@ -16,8 +16,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
 TRI, QUAD, TET, HEX = 0, 1, 2, 3
-# color_seed value selecting the reference's JPL priorities n - i (OR_COLOR_REFERENCE)
+# color_seed value selecting the reference's JPL priorities n - i (OR_COLOR_REFERENCE); the flag
+# COLOR_ROUNDS in a seed selects round colours (the reference's rule) with that seed's hashed
+# priorities instead of the default smallest free colour (OR_COLOR_ROUNDS)
 COLOR_REFERENCE = 0xFFFFFFFF
+COLOR_ROUNDS = 0x80000000
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -602,10 +605,11 @@ def element_metric_f64(fn, crit, pts, nrm=None):
 # ---- the reference's own mesh build and DMO (oracle/_ref/libref_vsdmo.so) --------------------
 # Built by ``make ref`` from the reference's mesh/ and dmo/ sources as they lie (ref_vsdmo.cu,
 # ref_prelude_vsdmo.h); it runs on the GPU. Colouring: the reference's color_jpl (priorities
-# n - i) stands in for its closed cusparseScsrcolor, unless COLOURING_CUSPARSE (the closed one)
-# or COLOURING_HASHED (the reference's JPL rounds with the library's hashed priorities) is asked.
+# n - i) stands in for its closed cusparseScsrcolor, unless COLOURING_CUSPARSE (the closed one),
+# COLOURING_HASHED (the reference's JPL rounds with the library's hashed priorities) or
+# COLOURING_FIRST_FIT (the library's default colouring of those priorities) is asked.
 REFVS_LIB_PATH = os.path.join(HERE, "_ref", "libref_vsdmo.so")
-COLOURING_JPL, COLOURING_CUSPARSE, COLOURING_HASHED = 0, 1, 2
+COLOURING_JPL, COLOURING_CUSPARSE, COLOURING_HASHED, COLOURING_FIRST_FIT = 0, 1, 2, 3
 _refvs = None
 
 

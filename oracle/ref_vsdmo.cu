@@ -42,9 +42,11 @@
 #include "dmo/DMOTriImplCub.h"
 #include "dmo/DMOQuadImplCub.h"
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <sstream>
+#include <vector>
 
 void refvs_cusparse_colouring(int nVertices, int* rowPtr, int* colInd, device_vector<int>& colors, int nnz);
 // the reference's JPL round kernel (mesh/VertexColoring.cu:76-105), defined there
@@ -53,7 +55,8 @@ __global__ void k_color_jpl_kernel(int start, int nVertices, int c, int* rowPtr,
 
 namespace {
 // 0: the reference's color_jpl (priorities n - i); 1: cusparseScsrcolor; 2: the reference's JPL
-// rounds with the library's hashed priorities (seed g_seed)
+// rounds with the library's hashed priorities (seed g_seed); 3: the library's default colouring
+// with those priorities (the smallest colour free among the higher-priority neighbours)
 int g_colouring = 0;
 uint32_t g_seed = 1;
 
@@ -81,11 +84,37 @@ void jpl_with_priorities(int n, int* rowPtr, int* colInd, device_vector<int>& co
         if ((int)thrust::count(colors.begin(), colors.end(), -1) == 0) break;
     }
 }
+
+
+// The greedy colouring in descending priority order: each vertex takes the smallest colour that
+// none of its already coloured (higher-priority) neighbours has -- the colours the library's JPL
+// rounds assign by default, computed here sequentially on the host.
+void first_fit_with_priorities(int n, int* rowPtr, int* colInd, device_vector<int>& colors, int nnz) {
+    std::vector<int> rp(n + 1), ci(std::max(nnz, 1)), order(n), col(n, -1);
+    gpuErrchk(cudaMemcpy(rp.data(), rowPtr, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    if (nnz > 0) gpuErrchk(cudaMemcpy(ci.data(), colInd, sizeof(int) * nnz, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> pr(n);
+    for (int i = 0; i < n; ++i) { pr[i] = hashed_priority((uint32_t)i, g_seed); order[i] = i; }
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return pr[a] > pr[b]; });
+    std::vector<char> used;
+    for (int i : order) {
+        used.assign((size_t)(rp[i + 1] - rp[i]) + 2, 0);
+        for (int e = rp[i]; e < rp[i + 1]; ++e) {
+            const int j = ci[e];
+            if (j != i && col[j] >= 0 && col[j] < (int)used.size()) used[col[j]] = 1;
+        }
+        int c = 0;
+        while (used[c]) ++c;
+        col[i] = c;
+    }
+    thrust::copy(col.begin(), col.end(), colors.begin());
+}
 }  // namespace
 
 void color_cuSPARSE(int nVertices, int* rowPtr, int* colInd, device_vector<int>& colors, int nnz) {
     if (g_colouring == 1) refvs_cusparse_colouring(nVertices, rowPtr, colInd, colors, nnz);
     else if (g_colouring == 2) jpl_with_priorities(nVertices, rowPtr, colInd, colors);
+    else if (g_colouring == 3) first_fit_with_priorities(nVertices, rowPtr, colInd, colors, nnz);
     else color_jpl(0, nVertices, rowPtr, colInd, colors);
 }
 
@@ -198,7 +227,8 @@ long copy_flags(void* out, const bool* dev, long n) {  // bool -> uint8
 extern "C" {
 
 /* 0: colour with the reference's color_jpl (default); 1: with cusparseScsrcolor; 2: with the
- * reference's JPL rounds and the library's hashed priorities of color_seed `seed`. */
+ * reference's JPL rounds and the library's hashed priorities of color_seed `seed`; 3: with the
+ * library's default colouring for that seed (the greedy colouring in priority order). */
 void refvs_set_colouring(int mode, uint32_t seed) {
     g_colouring = mode;
     g_seed = seed;

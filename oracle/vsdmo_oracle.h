@@ -72,9 +72,12 @@ int      or_mesh_info(const or_mesh* m, int which);
 long     or_mesh_array_len(const or_mesh* m, int id);          /* elements of the array   */
 int      or_mesh_array(const or_mesh* m, int id, void* out);    /* copies; 0 on success    */
 
-/* JPL colouring of a CSR graph with the seeded priorities, or with the reference's priorities
- * n - i when seed == OR_COLOR_REFERENCE; returns number of colours. */
+/* JPL colouring of a CSR graph: the smallest colour free among the coloured neighbours with the
+ * seeded priorities (default), the round as colour with OR_COLOR_ROUNDS in the seed, or the
+ * round with the reference's priorities n - i when seed == OR_COLOR_REFERENCE; returns the
+ * number of colours. */
 #define OR_COLOR_REFERENCE 0xFFFFFFFFu
+#define OR_COLOR_ROUNDS 0x80000000u
 int      or_color_jpl(int n, const int32_t* rowptr, const int32_t* col, uint32_t seed, int32_t* colors);
 uint32_t or_priority(uint32_t i, uint32_t seed);
 

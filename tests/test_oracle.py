@@ -153,19 +153,31 @@ def test_jpl_is_order_independent_and_valid(oracle_mod):
         rowptr[a + 1] += 1
     rowptr = np.cumsum(rowptr).astype(np.int32)
     col = np.array([b for _, b in pairs], np.int32)
-    c, nc = oracle_mod.color_jpl(rowptr, col, seed=7)
+    pr = np.array([oracle_mod.lib().or_priority(i, 7) for i in range(n)], dtype=np.uint64)
+    # round colours (COLOR_ROUNDS, the reference's rule): v was passed over in every round
+    # k < colour(v) because a neighbour still competing in that round (colour >= k) had a higher
+    # priority, and in its own round it beat every competitor
+    c, nc = oracle_mod.color_jpl(rowptr, col, seed=7 | oracle_mod.COLOR_ROUNDS)
     assert c.min() == 0 and c.max() == nc - 1
     for a, b in pairs:
         assert c[a] != c[b]
-    # JPL round rule: v was passed over in every round k < colour(v) because a neighbour
-    # still competing in that round (colour >= k) had a higher priority
-    pr = np.array([oracle_mod.lib().or_priority(i, 7) for i in range(n)], dtype=np.uint64)
     for v in range(n):
         nb = col[rowptr[v]:rowptr[v + 1]]
         for k in range(c[v]):
             assert any(c[u] >= k and pr[u] > pr[v] for u in nb)
-        # and in its own round it beat every competitor
         assert all(pr[v] > pr[u] for u in nb if c[u] >= c[v])
+    rounds = c
+    # default colours: the greedy colouring in descending priority order -- each vertex has the
+    # smallest colour that none of its higher-priority neighbours has -- with no more colours
+    # than the rounds
+    c, nc = oracle_mod.color_jpl(rowptr, col, seed=7)
+    assert c.min() == 0 and c.max() == nc - 1 and nc <= rounds.max() + 1
+    for a, b in pairs:
+        assert c[a] != c[b]
+    for v in range(n):
+        nb = col[rowptr[v]:rowptr[v + 1]]
+        taken = {int(c[u]) for u in nb if pr[u] > pr[v]}
+        assert c[v] == min(set(range(len(nb) + 1)) - taken)
 
 
 # ---- golden fixtures ------------------------------------------------------------------------------

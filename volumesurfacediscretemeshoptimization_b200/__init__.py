@@ -37,7 +37,7 @@ __all__ = ["QualityCriterium", "DMOMeshTri", "DMOMeshQuad", "DMOMeshTet", "DMOMe
            "DMOMeshQuadFactory", "DMOMeshTetFactory", "DMOMeshHexFactory", "DMOTetClass", "DMOHexClass",
            "DMOTriFlatClass", "DMOTriClass", "DMOQuadClass", "DMOQuadFlatClass", "BatchDMO", "ProposalModel",
            "VSDMOError", "Params", "default_params", "version", "read_mesh_file", "write_mesh_file",
-           "COLOR_REFERENCE"]
+           "COLOR_REFERENCE", "COLOR_ROUNDS"]
 
 A_XYZ, A_NEW_OF_OLD, A_ELEMS, A_SURF_TRIS, A_HE_ROWPTR, A_HALFEDGES, A_HF_ROWPTR, A_HALFFACES, \
     A_COL_FREE, A_COL_FEATURE, A_COL_INNER, A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D, \
@@ -52,8 +52,11 @@ _F32 = {A_XYZ, A_FACE_NORMALS, A_VERTEX_NORMALS}
 _U8 = {A_IS_BOUNDARY1D, A_IS_FEATURE, A_IS_BOUNDARY2D}
 I_ELEM_TYPE = 12
 # color_seed value selecting the reference's own JPL priorities n - i (VSDMO_COLOR_REFERENCE)
-# instead of the seeded hash; the reference's mesh/VertexColoring.cu:107-125
+# instead of the seeded hash; the reference's mesh/VertexColoring.cu:107-125. COLOR_ROUNDS | seed
+# (VSDMO_COLOR_ROUNDS) keeps the hashed priorities but colours by JPL round like the reference,
+# instead of the default smallest colour free among the higher-priority neighbours.
 COLOR_REFERENCE = 0xFFFFFFFF
+COLOR_ROUNDS = 0x80000000
 INFO_NAMES = ["nV", "nE", "nSurf", "nFeature", "nTris", "nHE", "nColorsFree", "nColorsFeature",
               "nColorsInner", "maxNumHalfedges", "maxNumTetrahedra", "isFlat"]
 

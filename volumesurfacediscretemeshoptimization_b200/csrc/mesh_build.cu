@@ -19,8 +19,12 @@
 //   * boundary / feature flags (dihedral > 20 deg, mesh/MeshGPUCommon.cu:466-495) and face /
 //     vertex normals (:363-434).
 // Sorting uses the stable LSD radix sort of prim.cu. Colouring runs the reference's JPL round
-// rule (mesh/VertexColoring.cu:76-105) with seeded hash priorities, or with the reference's own
-// priorities n - i (VertexColoring.cu:107-125) when the seed is VSDMO_COLOR_REFERENCE.
+// rule (mesh/VertexColoring.cu:76-105): by default with seeded hash priorities, each vertex
+// taking the smallest colour none of its higher-priority neighbours has (the greedy colouring in
+// priority order, computed round by round); with VSDMO_COLOR_ROUNDS in the seed the colour is the
+// round (the reference's rule) with the hashed priorities of the seed's other bits; with
+// VSDMO_COLOR_REFERENCE the colour is the round and the priorities are the reference's own n - i
+// (VertexColoring.cu:107-125).
 #include "vsdmo_internal.cuh"
 #include <climits>
 #include <cmath>
@@ -34,6 +38,7 @@ enum BuildErr { BE_OK = 0, BE_INDEX = 1, BE_NAN = 2, BE_DEGENERATE = 3, BE_NONMA
 // n: the number of vertices coloured together (i is local to them)
 __device__ __forceinline__ uint32_t priority(uint32_t i, uint32_t seed, uint32_t n) {
     if (seed == VSDMO_COLOR_REFERENCE) return n - i;
+    seed &= ~VSDMO_COLOR_ROUNDS;
     uint32_t h = i + seed * 0x9E3779B9u;
     h ^= h >> 16; h *= 0x85EBCA6Bu;
     h ^= h >> 13; h *= 0xC2B2AE35u;
@@ -325,22 +330,59 @@ __global__ void k_quad_edge_pairs(const int* quads, int nQ, int lo, int num, uin
 // ---- JPL colouring ---------------------------------------------------------------------------
 __global__ void k_fill_int(int* a, long n, int v) { GRID_STRIDE(i, n) a[i] = v; }
 
+// One JPL round c: an uncoloured vertex is coloured iff its priority beats every neighbour that
+// is uncoloured or coloured in this round (rnd: the round each vertex was coloured in, -1 before).
+// Its colour is c (round colours), or with first_fit the smallest colour none of its coloured
+// neighbours has: those all have higher priorities and earlier rounds (two neighbours are never
+// coloured in the same round), so the colours are the greedy colouring in priority order.
 // prev: the previous round's count of uncoloured vertices in the same host read (null for the
-// first round of one); when it is 0 every vertex has its colour and the round has nothing to do
-__global__ void k_jpl_round(int n, const int* rowptr, const int* col, uint32_t seed, int c, int* colors, int* remaining,
-                            const int* prev) {
+// first round of one); when it is 0 every vertex has its colour and the round has nothing to do.
+// maxc collects the largest first-fit colour.
+__global__ void k_jpl_round(int n, const int* rowptr, const int* col, uint32_t seed, int c, int first_fit, int* colors,
+                            int* rnd, int* remaining, const int* prev, int* maxc) {
     if (prev && *prev == 0) return;
     GRID_STRIDE(i, n) {
-        if (colors[i] != -1) continue;
-        uint32_t pi = priority((uint32_t)i, seed, (uint32_t)n);
+        if (rnd[i] != -1) continue;
+        const uint32_t pi = priority((uint32_t)i, seed, (uint32_t)n);
         bool f = true;
         for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
-            int j = col[e];
-            int jc = colors[j];
-            if ((jc != -1 && jc != c) || (int)i == j) continue;
+            const int j = col[e];
+            const int jr = rnd[j];
+            if ((jr != -1 && jr != c) || (int)i == j) continue;
             if (pi <= priority((uint32_t)j, seed, (uint32_t)n)) { f = false; break; }
         }
-        if (f) colors[i] = c; else atomicAdd(remaining, 1);
+        if (!f) {
+            atomicAdd(remaining, 1);
+            continue;
+        }
+        int colour = c;
+        if (first_fit) {
+            // smallest colour not taken by a neighbour coloured in an earlier round
+            unsigned long long used = 0ull;
+            for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+                const int j = col[e];
+                const int jr = rnd[j];
+                if (jr == -1 || jr == c || (int)i == j) continue;
+                const int cj = colors[j];
+                if (cj < 64) used |= 1ull << cj;
+            }
+            if (~used) {
+                colour = __ffsll((long long)~used) - 1;
+            } else {
+                for (colour = 64;; ++colour) {
+                    bool taken = false;
+                    for (int e = rowptr[i]; e < rowptr[i + 1] && !taken; ++e) {
+                        const int j = col[e];
+                        const int jr = rnd[j];
+                        taken = jr != -1 && jr != c && (int)i != j && colors[j] == colour;
+                    }
+                    if (!taken) break;
+                }
+            }
+            atomicMax(maxc, colour);
+        }
+        colors[i] = colour;
+        rnd[i] = c;
     }
 }
 
@@ -602,25 +644,32 @@ struct Builder {
             col.alloc(1, s);
         }
         // JPL rounds, CH per host read: round c leaves remaining[c % CH] uncoloured vertices; the
-        // rounds after the last one find nobody uncoloured and change nothing
+        // rounds after the last one find nobody uncoloured and change nothing; remaining[CH]
+        // collects the largest first-fit colour
         constexpr int CH = 16;
-        DBuf<int> colors(num, s), remaining(CH, s);
-        k_fill_int<<<G(num), 256, 0, s>>>(colors.p, num, -1);
+        const int first_fit = m.seed != VSDMO_COLOR_REFERENCE && !(m.seed & VSDMO_COLOR_ROUNDS) ? 1 : 0;
+        DBuf<int> colors(num, s), rnd(num, s), remaining(CH + 1, s);
+        k_fill_int<<<G(num), 256, 0, s>>>(rnd.p, num, -1);
         VSDMO_CHECK_LAUNCH();
+        remaining.zero();
         int nc = -1;
+        std::vector<int> left;
         for (int c0 = 0; nc < 0; c0 += CH) {
             if (c0 > num + 1) throw Error(VSDMO_E_CUDA, "colouring did not terminate");
-            remaining.zero();
+            VSDMO_CUDA(cudaMemsetAsync(remaining.p, 0, sizeof(int) * CH, s));
             for (int i = 0; i < CH; ++i) {
-                k_jpl_round<<<G(num), 256, 0, s>>>(num, rowptr.p, col.p, m.seed, c0 + i, colors.p, remaining.p + i,
-                                                   i > 0 ? remaining.p + i - 1 : nullptr);
+                k_jpl_round<<<G(num), 256, 0, s>>>(num, rowptr.p, col.p, m.seed, c0 + i, first_fit, colors.p, rnd.p,
+                                                   remaining.p + i, i > 0 ? remaining.p + i - 1 : nullptr,
+                                                   remaining.p + CH);
                 VSDMO_CHECK_LAUNCH();
             }
-            const std::vector<int> left = remaining.to_host();
+            left = remaining.to_host();
             for (int i = 0; i < CH && nc < 0; ++i)
                 if (left[i] == 0) nc = c0 + i + 1;
         }
-        // JPL colours are dense: every round colours the top-priority vertex left
+        if (first_fit) nc = left[CH] + 1;
+        // the colours are dense: every round colours the top-priority vertex left, and a
+        // first-fit colour k has neighbours of every colour below k
         // stable sort of the range by colour
         DBuf<uint32_t> ck(num, s), order(num, s);
         VSDMO_CUDA(cudaMemcpyAsync(ck.p, colors.p, sizeof(int) * num, cudaMemcpyDeviceToDevice, s));
