@@ -179,7 +179,7 @@ def test_learned_mode_monotone_and_gain(vsdmo):
         mesh = vsdmo.DMOMeshTet(xyz, tets)
         opt = vsdmo.DMOTetClass(mesh, n_iter=6)
         q0 = opt.getQuality()
-        opt.set_model(model, 4, 2)
+        opt.set_model(model, 4, 2, 0.012)
         opt.optimize()
         mn, mean = opt.history()
         assert np.all(np.diff(mn) >= -1e-6)          # the fallback keeps the minimum monotone
@@ -199,7 +199,7 @@ def test_learned_proposals_once_per_iteration(vsdmo):
     mesh = vsdmo.DMOMeshTet(xyz, tets)
     opt = vsdmo.DMOTetClass(mesh, n_iter=5)
     q0 = opt.getQuality()
-    opt.set_model(trained, 4, 2)
+    opt.set_model(trained, 4, 2, 0.012)
     opt.set_proposal_schedule(2)          # iterations 0, 1 per colour class, then once
     opt.optimize()
     mn, mean = opt.history()
@@ -209,7 +209,7 @@ def test_learned_proposals_once_per_iteration(vsdmo):
     assert acc + fb == 5 * (mesh.info["nV"] - mesh.info["nSurf"]) and acc > fb
     # the whole run with one launch per iteration
     opt2 = vsdmo.DMOTetClass(vsdmo.DMOMeshTet(xyz, tets), n_iter=1)
-    opt2.set_model(trained, 4, 2)
+    opt2.set_model(trained, 4, 2, 0.012)
     opt2.set_proposal_schedule(0)
     opt2.iterate(1)
     assert opt2.learned_counters()[0] > 0

@@ -446,7 +446,7 @@ class DMOTetClass(_DMOBase):
                                                   capacity, C.byref(n)))
         return n.value
 
-    def set_model(self, model, reduced_n: int = 4, reduced_depth: int = 2, reduced_scale: float = 0.012):
+    def set_model(self, model, reduced_n: int = 4, reduced_depth: int = 1, reduced_scale: float = 0.0175):
         """Learned mode: reduced grid around the model's proposal, plain search as fallback."""
         check(_capi.lib().vsdmo_opt_set_model(self.h, model.h if model is not None else None, reduced_n, reduced_depth,
                                               reduced_scale))

@@ -10,9 +10,10 @@ from __future__ import annotations
 import time
 
 # training and reduced-search settings used for the 100^3 tet cube measurements: one level of
-# 4^3 candidates at 0.02 of the plain search's first extent (measured against 1-3 levels, 3^3-5^3
-# candidates and scales 0.008-0.04 on that cube: the fewest milliseconds to plain's final minimum)
-DEFAULTS = {"reduced_n": 4, "reduced_depth": 1, "reduced_scale": 0.02,
+# 4^3 candidates at 0.0175 of the plain search's first extent (measured against 1-3 levels,
+# 3^3-5^3 candidates and scales 0.008-0.05 on that cube and on the same cube jittered with
+# another seed: the fewest milliseconds to plain's final minimum on both)
+DEFAULTS = {"reduced_n": 4, "reduced_depth": 1, "reduced_scale": 0.0175,
             "train_steps": (20000, 6000), "train_lr": (1e-3, 2e-4), "batch": 8192,
             "pairs_mesh": "tet cube 48^3, jitter 0.3h", "pairs_seed": 1000, "pairs_iterations": 20}
 
