@@ -330,8 +330,8 @@ def run_ours(args):
         prof = json.load(open(os.path.join(ROOT, "profiles", "dmo_tet_config2_traffic.json")))
     except Exception:
         pass
-    # k_dmo_tet's share of an iteration's device time (33 colour launches + 1 quality reduction),
-    # from the ncu launch list of this bench (profiles/launches_bench_config2.md)
+    # k_dmo_tet's share of an iteration's device time (one launch per colour class + the quality
+    # reduction), from the ncu launch list of profile_cases.py tet (profiles/k_dmo_tet_config2.md)
     share = prof.get("share_of_iteration", 0.988)
     kern_ms_step = iter_ms * share
     launches_step = n_col * N_ITER
