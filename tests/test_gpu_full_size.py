@@ -1,4 +1,4 @@
-"""The full-size benchmark workloads against the FP64 oracle.
+"""The full-size benchmark workloads against the FP64 oracle (final minimum and mean within 1e-4).
 
 tests/golden/full_size_fp64.json holds the FP64 restatement's minimum and mean element quality
 after every iteration of each workload (generated by tests/golden/make_full_size.py on the CPU:
@@ -13,10 +13,10 @@ config 2 alone is about 8 CPU-minutes). The library runs the same workload on th
 
 The final mean is within 1e-4 of the FP64 run on every workload, and so is the final minimum
 except on config 2: there every FP32 implementation of the search drifts from the FP64
-trajectory once near-tie decisions compound (all agree within 1e-5 through iteration 4; after 20
-iterations the library's minimum is 6.8e-4 below the FP64 one and the reference's own FP32
-kernel, run on the same colour classes, 4.0e-4 below), so its minimum is held to 1e-4 through
-iteration 4 and to 1e-3 at the end. On config 2 the first iteration is also compared vertex by
+trajectory once near-tie decisions compound (the oracle's float restatement, bitwise equal to
+the library, is within 1e-6 of FP64 through iteration 5, up to 3.1e-3 off at iteration 7 and
+4.4e-4 below it after 20; the mean stays within 8e-6 throughout), so its minimum is held to 1e-4
+through iteration 4 and to 1e-3 at the end. On config 2 the first iteration is also compared vertex by
 vertex, colour by colour from the same state: positions within 1e-5 h wherever the FP64
 decision margin exceeds 1e-5.
 """
