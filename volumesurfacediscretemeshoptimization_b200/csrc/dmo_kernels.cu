@@ -719,6 +719,7 @@ k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
     __shared__ float s_k[HEX_THREADS / 32];
     __shared__ int s_i[HEX_THREADS / 32];
     __shared__ float s_win[3];
+    __shared__ float s_qlast;
     __shared__ int s_czero;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int v = v0 + blockIdx.x;
@@ -781,7 +782,11 @@ k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
     float qWin = -FLT_MAX;
     for (int level = 0; level < depth; ++level) {
         const float Sx = ds * sx, Sy = ds * sy, Sz = ds * sz;
-        const float qLast = hex_key1(co, k, dx, dy, dz, es, ea);
+        // the key at the current position: one warp computes it while the others search
+        if (w == 0) {
+            const float q = hex_key1(co, k, dx, dy, dz, es, ea);
+            if (lane == 0) s_qlast = q;
+        }
         const float z = fmaf(grid_offset(ck), Sz, dz);
         const float y = fmaf(grid_offset(cj), Sy, dy);
         float x[4], t1x[4], t3x[4];
@@ -838,13 +843,12 @@ k_dmo_hex(float4* __restrict__ pos, const int* __restrict__ rowptr, const int4* 
             if (s_k[i] > bk || (s_k[i] == bk && s_i[i] < bi)) { bk = s_k[i]; bi = s_i[i]; }
         if (t == bi) { s_win[0] = pX; s_win[1] = pY; s_win[2] = pZ; }
         __syncthreads();
-        if (qLast < bk) { dx = s_win[0]; dy = s_win[1]; dz = s_win[2]; }
+        if (s_qlast < bk) { dx = s_win[0]; dy = s_win[1]; dz = s_win[2]; }
         qWin = bk;
         ds = ds * (2.0f / 7.0f);
         __syncthreads();   // s_k / s_win are rewritten by the next level
     }
-    const float qOld = hex_key1(co, k, 0.f, 0.f, 0.f, es, ea);
-    if (t == 0 && qOld < qWin) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
+    if (t == 0 && hex_key1(co, k, 0.f, 0.f, 0.f, es, ea) < qWin) pos[v] = tet_unscale(c0, dx, dy, dz, ex);
 }
 
 // ---- flat triangles ---------------------------------------------------------------------------
