@@ -36,7 +36,7 @@ def _rank_main(rank, world, port, out):
     t0 = time.perf_counter()
     for v0, v1 in om.color_ranges():
         x = om.dmo_color_f32(x, v0, v1, nthreads=1)
-    ms = (time.perf_counter() - t0) * 1e3 + 10.0 * r       # rank 1 made the slower one
+    ms = (time.perf_counter() - t0) * 1e3 + 1000.0 * r     # rank 1 made the slower one, whatever the load
     replicas.barrier(dist)
     ms_max = replicas.max_over_ranks(ms, dist)
     n_inner = om.info["nV"] - om.info["nSurf"]
