@@ -221,8 +221,17 @@ __device__ __forceinline__ void tet_critical(const float4* __restrict__ co, int 
 }
 
 // the lane's 16 candidates (fixed x, y[2], z[8]) over the critical tets: bit jj * 8 + q set when
-// the candidate survives (its key over the subset is not below thr)
-__device__ __forceinline__ unsigned tet_filter(const float4* __restrict__ co, const int (&crit)[TET_CRIT], int m,
+// the candidate survives (its key over the subset is not below thr). Used when thr <= 0 (the
+// ring has an inverted tet, whose key is its det); tet_filter_pos covers thr > 0.
+#ifndef TET_FILTER_NEG_INLINE
+#define TET_FILTER_NEG_INLINE 1
+#endif
+#if TET_FILTER_NEG_INLINE
+__device__ __forceinline__
+#else
+__device__ __noinline__
+#endif
+unsigned tet_filter(const float4* __restrict__ co, const int (&crit)[TET_CRIT], int m,
                                                float x, const float* y, const float* z, const float* tz, float thr) {
     const float tx = (3.0f * x) * x;
     const float ty[2] = { (3.0f * y[0]) * y[0], (3.0f * y[1]) * y[1] };
@@ -257,6 +266,48 @@ __device__ __forceinline__ unsigned tet_filter(const float4* __restrict__ co, co
             const bool below = dm[jj][q] < 0.f ? dm[jj][q] < thr : N[jj][q] < thr * D[jj][q];
             if (!below) alive |= 1u << (jj * 8 + q);
         }
+    return alive;
+}
+
+// thr > 0: a candidate survives when every critical tet has det > 0 and det^2 >= thr L^3, tested
+// as min over the tets of min(det, det^2 - thr L^3) > 0 -- one running minimum instead of a
+// fraction and a det. det, det^2 and L^3 are the values the fraction would be formed from, and
+// the fma rounds det^2 - thr L^3 once, so a tet whose key det^2 / L^3 is at least the current
+// key (thr lies 2^-14 of it lower) gives a positive value: every candidate that can beat the
+// current key survives.
+__device__ __forceinline__ unsigned tet_filter_pos(const float4* __restrict__ co, const int (&crit)[TET_CRIT], int m,
+                                                   float x, const float* y, const float* z, const float* tz,
+                                                   float thr) {
+    const float tx = (3.0f * x) * x;
+    const float ty[2] = { (3.0f * y[0]) * y[0], (3.0f * y[1]) * y[1] };
+    float s[2][NQ];
+#pragma unroll
+    for (int r = 0; r < TET_CRIT; ++r) {
+        if (r >= m) break;
+        const int t = crit[r];
+        const float4 K0 = co[2 * t], K1 = co[2 * t + 1];
+        const float detA = fmaf(K0.x, x, K0.w);
+        const float LA = K1.w + fmaf(K1.x, x, tx);
+        float lz[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) lz[q] = fmaf(K1.z, z[q], tz[q]);
+#pragma unroll
+        for (int jj = 0; jj < 2; ++jj) {
+            const float detB = fmaf(K0.y, y[jj], detA), LB = LA + fmaf(K1.y, y[jj], ty[jj]);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const float det = fmaf(K0.z, z[q], detB), L = LB + lz[q];
+                const float v = fminf(det, fmaf(-thr, (L * L) * L, det * det));
+                s[jj][q] = r == 0 ? v : fminf(s[jj][q], v);
+            }
+        }
+    }
+    unsigned alive = 0;
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+            if (s[jj][q] > 0.f) alive |= 1u << (jj * 8 + q);
     return alive;
 }
 
@@ -354,7 +405,8 @@ __device__ __forceinline__ bool tet_plain_search(const float4* __restrict__ co, 
         int crit[TET_CRIT];
         tet_critical(co, k, dx, dy, dz, lane, crit);
         const float thr = qLast - (fabsf(qLast) * 0x1p-14f + 1e-37f);
-        const unsigned alive = tet_filter(co, crit, min(TET_CRIT, k), x, y, z, tz, thr);
+        const unsigned alive = thr > 0.f ? tet_filter_pos(co, crit, min(TET_CRIT, k), x, y, z, tz, thr)
+                                         : tet_filter(co, crit, min(TET_CRIT, k), x, y, z, tz, thr);
         const int cnt = __popc(alive);
         int incl = cnt;
 #pragma unroll
