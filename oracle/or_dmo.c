@@ -443,7 +443,11 @@ static void tet_vertex_f32(const or_mesh* m, float* X, int v, float gs) {
  * else det^2 / L^3) for the current position and the proposal, the ordered fraction minimum
  * (tet_key) for the grid candidates; the best candidate of a level (largest key, lowest index
  * on ties) becomes the centre when it beats the best so far. The vertex moves when the best
- * beats the key of its current position; otherwise it is queued for the plain search. */
+ * beats the key of its current position; otherwise it is queued for the plain search.
+ * With rn = 4 the candidates are ranked by the ordered fraction minimum over the 8 tets of
+ * smallest per-tet key at the level's centre (picked by the order key of the float with the
+ * tet index in its low 5 bits, ties to the lower tet), and the best-ranked candidate counts
+ * with its ring minimum of the per-tet keys. */
 static float tet_key_piecemin(int k, const float* K, float x, float y, float z) {
     const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
     float m = FLT_MAX;
@@ -454,6 +458,57 @@ static float tet_key_piecemin(int k, const float* K, float x, float y, float z) 
         m = fminf(m, det < 0.f ? det : (det * det) / ((L * L) * L));
     }
     return m;
+}
+
+#define LEARNED_CRIT 8
+
+static float tet_piece_key_at(const float* c, float x, float y, float z) {
+    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    const float det = fmaf(c[2], z, fmaf(c[1], y, fmaf(c[0], x, c[3])));
+    const float L = ((c[7] + fmaf(c[4], x, tx)) + fmaf(c[5], y, ty)) + fmaf(c[6], z, tz);
+    return det < 0.f ? det : (det * det) / ((L * L) * L);
+}
+
+/* float order as unsigned order, the low 5 bits replaced by t & 31 */
+static uint32_t tet_order_key(float key, int t) {
+    uint32_t b;
+    memcpy(&b, &key, sizeof b);
+    const uint32_t o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    return (o & ~31u) | (uint32_t)(t & 31);
+}
+
+/* the min(LEARNED_CRIT, k) tets of smallest (order key, tet) at (x, y, z) */
+static int learned_critical(int k, const float* K, float x, float y, float z, int* crit) {
+    const int nt = k < LEARNED_CRIT ? k : LEARNED_CRIT;
+    for (int r = 0; r < nt; ++r) {
+        uint32_t best = 0xffffffffu;
+        int bt = -1;
+        for (int t = 0; t < k; ++t) {
+            int used = 0;
+            for (int q = 0; q < r; ++q) used |= crit[q] == t;
+            if (used) continue;
+            const uint32_t kt = tet_order_key(tet_piece_key_at(K + 8 * t, x, y, z), t);
+            if (bt < 0 || kt < best) { best = kt; bt = t; }
+        }
+        crit[r] = bt;
+    }
+    return nt;
+}
+
+/* tet_key over the tets crit[0 .. nt) in that order */
+static float tet_key_subset(const int* crit, int nt, const float* K, float x, float y, float z) {
+    const float tx = (3.0f * x) * x, ty = (3.0f * y) * y, tz = (3.0f * z) * z;
+    float N = 0.f, D = 1.f, dmin = 0.f;
+    for (int r = 0; r < nt; ++r) {
+        const float* c = K + 8 * crit[r];
+        const float det = fmaf(c[2], z, fmaf(c[1], y, fmaf(c[0], x, c[3])));
+        const float L = ((c[7] + fmaf(c[4], x, tx)) + fmaf(c[5], y, ty)) + fmaf(c[6], z, tz);
+        const float n = det * det, d = (L * L) * L;
+        if (r == 0) { N = n; D = d; dmin = det; continue; }
+        if (n * D < N * d) { N = n; D = d; }
+        dmin = fminf(dmin, det);
+    }
+    return dmin < 0.f ? dmin : N / D;
 }
 
 static int tet_learned_vertex_f32(const or_mesh* m, float* X, int v, const float* yv, float gs, int rn, int rdepth,
@@ -493,12 +548,21 @@ static int tet_learned_vertex_f32(const or_mesh* m, float* X, int v, const float
         for (int level = 0; level < rdepth; ++level) {
             float bk = -FLT_MAX;
             int bi = -1;
+            int crit[LEARNED_CRIT], nt = 0;
+            if (rn == 4) nt = learned_critical(k, K, c[0], c[1], c[2], crit);
             for (int ci = 0; ci < nc; ++ci) {
                 const int ix = ci % rn, iy = (ci / rn) % rn, iz = ci / (rn * rn);
-                const float q = tet_key(k, K, fmaf((float)(rn - 1 - 2 * ix) / (float)(rn - 1), rr[0], c[0]),
-                                        fmaf((float)(rn - 1 - 2 * iy) / (float)(rn - 1), rr[1], c[1]),
-                                        fmaf((float)(rn - 1 - 2 * iz) / (float)(rn - 1), rr[2], c[2]));
+                const float x = fmaf((float)(rn - 1 - 2 * ix) / (float)(rn - 1), rr[0], c[0]);
+                const float y = fmaf((float)(rn - 1 - 2 * iy) / (float)(rn - 1), rr[1], c[1]);
+                const float z = fmaf((float)(rn - 1 - 2 * iz) / (float)(rn - 1), rr[2], c[2]);
+                const float q = rn == 4 ? tet_key_subset(crit, nt, K, x, y, z) : tet_key(k, K, x, y, z);
                 if (bi < 0 || q > bk) { bk = q; bi = ci; }
+            }
+            if (rn == 4 && bk > best) {
+                const int ix = bi % rn, iy = (bi / rn) % rn, iz = bi / (rn * rn);
+                bk = tet_key_piecemin(k, K, fmaf((float)(rn - 1 - 2 * ix) / (float)(rn - 1), rr[0], c[0]),
+                                      fmaf((float)(rn - 1 - 2 * iy) / (float)(rn - 1), rr[1], c[1]),
+                                      fmaf((float)(rn - 1 - 2 * iz) / (float)(rn - 1), rr[2], c[2]));
             }
             if (bk > best) {
                 const int ix = bi % rn, iy = (bi / rn) % rn, iz = bi / (rn * rn);

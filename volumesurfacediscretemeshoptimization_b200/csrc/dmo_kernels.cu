@@ -630,6 +630,43 @@ __global__ void k_tet_targets(const float4* __restrict__ pos, int v0, int v1, co
 }
 
 // offsets of the reduced grid with n points per axis: (n - 1 - 2i) / (n - 1)
+// The 4^3 reduced search ranks its candidates by the LEARNED_CRIT tets of smallest exact key
+// at the level's centre (ties to the lower tet), then judges the best-ranked one by its full
+// ring key: within the small grid around the proposal the ring minimum of a candidate almost
+// always sits in one of those tets, and a third of the ring costs a third of the search.
+constexpr int LEARNED_CRIT = 8;
+
+__device__ __forceinline__ void learned_critical(const float4* __restrict__ co, int k, float x, float y, float z,
+                                                 int lane, int (&crit)[LEARNED_CRIT]) {
+    if (k <= 32) {
+        unsigned mine = lane < k ? tet_order_key(tet_piece_key(co, lane, x, y, z), lane) : 0xffffffffu;
+#pragma unroll
+        for (int r = 0; r < LEARNED_CRIT; ++r) {
+            const unsigned m = __reduce_min_sync(FULL, mine);
+            const int t = (int)(m & 31u);
+            crit[r] = t < k ? t : 0;
+            if (lane == t) mine = 0xffffffffu;
+        }
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < LEARNED_CRIT; ++r) {
+        unsigned best = 0xffffffffu;
+        int bt = 0;
+        for (int t = lane; t < k; t += 32) {
+            bool used = false;
+#pragma unroll
+            for (int q = 0; q < r; ++q) used |= (crit[q] == t);
+            if (used) continue;
+            const unsigned kt = tet_order_key(tet_piece_key(co, t, x, y, z), t & 31);
+            if (kt < best || (kt == best && t < bt)) { best = kt; bt = t; }
+        }
+        const unsigned m = __reduce_min_sync(FULL, best);
+        const unsigned tt = __reduce_min_sync(FULL, best == m ? (unsigned)bt : 0xffffffffu);
+        crit[r] = tt < (unsigned)k ? (int)tt : 0;
+    }
+}
+
 __device__ __forceinline__ float reduced_offset(int i, int n) { return (float)(n - 1 - 2 * i) / (float)(n - 1); }
 
 // Learned search: the network's displacement y (units of mm) centres a reduced grid of
@@ -687,7 +724,8 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
             int bi = 1 << 30;
             if (rn == 4) {
                 // 64 candidates, index ix + 4 iy + 16 iz: lane (ix, iy, iz0) also takes iz0 + 2,
-                // sharing the x and y parts of every tet; offsets (3 - 2i) / 3
+                // sharing the x and y parts of every tet; offsets (3 - 2i) / 3; ranked over the
+                // critical tets of the centre
                 const int ix = lane & 3, iy = (lane >> 2) & 3, iz0 = lane >> 4;
                 const float o4[4] = { 1.0f, 1.0f / 3.0f, -1.0f / 3.0f, -1.0f };
                 const float x = fmaf(o4[ix], rx, cx);
@@ -696,14 +734,20 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
                 const float tx = (3.0f * x) * x, ty = (3.0f * yy) * yy;
                 const float tz0 = (3.0f * z0) * z0, tz1 = (3.0f * z1) * z1;
                 float N0 = 0.f, D0 = 1.f, m0 = 0.f, N1 = 0.f, D1 = 1.f, m1 = 0.f;
-                for (int t = 0; t < k; ++t) {
+                int crit[LEARNED_CRIT];
+                learned_critical(co, k, cx, cy, cz, lane, crit);
+                const int nt = min(LEARNED_CRIT, k);
+#pragma unroll
+                for (int r = 0; r < LEARNED_CRIT; ++r) {
+                    if (r >= nt) break;
+                    const int t = crit[r];
                     const float4 K0 = co[2 * t], K1 = co[2 * t + 1];
                     const float detB = fmaf(K0.y, yy, fmaf(K0.x, x, K0.w));
                     const float LB = (K1.w + fmaf(K1.x, x, tx)) + fmaf(K1.y, yy, ty);
                     const float d0 = fmaf(K0.z, z0, detB), L0 = LB + fmaf(K1.z, z0, tz0);
                     const float d1 = fmaf(K0.z, z1, detB), L1 = LB + fmaf(K1.z, z1, tz1);
                     const float n0 = d0 * d0, e0 = (L0 * L0) * L0, n1 = d1 * d1, e1 = (L1 * L1) * L1;
-                    if (t == 0) { N0 = n0; D0 = e0; m0 = d0; N1 = n1; D1 = e1; m1 = d1; continue; }
+                    if (r == 0) { N0 = n0; D0 = e0; m0 = d0; N1 = n1; D1 = e1; m1 = d1; continue; }
                     if (n0 * D0 < N0 * e0) { N0 = n0; D0 = e0; }
                     if (n1 * D1 < N1 * e1) { N1 = n1; D1 = e1; }
                     m0 = fminf(m0, d0); m1 = fminf(m1, d1);
@@ -722,6 +766,12 @@ k_dmo_tet_learned(float4* __restrict__ pos, const int* __restrict__ rowptr, cons
                 }
             }
             warp_argmax(bk, bi);
+            if (rn == 4 && bi < nc && bk > best) {
+                // the best-ranked candidate is judged by its full ring key
+                const int ix = bi % rn, iy = (bi / rn) % rn, iz = bi / (rn * rn);
+                bk = tet_key_min(co, k, fmaf(reduced_offset(ix, rn), rx, cx), fmaf(reduced_offset(iy, rn), ry, cy),
+                                 fmaf(reduced_offset(iz, rn), rz, cz), lane);
+            }
             if (bi < nc && bk > best) {
                 const int ix = bi % rn, iy = (bi / rn) % rn, iz = bi / (rn * rn);
                 const float nx = fmaf(reduced_offset(ix, rn), rx, cx);
