@@ -1196,8 +1196,12 @@ __device__ __forceinline__ float element_quality(const int* __restrict__ el, int
     return q_tri2d(pos[t[0]], pos[t[1]], pos[t[2]]);
 }
 
-constexpr int QS_BLOCKS = 296;
+// the element loop is a chain of dependent loads (indices, then corners), bound by how many of
+// them are in flight: four elements per thread, one resident grid (80 registers: 3 blocks of
+// 256 threads per SM)
+constexpr int QS_BLOCKS = 148 * 3;
 constexpr int QS_THREADS = 256;
+constexpr int QS_UNROLL = 4;
 
 __global__ void __launch_bounds__(QS_THREADS)
 k_quality_stats(const int* __restrict__ el, int kind, long nE, const float4* __restrict__ pos, IterStats* stats,
@@ -1212,7 +1216,20 @@ k_quality_stats(const int* __restrict__ el, int kind, long nE, const float4* __r
     float mn = FLT_MAX;
     double sm = 0.0;
     int fl = 0;
-    for (long e = (long)blockIdx.x * QS_THREADS + threadIdx.x; e < nE; e += (long)QS_BLOCKS * QS_THREADS) {
+    const long st = (long)QS_BLOCKS * QS_THREADS;
+    long e = (long)blockIdx.x * QS_THREADS + threadIdx.x;
+    for (; e + (QS_UNROLL - 1) * st < nE; e += QS_UNROLL * st) {
+        float q[QS_UNROLL];
+#pragma unroll
+        for (int j = 0; j < QS_UNROLL; ++j) q[j] = element_quality(el, kind, pos, e + j * st);
+#pragma unroll
+        for (int j = 0; j < QS_UNROLL; ++j) {
+            mn = fminf(mn, q[j]);
+            sm += (double)q[j];
+            if (check && q[j] < lastMin - tol) ++fl;
+        }
+    }
+    for (; e < nE; e += st) {
         const float q = element_quality(el, kind, pos, e);
         mn = fminf(mn, q);
         sm += (double)q;
@@ -1235,10 +1252,27 @@ k_quality_stats(const int* __restrict__ el, int kind, long nE, const float4* __r
         last = atomicAdd(done, 1u) == QS_BLOCKS - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
+    if (!last) return;
+    // the last block folds the partials: thread t takes t, t + QS_THREADS, ... in order, then a
+    // fixed tree (the same order every run)
+    __threadfence();
+    {
         float a = FLT_MAX; double s = 0.0; int f = 0;
-        for (int i = 0; i < QS_BLOCKS; ++i) { a = fminf(a, ((volatile float*)pmin)[i]); s += ((volatile double*)psum)[i]; f += ((volatile int*)pfail)[i]; }
+        for (int i = threadIdx.x; i < QS_BLOCKS; i += QS_THREADS) {
+            a = fminf(a, ((volatile float*)pmin)[i]); s += ((volatile double*)psum)[i]; f += ((volatile int*)pfail)[i];
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            a = fminf(a, __shfl_xor_sync(FULL, a, o));
+            s += __shfl_xor_sync(FULL, s, o);
+            f += __shfl_xor_sync(FULL, f, o);
+        }
+        if (lane == 0) { smin[w] = a; ssum[w] = s; sfail[w] = f; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float a = smin[0]; double s = ssum[0]; int f = sfail[0];
+        for (int i = 1; i < QS_THREADS / 32; ++i) { a = fminf(a, smin[i]); s += ssum[i]; f += sfail[i]; }
         const int slot = init ? 0 : it + 1;
         stats[slot].min_q = a;
         stats[slot].sum_q = s;
