@@ -195,6 +195,36 @@ def test_surface_restart_rebuilds_state(oracle_mod, vsdmo):
     assert same_bits(gm.positions(), first)
 
 
+@pytest.mark.parametrize("cfg", ["config3_tri", "config3_quad"])
+def test_surface_restart_with_features_replays_bitwise(vsdmo, cfg):
+    """restart() rebuilds the feature state; from the same positions the movable feature
+    vertices and the sector surfaces come out the same, and the captured iterations are kept
+    (they are dropped when either changes). The second run repeats the first bit for bit, and
+    a restart from other positions matches a fresh optimiser started there."""
+    xyz, el = getattr(G, cfg)()
+    tri = cfg.endswith("tri")
+    mcls, ocls = (vsdmo.DMOMeshTri, vsdmo.DMOTriClass) if tri else (vsdmo.DMOMeshQuad, vsdmo.DMOQuadClass)
+    m = mcls(xyz, el)
+    assert m.info["nFeature"] > 0
+    o = ocls(m, n_iter=3)
+    x0 = m.positions()
+    o.optimize()
+    first, h1 = m.positions(), o.history()
+    m.set_positions(x0)
+    o.restart()
+    o.optimize()
+    assert same_bits(m.positions(), first)
+    assert np.array_equal(np.asarray(o.history()), np.asarray(h1))
+    m.set_positions(first)
+    o.restart()
+    o.optimize()
+    m2 = mcls(xyz, el)
+    m2.set_positions(first)
+    o2 = ocls(m2, n_iter=3)
+    o2.optimize()
+    assert same_bits(m.positions(), m2.positions())
+
+
 @pytest.mark.parametrize("cfg,kind,iters", [("config3_tri", TRI, 15), ("config3_quad", QUAD, 15)])
 def test_surface_benchmark_mesh_properties(oracle_mod, vsdmo, cfg, kind, iters):
     """the feature-free variant of the config 3 meshes (the specified noise is covered by

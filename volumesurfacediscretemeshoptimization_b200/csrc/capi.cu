@@ -148,9 +148,9 @@ __global__ void k_surface_state(const float4* pos, int nS, float4* X0, int* nn) 
 
 // The 1D pass only moves the feature vertices whose flag is set (two feature ring vertices at
 // 160 degrees or more); the others return at once. Their ids, class by class, let the pass
-// launch one warp per movable vertex and skip classes without any. A rebuild can change the
-// launch sizes, so captured iterations are dropped.
-void build_feature_movers(vsdmo_opt_s* o) {
+// launch one warp per movable vertex and skip classes without any. Returns whether the set
+// changed (the launch sizes of captured iterations then no longer hold).
+bool build_feature_movers(vsdmo_opt_s* o) {
     const Mesh& m = o->mesh->m;
     cudaStream_t s = m.stream;
     const int nFree = m.nSurf - m.nFeature;
@@ -166,11 +166,13 @@ void build_feature_movers(vsdmo_opt_s* o) {
             if (flags[v - nFree]) ids.push_back(v);
         if ((int)ids.size() > b) o->fmranges.push_back({b, (int)ids.size()});
     }
+    if (o->fmove.p && ids == o->fmove_ids) return false;
+    o->fmove_ids = ids;
     o->fmove.alloc(std::max<size_t>(ids.size(), 1), s);
     if (!ids.empty())
         VSDMO_CUDA(cudaMemcpyAsync(o->fmove.p, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice, s));
     VSDMO_CUDA(cudaStreamSynchronize(s));
-    o->drop_graphs();
+    return true;
 }
 
 // initial positions, normals, local surfaces and nn = identity from the current positions
@@ -199,11 +201,17 @@ void init_surface_state(vsdmo_opt_s* o) {
             o->fopt.alloc(m.nSurf, s);
         }
         init_feature_state(m, o->slide ? 1 : 0, o->LS1.p, o->fdeg.p, o->fopt.p, s);
-        build_feature_movers(o);
+        bool changed = build_feature_movers(o);
         if (surfaces) {
+            const void* before[3] = { o->srow.p, o->stab.p, o->FS.p };
+            const int ns = o->nsect;
             o->nsect = build_sectors(m, o->srow, o->stab, o->FS, s);
+            changed |= o->srow.p != before[0] || o->stab.p != before[1] || o->FS.p != before[2] || o->nsect != ns;
             if (!o->Xs.p) o->Xs.alloc(m.nSurf, s);
         }
+        // captured iterations hold the movers' launch sizes and the sector buffers' addresses;
+        // a restart from the same positions usually rebuilds both unchanged and keeps them
+        if (changed) o->drop_graphs();
     }
 }
 

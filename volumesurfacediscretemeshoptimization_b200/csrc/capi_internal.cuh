@@ -40,6 +40,7 @@ struct vsdmo_opt_s {
     // movable feature vertices (the 1D pass moves them, fopt set), class by class: fmove holds
     // their ids, fmranges[c] the range of class c in it (rebuilt with the flags)
     DBuf<int> fmove;
+    std::vector<int> fmove_ids;                // host copy of fmove
     std::vector<std::pair<int, int>> fmranges;
     DBuf<float4> X0;                           // surface mode: initial surface positions [nSurf]
     DBuf<float4> LS;                           // local surfaces [4 nSurf]
