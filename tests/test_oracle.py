@@ -284,3 +284,40 @@ def test_reference_quality_library_exports():
     if L is None:
         pytest.skip("the reference's quality functions were not built here")
     assert hasattr(L, "refq_eval")
+
+
+def test_learned_reduced_search_properties(oracle_mod):
+    """The oracle's learned search over one colour class (or_dmo_tet_learned_f32), on the CPU:
+    a vertex the reduced search moved did not lower the minimum quality of its ring (its 64
+    candidates are ranked over the 8 critical tets of the centre and the chosen one is accepted
+    on its full ring key); a queued vertex ends exactly where the plain search puts it; the
+    mesh minimum never drops."""
+    xyz, tets = G.tet_cube(8, seed=3)
+    m = oracle_mod.OracleMesh(oracle_mod.TET, xyz, tets)
+    x = m.xyz
+    el = m.arrays()["elems"].reshape(-1, 4)
+    v0, v1 = m.color_ranges()[0]
+    rng = np.random.default_rng(0)
+    Y = (0.02 * rng.standard_normal((v1 - v0, 16))).astype(np.float32)
+    x1, queued = m.dmo_tet_learned_f32(x, v0, v1, Y, rn=4, rdepth=1, rscale=0.0175)
+    plain = m.dmo_color_f32(x, v0, v1)
+    xv, x1v, pv = x.reshape(-1, 3), x1.reshape(-1, 3), plain.reshape(-1, 3)
+    q0, q1 = m.element_qualities_f64(x), m.element_qualities_f64(x1)
+    assert q1.min() >= q0.min()
+    reduced = ~queued
+    assert reduced.sum() > 0 and queued.sum() > 0
+    gain = []
+    for i, v in enumerate(range(v0, v1)):
+        ring = np.flatnonzero((el == v).any(1))
+        if queued[i]:
+            assert np.array_equal(x1v[v], pv[v])
+        else:
+            assert np.any(x1v[v] != xv[v])
+            gain.append(q1[ring].min() - q0[ring].min())
+    gain = np.array(gain)
+    # the f32 key strictly rose; in f64 it may tie within the float rounding of the positions
+    assert gain.min() > -1e-6 and (gain > 0).mean() > 0.9
+    # only this class moved
+    other = np.ones(len(xv), bool)
+    other[v0:v1] = False
+    assert np.array_equal(x1v[other], xv[other])
