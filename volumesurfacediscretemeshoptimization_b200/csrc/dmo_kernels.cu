@@ -270,11 +270,11 @@ unsigned tet_filter(const float4* __restrict__ co, const int (&crit)[TET_CRIT], 
 }
 
 // thr > 0: a candidate survives when every critical tet has det > 0 and det^2 >= thr L^3, tested
-// as min over the tets of det |det| - thr L^3 > 0 -- one running minimum instead of a fraction
-// and a det (det |det| is det^2 for det > 0 and makes the value negative otherwise). det, det^2
-// and L^3 are the values the fraction would be formed from, and the fma rounds det^2 - thr L^3
-// once, so a tet whose key det^2 / L^3 is at least the current key (thr lies 2^-14 of it lower)
-// gives a positive value: every candidate that can beat the current key survives.
+// as min over the tets of min(det, det^2 - thr L^3) > 0 -- one running minimum instead of a
+// fraction and a det. det, det^2 and L^3 are the values the fraction would be formed from, and
+// the fma rounds det^2 - thr L^3 once, so a tet whose key det^2 / L^3 is at least the current
+// key (thr lies 2^-14 of it lower) gives a positive value: every candidate that can beat the
+// current key survives.
 __device__ __forceinline__ unsigned tet_filter_pos(const float4* __restrict__ co, const int (&crit)[TET_CRIT], int m,
                                                    float x, const float* y, const float* z, const float* tz,
                                                    float thr) {
@@ -297,7 +297,7 @@ __device__ __forceinline__ unsigned tet_filter_pos(const float4* __restrict__ co
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
                 const float det = fmaf(K0.z, z[q], detB), L = LB + lz[q];
-                const float v = fmaf(-thr, (L * L) * L, det * fabsf(det));
+                const float v = fminf(det, fmaf(-thr, (L * L) * L, det * det));
                 s[jj][q] = r == 0 ? v : fminf(s[jj][q], v);
             }
         }
